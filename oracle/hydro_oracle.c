@@ -1,0 +1,709 @@
+/*
+ * hydro_oracle.c -- CPU restatement of EMMA's hydro level advance (the oracle).
+ *
+ * TEST INFRASTRUCTURE ONLY.  This is the checker the CUDA path is compared
+ * against; it is never linked into, or called by, the product library.
+ *
+ * It restates, on the reference's own oct-tree memory layout, what
+ * HydroSolver() (src/hydro_utils.c:3378) does for one AMR level:
+ *   gather of the 27-oct neighbourhood      src/hydro_utils.c:2852-3028 (default)
+ *                                           src/hydro_utils.c:2465-2845 (HYDROTEST)
+ *   MUSCL-Hancock predictor                 src/hydro_utils.c:976-1259
+ *   hybrid PVRS/TRRS/TSRS + Newton p*       src/hydro_utils.c:580-777
+ *   HLLC wave speeds and fluxes             src/hydro_utils.c:1264-1399, 1407-2238
+ *   flux-divergence update                  src/hydro_utils.c:3036-3088
+ *   scatter + fine->coarse correction       src/hydro_utils.c:3096-3303
+ *   field := fieldnew, split-cell averaging src/hydro_utils.c:3408-3483
+ * plus clean_new_hydro (:3501), L_comptstep_hydro (src/advanceamr.c:92) and the
+ * hydro-only subset of Advance_level (src/advanceamr.c:243-1299).
+ *
+ * Every floating-point expression keeps the reference's operation order so the
+ * results are bit-identical when both are built with gcc -O2 -ffp-contract=off
+ * (checked in tests/test_oracle_pin.py).  Differences in organisation, all
+ * value-preserving: MUSCL face states of a stencil cell are computed once per
+ * target oct and reused (the reference recomputes identical values up to 9
+ * times); the reference's abort() calls become error bits.
+ */
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "hydro_oracle.h"
+
+#define GAM (5. / 3.)     /* GAMMA, src/param.h:4 */
+#define P_MIN (1e-10)     /* PMIN,  src/param.h:20 */
+#define DEF_DENS 10.      /* DEFDENS, src/hydro_utils.c:19 */
+#define N_ITER_MAX 10     /* NITERMAX, src/hydro_utils.c:17 */
+#define ERR_TOL 1e-10     /* ERRTOL, src/hydro_utils.c:18 */
+
+/* ---- memory layout of the reference tree (src/prototypes.h:611,825,1028) */
+typedef struct { double d, u, v, w, p, a, E; } oW;      /* struct Wtype */
+typedef struct { double d, du, dv, dw, E, eint; } oU;  /* struct Utype */
+struct oOct;
+typedef struct oCell {
+  struct oOct *child;
+  double marked;
+  int idx;
+  oW field;
+  oW fieldnew;
+} oCell;
+typedef struct oOct {
+  oCell cell[8];
+  oCell *nei[6];
+  oCell *parent;
+  struct oOct *next, *prev, *nexthash;
+  double x, y, z;
+  int cpu;
+  int level;
+} oOct;
+_Static_assert(sizeof(oCell) == 136, "CELL layout");
+_Static_assert(sizeof(oOct) == 1200, "OCT layout");
+
+static int g_err = 0;
+static long long g_updates = 0;
+
+long long orc_cell_updates(void) { return g_updates; }
+void orc_reset_counters(void) { g_updates = 0; }
+int orc_sizeof_oct(void) { return (int)sizeof(oOct); }
+
+static oOct *oct_of(oCell *c) { return (oOct *)((char *)c - (size_t)c->idx * sizeof(oCell)); }
+
+/* Face neighbour of cell `ic` (icell = ix + 2 iy + 4 iz) in direction k
+ * (0:-x 1:+x 2:-y 3:+y 4:-z 5:+z), the mapping of getcellnei (src/oct.c:116):
+ * *same = 1 if inside the oct, else the neighbour is in the oct across face k. */
+static void cell_nei(int ic, int k, int *same, int *nc) {
+  int axis = k >> 1, bit = 1 << axis, plus = k & 1;
+  int inside = plus ? !(ic & bit) : (ic & bit);
+  *same = inside ? 1 : 0;
+  *nc = ic ^ bit;
+}
+
+/* ---------------------------------------------- primitives (src/hydro_utils.c:29-89) */
+static void get_E(oW *W) {
+  W->E = W->p / (GAM - 1.) + 0.5 * W->d * (W->u * W->u + W->v * W->v + W->w * W->w);
+}
+static void to_cons(const oW *W, oU *U) {
+  U->d = W->d;
+  U->du = W->d * W->u;
+  U->dv = W->d * W->v;
+  U->dw = W->d * W->w;
+  U->eint = W->p / (GAM - 1.);
+  U->E = W->E;
+}
+static void to_prim(const oU *U, oW *W) {
+  double dl = (U->d == 0. ? DEF_DENS : U->d);
+  W->d = U->d;
+  W->u = U->du / dl;
+  W->v = U->dv / dl;
+  W->w = U->dw / dl;
+  W->p = (GAM - 1.) * (U->E - ((U->du) * (U->du) + (U->dv) * (U->dv) + (U->dw) * (U->dw)) / (dl)*0.5);
+  W->E = U->E;
+  W->a = sqrt(GAM * W->p / dl);
+}
+
+/* ---------------------------------------------- MUSCL-Hancock (src/hydro_utils.c:201-269, 976-1259) */
+static double limit1(double m, double p) {
+  /* minmod_W with beta = 1 */
+  if (p > 0) return fmax(fmax(0., fmin(m, p)), fmin(m, p));
+  return fmin(fmin(0., fmax(m, p)), fmax(m, p));
+}
+
+/* primitive 5-vectors: 0:d 1:u 2:v 3:w 4:p */
+static void as5(const oW *W, double q[5]) { q[0] = W->d; q[1] = W->u; q[2] = W->v; q[3] = W->w; q[4] = W->p; }
+
+/* Half-step predictor -dt/(2dx) (A Dx + B Dy + C Dz) in primitive variables,
+ * matrix_jacobian (src/hydro_utils.c:976).  The non-zero entries are added in
+ * the reference's column order; skipped zero entries only ever add +-0. */
+static void predictor(const oW *W0, double dt, double dx, double D[3][5], double Wt[5]) {
+  double acc[5] = {0., 0., 0., 0., 0.};
+  double vel[3] = {W0->u, W0->v, W0->w};
+  double daa = W0->d * W0->a * W0->a;
+  double id = 1. / W0->d;
+  int dir, i;
+  for (dir = 0; dir < 3; dir++) {
+    double s = vel[dir];
+    /* column 0 */
+    acc[0] += s * D[dir][0];
+    /* column 1 */
+    if (dir == 0) acc[0] += W0->d * D[dir][1];
+    acc[1] += s * D[dir][1];
+    if (dir == 0) acc[4] += daa * D[dir][1];
+    /* column 2 */
+    if (dir == 1) acc[0] += W0->d * D[dir][2];
+    acc[2] += s * D[dir][2];
+    if (dir == 1) acc[4] += daa * D[dir][2];
+    /* column 3 */
+    if (dir == 2) acc[0] += W0->d * D[dir][3];
+    acc[3] += s * D[dir][3];
+    if (dir == 2) acc[4] += daa * D[dir][3];
+    /* column 4 */
+    acc[1 + dir] += id * D[dir][4];
+    acc[4] += s * D[dir][4];
+  }
+  for (i = 0; i < 5; i++) Wt[i] = acc[i] * (-dt / dx * 0.5);
+}
+
+/* ---------------------------------------------- per-oct stencil */
+typedef struct {
+  oW w[27][8];
+  char split[27][8];
+  /* memoised MUSCL face states, 6 per stencil cell */
+  oW face[27][8][6];
+  char done[27][8];
+} Stencil;
+
+static const int SLOT_OFF[6] = {-1, 1, -3, 3, -9, 9};
+static const int FACE_SLOT[7] = {12, 14, 10, 16, 4, 22, 13};
+
+/* MUSCL_BOUND2 on stencil cell (slot, ic): fills st->face[slot][ic][0..5]. */
+static void muscl_cell(Stencil *st, int slot, int ic, double dt, double dx) {
+  const oW *W0 = &st->w[slot][ic];
+  double q0[5], D[3][5], Wt[5];
+  static const double fx[6] = {-0.5, 0.5, 0.0, 0.0, 0.0, 0.0};
+  static const double fy[6] = {0.0, 0.0, -0.5, 0.5, 0.0, 0.0};
+  static const double fz[6] = {0.0, 0.0, 0.0, 0.0, -0.5, 0.5};
+  int dir, k, f;
+  as5(W0, q0);
+  for (dir = 0; dir < 3; dir++) {
+    int same, nc;
+    double qm[5], qp[5];
+    cell_nei(ic, 2 * dir, &same, &nc);
+    as5(&st->w[same ? slot : slot + SLOT_OFF[2 * dir]][nc], qm);
+    cell_nei(ic, 2 * dir + 1, &same, &nc);
+    as5(&st->w[same ? slot : slot + SLOT_OFF[2 * dir + 1]][nc], qp);
+    for (k = 0; k < 5; k++) D[dir][k] = limit1(q0[k] - qm[k], qp[k] - q0[k]);
+  }
+  predictor(W0, dt, dx, D, Wt);
+  for (f = 0; f < 6; f++) {
+    oW *Wi = &st->face[slot][ic][f];
+    double r[5];
+    for (k = 0; k < 5; k++) r[k] = q0[k] + fx[f] * D[0][k] + fy[f] * D[1][k] + fz[f] * D[2][k] + Wt[k];
+    Wi->d = r[0]; Wi->u = r[1]; Wi->v = r[2]; Wi->w = r[3];
+    Wi->p = fmax(r[4], P_MIN);
+    if (Wi->d < 0) g_err |= ORC_ERR_NEG_DENSITY;
+    get_E(Wi);
+    Wi->a = sqrt(GAM * Wi->p / Wi->d);
+  }
+  st->done[slot][ic] = 1;
+}
+
+static const oW *face_state(Stencil *st, int slot, int ic, int f, double dt, double dx) {
+  if (!st->done[slot][ic]) muscl_cell(st, slot, ic, dt, dx);
+  return &st->face[slot][ic][f];
+}
+
+/* ---------------------------------------------- Riemann solvers (src/hydro_utils.c:580-777) */
+typedef struct { double d, u, p, a; } oW1;
+
+static double f_root_prime(double p, const oW1 *L, const oW1 *R) {
+  double AL = 2. / ((GAM + 1.) * L->d), AR = 2. / ((GAM + 1.) * R->d);
+  double BL = (GAM - 1.) / (GAM + 1.) * L->p, BR = (GAM - 1.) / (GAM + 1.) * R->p;
+  double fL = (p > L->p ? sqrt(AL / (BL + p)) * (1. - (p - L->p) / (2. * (BL + p)))
+                        : pow(p / L->p, -(GAM + 1) / (2. * GAM)) / (L->d * L->a));
+  double fR = (p > R->p ? sqrt(AR / (BR + p)) * (1. - (p - R->p) / (2. * (BR + p)))
+                        : pow(p / R->p, -(GAM + 1) / (2. * GAM)) / (R->d * R->a));
+  return fL + fR;
+}
+
+static double f_root(double p, const oW1 *L, const oW1 *R, double *u) {
+  double AL = 2. / ((GAM + 1.) * L->d), AR = 2. / ((GAM + 1.) * R->d);
+  double BL = (GAM - 1.) / (GAM + 1.) * L->p, BR = (GAM - 1.) / (GAM + 1.) * R->p;
+  double fL = (p > L->p ? (p - L->p) * sqrt(AL / (BL + p))
+                        : 2. * L->a / (GAM - 1.) * (pow(p / L->p, (GAM - 1) / (2. * GAM)) - 1.));
+  double fR = (p > R->p ? (p - R->p) * sqrt(AR / (BR + p))
+                        : 2. * R->a / (GAM - 1.) * (pow(p / R->p, (GAM - 1) / (2. * GAM)) - 1.));
+  double du = R->u - L->u;
+  *u = 0.5 * (L->u + R->u) + 0.5 * (fR - fL);
+  return fL + fR + du;
+}
+
+/* findPressure_Hybrid (src/hydro_utils.c:625) */
+static double p_star_hybrid(const oW1 *L, const oW1 *R, double *ustar) {
+  double dbar = 0.5 * (L->d + R->d), abar = 0.5 * (L->a + R->a);
+  double ppvrs = 0.5 * ((L->p + R->p) + (L->u - R->u) * dbar * abar);
+  double pmax = fmax(L->p, R->p), pmin = fmin(L->p, R->p);
+  double pstar = ppvrs;
+  if (((pmax / pmin) < 2.) && ((pmin < pstar) && (pstar < pmax))) {
+    *ustar = 0.5 * ((L->u + R->u) + (L->p - R->p) / (dbar * abar));
+  } else if (pstar < pmin) {
+    double z = (GAM - 1.) / (2. * GAM);
+    double iz = (2. * GAM) / (GAM - 1.);
+    pstar = pow((L->a + R->a - (GAM - 1.) / 2. * (R->u - L->u)) / (L->a / pow(L->p, z) + R->a / pow(R->p, z)), iz);
+    *ustar = L->u - 2. * L->a / (GAM - 1.) * (pow(pstar / L->p, z) - 1.);
+  } else {
+    double p0 = fmax(0., ppvrs);
+    double AL = 2. / ((GAM + 1.) * L->d), AR = 2. / ((GAM + 1.) * R->d);
+    double BL = (GAM - 1.) / (GAM + 1.) * L->p, BR = (GAM - 1.) / (GAM + 1.) * R->p;
+    double GL = sqrt(AL / (p0 + BL)), GR = sqrt(AR / (p0 + BR));
+    pstar = (GL * L->p + GR * R->p - (R->u - L->u)) / (GL + GR);
+    *ustar = 0.5 * ((L->u + R->u) + (pstar - R->p) * GR - (pstar - L->p) * GL);
+  }
+  return pstar;
+}
+
+/* findPressure (src/hydro_utils.c:680): Newton iteration on the exact solver */
+static double p_star_exact(const oW1 *L, const oW1 *R, double *u) {
+  double unsurz = (2.0 * GAM) / (GAM - 1.0);
+  double pmin = fmin(L->p, R->p), pmax = fmax(L->p, R->p);
+  double AL = 2. / ((GAM + 1.) * L->d), AR = 2. / ((GAM + 1.) * R->d);
+  double BL = (GAM - 1.) / (GAM + 1.) * L->p, BR = (GAM - 1.) / (GAM + 1.) * R->p;
+  double ppv0 = 0.5 * (L->p + R->p) - 0.125 * (R->u - L->u) * (R->d + L->d) * (R->a + L->a);
+  double ptr0 = pow((L->a + R->a - 0.5 * (GAM - 1) * (R->u - L->u)) /
+                        (L->a / pow(L->p, 1. / unsurz) + R->a / pow(R->p, 1. / unsurz)),
+                    unsurz);
+  double ppv = fmax(ERR_TOL, ppv0), ptr = fmax(ERR_TOL, ptr0);
+  double GL = sqrt(AL / (ppv + BL)), GR = sqrt(AR / (ppv + BR));
+  double pts0 = (GL * L->p + GR * R->p - (R->u - L->u)) / (GL + GR);
+  double pts = fmax(ERR_TOL, pts0);
+  double p, dp, porg, err, u2;
+  int i;
+  if (((pmax / pmin) < 2.0) && ((pmin <= ppv) && (ppv <= pmax))) p = ppv;
+  else if (ppv < pmin) p = ptr;
+  else p = pts;
+  for (i = 0; i < N_ITER_MAX; i++) {
+    dp = f_root(p, L, R, &u2) / f_root_prime(p, L, R);
+    if (isnan(dp)) { g_err |= ORC_ERR_NAN; break; }
+    if (fabs(dp) < ERR_TOL) break;
+    while ((p - dp) < 0) dp = dp * 0.5;
+    porg = p;
+    p = p - dp;
+    err = 2. * fabs(p - porg) / (fabs(p + porg));
+    if (err < ERR_TOL) break;
+    if (f_root(p, L, R, &u2) < ERR_TOL) break;
+  }
+  f_root(p, L, R, &u2);
+  *u = u2;
+  return p;
+}
+
+/* speedestimate{X,Y,Z}_HLLC (src/hydro_utils.c:1264): normal velocity index n */
+static void wave_speeds(const oW *WL, const oW *WR, int n, double *SL, double *SR, double *ustar) {
+  oW1 L, R;
+  double pstar, qL, qR;
+  double vl[3] = {WL->u, WL->v, WL->w}, vr[3] = {WR->u, WR->v, WR->w};
+  L.d = WL->d; L.u = vl[n]; L.p = WL->p; L.a = sqrt(GAM * L.p / L.d);
+  R.d = WR->d; R.u = vr[n]; R.p = WR->p; R.a = sqrt(GAM * R.p / R.d);
+  pstar = p_star_hybrid(&L, &R, ustar);
+  if (pstar < 0) pstar = p_star_exact(&L, &R, ustar);
+  if (pstar < 0) g_err |= ORC_ERR_NEG_PSTAR;
+  qL = (pstar <= WL->p ? 1. : sqrt(1. + (GAM + 1.) / (2. * GAM) * ((pstar) / WL->p - 1.)));
+  qR = (pstar <= WR->p ? 1. : sqrt(1. + (GAM + 1.) / (2. * GAM) * ((pstar) / WR->p - 1.)));
+  *SL = L.u - L.a * qL;
+  *SR = R.u + R.a * qR;
+  if ((*SL) > (*SR)) {
+    *SL = fmin(L.u - L.a, R.u - R.a);
+    *SR = fmax(L.u + L.a, R.u + R.a);
+  }
+  if ((*SL) > (*SR)) g_err |= ORC_ERR_SLSR;
+  if (isnan(*ustar)) g_err |= ORC_ERR_NAN;
+}
+
+/* Euler flux along axis n of a conserved state, getflux_{X,Y,Z} (src/hydro_utils.c:916-968).
+ * m[] are the momenta, t1/t2 the transverse momentum indices in the order the
+ * reference sums them. */
+static void euler_flux(const oU *U, int n, double f[5]) {
+  double m[3] = {U->du, U->dv, U->dw};
+  double mn = m[n];
+  int t1 = (n == 0) ? 1 : 0, t2 = (n == 2) ? 1 : 2;
+  double all = U->du * U->du + U->dv * U->dv + U->dw * U->dw;
+  f[0] = mn;
+  f[1 + n] = 0.5 * (3. - GAM) * mn * mn / U->d + (GAM - 1.) * U->E - 0.5 * (GAM - 1.) * (m[t1] * m[t1] + m[t2] * m[t2]) / U->d;
+  f[1 + t1] = mn * m[t1] / U->d;
+  f[1 + t2] = mn * m[t2] / U->d;
+  f[4] = GAM * mn / U->d * U->E - 0.5 * (GAM - 1.) * mn / (U->d * U->d) * all;
+}
+
+/* HLLC flux across a face normal to axis n from left/right MUSCL states
+ * (src/hydro_utils.c:2055-2138, same branches for y :1783, z :1508). */
+static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5]) {
+  double SL, SR, ustar;
+  oU UL, UR;
+  int k;
+  for (k = 0; k < 5; k++) F[k] = 0.;
+  wave_speeds(WL, WR, n, &SL, &SR, &ustar);
+  to_cons(WL, &UL);
+  to_cons(WR, &UR);
+  if (SL >= 0.) {
+    euler_flux(&UL, n, F);
+  } else if (SR <= 0.) {
+    euler_flux(&UR, n, F);
+  } else if ((SL < 0.) && (ustar >= 0.)) {
+    const oW *W = WL;
+    const oU *U = &UL;
+    double vel[3] = {W->u, W->v, W->w}, mom[3] = {U->du, U->dv, U->dw};
+    double un = vel[n], fact;
+    euler_flux(U, n, F);
+    fact = W->d * (SL - un) / (SL - ustar);
+    F[0] += (fact * 1. - U->d) * SL;
+    for (k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : vel[k]) - mom[k]) * SL;
+    F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SL - un)))) - U->E) * SL;
+  } else if ((ustar <= 0.) && (SR > 0.)) {
+    const oW *W = WR;
+    const oU *U = &UR;
+    double vel[3] = {W->u, W->v, W->w}, mom[3] = {U->du, U->dv, U->dw};
+    double un = vel[n], fact;
+    euler_flux(U, n, F);
+    fact = W->d * (SR - un) / (SR - ustar);
+    F[0] += (fact * 1. - U->d) * SR;
+    for (k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : vel[k]) - mom[k]) * SR;
+    F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SR - un)))) - U->E) * SR;
+  }
+}
+
+/* ---------------------------------------------- gather (src/hydro_utils.c:2852-3028 / 2465-2845) */
+static int flag_on(int flags, int f) { return (flags & f) != 0; }
+
+/* coarse2fine_hydro2 (src/hydro_utils.c:311): limited-slope interpolation of a
+ * coarse leaf cell into 8 sub-cell states (HYDROTEST gather only). */
+static void interp_coarse(oCell *cell, oW Wi[8], int flags) {
+  oOct *oct = oct_of(cell);
+  double dxcur = pow(0.5, oct->level);
+  double q0[5], D[3][5];
+  const oW *W0 = &cell->field;
+  const oW *Wm = NULL, *Wp = NULL;
+  int dir, k, ix, iy, iz;
+  as5(W0, q0);
+  for (dir = 0; dir < 3; dir++) {
+    int same, nc;
+    double qm[5], qp[5];
+    cell_nei(cell->idx, 2 * dir, &same, &nc);
+    if (same) Wm = &oct->cell[nc].field;
+    else if (oct->nei[2 * dir] != NULL && oct->nei[2 * dir]->child != NULL) Wm = &oct->nei[2 * dir]->child->cell[nc].field;
+    if (flag_on(flags, ORC_TRANSXM) && oct->x == 0. && dir == 0) Wm = &cell->field;
+    if (flag_on(flags, ORC_TRANSYM) && oct->y == 0. && dir == 1) Wm = &cell->field;
+    if (flag_on(flags, ORC_TRANSZM) && oct->z == 0. && dir == 2) Wm = &cell->field;
+    cell_nei(cell->idx, 2 * dir + 1, &same, &nc);
+    if (same) Wp = &oct->cell[nc].field;
+    else if (oct->nei[2 * dir + 1] != NULL && oct->nei[2 * dir + 1]->child != NULL) Wp = &oct->nei[2 * dir + 1]->child->cell[nc].field;
+    if (flag_on(flags, ORC_TRANSXP) && (oct->x + 2. * dxcur) == 1. && dir == 0) Wp = &cell->field;
+    if (flag_on(flags, ORC_TRANSYP) && (oct->y + 2. * dxcur) == 1. && dir == 1) Wp = &cell->field;
+    if (flag_on(flags, ORC_TRANSZP) && (oct->z + 2. * dxcur) == 1. && dir == 2) Wp = &cell->field;
+    if (Wm == NULL || Wp == NULL) { g_err |= ORC_ERR_TREE; Wm = Wp = W0; }
+    as5(Wm, qm);
+    as5(Wp, qp);
+    for (k = 0; k < 5; k++) D[dir][k] = limit1(q0[k] - qm[k], qp[k] - q0[k]);
+  }
+  for (iz = 0; iz < 2; iz++)
+    for (iy = 0; iy < 2; iy++)
+      for (ix = 0; ix < 2; ix++) {
+        double ox = -0.25 + ix * 0.5, oy = -0.25 + iy * 0.5, oz = -0.25 + iz * 0.5;
+        double r[5];
+        oW *W = &Wi[ix + 2 * iy + 4 * iz];
+        for (k = 0; k < 5; k++) r[k] = q0[k] + ox * D[0][k] + oy * D[1][k] + oz * D[2][k];
+        W->d = r[0]; W->u = r[1]; W->v = r[2]; W->w = r[3]; W->p = r[4];
+        get_E(W);
+        W->a = sqrt(GAM * W->p / W->d);
+      }
+}
+
+/* mirror maps of the transmissive ghost octs (src/hydro_utils.c:2504-2610) */
+static const int MIRROR[6][8] = {
+    {0, 0, 2, 2, 4, 4, 6, 6}, /* -x */
+    {1, 1, 3, 3, 5, 5, 7, 7}, /* +x */
+    {0, 1, 0, 1, 4, 5, 4, 5}, /* -y */
+    {2, 3, 2, 3, 7, 6, 6, 7}, /* +y (as in the reference, cells 4/5 swapped) */
+    {0, 1, 2, 3, 0, 1, 2, 3}, /* -z */
+    {4, 5, 6, 7, 4, 5, 6, 7}, /* +z */
+};
+static const int TFLAG[6] = {ORC_TRANSXM, ORC_TRANSXP, ORC_TRANSYM, ORC_TRANSYP, ORC_TRANSZM, ORC_TRANSZP};
+
+static int at_boundary(const oOct *o, int k) {
+  double dx = pow(0.5, o->level);
+  switch (k) {
+    case 0: return o->x == 0.;
+    case 1: return (o->x + 2. * dx) == 1.;
+    case 2: return o->y == 0.;
+    case 3: return (o->y + 2. * dx) == 1.;
+    case 4: return o->z == 0.;
+    default: return (o->z + 2. * dx) == 1.;
+  }
+}
+
+/* One step of the recursive neighbour walk: from the level-(L-1) cell `cell`,
+ * find the level-(L-1) cell across direction k, fill stencil slot `slot`, and
+ * return that cell (the start of the next order of the walk). */
+static oCell *fill_slot(Stencil *st, int slot, oCell *cell, int k, int flags) {
+  oCell *nc = NULL;
+  const int *map = NULL;
+  oW Wi[8];
+  char ch[8];
+  int c;
+  int hydrotest = flag_on(flags, ORC_HYDROTEST);
+  if (cell->child != NULL) {
+    nc = cell->child->nei[k];
+    if (hydrotest && flag_on(flags, TFLAG[k]) && at_boundary(cell->child, k)) {
+      nc = cell;
+      map = MIRROR[k];
+    }
+  } else {
+    int same, vc;
+    oOct *oct = oct_of(cell);
+    cell_nei(cell->idx, k, &same, &vc);
+    if (same) {
+      nc = &oct->cell[vc];
+    } else {
+      if (oct->nei[k] != NULL && oct->nei[k]->child != NULL) nc = &oct->nei[k]->child->cell[vc];
+      if (hydrotest && flag_on(flags, TFLAG[k]) && at_boundary(oct, k)) {
+        nc = cell;
+        map = MIRROR[k];
+      }
+    }
+  }
+  if (nc == NULL) { g_err |= ORC_ERR_TREE; return NULL; }
+  if (nc->child != NULL) {
+    for (c = 0; c < 8; c++) { Wi[c] = nc->child->cell[c].field; ch[c] = (nc->child->cell[c].child != NULL); }
+  } else {
+    if (hydrotest) interp_coarse(nc, Wi, flags);
+    else for (c = 0; c < 8; c++) Wi[c] = nc->field;
+    for (c = 0; c < 8; c++) ch[c] = 0;
+  }
+  for (c = 0; c < 8; c++) {
+    int s = map ? map[c] : c;
+    st->w[slot][c] = Wi[s];
+    st->split[slot][c] = ch[s];
+  }
+  return nc;
+}
+
+/* recursive_neighbor_gather_oct (src/hydro_utils.c:2852): fill `slot` from the
+ * level-(L-1) cell across direction `k` of `cell`; order 1 (faces) recurses to
+ * order 2 (edges) in the directions off the first axis, order 2 to order 3
+ * (corners) off both axes.  Slots already visited are skipped, so the walk
+ * order decides which path fills an edge/corner slot, as in the reference. */
+static void walk(Stencil *st, char *visit, int slot, int i1, int i2, int order, int k, oCell *cell, int flags) {
+  int i;
+  oCell *nc = fill_slot(st, slot, cell, k, flags);
+  if (nc == NULL || order == 3) return;
+  for (i = 0; i < 6; i++) {
+    int s2;
+    if ((i >> 1) == (i1 >> 1)) continue;
+    if (order == 2 && (i >> 1) == (i2 >> 1)) continue;
+    s2 = slot + SLOT_OFF[i];
+    if (visit[s2]) continue;
+    visit[s2] = 1;
+    walk(st, visit, s2, i1, order == 1 ? i : i2, order + 1, i, nc, flags);
+  }
+}
+
+static void gather(Stencil *st, oOct *o, int flags) {
+  char visit[27];
+  int c, k;
+  memset(visit, 0, sizeof(visit));
+  memset(st->done, 0, sizeof(st->done));
+  for (c = 0; c < 8; c++) {
+    st->w[13][c] = o->cell[c].field;
+    st->split[13][c] = (o->cell[c].child != NULL);
+  }
+  visit[13] = 1;
+  for (k = 0; k < 6; k++) {
+    int slot = 13 + SLOT_OFF[k];
+    visit[slot] = 1;
+    walk(st, visit, slot, k, -1, 1, k, o->parent, flags);
+  }
+}
+
+/* ---------------------------------------------- level advance */
+static Stencil g_st;
+
+int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
+  oOct **firstoct = (oOct **)firstoct_v;
+  double dx = pow(0.5, level);
+  double dtsurdx = dt / dx;
+  oOct *o;
+  int c, k, n = 0;
+  g_err = 0;
+  for (o = firstoct[level - 1]; o != NULL; o = o->next) {
+    double flux[8][6][5];
+    if (o->cpu != 0) continue;
+    n++;
+    gather(&g_st, o, flags);
+    /* sweeps x, y, z: two faces per cell per direction, split neighbours cancelled */
+    for (c = 0; c < 8; c++) {
+      int dir;
+      for (dir = 0; dir < 3; dir++) {
+        int s;
+        for (s = 0; s < 2; s++) {
+          int kf = 2 * dir + s, same, vc, nslot;
+          const oW *Wc, *Wn;
+          double F[5];
+          cell_nei(c, kf, &same, &vc);
+          nslot = same ? 13 : FACE_SLOT[kf];
+          Wc = face_state(&g_st, 13, c, kf, dt, dx);
+          Wn = face_state(&g_st, nslot, vc, kf ^ 1, dt, dx);
+          if (s == 0) hllc_flux(Wn, Wc, dir, F);
+          else hllc_flux(Wc, Wn, dir, F);
+          for (k = 0; k < 5; k++) flux[c][kf][k] = F[k] * (double)(!g_st.split[nslot][vc]);
+        }
+      }
+    }
+    /* updatefield + scatterstencil, cell by cell in order */
+    for (c = 0; c < 8; c++) {
+      oCell *cell = &o->cell[c];
+      if (!g_st.split[13][c]) {
+        oU dU = {0., 0., 0., 0., 0., 0.}, U;
+        double one = 1., ekin;
+        int f;
+        for (f = 0; f < 6; f++) {
+          dU.d += flux[c][f][0] * dtsurdx * one;
+          dU.du += flux[c][f][1] * dtsurdx * one;
+          dU.dv += flux[c][f][2] * dtsurdx * one;
+          dU.dw += flux[c][f][3] * dtsurdx * one;
+          dU.E += flux[c][f][4] * dtsurdx * one;
+          one *= -1.;
+        }
+        if (isnan(cell->fieldnew.u)) g_err |= ORC_ERR_NAN;
+        to_cons(&cell->fieldnew, &U);
+        U.d += dU.d;
+        U.du += dU.du;
+        U.dv += dU.dv;
+        U.dw += dU.dw;
+        U.E += dU.E;
+        ekin = 0.5 * (U.du * U.du + U.dv * U.dv + U.dw * U.dw) / U.d;
+        U.eint = U.E - ekin;
+        U.eint = fmax(U.eint * (GAM - 1.), P_MIN) / (GAM - 1.);
+        to_prim(&U, &cell->fieldnew);
+        cell->fieldnew.p = fmax(cell->fieldnew.p, P_MIN);
+        cell->fieldnew.a = sqrt(GAM * cell->fieldnew.p / cell->fieldnew.d);
+        get_E(&cell->fieldnew);
+        if (isnan(cell->fieldnew.u)) g_err |= ORC_ERR_NAN;
+      }
+      /* fine -> coarse flux correction into unsplit coarse neighbours */
+      for (k = 0; k < 6; k++) {
+        int same, vc;
+        oCell *cc;
+        if (flag_on(flags, TFLAG[k]) && at_boundary(o, k)) continue;
+        cell_nei(c, k, &same, &vc);
+        if (same) continue;
+        cc = o->nei[k];
+        if (cc != NULL && cc->child == NULL) {
+          oW W = cc->fieldnew;
+          oU U;
+          int one = (k & 1) ? 1 : -1; /* (int)POW(-1., k+1) */
+          to_cons(&W, &U);
+          U.d += flux[c][k][0] * dtsurdx * one * 0.125;
+          U.du += flux[c][k][1] * dtsurdx * one * 0.125;
+          U.dv += flux[c][k][2] * dtsurdx * one * 0.125;
+          U.dw += flux[c][k][3] * dtsurdx * one * 0.125;
+          U.E += flux[c][k][4] * dtsurdx * one * 0.125;
+          to_prim(&U, &W);
+          cc->fieldnew = W;
+        }
+      }
+    }
+  }
+  /* field := fieldnew (leaves); split cells := mean of children's primitives */
+  if (n > 0) {
+    for (o = firstoct[level - 1]; o != NULL; o = o->next) {
+      for (c = 0; c < 8; c++) {
+        oCell *cell = &o->cell[c];
+        if (cell->child == NULL) {
+          cell->field = cell->fieldnew;
+          g_updates++;
+        } else {
+          oW W;
+          int i;
+          memset(&W, 0, sizeof(W));
+          for (i = 0; i < 8; i++) {
+            const oW *Wc = &cell->child->cell[i].field;
+            W.d += Wc->d * 0.125;
+            W.u += Wc->u * 0.125;
+            W.v += Wc->v * 0.125;
+            W.w += Wc->w * 0.125;
+            W.p += Wc->p * 0.125;
+          }
+          get_E(&W);
+          cell->field = W;
+        }
+      }
+    }
+  }
+  return g_err;
+}
+
+void orc_clean_new_hydro(void **firstoct_v, int level) {
+  oOct **firstoct = (oOct **)firstoct_v;
+  oOct *o;
+  int c;
+  for (o = firstoct[level - 1]; o != NULL; o = o->next)
+    for (c = 0; c < 8; c++) o->cell[c].fieldnew = o->cell[c].field;
+}
+
+/* L_comptstep_hydro (src/advanceamr.c:92), over every cell of the level */
+double orc_comptstep_hydro(void **firstoct_v, int level, double cfl) {
+  oOct **firstoct = (oOct **)firstoct_v;
+  double dt = 1e9, smax = 0., dxcur = pow(0.5, level);
+  oOct *o;
+  int c;
+  for (o = firstoct[level - 1]; o != NULL; o = o->next) {
+    if (o->cpu != 0) continue;
+    for (c = 0; c < 8; c++) {
+      const oW *W = &o->cell[c].field;
+      double va = sqrt(W->u * W->u + W->v * W->v + W->w * W->w);
+      double aa = sqrt(GAM * W->p / W->d);
+      smax = fmax(smax, va + aa);
+    }
+  }
+  if (smax > 0.) dt = fmin(dxcur * cfl / (smax * 3.), dt);
+  return dt;
+}
+
+/* ---------------------------------------------- level schedule (src/advanceamr.c:243-1299) */
+typedef struct {
+  oOct **first;
+  int lcoarse, lmax, nsub, flags;
+  double dt_param, time_max, cfl;
+  double *adt;
+  int err;
+} Sched;
+
+static int level_noct(oOct **first, int level) {
+  int n = 0;
+  oOct *o;
+  for (o = first[level - 1]; o != NULL; o = o->next) n++;
+  return n;
+}
+
+static double advance_level(Sched *S, int level, double tloc) {
+  double dt = 0., dtnew, dthydro, dtfine;
+  double *adt = S->adt;
+  int is = 0;
+  do {
+    orc_clean_new_hydro((void **)S->first, level);
+    dtnew = S->dt_param;
+    dtnew = ((S->time_max - tloc) < dtnew ? (S->time_max - tloc) : dtnew);
+    dthydro = orc_comptstep_hydro((void **)S->first, level, S->cfl);
+    dtnew = (dthydro < dtnew ? dthydro : dtnew);
+    adt[level - 1] = dtnew;
+    if (level == S->lcoarse) adt[level - 2] = adt[level - 1];
+    if (adt[level - 2] < adt[level - 1]) adt[level - 1] = adt[level - 2];
+    else adt[level - 1] = fmin(adt[level - 1], adt[level - 2] - dt);
+    if (level < S->lmax && level_noct(S->first, level + 1) > 0) {
+      dtfine = advance_level(S, level + 1, tloc);
+      adt[level - 1] = dtfine;
+      if (level == S->lcoarse) adt[level - 2] = adt[level - 1];
+    }
+    S->err |= orc_hydro_solver((void **)S->first, level, adt[level - 1], S->flags);
+    dt += adt[level - 1];
+    tloc += adt[level - 1];
+    is++;
+  } while ((dt < adt[level - 2]) && (is < S->nsub));
+  return dt;
+}
+
+double orc_run(void **firstoct, int lcoarse, int lmax, int nsteps, double dt_param,
+               double time_max, int nsub, double cfl, int flags, double tsim0,
+               double *adt, int *steps_done, int *err) {
+  Sched S;
+  int n, l;
+  double tsim = tsim0;
+  S.first = (oOct **)firstoct;
+  S.lcoarse = lcoarse; S.lmax = lmax; S.nsub = nsub; S.flags = flags;
+  S.dt_param = dt_param; S.time_max = time_max; S.cfl = cfl; S.adt = adt; S.err = 0;
+  for (l = 1; l <= lmax; l++) adt[l - 1] = dt_param;
+  for (n = 0; n < nsteps && tsim < time_max; n++) {
+    advance_level(&S, lcoarse, tsim);
+    tsim += adt[lcoarse - 1];
+  }
+  if (steps_done) *steps_done = n;
+  if (err) *err = S.err;
+  return tsim;
+}

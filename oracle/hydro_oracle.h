@@ -1,0 +1,53 @@
+/*
+ * hydro_oracle.h -- CPU restatement of EMMA's hydro level advance.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker).  Only tests/, __graft_entry__.smoke()
+ * and bench.py's cpu_baseline / reference arm may load liboracle.so.  The
+ * product library (libemmahydro.so) never links or calls it.
+ *
+ * The restatement works in place on an oct tree laid out like the reference's
+ * `struct OCT` built with -DWHYDRO2 -DRIEMANN_HLLC -DPRIMITIVE, REAL=double,
+ * NVAR=6 (src/prototypes.h:611,825,1028): 1200 bytes per oct.  It is pinned
+ * bit-for-bit against the reference compiled from its own sources
+ * (oracle/_ref, see oracle/Makefile and tests/test_oracle_pin.py).
+ */
+#ifndef EMMA_HYDRO_ORACLE_H
+#define EMMA_HYDRO_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* boundary / gather variant flags (compile-time -D switches in the reference) */
+#define ORC_TRANSXM 0x01   /* -DTRANSXM: transmissive at x=0 */
+#define ORC_TRANSXP 0x02   /* -DTRANSXP: transmissive at x=1 */
+#define ORC_TRANSYM 0x04
+#define ORC_TRANSYP 0x08
+#define ORC_TRANSZM 0x10
+#define ORC_TRANSZP 0x20
+#define ORC_HYDROTEST 0x40 /* -DHYDROTEST gather (src/hydro_utils.c:2464-2845) */
+
+/* error bits returned by the entry points (the reference aborts instead) */
+#define ORC_ERR_NEG_DENSITY 0x01   /* src/hydro_utils.c:1212 */
+#define ORC_ERR_NEG_PSTAR   0x02   /* src/hydro_utils.c:1283 */
+#define ORC_ERR_SLSR        0x04   /* src/hydro_utils.c:1298 */
+#define ORC_ERR_NAN         0x08   /* src/hydro_utils.c:1302, 2006, 3135 */
+#define ORC_ERR_TREE        0x10   /* missing neighbour (reference dereferences NULL) */
+
+/* firstoct[level-1] is the first oct of each level's `next` list. */
+int orc_hydro_solver(void **firstoct, int level, double dt, int flags);
+void orc_clean_new_hydro(void **firstoct, int level);
+double orc_comptstep_hydro(void **firstoct, int level, double cfl);
+/* Hydro-only Advance_level schedule; returns tsim after `nsteps` coarse steps.
+ * adt has lmax entries (in/out), like the reference's adt array. */
+double orc_run(void **firstoct, int lcoarse, int lmax, int nsteps, double dt_param,
+               double time_max, int nsub, double cfl, int flags, double tsim0,
+               double *adt, int *steps_done, int *err);
+long long orc_cell_updates(void);
+void orc_reset_counters(void);
+int orc_sizeof_oct(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
