@@ -1,0 +1,382 @@
+"""Benchmark of the hydro level advance on B200: cell-updates/s, mixed vs FP64.
+
+python bench.py [--gpus N] [--steps K] [--warmup W] [--config turb] [--impl mine|reference]
+
+A step is one coarse step of the hydro-only level schedule over the whole tree
+(all levels, subcycled), i.e. one pass of the hot path over one batch of
+synthetic input.  `value` = cell-updates/s of the mixed-precision path with the
+state resident in HBM (one cell-update = one leaf cell advanced by one level
+substep).  `e2e` = the same metric through the C ABI with host buffers: every
+step uploads the level states from pinned host memory and downloads them.
+The FP64 plain path is timed on the same workload and reported beside it.
+
+Multi-GPU: the path is run as independent replicas (one per rank), value =
+cell-updates of all ranks / max time over ranks.
+
+--impl reference times the reference's own CPU hydro (oracle/_ref, compiled from
+its sources; single-threaded, as the reference is) on a bounded sample of the
+same configuration.
+"""
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L2_BYTES = 126 * 1024 * 1024
+METRIC = "hydro cell-updates/s, mixed vs FP64 on 1 B200 at L1<=1e-5; % HBM roofline"
+ALG_BYTES_PER_CELL = 80  # 5 FP64 primitives read + 5 written per cell-update
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines() if r.strip()]
+        except Exception:
+            return out
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            r = [x.strip() for x in r]
+            try:
+                sm.append(float(r[1]))
+                smax.append(float(r[2]))
+            except Exception:
+                continue
+            for n, v in zip(names, r[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(smax), reasons=sorted(reasons), samples=len(sm))
+        return out
+
+
+def build_config(name):
+    from emma_b200 import configs
+    if name == "turb":
+        return configs.turb()
+    if name == "roofline":
+        return configs.random_uniform(level=8)
+    if name == "sod":
+        return configs.sod()
+    if name == "sedov":
+        return configs.sedov()
+    if name == "cosmo":
+        return configs.cosmo()
+    raise SystemExit(f"unknown config {name}")
+
+
+def traffic_per_cell(config, precision):
+    """DRAM bytes per cell-update of the level kernel from the committed ncu summary, if any."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    d = json.load(open(p))
+    return d.get(f"{config}/{precision}")
+
+
+def run_mine(args, rank, world):
+    import torch
+    from emma_b200 import ResidentHydro, PREC_FP64, PREC_MIXED, lib
+    from emma_b200._lib import ptr
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    L = lib()
+    cfg = build_config(args.config)
+    t0 = time.time()
+    tree = cfg.build()
+    build_s = time.time() - t0
+    levels = list(range(cfg.lcoarse, cfg.lmax + 1))
+    L.emma_hydro_set_stream(ctypes.c_void_p(stream.cuda_stream))
+    state_bytes = sum(5 * 8 * 8 * tree.noct(l) for l in levels)
+    flush = state_bytes < 2 * L2_BYTES
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda") if flush else None
+
+    results = {}
+    for prec_name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
+        r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl)
+        init_states = {l: r.state(l) for l in levels}
+        for _ in range(args.warmup):
+            r.coarse_step(nsub=cfg.nsub)
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        L.emma_hydro_reset_counters()
+        evs = []
+        with ClockSampler(dev) as clk:
+            torch.cuda.synchronize()
+            for _ in range(args.steps):
+                if flush:
+                    flush_buf.zero_()
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                r.coarse_step(nsub=cfg.nsub)
+                b.record(stream)
+                evs.append((a, b))
+            torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs)
+        updates = L.emma_hydro_cell_updates()
+        launches = L.emma_hydro_kernel_launches()
+        kavg, kcnt, kcells = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
+        L.emma_hydro_kernel_timing(ctypes.byref(kavg), ctypes.byref(kcnt), ctypes.byref(kcells))
+        status = r.status()
+        res = {"ms": ms, "updates": updates, "launches": launches, "kernel_avg_ms": kavg.value,
+               "kernel_launches": kcnt.value, "kernel_cells": kcells.value, "status": status,
+               "clocks": clk.summary()}
+        # e2e through the C ABI with host buffers: H2D states, coarse step, D2H states
+        pinned = {l: torch.from_numpy(init_states[l]).pin_memory() for l in levels}
+        outs = {l: torch.empty_like(pinned[l]).pin_memory() for l in levels}
+        for l in levels:
+            r.set_state(l, init_states[l])
+        torch.cuda.synchronize()
+        h2d = d2h = 0
+        e2e_ms = 0.0
+        for _ in range(args.steps):
+            if flush:
+                flush_buf.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for l in levels:
+                L.emma_hydro_set_level_state(l, ctypes.c_void_p(pinned[l].data_ptr()))
+                h2d += pinned[l].numel() * 8
+            r.coarse_step(nsub=cfg.nsub)
+            for l in levels:
+                L.emma_hydro_get_level_state(l, ctypes.c_void_p(outs[l].data_ptr()))
+                d2h += outs[l].numel() * 8
+            b.record(stream)
+            torch.cuda.synchronize()
+            e2e_ms += a.elapsed_time(b)
+        res["e2e_ms"] = e2e_ms
+        res["h2d"] = h2d // max(args.steps, 1)
+        res["d2h"] = d2h // max(args.steps, 1)
+        # state after `steps` coarse steps from the initial condition, for the L1 comparison
+        for l in levels:
+            r.set_state(l, init_states[l])
+        for _ in range(min(args.steps, 10)):
+            r.coarse_step(nsub=cfg.nsub)
+        res["final"] = {l: r.state(l) for l in levels}
+        results[prec_name] = res
+    # L1 of the mixed path against the FP64 path (the FP64 path equals the oracle to 1e-12)
+    fm, ff = results["mixed"]["final"], results["fp64"]["final"]
+    num = {k: 0.0 for k in ("rho", "p", "v")}
+    den = {k: 0.0 for k in ("rho", "p", "v")}
+    for l in levels:
+        dv = 0.5 ** (3 * l)
+        leaf = ~tree.split_mask(l)
+        a, b = fm[l][:, leaf], ff[l][:, leaf]
+        va, vb = np.sqrt((a[1:4] ** 2).sum(0)), np.sqrt((b[1:4] ** 2).sum(0))
+        for k, (x, y) in {"rho": (a[0], b[0]), "p": (a[4], b[4]), "v": (va, vb)}.items():
+            num[k] += np.abs(x - y).sum() * dv
+            den[k] += np.abs(y).sum() * dv
+    l1 = {k: float(num[k] / den[k]) for k in num}
+    return cfg, tree, results, l1, build_s, flush
+
+
+def cpu_baseline_sample(config):
+    """The reference's own CPU hydro on a bounded sample of the configuration."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from emma_b200 import configs
+    if not oracle.ref_available(tx=(config == "sod")):
+        return None
+    if config in ("turb",):
+        cfg, sample = configs.turb(level=6), "one level-6 step of the turbulent box generator (64^3, 262,144 cell-updates)"
+    elif config == "roofline":
+        cfg, sample = configs.random_uniform(level=6), "one level-6 step of the uniform random box (64^3, 262,144 cell-updates)"
+    elif config == "sod":
+        cfg, sample = configs.sod(level=6), "one step of the 64^3 Sod tube (262,144 cell-updates)"
+    else:
+        cfg, sample = configs.sedov(), "one coarse step of the Sedov tree (all levels, subcycled)"
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        ref = oracle.RefTree(cfg.lcoarse, cfg.lmax, tx=(config == "sod"),
+                             ngridmax=sum(8 ** (l - 1) for l in range(1, cfg.lcoarse + 1)) * 2 + 200000)
+        for i, lev in enumerate(range(cfg.lcoarse, cfg.lmax)):
+            pass
+        t = cfg.build(lambda lc, lm: ref) if cfg.lmax == cfg.lcoarse else None
+        if t is None:
+            return None
+        ref.reset_counters()
+        ref.run(1, nsub=cfg.nsub)
+        secs, cells = ref.hydro_seconds(), ref.cell_updates()
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    return {"value": cells / secs, "unit": "cell-updates/s", "cores": 1, "kind": "reference", "sample": sample,
+            "seconds": secs}
+
+
+def run_reference(args):
+    """--impl reference: the reference's CPU hydro, each step a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from emma_b200 import configs
+    cfgname = args.config
+    tx = cfgname == "sod"
+    line = {"impl": "reference", "metric": METRIC, "unit": "cell-updates/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True}
+    if not oracle.ref_available(tx=tx):
+        line["unavailable"] = "oracle/_ref (the reference CPU hydro compiled from its sources) is not built"
+        print(json.dumps(line))
+        return
+    level = 6
+    cfg = configs.turb(level=level) if cfgname == "turb" else configs.random_uniform(level=level)
+    saved = os.dup(1)
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
+    try:
+        ref = oracle.RefTree(level, level, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, level + 1)) + 16)
+        c = ref.cell_centres(level)
+        # same generator as the configuration, at the sample's size
+        t = cfg.build(lambda lc, lm: ref)
+        del t
+        for _ in range(args.warmup):
+            ref.run(1)
+        ref.reset_counters()
+        t0 = time.time()
+        ref.run(args.steps)
+        wall = time.time() - t0
+        secs, cells = ref.hydro_seconds(), ref.cell_updates()
+    finally:
+        os.dup2(saved, 1)
+        os.close(saved)
+        os.close(devnull)
+    v = cells / secs
+    sample = f"each step: one level-{level} step of the {cfgname} generator ({2 ** level}^3 = {8 ** level} cell-updates), 1 core"
+    line.update({"value": v, "ms_per_step": 1000 * secs / max(args.steps, 1), "scaling": "weak",
+                 "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                 "config": {"workload": f"{cfgname} (reference CPU sample at level {level})", "cells": 8 ** level},
+                 "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+                                  "sample": sample},
+                 "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                 "wall_s": wall})
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default="turb", choices=["turb", "roofline", "sod", "sedov", "cosmo"])
+    ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            run_reference(args)
+        return
+    import torch
+    import datetime
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    cfg, tree, res, l1, build_s, flushed = run_mine(args, rank, world)
+    mixed, fp64 = res["mixed"], res["fp64"]
+    # max over ranks of the timed device time
+    ms_m, ms_f, ms_e = mixed["ms"], fp64["ms"], mixed["e2e_ms"]
+    if world > 1:
+        t = torch.tensor([ms_m, ms_f, ms_e], device="cuda")
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_m, ms_f, ms_e = (float(x) for x in t.cpu())
+    upd_m = mixed["updates"] * world
+    value = upd_m / (ms_m * 1e-3)
+    value_fp64 = fp64["updates"] * world / (ms_f * 1e-3)
+    e2e = mixed["updates"] * world / (ms_e * 1e-3)
+    peak, peak_kind = peaks()
+    cells_per_launch = mixed["kernel_cells"] / max(mixed["kernel_launches"], 1)
+    achieved = ALG_BYTES_PER_CELL * cells_per_launch / (mixed["kernel_avg_ms"] * 1e-3) / 1e9
+    achieved_f = ALG_BYTES_PER_CELL * cells_per_launch / (fp64["kernel_avg_ms"] * 1e-3) / 1e9
+    tpc = traffic_per_cell(args.config, "mixed")
+    if rank != 0:
+        if world > 1:
+            torch.distributed.destroy_process_group()
+        return
+    cpu = None if args.no_cpu_baseline or world > 1 else cpu_baseline_sample(args.config)
+    line = {
+        "metric": METRIC, "value": value, "unit": "cell-updates/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_m / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 flux / f64 state", "data": "synthetic",
+        "config": {"workload": cfg.name, "levels": [cfg.lcoarse, cfg.lmax],
+                   "leaf_cells_per_step": mixed["updates"] // args.steps,
+                   "precision": "mixed (FP32 reconstruction/HLLC, FP64 compensated update)",
+                   "l2": "flushed between steps (256 MiB write)" if flushed else "state larger than L2",
+                   "parallelism": f"replicas x{world}", "cfl": cfg.cfl, "nsub": cfg.nsub},
+        "fp64": {"value": value_fp64, "unit": "cell-updates/s", "ms_per_step": ms_f / args.steps,
+                 "roofline_frac": achieved_f / peak, "status": fp64["status"]},
+        "mixed_over_fp64": value / value_fp64,
+        "l1_vs_fp64": l1,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": peak_kind, "traffic": (tpc * cells_per_launch) if tpc else None,
+                     "kernel": "level_advance_kernel<MathF32>", "alg_bytes_per_cell": ALG_BYTES_PER_CELL,
+                     "cells_per_launch": cells_per_launch, "avg_launch_ms": mixed["kernel_avg_ms"]},
+        "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": mixed["h2d"],
+                "d2h_bytes_per_step": mixed["d2h"]},
+        "gpu_launches": mixed["launches"],
+        "clocks": mixed["clocks"],
+        "status": mixed["status"],
+        "host_tree_build_s": build_s,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

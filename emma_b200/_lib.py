@@ -1,0 +1,100 @@
+"""ctypes bindings of libemmahydro.so (include/emma_hydro.h).
+
+The library is built in-tree (emma_b200/libemmahydro.so, see emma_b200/build.py).
+There is no fallback: if the shared library is missing or fails to load, every
+entry point raises, so a CUDA path that did not run can never look like one
+that did.
+"""
+import ctypes
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libemmahydro.so")
+
+_lib = None
+
+c_int, c_double, c_ll, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p
+P = ctypes.POINTER
+
+
+class EmmaHydroOptions(ctypes.Structure):
+    _fields_ = [("precision", c_int), ("trans_flags", c_int), ("cfl", c_double),
+                ("tile_octs", c_int), ("device", c_int)]
+
+
+PREC_FP64, PREC_MIXED = 0, 1
+TRANS_XM, TRANS_XP, TRANS_YM, TRANS_YP, TRANS_ZM, TRANS_ZP = 1, 2, 4, 8, 16, 32
+ST_NEG_DENSITY, ST_NEG_PSTAR, ST_NAN, ST_TREE, ST_CUDA, ST_ARG, ST_TIMEOUT = 1, 2, 4, 8, 16, 32, 64
+
+# (name, restype, argtypes) for every entry declared in include/emma_hydro.h
+SIGNATURES = [
+    ("emma_hydro_status", c_int, []),
+    ("emma_hydro_clear_status", None, []),
+    ("emma_hydro_last_error", ctypes.c_char_p, []),
+    ("emma_hydro_default_options", None, [P(EmmaHydroOptions)]),
+    ("HydroSolver", None, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_double]),
+    ("advancehydroGPU", c_int, [c_void_p, c_int, c_void_p, c_void_p, c_int, c_double, c_double]),
+    ("clean_new_hydro", None, [c_int, c_void_p, c_void_p, c_void_p]),
+    ("create_hydstencil_GPU", None, [c_void_p, c_int]),
+    ("destroy_hydstencil_GPU", None, [c_void_p, c_int]),
+    ("create_pinned_stencil", None, [P(c_void_p), c_int]),
+    ("destroy_pinned_stencil", None, [P(c_void_p), c_int]),
+    ("emma_hydro_init", c_int, [P(EmmaHydroOptions)]),
+    ("emma_hydro_set_options", c_int, [P(EmmaHydroOptions)]),
+    ("emma_hydro_shutdown", None, []),
+    ("emma_hydro_set_stream", c_int, [c_void_p]),
+    ("emma_hydro_kernel_launches", c_ll, []),
+    ("emma_hydro_tree_upload", c_int, [c_void_p, c_int, c_int, c_int]),
+    ("emma_hydro_tree_download", c_int, [c_void_p]),
+    ("emma_hydro_fields_upload", c_int, [c_void_p]),
+    ("emma_hydro_clean_new", c_int, [c_int]),
+    ("emma_hydro_comptstep", c_int, [c_int, P(c_double)]),
+    ("emma_hydro_advance_level", c_int, [c_int, c_double]),
+    ("emma_hydro_advance_coarse_step", c_int, [c_double, c_double, c_int, P(c_double), c_void_p]),
+    ("emma_hydro_level_noct", c_int, [c_int]),
+    ("emma_hydro_get_level_state", c_int, [c_int, c_void_p]),
+    ("emma_hydro_set_level_state", c_int, [c_int, c_void_p]),
+    ("emma_hydro_level_leaf_cells", c_ll, [c_int]),
+    ("emma_hydro_cell_updates", c_ll, []),
+    ("emma_hydro_reset_counters", None, []),
+    ("emma_hydro_kernel_timing", c_int, [P(c_double), P(c_ll), P(c_ll)]),
+    ("emma_hydro_plan_stats", c_int, [c_void_p, c_int, c_int, c_int, c_void_p]),
+    ("emma_tree_create", c_void_p, [c_int, c_int, c_ll]),
+    ("emma_tree_destroy", None, [c_void_p]),
+    ("emma_tree_refine", c_int, [c_void_p, c_int, c_void_p]),
+    ("emma_tree_firstoct", c_void_p, [c_void_p]),
+    ("emma_tree_noct", c_int, [c_void_p, c_int]),
+    ("emma_tree_oct_xyz", None, [c_void_p, c_int, c_void_p]),
+    ("emma_tree_set_field", None, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("emma_tree_get_field", None, [c_void_p, c_int, c_int, c_void_p]),
+    ("emma_tree_topology", None, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+]
+
+
+def lib():
+    """Load libemmahydro.so once; raise if it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libemmahydro.so is not built ({LIB_PATH}); run emma_b200.build.build()")
+    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+    for name, res, args in SIGNATURES:
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def ptr(a):
+    """Data pointer of a C-contiguous numpy array."""
+    assert a.flags["C_CONTIGUOUS"]
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def check(rc, what=""):
+    """Raise on a non-zero status bitmask returned by the library."""
+    if rc != 0:
+        msg = lib().emma_hydro_last_error().decode(errors="replace")
+        raise RuntimeError(f"libemmahydro {what} failed: status=0x{rc & 0xffffffff:x} {msg}")

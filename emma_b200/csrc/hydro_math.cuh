@@ -1,0 +1,371 @@
+// hydro_math.cuh -- per-cell and per-face hydro arithmetic for the level kernels.
+//
+// Two instantiations:
+//   MathF64 -- the plain path.  Every expression keeps the operation order of
+//              the reference CPU hydro (src/hydro_utils.c) so that, compiled with
+//              -fmad=false and IEEE division/square root, results match the
+//              reference to the last bit except where libm pow() differs from
+//              CUDA's pow() (TRRS branch and exact-solver fallback).
+//   MathF32 -- the mixed path's reconstruction, wave speeds and fluxes in FP32:
+//              the same algorithm with one reciprocal per density, fast
+//              division/square root and algebraic simplifications (d a^2 = gamma p).
+//
+// Primitive vectors are 5-wide: 0:d 1:u 2:v 3:w 4:p.  Face index k:
+// 0:-x 1:+x 2:-y 3:+y 4:-z 5:+z.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace emma {
+
+constexpr double kGam = 5. / 3.;   // GAMMA, src/param.h:4
+constexpr double kPmin = 1e-10;    // PMIN, src/param.h:20
+constexpr double kErrTol = 1e-10;  // ERRTOL, src/hydro_utils.c:18
+constexpr int kNiterMax = 10;      // NITERMAX, src/hydro_utils.c:17
+
+// status bits (mirrors EMMA_ST_* of emma_hydro.h)
+constexpr unsigned kStNegDensity = 0x01, kStNegPstar = 0x02, kStNan = 0x04, kStTree = 0x08;
+
+// ============================================================== FP64 (plain)
+struct MathF64 {
+  using R = double;
+
+  // minmod_W, beta = 1 (src/hydro_utils.c:201)
+  static __device__ __forceinline__ double limit(double m, double p) {
+    if (p > 0) return fmax(fmax(0., fmin(m, p)), fmin(m, p));
+    return fmin(fmin(0., fmax(m, p)), fmax(m, p));
+  }
+
+  // MUSCL_BOUND2 slopes + matrix_jacobian predictor (src/hydro_utils.c:976-1189).
+  // q0: cell, qm/qp: neighbours per axis.  Out: D[3][5] slopes, Wt[5] predictor.
+  static __device__ __forceinline__ void muscl(const double q0[5], const double qm[3][5], const double qp[3][5],
+                                               double dt, double dx, double D[3][5], double Wt[5]) {
+#pragma unroll
+    for (int dir = 0; dir < 3; dir++)
+#pragma unroll
+      for (int k = 0; k < 5; k++) D[dir][k] = limit(q0[k] - qm[dir][k], qp[dir][k] - q0[k]);
+    // stored sound speed of the cell, as U2W/scatter computes it (src/hydro_utils.c:64,3186)
+    const double a0 = sqrt(kGam * q0[4] / q0[0]);
+    const double daa = q0[0] * a0 * a0;
+    const double id = 1. / q0[0];
+    double acc[5] = {0., 0., 0., 0., 0.};
+#pragma unroll
+    for (int dir = 0; dir < 3; dir++) {
+      const double s = q0[1 + dir];
+      acc[0] += s * D[dir][0];
+      if (dir == 0) { acc[0] += q0[0] * D[0][1]; }
+      acc[1] += s * D[dir][1];
+      if (dir == 0) { acc[4] += daa * D[0][1]; }
+      if (dir == 1) { acc[0] += q0[0] * D[1][2]; }
+      acc[2] += s * D[dir][2];
+      if (dir == 1) { acc[4] += daa * D[1][2]; }
+      if (dir == 2) { acc[0] += q0[0] * D[2][3]; }
+      acc[3] += s * D[dir][3];
+      if (dir == 2) { acc[4] += daa * D[2][3]; }
+      acc[1 + dir] += id * D[dir][4];
+      acc[4] += s * D[dir][4];
+    }
+    const double fac = -dt / dx * 0.5;
+#pragma unroll
+    for (int i = 0; i < 5; i++) Wt[i] = acc[i] * fac;
+  }
+
+  // Face state k of a cell from its slopes and predictor (src/hydro_utils.c:1166-1247):
+  // W0 +-D/2 + Wt, pressure floor, then E and a.  Returns the 7 values d,u,v,w,p,a,E.
+  static __device__ __forceinline__ void face(const double q0[5], const double D[3][5], const double Wt[5], int k,
+                                              double W[7], unsigned &st) {
+    const double fx = (k == 0) ? -0.5 : (k == 1 ? 0.5 : 0.0);
+    const double fy = (k == 2) ? -0.5 : (k == 3 ? 0.5 : 0.0);
+    const double fz = (k == 4) ? -0.5 : (k == 5 ? 0.5 : 0.0);
+#pragma unroll
+    for (int i = 0; i < 5; i++) W[i] = q0[i] + fx * D[0][i] + fy * D[1][i] + fz * D[2][i] + Wt[i];
+    W[4] = fmax(W[4], kPmin);
+    if (W[0] < 0) st |= kStNegDensity;
+    W[6] = W[4] / (kGam - 1.) + 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]);
+    W[5] = sqrt(kGam * W[4] / W[0]);
+  }
+
+  struct S1 { double d, u, p, a; };
+
+  static __device__ double froot_prime(double p, const S1 &L, const S1 &R) {
+    double AL = 2. / ((kGam + 1.) * L.d), AR = 2. / ((kGam + 1.) * R.d);
+    double BL = (kGam - 1.) / (kGam + 1.) * L.p, BR = (kGam - 1.) / (kGam + 1.) * R.p;
+    double fL = (p > L.p ? sqrt(AL / (BL + p)) * (1. - (p - L.p) / (2. * (BL + p)))
+                         : pow(p / L.p, -(kGam + 1) / (2. * kGam)) / (L.d * L.a));
+    double fR = (p > R.p ? sqrt(AR / (BR + p)) * (1. - (p - R.p) / (2. * (BR + p)))
+                         : pow(p / R.p, -(kGam + 1) / (2. * kGam)) / (R.d * R.a));
+    return fL + fR;
+  }
+  static __device__ double froot(double p, const S1 &L, const S1 &R, double *u) {
+    double AL = 2. / ((kGam + 1.) * L.d), AR = 2. / ((kGam + 1.) * R.d);
+    double BL = (kGam - 1.) / (kGam + 1.) * L.p, BR = (kGam - 1.) / (kGam + 1.) * R.p;
+    double fL = (p > L.p ? (p - L.p) * sqrt(AL / (BL + p))
+                         : 2. * L.a / (kGam - 1.) * (pow(p / L.p, (kGam - 1) / (2. * kGam)) - 1.));
+    double fR = (p > R.p ? (p - R.p) * sqrt(AR / (BR + p))
+                         : 2. * R.a / (kGam - 1.) * (pow(p / R.p, (kGam - 1) / (2. * kGam)) - 1.));
+    *u = 0.5 * (L.u + R.u) + 0.5 * (fR - fL);
+    return fL + fR + (R.u - L.u);
+  }
+  // findPressure (src/hydro_utils.c:680): rare fallback when the hybrid estimate is negative
+  static __device__ __noinline__ double pstar_exact(const S1 &L, const S1 &R, double *u, unsigned &st) {
+    const double unsurz = (2.0 * kGam) / (kGam - 1.0);
+    double pmin = fmin(L.p, R.p), pmax = fmax(L.p, R.p);
+    double AL = 2. / ((kGam + 1.) * L.d), AR = 2. / ((kGam + 1.) * R.d);
+    double BL = (kGam - 1.) / (kGam + 1.) * L.p, BR = (kGam - 1.) / (kGam + 1.) * R.p;
+    double ppv0 = 0.5 * (L.p + R.p) - 0.125 * (R.u - L.u) * (R.d + L.d) * (R.a + L.a);
+    double ptr0 = pow((L.a + R.a - 0.5 * (kGam - 1) * (R.u - L.u)) /
+                          (L.a / pow(L.p, 1. / unsurz) + R.a / pow(R.p, 1. / unsurz)),
+                      unsurz);
+    double ppv = fmax(kErrTol, ppv0), ptr = fmax(kErrTol, ptr0);
+    double GL = sqrt(AL / (ppv + BL)), GR = sqrt(AR / (ppv + BR));
+    double pts = fmax(kErrTol, (GL * L.p + GR * R.p - (R.u - L.u)) / (GL + GR));
+    double p, u2;
+    if (((pmax / pmin) < 2.0) && ((pmin <= ppv) && (ppv <= pmax))) p = ppv;
+    else if (ppv < pmin) p = ptr;
+    else p = pts;
+    for (int i = 0; i < kNiterMax; i++) {
+      double dp = froot(p, L, R, &u2) / froot_prime(p, L, R);
+      if (isnan(dp)) { st |= kStNan; break; }
+      if (fabs(dp) < kErrTol) break;
+      for (int h = 0; h < 1100 && (p - dp) < 0; h++) dp = dp * 0.5;  // bounded halving
+      double porg = p;
+      p = p - dp;
+      double err = 2. * fabs(p - porg) / (fabs(p + porg));
+      if (err < kErrTol) break;
+      if (froot(p, L, R, &u2) < kErrTol) break;
+    }
+    froot(p, L, R, &u2);
+    *u = u2;
+    return p;
+  }
+
+  // findPressure_Hybrid + speedestimate*_HLLC (src/hydro_utils.c:625,1264)
+  static __device__ __forceinline__ void speeds(const double WL[7], const double WR[7], int n, double &SL, double &SR,
+                                                double &ustar, unsigned &st) {
+    S1 L{WL[0], WL[1 + n], WL[4], sqrt(kGam * WL[4] / WL[0])};
+    S1 R{WR[0], WR[1 + n], WR[4], sqrt(kGam * WR[4] / WR[0])};
+    double dbar = 0.5 * (L.d + R.d), abar = 0.5 * (L.a + R.a);
+    double ppvrs = 0.5 * ((L.p + R.p) + (L.u - R.u) * dbar * abar);
+    double pmax = fmax(L.p, R.p), pmin = fmin(L.p, R.p);
+    double pstar = ppvrs;
+    if (((pmax / pmin) < 2.) && ((pmin < pstar) && (pstar < pmax))) {
+      ustar = 0.5 * ((L.u + R.u) + (L.p - R.p) / (dbar * abar));
+    } else if (pstar < pmin) {
+      double z = (kGam - 1.) / (2. * kGam);
+      double iz = (2. * kGam) / (kGam - 1.);
+      pstar = pow((L.a + R.a - (kGam - 1.) / 2. * (R.u - L.u)) / (L.a / pow(L.p, z) + R.a / pow(R.p, z)), iz);
+      ustar = L.u - 2. * L.a / (kGam - 1.) * (pow(pstar / L.p, z) - 1.);
+    } else {
+      double p0 = fmax(0., ppvrs);
+      double AL = 2. / ((kGam + 1.) * L.d), AR = 2. / ((kGam + 1.) * R.d);
+      double BL = (kGam - 1.) / (kGam + 1.) * L.p, BR = (kGam - 1.) / (kGam + 1.) * R.p;
+      double GL = sqrt(AL / (p0 + BL)), GR = sqrt(AR / (p0 + BR));
+      pstar = (GL * L.p + GR * R.p - (R.u - L.u)) / (GL + GR);
+      ustar = 0.5 * ((L.u + R.u) + (pstar - R.p) * GR - (pstar - L.p) * GL);
+    }
+    if (pstar < 0) pstar = pstar_exact(L, R, &ustar, st);
+    if (pstar < 0) st |= kStNegPstar;
+    double qL = (pstar <= WL[4] ? 1. : sqrt(1. + (kGam + 1.) / (2. * kGam) * ((pstar) / WL[4] - 1.)));
+    double qR = (pstar <= WR[4] ? 1. : sqrt(1. + (kGam + 1.) / (2. * kGam) * ((pstar) / WR[4] - 1.)));
+    SL = L.u - L.a * qL;
+    SR = R.u + R.a * qR;
+    if (SL > SR) {
+      SL = fmin(L.u - L.a, R.u - R.a);
+      SR = fmax(L.u + L.a, R.u + R.a);
+    }
+    if (isnan(ustar)) st |= kStNan;
+  }
+
+  // getflux_{X,Y,Z} of W2U(W) (src/hydro_utils.c:66,916-968), axis n
+  static __device__ __forceinline__ void euler(const double W[7], int n, double f[5]) {
+    const double d = W[0];
+    const double m[3] = {W[0] * W[1], W[0] * W[2], W[0] * W[3]};
+    const double E = W[6];
+    const double mn = m[n];
+    const int t1 = (n == 0) ? 1 : 0, t2 = (n == 2) ? 1 : 2;
+    const double all = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
+    f[0] = mn;
+    f[1 + n] = 0.5 * (3. - kGam) * mn * mn / d + (kGam - 1.) * E - 0.5 * (kGam - 1.) * (m[t1] * m[t1] + m[t2] * m[t2]) / d;
+    f[1 + t1] = mn * m[t1] / d;
+    f[1 + t2] = mn * m[t2] / d;
+    f[4] = kGam * mn / d * E - 0.5 * (kGam - 1.) * mn / (d * d) * all;
+  }
+
+  // HLLC flux across a face normal to axis n (src/hydro_utils.c:2055-2138)
+  static __device__ __forceinline__ void hllc(const double WL[7], const double WR[7], int n, double F[5],
+                                              unsigned &st) {
+    double SL, SR, ustar;
+    speeds(WL, WR, n, SL, SR, ustar, st);
+#pragma unroll
+    for (int k = 0; k < 5; k++) F[k] = 0.;
+    if (SL >= 0.) {
+      euler(WL, n, F);
+    } else if (SR <= 0.) {
+      euler(WR, n, F);
+    } else {
+      const bool left = (SL < 0.) && (ustar >= 0.);
+      const bool right = (ustar <= 0.) && (SR > 0.);
+      if (left || right) {
+        const double *W = left ? WL : WR;
+        const double S = left ? SL : SR;
+        euler(W, n, F);
+        const double d = W[0], un = W[1 + n];
+        const double Ud = W[0], UE = W[6];
+        const double mom[3] = {W[0] * W[1], W[0] * W[2], W[0] * W[3]};
+        const double fact = d * (S - un) / (S - ustar);
+        F[0] += (fact * 1. - Ud) * S;
+#pragma unroll
+        for (int k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : W[1 + k]) - mom[k]) * S;
+        F[4] += (fact * (UE / Ud + (ustar - un) * (ustar + W[4] / (d * (S - un)))) - UE) * S;
+      }
+    }
+  }
+};
+
+// ============================================================== FP32 (mixed)
+struct MathF32 {
+  using R = float;
+  static constexpr float G = 5.f / 3.f;
+
+  static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+  static __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+
+  static __device__ __forceinline__ float limit(float m, float p) {
+    // minmod with beta = 1: 0 if signs differ, else the smaller magnitude
+    return (p > 0.f) ? fmaxf(0.f, fminf(m, p)) : fminf(0.f, fmaxf(m, p));
+  }
+
+  static __device__ __forceinline__ void muscl(const float q0[5], const float qm[3][5], const float qp[3][5],
+                                               float dtdx_half, float D[3][5], float Wt[5]) {
+#pragma unroll
+    for (int dir = 0; dir < 3; dir++)
+#pragma unroll
+      for (int k = 0; k < 5; k++) D[dir][k] = limit(q0[k] - qm[dir][k], qp[dir][k] - q0[k]);
+    const float id = rcp(q0[0]);
+    const float gp = G * q0[4];  // d a^2
+    float acc0 = q0[1] * D[0][0] + q0[0] * D[0][1] + q0[2] * D[1][0] + q0[0] * D[1][2] + q0[3] * D[2][0] + q0[0] * D[2][3];
+    float acc1 = q0[1] * D[0][1] + id * D[0][4] + q0[2] * D[1][1] + q0[3] * D[2][1];
+    float acc2 = q0[1] * D[0][2] + q0[2] * D[1][2] + id * D[1][4] + q0[3] * D[2][2];
+    float acc3 = q0[1] * D[0][3] + q0[2] * D[1][3] + q0[3] * D[2][3] + id * D[2][4];
+    float acc4 = gp * (D[0][1] + D[1][2] + D[2][3]) + q0[1] * D[0][4] + q0[2] * D[1][4] + q0[3] * D[2][4];
+    Wt[0] = -dtdx_half * acc0;
+    Wt[1] = -dtdx_half * acc1;
+    Wt[2] = -dtdx_half * acc2;
+    Wt[3] = -dtdx_half * acc3;
+    Wt[4] = -dtdx_half * acc4;
+  }
+
+  // Face state: W0 +- D/2 + Wt, pressure floor; returns d,u,v,w,p, 1/d and a
+  static __device__ __forceinline__ void face(const float q0[5], const float D[3][5], const float Wt[5], int k,
+                                              float W[7], unsigned &st) {
+    const int ax = k >> 1;
+    const float s = (k & 1) ? 0.5f : -0.5f;
+#pragma unroll
+    for (int i = 0; i < 5; i++) W[i] = q0[i] + s * D[ax][i] + Wt[i];
+    W[4] = fmaxf(W[4], (float)kPmin);
+    if (W[0] < 0.f) st |= kStNegDensity;
+    W[5] = rcp(W[0]);
+    W[6] = sqrtf(G * W[4] * W[5]);
+  }
+
+  static __device__ __noinline__ float pstar_exact(float dL, float uL, float pL, float aL, float dR, float uR,
+                                                   float pR, float aR, float *u) {
+    // Newton iteration on the exact two-rarefaction/shock function (Toro sec. 4.3)
+    const float g1 = (G - 1.f) / (2.f * G), g2 = (G + 1.f) / (2.f * G);
+    const float AL = 2.f / ((G + 1.f) * dL), AR = 2.f / ((G + 1.f) * dR);
+    const float BL = (G - 1.f) / (G + 1.f) * pL, BR = (G - 1.f) / (G + 1.f) * pR;
+    float p = fmaxf(1e-10f, 0.5f * (pL + pR) - 0.125f * (uR - uL) * (dL + dR) * (aL + aR));
+    float fL = 0.f, fR = 0.f;
+    for (int i = 0; i < kNiterMax; i++) {
+      float dfL, dfR;
+      if (p > pL) { float q = sqrtf(AL / (BL + p)); fL = (p - pL) * q; dfL = q * (1.f - (p - pL) / (2.f * (BL + p))); }
+      else { float r = __powf(p / pL, g1); fL = 2.f * aL / (G - 1.f) * (r - 1.f); dfL = __powf(p / pL, -g2) / (dL * aL); }
+      if (p > pR) { float q = sqrtf(AR / (BR + p)); fR = (p - pR) * q; dfR = q * (1.f - (p - pR) / (2.f * (BR + p))); }
+      else { float r = __powf(p / pR, g1); fR = 2.f * aR / (G - 1.f) * (r - 1.f); dfR = __powf(p / pR, -g2) / (dR * aR); }
+      float dp = (fL + fR + (uR - uL)) / (dfL + dfR);
+      if (!(fabsf(dp) >= 1e-10f)) break;
+      for (int h = 0; h < 200 && (p - dp) < 0.f; h++) dp *= 0.5f;
+      float porg = p;
+      p -= dp;
+      if (2.f * fabsf(p - porg) / fabsf(p + porg) < 1e-7f) break;
+    }
+    *u = 0.5f * (uL + uR) + 0.5f * (fR - fL);
+    return p;
+  }
+
+  static __device__ __forceinline__ void speeds(const float WL[7], const float WR[7], int n, float &SL, float &SR,
+                                                float &ustar, unsigned &st) {
+    const float dL = WL[0], uL = WL[1 + n], pL = WL[4], aL = WL[6];
+    const float dR = WR[0], uR = WR[1 + n], pR = WR[4], aR = WR[6];
+    const float dbar = 0.5f * (dL + dR), abar = 0.5f * (aL + aR);
+    const float ppvrs = 0.5f * ((pL + pR) + (uL - uR) * dbar * abar);
+    const float pmax = fmaxf(pL, pR), pmin = fminf(pL, pR);
+    float pstar = ppvrs;
+    if ((pmax < 2.f * pmin) && (pmin < pstar) && (pstar < pmax)) {
+      ustar = 0.5f * ((uL + uR) + fdiv(pL - pR, dbar * abar));
+    } else if (pstar < pmin) {
+      const float z = (G - 1.f) / (2.f * G), iz = (2.f * G) / (G - 1.f);
+      const float num = aL + aR - (G - 1.f) * 0.5f * (uR - uL);
+      const float den = aL * __powf(pL, -z) + aR * __powf(pR, -z);
+      pstar = __powf(fdiv(num, den), iz);
+      ustar = uL - 2.f * aL / (G - 1.f) * (__powf(fdiv(pstar, pL), z) - 1.f);
+    } else {
+      const float p0 = fmaxf(0.f, ppvrs);
+      const float AL = 2.f / (G + 1.f) * WL[5], AR = 2.f / (G + 1.f) * WR[5];
+      const float BL = (G - 1.f) / (G + 1.f) * pL, BR = (G - 1.f) / (G + 1.f) * pR;
+      const float GL = sqrtf(fdiv(AL, p0 + BL)), GR = sqrtf(fdiv(AR, p0 + BR));
+      pstar = fdiv(GL * pL + GR * pR - (uR - uL), GL + GR);
+      ustar = 0.5f * ((uL + uR) + (pstar - pR) * GR - (pstar - pL) * GL);
+    }
+    if (pstar < 0.f) pstar = pstar_exact(dL, uL, pL, aL, dR, uR, pR, aR, &ustar);
+    if (pstar < 0.f) st |= kStNegPstar;
+    const float g2 = (G + 1.f) / (2.f * G);
+    const float qL = (pstar <= pL) ? 1.f : sqrtf(1.f + g2 * (fdiv(pstar, pL) - 1.f));
+    const float qR = (pstar <= pR) ? 1.f : sqrtf(1.f + g2 * (fdiv(pstar, pR) - 1.f));
+    SL = uL - aL * qL;
+    SR = uR + aR * qR;
+    if (SL > SR) {
+      SL = fminf(uL - aL, uR - aR);
+      SR = fmaxf(uL + aL, uR + aR);
+    }
+    if (isnan(ustar)) st |= kStNan;
+  }
+
+  // W[7] = d,u,v,w,p,1/d,a.  Euler flux along axis n.
+  static __device__ __forceinline__ void euler(const float W[7], int n, float f[5], float &E) {
+    const float d = W[0], un = W[1 + n];
+    const float ke = 0.5f * d * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]);
+    E = W[4] * (1.f / (G - 1.f)) + ke;
+    f[0] = d * un;
+    f[1] = f[0] * W[1];
+    f[2] = f[0] * W[2];
+    f[3] = f[0] * W[3];
+    f[1 + n] += W[4];
+    f[4] = un * (E + W[4]);
+  }
+
+  static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st) {
+    float SL, SR, ustar;
+    speeds(WL, WR, n, SL, SR, ustar, st);
+    const bool useL = (SL >= 0.f) || (!(SR <= 0.f) && (ustar >= 0.f));
+    const float *W = useL ? WL : WR;
+    float E;
+    euler(W, n, F, E);
+    if (SL >= 0.f || SR <= 0.f) return;
+    if (!((SL < 0.f && ustar >= 0.f) || (ustar <= 0.f && SR > 0.f))) {
+#pragma unroll
+      for (int k = 0; k < 5; k++) F[k] = 0.f;
+      return;
+    }
+    const float S = useL ? SL : SR;
+    const float d = W[0], un = W[1 + n];
+    const float Smu = S - un;
+    const float fact = fdiv(d * Smu, S - ustar);
+    F[0] += (fact - d) * S;
+#pragma unroll
+    for (int k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : W[1 + k]) - d * W[1 + k]) * S;
+    F[4] += (fact * (E * W[5] + (ustar - un) * (ustar + fdiv(W[4], d * Smu))) - E) * S;
+  }
+};
+
+}  // namespace emma

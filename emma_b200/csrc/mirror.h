@@ -1,0 +1,39 @@
+// mirror.h -- host-side mirror of an EMMA oct tree: per-level oct lists,
+// split masks, child links and the tile plans the level kernels execute.
+#pragma once
+#include <string>
+#include <vector>
+#include "emma_oct.h"
+#include "plan_types.h"
+
+namespace emma {
+
+struct HostLevel {
+  int L = 0;
+  int noct = 0;
+  long long leaf = 0;                 // leaf cells
+  std::vector<struct OCT *> octs;     // list order (cpu == rank)
+  std::vector<uint8_t> split;         // per oct: bit c set if cell c has a child
+  std::vector<int32_t> child;         // per cell: index of the child oct at L+1, or -1
+  std::vector<TileDesc> tiles;
+  std::vector<uint32_t> keys;
+  std::vector<uint8_t> graph;
+  std::vector<uint16_t> halo;
+  std::vector<int32_t> inj_cells;     // level L-1 cells injected into this level's plans
+};
+
+struct HostTree {
+  int lcoarse = 0, lmax = 0, rank = 0, trans = 0;
+  std::vector<HostLevel> lev;  // indexed by level (0..lmax)
+};
+
+// Build the mirror of levels lcoarse..lmax and the tile plans of levels
+// plan_lo..plan_hi (a plan of level L needs the mirror of L-1 when L-1 >=
+// lcoarse).  Returns 0 on success, else an EMMA_ST_* bit with a message in `err`.
+int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int trans, int plan_lo, int plan_hi,
+                    HostTree &H, std::string &err);
+
+// Bounds check of every index the level kernels read (run by build_host_tree).
+int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string &err);
+
+}  // namespace emma

@@ -1,0 +1,59 @@
+// plan_types.h -- data shared by the host planner and the level kernels.
+#pragma once
+#include <stdint.h>
+
+namespace emma {
+
+// Virtual-oct keys of a tile plan: kind in bits 28..31, index in bits 0..27.
+//   kKeyReal        : an oct of this level, index in the level list
+//   kKeyInj         : a coarser leaf cell (level L-1, index oct*8+cell) whose
+//                     state fills all 8 cells, as the reference's gather injects
+//                     it (src/hydro_utils.c:2912-2944)
+//   kKeyGhost0 + k  : transmissive ghost across face k of an oct of this level,
+//                     filled through the reference's mirror map of face k
+//                     (src/hydro_utils.c:2504-2610)
+constexpr uint32_t kKeyReal = 0, kKeyInj = 1, kKeyGhost0 = 2;
+constexpr uint32_t kKeyNone = 0xFFFFFFFFu;
+constexpr uint32_t key_make(uint32_t kind, uint32_t idx) { return (kind << 28) | idx; }
+
+// Kernel shape the plans are cut for (tile octs, staged octs, halo cells).
+constexpr int kTileOcts = 32;
+constexpr int kSMax = 144;
+constexpr int kHMax = 288;
+
+struct TileDesc {
+  int oct0;       // first oct of the tile (level list index)
+  int noct;       // octs in the tile (<= kTileOcts)
+  int S;          // staged virtual octs (tile octs first)
+  int H;          // halo cells (staged cell codes s*8+c)
+  int keys_off;   // offset into the keys array
+  int graph_off;  // offset into the graph array (S*6 bytes; 255 = not staged)
+  int halo_off;   // offset into the halo array
+  int pad;
+};
+
+struct LevelArgs {
+  int L;
+  int noct;
+  const double *W;    // level state, planes d,u,v,w,p of 8*noct
+  double *Wn;         // next state (written)
+  const double *C;    // conserved corrections received from the finer level (may be null)
+  const double *B;    // optional update base: planes d,u,v,w,p,E of the caller's fieldnew
+                      // (drop-in mode); when null the base is W2U(W) + C
+  const double *Wc;   // level L-1 state (injected neighbours), may be null
+  double *Cc;         // level L-1 corrections (fine->coarse), may be null
+  long long nc8;      // plane stride of Wc/Cc
+  const double *Wf;   // level L+1 state (split-cell averaging), may be null
+  long long nf8;      // plane stride of Wf
+  const uint8_t *split;  // per oct bitmask of split cells
+  const int *child;      // per cell: child oct index at L+1, -1 for a leaf
+  const TileDesc *tiles;
+  const uint32_t *keys;
+  const uint8_t *graph;
+  const uint16_t *halo;
+  double dt, dx;
+  unsigned *status;
+  int ntiles;
+};
+
+}  // namespace emma

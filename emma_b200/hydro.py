@@ -1,0 +1,91 @@
+"""Host-side interface of the hydro level advance (mirrors the reference's entry points).
+
+ResidentHydro drives the resident path: upload a tree once, advance levels or
+coarse steps on the GPU, read states back.  The reference-named drop-in entries
+(HydroSolver, advancehydroGPU, clean_new_hydro) are exposed as functions with
+the reference's arguments; they operate on the caller's host tree in place.
+"""
+import ctypes
+
+import numpy as np
+
+from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
+
+
+def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0):
+    o = EmmaHydroOptions()
+    lib().emma_hydro_default_options(ctypes.byref(o))
+    o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
+    return o
+
+
+class ResidentHydro:
+    """Levels lcoarse..lmax of an oct tree resident on the GPU."""
+
+    def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0):
+        self.tree = tree
+        self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
+        L = lib()
+        o = options(precision, trans, cfl)
+        check(L.emma_hydro_init(ctypes.byref(o)), "init")
+        check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
+        L.emma_hydro_clear_status()
+        check(L.emma_hydro_tree_upload(tree.firstoct, self.lcoarse, self.lmax, rank), "tree_upload")
+        self.adt = np.zeros(self.lmax)
+        self.tsim = 0.0
+
+    def set_precision(self, precision, cfl=None):
+        o = options(precision, 0, cfl if cfl is not None else 0.85)
+        check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
+
+    def noct(self, level):
+        return lib().emma_hydro_level_noct(level)
+
+    def state(self, level):
+        n8 = 8 * self.noct(level)
+        out = np.zeros((5, n8))
+        if n8:
+            check(lib().emma_hydro_get_level_state(level, ptr(out)), "get_level_state")
+        return out
+
+    def set_state(self, level, st):
+        st = np.ascontiguousarray(st, dtype=np.float64)
+        check(lib().emma_hydro_set_level_state(level, ptr(st)), "set_level_state")
+
+    def comptstep(self, level):
+        dt = ctypes.c_double()
+        check(lib().emma_hydro_comptstep(level, ctypes.byref(dt)), "comptstep")
+        return dt.value
+
+    def clean_new(self, level):
+        check(lib().emma_hydro_clean_new(level), "clean_new")
+
+    def advance_level(self, level, dt):
+        check(lib().emma_hydro_advance_level(level, dt), "advance_level")
+
+    def coarse_step(self, dt_param=1e9, time_max=1e9, nsub=2):
+        t = ctypes.c_double(self.tsim)
+        check(lib().emma_hydro_advance_coarse_step(dt_param, time_max, nsub, ctypes.byref(t), ptr(self.adt)),
+              "advance_coarse_step")
+        self.tsim = t.value
+        return self.tsim
+
+    def status(self):
+        return lib().emma_hydro_status()
+
+    def download(self):
+        check(lib().emma_hydro_tree_download(self.tree.firstoct), "tree_download")
+
+
+def HydroSolver(level, firstoct, dtnew, cpu=None):
+    """Drop-in HydroSolver (src/hydro_utils.c:3378) on a host tree."""
+    lib().HydroSolver(level, None, firstoct, cpu, None, 0, dtnew)
+
+
+def advancehydroGPU(firstoct, level, dtnew, cpu=None):
+    """Drop-in advancehydroGPU (src/hydro_utils_gpu.cu:2470); returns octs advanced."""
+    return lib().advancehydroGPU(firstoct, level, cpu, None, 0, 0.5 ** level, dtnew)
+
+
+def clean_new_hydro(level, firstoct):
+    lib().clean_new_hydro(level, None, firstoct, None)

@@ -1,0 +1,89 @@
+"""Host oct tree (EMMA's struct OCT layout) built by libemmahydro.
+
+Thin wrapper over the emma_tree_* entries of include/emma_hydro.h: build the
+complete levels 1..lcoarse, refine cells selected by a predicate on their
+centres (reference construction order), set and read fields per level in list
+order (oct*8 + cell, cell = ix + 2 iy + 4 iz).
+"""
+import numpy as np
+
+from ._lib import lib, ptr
+
+# cell offsets inside an oct, in units of the cell size, cell = ix + 2 iy + 4 iz
+CELL_OFF = np.array([[c % 2, (c // 2) % 2, c // 4] for c in range(8)], dtype=np.float64)
+
+
+class OctTree:
+    """An EMMA oct tree in host memory (levels lcoarse..lmax are hydro levels)."""
+
+    def __init__(self, lcoarse, lmax, ngridmax=0):
+        self.lcoarse, self.lmax = lcoarse, lmax
+        self._t = lib().emma_tree_create(lcoarse, lmax, ngridmax)
+        if not self._t:
+            raise RuntimeError("emma_tree_create failed")
+
+    def close(self):
+        if self._t:
+            lib().emma_tree_destroy(self._t)
+            self._t = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def firstoct(self):
+        return lib().emma_tree_firstoct(self._t)
+
+    def noct(self, level):
+        return lib().emma_tree_noct(self._t, level)
+
+    def oct_xyz(self, level):
+        n = self.noct(level)
+        out = np.zeros((n, 3))
+        if n:
+            lib().emma_tree_oct_xyz(self._t, level, ptr(out))
+        return out
+
+    def cell_centres(self, level):
+        dx = 0.5 ** level
+        xyz = self.oct_xyz(level)
+        return (xyz[:, None, :] + (CELL_OFF[None] + 0.5) * dx).reshape(-1, 3)
+
+    def refine(self, level, mark):
+        mark = np.ascontiguousarray(mark, dtype=np.int8)
+        assert mark.size == 8 * self.noct(level)
+        rc = lib().emma_tree_refine(self._t, level, ptr(mark))
+        if rc < 0:
+            raise RuntimeError(f"refinement of level {level} refused for {-rc} cells (2:1 rule)")
+        return rc
+
+    def refine_where(self, level, pred):
+        return self.refine(level, pred(self.cell_centres(level)))
+
+    def set_fields(self, level, d, u, v, w, p):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (d, u, v, w, p)]
+        lib().emma_tree_set_field(self._t, level, *[ptr(a) for a in arrs])
+
+    def get_fields(self, level, which=0):
+        """(7, 8*noct): d,u,v,w,p,a,E of `field` (which=0) or `fieldnew` (which=1)."""
+        n = self.noct(level)
+        out = np.zeros((7, 8 * n))
+        if n:
+            lib().emma_tree_get_field(self._t, level, which, ptr(out))
+        return out
+
+    def topology(self, level):
+        n = self.noct(level)
+        nei = np.zeros(6 * n, np.int32)
+        par = np.zeros(n, np.int32)
+        ch = np.zeros(8 * n, np.int32)
+        lev = np.zeros(n, np.int32)
+        if n:
+            lib().emma_tree_topology(self._t, level, ptr(nei), ptr(par), ptr(ch), ptr(lev))
+        return nei.reshape(n, 6), par, ch.reshape(n, 8), lev
+
+    def split_mask(self, level):
+        return self.topology(level)[2].reshape(-1) >= 0

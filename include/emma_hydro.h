@@ -1,0 +1,167 @@
+/*
+ * emma_hydro.h -- C ABI of libemmahydro, a B200 (sm_100a) implementation of
+ * EMMA's hydro level advance: oct-neighbour gather, MUSCL-Hancock
+ * reconstruction, HLLC fluxes, flux-divergence update and scatter back to the
+ * oct tree, for one AMR level or for a whole coarse step of levels.
+ *
+ * Two ways in:
+ *  1. Drop-in entries with the reference's own names and signatures
+ *     (src/hydro_utils.h:9-10, src/hydro_utils_gpu.h:1-5).  They read and write
+ *     the caller's host oct tree (struct OCT, include/emma_oct.h) on every call,
+ *     so they cost PCIe traffic, exactly like the reference's GPU twin.
+ *  2. Resident entries (emma_hydro_*): upload the tree once, advance levels or
+ *     whole coarse steps on the GPU, download only for I/O.  This is the
+ *     performance path.
+ *
+ * Errors: the reference aborts on invalid states (src/hydro_utils.c:1212,1283,
+ * 1298,3135) and ignores CUDA errors.  Here every entry records a bitmask
+ * (EMMA_ST_*) readable with emma_hydro_status(); entries returning int return
+ * that bitmask of the call (0 = success, negative = argument/setup error).
+ * With EMMA_HYDRO_ABORT=1 in the environment the library aborts like the
+ * reference instead.
+ */
+#ifndef EMMA_HYDRO_H
+#define EMMA_HYDRO_H
+
+#include <stdint.h>
+#include "emma_oct.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define EMMA_ST_NEG_DENSITY 0x01  /* negative density in a face state   (src/hydro_utils.c:1212) */
+#define EMMA_ST_NEG_PSTAR   0x02  /* negative star pressure             (src/hydro_utils.c:1283) */
+#define EMMA_ST_NAN         0x04  /* NaN in a flux or an updated state  (src/hydro_utils.c:1302,3135) */
+#define EMMA_ST_TREE        0x08  /* tree the device path cannot stage (missing neighbour, unsupported slot) */
+#define EMMA_ST_CUDA        0x10  /* a CUDA call failed */
+#define EMMA_ST_ARG         0x20  /* bad argument (level out of range, NULL pointer, no tree) */
+#define EMMA_ST_TIMEOUT     0x40  /* a bounded device wait gave up */
+
+int emma_hydro_status(void);        /* sticky bitmask since the last clear */
+void emma_hydro_clear_status(void);
+const char *emma_hydro_last_error(void); /* human-readable text of the last error */
+
+/* ------------------------------------------------------------ options */
+#define EMMA_PREC_FP64  0  /* plain path: FP64 everywhere, reference operation order */
+#define EMMA_PREC_MIXED 1  /* FP32 reconstruction/Riemann/flux, FP64 compensated update */
+
+/* transmissive boundaries (the reference's -DTRANSXM ... -DTRANSZP) */
+#define EMMA_TRANS_XM 0x01
+#define EMMA_TRANS_XP 0x02
+#define EMMA_TRANS_YM 0x04
+#define EMMA_TRANS_YP 0x08
+#define EMMA_TRANS_ZM 0x10
+#define EMMA_TRANS_ZP 0x20
+
+struct EmmaHydroOptions {
+  int precision;        /* EMMA_PREC_* */
+  int trans_flags;      /* EMMA_TRANS_* */
+  double cfl;           /* Courant number of the level time step (reference param.h: 0.85) */
+  int tile_octs;        /* octs per CTA tile (0 = autotuned) */
+  int device;           /* CUDA device ordinal */
+};
+void emma_hydro_default_options(struct EmmaHydroOptions *opt);
+
+/* ------------------------------------------- drop-in entries (reference names) */
+
+/* HydroSolver (src/hydro_utils.h:9, src/hydro_utils.c:3378): advance every
+ * level-`level` oct of rank cpu->rank by dtnew.  Writes fieldnew of the level's
+ * leaf cells and of their unsplit coarser neighbours (fine->coarse flux
+ * correction), then field := fieldnew on leaves and the primitive mean of the
+ * children on split cells.  `param`, `stencil` and `stride` are accepted for
+ * signature compatibility and not used. */
+void HydroSolver(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu,
+                 struct HGRID *stencil, int stride, REAL dtnew);
+
+/* advancehydroGPU (src/hydro_utils_gpu.h:1, src/hydro_utils_gpu.cu:2470): the
+ * flux computation + scatter part of HydroSolver; returns the number of octs
+ * advanced (0 leaves the caller's final field update out, as in the reference). */
+int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struct HGRID *stencil,
+                    int stride, REAL dxcur, REAL dtnew);
+
+/* clean_new_hydro (src/hydro_utils.h:10, src/hydro_utils.c:3501): fieldnew := field. */
+void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu);
+
+/* Lifecycle entries (src/hydro_utils_gpu.h:2-5, src/hydro_utils_gpu.cu:25-43).
+ * create_hydstencil_GPU initialises the library's device context (the
+ * reference stores a device stencil in cpu->hyd_stencil; this library keeps its
+ * own context and leaves *cpu untouched).  create_pinned_stencil allocates the
+ * caller's page-locked HGRID scratch of `stride` entries as the reference does. */
+void create_hydstencil_GPU(struct CPUINFO *cpu, int stride);
+void destroy_hydstencil_GPU(struct CPUINFO *cpu, int stride);
+void create_pinned_stencil(struct HGRID **stencil, int stride);
+void destroy_pinned_stencil(struct HGRID **stencil, int stride);
+
+/* ---------------------------------------------------------- resident path */
+
+/* Create the device context (idempotent).  NULL options = defaults. */
+int emma_hydro_init(const struct EmmaHydroOptions *opt);
+int emma_hydro_set_options(const struct EmmaHydroOptions *opt);
+void emma_hydro_shutdown(void);
+/* Launch on the caller's CUDA stream (a cudaStream_t; NULL = the library's own
+ * stream).  Entries still synchronise the stream where they return host data. */
+int emma_hydro_set_stream(void *stream);
+
+/* Mirror levels lcoarse..lmax of the host tree (rank `rank`) onto the GPU:
+ * per-level SoA state (d,u,v,w,p of `field`), topology and tile plans.
+ * The tree structure must not change until the next upload. */
+int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int rank);
+/* Copy the device state back into `field` and `fieldnew` of the host tree
+ * (a and E recomputed as the reference stores them). */
+int emma_hydro_tree_download(struct OCT **firstoct);
+/* Re-read only the fields (same structure) / write only the fields. */
+int emma_hydro_fields_upload(struct OCT **firstoct);
+
+/* Level operations on the resident tree (reference counterparts in brackets). */
+int emma_hydro_clean_new(int level);                      /* [clean_new_hydro] */
+int emma_hydro_comptstep(int level, double *dt_out);      /* [L_comptstep_hydro, src/advanceamr.c:92] */
+int emma_hydro_advance_level(int level, double dt);       /* [HydroSolver] */
+
+/* One coarse step of the hydro-only level schedule (src/advanceamr.c:243-1299):
+ * finer levels first, up to `nsub` subcycles, CFL time steps.  `adt` (lmax
+ * entries, in/out) is the reference's per-level dt array; tsim is advanced. */
+int emma_hydro_advance_coarse_step(double dt_param, double time_max, int nsub,
+                                   double *tsim, double *adt);
+
+/* SoA access for tests and I/O: 5 planes (d,u,v,w,p) of 8*noct doubles each, list order. */
+int emma_hydro_level_noct(int level);
+int emma_hydro_get_level_state(int level, double *host_out);
+int emma_hydro_set_level_state(int level, const double *host_in);
+/* Leaf cell count of a level (cells advanced per level substep). */
+long long emma_hydro_level_leaf_cells(int level);
+/* Cell-updates performed since the last reset (leaf cells x level substeps). */
+long long emma_hydro_cell_updates(void);
+/* Kernels of this library launched since the last reset. */
+long long emma_hydro_kernel_launches(void);
+void emma_hydro_reset_counters(void);
+/* Average device time (ms) of the level kernel launches since the last reset,
+ * measured with CUDA events on the launching stream, and their count. */
+int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cells);
+
+/* Planning diagnostics, host only (no GPU needed): per level lcoarse..lmax,
+ * stats5[5*(L-lcoarse)+{0..4}] = octs, tiles, max staged octs per tile, max
+ * halo cells per tile, leaf cells.  Returns EMMA_ST_* bits of the planning. */
+int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int trans_flags, long long *stats5);
+
+/* --------------------------------------------------- host tree utilities */
+/* Build an oct tree with the reference's construction order
+ * (build_initial_grid src/amr.c:1507, L_refine_cells src/amr.c:286), for
+ * callers (tests, benchmarks) that have no EMMA tree.  One tree at a time. */
+struct EmmaTree;
+struct EmmaTree *emma_tree_create(int lcoarse, int lmax, long long ngridmax);
+void emma_tree_destroy(struct EmmaTree *t);
+int emma_tree_refine(struct EmmaTree *t, int level, const signed char *mark);
+struct OCT **emma_tree_firstoct(struct EmmaTree *t);
+int emma_tree_noct(struct EmmaTree *t, int level);
+void emma_tree_oct_xyz(struct EmmaTree *t, int level, double *xyz);
+void emma_tree_set_field(struct EmmaTree *t, int level, const double *d, const double *u,
+                         const double *v, const double *w, const double *p);
+void emma_tree_get_field(struct EmmaTree *t, int level, int which, double *out7);
+void emma_tree_topology(struct EmmaTree *t, int level, int *nei, int *parent, int *child, int *lev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,69 @@
+/*
+ * emma_oct.h -- the oct-tree memory layout that EMMA's hydro entry points pass
+ * around, declared for a build with -DWHYDRO2 (and neither -DWGRAV, -DWRAD,
+ * -DPIC nor -DWRADHYD), REAL = double, NVAR = 6.
+ *
+ * This is an interface, not an implementation: libemmahydro reads and writes the
+ * caller's tree in place, so the field order, types and padding must be exactly
+ * those of the reference (src/prototypes.h:611 Wtype, :653 Utype, :825 CELL,
+ * :1028 OCT).  Sizes are checked at compile time: CELL 136 B, OCT 1200 B.
+ * Only the members the hydro path uses are named; nothing else is assumed.
+ */
+#ifndef EMMA_OCT_H
+#define EMMA_OCT_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef double REAL;
+
+struct Wtype {           /* primitive state of a cell, src/prototypes.h:611 */
+  REAL d, u, v, w, p;    /* density, velocity, pressure */
+  REAL a;                /* sound speed */
+  REAL E;                /* total energy density */
+};
+
+struct OCT;
+
+struct CELL {            /* src/prototypes.h:825 (WHYDRO2 members only) */
+  struct OCT *child;     /* finer oct, NULL for a leaf */
+  REAL marked;           /* refinement mark */
+  int idx;               /* index of the cell within its oct: ix + 2 iy + 4 iz */
+  struct Wtype field;    /* state at the start of the level step */
+  struct Wtype fieldnew; /* state being built during the level step */
+};
+
+struct OCT {             /* src/prototypes.h:1028 */
+  struct CELL cell[8];
+  struct CELL *nei[6];   /* face neighbours at level-1: -x,+x,-y,+y,-z,+z */
+  struct CELL *parent;   /* parent cell at level-1 */
+  struct OCT *next;      /* next oct of the same level (list order) */
+  struct OCT *prev;
+  struct OCT *nexthash;
+  REAL x, y, z;          /* lower-left corner */
+  int cpu;               /* owning rank */
+  int level;             /* level of the cells of this oct */
+};
+
+/* Opaque in this library: only `rank` (the first member, offset 0 under every
+ * compile-time flag set of the reference) is read by the drop-in entries. */
+struct CPUINFO;
+struct RUNPARAMS;
+struct HGRID;
+
+#define EMMA_SIZEOF_HGRID 16576 /* sizeof(struct HGRID) for this build */
+
+#ifdef __cplusplus
+}
+#endif
+
+#ifdef __cplusplus
+static_assert(sizeof(struct CELL) == 136, "struct CELL must match the reference layout");
+static_assert(sizeof(struct OCT) == 1200, "struct OCT must match the reference layout");
+#else
+_Static_assert(sizeof(struct CELL) == 136, "struct CELL must match the reference layout");
+_Static_assert(sizeof(struct OCT) == 1200, "struct OCT must match the reference layout");
+#endif
+
+#endif

@@ -1,0 +1,172 @@
+"""ctypes bindings of the oracle libraries.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference arm, always as the checker or the timed CPU
+baseline, never on the product path.
+
+  Restatement  -- oracle/_build/liboracle.so, the C restatement of the hydro level
+                  advance (hydro_oracle.c); runs in place on any struct OCT tree.
+  RefTree      -- oracle/_ref/libemmaref[_tx].so, the reference's own CPU hydro
+                  compiled from its sources with ref_driver.c (tree built by the
+                  reference's build_initial_grid / L_refine_cells).
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
+REF_LIB = os.path.join(HERE, "_ref", "libemmaref.so")
+REF_LIB_TX = os.path.join(HERE, "_ref", "libemmaref_tx.so")
+
+HYDROTEST = 0x40
+c_int, c_double, c_void_p, c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
+
+
+def _p(a):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def flags_for(trans):
+    """Oracle flags for the library's transmissive flags (which follow HYDROTEST semantics)."""
+    return (trans | HYDROTEST) if trans else 0
+
+
+class Restatement:
+    _lib = None
+
+    def __init__(self):
+        if Restatement._lib is None:
+            if not os.path.exists(ORACLE_LIB):
+                raise RuntimeError(f"oracle restatement not built: {ORACLE_LIB}")
+            L = ctypes.CDLL(ORACLE_LIB)
+            L.orc_hydro_solver.argtypes = [c_void_p, c_int, c_double, c_int]
+            L.orc_hydro_solver.restype = c_int
+            L.orc_clean_new_hydro.argtypes = [c_void_p, c_int]
+            L.orc_comptstep_hydro.argtypes = [c_void_p, c_int, c_double]
+            L.orc_comptstep_hydro.restype = c_double
+            L.orc_run.argtypes = [c_void_p, c_int, c_int, c_int, c_double, c_double, c_int, c_double, c_int,
+                                  c_double, c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]
+            L.orc_run.restype = c_double
+            L.orc_cell_updates.restype = c_ll
+            Restatement._lib = L
+        self.L = Restatement._lib
+
+    def run(self, firstoct, lcoarse, lmax, nsteps, cfl, trans=0, nsub=2, dt_param=1e9, time_max=1e9, tsim0=0.0):
+        adt = np.zeros(lmax)
+        nd, err = c_int(), c_int()
+        t = self.L.orc_run(firstoct, lcoarse, lmax, nsteps, dt_param, time_max, nsub, cfl, flags_for(trans),
+                           tsim0, _p(adt), ctypes.byref(nd), ctypes.byref(err))
+        return t, adt, err.value
+
+    def hydro_solver(self, firstoct, level, dt, trans=0):
+        return self.L.orc_hydro_solver(firstoct, level, dt, flags_for(trans))
+
+    def clean_new(self, firstoct, level):
+        self.L.orc_clean_new_hydro(firstoct, level)
+
+    def comptstep(self, firstoct, level, cfl):
+        return self.L.orc_comptstep_hydro(firstoct, level, cfl)
+
+    def cell_updates(self):
+        return self.L.orc_cell_updates()
+
+    def reset(self):
+        self.L.orc_reset_counters()
+
+
+def ref_available(tx=False):
+    return os.path.exists(REF_LIB_TX if tx else REF_LIB)
+
+
+class RefTree:
+    """A tree built and advanced by the reference's own CPU hydro (one live tree per library)."""
+
+    _libs = {}
+
+    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024):
+        path = REF_LIB_TX if tx else REF_LIB
+        if path not in RefTree._libs:
+            if not os.path.exists(path):
+                raise RuntimeError(f"reference oracle not built: {path}")
+            L = ctypes.CDLL(path, mode=os.RTLD_NOW | os.RTLD_LOCAL)
+            L.ref_run.restype = c_double
+            L.ref_run.argtypes = [c_int, c_double, c_double, c_int, c_double, ctypes.POINTER(c_int)]
+            L.ref_comptstep_hydro.restype = c_double
+            L.ref_hydro_solver.argtypes = [c_int, c_double]
+            L.ref_grid_base.restype = c_void_p
+            L.ref_firstoct_array.restype = c_void_p
+            L.ref_hydro_seconds.restype = c_double
+            L.ref_cell_updates.restype = c_ll
+            L.ref_adt.restype = c_double
+            L.ref_init.argtypes = [c_int, c_int, c_int, c_int]
+            RefTree._libs[path] = L
+        self.L = RefTree._libs[path]
+        self.lcoarse, self.lmax = lcoarse, lmax
+        if ngridmax is None:
+            ngridmax = sum(8 ** (l - 1) for l in range(1, lcoarse + 1)) * (2 if lmax > lcoarse else 1) + 8 ** min(lmax, 7) // 2 + 1024
+        self.ngridmax = int(ngridmax)
+        if self.L.ref_init(lcoarse, lmax, self.ngridmax, hstride) != 0:
+            raise RuntimeError("ref_init failed")
+
+    @property
+    def firstoct(self):
+        return self.L.ref_firstoct_array()
+
+    def noct(self, level):
+        return self.L.ref_noct(level)
+
+    def oct_xyz(self, level):
+        n = self.noct(level)
+        out = np.zeros((n, 3))
+        if n:
+            self.L.ref_oct_xyz(level, _p(out))
+        return out
+
+    def cell_centres(self, level):
+        dx = 0.5 ** level
+        off = np.array([[c % 2, (c // 2) % 2, c // 4] for c in range(8)], dtype=np.float64)
+        return (self.oct_xyz(level)[:, None, :] + (off[None] + 0.5) * dx).reshape(-1, 3)
+
+    def refine(self, level, mark):
+        mark = np.ascontiguousarray(mark, dtype=np.int8)
+        return self.L.ref_refine(level, _p(mark))
+
+    def refine_where(self, level, pred):
+        return self.refine(level, pred(self.cell_centres(level)))
+
+    def set_fields(self, level, d, u, v, w, p):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (d, u, v, w, p)]
+        self.L.ref_set_field(level, *[_p(a) for a in arrs])
+
+    def get_fields(self, level, which=0):
+        n = self.noct(level)
+        out = np.zeros((7, 8 * n))
+        if n:
+            self.L.ref_get_field(level, which, _p(out))
+        return out
+
+    def topology(self, level):
+        n = self.noct(level)
+        nei = np.zeros(6 * n, np.int32)
+        par = np.zeros(n, np.int32)
+        ch = np.zeros(8 * n, np.int32)
+        lev = np.zeros(n, np.int32)
+        if n:
+            self.L.ref_topology(level, _p(nei), _p(par), _p(ch), _p(lev))
+        return nei.reshape(n, 6), par, ch.reshape(n, 8), lev
+
+    def run(self, nsteps, nsub=2, dt_param=1e9, time_max=1e9, tsim0=0.0):
+        nd = c_int()
+        t = self.L.ref_run(nsteps, dt_param, time_max, nsub, tsim0, ctypes.byref(nd))
+        return t, np.array([self.L.ref_adt(l) for l in range(1, self.lmax + 1)])
+
+    def hydro_seconds(self):
+        return self.L.ref_hydro_seconds()
+
+    def cell_updates(self):
+        return self.L.ref_cell_updates()
+
+    def reset_counters(self):
+        self.L.ref_reset_counters()

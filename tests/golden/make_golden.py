@@ -1,0 +1,61 @@
+"""Generate the golden fixtures from the reference's own CPU hydro (oracle/_ref).
+
+Run from the repository root where the reference checkout is available:
+    make -C oracle && python tests/golden/make_golden.py
+Each fixture: a seeded small tree (uniform or refined spheres about the box
+centre), the input primitive fields per level, and the reference's `field`
+(d,u,v,w,p,a,E) per level after `nsteps` coarse steps at CFL 0.8.
+"""
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(ROOT, "oracle"))
+import oracle  # noqa: E402
+
+CASES = [
+    # name, base, lmax, radii, nsteps, transmissive(x), field kind
+    ("uniform_l3_periodic", 3, 3, (), 3, 0, "random"),
+    ("sod_l4_transmissive", 4, 4, (), 8, 3, "sod"),
+    ("amr_l3_5_periodic", 3, 5, (0.35, 0.2), 2, 0, "random"),
+]
+
+
+def fields(kind, c, rng):
+    n = len(c)
+    if kind == "sod":
+        left = c[:, 0] < 0.5
+        z = np.zeros(n)
+        return np.where(left, 1.0, 0.125), z, z.copy(), z.copy(), np.where(left, 1.0, 0.1)
+    d = rng.uniform(0.5, 1.5, n)
+    p = rng.uniform(0.5, 1.5, n)
+    u, v, w = (rng.uniform(-0.5, 0.5, n) for _ in range(3))
+    return d, u, v, w, p
+
+
+def main():
+    for name, base, lmax, radii, nsteps, trans, kind in CASES:
+        ref = oracle.RefTree(base, lmax, tx=bool(trans), ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)))
+        for i, r in enumerate(radii):
+            ref.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
+        rng = np.random.default_rng(12345)
+        out = {"meta": np.array([base, lmax, nsteps, trans]), "radii": np.array(radii, dtype=np.float64)}
+        for l in range(base, lmax + 1):
+            f = fields(kind, ref.cell_centres(l), rng)
+            ref.set_fields(l, *f)
+            out[f"in_{l}"] = np.array(f)
+        tsim, adt = ref.run(nsteps)
+        out["tsim"] = np.array(tsim)
+        out["adt"] = adt
+        for l in range(base, lmax + 1):
+            out[f"out_{l}"] = ref.get_fields(l, 0)
+        path = os.path.join(HERE, name + ".npz")
+        np.savez_compressed(path, **out)
+        print(path, os.path.getsize(path), "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,43 @@
+"""The C-ABI library loads and exports every entry declared in include/*.h (no GPU needed)."""
+import ctypes
+import os
+import re
+
+from conftest import ROOT
+
+HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include"))) if f.endswith(".h")]
+
+
+def declared_functions():
+    names = set()
+    for h in HEADERS:
+        src = open(h).read()
+        src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+        src = re.sub(r"//[^\n]*", "", src)
+        for m in re.finditer(r"^[A-Za-z_][\w \*]*?\b([A-Za-z_]\w*)\s*\([^;{]*\)\s*;", src, flags=re.M):
+            name = m.group(1)
+            if name not in ("static_assert", "_Static_assert", "sizeof"):
+                names.add(name)
+    return names
+
+
+def test_headers_declare_the_reference_entries():
+    names = declared_functions()
+    for ref_name in ("HydroSolver", "advancehydroGPU", "clean_new_hydro", "create_hydstencil_GPU",
+                     "destroy_hydstencil_GPU", "create_pinned_stencil", "destroy_pinned_stencil"):
+        assert ref_name in names
+
+
+def test_library_exports_every_declared_symbol():
+    from emma_b200._lib import LIB_PATH, SIGNATURES
+    L = ctypes.CDLL(LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing
+    bound = {n for n, _, _ in SIGNATURES}
+    assert declared_functions() <= bound, declared_functions() - bound
+
+
+def test_struct_layout_matches_reference():
+    # struct OCT must be 1200 bytes (src/prototypes.h:1028 with -DWHYDRO2, REAL=double)
+    from oracle import Restatement
+    assert Restatement().L.orc_sizeof_oct() == 1200
