@@ -130,7 +130,9 @@ def run_mine(args, rank, world):
 
     dev = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(dev)
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it and the CUDA events below are recorded on it
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     L = lib()
     cfg = build_config(args.config)
     t0 = time.time()
@@ -241,13 +243,10 @@ def cpu_baseline_sample(config):
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
     try:
-        ref = oracle.RefTree(cfg.lcoarse, cfg.lmax, tx=(config == "sod"),
-                             ngridmax=sum(8 ** (l - 1) for l in range(1, cfg.lcoarse + 1)) * 2 + 200000)
-        for i, lev in enumerate(range(cfg.lcoarse, cfg.lmax)):
-            pass
-        t = cfg.build(lambda lc, lm: ref) if cfg.lmax == cfg.lcoarse else None
-        if t is None:
-            return None
+        # room for every oct plus the reference's free-oct chain head (src/emma.c:765)
+        ngrid = sum(8 ** (l - 1) for l in range(1, cfg.lmax + 1)) + 1024
+        ref = oracle.RefTree(cfg.lcoarse, cfg.lmax, tx=(config == "sod"), ngridmax=ngrid)
+        cfg.build(lambda lc, lm: ref)  # the configuration's own generator, on the reference's tree
         ref.reset_counters()
         ref.run(1, nsub=cfg.nsub)
         secs, cells = ref.hydro_seconds(), ref.cell_updates()
@@ -279,10 +278,7 @@ def run_reference(args):
     os.dup2(devnull, 1)
     try:
         ref = oracle.RefTree(level, level, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, level + 1)) + 16)
-        c = ref.cell_centres(level)
-        # same generator as the configuration, at the sample's size
-        t = cfg.build(lambda lc, lm: ref)
-        del t
+        cfg.build(lambda lc, lm: ref)  # same generator as the configuration, at the sample's size
         for _ in range(args.warmup):
             ref.run(1)
         ref.reset_counters()

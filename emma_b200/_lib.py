@@ -78,7 +78,9 @@ def lib():
         return _lib
     if not os.path.exists(LIB_PATH):
         raise RuntimeError(f"libemmahydro.so is not built ({LIB_PATH}); run emma_b200.build.build()")
-    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_GLOBAL)
+    # RTLD_LOCAL: the drop-in entries carry the reference's names (HydroSolver, ...);
+    # they must not interpose on another library that defines the same symbols
+    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_LOCAL)
     for name, res, args in SIGNATURES:
         fn = getattr(L, name)
         fn.restype = res

@@ -35,6 +35,7 @@ struct DevLevel {
   uint32_t *keys = nullptr;
   uint8_t *graph = nullptr;
   uint16_t *halo = nullptr;
+  uint16_t *bface = nullptr;
 };
 
 struct TimedLaunch {
@@ -147,6 +148,7 @@ void free_level(DevLevel &d) {
   cudaFree(d.keys);
   cudaFree(d.graph);
   cudaFree(d.halo);
+  cudaFree(d.bface);
   d = DevLevel();
 }
 
@@ -183,6 +185,7 @@ bool alloc_levels(const HostTree &H, std::vector<DevLevel> &dl, bool with_base) 
     if (!upload_vec(&d.keys, h.keys)) return false;
     if (!upload_vec(&d.graph, h.graph)) return false;
     if (!upload_vec(&d.halo, h.halo)) return false;
+    if (!upload_vec(&d.bface, h.bface)) return false;
   }
   return true;
 }
@@ -236,6 +239,7 @@ bool launch_level(const DevLevel *Lc, DevLevel &Ld, const DevLevel *Lf, double d
   a.keys = Ld.keys;
   a.graph = Ld.graph;
   a.halo = Ld.halo;
+  a.bface = Ld.bface;
   a.dt = dt;
   a.dx = std::pow(0.5, Ld.L);
   a.status = g.d_status;
@@ -545,6 +549,8 @@ int emma_hydro_set_stream(void *stream) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
   CK(cudaStreamSynchronize(g.stream));
   if (g.own_stream) CK(cudaStreamDestroy(g.stream));
+  // NULL selects a stream owned by the library (a caller wanting the legacy
+  // default stream passes cudaStreamLegacy)
   if (stream == nullptr) {
     CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
     g.own_stream = true;

@@ -142,8 +142,10 @@ struct MathF64 {
   // findPressure_Hybrid + speedestimate*_HLLC (src/hydro_utils.c:625,1264)
   static __device__ __forceinline__ void speeds(const double WL[7], const double WR[7], int n, double &SL, double &SR,
                                                 double &ustar, unsigned &st) {
-    S1 L{WL[0], WL[1 + n], WL[4], sqrt(kGam * WL[4] / WL[0])};
-    S1 R{WR[0], WR[1 + n], WR[4], sqrt(kGam * WR[4] / WR[0])};
+    const double uLn = (n == 0) ? WL[1] : ((n == 1) ? WL[2] : WL[3]);
+    const double uRn = (n == 0) ? WR[1] : ((n == 1) ? WR[2] : WR[3]);
+    S1 L{WL[0], uLn, WL[4], sqrt(kGam * WL[4] / WL[0])};
+    S1 R{WR[0], uRn, WR[4], sqrt(kGam * WR[4] / WR[0])};
     double dbar = 0.5 * (L.d + R.d), abar = 0.5 * (L.a + R.a);
     double ppvrs = 0.5 * ((L.p + R.p) + (L.u - R.u) * dbar * abar);
     double pmax = fmax(L.p, R.p), pmin = fmin(L.p, R.p);
@@ -176,49 +178,77 @@ struct MathF64 {
     if (isnan(ustar)) st |= kStNan;
   }
 
-  // getflux_{X,Y,Z} of W2U(W) (src/hydro_utils.c:66,916-968), axis n
-  static __device__ __forceinline__ void euler(const double W[7], int n, double f[5]) {
-    const double d = W[0];
-    const double m[3] = {W[0] * W[1], W[0] * W[2], W[0] * W[3]};
-    const double E = W[6];
-    const double mn = m[n];
-    const int t1 = (n == 0) ? 1 : 0, t2 = (n == 2) ? 1 : 2;
-    const double all = m[0] * m[0] + m[1] * m[1] + m[2] * m[2];
-    f[0] = mn;
-    f[1 + n] = 0.5 * (3. - kGam) * mn * mn / d + (kGam - 1.) * E - 0.5 * (kGam - 1.) * (m[t1] * m[t1] + m[t2] * m[t2]) / d;
-    f[1 + t1] = mn * m[t1] / d;
-    f[1 + t2] = mn * m[t2] / d;
-    f[4] = kGam * mn / d * E - 0.5 * (kGam - 1.) * mn / (d * d) * all;
+  // Face state toward face k from the slope along k's axis only (the other
+  // axes enter the reference's sum with coefficient 0).
+  static __device__ __forceinline__ void face_ax(const double q0[5], const double Dax[5], const double Wt[5], int k,
+                                                 double W[7], unsigned &st) {
+    const double f = (k & 1) ? 0.5 : -0.5;
+#pragma unroll
+    for (int i = 0; i < 5; i++) W[i] = q0[i] + f * Dax[i] + Wt[i];
+    W[4] = fmax(W[4], kPmin);
+    if (W[0] < 0) st |= kStNegDensity;
+    W[6] = W[4] / (kGam - 1.) + 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]);
+    W[5] = sqrt(kGam * W[4] / W[0]);
   }
 
-  // HLLC flux across a face normal to axis n (src/hydro_utils.c:2055-2138)
+  // State rotated to the face frame: r = {d, u_n, u_t1, u_t2, p, E, |m|^2},
+  // t1 < t2 the transverse axes in x,y,z order, |m|^2 summed in x,y,z order.
+  static __device__ __forceinline__ void rotate(const double W[7], int n, double r[7]) {
+    r[0] = W[0];
+    r[1] = (n == 0) ? W[1] : ((n == 1) ? W[2] : W[3]);
+    r[2] = (n == 0) ? W[2] : W[1];
+    r[3] = (n == 2) ? W[2] : W[3];
+    r[4] = W[4];
+    r[5] = W[6];
+    const double m0 = W[0] * W[1], m1 = W[0] * W[2], m2 = W[0] * W[3];
+    r[6] = m0 * m0 + m1 * m1 + m2 * m2;
+  }
+
+  // getflux_{X,Y,Z} of W2U(W) (src/hydro_utils.c:66,916-968) in the face frame
+  static __device__ __forceinline__ void euler_rot(const double r[7], double f[5]) {
+    const double d = r[0], E = r[5];
+    const double mn = d * r[1], mt1 = d * r[2], mt2 = d * r[3];
+    f[0] = mn;
+    f[1] = 0.5 * (3. - kGam) * mn * mn / d + (kGam - 1.) * E - 0.5 * (kGam - 1.) * (mt1 * mt1 + mt2 * mt2) / d;
+    f[2] = mn * mt1 / d;
+    f[3] = mn * mt2 / d;
+    f[4] = kGam * mn / d * E - 0.5 * (kGam - 1.) * mn / (d * d) * r[6];
+  }
+
+  // HLLC flux across a face normal to axis n (src/hydro_utils.c:2055-2138),
+  // returned in x,y,z order: F = {mass, mom_x, mom_y, mom_z, energy}.
   static __device__ __forceinline__ void hllc(const double WL[7], const double WR[7], int n, double F[5],
                                               unsigned &st) {
     double SL, SR, ustar;
     speeds(WL, WR, n, SL, SR, ustar, st);
-#pragma unroll
-    for (int k = 0; k < 5; k++) F[k] = 0.;
+    double rL[7], rR[7], G[5] = {0., 0., 0., 0., 0.};
+    rotate(WL, n, rL);
+    rotate(WR, n, rR);
     if (SL >= 0.) {
-      euler(WL, n, F);
+      euler_rot(rL, G);
     } else if (SR <= 0.) {
-      euler(WR, n, F);
+      euler_rot(rR, G);
     } else {
       const bool left = (SL < 0.) && (ustar >= 0.);
       const bool right = (ustar <= 0.) && (SR > 0.);
       if (left || right) {
-        const double *W = left ? WL : WR;
+        const double *r = left ? rL : rR;
         const double S = left ? SL : SR;
-        euler(W, n, F);
-        const double d = W[0], un = W[1 + n];
-        const double Ud = W[0], UE = W[6];
-        const double mom[3] = {W[0] * W[1], W[0] * W[2], W[0] * W[3]};
+        euler_rot(r, G);
+        const double d = r[0], un = r[1], E = r[5];
         const double fact = d * (S - un) / (S - ustar);
-        F[0] += (fact * 1. - Ud) * S;
-#pragma unroll
-        for (int k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : W[1 + k]) - mom[k]) * S;
-        F[4] += (fact * (UE / Ud + (ustar - un) * (ustar + W[4] / (d * (S - un)))) - UE) * S;
+        G[0] += (fact * 1. - d) * S;
+        G[1] += (fact * ustar - d * un) * S;
+        G[2] += (fact * r[2] - d * r[2]) * S;
+        G[3] += (fact * r[3] - d * r[3]) * S;
+        G[4] += (fact * (E / d + (ustar - un) * (ustar + r[4] / (d * (S - un)))) - E) * S;
       }
     }
+    F[0] = G[0];
+    F[1] = (n == 0) ? G[1] : G[2];
+    F[2] = (n == 0) ? G[2] : ((n == 1) ? G[1] : G[3]);
+    F[3] = (n == 2) ? G[1] : G[3];
+    F[4] = G[4];
   }
 };
 
@@ -255,13 +285,13 @@ struct MathF32 {
     Wt[4] = -dtdx_half * acc4;
   }
 
-  // Face state: W0 +- D/2 + Wt, pressure floor; returns d,u,v,w,p, 1/d and a
-  static __device__ __forceinline__ void face(const float q0[5], const float D[3][5], const float Wt[5], int k,
-                                              float W[7], unsigned &st) {
-    const int ax = k >> 1;
+  // Face state toward face k: W0 +- D_axis/2 + Wt, pressure floor.
+  // W = {d, u, v, w, p, 1/d, a}.
+  static __device__ __forceinline__ void face_ax(const float q0[5], const float Dax[5], const float Wt[5], int k,
+                                                 float W[7], unsigned &st) {
     const float s = (k & 1) ? 0.5f : -0.5f;
 #pragma unroll
-    for (int i = 0; i < 5; i++) W[i] = q0[i] + s * D[ax][i] + Wt[i];
+    for (int i = 0; i < 5; i++) W[i] = q0[i] + s * Dax[i] + Wt[i];
     W[4] = fmaxf(W[4], (float)kPmin);
     if (W[0] < 0.f) st |= kStNegDensity;
     W[5] = rcp(W[0]);
@@ -293,14 +323,17 @@ struct MathF32 {
     return p;
   }
 
-  static __device__ __forceinline__ void speeds(const float WL[7], const float WR[7], int n, float &SL, float &SR,
-                                                float &ustar, unsigned &st) {
-    const float dL = WL[0], uL = WL[1 + n], pL = WL[4], aL = WL[6];
-    const float dR = WR[0], uR = WR[1 + n], pR = WR[4], aR = WR[6];
+  // HLLC flux across a face normal to axis n; states W = {d,u,v,w,p,1/d,a}.
+  static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st) {
+    const float dL = WL[0], pL = WL[4], iL = WL[5], aL = WL[6];
+    const float dR = WR[0], pR = WR[4], iR = WR[5], aR = WR[6];
+    const float uL = (n == 0) ? WL[1] : ((n == 1) ? WL[2] : WL[3]);
+    const float uR = (n == 0) ? WR[1] : ((n == 1) ? WR[2] : WR[3]);
+    // hybrid PVRS / TRRS / TSRS star pressure (Toro sec. 9.5.2), as the reference
     const float dbar = 0.5f * (dL + dR), abar = 0.5f * (aL + aR);
     const float ppvrs = 0.5f * ((pL + pR) + (uL - uR) * dbar * abar);
     const float pmax = fmaxf(pL, pR), pmin = fminf(pL, pR);
-    float pstar = ppvrs;
+    float pstar = ppvrs, ustar;
     if ((pmax < 2.f * pmin) && (pmin < pstar) && (pstar < pmax)) {
       ustar = 0.5f * ((uL + uR) + fdiv(pL - pR, dbar * abar));
     } else if (pstar < pmin) {
@@ -311,7 +344,7 @@ struct MathF32 {
       ustar = uL - 2.f * aL / (G - 1.f) * (__powf(fdiv(pstar, pL), z) - 1.f);
     } else {
       const float p0 = fmaxf(0.f, ppvrs);
-      const float AL = 2.f / (G + 1.f) * WL[5], AR = 2.f / (G + 1.f) * WR[5];
+      const float AL = 2.f / (G + 1.f) * iL, AR = 2.f / (G + 1.f) * iR;
       const float BL = (G - 1.f) / (G + 1.f) * pL, BR = (G - 1.f) / (G + 1.f) * pR;
       const float GL = sqrtf(fdiv(AL, p0 + BL)), GR = sqrtf(fdiv(AR, p0 + BR));
       pstar = fdiv(GL * pL + GR * pR - (uR - uL), GL + GR);
@@ -322,49 +355,42 @@ struct MathF32 {
     const float g2 = (G + 1.f) / (2.f * G);
     const float qL = (pstar <= pL) ? 1.f : sqrtf(1.f + g2 * (fdiv(pstar, pL) - 1.f));
     const float qR = (pstar <= pR) ? 1.f : sqrtf(1.f + g2 * (fdiv(pstar, pR) - 1.f));
-    SL = uL - aL * qL;
-    SR = uR + aR * qR;
+    float SL = uL - aL * qL, SR = uR + aR * qR;
     if (SL > SR) {
       SL = fminf(uL - aL, uR - aR);
       SR = fmaxf(uL + aL, uR + aR);
     }
     if (isnan(ustar)) st |= kStNan;
-  }
-
-  // W[7] = d,u,v,w,p,1/d,a.  Euler flux along axis n.
-  static __device__ __forceinline__ void euler(const float W[7], int n, float f[5], float &E) {
-    const float d = W[0], un = W[1 + n];
-    const float ke = 0.5f * d * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]);
-    E = W[4] * (1.f / (G - 1.f)) + ke;
-    f[0] = d * un;
-    f[1] = f[0] * W[1];
-    f[2] = f[0] * W[2];
-    f[3] = f[0] * W[3];
-    f[1 + n] += W[4];
-    f[4] = un * (E + W[4]);
-  }
-
-  static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st) {
-    float SL, SR, ustar;
-    speeds(WL, WR, n, SL, SR, ustar, st);
+    // upwind side and its rotated state
     const bool useL = (SL >= 0.f) || (!(SR <= 0.f) && (ustar >= 0.f));
     const float *W = useL ? WL : WR;
-    float E;
-    euler(W, n, F, E);
-    if (SL >= 0.f || SR <= 0.f) return;
-    if (!((SL < 0.f && ustar >= 0.f) || (ustar <= 0.f && SR > 0.f))) {
-#pragma unroll
-      for (int k = 0; k < 5; k++) F[k] = 0.f;
-      return;
+    const float d = W[0], p = W[4], id = W[5];
+    const float un = useL ? uL : uR;
+    const float t1 = (n == 0) ? W[2] : W[1];
+    const float t2 = (n == 2) ? W[2] : W[3];
+    const float E = p * (1.f / (G - 1.f)) + 0.5f * d * (un * un + t1 * t1 + t2 * t2);
+    const float mn = d * un;
+    float G0 = mn, GN = mn * un + p, G1 = mn * t1, G2 = mn * t2, G4 = un * (E + p);
+    const bool star = !(SL >= 0.f || SR <= 0.f);
+    if (star) {
+      if ((SL < 0.f && ustar >= 0.f) || (ustar <= 0.f && SR > 0.f)) {
+        const float S = useL ? SL : SR;
+        const float Smu = S - un;
+        const float fact = fdiv(d * Smu, S - ustar);
+        G0 += (fact - d) * S;
+        GN += (fact * ustar - mn) * S;
+        G1 += (fact - d) * t1 * S;
+        G2 += (fact - d) * t2 * S;
+        G4 += (fact * (E * id + (ustar - un) * (ustar + fdiv(p, d * Smu))) - E) * S;
+      } else {
+        G0 = GN = G1 = G2 = G4 = 0.f;
+      }
     }
-    const float S = useL ? SL : SR;
-    const float d = W[0], un = W[1 + n];
-    const float Smu = S - un;
-    const float fact = fdiv(d * Smu, S - ustar);
-    F[0] += (fact - d) * S;
-#pragma unroll
-    for (int k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : W[1 + k]) - d * W[1 + k]) * S;
-    F[4] += (fact * (E * W[5] + (ustar - un) * (ustar + fdiv(W[4], d * Smu))) - E) * S;
+    F[0] = G0;
+    F[1] = (n == 0) ? GN : G1;
+    F[2] = (n == 0) ? G1 : ((n == 1) ? GN : G2);
+    F[3] = (n == 2) ? GN : G2;
+    F[4] = G4;
   }
 };
 

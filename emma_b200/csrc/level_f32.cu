@@ -4,14 +4,13 @@
 
 namespace emma {
 
-constexpr int kSMaxF32 = 160, kHMaxF32 = 320;
-using KF32 = LevelSmem<MathF32, kTileOcts, kSMaxF32, kHMaxF32>;
+using KF32 = LevelSmem<MathF32, kTileOcts, kSMax, kHMax, kBMax>;
 
 size_t level_smem_f32() { return KF32::bytes; }
 
 cudaError_t launch_level_f32(const LevelArgs &a, cudaStream_t s) {
   static bool attr = false;
-  auto k = level_advance_kernel<MathF32, kTileOcts, kSMaxF32, kHMaxF32>;
+  auto k = level_advance_kernel<MathF32, kTileOcts, kSMax, kHMax, kBMax>;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KF32::bytes);
     if (e != cudaSuccess) return e;

@@ -5,13 +5,13 @@
 
 namespace emma {
 
-using KF64 = LevelSmem<MathF64, kTileOcts, kSMax, kHMax>;
+using KF64 = LevelSmem<MathF64, kTileOcts, kSMax, kHMax, kBMax>;
 
 size_t level_smem_fp64() { return KF64::bytes; }
 
 cudaError_t launch_level_fp64(const LevelArgs &a, cudaStream_t s) {
   static bool attr = false;
-  auto k = level_advance_kernel<MathF64, kTileOcts, kSMax, kHMax>;
+  auto k = level_advance_kernel<MathF64, kTileOcts, kSMax, kHMax, kBMax>;
   if (!attr) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KF64::bytes);
     if (e != cudaSuccess) return e;

@@ -7,14 +7,16 @@
 //       ("virtual octs": a real oct, a coarser leaf cell injected into 8 cells
 //       as the reference's gather does, or a transmissive mirror ghost), with
 //       the neighbour graph between staged octs (precomputed per tile);
-//   P1  computes MUSCL-Hancock slopes and predictor once per needed cell: the
-//       tile cells plus the halo cells face-adjacent to them;
-//   P2  solves each face once (HLLC); a face is owned by the tile cell on its +
-//       side, faces on the tile's + boundary by the cell on their - side;
-//   P3  sums the six face fluxes in the reference's order (-x,+x,-y,+y,-z,+z),
-//       updates the conserved state, recovers primitives, applies the floors,
-//       restricts split cells from the finer level and adds the fine->coarse
-//       corrections of faces that border a coarser leaf (atomics, x 1/8).
+//   P1  MUSCL-Hancock once per needed cell: slopes + predictor of every tile
+//       cell (kept in shared memory), and for every halo entry (a cell outside
+//       the tile face-adjacent to it) the one face state it contributes;
+//   P2  one HLLC solve per face, as an axis-major task list spread evenly over
+//       the CTA: task (axis d, tile cell t) is the -d face of t; then the +d
+//       faces on the tile's + boundary;
+//   P3  per tile cell: the six face fluxes summed in the reference's order
+//       (-x,+x,-y,+y,-z,+z), conserved update, primitive recovery, floors;
+//       split cells get the primitive mean of their children; faces bordering
+//       a coarser leaf add the fine->coarse correction (atomics, x 1/8).
 // The reference does the same per oct on a 27-oct copy, recomputing each
 // cell's reconstruction up to 9 times and each face twice
 // (src/hydro_utils.c:1407-2238, 2973-3303).
@@ -34,74 +36,105 @@ __constant__ uint8_t c_mirror[6][8] = {
     {0, 0, 2, 2, 4, 4, 6, 6}, {1, 1, 3, 3, 5, 5, 7, 7}, {0, 1, 0, 1, 4, 5, 4, 5},
     {2, 3, 2, 3, 7, 6, 6, 7}, {0, 1, 2, 3, 0, 1, 2, 3}, {4, 5, 6, 7, 4, 5, 6, 7}};
 
-template <class M, int T, int SMAX, int HMAX>
+template <class M, int T, int SMAX, int HMAX, int BMAX>
 struct LevelSmem {
   using R = typename M::R;
-  static constexpr int NM = 8 * T + HMAX;  // MUSCL scratch entries
-  static constexpr size_t off_W = 0;                                        // R [5][SMAX*8]
-  static constexpr size_t off_M = off_W + sizeof(R) * 5 * SMAX * 8;         // R [20][NM]
-  static constexpr size_t off_F = off_M + sizeof(R) * 20 * NM;              // R [15][8T]
-  static constexpr size_t off_key = off_F + sizeof(R) * 15 * 8 * T;         // u32 [SMAX]
-  static constexpr size_t off_G = off_key + sizeof(uint32_t) * SMAX;        // u8 [SMAX*6]
-  static constexpr size_t off_H = (off_G + 6 * SMAX + 15) & ~size_t(15);    // u16 [SMAX*8]
-  static constexpr size_t off_S = off_H + sizeof(uint16_t) * SMAX * 8;      // u8 [SMAX*8]
-  static constexpr size_t bytes = (off_S + SMAX * 8 + 15) & ~size_t(15);
+  static constexpr int NT = 8 * T;  // tile cells = threads
+  static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
+  static constexpr size_t off_W = 0;                                       // R [5][SMAX*8] staged states
+  static constexpr size_t off_M = a16(off_W + sizeof(R) * 5 * SMAX * 8);   // R [20][NT] slopes + predictor
+  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 20 * NT);       // R [7][HMAX] halo face states
+  static constexpr size_t off_F = a16(off_HS + sizeof(R) * 7 * HMAX);      // R [5][3*NT] -d face fluxes
+  static constexpr size_t off_FB = a16(off_F + sizeof(R) * 5 * 3 * NT);    // R [5][BMAX] boundary + faces
+  static constexpr size_t off_key = a16(off_FB + sizeof(R) * 5 * BMAX);    // u32 [SMAX]
+  static constexpr size_t off_G = a16(off_key + sizeof(uint32_t) * SMAX);  // u8 [SMAX*6]
+  static constexpr size_t off_hmap = a16(off_G + 6 * SMAX);               // u16 [SMAX*8] first halo entry
+  static constexpr size_t off_halo = a16(off_hmap + 2 * SMAX * 8);        // u16 [HMAX] halo entries
+  static constexpr size_t off_bface = a16(off_halo + 2 * HMAX);           // u16 [BMAX] boundary faces
+  static constexpr size_t off_bmap = a16(off_bface + 2 * BMAX);           // u16 [3*NT] (cell,axis) -> face
+  static constexpr size_t off_sp = a16(off_bmap + 2 * 3 * NT);            // u8 [SMAX*8] split flags
+  static constexpr size_t bytes = a16(off_sp + SMAX * 8);
 };
 
-template <class M, int T, int SMAX, int HMAX>
+template <class M, int T, int SMAX, int HMAX, int BMAX>
 __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
     level_advance_kernel(const LevelArgs A) {
   using R = typename M::R;
-  using SM = LevelSmem<M, T, SMAX, HMAX>;
-  constexpr int NM = SM::NM;
+  using SM = LevelSmem<M, T, SMAX, HMAX, BMAX>;
+  constexpr int NT = SM::NT;
   extern __shared__ __align__(16) unsigned char smem[];
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
   R *sM = reinterpret_cast<R *>(smem + SM::off_M);
+  R *sHS = reinterpret_cast<R *>(smem + SM::off_HS);
   R *sF = reinterpret_cast<R *>(smem + SM::off_F);
+  R *sFB = reinterpret_cast<R *>(smem + SM::off_FB);
   uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key);
   uint8_t *sG = smem + SM::off_G;
-  uint16_t *sH = reinterpret_cast<uint16_t *>(smem + SM::off_H);
-  uint8_t *sSp = smem + SM::off_S;
+  uint16_t *sHmap = reinterpret_cast<uint16_t *>(smem + SM::off_hmap);
+  uint16_t *sHalo = reinterpret_cast<uint16_t *>(smem + SM::off_halo);
+  uint16_t *sBface = reinterpret_cast<uint16_t *>(smem + SM::off_bface);
+  uint16_t *sBmap = reinterpret_cast<uint16_t *>(smem + SM::off_bmap);
+  uint8_t *sSp = smem + SM::off_sp;
 
   const int tid = threadIdx.x;
   const TileDesc td = A.tiles[blockIdx.x];
-  const int n = td.noct, S = td.S, H = td.H;
-  const long long n8 = 8LL * A.noct;
+  const int n = td.noct, S = td.S, H = td.H, B = td.B;
+  const int n8 = 8 * n;
+  const long long N8 = 8LL * A.noct;
   unsigned st = 0;
-  if (S > SMAX || H > HMAX || n > T) {  // plan built for another kernel shape
+  if (S > SMAX || H > HMAX || B > BMAX || n > T || n < 1) {  // plan cut for another kernel shape
     if (tid == 0) atomicOr(A.status, kStTree);
     return;
   }
 
   // ------------------------------------------------------------------ P0
-  for (int i = tid; i < S; i += 8 * T) sKey[i] = A.keys[td.keys_off + i];
-  for (int i = tid; i < S * 6; i += 8 * T) sG[i] = A.graph[td.graph_off + i];
-  for (int i = tid; i < S * 8; i += 8 * T) sH[i] = 0xFFFF;
+  for (int i = tid; i < S; i += NT) sKey[i] = A.keys[td.keys_off + i];
+  for (int i = tid; i < S * 6; i += NT) sG[i] = A.graph[td.graph_off + i];
+  for (int i = tid; i < S * 8; i += NT) sHmap[i] = 0xFFFF;
+  for (int i = tid; i < H; i += NT) sHalo[i] = A.halo[td.halo_off + i];
+  for (int i = tid; i < B; i += NT) sBface[i] = A.bface[td.bface_off + i];
   __syncthreads();
-  for (int i = tid; i < H; i += 8 * T) sH[A.halo[td.halo_off + i]] = (uint16_t)(8 * T + i);
-  for (int i = tid; i < S * 8; i += 8 * T) {
+  for (int h = tid; h < H; h += NT) {
+    const int cell = sHalo[h] >> 3;
+    if (h == 0 || (sHalo[h - 1] >> 3) != cell) sHmap[cell] = (uint16_t)h;
+  }
+  for (int b = tid; b < B; b += NT) {
+    const int e = sBface[b];
+    sBmap[(e >> 2) * 3 + (e & 3)] = (uint16_t)b;
+  }
+#pragma unroll 2
+  for (int i = tid; i < S * 8; i += NT) {
     const int s = i >> 3, c = i & 7;
     const uint32_t key = sKey[s];
     const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
-    const double *src;
-    long long stride, off;
+    const double *src = A.W;
+    long long stride = N8, off;
     uint8_t sp = 0;
     if (kind == kKeyReal) {
-      src = A.W; stride = n8; off = 8LL * idx + c;
+      off = 8LL * idx + c;
       sp = (A.split[idx] >> c) & 1;
     } else if (kind == kKeyInj) {
-      src = A.Wc; stride = A.nc8; off = idx;
+      src = A.Wc;
+      stride = A.nc8;
+      off = idx;
       if (src == nullptr) {  // plan/launch mismatch: never read through a null level
         st |= kStTree;
-        src = A.W; stride = n8; off = 0;
+        src = A.W;
+        stride = N8;
+        off = 0;
       }
     } else {
       const int mc = c_mirror[kind - kKeyGhost0][c];
-      src = A.W; stride = n8; off = 8LL * idx + mc;
+      off = 8LL * idx + mc;
       sp = (A.split[idx] >> mc) & 1;
     }
-#pragma unroll
-    for (int v = 0; v < 5; v++) sW[v * SMAX * 8 + i] = (R)__ldg(src + v * stride + off);
+    const double v0 = __ldg(src + off), v1 = __ldg(src + stride + off), v2 = __ldg(src + 2 * stride + off);
+    const double v3 = __ldg(src + 3 * stride + off), v4 = __ldg(src + 4 * stride + off);
+    sW[0 * SMAX * 8 + i] = (R)v0;
+    sW[1 * SMAX * 8 + i] = (R)v1;
+    sW[2 * SMAX * 8 + i] = (R)v2;
+    sW[3 * SMAX * 8 + i] = (R)v3;
+    sW[4 * SMAX * 8 + i] = (R)v4;
     sSp[i] = sp;
   }
   __syncthreads();
@@ -117,20 +150,7 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
 #pragma unroll
     for (int v = 0; v < 5; v++) q[v] = sW[v * SMAX * 8 + s * 8 + c];
   };
-  auto mi_of = [&](int s, int c) -> int { return (s < n) ? (s * 8 + c) : (int)sH[s * 8 + c]; };
-
-  // ------------------------------------------------------------------ P1
-  const R dt = (R)A.dt, dx = (R)A.dx;
-  for (int j = tid; j < 8 * T + H; j += 8 * T) {
-    int s, c;
-    if (j < 8 * T) {
-      if (j >= 8 * n) continue;
-      s = j >> 3; c = j & 7;
-    } else {
-      const int e = A.halo[td.halo_off + (j - 8 * T)];
-      s = e >> 3; c = e & 7;
-    }
-    if (sSp[s * 8 + c]) continue;  // split cells have no flux: no reconstruction needed
+  auto muscl_of = [&](int s, int c, R D[3][5], R Wt[5]) {
     R q0[5], qm[3][5], qp[3][5];
     q_of(s, c, q0);
 #pragma unroll
@@ -143,104 +163,139 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
       if (s2 < 0) { st |= kStTree; s2 = s; c2 = c; }
       q_of(s2, c2, qp[dir]);
     }
-    R D[3][5], Wt[5];
-    if constexpr (sizeof(R) == 8) M::muscl(q0, qm, qp, dt, dx, D, Wt);
+    if constexpr (sizeof(R) == 8) M::muscl(q0, qm, qp, A.dt, A.dx, D, Wt);
     else M::muscl(q0, qm, qp, (R)(A.dt / A.dx * 0.5), D, Wt);
+  };
+
+  // ------------------------------------------------------------------ P1
+  for (int j = tid; j < n8 + H; j += NT) {
+    int s, c, k = -1;
+    if (j < n8) {
+      s = j >> 3;
+      c = j & 7;
+    } else {
+      const int e = sHalo[j - n8];
+      s = e >> 6;
+      c = (e >> 3) & 7;
+      k = e & 7;
+    }
+    if (sSp[s * 8 + c]) continue;  // split cells carry no flux: no reconstruction
+    R D[3][5], Wt[5];
+    muscl_of(s, c, D, Wt);
+    if (k < 0) {
 #pragma unroll
-    for (int dir = 0; dir < 3; dir++)
+      for (int dir = 0; dir < 3; dir++)
 #pragma unroll
-      for (int v = 0; v < 5; v++) sM[(dir * 5 + v) * NM + j] = D[dir][v];
+        for (int v = 0; v < 5; v++) sM[(dir * 5 + v) * NT + j] = D[dir][v];
 #pragma unroll
-    for (int v = 0; v < 5; v++) sM[(15 + v) * NM + j] = Wt[v];
+      for (int v = 0; v < 5; v++) sM[(15 + v) * NT + j] = Wt[v];
+    } else {
+      R q0[5], Dax[5], W[7];
+      q_of(s, c, q0);
+      const int ax = k >> 1;
+#pragma unroll
+      for (int v = 0; v < 5; v++) Dax[v] = (ax == 0) ? D[0][v] : ((ax == 1) ? D[1][v] : D[2][v]);
+      M::face_ax(q0, Dax, Wt, k, W, st);
+      const int h = j - n8;
+#pragma unroll
+      for (int v = 0; v < 7; v++) sHS[v * HMAX + h] = W[v];
+    }
   }
   __syncthreads();
 
-  auto face_of = [&](int s, int c, int mi, int k, R W[7]) {
-    R q0[5], D[3][5], Wt[5];
-    q_of(s, c, q0);
+  // face state k of tile cell t from its slopes and predictor
+  auto tile_face = [&](int t, int k, R W[7]) {
+    R q0[5], Dax[5], Wt[5];
+    q_of(t >> 3, t & 7, q0);
+    const int ax = k >> 1;
 #pragma unroll
-    for (int dir = 0; dir < 3; dir++)
+    for (int v = 0; v < 5; v++) {
+      Dax[v] = sM[(ax * 5 + v) * NT + t];
+      Wt[v] = sM[(15 + v) * NT + t];
+    }
+    M::face_ax(q0, Dax, Wt, k, W, st);
+  };
+  // stored face state k of halo cell `cell` (s*8+c); false if absent
+  auto halo_face = [&](int cell, int k, R W[7]) -> bool {
+    int h = sHmap[cell];
+    if (h == 0xFFFF) return false;
+    while (h < H && (sHalo[h] >> 3) == cell && (sHalo[h] & 7) != k) h++;
+    if (h >= H || (sHalo[h] >> 3) != cell) return false;
 #pragma unroll
-      for (int v = 0; v < 5; v++) D[dir][v] = sM[(dir * 5 + v) * NM + mi];
-#pragma unroll
-    for (int v = 0; v < 5; v++) Wt[v] = sM[(15 + v) * NM + mi];
-    M::face(q0, D, Wt, k, W, st);
+    for (int v = 0; v < 7; v++) W[v] = sHS[v * HMAX + h];
+    return true;
   };
 
   // ------------------------------------------------------------------ P2
-  R Fp[3][5];
-  bool own_plus[3] = {false, false, false};
-  const bool active = tid < 8 * n;
-  const int o = tid >> 3, c = tid & 7;
-  const bool my_split = active ? (sSp[tid] != 0) : true;
-  if (active) {
-#pragma unroll
-    for (int d = 0; d < 3; d++) {
-      // minus face: left = -d neighbour's +d state, right = own -d state
-      R F[5] = {0, 0, 0, 0, 0};
-      int c2;
-      int s2 = nb(o, c, 2 * d, c2);
-      if (!my_split) {
-        if (s2 < 0) {
-          st |= kStTree;
-        } else if (!sSp[s2 * 8 + c2]) {
-          const int mi = mi_of(s2, c2);
-          if (mi == 0xFFFF) {
-            st |= kStTree;
-          } else {
-            R WL[7], WR[7];
-            face_of(s2, c2, mi, 2 * d + 1, WL);
-            face_of(o, c, tid, 2 * d, WR);
-            M::hllc(WL, WR, d, F, st);
-          }
-        }
+  for (int f = tid; f < 3 * n8 + B; f += NT) {
+    int t, d;
+    bool plus;
+    if (f < 3 * n8) {
+      d = f / n8;
+      t = f - d * n8;
+      plus = false;
+    } else {
+      const int e = sBface[f - 3 * n8];
+      t = e >> 2;
+      d = e & 3;
+      plus = true;
+    }
+    const int o = t >> 3, c = t & 7;
+    const int k = 2 * d + (plus ? 1 : 0);
+    R F[5] = {0, 0, 0, 0, 0};
+    int c2;
+    const int s2 = nb(o, c, k, c2);
+    if (s2 < 0) {
+      st |= kStTree;
+    } else if (!sSp[t] && !sSp[s2 * 8 + c2]) {
+      R Wa[7], Wb[7];  // a: this cell's state at the face, b: the neighbour's
+      tile_face(t, k, Wa);
+      bool ok = true;
+      if (s2 < n) tile_face(s2 * 8 + c2, k ^ 1, Wb);
+      else ok = halo_face(s2 * 8 + c2, k ^ 1, Wb);
+      if (!ok) {
+        st |= kStTree;
+      } else if (plus) {
+        M::hllc(Wa, Wb, d, F, st);
+      } else {
+        M::hllc(Wb, Wa, d, F, st);
       }
+    }
+    if (plus) {
+      const int b = f - 3 * n8;
 #pragma unroll
-      for (int v = 0; v < 5; v++) sF[(d * 5 + v) * 8 * T + tid] = F[v];
-      // plus face on the tile boundary
+      for (int v = 0; v < 5; v++) sFB[v * BMAX + b] = F[v];
+    } else {
 #pragma unroll
-      for (int v = 0; v < 5; v++) Fp[d][v] = 0;
-      s2 = nb(o, c, 2 * d + 1, c2);
-      if (s2 < 0 || s2 >= n) {
-        own_plus[d] = true;
-        if (!my_split) {
-          if (s2 < 0) {
-            st |= kStTree;
-          } else if (!sSp[s2 * 8 + c2]) {
-            const int mi = mi_of(s2, c2);
-            if (mi == 0xFFFF) {
-              st |= kStTree;
-            } else {
-              R WL[7], WR[7];
-              face_of(o, c, tid, 2 * d + 1, WL);
-              face_of(s2, c2, mi, 2 * d, WR);
-              M::hllc(WL, WR, d, Fp[d], st);
-            }
-          }
-        }
-      }
+      for (int v = 0; v < 5; v++) sF[v * 3 * NT + d * NT + t] = F[v];
     }
   }
   __syncthreads();
 
   // ------------------------------------------------------------------ P3
-  if (active) {
+  if (tid < n8) {
+    const int o = tid >> 3, c = tid & 7;
     const long long gi = 8LL * (td.oct0 + o) + c;
+    double q[5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) q[v] = A.W[v * N8 + gi];
     double Wout[5];
-    if (my_split) {
+    if (sSp[tid]) {
       // split cell: primitive mean of the 8 children (src/hydro_utils.c:3420-3481);
       // without the finer level (drop-in mode) the caller averages on the host
-      const long long ch = A.child[gi];
       double acc[5] = {0., 0., 0., 0., 0.};
       if (A.Wf == nullptr) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) acc[v] = A.W[v * n8 + gi];
-      } else if (ch >= 0) {
-        for (int i = 0; i < 8; i++)
-#pragma unroll
-          for (int v = 0; v < 5; v++) acc[v] += A.Wf[v * A.nf8 + 8 * ch + i] * 0.125;
+        for (int v = 0; v < 5; v++) acc[v] = q[v];
       } else {
-        st |= kStTree;
+        const long long ch = A.child[gi];
+        if (ch >= 0) {
+          for (int i = 0; i < 8; i++)
+#pragma unroll
+            for (int v = 0; v < 5; v++) acc[v] += A.Wf[v * A.nf8 + 8 * ch + i] * 0.125;
+        } else {
+          st |= kStTree;
+        }
       }
 #pragma unroll
       for (int v = 0; v < 5; v++) Wout[v] = acc[v];
@@ -251,24 +306,18 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
 #pragma unroll
       for (int d = 0; d < 3; d++) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) Fd[2 * d][v] = (double)sF[(d * 5 + v) * 8 * T + tid];
-        if (own_plus[d]) {
+        for (int v = 0; v < 5; v++) Fd[2 * d][v] = (double)sF[v * 3 * NT + d * NT + tid];
+        int c2;
+        const int s2 = nb(o, c, 2 * d + 1, c2);
+        if (s2 >= 0 && s2 < n) {
 #pragma unroll
-          for (int v = 0; v < 5; v++) Fd[2 * d + 1][v] = (double)Fp[d][v];
+          for (int v = 0; v < 5; v++) Fd[2 * d + 1][v] = (double)sF[v * 3 * NT + d * NT + s2 * 8 + c2];
         } else {
-          int c2;
-          const int s2 = nb(o, c, 2 * d + 1, c2);
-          const int t2 = s2 * 8 + c2;
+          const int b = sBmap[tid * 3 + d];
 #pragma unroll
-          for (int v = 0; v < 5; v++) Fd[2 * d + 1][v] = (double)sF[(d * 5 + v) * 8 * T + t2];
+          for (int v = 0; v < 5; v++) Fd[2 * d + 1][v] = (double)sFB[v * BMAX + b];
         }
       }
-      double q[5];
-#pragma unroll
-      for (int v = 0; v < 5; v++) q[v] = A.W[v * n8 + gi];
-      double corr[5];
-#pragma unroll
-      for (int v = 0; v < 5; v++) corr[v] = (A.C != nullptr && A.B == nullptr) ? A.C[v * n8 + gi] : 0.;
       double Ud, Udu, Udv, Udw, UE;
       if constexpr (sizeof(R) == 8) {
         // updatefield (src/hydro_utils.c:3050-3082): dU = sum (+-F dt/dx), alternating signs
@@ -280,21 +329,28 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
           for (int v = 0; v < 5; v++) dU[v] += Fd[f][v] * dtsurdx * one;
           one *= -1.;
         }
-        // scatterstencil central update (src/hydro_utils.c:3129-3188): W2U + dU
+        // scatterstencil central update (src/hydro_utils.c:3129-3188): W2U(fieldnew) + dU
         if (A.B != nullptr) {
           const double bd = A.B[gi];
           Ud = bd;
-          Udu = bd * A.B[n8 + gi];
-          Udv = bd * A.B[2 * n8 + gi];
-          Udw = bd * A.B[3 * n8 + gi];
-          UE = A.B[5 * n8 + gi];
+          Udu = bd * A.B[N8 + gi];
+          Udv = bd * A.B[2 * N8 + gi];
+          Udw = bd * A.B[3 * N8 + gi];
+          UE = A.B[5 * N8 + gi];
         } else {
           const double E0 = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-          Ud = q[0] + corr[0];
-          Udu = q[0] * q[1] + corr[1];
-          Udv = q[0] * q[2] + corr[2];
-          Udw = q[0] * q[3] + corr[3];
-          UE = E0 + corr[4];
+          Ud = q[0];
+          Udu = q[0] * q[1];
+          Udv = q[0] * q[2];
+          Udw = q[0] * q[3];
+          UE = E0;
+          if (A.C != nullptr) {
+            Ud += A.C[gi];
+            Udu += A.C[N8 + gi];
+            Udv += A.C[2 * N8 + gi];
+            Udw += A.C[3 * N8 + gi];
+            UE += A.C[4 * N8 + gi];
+          }
         }
         Ud += dU[0];
         Udu += dU[1];
@@ -307,10 +363,16 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
         double s[5];
         if (A.B != nullptr) {
           const double bd = A.B[gi];
-          s[0] = bd; s[1] = bd * A.B[n8 + gi]; s[2] = bd * A.B[2 * n8 + gi]; s[3] = bd * A.B[3 * n8 + gi];
-          s[4] = A.B[5 * n8 + gi];
+          s[0] = bd;
+          s[1] = bd * A.B[N8 + gi];
+          s[2] = bd * A.B[2 * N8 + gi];
+          s[3] = bd * A.B[3 * N8 + gi];
+          s[4] = A.B[5 * N8 + gi];
         } else {
-          s[0] = q[0]; s[1] = q[0] * q[1]; s[2] = q[0] * q[2]; s[3] = q[0] * q[3];
+          s[0] = q[0];
+          s[1] = q[0] * q[1];
+          s[2] = q[0] * q[2];
+          s[3] = q[0] * q[3];
           s[4] = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
         }
         double comp[5] = {0., 0., 0., 0., 0.};
@@ -319,8 +381,10 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
           comp[v] += (fabs(s[v]) >= fabs(x)) ? ((s[v] - t) + x) : ((x - t) + s[v]);
           s[v] = t;
         };
+        if (A.C != nullptr && A.B == nullptr) {
 #pragma unroll
-        for (int v = 0; v < 5; v++) add(v, corr[v]);
+          for (int v = 0; v < 5; v++) add(v, A.C[v * N8 + gi]);
+        }
 #pragma unroll
         for (int f = 0; f < 6; f++)
 #pragma unroll
@@ -356,7 +420,7 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
       }
     }
 #pragma unroll
-    for (int v = 0; v < 5; v++) A.Wn[v * n8 + gi] = Wout[v];
+    for (int v = 0; v < 5; v++) A.Wn[v * N8 + gi] = Wout[v];
   }
   if (st) atomicOr(A.status, st);
 }

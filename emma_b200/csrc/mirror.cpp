@@ -145,7 +145,8 @@ struct TileBuild {
   std::vector<uint32_t> keys;
   std::vector<uint8_t> graph;
   std::vector<uint16_t> halo;
-  int S = 0, H = 0;
+  std::vector<uint16_t> bface;
+  int S = 0, H = 0, B = 0;
 };
 
 // Stage list, neighbour graph and halo of the tile [o0, o0+n).  Returns false
@@ -195,20 +196,28 @@ bool build_tile(Planner &P, int L, int o0, int n, TileBuild &tb) {
       auto it = (g == kKeyNone) ? pos.end() : pos.find(g);
       if (it != pos.end() && it->second < 255) tb.graph[6 * s + k] = (uint8_t)it->second;
     }
-  // halo: cells of non-tile staged octs face-adjacent to a tile oct
+  // halo entries: (cell of a non-tile staged oct, its face toward a tile oct)
   tb.halo.clear();
   for (int s = n; s < tb.S; s++)
     for (int c = 0; c < 8; c++)
       for (int k = 0; k < 6; k++) {
         if (inside(c, k)) continue;
         const int g = tb.graph[6 * s + k];
-        if (g != 255 && g < n) {
-          tb.halo.push_back((uint16_t)(8 * s + c));
-          break;
-        }
+        if (g != 255 && g < n) tb.halo.push_back((uint16_t)(((8 * s + c) << 3) | k));
       }
   tb.H = (int)tb.halo.size();
-  if (tb.H > kHMax) return true;  // too many halo cells: the caller shrinks the tile
+  if (tb.H > kHMax) return true;  // too many halo entries: the caller shrinks the tile
+  // + faces of tile cells that border a non-tile staged oct
+  tb.bface.clear();
+  for (int t = 0; t < 8 * n; t++)
+    for (int d = 0; d < 3; d++) {
+      const int k = 2 * d + 1, c = t & 7;
+      if (inside(c, k)) continue;
+      const int g = tb.graph[6 * (t >> 3) + k];
+      if (g == 255 || g >= n) tb.bface.push_back((uint16_t)(4 * t + d));
+    }
+  tb.B = (int)tb.bface.size();
+  if (tb.B > kBMax) return true;
   // every neighbour a reconstruction reads must be staged
   auto need = [&](int s, int c) -> bool {
     for (int k = 0; k < 6; k++) {
@@ -224,8 +233,9 @@ bool build_tile(Planner &P, int L, int o0, int n, TileBuild &tb) {
         P.msg = "unstaged neighbour of a tile cell";
         return false;
       }
-  for (uint16_t e : tb.halo)
-    if (!need(e >> 3, e & 7)) {
+  for (uint16_t e16 : tb.halo)
+    if (!need(e16 >> 6, (e16 >> 3) & 7)) {
+      const int e = e16 >> 3;
       P.err |= EMMA_ST_TREE;
       const uint32_t key = tb.keys[e >> 3];
       if (std::getenv("EMMA_PLAN_DEBUG")) {
@@ -297,7 +307,7 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
   }
   for (int L = std::max(lcoarse, plan_lo); L <= std::min(lmax, plan_hi); L++) {
     HostLevel &lv = H.lev[L];
-    std::unordered_map<std::string, int> gdedup, hdedup;
+    std::unordered_map<std::string, int> gdedup, hdedup, bdedup;
     std::vector<uint8_t> injmark;
     if (L > lcoarse) injmark.assign((size_t)8 * H.lev[L - 1].noct, 0);
     TileBuild tb;
@@ -309,10 +319,10 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
           err = P.msg;
           return (int)P.err;
         }
-        if ((tb.S <= kSMax && tb.H <= kHMax) || n == 1) break;
+        if ((tb.S <= kSMax && tb.H <= kHMax && tb.B <= kBMax) || n == 1) break;
         n = (n > 8) ? n - 4 : n - 1;
       }
-      if (tb.S > kSMax || tb.H > kHMax) {
+      if (tb.S > kSMax || tb.H > kHMax || tb.B > kBMax) {
         err = "single-oct tile exceeds the staging limits";
         return EMMA_ST_TREE;
       }
@@ -322,6 +332,7 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
       td.noct = n;
       td.S = tb.S;
       td.H = tb.H;
+      td.B = tb.B;
       td.keys_off = (int)lv.keys.size();
       lv.keys.insert(lv.keys.end(), tb.keys.begin(), tb.keys.end());
       for (uint32_t key : tb.keys)
@@ -343,6 +354,15 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
         hdedup.emplace(std::move(hk), td.halo_off);
       } else {
         td.halo_off = hit->second;
+      }
+      std::string bk(reinterpret_cast<const char *>(tb.bface.data()), tb.bface.size() * sizeof(uint16_t));
+      auto bit = bdedup.find(bk);
+      if (bit == bdedup.end()) {
+        td.bface_off = (int)lv.bface.size();
+        lv.bface.insert(lv.bface.end(), tb.bface.begin(), tb.bface.end());
+        bdedup.emplace(std::move(bk), td.bface_off);
+      } else {
+        td.bface_off = bit->second;
       }
       lv.tiles.push_back(td);
       o0 += n;
@@ -388,10 +408,21 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
           }
         }
       }
+      if (t.B < 0 || t.B > kBMax || t.bface_off < 0 || (size_t)t.bface_off + t.B > lv.bface.size()) {
+        err = "invalid boundary-face range at level " + std::to_string(L);
+        return EMMA_ST_TREE;
+      }
       for (int h = 0; h < t.H; h++) {
-        const int e = lv.halo[t.halo_off + h];
-        if (e < 8 * t.noct || e >= 8 * t.S) {
+        const int e = lv.halo[t.halo_off + h] >> 3, k = lv.halo[t.halo_off + h] & 7;
+        if (e < 8 * t.noct || e >= 8 * t.S || k > 5) {
           err = "invalid halo entry at level " + std::to_string(L);
+          return EMMA_ST_TREE;
+        }
+      }
+      for (int b = 0; b < t.B; b++) {
+        const int e = lv.bface[t.bface_off + b];
+        if ((e >> 2) >= 8 * t.noct || (e & 3) > 2) {
+          err = "invalid boundary face at level " + std::to_string(L);
           return EMMA_ST_TREE;
         }
       }

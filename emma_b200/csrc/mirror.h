@@ -19,6 +19,7 @@ struct HostLevel {
   std::vector<uint32_t> keys;
   std::vector<uint8_t> graph;
   std::vector<uint16_t> halo;
+  std::vector<uint16_t> bface;
   std::vector<int32_t> inj_cells;     // level L-1 cells injected into this level's plans
 };
 

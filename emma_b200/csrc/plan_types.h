@@ -16,20 +16,24 @@ constexpr uint32_t kKeyReal = 0, kKeyInj = 1, kKeyGhost0 = 2;
 constexpr uint32_t kKeyNone = 0xFFFFFFFFu;
 constexpr uint32_t key_make(uint32_t kind, uint32_t idx) { return (kind << 28) | idx; }
 
-// Kernel shape the plans are cut for (tile octs, staged octs, halo cells).
+// Kernel shape the plans are cut for: octs per tile, staged octs, directional
+// halo entries, boundary faces.
 constexpr int kTileOcts = 32;
 constexpr int kSMax = 144;
 constexpr int kHMax = 288;
+constexpr int kBMax = 160;
 
 struct TileDesc {
   int oct0;       // first oct of the tile (level list index)
   int noct;       // octs in the tile (<= kTileOcts)
   int S;          // staged virtual octs (tile octs first)
-  int H;          // halo cells (staged cell codes s*8+c)
+  int H;          // halo entries: (staged cell s*8+c) << 3 | face k of that cell toward the tile
+  int B;          // boundary faces: tile cell t*4 + axis whose + face borders a non-tile oct
   int keys_off;   // offset into the keys array
   int graph_off;  // offset into the graph array (S*6 bytes; 255 = not staged)
   int halo_off;   // offset into the halo array
-  int pad;
+  int bface_off;  // offset into the boundary-face array
+  int pad[3];
 };
 
 struct LevelArgs {
@@ -51,6 +55,7 @@ struct LevelArgs {
   const uint32_t *keys;
   const uint8_t *graph;
   const uint16_t *halo;
+  const uint16_t *bface;
   double dt, dx;
   unsigned *status;
   int ntiles;

@@ -104,3 +104,19 @@ def test_restatement_reproduces_golden(name):
     assert tsim == float(g["tsim"])
     for l in range(base, lmax + 1):
         assert np.array_equal(t.get_fields(l, 0), g[f"out_{l}"]), f"level {l}"
+
+
+@needs_ref
+def test_reference_library_runs_its_own_hydro():
+    """With libemmahydro loaded first (it exports HydroSolver too), the reference
+    library must still call its own HydroSolver: its CPU time per cell-update
+    stays in the reference's range and its result equals the restatement's."""
+    from emma_b200 import lib
+    lib()  # load the product library (exports the same drop-in names)
+    ref_vs_restatement(False, 3, 3, (), 1)
+    ref = oracle.RefTree(4, 4, ngridmax=1000)
+    random_fields(ref, [4])
+    ref.reset_counters()
+    ref.run(1)
+    assert ref.cell_updates() == 4096
+    assert ref.cell_updates() / ref.hydro_seconds() < 5e6  # a CPU, not a GPU
