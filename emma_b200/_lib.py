@@ -19,7 +19,7 @@ P = ctypes.POINTER
 
 class EmmaHydroOptions(ctypes.Structure):
     _fields_ = [("precision", c_int), ("trans_flags", c_int), ("cfl", c_double),
-                ("tile_octs", c_int), ("device", c_int)]
+                ("tile_octs", c_int), ("device", c_int), ("use_graph", c_int)]
 
 
 PREC_FP64, PREC_MIXED = 0, 1
@@ -51,6 +51,9 @@ SIGNATURES = [
     ("emma_hydro_comptstep", c_int, [c_int, P(c_double)]),
     ("emma_hydro_advance_level", c_int, [c_int, c_double]),
     ("emma_hydro_advance_coarse_step", c_int, [c_double, c_double, c_int, P(c_double), c_void_p]),
+    ("emma_hydro_advance_coarse_step_async", c_int, [c_double, c_double, c_int]),
+    ("emma_hydro_get_time", c_int, [P(c_double), c_void_p]),
+    ("emma_hydro_set_time", c_int, [c_double, c_void_p]),
     ("emma_hydro_level_noct", c_int, [c_int]),
     ("emma_hydro_get_level_state", c_int, [c_int, c_void_p]),
     ("emma_hydro_set_level_state", c_int, [c_int, c_void_p]),

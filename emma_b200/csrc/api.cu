@@ -1,5 +1,6 @@
 // api.cu -- C ABI of libemmahydro: device context, resident tree, level
-// schedule and the drop-in entries with the reference's names.
+// schedule (host-driven or a captured CUDA graph) and the drop-in entries with
+// the reference's names.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -12,11 +13,13 @@
 #include "emma_hydro.h"
 #include "mirror.h"
 #include "plan_types.h"
+#include "schedule.h"
 
 namespace emma {
-cudaError_t launch_level_fp64(const LevelArgs &a, cudaStream_t s);
-cudaError_t launch_level_f32(const LevelArgs &a, cudaStream_t s);
-cudaError_t launch_cfl(const double *W, long long n8, unsigned long long *out, int nsm, cudaStream_t s);
+cudaError_t launch_level_fp64(const BatchArgs &a, int nsm, cudaStream_t s);
+cudaError_t launch_level_f32(const BatchArgs &a, int nsm, cudaStream_t s);
+cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *gate, unsigned long long *out, int nsm,
+                       cudaStream_t s);
 }  // namespace emma
 
 using namespace emma;
@@ -24,11 +27,12 @@ using namespace emma;
 namespace {
 
 constexpr double kG = 5. / 3.;
+constexpr long long kWaitLimit = 1LL << 24;  // ~1 s of __nanosleep(64) polls
 
 struct DevLevel {
   int L = 0, noct = 0, ntiles = 0;
   long long n8 = 0, leaf = 0;
-  double *W = nullptr, *Wn = nullptr, *C = nullptr, *B = nullptr;
+  double *W0 = nullptr, *W1 = nullptr, *C = nullptr, *B = nullptr;
   uint8_t *split = nullptr;
   int *child = nullptr;
   TileDesc *tiles = nullptr;
@@ -36,6 +40,7 @@ struct DevLevel {
   uint8_t *graph = nullptr;
   uint16_t *halo = nullptr;
   uint16_t *bface = nullptr;
+  int *work = nullptr;  // (L << 24) | tile for every tile of the level
 };
 
 struct TimedLaunch {
@@ -43,31 +48,39 @@ struct TimedLaunch {
   long long cells;
 };
 
+struct Tree {
+  bool valid = false;
+  int lcoarse = 0, lmax = 0;
+  HostTree host;
+  std::vector<DevLevel> lev;
+  LevelArgs *d_lv = nullptr;  // kMaxLevels slots, indexed by level
+};
+
 struct Ctx {
   bool ready = false;
   EmmaHydroOptions opt;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;
   int nsm = 148;
   unsigned *d_status = nullptr;
-  unsigned long long *d_smax = nullptr;
-  unsigned long long *h_smax = nullptr;
+  unsigned *d_done = nullptr;    // kMaxLevels completion counters
+  SchedState *d_S = nullptr;
+  SchedState *h_S = nullptr;     // pinned staging of the schedule state
   unsigned status = 0;
   std::string last_error;
-  // resident tree
-  bool have_tree = false;
-  int lcoarse = 0, lmax = 0;
-  HostTree host;
-  std::vector<DevLevel> lev;
+  Tree res;                      // resident tree
+  int *d_work_all = nullptr;     // batched work list, finest level first
+  int nwork_all = 0;
+  cudaGraphExec_t graph = nullptr;
+  int graph_nsub = -1, graph_prec = -1;
   // drop-in cache
   struct OCT **drop_first = nullptr;
-  int drop_level = -1, drop_lo = 0, drop_hi = 0;
+  int drop_level = -1;
   std::vector<long long> drop_sig;
-  HostTree drop_host;
-  std::vector<DevLevel> drop_lev;
+  Tree drop;
   // pinned staging
   double *pin = nullptr;
   size_t pin_bytes = 0;
-  bool own_stream = true;
   // counters and timing
   long long updates = 0;
   long long kernel_launches = 0;
@@ -137,9 +150,15 @@ void parallel_for(long long n, F f) {
   for (auto &t : th) t.join();
 }
 
+void drop_graph() {
+  if (g.graph) cudaGraphExecDestroy(g.graph);
+  g.graph = nullptr;
+  g.graph_nsub = g.graph_prec = -1;
+}
+
 void free_level(DevLevel &d) {
-  cudaFree(d.W);
-  cudaFree(d.Wn);
+  cudaFree(d.W0);
+  cudaFree(d.W1);
   cudaFree(d.C);
   cudaFree(d.B);
   cudaFree(d.split);
@@ -149,7 +168,16 @@ void free_level(DevLevel &d) {
   cudaFree(d.graph);
   cudaFree(d.halo);
   cudaFree(d.bface);
+  cudaFree(d.work);
   d = DevLevel();
+}
+
+void free_tree(Tree &t) {
+  for (auto &d : t.lev) free_level(d);
+  t.lev.clear();
+  cudaFree(t.d_lv);
+  t.d_lv = nullptr;
+  t.valid = false;
 }
 
 template <class T>
@@ -160,20 +188,25 @@ bool upload_vec(T **dst, const std::vector<T> &v) {
   return ck(cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy plan");
 }
 
-// Allocate device arrays of the mirrored levels and copy topology + plans.
-bool alloc_levels(const HostTree &H, std::vector<DevLevel> &dl, bool with_base) {
-  dl.assign(H.lev.size(), DevLevel());
+// Allocate device arrays of the mirrored levels, copy topology + plans, and
+// initialise the device level slots.
+bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
+  t.lev.assign(H.lev.size(), DevLevel());
+  t.lcoarse = H.lcoarse;
+  t.lmax = H.lmax;
+  if (!ck(cudaMalloc(&t.d_lv, sizeof(LevelArgs) * kMaxLevels), "cudaMalloc level slots")) return false;
+  if (!ck(cudaMemset(t.d_lv, 0, sizeof(LevelArgs) * kMaxLevels), "cudaMemset level slots")) return false;
   for (int L = H.lcoarse; L <= H.lmax; L++) {
     const HostLevel &h = H.lev[L];
-    DevLevel &d = dl[L];
+    DevLevel &d = t.lev[L];
     d.L = L;
     d.noct = h.noct;
     d.n8 = 8LL * h.noct;
     d.leaf = h.leaf;
     d.ntiles = (int)h.tiles.size();
     const size_t bytes = sizeof(double) * 5 * (size_t)std::max<long long>(d.n8, 1);
-    if (!ck(cudaMalloc(&d.W, bytes), "cudaMalloc W")) return false;
-    if (!ck(cudaMalloc(&d.Wn, bytes), "cudaMalloc Wn")) return false;
+    if (!ck(cudaMalloc(&d.W0, bytes), "cudaMalloc W")) return false;
+    if (!ck(cudaMalloc(&d.W1, bytes), "cudaMalloc Wn")) return false;
     if (!ck(cudaMalloc(&d.C, bytes), "cudaMalloc C")) return false;
     if (!ck(cudaMemset(d.C, 0, bytes), "cudaMemset C")) return false;
     if (with_base && !h.tiles.empty())
@@ -186,8 +219,35 @@ bool alloc_levels(const HostTree &H, std::vector<DevLevel> &dl, bool with_base) 
     if (!upload_vec(&d.graph, h.graph)) return false;
     if (!upload_vec(&d.halo, h.halo)) return false;
     if (!upload_vec(&d.bface, h.bface)) return false;
+    std::vector<int> work((size_t)d.ntiles);
+    for (int i = 0; i < d.ntiles; i++) work[i] = (L << kWorkSlotShift) | i;
+    if (!upload_vec(&d.work, work)) return false;
+    LevelArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.L = L;
+    a.noct = d.noct;
+    a.W = d.W0;
+    a.Wn = d.W1;
+    a.C = d.C;
+    a.B = nullptr;
+    a.nc8 = (L > H.lcoarse) ? 8LL * H.lev[L - 1].noct : 0;
+    a.nf8 = (L < H.lmax) ? 8LL * H.lev[L + 1].noct : 0;
+    a.split = d.split;
+    a.child = d.child;
+    a.tiles = d.tiles;
+    a.keys = d.keys;
+    a.graph = d.graph;
+    a.halo = d.halo;
+    a.bface = d.bface;
+    a.dx = std::pow(0.5, L);
+    a.ntiles = d.ntiles;
+    a.wait_slot = -1;
+    a.leaf = d.leaf;
+    k_set_args<<<1, 1, 0, g.stream>>>(t.d_lv, L, a);
+    if (!ck(cudaGetLastError(), "k_set_args")) return false;
   }
-  return true;
+  t.valid = true;
+  return ck(cudaStreamSynchronize(g.stream), "sync after tree allocation");
 }
 
 // Pack `field` (which=0) or `fieldnew` (which=1, 6 planes incl. E) of a level.
@@ -215,59 +275,54 @@ inline void finish_prims(struct Wtype &W) {
   W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
 }
 
-bool launch_level(const DevLevel *Lc, DevLevel &Ld, const DevLevel *Lf, double dt, bool dropin) {
-  LevelArgs a;
-  std::memset(&a, 0, sizeof(a));
-  a.L = Ld.L;
-  a.noct = Ld.noct;
-  a.W = Ld.W;
-  a.Wn = Ld.Wn;
-  a.C = dropin ? nullptr : Ld.C;
-  a.B = dropin ? Ld.B : nullptr;
-  if (Lc != nullptr && Lc->noct > 0) {
-    a.Wc = Lc->W;
-    a.Cc = Lc->C;
-    a.nc8 = Lc->n8;
-  }
-  if (Lf != nullptr && Lf->noct > 0 && !dropin) {
-    a.Wf = Lf->W;
-    a.nf8 = Lf->n8;
-  }
-  a.split = Ld.split;
-  a.child = Ld.child;
-  a.tiles = Ld.tiles;
-  a.keys = Ld.keys;
-  a.graph = Ld.graph;
-  a.halo = Ld.halo;
-  a.bface = Ld.bface;
-  a.dt = dt;
-  a.dx = std::pow(0.5, Ld.L);
+bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, long long cells) {
+  BatchArgs a;
+  a.lv = d_lv;
+  a.work = work;
+  a.nwork = nwork;
+  a.done = g.d_done;
+  a.gate = gate;
   a.status = g.d_status;
-  a.ntiles = Ld.ntiles;
+  a.wait_limit = kWaitLimit;
   TimedLaunch tl{};
-  if (g.timing) {
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  cudaStreamIsCapturing(g.stream, &cap);
+  const bool timed = g.timing && cap == cudaStreamCaptureStatusNone;
+  if (timed) {
     tl.a = get_event();
     tl.b = get_event();
     cudaEventRecord(tl.a, g.stream);
   }
-  cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED) ? launch_level_f32(a, g.stream) : launch_level_fp64(a, g.stream);
-  if (Ld.ntiles > 0) g.kernel_launches++;
-  if (g.timing) {
+  cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED) ? launch_level_f32(a, g.nsm, g.stream)
+                                                       : launch_level_fp64(a, g.nsm, g.stream);
+  if (nwork > 0) g.kernel_launches++;
+  if (timed) {
     cudaEventRecord(tl.b, g.stream);
-    tl.cells = Ld.leaf;
+    tl.cells = cells;
     g.launches.push_back(tl);
   }
   return ck(e, "level kernel launch");
 }
 
 int level_ok(int level) {
-  if (!g.have_tree || level < g.lcoarse || level > g.lmax) {
+  if (!g.res.valid || level < g.res.lcoarse || level > g.res.lmax) {
     fail(EMMA_ST_ARG, "level " + std::to_string(level) + " is not mirrored");
     return 0;
   }
   return 1;
 }
 
+// current state buffer of a resident level (the device slot is authoritative)
+double *current_state(int level) {
+  double *p = nullptr;
+  if (!ck(cudaMemcpyAsync(&p, &g.res.d_lv[level].W, sizeof(double *), cudaMemcpyDeviceToHost, g.stream),
+          "read level slot") ||
+      !ck(cudaStreamSynchronize(g.stream), "sync"))
+    return nullptr;
+  return p;
+}
+
+// ------------------------------------------------------------ host schedule
 // hydro-only Advance_level schedule (src/advanceamr.c:243-1299), host driven
 struct Sched {
   double dt_param, time_max;
@@ -287,13 +342,13 @@ double advance_level(Sched &S, int level, double tloc) {
     S.err |= emma_hydro_comptstep(level, &dthydro);
     dtnew = (dthydro < dtnew ? dthydro : dtnew);
     adt[level - 1] = dtnew;
-    if (level == g.lcoarse) adt[level - 2] = adt[level - 1];
+    if (level == g.res.lcoarse) adt[level - 2] = adt[level - 1];
     if (adt[level - 2] < adt[level - 1]) adt[level - 1] = adt[level - 2];
     else adt[level - 1] = std::fmin(adt[level - 1], adt[level - 2] - dt);
-    if (level < g.lmax && g.lev[level + 1].noct > 0) {
+    if (level < g.res.lmax && g.res.lev[level + 1].noct > 0) {
       dtfine = advance_level(S, level + 1, tloc);
       adt[level - 1] = dtfine;
-      if (level == g.lcoarse) adt[level - 2] = adt[level - 1];
+      if (level == g.res.lcoarse) adt[level - 2] = adt[level - 1];
     }
     S.err |= emma_hydro_advance_level(level, adt[level - 1]);
     dt += adt[level - 1];
@@ -301,6 +356,111 @@ double advance_level(Sched &S, int level, double tloc) {
     is++;
   } while ((dt < adt[level - 2]) && (is < S.nsub) && S.err == 0);
   return dt;
+}
+
+// --------------------------------------------------------- device schedule
+int finest_level() {
+  int lf = g.res.lcoarse;
+  while (lf < g.res.lmax && g.res.lev[lf + 1].noct > 0) lf++;
+  return lf;
+}
+
+// emit one Advance_level(L) call: nsub gated iterations (schedule.cu)
+bool emit_level(int L, int nsub) {
+  const Tree &t = g.res;
+  const DevLevel &d = t.lev[L];
+  const int lf = finest_level();
+  const bool has_fine = L < lf;
+  SchedState *S = g.d_S;
+  for (int it = 0; it < nsub; it++) {
+    k_sub_begin<<<1, 1, 0, g.stream>>>(S, L, it);
+    const int *gate = &S->active[L];
+    const long long n5 = 5 * d.n8;
+    k_clear<<<(unsigned)std::max<long long>(1, std::min<long long>((n5 + 255) / 256, 4LL * g.nsm)), 256, 0,
+              g.stream>>>(d.C, n5, gate);
+    if (!ck(launch_cfl(t.d_lv, L, d.n8, gate, &S->smax[L], g.nsm, g.stream), "cfl launch")) return false;
+    k_sub_dt<<<1, 1, 0, g.stream>>>(S, L);
+    if (has_fine && !emit_level(L + 1, nsub)) return false;
+    k_sub_prelaunch<<<1, 1, 0, g.stream>>>(S, t.d_lv, L, has_fine ? 1 : 0);
+    if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf)) return false;
+    k_sub_end<<<1, 1, 0, g.stream>>>(S, t.d_lv, L);
+    if (!ck(cudaGetLastError(), "schedule kernel")) return false;
+  }
+  return true;
+}
+
+// one coarse step, all on the device
+bool emit_coarse_step(int nsub) {
+  const Tree &t = g.res;
+  SchedState *S = g.d_S;
+  const int lc = t.lcoarse, lf = finest_level();
+  if (nsub == 1 || lf == lc) {
+    // one dt for every level: CFL per level, then all levels in one launch
+    for (int L = lc; L <= lf; L++) {
+      const DevLevel &d = t.lev[L];
+      if (!ck(cudaMemsetAsync(&S->smax[L], 0, sizeof(unsigned long long), g.stream), "memset smax")) return false;
+      if (!ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C")) return false;
+      if (!ck(launch_cfl(t.d_lv, L, d.n8, nullptr, &S->smax[L], g.nsm, g.stream), "cfl launch")) return false;
+    }
+    k_batch_begin<<<1, 1, 0, g.stream>>>(S, t.d_lv, g.d_done);
+    long long cells = 0;
+    for (int L = lc; L <= lf; L++) cells += t.lev[L].leaf;
+    if (!launch_batch(t.d_lv, g.d_work_all, g.nwork_all, nullptr, cells)) return false;
+    k_batch_end<<<1, 1, 0, g.stream>>>(S, t.d_lv);
+    return ck(cudaGetLastError(), "schedule kernel");
+  }
+  if (!emit_level(lc, nsub)) return false;
+  k_sub_final<<<1, 1, 0, g.stream>>>(S);
+  return ck(cudaGetLastError(), "schedule kernel");
+}
+
+bool ensure_graph(int nsub) {
+  if (g.graph && g.graph_nsub == nsub && g.graph_prec == g.opt.precision) return true;
+  drop_graph();
+  cudaGraph_t graph = nullptr;
+  if (!ck(cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return false;
+  const bool ok = emit_coarse_step(nsub);
+  cudaError_t e = cudaStreamEndCapture(g.stream, &graph);
+  if (!ok || !ck(e, "end capture")) {
+    if (graph) cudaGraphDestroy(graph);
+    return false;
+  }
+  e = cudaGraphInstantiate(&g.graph, graph, 0);
+  cudaGraphDestroy(graph);
+  if (!ck(e, "graph instantiate")) {
+    g.graph = nullptr;
+    return false;
+  }
+  g.graph_nsub = nsub;
+  g.graph_prec = g.opt.precision;
+  return true;
+}
+
+bool write_sched_params(double dt_param, double time_max, int nsub, const double *tsim, const double *adt) {
+  SchedState &h = *g.h_S;
+  if (!ck(cudaStreamSynchronize(g.stream), "sync")) return false;
+  h.dt_param = dt_param;
+  h.time_max = time_max;
+  h.cfl = g.opt.cfl;
+  if (!ck(cudaMemcpyAsync(&g.d_S->dt_param, &h.dt_param, 3 * sizeof(double), cudaMemcpyHostToDevice, g.stream),
+          "write schedule parameters"))
+    return false;
+  h.nsub = nsub;
+  if (!ck(cudaMemcpyAsync(&g.d_S->nsub, &h.nsub, sizeof(int), cudaMemcpyHostToDevice, g.stream), "write nsub"))
+    return false;
+  if (tsim != nullptr) {
+    h.tsim = *tsim;
+    if (!ck(cudaMemcpyAsync(&g.d_S->tsim, &h.tsim, sizeof(double), cudaMemcpyHostToDevice, g.stream), "write tsim"))
+      return false;
+  }
+  if (adt != nullptr) {
+    for (int l = 0; l < g.res.lmax && l < kMaxLevels; l++) h.adt[l] = adt[l];
+    if (!ck(cudaMemcpyAsync(g.d_S->adt, h.adt, sizeof(double) * std::min(g.res.lmax, kMaxLevels),
+                            cudaMemcpyHostToDevice, g.stream),
+            "write adt"))
+      return false;
+  }
+  return ck(cudaStreamSynchronize(g.stream), "sync");
 }
 
 }  // namespace
@@ -334,11 +494,12 @@ void emma_hydro_default_options(struct EmmaHydroOptions *opt) {
   opt->cfl = 0.85;
   opt->tile_octs = 0;
   opt->device = 0;
+  opt->use_graph = 1;
 }
 
 int emma_hydro_init(const struct EmmaHydroOptions *opt) {
   if (g.ready) {
-    if (opt) g.opt = *opt;
+    if (opt) return emma_hydro_set_options(opt);
     return 0;
   }
   emma_hydro_default_options(&g.opt);
@@ -348,8 +509,12 @@ int emma_hydro_init(const struct EmmaHydroOptions *opt) {
   CK(cudaDeviceGetAttribute(&g.nsm, cudaDevAttrMultiProcessorCount, g.opt.device));
   CK(cudaMalloc(&g.d_status, sizeof(unsigned)));
   CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
-  CK(cudaMalloc(&g.d_smax, sizeof(unsigned long long)));
-  CK(cudaMallocHost(&g.h_smax, sizeof(unsigned long long)));
+  CK(cudaMalloc(&g.d_done, sizeof(unsigned) * kMaxLevels));
+  CK(cudaMemset(g.d_done, 0, sizeof(unsigned) * kMaxLevels));
+  CK(cudaMalloc(&g.d_S, sizeof(SchedState)));
+  CK(cudaMemset(g.d_S, 0, sizeof(SchedState)));
+  CK(cudaMallocHost(&g.h_S, sizeof(SchedState)));
+  std::memset(g.h_S, 0, sizeof(SchedState));
   g.ready = true;
   return 0;
 }
@@ -359,7 +524,7 @@ int emma_hydro_set_options(const struct EmmaHydroOptions *opt) {
   if (!g.ready) return emma_hydro_init(opt);
   const int old_trans = g.opt.trans_flags;
   g.opt = *opt;
-  if (g.have_tree && old_trans != opt->trans_flags) {
+  if (g.res.valid && old_trans != opt->trans_flags) {
     fail(EMMA_ST_ARG, "transmissive flags changed: upload the tree again");
     return EMMA_ST_ARG;
   }
@@ -369,61 +534,96 @@ int emma_hydro_set_options(const struct EmmaHydroOptions *opt) {
 void emma_hydro_shutdown(void) {
   if (!g.ready) return;
   cudaStreamSynchronize(g.stream);
-  for (auto &d : g.lev) free_level(d);
-  for (auto &d : g.drop_lev) free_level(d);
-  g.lev.clear();
-  g.drop_lev.clear();
+  drop_graph();
+  free_tree(g.res);
+  free_tree(g.drop);
+  cudaFree(g.d_work_all);
   for (auto &t : g.launches) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
   }
   for (auto e : g.free_events) cudaEventDestroy(e);
-  g.launches.clear();
-  g.free_events.clear();
   cudaFree(g.d_status);
-  cudaFree(g.d_smax);
-  cudaFreeHost(g.h_smax);
+  cudaFree(g.d_done);
+  cudaFree(g.d_S);
+  cudaFreeHost(g.h_S);
   if (g.pin) cudaFreeHost(g.pin);
   if (g.own_stream) cudaStreamDestroy(g.stream);
   g = Ctx();
 }
 
+int emma_hydro_set_stream(void *stream) {
+  if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
+  CK(cudaStreamSynchronize(g.stream));
+  drop_graph();
+  if (g.own_stream) CK(cudaStreamDestroy(g.stream));
+  // NULL selects a stream owned by the library (a caller wanting the legacy
+  // default stream passes cudaStreamLegacy)
+  if (stream == nullptr) {
+    CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+    g.own_stream = true;
+  } else {
+    g.stream = static_cast<cudaStream_t>(stream);
+    g.own_stream = false;
+  }
+  return 0;
+}
+
 // ------------------------------------------------------------ resident path
 int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int rank) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
-  if (firstoct == nullptr || lcoarse < 2 || lmax < lcoarse) {
+  if (firstoct == nullptr || lcoarse < 2 || lmax < lcoarse || lmax >= kMaxLevels) {
     fail(EMMA_ST_ARG, "bad tree arguments");
     return EMMA_ST_ARG;
   }
   CK(cudaStreamSynchronize(g.stream));
-  for (auto &d : g.lev) free_level(d);
-  g.have_tree = false;
+  drop_graph();
+  free_tree(g.res);
+  cudaFree(g.d_work_all);
+  g.d_work_all = nullptr;
+  g.nwork_all = 0;
   std::string err;
-  int rc = build_host_tree(firstoct, lcoarse, lmax, rank, g.opt.trans_flags, lcoarse, lmax, g.host, err);
+  int rc = build_host_tree(firstoct, lcoarse, lmax, rank, g.opt.trans_flags, lcoarse, lmax, g.res.host, err);
   if (rc != 0) {
     fail((unsigned)rc, err);
     return rc;
   }
-  if (!alloc_levels(g.host, g.lev, false)) return EMMA_ST_CUDA;
-  g.lcoarse = lcoarse;
-  g.lmax = lmax;
-  g.have_tree = true;
+  if (!alloc_tree(g.res.host, g.res, false)) return EMMA_ST_CUDA;
+  // batched work list: finest level first, each level's tiles in order
+  std::vector<int> all;
+  for (int L = lmax; L >= lcoarse; L--)
+    for (int i = 0; i < g.res.lev[L].ntiles; i++) all.push_back((L << kWorkSlotShift) | i);
+  if (!upload_vec(&g.d_work_all, all)) return EMMA_ST_CUDA;
+  g.nwork_all = (int)all.size();
+  // schedule constants
+  SchedState &h = *g.h_S;
+  std::memset(&h, 0, sizeof(h));
+  h.lcoarse = lcoarse;
+  h.lmax = lmax;
+  h.cfl = g.opt.cfl;
+  h.dt_param = 1e9;
+  h.time_max = 1e9;
+  h.nsub = 2;
+  for (int L = 0; L < kMaxLevels; L++) h.dx[L] = std::pow(0.5, L);
+  CK(cudaMemcpy(g.d_S, &h, sizeof(SchedState), cudaMemcpyHostToDevice));
   return emma_hydro_fields_upload(firstoct);
 }
 
 int emma_hydro_fields_upload(struct OCT **firstoct) {
   (void)firstoct;
-  if (!g.have_tree) {
+  if (!g.res.valid) {
     fail(EMMA_ST_ARG, "no tree uploaded");
     return EMMA_ST_ARG;
   }
-  for (int L = g.lcoarse; L <= g.lmax; L++) {
-    const HostLevel &h = g.host.lev[L];
+  for (int L = g.res.lcoarse; L <= g.res.lmax; L++) {
+    const HostLevel &h = g.res.host.lev[L];
     if (h.noct == 0) continue;
+    double *W = current_state(L);
+    if (W == nullptr) return EMMA_ST_CUDA;
     const size_t bytes = sizeof(double) * 5 * 8 * (size_t)h.noct;
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
     pack_level(h, 0, g.pin);
-    CK(cudaMemcpyAsync(g.lev[L].W, g.pin, bytes, cudaMemcpyHostToDevice, g.stream));
+    CK(cudaMemcpyAsync(W, g.pin, bytes, cudaMemcpyHostToDevice, g.stream));
     CK(cudaStreamSynchronize(g.stream));
   }
   return 0;
@@ -431,17 +631,19 @@ int emma_hydro_fields_upload(struct OCT **firstoct) {
 
 int emma_hydro_tree_download(struct OCT **firstoct) {
   (void)firstoct;
-  if (!g.have_tree) {
+  if (!g.res.valid) {
     fail(EMMA_ST_ARG, "no tree uploaded");
     return EMMA_ST_ARG;
   }
-  for (int L = g.lcoarse; L <= g.lmax; L++) {
-    const HostLevel &h = g.host.lev[L];
+  for (int L = g.res.lcoarse; L <= g.res.lmax; L++) {
+    const HostLevel &h = g.res.host.lev[L];
     if (h.noct == 0) continue;
+    double *W = current_state(L);
+    if (W == nullptr) return EMMA_ST_CUDA;
     const long long n8 = 8LL * h.noct;
     const size_t bytes = sizeof(double) * 5 * (size_t)n8;
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
-    CK(cudaMemcpyAsync(g.pin, g.lev[L].W, bytes, cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(g.pin, W, bytes, cudaMemcpyDeviceToHost, g.stream));
     CK(cudaStreamSynchronize(g.stream));
     const double *p = g.pin;
     parallel_for(h.noct, [&](long long a, long long b) {
@@ -466,34 +668,38 @@ int emma_hydro_tree_download(struct OCT **firstoct) {
 }
 
 int emma_hydro_level_noct(int level) {
-  if (!g.have_tree || level < g.lcoarse || level > g.lmax) return 0;
-  return g.lev[level].noct;
+  if (!g.res.valid || level < g.res.lcoarse || level > g.res.lmax) return 0;
+  return g.res.lev[level].noct;
 }
 
 long long emma_hydro_level_leaf_cells(int level) {
-  if (!g.have_tree || level < g.lcoarse || level > g.lmax) return 0;
-  return g.lev[level].leaf;
+  if (!g.res.valid || level < g.res.lcoarse || level > g.res.lmax) return 0;
+  return g.res.lev[level].leaf;
 }
 
 int emma_hydro_get_level_state(int level, double *host_out) {
   if (!level_ok(level) || host_out == nullptr) return EMMA_ST_ARG;
-  const DevLevel &d = g.lev[level];
-  CK(cudaMemcpyAsync(host_out, d.W, sizeof(double) * 5 * d.n8, cudaMemcpyDeviceToHost, g.stream));
+  const DevLevel &d = g.res.lev[level];
+  double *W = current_state(level);
+  if (W == nullptr) return EMMA_ST_CUDA;
+  CK(cudaMemcpyAsync(host_out, W, sizeof(double) * 5 * d.n8, cudaMemcpyDeviceToHost, g.stream));
   CK(cudaStreamSynchronize(g.stream));
   return 0;
 }
 
 int emma_hydro_set_level_state(int level, const double *host_in) {
   if (!level_ok(level) || host_in == nullptr) return EMMA_ST_ARG;
-  const DevLevel &d = g.lev[level];
-  CK(cudaMemcpyAsync(d.W, host_in, sizeof(double) * 5 * d.n8, cudaMemcpyHostToDevice, g.stream));
+  const DevLevel &d = g.res.lev[level];
+  double *W = current_state(level);
+  if (W == nullptr) return EMMA_ST_CUDA;
+  CK(cudaMemcpyAsync(W, host_in, sizeof(double) * 5 * d.n8, cudaMemcpyHostToDevice, g.stream));
   CK(cudaStreamSynchronize(g.stream));
   return 0;
 }
 
 int emma_hydro_clean_new(int level) {
   if (!level_ok(level)) return EMMA_ST_ARG;
-  const DevLevel &d = g.lev[level];
+  const DevLevel &d = g.res.lev[level];
   if (d.n8 == 0) return 0;
   CK(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream));
   return 0;
@@ -501,16 +707,17 @@ int emma_hydro_clean_new(int level) {
 
 int emma_hydro_comptstep(int level, double *dt_out) {
   if (!level_ok(level) || dt_out == nullptr) return EMMA_ST_ARG;
-  const DevLevel &d = g.lev[level];
+  const DevLevel &d = g.res.lev[level];
   double dt = 1e9;
   if (d.n8 > 0) {
-    CK(cudaMemsetAsync(g.d_smax, 0, sizeof(unsigned long long), g.stream));
-    CK(launch_cfl(d.W, d.n8, g.d_smax, g.nsm, g.stream));
+    unsigned long long *slot = &g.d_S->smax[level];
+    CK(cudaMemsetAsync(slot, 0, sizeof(unsigned long long), g.stream));
+    CK(launch_cfl(g.res.d_lv, level, d.n8, nullptr, slot, g.nsm, g.stream));
     g.kernel_launches++;
-    CK(cudaMemcpyAsync(g.h_smax, g.d_smax, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
+    CK(cudaMemcpyAsync(&g.h_S->smax[level], slot, sizeof(unsigned long long), cudaMemcpyDeviceToHost, g.stream));
     CK(cudaStreamSynchronize(g.stream));
     double smax;
-    std::memcpy(&smax, g.h_smax, sizeof(double));
+    std::memcpy(&smax, &g.h_S->smax[level], sizeof(double));
     const double dxcur = std::pow(0.5, level);
     if (smax > 0.) dt = std::fmin(dxcur * g.opt.cfl / (smax * 3.), dt);
   }
@@ -520,51 +727,87 @@ int emma_hydro_comptstep(int level, double *dt_out) {
 
 int emma_hydro_advance_level(int level, double dt) {
   if (!level_ok(level)) return EMMA_ST_ARG;
-  DevLevel &d = g.lev[level];
+  DevLevel &d = g.res.lev[level];
   if (d.noct == 0) return 0;
-  const DevLevel *Lc = (level > g.lcoarse) ? &g.lev[level - 1] : nullptr;
-  const DevLevel *Lf = (level < g.lmax) ? &g.lev[level + 1] : nullptr;
-  if (!launch_level(Lc, d, Lf, dt, false)) return EMMA_ST_CUDA;
-  std::swap(d.W, d.Wn);
+  k_bind_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, g.res.lcoarse, g.res.lmax, dt);
+  CK(cudaGetLastError());
+  if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf)) return EMMA_ST_CUDA;
+  k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
+  CK(cudaGetLastError());
   g.updates += d.leaf;
   return 0;
 }
 
 int emma_hydro_advance_coarse_step(double dt_param, double time_max, int nsub, double *tsim, double *adt) {
-  if (!g.have_tree || tsim == nullptr || adt == nullptr) {
+  if (!g.res.valid || tsim == nullptr || adt == nullptr) {
     fail(EMMA_ST_ARG, "advance_coarse_step: no tree or null pointer");
     return EMMA_ST_ARG;
   }
-  Sched S{dt_param, time_max, nsub, adt, 0};
-  advance_level(S, g.lcoarse, *tsim);
-  *tsim += adt[g.lcoarse - 1];
-  return S.err;
+  if (!g.opt.use_graph) {
+    Sched S{dt_param, time_max, nsub, adt, 0};
+    advance_level(S, g.res.lcoarse, *tsim);
+    *tsim += adt[g.res.lcoarse - 1];
+    return S.err;
+  }
+  if (!write_sched_params(dt_param, time_max, nsub, tsim, adt)) return EMMA_ST_CUDA;
+  int rc = emma_hydro_advance_coarse_step_async(dt_param, time_max, nsub);
+  if (rc != 0) return rc;
+  return emma_hydro_get_time(tsim, adt);
 }
 
-long long emma_hydro_cell_updates(void) { return g.updates; }
-
-long long emma_hydro_kernel_launches(void) { return g.kernel_launches; }
-
-int emma_hydro_set_stream(void *stream) {
-  if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
-  CK(cudaStreamSynchronize(g.stream));
-  if (g.own_stream) CK(cudaStreamDestroy(g.stream));
-  // NULL selects a stream owned by the library (a caller wanting the legacy
-  // default stream passes cudaStreamLegacy)
-  if (stream == nullptr) {
-    CK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
-    g.own_stream = true;
-  } else {
-    g.stream = static_cast<cudaStream_t>(stream);
-    g.own_stream = false;
+int emma_hydro_advance_coarse_step_async(double dt_param, double time_max, int nsub) {
+  if (!g.res.valid || nsub < 1) {
+    fail(EMMA_ST_ARG, "advance_coarse_step_async: no tree or nsub < 1");
+    return EMMA_ST_ARG;
   }
+  SchedState &h = *g.h_S;
+  if (h.dt_param != dt_param || h.time_max != time_max || h.nsub != nsub || h.cfl != g.opt.cfl)
+    if (!write_sched_params(dt_param, time_max, nsub, nullptr, nullptr)) return EMMA_ST_CUDA;
+  if (!ensure_graph(nsub)) return EMMA_ST_CUDA;
+  CK(cudaGraphLaunch(g.graph, g.stream));
   return 0;
 }
+
+int emma_hydro_get_time(double *tsim, double *adt) {
+  if (!g.res.valid) return EMMA_ST_ARG;
+  CK(cudaMemcpyAsync(g.h_S, g.d_S, sizeof(SchedState), cudaMemcpyDeviceToHost, g.stream));
+  CK(cudaStreamSynchronize(g.stream));
+  if (tsim) *tsim = g.h_S->tsim;
+  if (adt)
+    for (int l = 0; l < g.res.lmax && l < kMaxLevels; l++) adt[l] = g.h_S->adt[l];
+  return 0;
+}
+
+int emma_hydro_set_time(double tsim, const double *adt) {
+  if (!g.res.valid) return EMMA_ST_ARG;
+  SchedState &h = *g.h_S;
+  return write_sched_params(h.dt_param == 0. ? 1e9 : h.dt_param, h.time_max == 0. ? 1e9 : h.time_max,
+                            h.nsub == 0 ? 2 : h.nsub, &tsim, adt)
+             ? 0
+             : EMMA_ST_CUDA;
+}
+
+long long emma_hydro_cell_updates(void) {
+  long long dev = 0;
+  if (g.ready && g.res.valid) {
+    long long *p = &g.h_S->updates;
+    cudaMemcpyAsync(p, &g.d_S->updates, sizeof(long long), cudaMemcpyDeviceToHost, g.stream);
+    cudaStreamSynchronize(g.stream);
+    dev = *p;
+  }
+  return g.updates + dev;
+}
+
+long long emma_hydro_kernel_launches(void) { return g.kernel_launches; }
 
 void emma_hydro_reset_counters(void) {
   g.updates = 0;
   g.kernel_launches = 0;
-  if (g.ready) cudaStreamSynchronize(g.stream);
+  if (g.ready) {
+    cudaStreamSynchronize(g.stream);
+    if (g.d_S) cudaMemsetAsync(&g.d_S->updates, 0, sizeof(long long), g.stream);
+    cudaStreamSynchronize(g.stream);
+  }
   for (auto &t : g.launches) {
     g.free_events.push_back(t.a);
     g.free_events.push_back(t.b);
@@ -591,7 +834,7 @@ int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cel
 
 // Host-only planning diagnostics (no GPU needed): builds and validates the tile
 // plans of levels lcoarse..lmax and reports, per level, {octs, tiles, max staged
-// octs, max halo cells, leaf cells}.  Returns the status bits of the planning.
+// octs, max halo entries, leaf cells}.  Returns the status bits of the planning.
 int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int trans, long long *stats5) {
   HostTree H;
   std::string err;
@@ -647,7 +890,7 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   (void)stride;
   (void)dxcur;
   if (!g.ready && emma_hydro_init(nullptr) != 0) return 0;
-  if (firstoct == nullptr || level < 2 || firstoct[level - 1] == nullptr) return 0;
+  if (firstoct == nullptr || level < 2 || level >= kMaxLevels - 1 || firstoct[level - 1] == nullptr) return 0;
   const int rank = dropin_rank(cpu);
   // levels present around `level`: L-1 always exists; L+1 only if a cell is split
   bool has_fine = false;
@@ -656,29 +899,26 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
       if (o->cell[c].child != nullptr) has_fine = true;
   const int lo = level - 1, hi = has_fine ? level + 1 : level;
   std::vector<long long> sig = tree_signature(firstoct, lo, hi);
-  if (g.drop_first != firstoct || g.drop_level != level || sig != g.drop_sig) {
+  if (g.drop_first != firstoct || g.drop_level != level || sig != g.drop_sig || !g.drop.valid) {
     cudaStreamSynchronize(g.stream);
-    for (auto &d : g.drop_lev) free_level(d);
-    g.drop_lev.clear();
+    free_tree(g.drop);
     g.drop_level = -1;
     std::string err;
-    int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, g.drop_host, err);
+    int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, g.drop.host, err);
     if (rc != 0) {
       fail((unsigned)rc, err);
       return 0;
     }
-    if (!alloc_levels(g.drop_host, g.drop_lev, true)) return 0;
+    if (!alloc_tree(g.drop.host, g.drop, true)) return 0;
     g.drop_first = firstoct;
     g.drop_level = level;
-    g.drop_lo = lo;
-    g.drop_hi = hi;
     g.drop_sig = sig;
   }
-  HostTree &H = g.drop_host;
+  HostTree &H = g.drop.host;
   const HostLevel &h = H.lev[level];
   const HostLevel &hc = H.lev[level - 1];
-  DevLevel &d = g.drop_lev[level];
-  DevLevel &dc = g.drop_lev[level - 1];
+  DevLevel &d = g.drop.lev[level];
+  DevLevel &dc = g.drop.lev[level - 1];
   if (h.noct == 0) return 0;
   const long long n8 = d.n8, nc8 = dc.n8;
   const size_t need = sizeof(double) * std::max<long long>(11 * n8, 5 * nc8);
@@ -686,24 +926,51 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   // upload: level field (5 planes) + fieldnew (6 planes), coarser field
   pack_level(h, 0, g.pin);
   pack_level(h, 1, g.pin + 5 * n8);
-  if (!ck(cudaMemcpyAsync(d.W, g.pin, sizeof(double) * 5 * n8, cudaMemcpyHostToDevice, g.stream), "H2D W")) return 0;
+  if (!ck(cudaMemcpyAsync(d.W0, g.pin, sizeof(double) * 5 * n8, cudaMemcpyHostToDevice, g.stream), "H2D W")) return 0;
   if (!ck(cudaMemcpyAsync(d.B, g.pin + 5 * n8, sizeof(double) * 6 * n8, cudaMemcpyHostToDevice, g.stream), "H2D B"))
     return 0;
-  if (nc8 > 0 && !h.inj_cells.empty()) {
+  const bool coarse = nc8 > 0 && !h.inj_cells.empty();
+  if (coarse) {
     if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
     pack_level(hc, 0, g.pin);
-    if (!ck(cudaMemcpyAsync(dc.W, g.pin, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))
+    if (!ck(cudaMemcpyAsync(dc.W0, g.pin, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))
       return 0;
     if (!ck(cudaMemsetAsync(dc.C, 0, sizeof(double) * 5 * nc8, g.stream), "memset Cc")) return 0;
   }
-  if (!launch_level(nc8 > 0 ? &dc : nullptr, d, nullptr, dtnew, true)) return 0;
+  LevelArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.L = level;
+  a.noct = d.noct;
+  a.W = d.W0;
+  a.Wn = d.W1;
+  a.C = nullptr;
+  a.B = d.B;
+  a.Wc = coarse ? dc.W0 : nullptr;
+  a.Cc = coarse ? dc.C : nullptr;
+  a.nc8 = nc8;
+  a.Wf = nullptr;
+  a.split = d.split;
+  a.child = d.child;
+  a.tiles = d.tiles;
+  a.keys = d.keys;
+  a.graph = d.graph;
+  a.halo = d.halo;
+  a.bface = d.bface;
+  a.dt = dtnew;
+  a.dx = std::pow(0.5, level);
+  a.ntiles = d.ntiles;
+  a.wait_slot = -1;
+  a.leaf = d.leaf;
+  k_set_args<<<1, 1, 0, g.stream>>>(g.drop.d_lv, level, a);
+  if (!ck(cudaGetLastError(), "k_set_args")) return 0;
+  if (!launch_batch(g.drop.d_lv, d.work, d.ntiles, nullptr, d.leaf)) return 0;
   // download the level's new state into fieldnew (leaf cells)
-  if (!ck(cudaMemcpyAsync(g.pin, d.Wn, sizeof(double) * 5 * n8, cudaMemcpyDeviceToHost, g.stream), "D2H Wn")) return 0;
+  if (!ck(cudaMemcpyAsync(g.pin, d.W1, sizeof(double) * 5 * n8, cudaMemcpyDeviceToHost, g.stream), "D2H Wn")) return 0;
   if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
   {
     const double *p = g.pin;
-    parallel_for(h.noct, [&](long long a, long long b) {
-      for (long long i = a; i < b; i++) {
+    parallel_for(h.noct, [&](long long a0, long long b0) {
+      for (long long i = a0; i < b0; i++) {
         struct OCT *o = h.octs[i];
         for (int c = 0; c < 8; c++) {
           if (o->cell[c].child != nullptr) continue;
@@ -720,7 +987,7 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
     });
   }
   // fine -> coarse corrections: fieldnew = U2W(W2U(fieldnew) + dU) per coarse cell
-  if (nc8 > 0 && !h.inj_cells.empty()) {
+  if (coarse) {
     if (!ck(cudaMemcpyAsync(g.pin, dc.C, sizeof(double) * 5 * nc8, cudaMemcpyDeviceToHost, g.stream), "D2H Cc"))
       return 0;
     if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
@@ -797,8 +1064,7 @@ void destroy_hydstencil_GPU(struct CPUINFO *cpu, int stride) {
   (void)stride;
   if (!g.ready) return;
   cudaStreamSynchronize(g.stream);
-  for (auto &d : g.drop_lev) free_level(d);
-  g.drop_lev.clear();
+  free_tree(g.drop);
   g.drop_level = -1;
   g.drop_first = nullptr;
 }

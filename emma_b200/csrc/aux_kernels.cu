@@ -3,10 +3,14 @@
 // (src/advanceamr.c:122-128), so that the level dt is bit-identical.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include "plan_types.h"
 
 namespace emma {
 
-__global__ void cfl_smax_kernel(const double *__restrict__ W, long long n8, unsigned long long *out) {
+__global__ void cfl_smax_kernel(const LevelArgs *lv, int slot, const int *gate, unsigned long long *out) {
+  if (gate != nullptr && *gate == 0) return;
+  const double *__restrict__ W = lv[slot].W;
+  const long long n8 = 8LL * lv[slot].noct;
   double m = 0.;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n8; i += (long long)gridDim.x * blockDim.x) {
     const double d = W[i], u = W[n8 + i], v = W[2 * n8 + i], w = W[3 * n8 + i], p = W[4 * n8 + i];
@@ -27,12 +31,13 @@ __global__ void cfl_smax_kernel(const double *__restrict__ W, long long n8, unsi
   }
 }
 
-cudaError_t launch_cfl(const double *W, long long n8, unsigned long long *out, int nsm, cudaStream_t s) {
+cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *gate, unsigned long long *out, int nsm,
+                       cudaStream_t s) {
   long long blocks = (n8 + 255) / 256;
   long long cap = 4LL * nsm;
   if (blocks > cap) blocks = cap;
   if (blocks < 1) blocks = 1;
-  cfl_smax_kernel<<<(unsigned)blocks, 256, 0, s>>>(W, n8, out);
+  cfl_smax_kernel<<<(unsigned)blocks, 256, 0, s>>>(lv, slot, gate, out);
   return cudaGetLastError();
 }
 

@@ -24,7 +24,7 @@ constexpr double kErrTol = 1e-10;  // ERRTOL, src/hydro_utils.c:18
 constexpr int kNiterMax = 10;      // NITERMAX, src/hydro_utils.c:17
 
 // status bits (mirrors EMMA_ST_* of emma_hydro.h)
-constexpr unsigned kStNegDensity = 0x01, kStNegPstar = 0x02, kStNan = 0x04, kStTree = 0x08;
+constexpr unsigned kStNegDensity = 0x01, kStNegPstar = 0x02, kStNan = 0x04, kStTree = 0x08, kStTimeout = 0x40;
 
 // ============================================================== FP64 (plain)
 struct MathF64 {

@@ -57,12 +57,11 @@ struct LevelSmem {
 };
 
 template <class M, int T, int SMAX, int HMAX, int BMAX>
-__global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
-    level_advance_kernel(const LevelArgs A) {
+__device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs &A, const int slot, const int tile,
+                                           unsigned char *smem, unsigned &st) {
   using R = typename M::R;
   using SM = LevelSmem<M, T, SMAX, HMAX, BMAX>;
   constexpr int NT = SM::NT;
-  extern __shared__ __align__(16) unsigned char smem[];
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
   R *sM = reinterpret_cast<R *>(smem + SM::off_M);
   R *sHS = reinterpret_cast<R *>(smem + SM::off_HS);
@@ -77,13 +76,13 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
   uint8_t *sSp = smem + SM::off_sp;
 
   const int tid = threadIdx.x;
-  const TileDesc td = A.tiles[blockIdx.x];
+  const TileDesc td = A.tiles[tile];
   const int n = td.noct, S = td.S, H = td.H, B = td.B;
   const int n8 = 8 * n;
   const long long N8 = 8LL * A.noct;
-  unsigned st = 0;
   if (S > SMAX || H > HMAX || B > BMAX || n > T || n < 1) {  // plan cut for another kernel shape
-    if (tid == 0) atomicOr(A.status, kStTree);
+    st |= kStTree;
+    if (tid == 0) atomicAdd(Bt.done + slot, 1u);  // keep batched waits bounded
     return;
   }
 
@@ -102,7 +101,7 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
     const int e = sBface[b];
     sBmap[(e >> 2) * 3 + (e & 3)] = (uint16_t)b;
   }
-#pragma unroll 2
+#pragma unroll 4
   for (int i = tid; i < S * 8; i += NT) {
     const int s = i >> 3, c = i & 7;
     const uint32_t key = sKey[s];
@@ -273,6 +272,23 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
   __syncthreads();
 
   // ------------------------------------------------------------------ P3
+  // In a batched launch the finer level's update (its corrections into C and
+  // its new state, averaged into split cells here) must be complete first.
+  if (A.wait_slot >= 0) {
+    if (tid == 0) {
+      const unsigned need = (unsigned)Bt.lv[A.wait_slot].ntiles;
+      long long it = 0;
+      while (*reinterpret_cast<volatile unsigned *>(Bt.done + A.wait_slot) < need) {
+        if (++it > Bt.wait_limit) {
+          st |= kStTimeout;
+          break;
+        }
+        __nanosleep(64);
+      }
+      __threadfence();
+    }
+    __syncthreads();
+  }
   if (tid < n8) {
     const int o = tid >> 3, c = tid & 7;
     const long long gi = 8LL * (td.oct0 + o) + c;
@@ -292,7 +308,7 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
         if (ch >= 0) {
           for (int i = 0; i < 8; i++)
 #pragma unroll
-            for (int v = 0; v < 5; v++) acc[v] += A.Wf[v * A.nf8 + 8 * ch + i] * 0.125;
+            for (int v = 0; v < 5; v++) acc[v] += __ldcg(A.Wf + v * A.nf8 + 8 * ch + i) * 0.125;
         } else {
           st |= kStTree;
         }
@@ -301,56 +317,48 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
       for (int v = 0; v < 5; v++) Wout[v] = acc[v];
     } else {
       const double dtsurdx = A.dt / A.dx;
-      // fluxes of the six faces in the reference's order
-      double Fd[6][5];
-#pragma unroll
-      for (int d = 0; d < 3; d++) {
-#pragma unroll
-        for (int v = 0; v < 5; v++) Fd[2 * d][v] = (double)sF[v * 3 * NT + d * NT + tid];
+      // flux of face k (0:-x 1:+x ...) of this cell, from the face tasks of P2
+      auto flux = [&](int k, int v) -> double {
+        const int d = k >> 1;
+        if (!(k & 1)) return (double)sF[v * 3 * NT + d * NT + tid];
         int c2;
-        const int s2 = nb(o, c, 2 * d + 1, c2);
-        if (s2 >= 0 && s2 < n) {
+        const int s2 = nb(o, c, k, c2);
+        if (s2 >= 0 && s2 < n) return (double)sF[v * 3 * NT + d * NT + s2 * 8 + c2];
+        return (double)sFB[v * BMAX + sBmap[tid * 3 + d]];
+      };
+      // updatefield (src/hydro_utils.c:3050-3082): dU = sum over faces -x,+x,-y,+y,-z,+z
+      // of (+-F dt/dx), signs alternating from +
+      double dU[5] = {0., 0., 0., 0., 0.};
+      double one = 1.;
 #pragma unroll
-          for (int v = 0; v < 5; v++) Fd[2 * d + 1][v] = (double)sF[v * 3 * NT + d * NT + s2 * 8 + c2];
-        } else {
-          const int b = sBmap[tid * 3 + d];
+      for (int k = 0; k < 6; k++) {
 #pragma unroll
-          for (int v = 0; v < 5; v++) Fd[2 * d + 1][v] = (double)sFB[v * BMAX + b];
-        }
+        for (int v = 0; v < 5; v++) dU[v] += flux(k, v) * dtsurdx * one;
+        one *= -1.;
       }
       double Ud, Udu, Udv, Udw, UE;
+      if (A.B != nullptr) {  // drop-in: W2U of the caller's fieldnew
+        const double bd = A.B[gi];
+        Ud = bd;
+        Udu = bd * A.B[N8 + gi];
+        Udv = bd * A.B[2 * N8 + gi];
+        Udw = bd * A.B[3 * N8 + gi];
+        UE = A.B[5 * N8 + gi];
+      } else {  // resident: W2U(field) + corrections received from the finer level
+        Ud = q[0];
+        Udu = q[0] * q[1];
+        Udv = q[0] * q[2];
+        Udw = q[0] * q[3];
+        UE = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+      }
       if constexpr (sizeof(R) == 8) {
-        // updatefield (src/hydro_utils.c:3050-3082): dU = sum (+-F dt/dx), alternating signs
-        double dU[5] = {0., 0., 0., 0., 0.};
-        double one = 1.;
-#pragma unroll
-        for (int f = 0; f < 6; f++) {
-#pragma unroll
-          for (int v = 0; v < 5; v++) dU[v] += Fd[f][v] * dtsurdx * one;
-          one *= -1.;
-        }
-        // scatterstencil central update (src/hydro_utils.c:3129-3188): W2U(fieldnew) + dU
-        if (A.B != nullptr) {
-          const double bd = A.B[gi];
-          Ud = bd;
-          Udu = bd * A.B[N8 + gi];
-          Udv = bd * A.B[2 * N8 + gi];
-          Udw = bd * A.B[3 * N8 + gi];
-          UE = A.B[5 * N8 + gi];
-        } else {
-          const double E0 = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-          Ud = q[0];
-          Udu = q[0] * q[1];
-          Udv = q[0] * q[2];
-          Udw = q[0] * q[3];
-          UE = E0;
-          if (A.C != nullptr) {
-            Ud += A.C[gi];
-            Udu += A.C[N8 + gi];
-            Udv += A.C[2 * N8 + gi];
-            Udw += A.C[3 * N8 + gi];
-            UE += A.C[4 * N8 + gi];
-          }
+        // scatterstencil central update (src/hydro_utils.c:3129-3188), reference order
+        if (A.B == nullptr && A.C != nullptr) {
+          Ud += __ldcg(A.C + gi);
+          Udu += __ldcg(A.C + N8 + gi);
+          Udv += __ldcg(A.C + 2 * N8 + gi);
+          Udw += __ldcg(A.C + 3 * N8 + gi);
+          UE += __ldcg(A.C + 4 * N8 + gi);
         }
         Ud += dU[0];
         Udu += dU[1];
@@ -358,42 +366,25 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
         Udw += dU[3];
         UE += dU[4];
       } else {
-        // mixed: FP32 fluxes, FP64 Neumaier-compensated accumulation of
-        // W2U(state) + corrections + sum(+-F dt/dx)
-        double s[5];
-        if (A.B != nullptr) {
-          const double bd = A.B[gi];
-          s[0] = bd;
-          s[1] = bd * A.B[N8 + gi];
-          s[2] = bd * A.B[2 * N8 + gi];
-          s[3] = bd * A.B[3 * N8 + gi];
-          s[4] = A.B[5 * N8 + gi];
-        } else {
-          s[0] = q[0];
-          s[1] = q[0] * q[1];
-          s[2] = q[0] * q[2];
-          s[3] = q[0] * q[3];
-          s[4] = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
-        }
-        double comp[5] = {0., 0., 0., 0., 0.};
+        // mixed: FP32 face fluxes summed in FP64, added to the FP64 conserved state
+        // with Neumaier-compensated summation (base + corrections + dU)
+        double sum[5] = {Ud, Udu, Udv, Udw, UE}, comp[5] = {0., 0., 0., 0., 0.};
         auto add = [&](int v, double x) {
-          const double t = s[v] + x;
-          comp[v] += (fabs(s[v]) >= fabs(x)) ? ((s[v] - t) + x) : ((x - t) + s[v]);
-          s[v] = t;
+          const double t = sum[v] + x;
+          comp[v] += (fabs(sum[v]) >= fabs(x)) ? ((sum[v] - t) + x) : ((x - t) + sum[v]);
+          sum[v] = t;
         };
-        if (A.C != nullptr && A.B == nullptr) {
+        if (A.B == nullptr && A.C != nullptr) {
 #pragma unroll
-          for (int v = 0; v < 5; v++) add(v, A.C[v * N8 + gi]);
+          for (int v = 0; v < 5; v++) add(v, __ldcg(A.C + v * N8 + gi));
         }
 #pragma unroll
-        for (int f = 0; f < 6; f++)
-#pragma unroll
-          for (int v = 0; v < 5; v++) add(v, (f & 1) ? -(Fd[f][v] * dtsurdx) : (Fd[f][v] * dtsurdx));
-        Ud = s[0] + comp[0];
-        Udu = s[1] + comp[1];
-        Udv = s[2] + comp[2];
-        Udw = s[3] + comp[3];
-        UE = s[4] + comp[4];
+        for (int v = 0; v < 5; v++) add(v, dU[v]);
+        Ud = sum[0] + comp[0];
+        Udu = sum[1] + comp[1];
+        Udv = sum[2] + comp[2];
+        Udw = sum[3] + comp[3];
+        UE = sum[4] + comp[4];
       }
       // U2W (src/hydro_utils.c:35-64), pressure floor, E - Ekin recovery
       const double dl = (Ud == 0. ? 10. : Ud);
@@ -416,13 +407,36 @@ __global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 2)
         const long long cc = key & 0x0FFFFFFFu;
         const double one = (k & 1) ? 1. : -1.;
 #pragma unroll
-        for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, Fd[k][v] * dtsurdx * one * 0.125);
+        for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, flux(k, v) * dtsurdx * one * 0.125);
       }
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) A.Wn[v * N8 + gi] = Wout[v];
   }
-  if (st) atomicOr(A.status, st);
+  __syncthreads();
+  if (tid == 0) {
+    __threadfence();
+    atomicAdd(Bt.done + slot, 1u);
+  }
+}
+
+// Persistent launch over a work list of (level slot, tile) items.  All CTAs are
+// co-resident (grid <= occupancy x SMs) and take items in list order, so a
+// tile waiting for a finer level (listed first) never blocks the CTAs that
+// still have to finish that level.
+template <class M, int T, int SMAX, int HMAX, int BMAX>
+__global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 3)
+    level_batch_kernel(const BatchArgs Bt) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  if (Bt.gate != nullptr && *Bt.gate == 0) return;
+  unsigned st = 0;
+  for (int w = blockIdx.x; w < Bt.nwork; w += gridDim.x) {
+    const int item = Bt.work[w];
+    const int slot = item >> kWorkSlotShift, tile = item & ((1 << kWorkSlotShift) - 1);
+    level_tile<M, T, SMAX, HMAX, BMAX>(Bt, Bt.lv[slot], slot, tile, smem, st);
+    __syncthreads();
+  }
+  if (st) atomicOr(Bt.status, st);
 }
 
 }  // namespace emma

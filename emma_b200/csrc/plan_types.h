@@ -19,9 +19,9 @@ constexpr uint32_t key_make(uint32_t kind, uint32_t idx) { return (kind << 28) |
 // Kernel shape the plans are cut for: octs per tile, staged octs, directional
 // halo entries, boundary faces.
 constexpr int kTileOcts = 32;
-constexpr int kSMax = 144;
-constexpr int kHMax = 288;
-constexpr int kBMax = 160;
+constexpr int kSMax = 136;
+constexpr int kHMax = 256;
+constexpr int kBMax = 128;
 
 struct TileDesc {
   int oct0;       // first oct of the tile (level list index)
@@ -36,18 +36,21 @@ struct TileDesc {
   int pad[3];
 };
 
+// Arguments of one level, resident in device memory (one slot per level).
+// Schedule kernels update dt and the state buffers between launches, so a
+// captured CUDA graph can run a whole coarse step without the host.
 struct LevelArgs {
   int L;
   int noct;
-  const double *W;    // level state, planes d,u,v,w,p of 8*noct
-  double *Wn;         // next state (written)
-  const double *C;    // conserved corrections received from the finer level (may be null)
+  double *W;          // level state, planes d,u,v,w,p of 8*noct
+  double *Wn;         // next state (written by the level kernel)
+  double *C;          // conserved corrections received from the finer level
   const double *B;    // optional update base: planes d,u,v,w,p,E of the caller's fieldnew
                       // (drop-in mode); when null the base is W2U(W) + C
-  const double *Wc;   // level L-1 state (injected neighbours), may be null
+  const double *Wc;   // level L-1 state read for injected neighbours, may be null
   double *Cc;         // level L-1 corrections (fine->coarse), may be null
   long long nc8;      // plane stride of Wc/Cc
-  const double *Wf;   // level L+1 state (split-cell averaging), may be null
+  const double *Wf;   // level L+1 state for split-cell averaging, may be null
   long long nf8;      // plane stride of Wf
   const uint8_t *split;  // per oct bitmask of split cells
   const int *child;      // per cell: child oct index at L+1, -1 for a leaf
@@ -57,8 +60,25 @@ struct LevelArgs {
   const uint16_t *halo;
   const uint16_t *bface;
   double dt, dx;
-  unsigned *status;
   int ntiles;
+  int wait_slot;      // level whose tiles must all be updated before this level's
+                      // update phase starts (batched launches), -1 for none
+  long long leaf;     // leaf cells (cell-updates of one substep)
 };
+
+// A launch of the level kernel: a list of (level slot, tile) work items,
+// processed by a persistent grid in list order.
+struct BatchArgs {
+  LevelArgs *lv;        // device array of level slots
+  const int *work;      // (slot << 24) | tile
+  int nwork;
+  unsigned *done;       // per slot: tiles whose update phase has completed
+  const int *gate;      // launch does nothing unless *gate != 0 (null: always run)
+  unsigned *status;
+  long long wait_limit; // bounded spin on `done` before reporting a timeout
+};
+
+constexpr int kWorkSlotShift = 24;
+constexpr int kMaxLevels = 32;
 
 }  // namespace emma

@@ -1,0 +1,33 @@
+// schedule.h -- device state of the level schedule (see schedule.cu).
+#pragma once
+#include "plan_types.h"
+
+namespace emma {
+
+struct SchedState {
+  double tsim, dt_param, time_max, cfl;
+  double adt[kMaxLevels];               // the reference's adt array, index level-1
+  double dx[kMaxLevels];                // cell size per level
+  unsigned long long smax[kMaxLevels];  // max signal speed per level (bits of a non-negative double)
+  double dtacc[kMaxLevels];             // dt accumulated by the current Advance_level(L) call
+  double tloc[kMaxLevels];              // its local time
+  int is[kMaxLevels];                   // its iteration count
+  int active[kMaxLevels];               // gate of the current iteration of level L
+  long long updates;                    // cell-updates performed (leaf cells x substeps)
+  int lcoarse, lmax, nsub;
+  int gate_all;
+};
+
+__global__ void k_set_args(LevelArgs *lv, int slot, LevelArgs a);
+__global__ void k_bind_level(LevelArgs *lv, int L, int lcoarse, int lmax, double dt);
+__global__ void k_swap_level(LevelArgs *lv, int L, const int *gate);
+__global__ void k_clear(double *p, long long n, const int *gate);
+__global__ void k_batch_begin(SchedState *S, LevelArgs *lv, unsigned *done);
+__global__ void k_batch_end(SchedState *S, LevelArgs *lv);
+__global__ void k_sub_begin(SchedState *S, int L, int it);
+__global__ void k_sub_dt(SchedState *S, int L);
+__global__ void k_sub_prelaunch(SchedState *S, LevelArgs *lv, int L, int has_fine);
+__global__ void k_sub_end(SchedState *S, LevelArgs *lv, int L);
+__global__ void k_sub_final(SchedState *S);
+
+}  // namespace emma

@@ -12,21 +12,23 @@ import numpy as np
 from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
-def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0):
+def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True):
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
+    o.use_graph = 1 if use_graph else 0
     return o
 
 
 class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
-    def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0):
+    def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True):
         self.tree = tree
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
+        self.trans, self.cfl, self.use_graph = trans, cfl, use_graph
         L = lib()
-        o = options(precision, trans, cfl)
+        o = options(precision, trans, cfl, use_graph=use_graph)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
         check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
         L.emma_hydro_clear_status()
@@ -34,9 +36,19 @@ class ResidentHydro:
         self.adt = np.zeros(self.lmax)
         self.tsim = 0.0
 
-    def set_precision(self, precision, cfl=None):
-        o = options(precision, 0, cfl if cfl is not None else 0.85)
+    def set_precision(self, precision):
+        o = options(precision, self.trans, self.cfl, use_graph=self.use_graph)
         check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
+
+    def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):
+        """Queue one coarse step on the device schedule without waiting."""
+        check(lib().emma_hydro_advance_coarse_step_async(dt_param, time_max, nsub), "advance_coarse_step_async")
+
+    def time(self):
+        t = ctypes.c_double()
+        check(lib().emma_hydro_get_time(ctypes.byref(t), ptr(self.adt)), "get_time")
+        self.tsim = t.value
+        return self.tsim
 
     def noct(self, level):
         return lib().emma_hydro_level_noct(level)

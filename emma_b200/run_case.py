@@ -25,14 +25,21 @@ def main():
     r = ResidentHydro(tree, precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64, trans=cfg.trans,
                       cfl=cfg.cfl)
     L = lib()
-    L.emma_hydro_reset_counters()
+    per_step = []
+    tot_ms, tot_n, tot_cells = 0.0, 0, 0
     for _ in range(a.steps):
+        L.emma_hydro_reset_counters()
         r.coarse_step(nsub=cfg.nsub)
-    avg, n, cells = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
-    L.emma_hydro_kernel_timing(ctypes.byref(avg), ctypes.byref(n), ctypes.byref(cells))
-    print(json.dumps({"config": cfg.name, "precision": a.precision, "status": r.status(), "launches": n.value,
-                      "avg_launch_ms": avg.value, "cells_per_launch": cells.value / max(n.value, 1),
-                      "cell_updates_per_s_kernel": cells.value / (avg.value * n.value * 1e-3) if n.value else None}))
+        avg, n, cells = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
+        L.emma_hydro_kernel_timing(ctypes.byref(avg), ctypes.byref(n), ctypes.byref(cells))
+        per_step.append(round(avg.value * n.value, 4))
+        tot_ms += avg.value * n.value
+        tot_n += n.value
+        tot_cells += cells.value
+    print(json.dumps({"config": cfg.name, "precision": a.precision, "status": r.status(), "launches": tot_n,
+                      "avg_launch_ms": tot_ms / max(tot_n, 1), "cells_per_launch": tot_cells / max(tot_n, 1),
+                      "kernel_ms_per_step": per_step,
+                      "cell_updates_per_s_kernel": tot_cells / (tot_ms * 1e-3) if tot_ms else None}))
 
 
 if __name__ == "__main__":

@@ -61,6 +61,7 @@ struct EmmaHydroOptions {
   double cfl;           /* Courant number of the level time step (reference param.h: 0.85) */
   int tile_octs;        /* octs per CTA tile (0 = autotuned) */
   int device;           /* CUDA device ordinal */
+  int use_graph;        /* coarse steps as a captured CUDA graph with a device-side schedule */
 };
 void emma_hydro_default_options(struct EmmaHydroOptions *opt);
 
@@ -124,6 +125,12 @@ int emma_hydro_advance_level(int level, double dt);       /* [HydroSolver] */
  * entries, in/out) is the reference's per-level dt array; tsim is advanced. */
 int emma_hydro_advance_coarse_step(double dt_param, double time_max, int nsub,
                                    double *tsim, double *adt);
+/* The same, queued on the library's stream without waiting: time and dt stay
+ * on the device (start from the last values set or returned).  Read them with
+ * emma_hydro_get_time, which synchronises. */
+int emma_hydro_advance_coarse_step_async(double dt_param, double time_max, int nsub);
+int emma_hydro_get_time(double *tsim, double *adt);
+int emma_hydro_set_time(double tsim, const double *adt);
 
 /* SoA access for tests and I/O: 5 planes (d,u,v,w,p) of 8*noct doubles each, list order. */
 int emma_hydro_level_noct(int level);
