@@ -524,9 +524,14 @@ int emma_hydro_set_options(const struct EmmaHydroOptions *opt) {
   if (!g.ready) return emma_hydro_init(opt);
   const int old_trans = g.opt.trans_flags;
   g.opt = *opt;
-  if (g.res.valid && old_trans != opt->trans_flags) {
-    fail(EMMA_ST_ARG, "transmissive flags changed: upload the tree again");
-    return EMMA_ST_ARG;
+  if (old_trans != opt->trans_flags) {
+    // the tile plans encode the boundary ghosts: a resident tree must be uploaded again
+    cudaStreamSynchronize(g.stream);
+    drop_graph();
+    free_tree(g.res);
+    free_tree(g.drop);
+    g.drop_level = -1;
+    g.drop_first = nullptr;
   }
   return 0;
 }

@@ -22,8 +22,9 @@ def main():
            "sod": lambda: configs.sod(level=a.level), "sedov": configs.sedov, "cosmo": configs.cosmo,
            "amr": configs.small_amr}[a.config]()
     tree = cfg.build()
+    # host-driven schedule: every level-kernel launch is timed with CUDA events
     r = ResidentHydro(tree, precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64, trans=cfg.trans,
-                      cfl=cfg.cfl)
+                      cfl=cfg.cfl, use_graph=False)
     L = lib()
     per_step = []
     tot_ms, tot_n, tot_cells = 0.0, 0, 0
