@@ -123,6 +123,19 @@ def traffic_per_cell(config, precision):
     return d.get(f"{config}/{precision}")
 
 
+def graph_kernel_count(cfg, tree):
+    """Kernels of this library in one captured coarse step (CFL reductions,
+    schedule kernels, level-kernel launches)."""
+    levels = [l for l in range(cfg.lcoarse, cfg.lmax + 1) if tree.noct(l) > 0]
+    if cfg.nsub == 1 or len(levels) == 1:
+        return len(levels) + 3  # CFL per level, batch begin, level kernel, batch end
+    n, per = 0, 1
+    for _ in levels:
+        per *= cfg.nsub
+        n += per * 7  # begin, clear, CFL, dt, prelaunch, level kernel, end per gated iteration
+    return n + 1
+
+
 def run_mine(args, rank, world):
     import torch
     from emma_b200 import ResidentHydro, PREC_FP64, PREC_MIXED, lib
@@ -146,11 +159,14 @@ def run_mine(args, rank, world):
 
     results = {}
     for prec_name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
-        r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl)
+        # whole coarse steps: CUDA graph with the device-side level schedule
+        r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=True)
         init_states = {l: r.state(l) for l in levels}
-        for _ in range(args.warmup):
-            r.coarse_step(nsub=cfg.nsub)
+        r.coarse_step(nsub=cfg.nsub)  # builds and instantiates the graph
+        for _ in range(max(args.warmup - 1, 0)):
+            r.step_async(nsub=cfg.nsub)
         torch.cuda.synchronize()
+        r.time()
         if world > 1:
             torch.distributed.barrier()
         L.emma_hydro_reset_counters()
@@ -162,36 +178,48 @@ def run_mine(args, rank, world):
                     flush_buf.zero_()
                 a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
                 a.record(stream)
-                r.coarse_step(nsub=cfg.nsub)
+                r.step_async(nsub=cfg.nsub)
                 b.record(stream)
                 evs.append((a, b))
             torch.cuda.synchronize()
         ms = sum(a.elapsed_time(b) for a, b in evs)
         updates = L.emma_hydro_cell_updates()
-        launches = L.emma_hydro_kernel_launches()
+        status = r.status()
+        launches_per_step = graph_kernel_count(cfg, tree)
+        res = {"ms": ms, "updates": updates, "launches": launches_per_step * args.steps, "status": status,
+               "clocks": clk.summary()}
+        # level-kernel time per launch: the same steps on the host-driven schedule,
+        # each level-kernel launch timed with CUDA events on the library stream
+        r2 = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=False)
+        for _ in range(2):
+            r2.coarse_step(nsub=cfg.nsub)
+        L.emma_hydro_reset_counters()
+        for _ in range(min(args.steps, 5)):
+            if flush:
+                flush_buf.zero_()
+                torch.cuda.synchronize()
+            r2.coarse_step(nsub=cfg.nsub)
         kavg, kcnt, kcells = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
         L.emma_hydro_kernel_timing(ctypes.byref(kavg), ctypes.byref(kcnt), ctypes.byref(kcells))
-        status = r.status()
-        res = {"ms": ms, "updates": updates, "launches": launches, "kernel_avg_ms": kavg.value,
-               "kernel_launches": kcnt.value, "kernel_cells": kcells.value, "status": status,
-               "clocks": clk.summary()}
+        res.update(kernel_avg_ms=kavg.value, kernel_launches=kcnt.value, kernel_cells=kcells.value)
         # e2e through the C ABI with host buffers: H2D states, coarse step, D2H states
+        r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=True)
         pinned = {l: torch.from_numpy(init_states[l]).pin_memory() for l in levels}
         outs = {l: torch.empty_like(pinned[l]).pin_memory() for l in levels}
-        for l in levels:
-            r.set_state(l, init_states[l])
+        r.coarse_step(nsub=cfg.nsub)
         torch.cuda.synchronize()
         h2d = d2h = 0
         e2e_ms = 0.0
         for _ in range(args.steps):
             if flush:
                 flush_buf.zero_()
+            torch.cuda.synchronize()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             for l in levels:
                 L.emma_hydro_set_level_state(l, ctypes.c_void_p(pinned[l].data_ptr()))
                 h2d += pinned[l].numel() * 8
-            r.coarse_step(nsub=cfg.nsub)
+            r.step_async(nsub=cfg.nsub)
             for l in levels:
                 L.emma_hydro_get_level_state(l, ctypes.c_void_p(outs[l].data_ptr()))
                 d2h += outs[l].numel() * 8
@@ -201,9 +229,10 @@ def run_mine(args, rank, world):
         res["e2e_ms"] = e2e_ms
         res["h2d"] = h2d // max(args.steps, 1)
         res["d2h"] = d2h // max(args.steps, 1)
-        # state after `steps` coarse steps from the initial condition, for the L1 comparison
+        # state after a few coarse steps from the initial condition, for the L1 comparison
         for l in levels:
             r.set_state(l, init_states[l])
+        r.tsim = 0.0
         for _ in range(min(args.steps, 10)):
             r.coarse_step(nsub=cfg.nsub)
         res["final"] = {l: r.state(l) for l in levels}
