@@ -7,8 +7,10 @@
 //              reference to the last bit except where libm pow() differs from
 //              CUDA's pow() (TRRS branch and exact-solver fallback).
 //   MathF32 -- the mixed path's reconstruction, wave speeds and fluxes in FP32:
-//              the same algorithm with one reciprocal per density, fast
-//              division/square root and algebraic simplifications (d a^2 = gamma p).
+//              the same algorithm with one reciprocal per density, approximate
+//              (single-instruction) division, reciprocal and square root
+//              (level_f32.cu is built with -use_fast_math) and algebraic
+//              simplifications (d a^2 = gamma p).
 //
 // Primitive vectors are 5-wide: 0:d 1:u 2:v 3:w 4:p.  Face index k:
 // 0:-x 1:+x 2:-y 3:+y 4:-z 5:+z.
@@ -257,7 +259,8 @@ struct MathF32 {
   using R = float;
   static constexpr float G = 5.f / 3.f;
 
-  static __device__ __forceinline__ float rcp(float x) { return __frcp_rn(x); }
+  // approximate reciprocal / division (built with -use_fast_math: single MUFU ops)
+  static __device__ __forceinline__ float rcp(float x) { return __fdividef(1.f, x); }
   static __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
   static __device__ __forceinline__ float limit(float m, float p) {

@@ -31,6 +31,39 @@ __device__ __forceinline__ bool nei_inside(int c, int k) {
   return (k & 1) ? !(c & bit) : (c & bit);
 }
 
+// 4-wide shared-memory groups: one 128-bit access per group for FP32 (float4),
+// two for FP64 (double2 pairs).
+template <class R>
+struct Q4;
+template <>
+struct Q4<float> {
+  static __device__ __forceinline__ void st(float *b, int i, float x, float y, float z, float w) {
+    reinterpret_cast<float4 *>(b)[i] = make_float4(x, y, z, w);
+  }
+  static __device__ __forceinline__ void ld(const float *b, int i, float &x, float &y, float &z, float &w) {
+    const float4 v = reinterpret_cast<const float4 *>(b)[i];
+    x = v.x;
+    y = v.y;
+    z = v.z;
+    w = v.w;
+  }
+};
+template <>
+struct Q4<double> {
+  static __device__ __forceinline__ void st(double *b, int i, double x, double y, double z, double w) {
+    reinterpret_cast<double2 *>(b)[2 * i] = make_double2(x, y);
+    reinterpret_cast<double2 *>(b)[2 * i + 1] = make_double2(z, w);
+  }
+  static __device__ __forceinline__ void ld(const double *b, int i, double &x, double &y, double &z, double &w) {
+    const double2 a = reinterpret_cast<const double2 *>(b)[2 * i];
+    const double2 c = reinterpret_cast<const double2 *>(b)[2 * i + 1];
+    x = a.x;
+    y = a.y;
+    z = c.x;
+    w = c.y;
+  }
+};
+
 // mirror maps of the transmissive ghost octs (src/hydro_utils.c:2504-2610)
 __constant__ uint8_t c_mirror[6][8] = {
     {0, 0, 2, 2, 4, 4, 6, 6}, {1, 1, 3, 3, 5, 5, 7, 7}, {0, 1, 0, 1, 4, 5, 4, 5},
@@ -41,12 +74,15 @@ struct LevelSmem {
   using R = typename M::R;
   static constexpr int NT = 8 * T;  // tile cells = threads
   static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
-  static constexpr size_t off_W = 0;                                       // R [5][SMAX*8] staged states
-  static constexpr size_t off_M = a16(off_W + sizeof(R) * 5 * SMAX * 8);   // R [20][NT] slopes + predictor
-  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 20 * NT);       // R [7][HMAX] halo face states
-  static constexpr size_t off_F = a16(off_HS + sizeof(R) * 7 * HMAX);      // R [5][3*NT] -d face fluxes
-  static constexpr size_t off_FB = a16(off_F + sizeof(R) * 5 * 3 * NT);    // R [5][BMAX] boundary + faces
-  static constexpr size_t off_key = a16(off_FB + sizeof(R) * 5 * BMAX);    // u32 [SMAX]
+  static constexpr size_t off_W = 0;                                        // R4 [SMAX*8] (d,u,v,w)
+  static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * SMAX * 8);   // R  [SMAX*8] p
+  static constexpr size_t off_M = a16(off_Wp + sizeof(R) * SMAX * 8);       // R4 [5][NT] slopes + predictor
+  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 4 * 5 * NT);     // R4 [2][HMAX] halo face states
+  static constexpr size_t off_F = a16(off_HS + sizeof(R) * 4 * 2 * HMAX);   // R4 [3*NT] + R [3*NT] -d face fluxes
+  static constexpr size_t off_F4 = a16(off_F + sizeof(R) * 4 * 3 * NT);
+  static constexpr size_t off_FB = a16(off_F4 + sizeof(R) * 3 * NT);        // R4 [BMAX] + R [BMAX] boundary faces
+  static constexpr size_t off_FB4 = a16(off_FB + sizeof(R) * 4 * BMAX);
+  static constexpr size_t off_key = a16(off_FB4 + sizeof(R) * BMAX);       // u32 [SMAX]
   static constexpr size_t off_G = a16(off_key + sizeof(uint32_t) * SMAX);  // u8 [SMAX*6]
   static constexpr size_t off_hmap = a16(off_G + 6 * SMAX);               // u16 [SMAX*8] first halo entry
   static constexpr size_t off_halo = a16(off_hmap + 2 * SMAX * 8);        // u16 [HMAX] halo entries
@@ -62,11 +98,15 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   using R = typename M::R;
   using SM = LevelSmem<M, T, SMAX, HMAX, BMAX>;
   constexpr int NT = SM::NT;
+  using V = Q4<R>;
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
+  R *sWp = reinterpret_cast<R *>(smem + SM::off_Wp);
   R *sM = reinterpret_cast<R *>(smem + SM::off_M);
   R *sHS = reinterpret_cast<R *>(smem + SM::off_HS);
   R *sF = reinterpret_cast<R *>(smem + SM::off_F);
+  R *sF4 = reinterpret_cast<R *>(smem + SM::off_F4);
   R *sFB = reinterpret_cast<R *>(smem + SM::off_FB);
+  R *sFB4 = reinterpret_cast<R *>(smem + SM::off_FB4);
   uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key);
   uint8_t *sG = smem + SM::off_G;
   uint16_t *sHmap = reinterpret_cast<uint16_t *>(smem + SM::off_hmap);
@@ -129,11 +169,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
     const double v0 = __ldg(src + off), v1 = __ldg(src + stride + off), v2 = __ldg(src + 2 * stride + off);
     const double v3 = __ldg(src + 3 * stride + off), v4 = __ldg(src + 4 * stride + off);
-    sW[0 * SMAX * 8 + i] = (R)v0;
-    sW[1 * SMAX * 8 + i] = (R)v1;
-    sW[2 * SMAX * 8 + i] = (R)v2;
-    sW[3 * SMAX * 8 + i] = (R)v3;
-    sW[4 * SMAX * 8 + i] = (R)v4;
+    V::st(sW, i, (R)v0, (R)v1, (R)v2, (R)v3);
+    sWp[i] = (R)v4;
     sSp[i] = sp;
   }
   __syncthreads();
@@ -146,8 +183,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     return g == 255 ? -1 : g;
   };
   auto q_of = [&](int s, int c, R q[5]) {
-#pragma unroll
-    for (int v = 0; v < 5; v++) q[v] = sW[v * SMAX * 8 + s * 8 + c];
+    V::ld(sW, s * 8 + c, q[0], q[1], q[2], q[3]);
+    q[4] = sWp[s * 8 + c];
   };
   auto muscl_of = [&](int s, int c, R D[3][5], R Wt[5]) {
     R q0[5], qm[3][5], qp[3][5];
@@ -182,12 +219,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     R D[3][5], Wt[5];
     muscl_of(s, c, D, Wt);
     if (k < 0) {
+      // groups: D_x(d,u,v,w), D_y(..), D_z(..), Wt(d,u,v,w), (D_x.p, D_y.p, D_z.p, Wt.p)
 #pragma unroll
-      for (int dir = 0; dir < 3; dir++)
-#pragma unroll
-        for (int v = 0; v < 5; v++) sM[(dir * 5 + v) * NT + j] = D[dir][v];
-#pragma unroll
-      for (int v = 0; v < 5; v++) sM[(15 + v) * NT + j] = Wt[v];
+      for (int dir = 0; dir < 3; dir++) V::st(sM, dir * NT + j, D[dir][0], D[dir][1], D[dir][2], D[dir][3]);
+      V::st(sM, 3 * NT + j, Wt[0], Wt[1], Wt[2], Wt[3]);
+      V::st(sM, 4 * NT + j, D[0][4], D[1][4], D[2][4], Wt[4]);
     } else {
       R q0[5], Dax[5], W[7];
       q_of(s, c, q0);
@@ -196,8 +232,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       for (int v = 0; v < 5; v++) Dax[v] = (ax == 0) ? D[0][v] : ((ax == 1) ? D[1][v] : D[2][v]);
       M::face_ax(q0, Dax, Wt, k, W, st);
       const int h = j - n8;
-#pragma unroll
-      for (int v = 0; v < 7; v++) sHS[v * HMAX + h] = W[v];
+      V::st(sHS, h, W[0], W[1], W[2], W[3]);
+      V::st(sHS, HMAX + h, W[4], W[5], W[6], (R)0);
     }
   }
   __syncthreads();
@@ -207,11 +243,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     R q0[5], Dax[5], Wt[5];
     q_of(t >> 3, t & 7, q0);
     const int ax = k >> 1;
-#pragma unroll
-    for (int v = 0; v < 5; v++) {
-      Dax[v] = sM[(ax * 5 + v) * NT + t];
-      Wt[v] = sM[(15 + v) * NT + t];
-    }
+    R p0, p1, p2;
+    V::ld(sM, ax * NT + t, Dax[0], Dax[1], Dax[2], Dax[3]);
+    V::ld(sM, 3 * NT + t, Wt[0], Wt[1], Wt[2], Wt[3]);
+    V::ld(sM, 4 * NT + t, p0, p1, p2, Wt[4]);
+    Dax[4] = (ax == 0) ? p0 : ((ax == 1) ? p1 : p2);
     M::face_ax(q0, Dax, Wt, k, W, st);
   };
   // stored face state k of halo cell `cell` (s*8+c); false if absent
@@ -220,8 +256,9 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     if (h == 0xFFFF) return false;
     while (h < H && (sHalo[h] >> 3) == cell && (sHalo[h] & 7) != k) h++;
     if (h >= H || (sHalo[h] >> 3) != cell) return false;
-#pragma unroll
-    for (int v = 0; v < 7; v++) W[v] = sHS[v * HMAX + h];
+    R pad;
+    V::ld(sHS, h, W[0], W[1], W[2], W[3]);
+    V::ld(sHS, HMAX + h, W[4], W[5], W[6], pad);
     return true;
   };
 
@@ -262,11 +299,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
     if (plus) {
       const int b = f - 3 * n8;
-#pragma unroll
-      for (int v = 0; v < 5; v++) sFB[v * BMAX + b] = F[v];
+      V::st(sFB, b, F[0], F[1], F[2], F[3]);
+      sFB4[b] = F[4];
     } else {
-#pragma unroll
-      for (int v = 0; v < 5; v++) sF[v * 3 * NT + d * NT + t] = F[v];
+      V::st(sF, d * NT + t, F[0], F[1], F[2], F[3]);
+      sF4[d * NT + t] = F[4];
     }
   }
   __syncthreads();
@@ -318,13 +355,33 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     } else {
       const double dtsurdx = A.dt / A.dx;
       // flux of face k (0:-x 1:+x ...) of this cell, from the face tasks of P2
-      auto flux = [&](int k, int v) -> double {
+      auto flux_slot = [&](int k, const R *&b4, const R *&b1, int &idx) {
         const int d = k >> 1;
-        if (!(k & 1)) return (double)sF[v * 3 * NT + d * NT + tid];
+        b4 = sF;
+        b1 = sF4;
+        idx = d * NT + tid;
+        if (!(k & 1)) return;
         int c2;
         const int s2 = nb(o, c, k, c2);
-        if (s2 >= 0 && s2 < n) return (double)sF[v * 3 * NT + d * NT + s2 * 8 + c2];
-        return (double)sFB[v * BMAX + sBmap[tid * 3 + d]];
+        if (s2 >= 0 && s2 < n) {
+          idx = d * NT + s2 * 8 + c2;
+        } else {
+          b4 = sFB;
+          b1 = sFB4;
+          idx = sBmap[tid * 3 + d];
+        }
+      };
+      auto flux5 = [&](int k, double F[5]) {
+        const R *b4, *b1;
+        int idx;
+        flux_slot(k, b4, b1, idx);
+        R f0, f1, f2, f3;
+        V::ld(b4, idx, f0, f1, f2, f3);
+        F[0] = (double)f0;
+        F[1] = (double)f1;
+        F[2] = (double)f2;
+        F[3] = (double)f3;
+        F[4] = (double)b1[idx];
       };
       // updatefield (src/hydro_utils.c:3050-3082): dU = sum over faces -x,+x,-y,+y,-z,+z
       // of (+-F dt/dx), signs alternating from +
@@ -332,8 +389,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       double one = 1.;
 #pragma unroll
       for (int k = 0; k < 6; k++) {
+        double F[5];
+        flux5(k, F);
 #pragma unroll
-        for (int v = 0; v < 5; v++) dU[v] += flux(k, v) * dtsurdx * one;
+        for (int v = 0; v < 5; v++) dU[v] += F[v] * dtsurdx * one;
         one *= -1.;
       }
       double Ud, Udu, Udv, Udw, UE;
@@ -389,10 +448,18 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       // U2W (src/hydro_utils.c:35-64), pressure floor, E - Ekin recovery
       const double dl = (Ud == 0. ? 10. : Ud);
       Wout[0] = Ud;
-      Wout[1] = Udu / dl;
-      Wout[2] = Udv / dl;
-      Wout[3] = Udw / dl;
-      Wout[4] = (kGam - 1.) * (UE - ((Udu) * (Udu) + (Udv) * (Udv) + (Udw) * (Udw)) / (dl) * 0.5);
+      if constexpr (sizeof(R) == 8) {
+        Wout[1] = Udu / dl;
+        Wout[2] = Udv / dl;
+        Wout[3] = Udw / dl;
+        Wout[4] = (kGam - 1.) * (UE - ((Udu) * (Udu) + (Udv) * (Udv) + (Udw) * (Udw)) / (dl) * 0.5);
+      } else {
+        const double inv = 1. / dl;  // mixed path: one FP64 division per cell
+        Wout[1] = Udu * inv;
+        Wout[2] = Udv * inv;
+        Wout[3] = Udw * inv;
+        Wout[4] = (kGam - 1.) * (UE - (Udu * Udu + Udv * Udv + Udw * Udw) * inv * 0.5);
+      }
       Wout[4] = fmax(Wout[4], kPmin);
       if (isnan(Wout[1]) || isnan(Wout[4]) || isnan(Wout[0])) st |= kStNan;
 
@@ -406,8 +473,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         if ((key >> 28) != kKeyInj) continue;
         const long long cc = key & 0x0FFFFFFFu;
         const double one = (k & 1) ? 1. : -1.;
+        double F[5];
+        flux5(k, F);
 #pragma unroll
-        for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, flux(k, v) * dtsurdx * one * 0.125);
+        for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, F[v] * dtsurdx * one * 0.125);
       }
     }
 #pragma unroll
