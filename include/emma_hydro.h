@@ -152,6 +152,24 @@ int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cel
  * halo cells per tile, leaf cells.  Returns EMMA_ST_* bits of the planning. */
 int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int trans_flags, long long *stats5);
 
+/* Level time step computed without allocating any memory.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc: a solver whose
+ * device memory all belongs to a host code's pool, or a process that must not
+ * allocate after start-up.  `d_state` is a level state ALREADY on the current
+ * device, laid out like emma_hydro_get_level_state's (5 planes d,u,v,w,p of
+ * `ncells` doubles); *dt_out receives what emma_hydro_comptstep returns for
+ * that state at `level` with Courant number `cfl`.  Works on the current
+ * device and needs neither emma_hydro_init nor a resident tree.
+ * Scratch is a fixed 128 KiB array inside the library, held on every GPU that
+ * loads it until exit, so ncells is limited to 33554432 (EMMA_ST_ARG beyond).
+ * The first call on each device looks up the array's address (make it before
+ * any stream capture).  Calls overlapping on the GPU share the array and race.
+ * Runs on `stream` (a cudaStream_t, NULL = legacy default stream) and
+ * synchronises it.  Returns EMMA_ST_* bits of this call only (it does not
+ * touch emma_hydro_status). */
+int emma_hydro_level_dt_noalloc(const double *d_state, long long ncells, int level, double cfl,
+                                void *stream, double *dt_out);
+
 /* --------------------------------------------------- host tree utilities */
 /* Build an oct tree with the reference's construction order
  * (build_initial_grid src/amr.c:1507, L_refine_cells src/amr.c:286), for
