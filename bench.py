@@ -387,7 +387,7 @@ def main():
         "l1_vs_fp64": l1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": (tpc * cells_per_launch) if tpc else None,
-                     "kernel": "level_advance_kernel<MathF32>", "alg_bytes_per_cell": ALG_BYTES_PER_CELL,
+                     "kernel": "level_batch_kernel<MathF32>", "alg_bytes_per_cell": ALG_BYTES_PER_CELL,
                      "cells_per_launch": cells_per_launch, "avg_launch_ms": mixed["kernel_avg_ms"]},
         "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": mixed["h2d"],
                 "d2h_bytes_per_step": mixed["d2h"]},

@@ -37,9 +37,6 @@ struct DevLevel {
   int *child = nullptr;
   TileDesc *tiles = nullptr;
   uint32_t *keys = nullptr;
-  uint8_t *graph = nullptr;
-  uint16_t *halo = nullptr;
-  uint16_t *bface = nullptr;
   int *work = nullptr;  // (L << 24) | tile for every tile of the level
 };
 
@@ -165,9 +162,6 @@ void free_level(DevLevel &d) {
   cudaFree(d.child);
   cudaFree(d.tiles);
   cudaFree(d.keys);
-  cudaFree(d.graph);
-  cudaFree(d.halo);
-  cudaFree(d.bface);
   cudaFree(d.work);
   d = DevLevel();
 }
@@ -216,9 +210,6 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     if (!upload_vec(&d.child, h.child)) return false;
     if (!upload_vec(&d.tiles, h.tiles)) return false;
     if (!upload_vec(&d.keys, h.keys)) return false;
-    if (!upload_vec(&d.graph, h.graph)) return false;
-    if (!upload_vec(&d.halo, h.halo)) return false;
-    if (!upload_vec(&d.bface, h.bface)) return false;
     std::vector<int> work((size_t)d.ntiles);
     for (int i = 0; i < d.ntiles; i++) work[i] = (L << kWorkSlotShift) | i;
     if (!upload_vec(&d.work, work)) return false;
@@ -236,9 +227,6 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     a.child = d.child;
     a.tiles = d.tiles;
     a.keys = d.keys;
-    a.graph = d.graph;
-    a.halo = d.halo;
-    a.bface = d.bface;
     a.dx = std::pow(0.5, L);
     a.ntiles = d.ntiles;
     a.wait_slot = -1;
@@ -839,7 +827,8 @@ int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cel
 
 // Host-only planning diagnostics (no GPU needed): builds and validates the tile
 // plans of levels lcoarse..lmax and reports, per level, {octs, tiles, max staged
-// octs, max halo entries, leaf cells}.  Returns the status bits of the planning.
+// octs per tile, staged octs of all tiles, leaf cells}.  Returns the status bits
+// of the planning.
 int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int trans, long long *stats5) {
   HostTree H;
   std::string err;
@@ -851,9 +840,11 @@ int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int tran
   for (int L = lcoarse; L <= lmax; L++) {
     const HostLevel &h = H.lev[L];
     long long ms = 0, mh = 0;
-    for (const TileDesc &t : h.tiles) {
-      ms = std::max<long long>(ms, t.S);
-      mh = std::max<long long>(mh, t.H);
+    for (size_t t = 0; t < h.tiles.size(); t++) {
+      long long s = 0;
+      for (int i = 0; i < kSlots; i++) s += (h.keys[t * kSlots + i] != kKeyNone);
+      ms = std::max(ms, s);
+      mh += s;
     }
     long long *o = stats5 + 5 * (L - lcoarse);
     o[0] = h.noct;
@@ -934,7 +925,7 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   if (!ck(cudaMemcpyAsync(d.W0, g.pin, sizeof(double) * 5 * n8, cudaMemcpyHostToDevice, g.stream), "H2D W")) return 0;
   if (!ck(cudaMemcpyAsync(d.B, g.pin + 5 * n8, sizeof(double) * 6 * n8, cudaMemcpyHostToDevice, g.stream), "H2D B"))
     return 0;
-  const bool coarse = nc8 > 0 && !h.inj_cells.empty();
+  const bool coarse = nc8 > 0 && h.reads_coarse;
   if (coarse) {
     if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
     pack_level(hc, 0, g.pin);
@@ -958,9 +949,6 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   a.child = d.child;
   a.tiles = d.tiles;
   a.keys = d.keys;
-  a.graph = d.graph;
-  a.halo = d.halo;
-  a.bface = d.bface;
   a.dt = dtnew;
   a.dx = std::pow(0.5, level);
   a.ntiles = d.ntiles;

@@ -301,6 +301,18 @@ struct MathF32 {
     W[6] = sqrtf(G * W[4] * W[5]);
   }
 
+  // Face state toward face k from the predicted centre state X = W0 + Wt.
+  static __device__ __forceinline__ void face_px(const float X[5], const float Dax[5], int k, float W[7],
+                                                 unsigned &st) {
+    const float s = (k & 1) ? 0.5f : -0.5f;
+#pragma unroll
+    for (int i = 0; i < 5; i++) W[i] = __fmaf_rn(s, Dax[i], X[i]);  // explicit: same rounding at every call site
+    W[4] = fmaxf(W[4], (float)kPmin);
+    if (W[0] < 0.f) st |= kStNegDensity;
+    W[5] = rcp(W[0]);
+    W[6] = sqrtf(G * W[4] * W[5]);
+  }
+
   static __device__ __noinline__ float pstar_exact(float dL, float uL, float pL, float aL, float dR, float uR,
                                                    float pR, float aR, float *u) {
     // Newton iteration on the exact two-rarefaction/shock function (Toro sec. 4.3)

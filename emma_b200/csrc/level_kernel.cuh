@@ -1,22 +1,21 @@
 // level_kernel.cuh -- the hydro level advance on the GPU, one CTA per tile.
 //
-// A tile is a run of up to T consecutive octs of one level (list order, which
-// is spatially clustered: Morton order on complete levels).  Each CTA:
-//   P0  stages into shared memory every oct the tile's MUSCL stencils touch:
-//       the tile octs, their 6 face and 12 edge neighbours at the same level
-//       ("virtual octs": a real oct, a coarser leaf cell injected into 8 cells
-//       as the reference's gather does, or a transmissive mirror ghost), with
-//       the neighbour graph between staged octs (precomputed per tile);
-//   P1  MUSCL-Hancock once per needed cell: slopes + predictor of every tile
-//       cell (kept in shared memory), and for every halo entry (a cell outside
-//       the tile face-adjacent to it) the one face state it contributes;
-//   P2  one HLLC solve per face, as an axis-major task list spread evenly over
-//       the CTA: task (axis d, tile cell t) is the -d face of t; then the +d
-//       faces on the tile's + boundary;
-//   P3  per tile cell: the six face fluxes summed in the reference's order
-//       (-x,+x,-y,+y,-z,+z), conserved update, primitive recovery, floors;
-//       split cells get the primitive mean of their children; faces bordering
-//       a coarser leaf add the fine->coarse correction (atomics, x 1/8).
+// A tile is a brick of 4x4x2 oct positions of one level (8x8x4 cells, one
+// thread per cell) holding at least one oct of the level.  Each CTA:
+//   P0  stages a 6x6x4-slot box (the brick and a ring of one oct) of "virtual
+//       octs": a real oct of the level, a coarser leaf cell injected into 8
+//       cells as the reference's gather does, or a transmissive mirror ghost;
+//       only the slots a stencil reads (faces and edges of the tile octs) are
+//       filled.  Neighbours are then fixed offsets in the 12x12x8-cell box;
+//   P1  MUSCL-Hancock once per needed cell: slopes + predictor of every brick
+//       cell that is a leaf of the tile or borders one, and for every ring cell
+//       face-adjacent to the brick the one face state it contributes;
+//   P2  one HLLC solve per face: three rounds (the -x, -y, -z face of every
+//       brick cell), then the + faces on the brick boundary;
+//   P3  per leaf of the tile: the six face fluxes summed in the reference's
+//       order (-x,+x,-y,+y,-z,+z), conserved update, primitive recovery,
+//       floors; split cells get the primitive mean of their children; faces
+//       bordering a coarser leaf add the fine->coarse correction (atomics, x 1/8).
 // The reference does the same per oct on a 27-oct copy, recomputing each
 // cell's reconstruction up to 9 times and each face twice
 // (src/hydro_utils.c:1407-2238, 2973-3303).
@@ -25,11 +24,6 @@
 #include "plan_types.h"
 
 namespace emma {
-
-__device__ __forceinline__ bool nei_inside(int c, int k) {
-  const int bit = 1 << (k >> 1);
-  return (k & 1) ? !(c & bit) : (c & bit);
-}
 
 // 4-wide shared-memory groups: one 128-bit access per group for FP32 (float4),
 // two for FP64 (double2 pairs).
@@ -69,90 +63,108 @@ __constant__ uint8_t c_mirror[6][8] = {
     {0, 0, 2, 2, 4, 4, 6, 6}, {1, 1, 3, 3, 5, 5, 7, 7}, {0, 1, 0, 1, 4, 5, 4, 5},
     {2, 3, 2, 3, 7, 6, 6, 7}, {0, 1, 2, 3, 0, 1, 2, 3}, {4, 5, 6, 7, 4, 5, 6, 7}};
 
-template <class M, int T, int SMAX, int HMAX, int BMAX>
-struct LevelSmem {
+// cell flags of the staged box
+constexpr uint8_t kFPresent = 1, kFSplit = 2, kFTile = 4, kFInj = 8;
+__device__ __forceinline__ bool f_ok(uint8_t f) { return (f & (kFPresent | kFSplit)) == kFPresent; }
+__device__ __forceinline__ bool f_tileleaf(uint8_t f) {
+  return (f & (kFPresent | kFSplit | kFTile)) == (kFPresent | kFTile);
+}
+
+// Shared memory of one brick.  Brick cell t = x + 8 (y + 8 z) sits at box cell
+// (x+2) + 12 ((y+2) + 12 (z+2)).  Ring cell j (face-adjacent to the brick):
+// j < 32 -x side (y + 8 z), 32.. +x side, 64.. -y (x + 8 z), 96.. +y,
+// 128.. -z (x + 8 y), 192.. +z.  Face arrays, -d face of brick cell (x,y,z):
+// x: x + 9 (y + 8 z), y: 288 + x + 8 (y + 9 z), z: 576 + x + 8 (y + 8 z),
+// with coordinate 8 (x, y) or 4 (z) for the + faces on the brick boundary.
+template <class M>
+struct BrickSmem {
   using R = typename M::R;
-  static constexpr int NT = 8 * T;  // tile cells = threads
+  static constexpr bool kF64 = sizeof(R) == 8;
   static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
-  static constexpr size_t off_W = 0;                                        // R4 [SMAX*8] (d,u,v,w)
-  static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * SMAX * 8);   // R  [SMAX*8] p
-  static constexpr size_t off_M = a16(off_Wp + sizeof(R) * SMAX * 8);       // R4 [5][NT] slopes + predictor
-  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 4 * 5 * NT);     // R4 [2][HMAX] halo face states
-  static constexpr size_t off_F = a16(off_HS + sizeof(R) * 4 * 2 * HMAX);   // R4 [3*NT] + R [3*NT] -d face fluxes
-  static constexpr size_t off_F4 = a16(off_F + sizeof(R) * 4 * 3 * NT);
-  static constexpr size_t off_FB = a16(off_F4 + sizeof(R) * 3 * NT);        // R4 [BMAX] + R [BMAX] boundary faces
-  static constexpr size_t off_FB4 = a16(off_FB + sizeof(R) * 4 * BMAX);
-  static constexpr size_t off_key = a16(off_FB4 + sizeof(R) * BMAX);       // u32 [SMAX]
-  static constexpr size_t off_G = a16(off_key + sizeof(uint32_t) * SMAX);  // u8 [SMAX*6]
-  static constexpr size_t off_hmap = a16(off_G + 6 * SMAX);               // u16 [SMAX*8] first halo entry
-  static constexpr size_t off_halo = a16(off_hmap + 2 * SMAX * 8);        // u16 [HMAX] halo entries
-  static constexpr size_t off_bface = a16(off_halo + 2 * HMAX);           // u16 [BMAX] boundary faces
-  static constexpr size_t off_bmap = a16(off_bface + 2 * BMAX);           // u16 [3*NT] (cell,axis) -> face
-  static constexpr size_t off_sp = a16(off_bmap + 2 * 3 * NT);            // u8 [SMAX*8] split flags
-  static constexpr size_t bytes = a16(off_sp + SMAX * 8);
+  static constexpr size_t off_key = 0;                                           // u32 [kSlots]
+  static constexpr size_t off_st = a16(off_key + 4 * kSlots);                    // u8  [kBox] cell flags
+  static constexpr size_t off_W = a16(off_st + kBox);                            // R4  [kBox] (d,u,v,w)
+  static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * kBox);            // R   [kBox] p
+  static constexpr size_t off_M = a16(off_Wp + sizeof(R) * kBox);                // R4  [5][kNT] slopes, predictor
+  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 4 * 5 * kNT);         // R4  [2][kHaloCells] ring faces
+  static constexpr size_t off_Q = a16(off_HS + sizeof(R) * 4 * 2 * kHaloCells);  // f64 [5][kNT] (FP32 path)
+  static constexpr size_t q_bytes = kF64 ? 0 : sizeof(double) * 5 * kNT;
+  // face fluxes: the FP32 path reuses the staged box, dead after reconstruction
+  static constexpr size_t off_F = kF64 ? a16(off_Q + q_bytes) : off_W;  // R4 [kFaces]
+  static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * kFaces);  // R  [kFaces]
+  static constexpr size_t bytes = kF64 ? a16(off_F1 + sizeof(R) * kFaces) : a16(off_Q + q_bytes);
+  static_assert(kF64 || off_F1 + sizeof(R) * kFaces <= off_M, "FP32 face fluxes must fit in the staged box");
 };
 
-template <class M, int T, int SMAX, int HMAX, int BMAX>
+__device__ __forceinline__ int box_of(int x, int y, int z) { return (x + 2) + kBoxX * ((y + 2) + kBoxY * (z + 2)); }
+
+// ring cell j: box cell, its face k toward the brick and the brick cell across it
+__device__ __forceinline__ void ring_cell(int j, int &b, int &k, int &bin) {
+  if (j < 64) {
+    const int side = j >> 5, y = j & 7, z = (j >> 3) & 3;
+    b = (side ? 10 : 1) + kBoxX * ((y + 2) + kBoxY * (z + 2));
+    k = side ? 0 : 1;
+    bin = b + (side ? -1 : 1);
+  } else if (j < 128) {
+    const int i = j - 64, side = i >> 5, x = i & 7, z = (i >> 3) & 3;
+    b = (x + 2) + kBoxX * ((side ? 10 : 1) + kBoxY * (z + 2));
+    k = side ? 2 : 3;
+    bin = b + (side ? -kBoxX : kBoxX);
+  } else {
+    const int i = j - 128, side = i >> 6, x = i & 7, y = (i >> 3) & 7;
+    b = (x + 2) + kBoxX * ((y + 2) + kBoxY * (side ? 6 : 1));
+    k = side ? 4 : 5;
+    bin = b + (side ? -kBoxX * kBoxY : kBoxX * kBoxY);
+  }
+}
+
+template <class M>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs &A, const int slot, const int tile,
                                            unsigned char *smem, unsigned &st) {
   using R = typename M::R;
-  using SM = LevelSmem<M, T, SMAX, HMAX, BMAX>;
-  constexpr int NT = SM::NT;
+  using SM = BrickSmem<M>;
+  constexpr bool F64 = SM::kF64;
   using V = Q4<R>;
+  uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key);
+  uint8_t *sSt = smem + SM::off_st;
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
   R *sWp = reinterpret_cast<R *>(smem + SM::off_Wp);
   R *sM = reinterpret_cast<R *>(smem + SM::off_M);
   R *sHS = reinterpret_cast<R *>(smem + SM::off_HS);
+  double *sQ = reinterpret_cast<double *>(smem + SM::off_Q);
   R *sF = reinterpret_cast<R *>(smem + SM::off_F);
-  R *sF4 = reinterpret_cast<R *>(smem + SM::off_F4);
-  R *sFB = reinterpret_cast<R *>(smem + SM::off_FB);
-  R *sFB4 = reinterpret_cast<R *>(smem + SM::off_FB4);
-  uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key);
-  uint8_t *sG = smem + SM::off_G;
-  uint16_t *sHmap = reinterpret_cast<uint16_t *>(smem + SM::off_hmap);
-  uint16_t *sHalo = reinterpret_cast<uint16_t *>(smem + SM::off_halo);
-  uint16_t *sBface = reinterpret_cast<uint16_t *>(smem + SM::off_bface);
-  uint16_t *sBmap = reinterpret_cast<uint16_t *>(smem + SM::off_bmap);
-  uint8_t *sSp = smem + SM::off_sp;
+  R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
 
   const int tid = threadIdx.x;
-  const TileDesc td = A.tiles[tile];
-  const int n = td.noct, S = td.S, H = td.H, B = td.B;
-  const int n8 = 8 * n;
+  const uint32_t mask = A.tiles[tile].mask;
   const long long N8 = 8LL * A.noct;
-  if (S > SMAX || H > HMAX || B > BMAX || n > T || n < 1) {  // plan cut for another kernel shape
-    st |= kStTree;
-    if (tid == 0) atomicAdd(Bt.done + slot, 1u);  // keep batched waits bounded
-    return;
-  }
+  const int tx = tid & 7, ty = (tid >> 3) & 7, tz = tid >> 6;
+  const int tb = box_of(tx, ty, tz);
 
   // ------------------------------------------------------------------ P0
-  for (int i = tid; i < S; i += NT) sKey[i] = A.keys[td.keys_off + i];
-  for (int i = tid; i < S * 6; i += NT) sG[i] = A.graph[td.graph_off + i];
-  for (int i = tid; i < S * 8; i += NT) sHmap[i] = 0xFFFF;
-  for (int i = tid; i < H; i += NT) sHalo[i] = A.halo[td.halo_off + i];
-  for (int i = tid; i < B; i += NT) sBface[i] = A.bface[td.bface_off + i];
+  for (int i = tid; i < kSlots; i += kNT) sKey[i] = A.keys[(size_t)tile * kSlots + i];
   __syncthreads();
-  for (int h = tid; h < H; h += NT) {
-    const int cell = sHalo[h] >> 3;
-    if (h == 0 || (sHalo[h - 1] >> 3) != cell) sHmap[cell] = (uint16_t)h;
-  }
-  for (int b = tid; b < B; b += NT) {
-    const int e = sBface[b];
-    sBmap[(e >> 2) * 3 + (e & 3)] = (uint16_t)b;
-  }
-#pragma unroll 4
-  for (int i = tid; i < S * 8; i += NT) {
+#pragma unroll 2
+  for (int i = tid; i < kBox; i += kNT) {
     const int s = i >> 3, c = i & 7;
+    const int sz = s / (kSlotX * kSlotY), r = s - (kSlotX * kSlotY) * sz, sy = r / kSlotX, sx = r - kSlotX * sy;
+    const int b = (2 * sx + (c & 1)) + kBoxX * ((2 * sy + ((c >> 1) & 1)) + kBoxY * (2 * sz + (c >> 2)));
     const uint32_t key = sKey[s];
+    if (key == kKeyNone) {
+      sSt[b] = 0;
+      continue;
+    }
     const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
     const double *src = A.W;
     long long stride = N8, off;
-    uint8_t sp = 0;
+    uint8_t f = kFPresent;
     if (kind == kKeyReal) {
       off = 8LL * idx + c;
-      sp = (A.split[idx] >> c) & 1;
+      if ((A.split[idx] >> c) & 1) f |= kFSplit;
+      const unsigned ux = sx - 1, uy = sy - 1, uz = sz - 1;
+      if (ux < 4u && uy < 4u && uz < 2u && ((mask >> (ux + 4 * uy + 16 * uz)) & 1)) f |= kFTile;
     } else if (kind == kKeyInj) {
+      f |= kFInj;
       src = A.Wc;
       stride = A.nc8;
       off = idx;
@@ -165,146 +177,152 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     } else {
       const int mc = c_mirror[kind - kKeyGhost0][c];
       off = 8LL * idx + mc;
-      sp = (A.split[idx] >> mc) & 1;
+      if ((A.split[idx] >> mc) & 1) f |= kFSplit;
     }
     const double v0 = __ldg(src + off), v1 = __ldg(src + stride + off), v2 = __ldg(src + 2 * stride + off);
     const double v3 = __ldg(src + 3 * stride + off), v4 = __ldg(src + 4 * stride + off);
-    V::st(sW, i, (R)v0, (R)v1, (R)v2, (R)v3);
-    sWp[i] = (R)v4;
-    sSp[i] = sp;
+    V::st(sW, b, (R)v0, (R)v1, (R)v2, (R)v3);
+    sWp[b] = (R)v4;
+    sSt[b] = f;
+    if constexpr (!F64) {
+      if (f & kFTile) {
+        const int t = (b % kBoxX - 2) + 8 * ((b / kBoxX) % kBoxY - 2) + 64 * (b / (kBoxX * kBoxY) - 2);
+        sQ[t] = v0;
+        sQ[kNT + t] = v1;
+        sQ[2 * kNT + t] = v2;
+        sQ[3 * kNT + t] = v3;
+        sQ[4 * kNT + t] = v4;
+      }
+    }
   }
   __syncthreads();
 
-  // staged-cell neighbour across face k (same oct or via the graph); -1 if absent
-  auto nb = [&](int s, int c, int k, int &c2) -> int {
-    c2 = c ^ (1 << (k >> 1));
-    if (nei_inside(c, k)) return s;
-    const int g = sG[s * 6 + k];
-    return g == 255 ? -1 : g;
-  };
-  auto q_of = [&](int s, int c, R q[5]) {
-    V::ld(sW, s * 8 + c, q[0], q[1], q[2], q[3]);
-    q[4] = sWp[s * 8 + c];
-  };
-  auto muscl_of = [&](int s, int c, R D[3][5], R Wt[5]) {
-    R q0[5], qm[3][5], qp[3][5];
-    q_of(s, c, q0);
-#pragma unroll
-    for (int dir = 0; dir < 3; dir++) {
-      int c2;
-      int s2 = nb(s, c, 2 * dir, c2);
-      if (s2 < 0) { st |= kStTree; s2 = s; c2 = c; }
-      q_of(s2, c2, qm[dir]);
-      s2 = nb(s, c, 2 * dir + 1, c2);
-      if (s2 < 0) { st |= kStTree; s2 = s; c2 = c; }
-      q_of(s2, c2, qp[dir]);
-    }
-    if constexpr (sizeof(R) == 8) M::muscl(q0, qm, qp, A.dt, A.dx, D, Wt);
-    else M::muscl(q0, qm, qp, (R)(A.dt / A.dx * 0.5), D, Wt);
+  auto q_at = [&](int b, R q[5]) {
+    V::ld(sW, b, q[0], q[1], q[2], q[3]);
+    q[4] = sWp[b];
   };
 
   // ------------------------------------------------------------------ P1
-  for (int j = tid; j < n8 + H; j += NT) {
-    int s, c, k = -1;
-    if (j < n8) {
-      s = j >> 3;
-      c = j & 7;
+  // Pass 0: brick cell tid (slopes and predictor, when it is a leaf of the tile
+  // or borders one); pass 1: ring cell tid (the one face state it contributes).
+  // One call site each for the reconstruction and the face state, so that a
+  // face on a brick boundary, solved by both bricks, rounds the same in both.
+#pragma unroll 1
+  for (int pass = 0; pass < 2; pass++) {
+    int b = tb, k = 0, bin = tb;
+    bool need;
+    if (pass == 0) {
+      const uint8_t f = sSt[tb];
+      need = f_tileleaf(f);
+      if (!need && f_ok(f))
+        need = f_tileleaf(sSt[tb - 1]) || f_tileleaf(sSt[tb + 1]) || f_tileleaf(sSt[tb - kBoxX]) ||
+               f_tileleaf(sSt[tb + kBoxX]) || f_tileleaf(sSt[tb - kBoxX * kBoxY]) ||
+               f_tileleaf(sSt[tb + kBoxX * kBoxY]);
     } else {
-      const int e = sHalo[j - n8];
-      s = e >> 6;
-      c = (e >> 3) & 7;
-      k = e & 7;
+      ring_cell(tid, b, k, bin);
+      need = f_ok(sSt[b]) && f_tileleaf(sSt[bin]);
     }
-    if (sSp[s * 8 + c]) continue;  // split cells carry no flux: no reconstruction
-    R D[3][5], Wt[5];
-    muscl_of(s, c, D, Wt);
-    if (k < 0) {
-      // groups: D_x(d,u,v,w), D_y(..), D_z(..), Wt(d,u,v,w), (D_x.p, D_y.p, D_z.p, Wt.p)
+    if (!need) continue;
+    R q0[5], qm[3][5], qp[3][5], D[3][5], Wt[5], X[5];
+    q_at(b, q0);
+    q_at(b - 1, qm[0]);
+    q_at(b + 1, qp[0]);
+    q_at(b - kBoxX, qm[1]);
+    q_at(b + kBoxX, qp[1]);
+    q_at(b - kBoxX * kBoxY, qm[2]);
+    q_at(b + kBoxX * kBoxY, qp[2]);
+    if constexpr (F64) M::muscl(q0, qm, qp, A.dt, A.dx, D, Wt);
+    else M::muscl(q0, qm, qp, (R)(A.dt / A.dx * 0.5), D, Wt);
+    // X = W0 + Wt (FP32 path) or Wt (FP64 path, which adds W0 in the reference's order)
 #pragma unroll
-      for (int dir = 0; dir < 3; dir++) V::st(sM, dir * NT + j, D[dir][0], D[dir][1], D[dir][2], D[dir][3]);
-      V::st(sM, 3 * NT + j, Wt[0], Wt[1], Wt[2], Wt[3]);
-      V::st(sM, 4 * NT + j, D[0][4], D[1][4], D[2][4], Wt[4]);
+    for (int v = 0; v < 5; v++) X[v] = F64 ? Wt[v] : q0[v] + Wt[v];
+    if (pass == 0) {
+      // groups: D_x(d,u,v,w), D_y, D_z, X(d,u,v,w), (D_x.p, D_y.p, D_z.p, X.p)
+#pragma unroll
+      for (int dir = 0; dir < 3; dir++) V::st(sM, dir * kNT + tid, D[dir][0], D[dir][1], D[dir][2], D[dir][3]);
+      V::st(sM, 3 * kNT + tid, X[0], X[1], X[2], X[3]);
+      V::st(sM, 4 * kNT + tid, D[0][4], D[1][4], D[2][4], X[4]);
     } else {
-      R q0[5], Dax[5], W[7];
-      q_of(s, c, q0);
       const int ax = k >> 1;
+      R Dax[5], W[7];
 #pragma unroll
       for (int v = 0; v < 5; v++) Dax[v] = (ax == 0) ? D[0][v] : ((ax == 1) ? D[1][v] : D[2][v]);
-      M::face_ax(q0, Dax, Wt, k, W, st);
-      const int h = j - n8;
-      V::st(sHS, h, W[0], W[1], W[2], W[3]);
-      V::st(sHS, HMAX + h, W[4], W[5], W[6], (R)0);
+      if constexpr (F64) M::face_ax(q0, Dax, Wt, k, W, st);
+      else M::face_px(X, Dax, k, W, st);
+      V::st(sHS, tid, W[0], W[1], W[2], W[3]);
+      V::st(sHS, kHaloCells + tid, W[4], W[5], W[6], (R)0);
     }
   }
   __syncthreads();
 
-  // face state k of tile cell t from its slopes and predictor
-  auto tile_face = [&](int t, int k, R W[7]) {
-    R q0[5], Dax[5], Wt[5];
-    q_of(t >> 3, t & 7, q0);
+  // face state k of brick cell t (box cell b) from its slopes and predictor
+  auto brick_face = [&](int t, int b, int k, R W[7]) {
     const int ax = k >> 1;
-    R p0, p1, p2;
-    V::ld(sM, ax * NT + t, Dax[0], Dax[1], Dax[2], Dax[3]);
-    V::ld(sM, 3 * NT + t, Wt[0], Wt[1], Wt[2], Wt[3]);
-    V::ld(sM, 4 * NT + t, p0, p1, p2, Wt[4]);
+    R Dax[5], X[5], p0, p1, p2;
+    V::ld(sM, ax * kNT + t, Dax[0], Dax[1], Dax[2], Dax[3]);
+    V::ld(sM, 3 * kNT + t, X[0], X[1], X[2], X[3]);
+    V::ld(sM, 4 * kNT + t, p0, p1, p2, X[4]);
     Dax[4] = (ax == 0) ? p0 : ((ax == 1) ? p1 : p2);
-    M::face_ax(q0, Dax, Wt, k, W, st);
+    if constexpr (F64) {
+      R q0[5];
+      q_at(b, q0);
+      M::face_ax(q0, Dax, X, k, W, st);
+    } else {
+      M::face_px(X, Dax, k, W, st);
+    }
   };
-  // stored face state k of halo cell `cell` (s*8+c); false if absent
-  auto halo_face = [&](int cell, int k, R W[7]) -> bool {
-    int h = sHmap[cell];
-    if (h == 0xFFFF) return false;
-    while (h < H && (sHalo[h] >> 3) == cell && (sHalo[h] & 7) != k) h++;
-    if (h >= H || (sHalo[h] >> 3) != cell) return false;
+  auto ring_face = [&](int j, R W[7]) {
     R pad;
-    V::ld(sHS, h, W[0], W[1], W[2], W[3]);
-    V::ld(sHS, HMAX + h, W[4], W[5], W[6], pad);
-    return true;
+    V::ld(sHS, j, W[0], W[1], W[2], W[3]);
+    V::ld(sHS, kHaloCells + j, W[4], W[5], W[6], pad);
   };
 
   // ------------------------------------------------------------------ P2
-  for (int f = tid; f < 3 * n8 + B; f += NT) {
-    int t, d;
-    bool plus;
-    if (f < 3 * n8) {
-      d = f / n8;
-      t = f - d * n8;
-      plus = false;
+  // Rounds 0..2: the -d face of every brick cell; round 3 (threads < 128): the
+  // + faces on the brick boundary.  One HLLC call site for all rounds.
+#pragma unroll 1
+  for (int r = 0; r < 4; r++) {
+    if (r == 3 && tid >= 128) break;
+    int d, e, tL, bL, jL = -1, tR, bR, jR = -1;
+    if (r < 3) {
+      d = r;
+      const int bs = (d == 0) ? 1 : ((d == 1) ? kBoxX : kBoxX * kBoxY);
+      const int ts = (d == 0) ? 1 : ((d == 1) ? 8 : 64);
+      const int coord = (d == 0) ? tx : ((d == 1) ? ty : tz);
+      e = (d == 0) ? (tx + 9 * (ty + 8 * tz)) : ((d == 1) ? (kFacesX + tx + 8 * (ty + 9 * tz)) : (kFacesX + kFacesY + tid));
+      tR = tid;
+      bR = tb;
+      tL = tid - ts;
+      bL = tb - bs;
+      if (coord == 0) jL = (d == 0) ? (ty + 8 * tz) : ((d == 1) ? (64 + tx + 8 * tz) : (128 + tx + 8 * ty));
     } else {
-      const int e = sBface[f - 3 * n8];
-      t = e >> 2;
-      d = e & 3;
-      plus = true;
-    }
-    const int o = t >> 3, c = t & 7;
-    const int k = 2 * d + (plus ? 1 : 0);
-    R F[5] = {0, 0, 0, 0, 0};
-    int c2;
-    const int s2 = nb(o, c, k, c2);
-    if (s2 < 0) {
-      st |= kStTree;
-    } else if (!sSp[t] && !sSp[s2 * 8 + c2]) {
-      R Wa[7], Wb[7];  // a: this cell's state at the face, b: the neighbour's
-      tile_face(t, k, Wa);
-      bool ok = true;
-      if (s2 < n) tile_face(s2 * 8 + c2, k ^ 1, Wb);
-      else ok = halo_face(s2 * 8 + c2, k ^ 1, Wb);
-      if (!ok) {
-        st |= kStTree;
-      } else if (plus) {
-        M::hllc(Wa, Wb, d, F, st);
+      int x, y, z;
+      if (tid < 32) {
+        d = 0; x = 7; y = tid & 7; z = tid >> 3; jR = 32 + tid; e = 8 + 9 * (y + 8 * z);
+      } else if (tid < 64) {
+        d = 1; x = tid & 7; y = 7; z = (tid - 32) >> 3; jR = 96 + (tid - 32); e = kFacesX + x + 8 * (8 + 9 * z);
       } else {
-        M::hllc(Wb, Wa, d, F, st);
+        d = 2; x = tid & 7; y = (tid - 64) >> 3; z = 3; jR = 192 + (tid - 64);
+        e = kFacesX + kFacesY + x + 8 * (y + 32);
       }
+      const int bs = (d == 0) ? 1 : ((d == 1) ? kBoxX : kBoxX * kBoxY);
+      tL = x + 8 * (y + 8 * z);
+      bL = box_of(x, y, z);
+      tR = tL;
+      bR = bL + bs;
     }
-    if (plus) {
-      const int b = f - 3 * n8;
-      V::st(sFB, b, F[0], F[1], F[2], F[3]);
-      sFB4[b] = F[4];
-    } else {
-      V::st(sF, d * NT + t, F[0], F[1], F[2], F[3]);
-      sF4[d * NT + t] = F[4];
+    const uint8_t fL = sSt[bL], fR = sSt[bR];
+    R F[5] = {0, 0, 0, 0, 0};
+    if ((f_tileleaf(fL) || f_tileleaf(fR)) && f_ok(fL) && f_ok(fR)) {
+      R WL[7], WR[7];
+      if (jL >= 0) ring_face(jL, WL);
+      else brick_face(tL, bL, 2 * d + 1, WL);
+      if (jR >= 0) ring_face(jR, WR);
+      else brick_face(tR, bR, 2 * d, WR);
+      M::hllc(WL, WR, d, F, st);
     }
+    V::st(sF, e, F[0], F[1], F[2], F[3]);
+    sF1[e] = F[4];
   }
   __syncthreads();
 
@@ -326,14 +344,21 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
     __syncthreads();
   }
-  if (tid < n8) {
-    const int o = tid >> 3, c = tid & 7;
-    const long long gi = 8LL * (td.oct0 + o) + c;
+  const uint8_t fme = sSt[tb];
+  if (fme & kFTile) {
+    const int s = ((tx + 2) >> 1) + kSlotX * (((ty + 2) >> 1) + kSlotY * ((tz + 2) >> 1));
+    const int c = (tx & 1) | ((ty & 1) << 1) | ((tz & 1) << 2);
+    const long long gi = 8LL * (sKey[s] & 0x0FFFFFFFu) + c;
     double q[5];
+    if constexpr (F64) {
+      V::ld(sW, tb, q[0], q[1], q[2], q[3]);
+      q[4] = sWp[tb];
+    } else {
 #pragma unroll
-    for (int v = 0; v < 5; v++) q[v] = A.W[v * N8 + gi];
+      for (int v = 0; v < 5; v++) q[v] = sQ[v * kNT + tid];
+    }
     double Wout[5];
-    if (sSp[tid]) {
+    if (fme & kFSplit) {
       // split cell: primitive mean of the 8 children (src/hydro_utils.c:3420-3481);
       // without the finer level (drop-in mode) the caller averages on the host
       double acc[5] = {0., 0., 0., 0., 0.};
@@ -354,47 +379,18 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       for (int v = 0; v < 5; v++) Wout[v] = acc[v];
     } else {
       const double dtsurdx = A.dt / A.dx;
-      // flux of face k (0:-x 1:+x ...) of this cell, from the face tasks of P2
-      auto flux_slot = [&](int k, const R *&b4, const R *&b1, int &idx) {
-        const int d = k >> 1;
-        b4 = sF;
-        b1 = sF4;
-        idx = d * NT + tid;
-        if (!(k & 1)) return;
-        int c2;
-        const int s2 = nb(o, c, k, c2);
-        if (s2 >= 0 && s2 < n) {
-          idx = d * NT + s2 * 8 + c2;
-        } else {
-          b4 = sFB;
-          b1 = sFB4;
-          idx = sBmap[tid * 3 + d];
-        }
-      };
+      // face e of this cell: -x,+x,-y,+y,-z,+z
+      const int ex = tx + 9 * (ty + 8 * tz), ey = kFacesX + tx + 8 * (ty + 9 * tz), ez = kFacesX + kFacesY + tid;
       auto flux5 = [&](int k, double F[5]) {
-        const R *b4, *b1;
-        int idx;
-        flux_slot(k, b4, b1, idx);
+        const int e = (k < 2) ? (ex + (k & 1)) : ((k < 4) ? (ey + 8 * (k & 1)) : (ez + 64 * (k & 1)));
         R f0, f1, f2, f3;
-        V::ld(b4, idx, f0, f1, f2, f3);
+        V::ld(sF, e, f0, f1, f2, f3);
         F[0] = (double)f0;
         F[1] = (double)f1;
         F[2] = (double)f2;
         F[3] = (double)f3;
-        F[4] = (double)b1[idx];
+        F[4] = (double)sF1[e];
       };
-      // updatefield (src/hydro_utils.c:3050-3082): dU = sum over faces -x,+x,-y,+y,-z,+z
-      // of (+-F dt/dx), signs alternating from +
-      double dU[5] = {0., 0., 0., 0., 0.};
-      double one = 1.;
-#pragma unroll
-      for (int k = 0; k < 6; k++) {
-        double F[5];
-        flux5(k, F);
-#pragma unroll
-        for (int v = 0; v < 5; v++) dU[v] += F[v] * dtsurdx * one;
-        one *= -1.;
-      }
       double Ud, Udu, Udv, Udw, UE;
       if (A.B != nullptr) {  // drop-in: W2U of the caller's fieldnew
         const double bd = A.B[gi];
@@ -410,7 +406,19 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         Udw = q[0] * q[3];
         UE = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
       }
-      if constexpr (sizeof(R) == 8) {
+      if constexpr (F64) {
+        // updatefield (src/hydro_utils.c:3050-3082): dU = sum over faces -x,+x,-y,+y,-z,+z
+        // of (+-F dt/dx), signs alternating from +
+        double dU[5] = {0., 0., 0., 0., 0.};
+        double one = 1.;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          double F[5];
+          flux5(k, F);
+#pragma unroll
+          for (int v = 0; v < 5; v++) dU[v] += F[v] * dtsurdx * one;
+          one *= -1.;
+        }
         // scatterstencil central update (src/hydro_utils.c:3129-3188), reference order
         if (A.B == nullptr && A.C != nullptr) {
           Ud += __ldcg(A.C + gi);
@@ -425,8 +433,16 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         Udw += dU[3];
         UE += dU[4];
       } else {
-        // mixed: FP32 face fluxes summed in FP64, added to the FP64 conserved state
-        // with Neumaier-compensated summation (base + corrections + dU)
+        // mixed: FP32 face fluxes, their divergence accumulated in FP64 and added to
+        // the FP64 conserved state with Neumaier-compensated summation (base + corrections + dU)
+        double dU[5] = {0., 0., 0., 0., 0.};
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          double F[5];
+          flux5(k, F);
+#pragma unroll
+          for (int v = 0; v < 5; v++) dU[v] = (k & 1) ? dU[v] - F[v] : dU[v] + F[v];
+        }
         double sum[5] = {Ud, Udu, Udv, Udw, UE}, comp[5] = {0., 0., 0., 0., 0.};
         auto add = [&](int v, double x) {
           const double t = sum[v] + x;
@@ -438,7 +454,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
           for (int v = 0; v < 5; v++) add(v, __ldcg(A.C + v * N8 + gi));
         }
 #pragma unroll
-        for (int v = 0; v < 5; v++) add(v, dU[v]);
+        for (int v = 0; v < 5; v++) add(v, dU[v] * dtsurdx);
         Ud = sum[0] + comp[0];
         Udu = sum[1] + comp[1];
         Udv = sum[2] + comp[2];
@@ -448,7 +464,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       // U2W (src/hydro_utils.c:35-64), pressure floor, E - Ekin recovery
       const double dl = (Ud == 0. ? 10. : Ud);
       Wout[0] = Ud;
-      if constexpr (sizeof(R) == 8) {
+      if constexpr (F64) {
         Wout[1] = Udu / dl;
         Wout[2] = Udv / dl;
         Wout[3] = Udw / dl;
@@ -466,12 +482,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       // fine -> coarse correction into unsplit coarser neighbours (src/hydro_utils.c:3206-3295)
 #pragma unroll
       for (int k = 0; k < 6; k++) {
-        if (nei_inside(c, k)) continue;
-        const int g = sG[o * 6 + k];
-        if (g == 255) continue;
-        const uint32_t key = sKey[g];
-        if ((key >> 28) != kKeyInj) continue;
-        const long long cc = key & 0x0FFFFFFFu;
+        const int bs = (k < 2) ? 1 : ((k < 4) ? kBoxX : kBoxX * kBoxY);
+        const int b2 = (k & 1) ? tb + bs : tb - bs;
+        if (!(sSt[b2] & kFInj)) continue;
+        const int x2 = b2 % kBoxX, y2 = (b2 / kBoxX) % kBoxY, z2 = b2 / (kBoxX * kBoxY);
+        const long long cc = sKey[(x2 >> 1) + kSlotX * ((y2 >> 1) + kSlotY * (z2 >> 1))] & 0x0FFFFFFFu;
         const double one = (k & 1) ? 1. : -1.;
         double F[5];
         flux5(k, F);
@@ -493,16 +508,15 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 // co-resident (grid <= occupancy x SMs) and take items in list order, so a
 // tile waiting for a finer level (listed first) never blocks the CTAs that
 // still have to finish that level.
-template <class M, int T, int SMAX, int HMAX, int BMAX>
-__global__ void __launch_bounds__(8 * T, (sizeof(typename M::R) == 8) ? 1 : 3)
-    level_batch_kernel(const BatchArgs Bt) {
+template <class M>
+__global__ void __launch_bounds__(kNT, (sizeof(typename M::R) == 8) ? 1 : 3) level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
   unsigned st = 0;
   for (int w = blockIdx.x; w < Bt.nwork; w += gridDim.x) {
     const int item = Bt.work[w];
     const int slot = item >> kWorkSlotShift, tile = item & ((1 << kWorkSlotShift) - 1);
-    level_tile<M, T, SMAX, HMAX, BMAX>(Bt, Bt.lv[slot], slot, tile, smem, st);
+    level_tile<M>(Bt, Bt.lv[slot], slot, tile, smem, st);
     __syncthreads();
   }
   if (st) atomicOr(Bt.status, st);

@@ -8,8 +8,9 @@
 // walk always lands on the geometric level-(L-1) cell, so the block is a window
 // of one "virtual level-L grid" in which every position holds either a real
 // level-L cell or an injected coarser leaf.  vnbr() below steps through that
-// virtual grid one oct at a time; a tile stages the union of the windows of
-// its octs (faces and edges; MUSCL never reads the corners) without duplicates.
+// virtual grid one oct at a time.  A tile is a 4x4x2 brick of level-L oct
+// positions; it stages, at their grid positions in a 6x6x4 slot box, the union
+// of the windows of its octs (faces and edges: MUSCL never reads the corners).
 //
 // With transmissive boundaries (the reference's -DHYDROTEST -DTRANS*), the
 // face slot across a boundary is the mirror of the boundary oct through the
@@ -141,119 +142,132 @@ struct Planner {
   }
 };
 
-struct TileBuild {
-  std::vector<uint32_t> keys;
-  std::vector<uint8_t> graph;
-  std::vector<uint16_t> halo;
-  std::vector<uint16_t> bface;
-  int S = 0, H = 0, B = 0;
-};
+// mirror map of the transmissive ghost octs (src/hydro_utils.c:2504-2610):
+// ghost cell c across face k takes cell kMirror[k][c] of the boundary oct
+constexpr uint8_t kMirror[6][8] = {{0, 0, 2, 2, 4, 4, 6, 6}, {1, 1, 3, 3, 5, 5, 7, 7}, {0, 1, 0, 1, 4, 5, 4, 5},
+                                   {2, 3, 2, 3, 7, 6, 6, 7}, {0, 1, 2, 3, 0, 1, 2, 3}, {4, 5, 6, 7, 4, 5, 6, 7}};
+constexpr int kDir[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
+constexpr int kBoxStride[3] = {1, kBoxX, kBoxX * kBoxY};
 
-// Stage list, neighbour graph and halo of the tile [o0, o0+n).  Returns false
-// if a needed neighbour is missing (error bit set in the planner).
-bool build_tile(Planner &P, int L, int o0, int n, TileBuild &tb) {
-  std::unordered_map<uint32_t, int> pos;
-  pos.reserve(256);
-  tb.keys.clear();
-  auto add = [&](uint32_t key) {
-    if (key == kKeyNone) return;
-    if (pos.find(key) == pos.end()) {
-      pos.emplace(key, (int)tb.keys.size());
-      tb.keys.push_back(key);
-    }
+// cell flags of the staged box, as the level kernel derives them
+enum : uint8_t { kFPresent = 1, kFSplit = 2, kFTile = 4, kFInj = 8 };
+inline bool f_ok(uint8_t f) { return (f & (kFPresent | kFSplit)) == kFPresent; }
+inline bool f_tileleaf(uint8_t f) { return (f & (kFPresent | kFSplit | kFTile)) == (kFPresent | kFTile); }
+
+// Slot keys of the brick at oct origin (ox,oy,oz) holding `octs` (level list
+// indices, positions in `pos`).  Fills keys[kSlots] and the mask.
+bool plan_brick(Planner &P, int L, const std::vector<int> &octs, const std::vector<int32_t> &pos, int ox, int oy,
+                int oz, uint32_t *keys, uint32_t &mask) {
+  std::fill(keys, keys + kSlots, kKeyNone);
+  mask = 0;
+  auto put = [&](int sx, int sy, int sz, uint32_t key) -> bool {
+    if (key == kKeyNone) return true;
+    if (sx < 0 || sx >= kSlotX || sy < 0 || sy >= kSlotY || sz < 0 || sz >= kSlotZ) return false;
+    uint32_t &k = keys[sx + kSlotX * (sy + kSlotY * sz)];
+    if (k == kKeyNone) k = key;
+    return k == key;
   };
-  for (int t = 0; t < n; t++) add(key_make(kKeyReal, (uint32_t)(o0 + t)));
-  for (int t = 0; t < n; t++) {
-    const uint32_t self = key_make(kKeyReal, (uint32_t)(o0 + t));
-    for (int k = 0; k < 6; k++) {
-      const uint32_t f = P.vnbr(L, self, k);
-      if (f == kKeyNone) {
-        P.err |= EMMA_ST_TREE;
-        P.msg = "missing face neighbour of a level-" + std::to_string(L) + " oct";
-        return false;
-      }
-      add(f);
-    }
+  auto bad = [&](const std::string &m) {
+    P.err |= EMMA_ST_TREE;
+    P.msg = m + " (level " + std::to_string(L) + ", brick at oct " + std::to_string(ox) + "," + std::to_string(oy) +
+            "," + std::to_string(oz) + ")";
+    return false;
+  };
+  for (int o : octs) {
+    const int ix = pos[3 * o] - ox, iy = pos[3 * o + 1] - oy, iz = pos[3 * o + 2] - oz;
+    mask |= 1u << (ix + kBrickX * (iy + kBrickY * iz));
+    if (!put(ix + 1, iy + 1, iz + 1, key_make(kKeyReal, (uint32_t)o))) return bad("two octs at one brick position");
   }
-  // edges: neighbours of the face neighbours off the face axis
-  for (int t = 0; t < n; t++) {
-    const uint32_t self = key_make(kKeyReal, (uint32_t)(o0 + t));
+  for (int o : octs) {
+    const int sx = pos[3 * o] - ox + 1, sy = pos[3 * o + 1] - oy + 1, sz = pos[3 * o + 2] - oz + 1;
+    const uint32_t self = key_make(kKeyReal, (uint32_t)o);
     for (int k = 0; k < 6; k++) {
       const uint32_t f = P.vnbr(L, self, k);
+      if (f == kKeyNone) return bad("missing face neighbour of an oct");
+      if (!put(sx + kDir[k][0], sy + kDir[k][1], sz + kDir[k][2], f)) return bad("inconsistent face neighbour");
       for (int j = 0; j < 6; j++) {
         if ((j >> 1) == (k >> 1)) continue;
-        add(P.vnbr(L, f, j));
+        if (!put(sx + kDir[k][0] + kDir[j][0], sy + kDir[k][1] + kDir[j][1], sz + kDir[k][2] + kDir[j][2],
+                 P.vnbr(L, f, j)))
+          return bad("inconsistent edge neighbour");
       }
     }
   }
-  tb.S = (int)tb.keys.size();
-  tb.H = 0;
-  if (tb.S > kSMax) return true;  // too many staged octs: the caller shrinks the tile
-  tb.graph.assign((size_t)tb.S * 6, 255);
-  for (int s = 0; s < tb.S; s++)
-    for (int k = 0; k < 6; k++) {
-      const uint32_t g = P.vnbr(L, tb.keys[s], k);
-      auto it = (g == kKeyNone) ? pos.end() : pos.find(g);
-      if (it != pos.end() && it->second < 255) tb.graph[6 * s + k] = (uint8_t)it->second;
-    }
-  // halo entries: (cell of a non-tile staged oct, its face toward a tile oct)
-  tb.halo.clear();
-  for (int s = n; s < tb.S; s++)
-    for (int c = 0; c < 8; c++)
-      for (int k = 0; k < 6; k++) {
-        if (inside(c, k)) continue;
-        const int g = tb.graph[6 * s + k];
-        if (g != 255 && g < n) tb.halo.push_back((uint16_t)(((8 * s + c) << 3) | k));
-      }
-  tb.H = (int)tb.halo.size();
-  if (tb.H > kHMax) return true;  // too many halo entries: the caller shrinks the tile
-  // + faces of tile cells that border a non-tile staged oct
-  tb.bface.clear();
-  for (int t = 0; t < 8 * n; t++)
-    for (int d = 0; d < 3; d++) {
-      const int k = 2 * d + 1, c = t & 7;
-      if (inside(c, k)) continue;
-      const int g = tb.graph[6 * (t >> 3) + k];
-      if (g == 255 || g >= n) tb.bface.push_back((uint16_t)(4 * t + d));
-    }
-  tb.B = (int)tb.bface.size();
-  if (tb.B > kBMax) return true;
-  // every neighbour a reconstruction reads must be staged
-  auto need = [&](int s, int c) -> bool {
-    for (int k = 0; k < 6; k++) {
-      if (inside(c, k)) continue;
-      if (tb.graph[6 * s + k] == 255) return false;
-    }
-    return true;
-  };
-  for (int s = 0; s < n; s++)
-    for (int c = 0; c < 8; c++)
-      if (!need(s, c)) {
-        P.err |= EMMA_ST_TREE;
-        P.msg = "unstaged neighbour of a tile cell";
-        return false;
-      }
-  for (uint16_t e16 : tb.halo)
-    if (!need(e16 >> 6, (e16 >> 3) & 7)) {
-      const int e = e16 >> 3;
-      P.err |= EMMA_ST_TREE;
-      const uint32_t key = tb.keys[e >> 3];
-      if (std::getenv("EMMA_PLAN_DEBUG")) {
-        std::fprintf(stderr, "tile o0=%d n=%d S=%d H=%d failing staged %d cell %d\n", o0, n, tb.S, tb.H, e >> 3, e & 7);
-        for (int s = 0; s < tb.S; s++) {
-          std::fprintf(stderr, "  s=%3d kind=%u idx=%u g=", s, tb.keys[s] >> 28, tb.keys[s] & 0x0FFFFFFFu);
-          for (int k = 0; k < 6; k++) {
-            uint32_t vk = P.vnbr(L, tb.keys[s], k);
-            std::fprintf(stderr, " %3d(%u:%u)", tb.graph[6 * s + k], vk == kKeyNone ? 9 : vk >> 28, vk & 0x0FFFFFFFu);
-          }
-          std::fprintf(stderr, "\n");
+  return true;
+}
+
+// Cell flags of a planned brick and the checks that every stencil the kernel
+// evaluates reads staged cells only.  Collects the level L-1 cells that receive
+// fine->coarse corrections.
+bool check_brick(Planner &P, int L, const uint32_t *keys, uint32_t mask, std::vector<uint8_t> *corrected) {
+  const HostLevel &lv = P.H.lev[L];
+  uint8_t fl[kBox];
+  for (int s = 0; s < kSlots; s++) {
+    const int sz = s / (kSlotX * kSlotY), sy = (s / kSlotX) % kSlotY, sx = s % kSlotX;
+    const bool inner = sx >= 1 && sx <= kBrickX && sy >= 1 && sy <= kBrickY && sz >= 1 && sz <= kBrickZ;
+    for (int c = 0; c < 8; c++) {
+      const int b = (2 * sx + (c & 1)) + kBoxX * ((2 * sy + ((c >> 1) & 1)) + kBoxY * (2 * sz + (c >> 2)));
+      const uint32_t key = keys[s];
+      uint8_t f = 0;
+      if (key != kKeyNone) {
+        const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
+        f = kFPresent;
+        if (kind == kKeyReal) {
+          if ((lv.split[idx] >> c) & 1) f |= kFSplit;
+          if (inner && ((mask >> ((sx - 1) + kBrickX * ((sy - 1) + kBrickY * (sz - 1)))) & 1)) f |= kFTile;
+        } else if (kind == kKeyInj) {
+          f |= kFInj;
+        } else {
+          if ((lv.split[idx] >> kMirror[kind - kKeyGhost0][c]) & 1) f |= kFSplit;
         }
       }
-      P.msg = "unstaged neighbour of a halo cell (level " + std::to_string(L) + ", tile at oct " +
-              std::to_string(o0) + ", staged kind " + std::to_string(key >> 28) + " index " +
-              std::to_string(key & 0x0FFFFFFFu) + ", cell " + std::to_string(e & 7) + ")";
-      return false;
+      fl[b] = f;
     }
+  }
+  auto all_nbrs = [&](int b) {
+    for (int a = 0; a < 3; a++)
+      if (!(fl[b - kBoxStride[a]] & kFPresent) || !(fl[b + kBoxStride[a]] & kFPresent)) return false;
+    return true;
+  };
+  auto fail = [&](const char *m) {
+    P.err |= EMMA_ST_TREE;
+    P.msg = std::string(m) + " (level " + std::to_string(L) + ")";
+    return false;
+  };
+  // brick cells: reconstructed if a leaf of the tile or face-adjacent to one
+  for (int z = 2; z < 2 + 2 * kBrickZ; z++)
+    for (int y = 2; y < 2 + 2 * kBrickY; y++)
+      for (int x = 2; x < 2 + 2 * kBrickX; x++) {
+        const int b = x + kBoxX * (y + kBoxY * z);
+        bool near = f_tileleaf(fl[b]);
+        for (int a = 0; a < 3; a++)
+          near = near || f_tileleaf(fl[b - kBoxStride[a]]) || f_tileleaf(fl[b + kBoxStride[a]]);
+        if (f_ok(fl[b]) && near && !all_nbrs(b)) return fail("unstaged neighbour of a reconstructed cell");
+        if (!f_tileleaf(fl[b])) continue;
+        for (int a = 0; a < 3; a++)
+          for (int sgn = -1; sgn <= 1; sgn += 2) {
+            const int b2 = b + sgn * kBoxStride[a];
+            if (!(fl[b2] & kFPresent)) return fail("unstaged face neighbour of a leaf cell");
+            if (corrected && (fl[b2] & kFInj)) {
+              const int x2 = b2 % kBoxX, y2 = (b2 / kBoxX) % kBoxY, z2 = b2 / (kBoxX * kBoxY);
+              (*corrected)[keys[(x2 >> 1) + kSlotX * ((y2 >> 1) + kSlotY * (z2 >> 1))] & 0x0FFFFFFFu] = 1;
+            }
+          }
+      }
+  // ring cells face-adjacent to a leaf of the tile: reconstructed too
+  for (int z = 1; z < kBoxZ - 1; z++)
+    for (int y = 1; y < kBoxY - 1; y++)
+      for (int x = 1; x < kBoxX - 1; x++) {
+        const bool ix = x >= 2 && x < 2 + 2 * kBrickX, iy = y >= 2 && y < 2 + 2 * kBrickY,
+                   iz = z >= 2 && z < 2 + 2 * kBrickZ;
+        if ((int)ix + (int)iy + (int)iz != 2) continue;  // face layer of the brick, not an edge
+        const int b = x + kBoxX * (y + kBoxY * z);
+        int bin = b;
+        if (!ix) bin = b + (x < 2 ? 1 : -1);
+        if (!iy) bin = b + (y < 2 ? kBoxX : -kBoxX);
+        if (!iz) bin = b + (z < 2 ? kBoxX * kBoxY : -kBoxX * kBoxY);
+        if (f_ok(fl[b]) && f_tileleaf(fl[bin]) && !all_nbrs(b)) return fail("unstaged neighbour of a ring cell");
+      }
   return true;
 }
 
@@ -307,68 +321,56 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
   }
   for (int L = std::max(lcoarse, plan_lo); L <= std::min(lmax, plan_hi); L++) {
     HostLevel &lv = H.lev[L];
-    std::unordered_map<std::string, int> gdedup, hdedup, bdedup;
-    std::vector<uint8_t> injmark;
-    if (L > lcoarse) injmark.assign((size_t)8 * H.lev[L - 1].noct, 0);
-    TileBuild tb;
-    int o0 = 0;
-    while (o0 < lv.noct) {
-      int n = std::min(kTileOcts, lv.noct - o0);
-      for (;;) {
-        if (!build_tile(P, L, o0, n, tb)) {
-          err = P.msg;
-          return (int)P.err;
+    if (lv.noct == 0) continue;
+    // integer oct positions on the level grid, grouped into bricks in list order
+    const double scale = std::ldexp(1.0, L - 1);
+    const int n = 1 << (L - 1);
+    std::vector<int32_t> pos((size_t)3 * lv.noct);
+    std::unordered_map<uint64_t, int> brick;
+    std::vector<std::vector<int>> members;
+    for (int i = 0; i < lv.noct; i++) {
+      const struct OCT *o = lv.octs[i];
+      const double q[3] = {o->x * scale, o->y * scale, o->z * scale};
+      for (int a = 0; a < 3; a++) {
+        const double r = std::floor(q[a] + 0.5);
+        if (r != q[a] || r < 0 || r >= n) {
+          err = "oct position off the level grid at level " + std::to_string(L);
+          return EMMA_ST_TREE;
         }
-        if ((tb.S <= kSMax && tb.H <= kHMax && tb.B <= kBMax) || n == 1) break;
-        n = (n > 8) ? n - 4 : n - 1;
+        pos[3 * i + a] = (int32_t)r;
       }
-      if (tb.S > kSMax || tb.H > kHMax || tb.B > kBMax) {
-        err = "single-oct tile exceeds the staging limits";
-        return EMMA_ST_TREE;
+      const uint64_t bk = ((uint64_t)(pos[3 * i] / kBrickX) << 42) | ((uint64_t)(pos[3 * i + 1] / kBrickY) << 21) |
+                          (uint64_t)(pos[3 * i + 2] / kBrickZ);
+      auto it = brick.find(bk);
+      if (it == brick.end()) {
+        it = brick.emplace(bk, (int)members.size()).first;
+        members.emplace_back();
       }
-      TileDesc td;
-      std::memset(&td, 0, sizeof(td));
-      td.oct0 = o0;
-      td.noct = n;
-      td.S = tb.S;
-      td.H = tb.H;
-      td.B = tb.B;
-      td.keys_off = (int)lv.keys.size();
-      lv.keys.insert(lv.keys.end(), tb.keys.begin(), tb.keys.end());
-      for (uint32_t key : tb.keys)
-        if ((key >> 28) == kKeyInj && !injmark.empty()) injmark[key & 0x0FFFFFFFu] = 1;
-      std::string gk(reinterpret_cast<const char *>(tb.graph.data()), tb.graph.size());
-      auto git = gdedup.find(gk);
-      if (git == gdedup.end()) {
-        td.graph_off = (int)lv.graph.size();
-        lv.graph.insert(lv.graph.end(), tb.graph.begin(), tb.graph.end());
-        gdedup.emplace(std::move(gk), td.graph_off);
-      } else {
-        td.graph_off = git->second;
-      }
-      std::string hk(reinterpret_cast<const char *>(tb.halo.data()), tb.halo.size() * sizeof(uint16_t));
-      auto hit = hdedup.find(hk);
-      if (hit == hdedup.end()) {
-        td.halo_off = (int)lv.halo.size();
-        lv.halo.insert(lv.halo.end(), tb.halo.begin(), tb.halo.end());
-        hdedup.emplace(std::move(hk), td.halo_off);
-      } else {
-        td.halo_off = hit->second;
-      }
-      std::string bk(reinterpret_cast<const char *>(tb.bface.data()), tb.bface.size() * sizeof(uint16_t));
-      auto bit = bdedup.find(bk);
-      if (bit == bdedup.end()) {
-        td.bface_off = (int)lv.bface.size();
-        lv.bface.insert(lv.bface.end(), tb.bface.begin(), tb.bface.end());
-        bdedup.emplace(std::move(bk), td.bface_off);
-      } else {
-        td.bface_off = bit->second;
-      }
-      lv.tiles.push_back(td);
-      o0 += n;
+      members[it->second].push_back(i);
     }
-    for (size_t i = 0; i < injmark.size(); i++)
-      if (injmark[i]) lv.inj_cells.push_back((int32_t)i);
+    std::vector<uint8_t> corrected;
+    if (L > lcoarse) corrected.assign((size_t)8 * H.lev[L - 1].noct, 0);
+    lv.tiles.resize(members.size());
+    lv.keys.assign(members.size() * (size_t)kSlots, kKeyNone);
+    for (size_t t = 0; t < members.size(); t++) {
+      const int o0 = members[t][0];
+      TileDesc &td = lv.tiles[t];
+      std::memset(&td, 0, sizeof(td));
+      td.ox = pos[3 * o0] / kBrickX * kBrickX;
+      td.oy = pos[3 * o0 + 1] / kBrickY * kBrickY;
+      td.oz = pos[3 * o0 + 2] / kBrickZ * kBrickZ;
+      td.noct = (int)members[t].size();
+      uint32_t *keys = &lv.keys[t * kSlots];
+      if (!plan_brick(P, L, members[t], pos, td.ox, td.oy, td.oz, keys, td.mask) ||
+          !check_brick(P, L, keys, td.mask, corrected.empty() ? nullptr : &corrected)) {
+        err = P.msg;
+        return (int)P.err;
+      }
+    }
+    for (size_t i = 0; i < corrected.size(); i++)
+      if (corrected[i]) lv.inj_cells.push_back((int32_t)i);
+    for (uint32_t key : lv.keys)
+      if (key != kKeyNone && (key >> 28) == kKeyInj) lv.reads_coarse = true;
   }
   return validate_host_tree(H, plan_lo, plan_hi, err);
 }
@@ -380,51 +382,40 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
     const HostLevel &lv = H.lev[L];
     const long long ncoarse8 = (L > H.lcoarse) ? 8LL * H.lev[L - 1].noct : 0;
     const long long nfine = (L < H.lmax) ? H.lev[L + 1].noct : 0;
+    if (lv.keys.size() != lv.tiles.size() * (size_t)kSlots) {
+      err = "slot keys do not match the tiles at level " + std::to_string(L);
+      return EMMA_ST_TREE;
+    }
+    std::vector<uint8_t> seen((size_t)lv.noct, 0);
     long long covered = 0;
-    for (const TileDesc &t : lv.tiles) {
-      if (t.noct < 1 || t.noct > kTileOcts || t.oct0 != covered || t.S < t.noct || t.S > kSMax || t.H < 0 ||
-          t.H > kHMax || t.keys_off < 0 || (size_t)t.keys_off + t.S > lv.keys.size() || t.graph_off < 0 ||
-          (size_t)t.graph_off + 6 * (size_t)t.S > lv.graph.size() || t.halo_off < 0 ||
-          (size_t)t.halo_off + t.H > lv.halo.size()) {
+    for (size_t t = 0; t < lv.tiles.size(); t++) {
+      const TileDesc &td = lv.tiles[t];
+      if (td.mask == 0 || td.noct != __builtin_popcount(td.mask)) {
         err = "invalid tile descriptor at level " + std::to_string(L);
         return EMMA_ST_TREE;
       }
-      covered += t.noct;
-      for (int s = 0; s < t.S; s++) {
-        const uint32_t key = lv.keys[t.keys_off + s];
+      for (int s = 0; s < kSlots; s++) {
+        const uint32_t key = lv.keys[t * kSlots + s];
+        if (key == kKeyNone) continue;
         const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
         const bool ok = (kind == kKeyReal || (kind >= kKeyGhost0 && kind < kKeyGhost0 + 6)) ? (idx < (uint32_t)lv.noct)
                         : (kind == kKeyInj) ? ((long long)idx < ncoarse8)
                                             : false;
-        if (!ok || (s < t.noct && key != key_make(kKeyReal, (uint32_t)(t.oct0 + s)))) {
+        if (!ok) {
           err = "invalid staged key at level " + std::to_string(L);
           return EMMA_ST_TREE;
         }
-        for (int k = 0; k < 6; k++) {
-          const int g = lv.graph[t.graph_off + 6 * s + k];
-          if (g != 255 && g >= t.S) {
-            err = "invalid graph entry at level " + std::to_string(L);
-            return EMMA_ST_TREE;
-          }
-        }
       }
-      if (t.B < 0 || t.B > kBMax || t.bface_off < 0 || (size_t)t.bface_off + t.B > lv.bface.size()) {
-        err = "invalid boundary-face range at level " + std::to_string(L);
-        return EMMA_ST_TREE;
-      }
-      for (int h = 0; h < t.H; h++) {
-        const int e = lv.halo[t.halo_off + h] >> 3, k = lv.halo[t.halo_off + h] & 7;
-        if (e < 8 * t.noct || e >= 8 * t.S || k > 5) {
-          err = "invalid halo entry at level " + std::to_string(L);
+      for (int m = 0; m < kTileOcts; m++) {
+        if (!((td.mask >> m) & 1)) continue;
+        const int sx = 1 + m % kBrickX, sy = 1 + (m / kBrickX) % kBrickY, sz = 1 + m / (kBrickX * kBrickY);
+        const uint32_t key = lv.keys[t * kSlots + sx + kSlotX * (sy + kSlotY * sz)];
+        if ((key >> 28) != kKeyReal || seen[key & 0x0FFFFFFFu]) {
+          err = "tile oct missing or advanced twice at level " + std::to_string(L);
           return EMMA_ST_TREE;
         }
-      }
-      for (int b = 0; b < t.B; b++) {
-        const int e = lv.bface[t.bface_off + b];
-        if ((e >> 2) >= 8 * t.noct || (e & 3) > 2) {
-          err = "invalid boundary face at level " + std::to_string(L);
-          return EMMA_ST_TREE;
-        }
+        seen[key & 0x0FFFFFFFu] = 1;
+        covered++;
       }
     }
     if (covered != lv.noct) {

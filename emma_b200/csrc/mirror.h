@@ -15,12 +15,10 @@ struct HostLevel {
   std::vector<struct OCT *> octs;     // list order (cpu == rank)
   std::vector<uint8_t> split;         // per oct: bit c set if cell c has a child
   std::vector<int32_t> child;         // per cell: index of the child oct at L+1, or -1
-  std::vector<TileDesc> tiles;
-  std::vector<uint32_t> keys;
-  std::vector<uint8_t> graph;
-  std::vector<uint16_t> halo;
-  std::vector<uint16_t> bface;
-  std::vector<int32_t> inj_cells;     // level L-1 cells injected into this level's plans
+  std::vector<TileDesc> tiles;        // brick tiles, in order of their first oct in the list
+  std::vector<uint32_t> keys;         // kSlots slot keys per tile
+  std::vector<int32_t> inj_cells;     // level L-1 cells that receive fine->coarse corrections
+  bool reads_coarse = false;          // some tile stages an injected level L-1 cell
 };
 
 struct HostTree {

@@ -16,23 +16,26 @@ constexpr uint32_t kKeyReal = 0, kKeyInj = 1, kKeyGhost0 = 2;
 constexpr uint32_t kKeyNone = 0xFFFFFFFFu;
 constexpr uint32_t key_make(uint32_t kind, uint32_t idx) { return (kind << 28) | idx; }
 
-// Kernel shape the plans are cut for: octs per tile, staged octs, directional
-// halo entries, boundary faces.
-constexpr int kTileOcts = 32;
-constexpr int kSMax = 136;
-constexpr int kHMax = 256;
-constexpr int kBMax = 128;
+// Brick tiles.  A tile is one brick of 4 x 4 x 2 oct positions of a level's
+// grid holding at least one oct of the level (mask: which).  The kernel stages
+// a 6 x 6 x 4 box of virtual-oct slots (the brick and a ring of one oct), i.e.
+// 12 x 12 x 8 cells, so that every neighbour a stencil reads sits at a fixed
+// offset (+-1, +-12, +-144 cells).  Slot s = sx + 6 (sy + 6 sz); the brick
+// interior is sx,sy in 1..4, sz in 1..2; slots no stencil reads hold kKeyNone.
+constexpr int kBrickX = 4, kBrickY = 4, kBrickZ = 2, kTileOcts = kBrickX * kBrickY * kBrickZ;
+constexpr int kSlotX = kBrickX + 2, kSlotY = kBrickY + 2, kSlotZ = kBrickZ + 2;
+constexpr int kSlots = kSlotX * kSlotY * kSlotZ;                       // 144
+constexpr int kBoxX = 2 * kSlotX, kBoxY = 2 * kSlotY, kBoxZ = 2 * kSlotZ;
+constexpr int kBox = kBoxX * kBoxY * kBoxZ;                            // 1152 staged cells
+constexpr int kNT = 8 * kTileOcts;                                     // 256 brick cells = threads
+constexpr int kHaloCells = 2 * (8 * 4) * 2 + 2 * (8 * 8);              // 256 cells face-adjacent to the brick
+constexpr int kFacesX = 9 * 8 * 4, kFacesY = 8 * 9 * 4, kFacesZ = 8 * 8 * 5;
+constexpr int kFaces = kFacesX + kFacesY + kFacesZ;                    // 896 faces of the brick cells
 
 struct TileDesc {
-  int oct0;       // first oct of the tile (level list index)
-  int noct;       // octs in the tile (<= kTileOcts)
-  int S;          // staged virtual octs (tile octs first)
-  int H;          // halo entries: (staged cell s*8+c) << 3 | face k of that cell toward the tile
-  int B;          // boundary faces: tile cell t*4 + axis whose + face borders a non-tile oct
-  int keys_off;   // offset into the keys array
-  int graph_off;  // offset into the graph array (S*6 bytes; 255 = not staged)
-  int halo_off;   // offset into the halo array
-  int bface_off;  // offset into the boundary-face array
+  uint32_t mask;  // bit (ix + 4 iy + 16 iz): brick position holds an oct of this level
+  int noct;       // octs in the tile (popcount of mask)
+  int ox, oy, oz; // brick origin in oct coordinates of the level
   int pad[3];
 };
 
@@ -55,10 +58,7 @@ struct LevelArgs {
   const uint8_t *split;  // per oct bitmask of split cells
   const int *child;      // per cell: child oct index at L+1, -1 for a leaf
   const TileDesc *tiles;
-  const uint32_t *keys;
-  const uint8_t *graph;
-  const uint16_t *halo;
-  const uint16_t *bface;
+  const uint32_t *keys;  // kSlots keys per tile
   double dt, dx;
   int ntiles;
   int wait_slot;      // level whose tiles must all be updated before this level's

@@ -148,8 +148,9 @@ void emma_hydro_reset_counters(void);
 int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cells);
 
 /* Planning diagnostics, host only (no GPU needed): per level lcoarse..lmax,
- * stats5[5*(L-lcoarse)+{0..4}] = octs, tiles, max staged octs per tile, max
- * halo cells per tile, leaf cells.  Returns EMMA_ST_* bits of the planning. */
+ * stats5[5*(L-lcoarse)+{0..4}] = octs, tiles (4x4x2-oct bricks), max staged
+ * octs per tile, staged octs summed over the tiles, leaf cells.  Returns
+ * EMMA_ST_* bits of the planning. */
 int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int trans_flags, long long *stats5);
 
 /* Level time step computed without allocating any memory.  No counterpart in
