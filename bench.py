@@ -130,9 +130,11 @@ def graph_kernel_count(cfg, tree):
     if cfg.nsub == 1 or len(levels) == 1:
         return len(levels) + 3  # CFL per level, batch begin, level kernel, batch end
     n, per = 0, 1
-    for _ in levels:
+    for l in levels:
         per *= cfg.nsub
-        n += per * 7  # begin, clear, CFL, dt, prelaunch, level kernel, end per gated iteration
+        # begin, CFL, dt, prelaunch, level kernel, end per gated iteration, plus the
+        # clear of the correction buffer on levels that have a finer level
+        n += per * (6 + (1 if l != levels[-1] else 0))
     return n + 1
 
 

@@ -201,8 +201,13 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     const size_t bytes = sizeof(double) * 5 * (size_t)std::max<long long>(d.n8, 1);
     if (!ck(cudaMalloc(&d.W0, bytes), "cudaMalloc W")) return false;
     if (!ck(cudaMalloc(&d.W1, bytes), "cudaMalloc Wn")) return false;
-    if (!ck(cudaMalloc(&d.C, bytes), "cudaMalloc C")) return false;
-    if (!ck(cudaMemset(d.C, 0, bytes), "cudaMemset C")) return false;
+    // corrections arrive only from the finer level: a level without split cells has none
+    bool has_split = false;
+    for (uint8_t m : h.split) has_split = has_split || m != 0;
+    if (has_split) {
+      if (!ck(cudaMalloc(&d.C, bytes), "cudaMalloc C")) return false;
+      if (!ck(cudaMemset(d.C, 0, bytes), "cudaMemset C")) return false;
+    }
     if (with_base && !h.tiles.empty())
       if (!ck(cudaMalloc(&d.B, sizeof(double) * 6 * (size_t)std::max<long long>(d.n8, 1)), "cudaMalloc B"))
         return false;
@@ -364,8 +369,9 @@ bool emit_level(int L, int nsub) {
     k_sub_begin<<<1, 1, 0, g.stream>>>(S, L, it);
     const int *gate = &S->active[L];
     const long long n5 = 5 * d.n8;
-    k_clear<<<(unsigned)std::max<long long>(1, std::min<long long>((n5 + 255) / 256, 4LL * g.nsm)), 256, 0,
-              g.stream>>>(d.C, n5, gate);
+    if (d.C != nullptr)
+      k_clear<<<(unsigned)std::max<long long>(1, std::min<long long>((n5 + 255) / 256, 4LL * g.nsm)), 256, 0,
+                g.stream>>>(d.C, n5, gate);
     if (!ck(launch_cfl(t.d_lv, L, d.n8, gate, &S->smax[L], g.nsm, g.stream), "cfl launch")) return false;
     k_sub_dt<<<1, 1, 0, g.stream>>>(S, L);
     if (has_fine && !emit_level(L + 1, nsub)) return false;
@@ -387,7 +393,8 @@ bool emit_coarse_step(int nsub) {
     for (int L = lc; L <= lf; L++) {
       const DevLevel &d = t.lev[L];
       if (!ck(cudaMemsetAsync(&S->smax[L], 0, sizeof(unsigned long long), g.stream), "memset smax")) return false;
-      if (!ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C")) return false;
+      if (d.C != nullptr && !ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C"))
+        return false;
       if (!ck(launch_cfl(t.d_lv, L, d.n8, nullptr, &S->smax[L], g.nsm, g.stream), "cfl launch")) return false;
     }
     k_batch_begin<<<1, 1, 0, g.stream>>>(S, t.d_lv, g.d_done);
@@ -693,7 +700,7 @@ int emma_hydro_set_level_state(int level, const double *host_in) {
 int emma_hydro_clean_new(int level) {
   if (!level_ok(level)) return EMMA_ST_ARG;
   const DevLevel &d = g.res.lev[level];
-  if (d.n8 == 0) return 0;
+  if (d.n8 == 0 || d.C == nullptr) return 0;
   CK(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream));
   return 0;
 }
@@ -925,7 +932,7 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   if (!ck(cudaMemcpyAsync(d.W0, g.pin, sizeof(double) * 5 * n8, cudaMemcpyHostToDevice, g.stream), "H2D W")) return 0;
   if (!ck(cudaMemcpyAsync(d.B, g.pin + 5 * n8, sizeof(double) * 6 * n8, cudaMemcpyHostToDevice, g.stream), "H2D B"))
     return 0;
-  const bool coarse = nc8 > 0 && h.reads_coarse;
+  const bool coarse = nc8 > 0 && h.reads_coarse && dc.C != nullptr;
   if (coarse) {
     if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
     pack_level(hc, 0, g.pin);

@@ -81,8 +81,16 @@ struct BrickSmem {
   using R = typename M::R;
   static constexpr bool kF64 = sizeof(R) == 8;
   static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
-  static constexpr size_t off_key = 0;                                           // u32 [kSlots]
-  static constexpr size_t off_st = a16(off_key + 4 * kSlots);                    // u8  [kBox] cell flags
+  static constexpr size_t off_args = 0;                                          // LevelArgs of the tile's level
+  static constexpr size_t off_key = a16(off_args + sizeof(LevelArgs));           // u32 [kSlots]
+  static constexpr size_t off_ob = a16(off_key + 4 * kSlots);                    // i32 [kSlots] source offset
+  static constexpr size_t off_sf = a16(off_ob + 4 * kSlots);                     // u8  [kSlots] slot flags
+  static constexpr size_t off_spm = a16(off_sf + kSlots);                        // u8  [kSlots] split mask (cell order)
+  static constexpr size_t off_cmk = a16(off_spm + kSlots);                       // u8  [kSlots] cell map
+  static constexpr size_t off_sbase = a16(off_cmk + kSlots);                     // u16 [kSlots] box cell of child 0
+  static constexpr size_t off_sbit = a16(off_sbase + 2 * kSlots);                // u8  [kSlots] brick position or 255
+  static constexpr size_t off_tbase = a16(off_sbit + kSlots);                    // u8  [kSlots] brick cell of child 0
+  static constexpr size_t off_st = a16(off_tbase + kSlots);                      // u8  [kBox] cell flags
   static constexpr size_t off_W = a16(off_st + kBox);                            // R4  [kBox] (d,u,v,w)
   static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * kBox);            // R   [kBox] p
   static constexpr size_t off_M = a16(off_Wp + sizeof(R) * kBox);                // R4  [5][kNT] slopes, predictor
@@ -118,14 +126,38 @@ __device__ __forceinline__ void ring_cell(int j, int &b, int &k, int &bin) {
   }
 }
 
+// Per-CTA slot tables (tile independent): box cell of child 0, brick position
+// bit (255 outside the brick), brick cell of child 0.
 template <class M>
-__device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs &A, const int slot, const int tile,
+__device__ __forceinline__ void slot_tables(unsigned char *smem) {
+  using SM = BrickSmem<M>;
+  uint16_t *sBase = reinterpret_cast<uint16_t *>(smem + SM::off_sbase);
+  uint8_t *sBit = smem + SM::off_sbit;
+  uint8_t *sTb = smem + SM::off_tbase;
+  for (int s = threadIdx.x; s < kSlots; s += blockDim.x) {
+    const int sz = s / (kSlotX * kSlotY), sy = (s / kSlotX) % kSlotY, sx = s % kSlotX;
+    sBase[s] = (uint16_t)(2 * sx + kBoxX * (2 * sy + kBoxY * 2 * sz));
+    const bool inner = sx >= 1 && sx <= kBrickX && sy >= 1 && sy <= kBrickY && sz >= 1 && sz <= kBrickZ;
+    sBit[s] = inner ? (uint8_t)((sx - 1) + kBrickX * ((sy - 1) + kBrickY * (sz - 1))) : (uint8_t)255;
+    sTb[s] = inner ? (uint8_t)(2 * (sx - 1) + 8 * (2 * (sy - 1) + 8 * 2 * (sz - 1))) : (uint8_t)0;
+  }
+}
+
+template <class M>
+__device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
                                            unsigned char *smem, unsigned &st) {
   using R = typename M::R;
   using SM = BrickSmem<M>;
   constexpr bool F64 = SM::kF64;
   using V = Q4<R>;
   uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key);
+  int *sOb = reinterpret_cast<int *>(smem + SM::off_ob);
+  uint8_t *sSf = smem + SM::off_sf;
+  uint8_t *sSpm = smem + SM::off_spm;
+  uint8_t *sCmk = smem + SM::off_cmk;
+  const uint16_t *sBase = reinterpret_cast<const uint16_t *>(smem + SM::off_sbase);
+  const uint8_t *sBit = smem + SM::off_sbit;
+  const uint8_t *sTb = smem + SM::off_tbase;
   uint8_t *sSt = smem + SM::off_st;
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
   R *sWp = reinterpret_cast<R *>(smem + SM::off_Wp);
@@ -136,62 +168,96 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
 
   const int tid = threadIdx.x;
-  const uint32_t mask = A.tiles[tile].mask;
+  // the level's arguments, read once per tile into shared memory
+  LevelArgs &A = *reinterpret_cast<LevelArgs *>(smem + SM::off_args);
+  static_assert(sizeof(LevelArgs) % 4 == 0, "LevelArgs copied as 32-bit words");
+  if (tid < (int)(sizeof(LevelArgs) / 4))
+    reinterpret_cast<uint32_t *>(&A)[tid] = reinterpret_cast<const uint32_t *>(gA)[tid];
+  __syncthreads();
   const long long N8 = 8LL * A.noct;
   const int tx = tid & 7, ty = (tid >> 3) & 7, tz = tid >> 6;
   const int tb = box_of(tx, ty, tz);
 
   // ------------------------------------------------------------------ P0
-  for (int i = tid; i < kSlots; i += kNT) sKey[i] = A.keys[(size_t)tile * kSlots + i];
-  __syncthreads();
-#pragma unroll 2
-  for (int i = tid; i < kBox; i += kNT) {
-    const int s = i >> 3, c = i & 7;
-    const int sz = s / (kSlotX * kSlotY), r = s - (kSlotX * kSlotY) * sz, sy = r / kSlotX, sx = r - kSlotX * sy;
-    const int b = (2 * sx + (c & 1)) + kBoxX * ((2 * sy + ((c >> 1) & 1)) + kBoxY * (2 * sz + (c >> 2)));
-    const uint32_t key = sKey[s];
-    if (key == kKeyNone) {
-      sSt[b] = 0;
-      continue;
-    }
-    const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
-    const double *src = A.W;
-    long long stride = N8, off;
-    uint8_t f = kFPresent;
-    if (kind == kKeyReal) {
-      off = 8LL * idx + c;
-      if ((A.split[idx] >> c) & 1) f |= kFSplit;
-      const unsigned ux = sx - 1, uy = sy - 1, uz = sz - 1;
-      if (ux < 4u && uy < 4u && uz < 2u && ((mask >> (ux + 4 * uy + 16 * uz)) & 1)) f |= kFTile;
-    } else if (kind == kKeyInj) {
-      f |= kFInj;
-      src = A.Wc;
-      stride = A.nc8;
-      off = idx;
-      if (src == nullptr) {  // plan/launch mismatch: never read through a null level
-        st |= kStTree;
-        src = A.W;
-        stride = N8;
-        off = 0;
+  // per slot: key, source offset, flags, split mask in cell order, cell map
+  // (0: cell c of an oct, 1: an injected cell, 2+k: mirror across face k)
+  if (tid < kSlots) {
+    const uint32_t mask = A.tiles[tile].mask;
+    const uint32_t key = A.keys[(size_t)tile * kSlots + tid];
+    uint8_t sf = 0, spm = 0, cmk = 0;
+    int ob = 0;
+    if (key != kKeyNone) {
+      const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
+      sf = kFPresent;
+      if (kind == kKeyReal) {
+        ob = 8 * (int)idx;
+        spm = A.split[idx];
+        const uint8_t bit = sBit[tid];
+        if (bit != 255 && ((mask >> bit) & 1)) sf |= kFTile;
+      } else if (kind == kKeyInj) {
+        cmk = 1;
+        if (A.Wc != nullptr) {
+          ob = (int)idx;
+          sf |= kFInj;
+        } else {
+          st |= kStTree;  // plan/launch mismatch: never read through a null level
+        }
+      } else {
+        const int k0 = (int)(kind - kKeyGhost0);
+        ob = 8 * (int)idx;
+        cmk = (uint8_t)(2 + k0);
+        const uint8_t raw = A.split[idx];
+#pragma unroll
+        for (int c = 0; c < 8; c++) spm |= (uint8_t)(((raw >> c_mirror[k0][c]) & 1) << c);
       }
-    } else {
-      const int mc = c_mirror[kind - kKeyGhost0][c];
-      off = 8LL * idx + mc;
-      if ((A.split[idx] >> mc) & 1) f |= kFSplit;
     }
-    const double v0 = __ldg(src + off), v1 = __ldg(src + stride + off), v2 = __ldg(src + 2 * stride + off);
-    const double v3 = __ldg(src + 3 * stride + off), v4 = __ldg(src + 4 * stride + off);
-    V::st(sW, b, (R)v0, (R)v1, (R)v2, (R)v3);
-    sWp[b] = (R)v4;
-    sSt[b] = f;
-    if constexpr (!F64) {
-      if (f & kFTile) {
-        const int t = (b % kBoxX - 2) + 8 * ((b / kBoxX) % kBoxY - 2) + 64 * (b / (kBoxX * kBoxY) - 2);
-        sQ[t] = v0;
-        sQ[kNT + t] = v1;
-        sQ[2 * kNT + t] = v2;
-        sQ[3 * kNT + t] = v3;
-        sQ[4 * kNT + t] = v4;
+    sKey[tid] = key;
+    sOb[tid] = ob;
+    sSf[tid] = sf;
+    sSpm[tid] = spm;
+    sCmk[tid] = cmk;
+  }
+  __syncthreads();
+  {
+    // thread tid stages child c = tid & 7 of slots tid/8 + 32 m
+    const int c = tid & 7, s0 = tid >> 3;
+    const int cb = (c & 1) + kBoxX * (((c >> 1) & 1) + kBoxY * (c >> 2));
+    const int ct = (c & 1) + 8 * (((c >> 1) & 1) + 8 * (c >> 2));
+    unsigned mir = 0;  // mirrored child of c for ghosts across faces 0..5, 3 bits each
+#pragma unroll
+    for (int k = 0; k < 6; k++) mir |= (unsigned)c_mirror[k][c] << (3 * k);
+    const double *W = A.W, *Wc = A.Wc;
+    const long long nc8 = A.nc8;
+#pragma unroll
+    for (int m = 0; m < 5; m++) {
+      if (m == 4 && tid >= kBox - 4 * kNT) break;
+      const int s = s0 + 32 * m;
+      const int b = sBase[s] + cb;
+      const uint8_t sf = sSf[s];
+      if (sf == 0) {
+        sSt[b] = 0;
+        continue;
+      }
+      const int cmk = sCmk[s];
+      const int cm = (cmk == 0) ? c : ((cmk == 1) ? 0 : (int)((mir >> (3 * (cmk - 2))) & 7));
+      const bool inj = sf & kFInj;
+      const double *p = (inj ? Wc : W) + (long long)sOb[s] + cm;
+      const long long stride = inj ? nc8 : N8;
+      const double v0 = __ldg(p), v1 = __ldg(p + stride), v2 = __ldg(p + 2 * stride);
+      const double v3 = __ldg(p + 3 * stride), v4 = __ldg(p + 4 * stride);
+      V::st(sW, b, (R)v0, (R)v1, (R)v2, (R)v3);
+      sWp[b] = (R)v4;
+      const uint8_t f = sf | (((sSpm[s] >> c) & 1) ? kFSplit : 0);
+      sSt[b] = f;
+      if constexpr (!F64) {
+        if (f & kFTile) {
+          const int t = sTb[s] + ct;
+          sQ[t] = v0;
+          sQ[kNT + t] = v1;
+          sQ[2 * kNT + t] = v2;
+          sQ[3 * kNT + t] = v3;
+          sQ[4 * kNT + t] = v4;
+        }
       }
     }
   }
@@ -484,7 +550,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       for (int k = 0; k < 6; k++) {
         const int bs = (k < 2) ? 1 : ((k < 4) ? kBoxX : kBoxX * kBoxY);
         const int b2 = (k & 1) ? tb + bs : tb - bs;
-        if (!(sSt[b2] & kFInj)) continue;
+        if (!(sSt[b2] & kFInj) || A.Cc == nullptr) continue;
         const int x2 = b2 % kBoxX, y2 = (b2 / kBoxX) % kBoxY, z2 = b2 / (kBoxX * kBoxY);
         const long long cc = sKey[(x2 >> 1) + kSlotX * ((y2 >> 1) + kSlotY * (z2 >> 1))] & 0x0FFFFFFFu;
         const double one = (k & 1) ? 1. : -1.;
@@ -512,11 +578,13 @@ template <class M>
 __global__ void __launch_bounds__(kNT, (sizeof(typename M::R) == 8) ? 1 : 3) level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
+  slot_tables<M>(smem);
+  __syncthreads();
   unsigned st = 0;
   for (int w = blockIdx.x; w < Bt.nwork; w += gridDim.x) {
     const int item = Bt.work[w];
     const int slot = item >> kWorkSlotShift, tile = item & ((1 << kWorkSlotShift) - 1);
-    level_tile<M>(Bt, Bt.lv[slot], slot, tile, smem, st);
+    level_tile<M>(Bt, Bt.lv + slot, slot, tile, smem, st);
     __syncthreads();
   }
   if (st) atomicOr(Bt.status, st);
