@@ -219,44 +219,67 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   }
   __syncthreads();
   {
-    // thread tid stages child c = tid & 7 of slots tid/8 + 32 m
-    const int c = tid & 7, s0 = tid >> 3;
-    const int cb = (c & 1) + kBoxX * (((c >> 1) & 1) + kBoxY * (c >> 2));
-    const int ct = (c & 1) + 8 * (((c >> 1) & 1) + 8 * (c >> 2));
-    unsigned mir = 0;  // mirrored child of c for ghosts across faces 0..5, 3 bits each
+    // Thread tid stages the pair q = tid & 3 of x-neighbour children (2q, 2q+1)
+    // of slots tid/4 + 64 m, two cells per 16-byte load.  Ghost children come
+    // from one pair of the boundary oct too (the mirror maps keep x-pairs).
+    const int q = tid & 3, s0 = tid >> 2, c0 = 2 * q;
+    const int cb = kBoxX * ((q & 1) + kBoxY * (q >> 1));
+    const int ct = 8 * ((q & 1) + 8 * (q >> 1));
+    unsigned mir = 0;  // per ghost face k, 4 bits: source pair, element of child c0, of child c0+1
 #pragma unroll
-    for (int k = 0; k < 6; k++) mir |= (unsigned)c_mirror[k][c] << (3 * k);
+    for (int k = 0; k < 6; k++) {
+      const unsigned m0 = c_mirror[k][c0], m1 = c_mirror[k][c0 + 1];
+      mir |= ((m0 >> 1) | ((m0 & 1) << 2) | ((m1 & 1) << 3)) << (4 * k);
+    }
     const double *W = A.W, *Wc = A.Wc;
     const long long nc8 = A.nc8;
 #pragma unroll
-    for (int m = 0; m < 5; m++) {
-      if (m == 4 && tid >= kBox - 4 * kNT) break;
-      const int s = s0 + 32 * m;
-      const int b = sBase[s] + cb;
+    for (int m = 0; m < 3; m++) {
+      if (m == 2 && tid >= kBox / 2 - 2 * kNT) break;
+      const int s = s0 + 64 * m;
+      const int b0 = sBase[s] + cb;
       const uint8_t sf = sSf[s];
       if (sf == 0) {
-        sSt[b] = 0;
+        sSt[b0] = 0;
+        sSt[b0 + 1] = 0;
         continue;
       }
       const int cmk = sCmk[s];
-      const int cm = (cmk == 0) ? c : ((cmk == 1) ? 0 : (int)((mir >> (3 * (cmk - 2))) & 7));
-      const bool inj = sf & kFInj;
-      const double *p = (inj ? Wc : W) + (long long)sOb[s] + cm;
-      const long long stride = inj ? nc8 : N8;
-      const double v0 = __ldg(p), v1 = __ldg(p + stride), v2 = __ldg(p + 2 * stride);
-      const double v3 = __ldg(p + 3 * stride), v4 = __ldg(p + 4 * stride);
-      V::st(sW, b, (R)v0, (R)v1, (R)v2, (R)v3);
-      sWp[b] = (R)v4;
-      const uint8_t f = sf | (((sSpm[s] >> c) & 1) ? kFSplit : 0);
-      sSt[b] = f;
+      double x0[5], x1[5];
+      if (cmk == 1) {  // injected coarser cell: one value for both children
+        const bool inj = sf & kFInj;
+        const double *p = (inj ? Wc : W) + (long long)sOb[s];
+        const long long stride = inj ? nc8 : N8;
+#pragma unroll
+        for (int v = 0; v < 5; v++) x0[v] = x1[v] = __ldg(p + v * stride);
+      } else {
+        unsigned code = (unsigned)q | (1u << 3);  // pair q, elements 0 and 1
+        if (cmk >= 2) code = (mir >> (4 * (cmk - 2))) & 15u;
+        const double *p = W + (long long)sOb[s] + 2 * (code & 3);
+        const bool e0 = (code >> 2) & 1, e1 = (code >> 3) & 1;
+#pragma unroll
+        for (int v = 0; v < 5; v++) {
+          const double2 x = __ldg(reinterpret_cast<const double2 *>(p + v * N8));
+          x0[v] = e0 ? x.y : x.x;
+          x1[v] = e1 ? x.y : x.x;
+        }
+      }
+      V::st(sW, b0, (R)x0[0], (R)x0[1], (R)x0[2], (R)x0[3]);
+      V::st(sW, b0 + 1, (R)x1[0], (R)x1[1], (R)x1[2], (R)x1[3]);
+      sWp[b0] = (R)x0[4];
+      sWp[b0 + 1] = (R)x1[4];
+      const uint8_t spm = sSpm[s];
+      const uint8_t f0 = sf | (((spm >> c0) & 1) ? kFSplit : 0), f1 = sf | (((spm >> (c0 + 1)) & 1) ? kFSplit : 0);
+      sSt[b0] = f0;
+      sSt[b0 + 1] = f1;
       if constexpr (!F64) {
-        if (f & kFTile) {
+        if (sf & kFTile) {
           const int t = sTb[s] + ct;
-          sQ[t] = v0;
-          sQ[kNT + t] = v1;
-          sQ[2 * kNT + t] = v2;
-          sQ[3 * kNT + t] = v3;
-          sQ[4 * kNT + t] = v4;
+#pragma unroll
+          for (int v = 0; v < 5; v++) {
+            sQ[v * kNT + t] = x0[v];
+            sQ[v * kNT + t + 1] = x1[v];
+          }
         }
       }
     }
