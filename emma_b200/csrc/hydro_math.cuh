@@ -264,8 +264,9 @@ struct MathF32 {
   static __device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
 
   static __device__ __forceinline__ float limit(float m, float p) {
-    // minmod with beta = 1: 0 if signs differ, else the smaller magnitude
-    return (p > 0.f) ? fmaxf(0.f, fminf(m, p)) : fminf(0.f, fmaxf(m, p));
+    // minmod with beta = 1: 0 if signs differ, else the smaller magnitude, as the
+    // median of (0, m, p): four min/max operations, no compare
+    return fmaxf(fminf(m, p), fminf(fmaxf(m, p), 0.f));
   }
 
   static __device__ __forceinline__ void muscl(const float q0[5], const float qm[3][5], const float qp[3][5],
@@ -313,7 +314,7 @@ struct MathF32 {
     W[6] = sqrtf(G * W[4] * W[5]);
   }
 
-  static __device__ __noinline__ float pstar_exact(float dL, float uL, float pL, float aL, float dR, float uR,
+  static __device__ __forceinline__ float pstar_exact(float dL, float uL, float pL, float aL, float dR, float uR,
                                                    float pR, float aR, float *u) {
     // Newton iteration on the exact two-rarefaction/shock function (Toro sec. 4.3)
     const float g1 = (G - 1.f) / (2.f * G), g2 = (G + 1.f) / (2.f * G);
