@@ -116,11 +116,14 @@ def build_config(name):
 
 def traffic_per_cell(config, precision):
     """DRAM bytes per cell-update of the level kernel from the committed ncu summary, if any."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+    p = os.path.join(ROOT, "profiles", "traffic.txt")
     if not os.path.exists(p):
         return None
-    d = json.load(open(p))
-    return d.get(f"{config}/{precision}")
+    for line in open(p):
+        f = line.split()
+        if f and not f[0].startswith("#") and f[0] == f"{config}/{precision}":
+            return float(f[1])
+    return None
 
 
 def graph_kernel_count(cfg, tree):
