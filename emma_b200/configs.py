@@ -190,6 +190,23 @@ def _balance_marks(t, lev, mark):
     return g[tuple(ijk.T)]
 
 
+def _check_rule(t, lev, mark):
+    """Cancel the marks of cells whose oct lacks one of its 26 neighbour octs at
+    this level, as the reference's L_check_rule does (src/amr.c:746-868: the
+    face, edge and corner neighbours of the oct must all exist)."""
+    n = 2 ** (lev - 1)
+    ijk = np.rint(t.oct_xyz(lev) * n).astype(np.int64) % n
+    occ = np.zeros((n, n, n), bool)
+    occ[tuple(ijk.T)] = True
+    ok = occ.copy()
+    for dx in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            for dz in (-1, 0, 1):
+                if dx or dy or dz:
+                    ok &= np.roll(occ, (dx, dy, dz), axis=(0, 1, 2))
+    return mark & np.repeat(ok[tuple(ijk.T)], 8)
+
+
 def cosmo(base=7, lmax=10, seed=SEED, sigma=None, steps=20, target_cells=(5e6, 1e7)):
     cfg = Config("cosmo", base, lmax, steps)
     n = 2 ** base
@@ -223,7 +240,7 @@ def cosmo(base=7, lmax=10, seed=SEED, sigma=None, steps=20, target_cells=(5e6, 1
         for lev in range(base, lmax):
             c = t.cell_centres(lev)
             mark = rho_at(c) > 8.0
-            mark = _balance_marks(t, lev, mark)
+            mark = _check_rule(t, lev, _balance_marks(t, lev, mark))
             t.refine(lev, mark)
         # velocities from the potential of the same field, phi_k = -delta_k / k^2
         k1 = np.fft.fftfreq(n, d=1.0 / n) * 2 * np.pi
