@@ -16,8 +16,10 @@
 #include "schedule.h"
 
 namespace emma {
-cudaError_t launch_level_fp64(const BatchArgs &a, int nsm, cudaStream_t s);
-cudaError_t launch_level_f32(const BatchArgs &a, int nsm, cudaStream_t s);
+cudaError_t launch_level_fp64(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
+                              int *occupancy);
+cudaError_t launch_level_f32(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
+                             int *occupancy);
 cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *gate, unsigned long long *out, int nsm,
                        cudaStream_t s);
 }  // namespace emma
@@ -38,6 +40,11 @@ struct DevLevel {
   TileDesc *tiles = nullptr;
   uint32_t *keys = nullptr;
   int *work = nullptr;  // (L << 24) | tile for every tile of the level
+  int shape = 0;        // brick shape of the plan (kShapes)
+  int ctas = 0;         // CTAs per SM of its launches (0: the occupancy limit)
+  // autotuner record: chosen shape/CTAs and the swept times (ms per launch, 0 = not run)
+  bool tuned = false;
+  double sweep_ms[kNumShapes][4] = {};
 };
 
 struct TimedLaunch {
@@ -198,6 +205,7 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     d.n8 = 8LL * h.noct;
     d.leaf = h.leaf;
     d.ntiles = (int)h.tiles.size();
+    d.shape = h.shape;
     const size_t bytes = sizeof(double) * 5 * (size_t)std::max<long long>(d.n8, 1);
     if (!ck(cudaMalloc(&d.W0, bytes), "cudaMalloc W")) return false;
     if (!ck(cudaMalloc(&d.W1, bytes), "cudaMalloc Wn")) return false;
@@ -232,6 +240,7 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     a.child = d.child;
     a.tiles = d.tiles;
     a.keys = d.keys;
+    a.shape = h.shape;
     a.dx = std::pow(0.5, L);
     a.ntiles = d.ntiles;
     a.wait_slot = -1;
@@ -268,7 +277,8 @@ inline void finish_prims(struct Wtype &W) {
   W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
 }
 
-bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, long long cells) {
+bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, long long cells, unsigned shapes,
+                  int ctas) {
   BatchArgs a;
   a.lv = d_lv;
   a.work = work;
@@ -286,8 +296,9 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
     tl.b = get_event();
     cudaEventRecord(tl.a, g.stream);
   }
-  cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED) ? launch_level_f32(a, g.nsm, g.stream)
-                                                       : launch_level_fp64(a, g.nsm, g.stream);
+  cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED)
+                      ? launch_level_f32(a, shapes, g.nsm, ctas, g.stream, nullptr)
+                      : launch_level_fp64(a, shapes, g.nsm, ctas, g.stream, nullptr);
   if (nwork > 0) g.kernel_launches++;
   if (timed) {
     cudaEventRecord(tl.b, g.stream);
@@ -376,7 +387,7 @@ bool emit_level(int L, int nsub) {
     k_sub_dt<<<1, 1, 0, g.stream>>>(S, L);
     if (has_fine && !emit_level(L + 1, nsub)) return false;
     k_sub_prelaunch<<<1, 1, 0, g.stream>>>(S, t.d_lv, L, has_fine ? 1 : 0);
-    if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf)) return false;
+    if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf, 1u << d.shape, d.ctas)) return false;
     k_sub_end<<<1, 1, 0, g.stream>>>(S, t.d_lv, L);
     if (!ck(cudaGetLastError(), "schedule kernel")) return false;
   }
@@ -399,8 +410,17 @@ bool emit_coarse_step(int nsub) {
     }
     k_batch_begin<<<1, 1, 0, g.stream>>>(S, t.d_lv, g.d_done);
     long long cells = 0;
-    for (int L = lc; L <= lf; L++) cells += t.lev[L].leaf;
-    if (!launch_batch(t.d_lv, g.d_work_all, g.nwork_all, nullptr, cells)) return false;
+    unsigned shapes = 0;
+    int ctas = 0, most = -1;
+    for (int L = lc; L <= lf; L++) {
+      cells += t.lev[L].leaf;
+      shapes |= 1u << t.lev[L].shape;
+      if (t.lev[L].ntiles > most) {  // CTAs per SM tuned for the level with the most tiles
+        most = t.lev[L].ntiles;
+        ctas = t.lev[L].ctas;
+      }
+    }
+    if (!launch_batch(t.d_lv, g.d_work_all, g.nwork_all, nullptr, cells, shapes, ctas)) return false;
     k_batch_end<<<1, 1, 0, g.stream>>>(S, t.d_lv);
     return ck(cudaGetLastError(), "schedule kernel");
   }
@@ -570,6 +590,141 @@ int emma_hydro_set_stream(void *stream) {
 }
 
 // ------------------------------------------------------------ resident path
+// Brick shape requested by the options: -1 = autotuned, else an index into kShapes.
+int requested_shape(int tile_octs) {
+  if (tile_octs == 0) return -1;
+  for (int i = 0; i < kNumShapes; i++)
+    if (kShapes[i].octs() == tile_octs) return i;
+  return -2;
+}
+
+// Autotuner.  For every level of the resident tree it times single-level
+// launches of the level kernel on the level's own state (dt = 0: the arithmetic
+// of a real step, no change of state) for each candidate brick shape (4x4x2
+// octs x 1 brick, 2x2x2 octs x 4 bricks: the stencil-batch size and octs per
+// tile) and each number of co-resident CTAs per SM (1 .. occupancy: how many
+// tiles are staged in flight per SM), and keeps the fastest.  Complete levels
+// only try the 4x4x2 brick (every brick is full).  Side effects of the trial
+// launches (corrections added to the coarser level, completion counters,
+// status bits) are undone afterwards.
+bool autotune_tree(Tree &t, int shape_req) {
+  unsigned status0 = 0;
+  if (!ck(cudaStreamSynchronize(g.stream), "sync") ||
+      !ck(cudaMemcpy(&status0, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost), "status"))
+    return false;
+  const bool timing0 = g.timing;
+  const long long launches0 = g.kernel_launches;
+  g.timing = false;
+  cudaEvent_t e0 = get_event(), e1 = get_event();
+  bool ok = true;
+  for (int L = t.lcoarse; L <= t.lmax && ok; L++) {
+    DevLevel &d = t.lev[L];
+    HostLevel &h = t.host.lev[L];
+    if (d.ntiles == 0) continue;
+    const bool complete = h.noct == (1LL << (3 * (L - 1)));
+    double best = 0;
+    int best_shape = d.shape, best_ctas = 0;
+    for (int s = 0; s < kNumShapes && ok; s++) {
+      if (shape_req >= 0 && s != shape_req) continue;
+      if (shape_req < 0 && complete && s != 0) continue;
+      // the candidate plan on the device (the current one, or a re-plan)
+      TileDesc *tiles = d.tiles;
+      uint32_t *keys = d.keys;
+      int *work = d.work;
+      int ntiles = d.ntiles;
+      HostLevel alt;
+      if (s != d.shape) {
+        std::string err;
+        alt = h;
+        HostLevel saved = h;
+        h = alt;
+        const int rc = replan_level(t.host, L, s, err);
+        alt = h;
+        h = saved;
+        if (rc != 0) continue;  // shape not plannable here: skip the candidate
+        ntiles = (int)alt.tiles.size();
+        std::vector<int> wl((size_t)ntiles);
+        for (int i = 0; i < ntiles; i++) wl[i] = (L << kWorkSlotShift) | i;
+        if (!upload_vec(&tiles, alt.tiles) || !upload_vec(&keys, alt.keys) || !upload_vec(&work, wl)) {
+          ok = false;
+          break;
+        }
+      }
+      LevelArgs *slot = t.d_lv + L;
+      const int shape_i = s;
+      ok = ck(cudaMemcpyAsync(&slot->tiles, &tiles, sizeof(tiles), cudaMemcpyHostToDevice, g.stream), "tune") &&
+           ck(cudaMemcpyAsync(&slot->keys, &keys, sizeof(keys), cudaMemcpyHostToDevice, g.stream), "tune") &&
+           ck(cudaMemcpyAsync(&slot->shape, &shape_i, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune") &&
+           ck(cudaMemcpyAsync(&slot->ntiles, &ntiles, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune");
+      k_bind_level<<<1, 1, 0, g.stream>>>(t.d_lv, L, t.lcoarse, t.lmax, 0.);
+      int occ = 0;
+      BatchArgs probe{};
+      if (ok)
+        ok = ck((g.opt.precision == EMMA_PREC_MIXED) ? launch_level_f32(probe, 1u << s, g.nsm, 0, g.stream, &occ)
+                                                      : launch_level_fp64(probe, 1u << s, g.nsm, 0, g.stream, &occ),
+                "occupancy");
+      for (int c = 1; ok && c <= std::min(occ, 4); c++) {
+        double ms = 0;
+        for (int rep = 0; rep < 4 && ok; rep++) {  // one warm-up, three timed
+          ok = ck(cudaEventRecord(e0, g.stream), "event");
+          ok = ok && launch_batch(t.d_lv, work, ntiles, nullptr, 0, 1u << s, c);
+          ok = ok && ck(cudaEventRecord(e1, g.stream), "event") && ck(cudaEventSynchronize(e1), "event");
+          float f = 0;
+          if (ok && rep > 0 && cudaEventElapsedTime(&f, e0, e1) == cudaSuccess) ms += f / 3.;
+        }
+        d.sweep_ms[s][c - 1] = ms;
+        if (ok && (best == 0 || ms < best)) {
+          best = ms;
+          best_shape = s;
+          best_ctas = c;
+        }
+      }
+      if (s != d.shape) {
+        if (ok && best_shape == s) {
+          // the re-plan wins so far: it becomes the level's plan
+          cudaStreamSynchronize(g.stream);
+          cudaFree(d.tiles);
+          cudaFree(d.keys);
+          cudaFree(d.work);
+          d.tiles = tiles;
+          d.keys = keys;
+          d.work = work;
+          d.ntiles = ntiles;
+          d.shape = s;
+          h = alt;
+        } else {
+          cudaStreamSynchronize(g.stream);
+          cudaFree(tiles);
+          cudaFree(keys);
+          cudaFree(work);
+        }
+      }
+    }
+    // bind the kept plan
+    LevelArgs *slot = t.d_lv + L;
+    ok = ok && ck(cudaMemcpyAsync(&slot->tiles, &d.tiles, sizeof(d.tiles), cudaMemcpyHostToDevice, g.stream), "tune") &&
+         ck(cudaMemcpyAsync(&slot->keys, &d.keys, sizeof(d.keys), cudaMemcpyHostToDevice, g.stream), "tune") &&
+         ck(cudaMemcpyAsync(&slot->shape, &d.shape, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune") &&
+         ck(cudaMemcpyAsync(&slot->ntiles, &d.ntiles, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune") &&
+         ck(cudaStreamSynchronize(g.stream), "tune");
+    d.ctas = best_ctas;
+    d.tuned = ok;
+  }
+  // undo the trial launches: corrections, completion counters, status
+  for (int L = t.lcoarse; L <= t.lmax && ok; L++) {
+    const DevLevel &d = t.lev[L];
+    if (d.C != nullptr) ok = ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C");
+  }
+  ok = ok && ck(cudaMemsetAsync(g.d_done, 0, sizeof(unsigned) * kMaxLevels, g.stream), "memset done") &&
+       ck(cudaMemcpyAsync(g.d_status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice, g.stream), "status") &&
+       ck(cudaStreamSynchronize(g.stream), "sync");
+  g.free_events.push_back(e0);
+  g.free_events.push_back(e1);
+  g.timing = timing0;
+  g.kernel_launches = launches0;
+  return ok;
+}
+
 int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int rank) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
   if (firstoct == nullptr || lcoarse < 2 || lmax < lcoarse || lmax >= kMaxLevels) {
@@ -583,18 +738,19 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
   g.d_work_all = nullptr;
   g.nwork_all = 0;
   std::string err;
-  int rc = build_host_tree(firstoct, lcoarse, lmax, rank, g.opt.trans_flags, lcoarse, lmax, g.res.host, err);
+  const int shape_req = requested_shape(g.opt.tile_octs);
+  if (shape_req < -1) {
+    fail(EMMA_ST_ARG, "tile_octs must be 0 (autotuned), 32 or 8");
+    return EMMA_ST_ARG;
+  }
+  std::vector<int> shapes((size_t)lmax + 1, shape_req);
+  int rc = build_host_tree(firstoct, lcoarse, lmax, rank, g.opt.trans_flags, lcoarse, lmax, g.res.host, err,
+                           shapes.data());
   if (rc != 0) {
     fail((unsigned)rc, err);
     return rc;
   }
   if (!alloc_tree(g.res.host, g.res, false)) return EMMA_ST_CUDA;
-  // batched work list: finest level first, each level's tiles in order
-  std::vector<int> all;
-  for (int L = lmax; L >= lcoarse; L--)
-    for (int i = 0; i < g.res.lev[L].ntiles; i++) all.push_back((L << kWorkSlotShift) | i);
-  if (!upload_vec(&g.d_work_all, all)) return EMMA_ST_CUDA;
-  g.nwork_all = (int)all.size();
   // schedule constants
   SchedState &h = *g.h_S;
   std::memset(&h, 0, sizeof(h));
@@ -606,7 +762,16 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
   h.nsub = 2;
   for (int L = 0; L < kMaxLevels; L++) h.dx[L] = std::pow(0.5, L);
   CK(cudaMemcpy(g.d_S, &h, sizeof(SchedState), cudaMemcpyHostToDevice));
-  return emma_hydro_fields_upload(firstoct);
+  rc = emma_hydro_fields_upload(firstoct);
+  if (rc != 0) return rc;
+  if (!autotune_tree(g.res, shape_req)) return EMMA_ST_CUDA;
+  // batched work list: finest level first, each level's tiles in order
+  std::vector<int> all;
+  for (int L = lmax; L >= lcoarse; L--)
+    for (int i = 0; i < g.res.lev[L].ntiles; i++) all.push_back((L << kWorkSlotShift) | i);
+  if (!upload_vec(&g.d_work_all, all)) return EMMA_ST_CUDA;
+  g.nwork_all = (int)all.size();
+  return 0;
 }
 
 int emma_hydro_fields_upload(struct OCT **firstoct) {
@@ -731,7 +896,7 @@ int emma_hydro_advance_level(int level, double dt) {
   if (d.noct == 0) return 0;
   k_bind_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, g.res.lcoarse, g.res.lmax, dt);
   CK(cudaGetLastError());
-  if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf)) return EMMA_ST_CUDA;
+  if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return EMMA_ST_CUDA;
   k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
   CK(cudaGetLastError());
   g.updates += d.leaf;
@@ -815,6 +980,17 @@ void emma_hydro_reset_counters(void) {
   g.launches.clear();
 }
 
+int emma_hydro_tuning(int level, int *tile_octs, int *ctas_per_sm, double *sweep_ms) {
+  if (!level_ok(level)) return EMMA_ST_ARG;
+  const DevLevel &d = g.res.lev[level];
+  if (tile_octs) *tile_octs = kShapes[d.shape].octs();
+  if (ctas_per_sm) *ctas_per_sm = d.ctas;
+  if (sweep_ms)
+    for (int s = 0; s < kNumShapes; s++)
+      for (int c = 0; c < 4; c++) sweep_ms[4 * s + c] = d.sweep_ms[s][c];
+  return d.tuned ? 0 : EMMA_ST_ARG;
+}
+
 int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cells) {
   if (!g.ready) return EMMA_ST_ARG;
   CK(cudaStreamSynchronize(g.stream));
@@ -849,7 +1025,8 @@ int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int tran
     long long ms = 0, mh = 0;
     for (size_t t = 0; t < h.tiles.size(); t++) {
       long long s = 0;
-      for (int i = 0; i < kSlots; i++) s += (h.keys[t * kSlots + i] != kKeyNone);
+      const int ns = kShapes[h.shape].tile_slots();
+      for (int i = 0; i < ns; i++) s += (h.keys[t * ns + i] != kKeyNone);
       ms = std::max(ms, s);
       mh += s;
     }
@@ -907,7 +1084,9 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
     free_tree(g.drop);
     g.drop_level = -1;
     std::string err;
-    int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, g.drop.host, err);
+    std::vector<int> shapes((size_t)hi + 1, std::max(-1, requested_shape(g.opt.tile_octs)));
+    int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, g.drop.host, err,
+                             shapes.data());
     if (rc != 0) {
       fail((unsigned)rc, err);
       return 0;
@@ -956,6 +1135,7 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   a.child = d.child;
   a.tiles = d.tiles;
   a.keys = d.keys;
+  a.shape = h.shape;
   a.dt = dtnew;
   a.dx = std::pow(0.5, level);
   a.ntiles = d.ntiles;
@@ -963,7 +1143,7 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   a.leaf = d.leaf;
   k_set_args<<<1, 1, 0, g.stream>>>(g.drop.d_lv, level, a);
   if (!ck(cudaGetLastError(), "k_set_args")) return 0;
-  if (!launch_batch(g.drop.d_lv, d.work, d.ntiles, nullptr, d.leaf)) return 0;
+  if (!launch_batch(g.drop.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return 0;
   // download the level's new state into fieldnew (leaf cells)
   if (!ck(cudaMemcpyAsync(g.pin, d.W1, sizeof(double) * 5 * n8, cudaMemcpyDeviceToHost, g.stream), "D2H Wn")) return 0;
   if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;

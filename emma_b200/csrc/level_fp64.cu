@@ -5,26 +5,9 @@
 
 namespace emma {
 
-using KF64 = BrickSmem<MathF64>;
-
-size_t level_smem_fp64() { return KF64::bytes; }
-
-// Persistent launch of a work list: grid = co-resident CTAs (occupancy x SMs).
-cudaError_t launch_level_fp64(const BatchArgs &a, int nsm, cudaStream_t s) {
-  static int blocks_per_sm = 0;
-  auto k = level_batch_kernel<MathF64>;
-  if (blocks_per_sm == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)KF64::bytes);
-    if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks_per_sm, k, kNT, KF64::bytes);
-    if (e != cudaSuccess) return e;
-    if (blocks_per_sm < 1) return cudaErrorInvalidConfiguration;
-  }
-  if (a.nwork == 0) return cudaSuccess;
-  int grid = blocks_per_sm * nsm;
-  if (grid > a.nwork) grid = a.nwork;
-  k<<<grid, kNT, KF64::bytes, s>>>(a);
-  return cudaGetLastError();
+cudaError_t launch_level_fp64(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
+                              int *occupancy) {
+  return launch_level_any<MathF64>(a, shapes, nsm, ctas_per_sm, s, occupancy);
 }
 
 }  // namespace emma

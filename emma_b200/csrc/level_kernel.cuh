@@ -1,12 +1,13 @@
 // level_kernel.cuh -- the hydro level advance on the GPU, one CTA per tile.
 //
-// A tile is a brick of 4x4x2 oct positions of one level (8x8x4 cells, one
-// thread per cell) holding at least one oct of the level.  Each CTA:
-//   P0  stages a 6x6x4-slot box (the brick and a ring of one oct) of "virtual
-//       octs": a real oct of the level, a coarser leaf cell injected into 8
-//       cells as the reference's gather does, or a transmissive mirror ghost;
-//       only the slots a stencil reads (faces and edges of the tile octs) are
-//       filled.  Neighbours are then fixed offsets in the 12x12x8-cell box;
+// A tile is NB bricks of BX x BY x BZ oct positions of one level (one thread
+// per brick cell, 256 per CTA) holding at least one oct of the level.  For each
+// brick the CTA:
+//   P0  stages a (BX+2) x (BY+2) x (BZ+2)-slot box (the brick and a ring of one
+//       oct) of "virtual octs": a real oct of the level, a coarser leaf cell
+//       injected into 8 cells as the reference's gather does, or a transmissive
+//       mirror ghost; only the slots a stencil reads (faces and edges of the
+//       tile octs) are filled.  Neighbours are then fixed offsets in the box;
 //   P1  MUSCL-Hancock once per needed cell: slopes + predictor of every brick
 //       cell that is a leaf of the tile or borders one, and for every ring cell
 //       face-adjacent to the brick the one face state it contributes;
@@ -70,94 +71,140 @@ __device__ __forceinline__ bool f_tileleaf(uint8_t f) {
   return (f & (kFPresent | kFSplit | kFTile)) == (kFPresent | kFTile);
 }
 
-// Shared memory of one brick.  Brick cell t = x + 8 (y + 8 z) sits at box cell
-// (x+2) + 12 ((y+2) + 12 (z+2)).  Ring cell j (face-adjacent to the brick):
-// j < 32 -x side (y + 8 z), 32.. +x side, 64.. -y (x + 8 z), 96.. +y,
-// 128.. -z (x + 8 y), 192.. +z.  Face arrays, -d face of brick cell (x,y,z):
-// x: x + 9 (y + 8 z), y: 288 + x + 8 (y + 9 z), z: 576 + x + 8 (y + 8 z),
-// with coordinate 8 (x, y) or 4 (z) for the + faces on the brick boundary.
-template <class M>
-struct BrickSmem {
+// Geometry of a tile of NB bricks of BX x BY x BZ octs.  Brick cell
+// t = x + CX (y + CY z) sits at box cell (x+2) + XX ((y+2) + XY (z+2)).  Ring cell
+// j (face-adjacent to the brick): -x side (y + CY z), +x side, -y (x + CX z), +y,
+// -z (x + CX y), +z.  Face arrays, -d face of brick cell (x,y,z):
+// x: x + (CX+1)(y + CY z), y: FX + x + CX (y + (CY+1) z), z: FX + FY + x + CX (y + CY z),
+// with coordinate CX, CY or CZ for the + faces on the brick boundary.
+template <int BX, int BY, int BZ, int NB>
+struct Geom {
+  static constexpr int kNB = NB, kOcts = BX * BY * BZ;
+  static constexpr int CX = 2 * BX, CY = 2 * BY, CZ = 2 * BZ, kCells = CX * CY * CZ;
+  static constexpr int SX = BX + 2, SY = BY + 2, SZ = BZ + 2, kSlots = SX * SY * SZ;
+  static constexpr int XX = 2 * SX, XY = 2 * SY, XZ = 2 * SZ, kBox = XX * XY * XZ, XS = XX * XY;
+  static constexpr int kPX = CY * CZ, kPY = CX * CZ, kPZ = CX * CY;  // cells of one face layer
+  static constexpr int kRing = 2 * (kPX + kPY + kPZ), kPlus = kPX + kPY + kPZ;
+  static constexpr int kFX = (CX + 1) * CY * CZ, kFY = CX * (CY + 1) * CZ, kFZ = CX * CY * (CZ + 1);
+  static constexpr int kFaces = kFX + kFY + kFZ;
+  static_assert(NB * kCells == kThreads, "one thread per brick cell");
+  static_assert(NB * kOcts <= 32, "tile mask is 32 bits");
+
+  static __device__ __forceinline__ int box_of(int x, int y, int z) { return (x + 2) + XX * ((y + 2) + XY * (z + 2)); }
+  static __device__ __forceinline__ void cell_of(int t, int &x, int &y, int &z) {
+    x = t % CX;
+    y = (t / CX) % CY;
+    z = t / (CX * CY);
+  }
+  // ring cell j: box cell, its face k toward the brick and the brick cell across it
+  static __device__ __forceinline__ void ring_cell(int j, int &b, int &k, int &bin) {
+    if (j < 2 * kPX) {
+      const int side = j >= kPX, i = j - side * kPX, y = i % CY, z = i / CY;
+      b = (side ? CX + 2 : 1) + XX * ((y + 2) + XY * (z + 2));
+      k = side ? 0 : 1;
+      bin = b + (side ? -1 : 1);
+    } else if (j < 2 * (kPX + kPY)) {
+      int i = j - 2 * kPX;
+      const int side = i >= kPY;
+      i -= side * kPY;
+      const int x = i % CX, z = i / CX;
+      b = (x + 2) + XX * ((side ? CY + 2 : 1) + XY * (z + 2));
+      k = side ? 2 : 3;
+      bin = b + (side ? -XX : XX);
+    } else {
+      int i = j - 2 * (kPX + kPY);
+      const int side = i >= kPZ;
+      i -= side * kPZ;
+      const int x = i % CX, y = i / CX;
+      b = (x + 2) + XX * ((y + 2) + XY * (side ? CZ + 2 : 1));
+      k = side ? 4 : 5;
+      bin = b + (side ? -XS : XS);
+    }
+  }
+  // ring cell across the -d (plus = false) or +d face of brick cell (x,y,z) on the brick boundary
+  static __device__ __forceinline__ int ring_index(int d, bool plus, int x, int y, int z) {
+    if (d == 0) return (plus ? kPX : 0) + y + CY * z;
+    if (d == 1) return 2 * kPX + (plus ? kPY : 0) + x + CX * z;
+    return 2 * (kPX + kPY) + (plus ? kPZ : 0) + x + CX * y;
+  }
+  static __device__ __forceinline__ int face_index(int d, int x, int y, int z) {
+    if (d == 0) return x + (CX + 1) * (y + CY * z);
+    if (d == 1) return kFX + x + CX * (y + (CY + 1) * z);
+    return kFX + kFY + x + CX * (y + CY * z);
+  }
+};
+using GeomA = Geom<4, 4, 2, 1>;  // kShapes[0]
+using GeomB = Geom<2, 2, 2, 4>;  // kShapes[1]
+static_assert(GeomA::kOcts == 32 && GeomB::kOcts == 8, "shapes match kShapes");
+
+// Per-CTA slot tables of both shapes (tile independent), at the start of
+// shared memory: box cell of child 0, brick position bit (255 outside the
+// brick), brick cell of child 0.
+template <class G>
+struct SlotTab {
+  static constexpr size_t bytes = ((size_t)G::kSlots * 4 + 15) & ~size_t(15);
+};
+constexpr size_t kTabOffB = SlotTab<GeomA>::bytes;
+constexpr size_t kTabBytes = kTabOffB + SlotTab<GeomB>::bytes;
+
+template <class G>
+__device__ __forceinline__ void slot_tables(unsigned char *tab) {
+  uint16_t *sBase = reinterpret_cast<uint16_t *>(tab);
+  uint8_t *sBit = tab + 2 * G::kSlots;
+  uint8_t *sTb = tab + 3 * G::kSlots;
+  for (int s = threadIdx.x; s < G::kSlots; s += blockDim.x) {
+    const int sz = s / (G::SX * G::SY), sy = (s / G::SX) % G::SY, sx = s % G::SX;
+    sBase[s] = (uint16_t)(2 * sx + G::XX * (2 * sy + G::XY * 2 * sz));
+    const bool inner = sx >= 1 && sx <= G::SX - 2 && sy >= 1 && sy <= G::SY - 2 && sz >= 1 && sz <= G::SZ - 2;
+    sBit[s] = inner ? (uint8_t)((sx - 1) + (G::SX - 2) * ((sy - 1) + (G::SY - 2) * (sz - 1))) : (uint8_t)255;
+    sTb[s] = inner ? (uint8_t)(2 * (sx - 1) + G::CX * (2 * (sy - 1) + G::CY * 2 * (sz - 1))) : (uint8_t)0;
+  }
+}
+
+// Shared memory of one tile, after the slot tables.
+template <class M, class G>
+struct TileSmem {
   using R = typename M::R;
   static constexpr bool kF64 = sizeof(R) == 8;
+  static constexpr int NS = G::kNB * G::kSlots, NBOX = G::kNB * G::kBox, NRING = G::kNB * G::kRing;
+  static constexpr int NF = G::kNB * G::kFaces;
   static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
-  static constexpr size_t off_args = 0;                                          // LevelArgs of the tile's level
-  static constexpr size_t off_key = a16(off_args + sizeof(LevelArgs));           // u32 [kSlots]
-  static constexpr size_t off_ob = a16(off_key + 4 * kSlots);                    // i32 [kSlots] source offset
-  static constexpr size_t off_sf = a16(off_ob + 4 * kSlots);                     // u8  [kSlots] slot flags
-  static constexpr size_t off_spm = a16(off_sf + kSlots);                        // u8  [kSlots] split mask (cell order)
-  static constexpr size_t off_cmk = a16(off_spm + kSlots);                       // u8  [kSlots] cell map
-  static constexpr size_t off_sbase = a16(off_cmk + kSlots);                     // u16 [kSlots] box cell of child 0
-  static constexpr size_t off_sbit = a16(off_sbase + 2 * kSlots);                // u8  [kSlots] brick position or 255
-  static constexpr size_t off_tbase = a16(off_sbit + kSlots);                    // u8  [kSlots] brick cell of child 0
-  static constexpr size_t off_st = a16(off_tbase + kSlots);                      // u8  [kBox] cell flags
-  static constexpr size_t off_W = a16(off_st + kBox);                            // R4  [kBox] (d,u,v,w)
-  static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * kBox);            // R   [kBox] p
-  static constexpr size_t off_M = a16(off_Wp + sizeof(R) * kBox);                // R4  [5][kNT] slopes, predictor
-  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 4 * 5 * kNT);         // R4  [2][kHaloCells] ring faces
-  static constexpr size_t off_Q = a16(off_HS + sizeof(R) * 4 * 2 * kHaloCells);  // f64 [5][kNT] (FP32 path)
-  static constexpr size_t q_bytes = kF64 ? 0 : sizeof(double) * 5 * kNT;
+  static constexpr size_t off_args = kTabBytes;                                // LevelArgs of the tile's level
+  static constexpr size_t off_key = a16(off_args + sizeof(LevelArgs));         // u32 [NS]
+  static constexpr size_t off_ob = a16(off_key + 4 * NS);                      // i32 [NS] source offset
+  static constexpr size_t off_sf = a16(off_ob + 4 * NS);                       // u8  [NS] slot flags
+  static constexpr size_t off_spm = a16(off_sf + NS);                          // u8  [NS] split mask (cell order)
+  static constexpr size_t off_cmk = a16(off_spm + NS);                         // u8  [NS] cell map
+  static constexpr size_t off_st = a16(off_cmk + NS);                          // u8  [NBOX] cell flags
+  static constexpr size_t off_W = a16(off_st + NBOX);                          // R4  [NBOX] (d,u,v,w)
+  static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * NBOX);          // R   [NBOX] p
+  static constexpr size_t off_M = a16(off_Wp + sizeof(R) * NBOX);              // R4  [5][kThreads]
+  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 4 * 5 * kThreads);  // R4  [2][NRING] ring faces
+  static constexpr size_t off_Q = a16(off_HS + sizeof(R) * 4 * 2 * NRING);     // f64 [5][kThreads] (FP32 path)
+  static constexpr size_t q_bytes = kF64 ? 0 : sizeof(double) * 5 * kThreads;
   // face fluxes: the FP32 path reuses the staged box, dead after reconstruction
-  static constexpr size_t off_F = kF64 ? a16(off_Q + q_bytes) : off_W;  // R4 [kFaces]
-  static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * kFaces);  // R  [kFaces]
-  static constexpr size_t bytes = kF64 ? a16(off_F1 + sizeof(R) * kFaces) : a16(off_Q + q_bytes);
-  static_assert(kF64 || off_F1 + sizeof(R) * kFaces <= off_M, "FP32 face fluxes must fit in the staged box");
+  static constexpr size_t off_F = kF64 ? a16(off_Q + q_bytes) : off_W;  // R4 [NF]
+  static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
+  static constexpr size_t bytes = kF64 ? a16(off_F1 + sizeof(R) * NF) : a16(off_Q + q_bytes);
+  static_assert(kF64 || off_F1 + sizeof(R) * NF <= off_M, "FP32 face fluxes must fit in the staged box");
 };
 
-__device__ __forceinline__ int box_of(int x, int y, int z) { return (x + 2) + kBoxX * ((y + 2) + kBoxY * (z + 2)); }
-
-// ring cell j: box cell, its face k toward the brick and the brick cell across it
-__device__ __forceinline__ void ring_cell(int j, int &b, int &k, int &bin) {
-  if (j < 64) {
-    const int side = j >> 5, y = j & 7, z = (j >> 3) & 3;
-    b = (side ? 10 : 1) + kBoxX * ((y + 2) + kBoxY * (z + 2));
-    k = side ? 0 : 1;
-    bin = b + (side ? -1 : 1);
-  } else if (j < 128) {
-    const int i = j - 64, side = i >> 5, x = i & 7, z = (i >> 3) & 3;
-    b = (x + 2) + kBoxX * ((side ? 10 : 1) + kBoxY * (z + 2));
-    k = side ? 2 : 3;
-    bin = b + (side ? -kBoxX : kBoxX);
-  } else {
-    const int i = j - 128, side = i >> 6, x = i & 7, y = (i >> 3) & 7;
-    b = (x + 2) + kBoxX * ((y + 2) + kBoxY * (side ? 6 : 1));
-    k = side ? 4 : 5;
-    bin = b + (side ? -kBoxX * kBoxY : kBoxX * kBoxY);
-  }
-}
-
-// Per-CTA slot tables (tile independent): box cell of child 0, brick position
-// bit (255 outside the brick), brick cell of child 0.
-template <class M>
-__device__ __forceinline__ void slot_tables(unsigned char *smem) {
-  using SM = BrickSmem<M>;
-  uint16_t *sBase = reinterpret_cast<uint16_t *>(smem + SM::off_sbase);
-  uint8_t *sBit = smem + SM::off_sbit;
-  uint8_t *sTb = smem + SM::off_tbase;
-  for (int s = threadIdx.x; s < kSlots; s += blockDim.x) {
-    const int sz = s / (kSlotX * kSlotY), sy = (s / kSlotX) % kSlotY, sx = s % kSlotX;
-    sBase[s] = (uint16_t)(2 * sx + kBoxX * (2 * sy + kBoxY * 2 * sz));
-    const bool inner = sx >= 1 && sx <= kBrickX && sy >= 1 && sy <= kBrickY && sz >= 1 && sz <= kBrickZ;
-    sBit[s] = inner ? (uint8_t)((sx - 1) + kBrickX * ((sy - 1) + kBrickY * (sz - 1))) : (uint8_t)255;
-    sTb[s] = inner ? (uint8_t)(2 * (sx - 1) + 8 * (2 * (sy - 1) + 8 * 2 * (sz - 1))) : (uint8_t)0;
-  }
-}
-
-template <class M>
+template <class M, class G>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
-                                           unsigned char *smem, unsigned &st) {
+                                           unsigned char *smem, const unsigned char *tab, unsigned &st) {
   using R = typename M::R;
-  using SM = BrickSmem<M>;
+  using SM = TileSmem<M, G>;
   constexpr bool F64 = SM::kF64;
+  constexpr int NS = SM::NS, NRING = SM::NRING;
   using V = Q4<R>;
   uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key);
   int *sOb = reinterpret_cast<int *>(smem + SM::off_ob);
   uint8_t *sSf = smem + SM::off_sf;
   uint8_t *sSpm = smem + SM::off_spm;
   uint8_t *sCmk = smem + SM::off_cmk;
-  const uint16_t *sBase = reinterpret_cast<const uint16_t *>(smem + SM::off_sbase);
-  const uint8_t *sBit = smem + SM::off_sbit;
-  const uint8_t *sTb = smem + SM::off_tbase;
+  const uint16_t *sBase = reinterpret_cast<const uint16_t *>(tab);
+  const uint8_t *sBit = tab + 2 * G::kSlots;
+  const uint8_t *sTb = tab + 3 * G::kSlots;
   uint8_t *sSt = smem + SM::off_st;
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
   R *sWp = reinterpret_cast<R *>(smem + SM::off_Wp);
@@ -175,47 +222,53 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     reinterpret_cast<uint32_t *>(&A)[tid] = reinterpret_cast<const uint32_t *>(gA)[tid];
   __syncthreads();
   const long long N8 = 8LL * A.noct;
-  const int tx = tid & 7, ty = (tid >> 3) & 7, tz = tid >> 6;
-  const int tb = box_of(tx, ty, tz);
+  const int tn = tid / G::kCells, tt = tid - tn * G::kCells;  // brick of the tile, cell of the brick
+  int tx, ty, tz;
+  G::cell_of(tt, tx, ty, tz);
+  const int bo = tn * G::kBox;                 // this brick's box in the tile's boxes
+  const int tb = bo + G::box_of(tx, ty, tz);   // this thread's brick cell
 
   // ------------------------------------------------------------------ P0
   // per slot: key, source offset, flags, split mask in cell order, cell map
   // (0: cell c of an oct, 1: an injected cell, 2+k: mirror across face k)
-  if (tid < kSlots) {
+  {
     const uint32_t mask = A.tiles[tile].mask;
-    const uint32_t key = A.keys[(size_t)tile * kSlots + tid];
-    uint8_t sf = 0, spm = 0, cmk = 0;
-    int ob = 0;
-    if (key != kKeyNone) {
-      const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
-      sf = kFPresent;
-      if (kind == kKeyReal) {
-        ob = 8 * (int)idx;
-        spm = A.split[idx];
-        const uint8_t bit = sBit[tid];
-        if (bit != 255 && ((mask >> bit) & 1)) sf |= kFTile;
-      } else if (kind == kKeyInj) {
-        cmk = 1;
-        if (A.Wc != nullptr) {
-          ob = (int)idx;
-          sf |= kFInj;
+    for (int i = tid; i < NS; i += kThreads) {
+      const int nb = i / G::kSlots, s = i - nb * G::kSlots;
+      const uint32_t key = A.keys[(size_t)tile * NS + i];
+      uint8_t sf = 0, spm = 0, cmk = 0;
+      int ob = 0;
+      if (key != kKeyNone) {
+        const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
+        sf = kFPresent;
+        if (kind == kKeyReal) {
+          ob = 8 * (int)idx;
+          spm = A.split[idx];
+          const uint8_t bit = sBit[s];
+          if (bit != 255 && ((mask >> (nb * G::kOcts + bit)) & 1)) sf |= kFTile;
+        } else if (kind == kKeyInj) {
+          cmk = 1;
+          if (A.Wc != nullptr) {
+            ob = (int)idx;
+            sf |= kFInj;
+          } else {
+            st |= kStTree;  // plan/launch mismatch: never read through a null level
+          }
         } else {
-          st |= kStTree;  // plan/launch mismatch: never read through a null level
-        }
-      } else {
-        const int k0 = (int)(kind - kKeyGhost0);
-        ob = 8 * (int)idx;
-        cmk = (uint8_t)(2 + k0);
-        const uint8_t raw = A.split[idx];
+          const int k0 = (int)(kind - kKeyGhost0);
+          ob = 8 * (int)idx;
+          cmk = (uint8_t)(2 + k0);
+          const uint8_t raw = A.split[idx];
 #pragma unroll
-        for (int c = 0; c < 8; c++) spm |= (uint8_t)(((raw >> c_mirror[k0][c]) & 1) << c);
+          for (int c = 0; c < 8; c++) spm |= (uint8_t)(((raw >> c_mirror[k0][c]) & 1) << c);
+        }
       }
+      sKey[i] = key;
+      sOb[i] = ob;
+      sSf[i] = sf;
+      sSpm[i] = spm;
+      sCmk[i] = cmk;
     }
-    sKey[tid] = key;
-    sOb[tid] = ob;
-    sSf[tid] = sf;
-    sSpm[tid] = spm;
-    sCmk[tid] = cmk;
   }
   __syncthreads();
   {
@@ -223,8 +276,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     // of slots tid/4 + 64 m, two cells per 16-byte load.  Ghost children come
     // from one pair of the boundary oct too (the mirror maps keep x-pairs).
     const int q = tid & 3, s0 = tid >> 2, c0 = 2 * q;
-    const int cb = kBoxX * ((q & 1) + kBoxY * (q >> 1));
-    const int ct = 8 * ((q & 1) + 8 * (q >> 1));
+    const int cb = G::XX * ((q & 1) + G::XY * (q >> 1));
+    const int ct = G::CX * ((q & 1) + G::CY * (q >> 1));
     unsigned mir = 0;  // per ghost face k, 4 bits: source pair, element of child c0, of child c0+1
 #pragma unroll
     for (int k = 0; k < 6; k++) {
@@ -233,29 +286,31 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
     const double *W = A.W, *Wc = A.Wc;
     const long long nc8 = A.nc8;
+    constexpr int kIter = (4 * NS + kThreads - 1) / kThreads;
 #pragma unroll
-    for (int m = 0; m < 3; m++) {
-      if (m == 2 && tid >= kBox / 2 - 2 * kNT) break;
-      const int s = s0 + 64 * m;
-      const int b0 = sBase[s] + cb;
-      const uint8_t sf = sSf[s];
+    for (int m = 0; m < kIter; m++) {
+      const int sg = s0 + (kThreads / 4) * m;  // slot of the tile
+      if (sg >= NS) break;
+      const int nb = sg / G::kSlots, s = sg - nb * G::kSlots;
+      const int b0 = nb * G::kBox + sBase[s] + cb;
+      const uint8_t sf = sSf[sg];
       if (sf == 0) {
         sSt[b0] = 0;
         sSt[b0 + 1] = 0;
         continue;
       }
-      const int cmk = sCmk[s];
+      const int cmk = sCmk[sg];
       double x0[5], x1[5];
       if (cmk == 1) {  // injected coarser cell: one value for both children
         const bool inj = sf & kFInj;
-        const double *p = (inj ? Wc : W) + (long long)sOb[s];
+        const double *p = (inj ? Wc : W) + (long long)sOb[sg];
         const long long stride = inj ? nc8 : N8;
 #pragma unroll
         for (int v = 0; v < 5; v++) x0[v] = x1[v] = __ldg(p + v * stride);
       } else {
         unsigned code = (unsigned)q | (1u << 3);  // pair q, elements 0 and 1
         if (cmk >= 2) code = (mir >> (4 * (cmk - 2))) & 15u;
-        const double *p = W + (long long)sOb[s] + 2 * (code & 3);
+        const double *p = W + (long long)sOb[sg] + 2 * (code & 3);
         const bool e0 = (code >> 2) & 1, e1 = (code >> 3) & 1;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
@@ -268,17 +323,17 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       V::st(sW, b0 + 1, (R)x1[0], (R)x1[1], (R)x1[2], (R)x1[3]);
       sWp[b0] = (R)x0[4];
       sWp[b0 + 1] = (R)x1[4];
-      const uint8_t spm = sSpm[s];
+      const uint8_t spm = sSpm[sg];
       const uint8_t f0 = sf | (((spm >> c0) & 1) ? kFSplit : 0), f1 = sf | (((spm >> (c0 + 1)) & 1) ? kFSplit : 0);
       sSt[b0] = f0;
       sSt[b0 + 1] = f1;
       if constexpr (!F64) {
         if (sf & kFTile) {
-          const int t = sTb[s] + ct;
+          const int t = nb * G::kCells + sTb[s] + ct;
 #pragma unroll
           for (int v = 0; v < 5; v++) {
-            sQ[v * kNT + t] = x0[v];
-            sQ[v * kNT + t + 1] = x1[v];
+            sQ[v * kThreads + t] = x0[v];
+            sQ[v * kThreads + t + 1] = x1[v];
           }
         }
       }
@@ -292,23 +347,28 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   };
 
   // ------------------------------------------------------------------ P1
-  // Pass 0: brick cell tid (slopes and predictor, when it is a leaf of the tile
-  // or borders one); pass 1: ring cell tid (the one face state it contributes).
-  // One call site each for the reconstruction and the face state, so that a
-  // face on a brick boundary, solved by both bricks, rounds the same in both.
+  // Items < kThreads: brick cell tid (slopes and predictor, when it is a leaf of
+  // the tile or borders one); then the ring cells (the one face state each
+  // contributes).  One call site each for the reconstruction and the face
+  // state, so that a face on a brick boundary, solved by both bricks, rounds
+  // the same in both.
 #pragma unroll 1
-  for (int pass = 0; pass < 2; pass++) {
-    int b = tb, k = 0, bin = tb;
+  for (int w = tid; w < kThreads + NRING; w += kThreads) {
+    int b = tb, k = 0, r = 0;
     bool need;
-    if (pass == 0) {
+    if (w < kThreads) {
       const uint8_t f = sSt[tb];
       need = f_tileleaf(f);
       if (!need && f_ok(f))
-        need = f_tileleaf(sSt[tb - 1]) || f_tileleaf(sSt[tb + 1]) || f_tileleaf(sSt[tb - kBoxX]) ||
-               f_tileleaf(sSt[tb + kBoxX]) || f_tileleaf(sSt[tb - kBoxX * kBoxY]) ||
-               f_tileleaf(sSt[tb + kBoxX * kBoxY]);
+        need = f_tileleaf(sSt[tb - 1]) || f_tileleaf(sSt[tb + 1]) || f_tileleaf(sSt[tb - G::XX]) ||
+               f_tileleaf(sSt[tb + G::XX]) || f_tileleaf(sSt[tb - G::XS]) || f_tileleaf(sSt[tb + G::XS]);
     } else {
-      ring_cell(tid, b, k, bin);
+      r = w - kThreads;
+      const int nb = r / G::kRing;
+      int bin;
+      G::ring_cell(r - nb * G::kRing, b, k, bin);
+      b += nb * G::kBox;
+      bin += nb * G::kBox;
       need = f_ok(sSt[b]) && f_tileleaf(sSt[bin]);
     }
     if (!need) continue;
@@ -316,21 +376,21 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     q_at(b, q0);
     q_at(b - 1, qm[0]);
     q_at(b + 1, qp[0]);
-    q_at(b - kBoxX, qm[1]);
-    q_at(b + kBoxX, qp[1]);
-    q_at(b - kBoxX * kBoxY, qm[2]);
-    q_at(b + kBoxX * kBoxY, qp[2]);
+    q_at(b - G::XX, qm[1]);
+    q_at(b + G::XX, qp[1]);
+    q_at(b - G::XS, qm[2]);
+    q_at(b + G::XS, qp[2]);
     if constexpr (F64) M::muscl(q0, qm, qp, A.dt, A.dx, D, Wt);
     else M::muscl(q0, qm, qp, (R)(A.dt / A.dx * 0.5), D, Wt);
     // X = W0 + Wt (FP32 path) or Wt (FP64 path, which adds W0 in the reference's order)
 #pragma unroll
     for (int v = 0; v < 5; v++) X[v] = F64 ? Wt[v] : q0[v] + Wt[v];
-    if (pass == 0) {
+    if (w < kThreads) {
       // groups: D_x(d,u,v,w), D_y, D_z, X(d,u,v,w), (D_x.p, D_y.p, D_z.p, X.p)
 #pragma unroll
-      for (int dir = 0; dir < 3; dir++) V::st(sM, dir * kNT + tid, D[dir][0], D[dir][1], D[dir][2], D[dir][3]);
-      V::st(sM, 3 * kNT + tid, X[0], X[1], X[2], X[3]);
-      V::st(sM, 4 * kNT + tid, D[0][4], D[1][4], D[2][4], X[4]);
+      for (int dir = 0; dir < 3; dir++) V::st(sM, dir * kThreads + tid, D[dir][0], D[dir][1], D[dir][2], D[dir][3]);
+      V::st(sM, 3 * kThreads + tid, X[0], X[1], X[2], X[3]);
+      V::st(sM, 4 * kThreads + tid, D[0][4], D[1][4], D[2][4], X[4]);
     } else {
       const int ax = k >> 1;
       R Dax[5], W[7];
@@ -338,19 +398,19 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       for (int v = 0; v < 5; v++) Dax[v] = (ax == 0) ? D[0][v] : ((ax == 1) ? D[1][v] : D[2][v]);
       if constexpr (F64) M::face_ax(q0, Dax, Wt, k, W, st);
       else M::face_px(X, Dax, k, W, st);
-      V::st(sHS, tid, W[0], W[1], W[2], W[3]);
-      V::st(sHS, kHaloCells + tid, W[4], W[5], W[6], (R)0);
+      V::st(sHS, r, W[0], W[1], W[2], W[3]);
+      V::st(sHS, NRING + r, W[4], W[5], W[6], (R)0);
     }
   }
   __syncthreads();
 
-  // face state k of brick cell t (box cell b) from its slopes and predictor
+  // face state k of brick cell t (index into the tile's cells, box cell b)
   auto brick_face = [&](int t, int b, int k, R W[7]) {
     const int ax = k >> 1;
     R Dax[5], X[5], p0, p1, p2;
-    V::ld(sM, ax * kNT + t, Dax[0], Dax[1], Dax[2], Dax[3]);
-    V::ld(sM, 3 * kNT + t, X[0], X[1], X[2], X[3]);
-    V::ld(sM, 4 * kNT + t, p0, p1, p2, X[4]);
+    V::ld(sM, ax * kThreads + t, Dax[0], Dax[1], Dax[2], Dax[3]);
+    V::ld(sM, 3 * kThreads + t, X[0], X[1], X[2], X[3]);
+    V::ld(sM, 4 * kThreads + t, p0, p1, p2, X[4]);
     Dax[4] = (ax == 0) ? p0 : ((ax == 1) ? p1 : p2);
     if constexpr (F64) {
       R q0[5];
@@ -360,45 +420,49 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       M::face_px(X, Dax, k, W, st);
     }
   };
-  auto ring_face = [&](int j, R W[7]) {
+  auto ring_face = [&](int r, R W[7]) {
     R pad;
-    V::ld(sHS, j, W[0], W[1], W[2], W[3]);
-    V::ld(sHS, kHaloCells + j, W[4], W[5], W[6], pad);
+    V::ld(sHS, r, W[0], W[1], W[2], W[3]);
+    V::ld(sHS, NRING + r, W[4], W[5], W[6], pad);
   };
 
   // ------------------------------------------------------------------ P2
-  // Rounds 0..2: the -d face of every brick cell; round 3 (threads < 128): the
-  // + faces on the brick boundary.  One HLLC call site for all rounds.
+  // Rounds 0..2: the -d face of every brick cell; then the + faces on the brick
+  // boundaries.  One HLLC call site for all rounds.
+  constexpr int kPlusTasks = G::kNB * G::kPlus;
 #pragma unroll 1
-  for (int r = 0; r < 4; r++) {
-    if (r == 3 && tid >= 128) break;
+  for (int w = tid; w < 3 * kThreads + kPlusTasks; w += kThreads) {
     int d, e, tL, bL, jL = -1, tR, bR, jR = -1;
-    if (r < 3) {
-      d = r;
-      const int bs = (d == 0) ? 1 : ((d == 1) ? kBoxX : kBoxX * kBoxY);
-      const int ts = (d == 0) ? 1 : ((d == 1) ? 8 : 64);
+    if (w < 3 * kThreads) {
+      d = w / kThreads;
+      const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+      const int ts = (d == 0) ? 1 : ((d == 1) ? G::CX : G::CX * G::CY);
       const int coord = (d == 0) ? tx : ((d == 1) ? ty : tz);
-      e = (d == 0) ? (tx + 9 * (ty + 8 * tz)) : ((d == 1) ? (kFacesX + tx + 8 * (ty + 9 * tz)) : (kFacesX + kFacesY + tid));
+      e = tn * G::kFaces + G::face_index(d, tx, ty, tz);
       tR = tid;
       bR = tb;
       tL = tid - ts;
       bL = tb - bs;
-      if (coord == 0) jL = (d == 0) ? (ty + 8 * tz) : ((d == 1) ? (64 + tx + 8 * tz) : (128 + tx + 8 * ty));
+      if (coord == 0) jL = tn * G::kRing + G::ring_index(d, false, tx, ty, tz);
     } else {
-      int x, y, z;
-      if (tid < 32) {
-        d = 0; x = 7; y = tid & 7; z = tid >> 3; jR = 32 + tid; e = 8 + 9 * (y + 8 * z);
-      } else if (tid < 64) {
-        d = 1; x = tid & 7; y = 7; z = (tid - 32) >> 3; jR = 96 + (tid - 32); e = kFacesX + x + 8 * (8 + 9 * z);
+      const int p = w - 3 * kThreads, nb = p / G::kPlus;
+      int j = p - nb * G::kPlus, x, y, z;
+      if (j < G::kPX) {
+        d = 0; x = G::CX - 1; y = j % G::CY; z = j / G::CY;
+      } else if (j < G::kPX + G::kPY) {
+        j -= G::kPX;
+        d = 1; x = j % G::CX; y = G::CY - 1; z = j / G::CX;
       } else {
-        d = 2; x = tid & 7; y = (tid - 64) >> 3; z = 3; jR = 192 + (tid - 64);
-        e = kFacesX + kFacesY + x + 8 * (y + 32);
+        j -= G::kPX + G::kPY;
+        d = 2; x = j % G::CX; y = j / G::CX; z = G::CZ - 1;
       }
-      const int bs = (d == 0) ? 1 : ((d == 1) ? kBoxX : kBoxX * kBoxY);
-      tL = x + 8 * (y + 8 * z);
-      bL = box_of(x, y, z);
+      const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+      tL = nb * G::kCells + x + G::CX * (y + G::CY * z);
+      bL = nb * G::kBox + G::box_of(x, y, z);
       tR = tL;
       bR = bL + bs;
+      jR = nb * G::kRing + G::ring_index(d, true, x, y, z);
+      e = nb * G::kFaces + G::face_index(d, x + (d == 0), y + (d == 1), z + (d == 2));
     }
     const uint8_t fL = sSt[bL], fR = sSt[bR];
     R F[5] = {0, 0, 0, 0, 0};
@@ -435,7 +499,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   }
   const uint8_t fme = sSt[tb];
   if (fme & kFTile) {
-    const int s = ((tx + 2) >> 1) + kSlotX * (((ty + 2) >> 1) + kSlotY * ((tz + 2) >> 1));
+    const int s = tn * G::kSlots + ((tx + 2) >> 1) + G::SX * (((ty + 2) >> 1) + G::SY * ((tz + 2) >> 1));
     const int c = (tx & 1) | ((ty & 1) << 1) | ((tz & 1) << 2);
     const long long gi = 8LL * (sKey[s] & 0x0FFFFFFFu) + c;
     double q[5];
@@ -444,7 +508,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       q[4] = sWp[tb];
     } else {
 #pragma unroll
-      for (int v = 0; v < 5; v++) q[v] = sQ[v * kNT + tid];
+      for (int v = 0; v < 5; v++) q[v] = sQ[v * kThreads + tid];
     }
     double Wout[5];
     if (fme & kFSplit) {
@@ -469,9 +533,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     } else {
       const double dtsurdx = A.dt / A.dx;
       // face e of this cell: -x,+x,-y,+y,-z,+z
-      const int ex = tx + 9 * (ty + 8 * tz), ey = kFacesX + tx + 8 * (ty + 9 * tz), ez = kFacesX + kFacesY + tid;
+      const int eb = tn * G::kFaces;
+      const int ex = eb + G::face_index(0, tx, ty, tz), ey = eb + G::face_index(1, tx, ty, tz),
+                ez = eb + G::face_index(2, tx, ty, tz);
       auto flux5 = [&](int k, double F[5]) {
-        const int e = (k < 2) ? (ex + (k & 1)) : ((k < 4) ? (ey + 8 * (k & 1)) : (ez + 64 * (k & 1)));
+        const int e = (k < 2) ? (ex + (k & 1)) : ((k < 4) ? (ey + G::CX * (k & 1)) : (ez + G::CX * G::CY * (k & 1)));
         R f0, f1, f2, f3;
         V::ld(sF, e, f0, f1, f2, f3);
         F[0] = (double)f0;
@@ -571,11 +637,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       // fine -> coarse correction into unsplit coarser neighbours (src/hydro_utils.c:3206-3295)
 #pragma unroll
       for (int k = 0; k < 6; k++) {
-        const int bs = (k < 2) ? 1 : ((k < 4) ? kBoxX : kBoxX * kBoxY);
+        const int bs = (k < 2) ? 1 : ((k < 4) ? G::XX : G::XS);
         const int b2 = (k & 1) ? tb + bs : tb - bs;
         if (!(sSt[b2] & kFInj) || A.Cc == nullptr) continue;
-        const int x2 = b2 % kBoxX, y2 = (b2 / kBoxX) % kBoxY, z2 = b2 / (kBoxX * kBoxY);
-        const long long cc = sKey[(x2 >> 1) + kSlotX * ((y2 >> 1) + kSlotY * (z2 >> 1))] & 0x0FFFFFFFu;
+        const int bl = b2 - bo;
+        const int x2 = bl % G::XX, y2 = (bl / G::XX) % G::XY, z2 = bl / G::XS;
+        const long long cc =
+            sKey[tn * G::kSlots + (x2 >> 1) + G::SX * ((y2 >> 1) + G::SY * (z2 >> 1))] & 0x0FFFFFFFu;
         const double one = (k & 1) ? 1. : -1.;
         double F[5];
         flux5(k, F);
@@ -593,24 +661,80 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   }
 }
 
+// Bytes of dynamic shared memory of a kernel handling the shapes in `shapes`
+// (bit i: kShapes[i]).
+template <class M>
+constexpr size_t level_smem_bytes(unsigned shapes) {
+  const size_t a = (shapes & 1u) ? TileSmem<M, GeomA>::bytes : 0, b = (shapes & 2u) ? TileSmem<M, GeomB>::bytes : 0;
+  return a > b ? a : b;
+}
+
 // Persistent launch over a work list of (level slot, tile) items.  All CTAs are
 // co-resident (grid <= occupancy x SMs) and take items in list order, so a
 // tile waiting for a finer level (listed first) never blocks the CTAs that
-// still have to finish that level.
-template <class M>
-__global__ void __launch_bounds__(kNT, (sizeof(typename M::R) == 8) ? 1 : 3) level_batch_kernel(const BatchArgs Bt) {
+// still have to finish that level.  SHAPES: the brick shapes the levels of the
+// launch use (bit i: kShapes[i]); each level's plan names its own.
+template <class M, unsigned SHAPES>
+__global__ void __launch_bounds__(kThreads, (sizeof(typename M::R) == 8) ? 1 : 3) level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
-  slot_tables<M>(smem);
+  if constexpr ((SHAPES & 1u) != 0) slot_tables<GeomA>(smem);
+  if constexpr ((SHAPES & 2u) != 0) slot_tables<GeomB>(smem + kTabOffB);
   __syncthreads();
   unsigned st = 0;
   for (int w = blockIdx.x; w < Bt.nwork; w += gridDim.x) {
     const int item = Bt.work[w];
     const int slot = item >> kWorkSlotShift, tile = item & ((1 << kWorkSlotShift) - 1);
-    level_tile<M>(Bt, Bt.lv + slot, slot, tile, smem, st);
+    const LevelArgs *gA = Bt.lv + slot;
+    if constexpr (SHAPES == 1u) {
+      level_tile<M, GeomA>(Bt, gA, slot, tile, smem, smem, st);
+    } else if constexpr (SHAPES == 2u) {
+      level_tile<M, GeomB>(Bt, gA, slot, tile, smem, smem + kTabOffB, st);
+    } else {
+      if (gA->shape == 0) level_tile<M, GeomA>(Bt, gA, slot, tile, smem, smem, st);
+      else level_tile<M, GeomB>(Bt, gA, slot, tile, smem, smem + kTabOffB, st);
+    }
     __syncthreads();
   }
   if (st) atomicOr(Bt.status, st);
+}
+
+}  // namespace emma
+
+namespace emma {
+
+// Launch of a work list on a persistent grid of ctas_per_sm CTAs per SM (0 or
+// above the occupancy limit: the limit), so that every CTA is co-resident.
+template <class M, unsigned SHAPES>
+cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cudaStream_t s, int *occupancy) {
+  static int occ = 0;
+  auto k = level_batch_kernel<M, SHAPES>;
+  constexpr size_t bytes = level_smem_bytes<M>(SHAPES);
+  if (occ == 0) {
+    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kThreads, bytes);
+    if (e != cudaSuccess) return e;
+    if (occ < 1) return cudaErrorInvalidConfiguration;
+  }
+  if (occupancy != nullptr) *occupancy = occ;
+  if (a.nwork == 0) return cudaSuccess;
+  const int per = (ctas_per_sm > 0 && ctas_per_sm < occ) ? ctas_per_sm : occ;
+  int grid = per * nsm;
+  if (grid > a.nwork) grid = a.nwork;
+  k<<<grid, kThreads, bytes, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <class M>
+cudaError_t launch_level_any(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
+                             int *occupancy) {
+  switch (shapes) {
+    case 1u: return launch_level_shapes<M, 1u>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u: return launch_level_shapes<M, 2u>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u: return launch_level_shapes<M, 3u>(a, nsm, ctas_per_sm, s, occupancy);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 }  // namespace emma

@@ -8,9 +8,10 @@
 // walk always lands on the geometric level-(L-1) cell, so the block is a window
 // of one "virtual level-L grid" in which every position holds either a real
 // level-L cell or an injected coarser leaf.  vnbr() below steps through that
-// virtual grid one oct at a time.  A tile is a 4x4x2 brick of level-L oct
-// positions; it stages, at their grid positions in a 6x6x4 slot box, the union
-// of the windows of its octs (faces and edges: MUSCL never reads the corners).
+// virtual grid one oct at a time.  A brick is a block of level-L oct positions
+// (4x4x2 or 2x2x2, kShapes); it stages, at their grid positions in a slot box
+// one oct wider on every side, the union of the windows of its octs (faces and
+// edges: MUSCL never reads the corners).  A tile is one or more bricks.
 //
 // With transmissive boundaries (the reference's -DHYDROTEST -DTRANS*), the
 // face slot across a boundary is the mirror of the boundary oct through the
@@ -66,6 +67,7 @@ struct PtrMap {
   }
 };
 
+inline int pos_floor(int p, int b) { return p / b * b; }
 inline bool inside(int c, int k) {
   const int bit = 1 << (k >> 1);
   return (k & 1) ? !(c & bit) : (c & bit);
@@ -147,23 +149,31 @@ struct Planner {
 constexpr uint8_t kMirror[6][8] = {{0, 0, 2, 2, 4, 4, 6, 6}, {1, 1, 3, 3, 5, 5, 7, 7}, {0, 1, 0, 1, 4, 5, 4, 5},
                                    {2, 3, 2, 3, 7, 6, 6, 7}, {0, 1, 2, 3, 0, 1, 2, 3}, {4, 5, 6, 7, 4, 5, 6, 7}};
 constexpr int kDir[6][3] = {{-1, 0, 0}, {1, 0, 0}, {0, -1, 0}, {0, 1, 0}, {0, 0, -1}, {0, 0, 1}};
-constexpr int kBoxStride[3] = {1, kBoxX, kBoxX * kBoxY};
 
 // cell flags of the staged box, as the level kernel derives them
 enum : uint8_t { kFPresent = 1, kFSplit = 2, kFTile = 4, kFInj = 8 };
 inline bool f_ok(uint8_t f) { return (f & (kFPresent | kFSplit)) == kFPresent; }
 inline bool f_tileleaf(uint8_t f) { return (f & (kFPresent | kFSplit | kFTile)) == (kFPresent | kFTile); }
 
+// derived sizes of one brick of a shape
+struct Box {
+  int bx, by, bz, sx, sy, sz, xx, xy, xz, slots, cells;
+  explicit Box(const BrickShape &s)
+      : bx(s.bx), by(s.by), bz(s.bz), sx(s.bx + 2), sy(s.by + 2), sz(s.bz + 2), xx(2 * sx), xy(2 * sy),
+        xz(2 * sz), slots(sx * sy * sz), cells(xx * xy * xz) {}
+  int stride(int a) const { return a == 0 ? 1 : (a == 1 ? xx : xx * xy); }
+};
+
 // Slot keys of the brick at oct origin (ox,oy,oz) holding `octs` (level list
-// indices, positions in `pos`).  Fills keys[kSlots] and the mask.
-bool plan_brick(Planner &P, int L, const std::vector<int> &octs, const std::vector<int32_t> &pos, int ox, int oy,
-                int oz, uint32_t *keys, uint32_t &mask) {
-  std::fill(keys, keys + kSlots, kKeyNone);
+// indices, positions in `pos`).  Fills keys[slots] and the brick's mask.
+bool plan_brick(Planner &P, int L, const Box &G, const std::vector<int> &octs, const std::vector<int32_t> &pos,
+                int ox, int oy, int oz, uint32_t *keys, uint32_t &mask) {
+  std::fill(keys, keys + G.slots, kKeyNone);
   mask = 0;
   auto put = [&](int sx, int sy, int sz, uint32_t key) -> bool {
     if (key == kKeyNone) return true;
-    if (sx < 0 || sx >= kSlotX || sy < 0 || sy >= kSlotY || sz < 0 || sz >= kSlotZ) return false;
-    uint32_t &k = keys[sx + kSlotX * (sy + kSlotY * sz)];
+    if (sx < 0 || sx >= G.sx || sy < 0 || sy >= G.sy || sz < 0 || sz >= G.sz) return false;
+    uint32_t &k = keys[sx + G.sx * (sy + G.sy * sz)];
     if (k == kKeyNone) k = key;
     return k == key;
   };
@@ -175,7 +185,7 @@ bool plan_brick(Planner &P, int L, const std::vector<int> &octs, const std::vect
   };
   for (int o : octs) {
     const int ix = pos[3 * o] - ox, iy = pos[3 * o + 1] - oy, iz = pos[3 * o + 2] - oz;
-    mask |= 1u << (ix + kBrickX * (iy + kBrickY * iz));
+    mask |= 1u << (ix + G.bx * (iy + G.by * iz));
     if (!put(ix + 1, iy + 1, iz + 1, key_make(kKeyReal, (uint32_t)o))) return bad("two octs at one brick position");
   }
   for (int o : octs) {
@@ -197,16 +207,17 @@ bool plan_brick(Planner &P, int L, const std::vector<int> &octs, const std::vect
 }
 
 // Cell flags of a planned brick and the checks that every stencil the kernel
-// evaluates reads staged cells only.  Collects the level L-1 cells that receive
+// evaluates reads staged cells only.  Marks the level L-1 cells that receive
 // fine->coarse corrections.
-bool check_brick(Planner &P, int L, const uint32_t *keys, uint32_t mask, std::vector<uint8_t> *corrected) {
+bool check_brick(Planner &P, int L, const Box &G, const uint32_t *keys, uint32_t mask,
+                 std::vector<uint8_t> *corrected) {
   const HostLevel &lv = P.H.lev[L];
-  uint8_t fl[kBox];
-  for (int s = 0; s < kSlots; s++) {
-    const int sz = s / (kSlotX * kSlotY), sy = (s / kSlotX) % kSlotY, sx = s % kSlotX;
-    const bool inner = sx >= 1 && sx <= kBrickX && sy >= 1 && sy <= kBrickY && sz >= 1 && sz <= kBrickZ;
+  std::vector<uint8_t> fl((size_t)G.cells, 0);
+  for (int s = 0; s < G.slots; s++) {
+    const int sz = s / (G.sx * G.sy), sy = (s / G.sx) % G.sy, sx = s % G.sx;
+    const bool inner = sx >= 1 && sx <= G.bx && sy >= 1 && sy <= G.by && sz >= 1 && sz <= G.bz;
     for (int c = 0; c < 8; c++) {
-      const int b = (2 * sx + (c & 1)) + kBoxX * ((2 * sy + ((c >> 1) & 1)) + kBoxY * (2 * sz + (c >> 2)));
+      const int b = (2 * sx + (c & 1)) + G.xx * ((2 * sy + ((c >> 1) & 1)) + G.xy * (2 * sz + (c >> 2)));
       const uint32_t key = keys[s];
       uint8_t f = 0;
       if (key != kKeyNone) {
@@ -214,7 +225,7 @@ bool check_brick(Planner &P, int L, const uint32_t *keys, uint32_t mask, std::ve
         f = kFPresent;
         if (kind == kKeyReal) {
           if ((lv.split[idx] >> c) & 1) f |= kFSplit;
-          if (inner && ((mask >> ((sx - 1) + kBrickX * ((sy - 1) + kBrickY * (sz - 1)))) & 1)) f |= kFTile;
+          if (inner && ((mask >> ((sx - 1) + G.bx * ((sy - 1) + G.by * (sz - 1)))) & 1)) f |= kFTile;
         } else if (kind == kKeyInj) {
           f |= kFInj;
         } else {
@@ -226,7 +237,7 @@ bool check_brick(Planner &P, int L, const uint32_t *keys, uint32_t mask, std::ve
   }
   auto all_nbrs = [&](int b) {
     for (int a = 0; a < 3; a++)
-      if (!(fl[b - kBoxStride[a]] & kFPresent) || !(fl[b + kBoxStride[a]] & kFPresent)) return false;
+      if (!(fl[b - G.stride(a)] & kFPresent) || !(fl[b + G.stride(a)] & kFPresent)) return false;
     return true;
   };
   auto fail = [&](const char *m) {
@@ -234,41 +245,129 @@ bool check_brick(Planner &P, int L, const uint32_t *keys, uint32_t mask, std::ve
     P.msg = std::string(m) + " (level " + std::to_string(L) + ")";
     return false;
   };
+  const int x0 = 2, x1 = 2 + 2 * G.bx, y0 = 2, y1 = 2 + 2 * G.by, z0 = 2, z1 = 2 + 2 * G.bz;
   // brick cells: reconstructed if a leaf of the tile or face-adjacent to one
-  for (int z = 2; z < 2 + 2 * kBrickZ; z++)
-    for (int y = 2; y < 2 + 2 * kBrickY; y++)
-      for (int x = 2; x < 2 + 2 * kBrickX; x++) {
-        const int b = x + kBoxX * (y + kBoxY * z);
+  for (int z = z0; z < z1; z++)
+    for (int y = y0; y < y1; y++)
+      for (int x = x0; x < x1; x++) {
+        const int b = x + G.xx * (y + G.xy * z);
         bool near = f_tileleaf(fl[b]);
         for (int a = 0; a < 3; a++)
-          near = near || f_tileleaf(fl[b - kBoxStride[a]]) || f_tileleaf(fl[b + kBoxStride[a]]);
+          near = near || f_tileleaf(fl[b - G.stride(a)]) || f_tileleaf(fl[b + G.stride(a)]);
         if (f_ok(fl[b]) && near && !all_nbrs(b)) return fail("unstaged neighbour of a reconstructed cell");
         if (!f_tileleaf(fl[b])) continue;
         for (int a = 0; a < 3; a++)
           for (int sgn = -1; sgn <= 1; sgn += 2) {
-            const int b2 = b + sgn * kBoxStride[a];
+            const int b2 = b + sgn * G.stride(a);
             if (!(fl[b2] & kFPresent)) return fail("unstaged face neighbour of a leaf cell");
             if (corrected && (fl[b2] & kFInj)) {
-              const int x2 = b2 % kBoxX, y2 = (b2 / kBoxX) % kBoxY, z2 = b2 / (kBoxX * kBoxY);
-              (*corrected)[keys[(x2 >> 1) + kSlotX * ((y2 >> 1) + kSlotY * (z2 >> 1))] & 0x0FFFFFFFu] = 1;
+              const int xb = b2 % G.xx, yb = (b2 / G.xx) % G.xy, zb = b2 / (G.xx * G.xy);
+              (*corrected)[keys[(xb >> 1) + G.sx * ((yb >> 1) + G.sy * (zb >> 1))] & 0x0FFFFFFFu] = 1;
             }
           }
       }
   // ring cells face-adjacent to a leaf of the tile: reconstructed too
-  for (int z = 1; z < kBoxZ - 1; z++)
-    for (int y = 1; y < kBoxY - 1; y++)
-      for (int x = 1; x < kBoxX - 1; x++) {
-        const bool ix = x >= 2 && x < 2 + 2 * kBrickX, iy = y >= 2 && y < 2 + 2 * kBrickY,
-                   iz = z >= 2 && z < 2 + 2 * kBrickZ;
+  for (int z = 1; z < G.xz - 1; z++)
+    for (int y = 1; y < G.xy - 1; y++)
+      for (int x = 1; x < G.xx - 1; x++) {
+        const bool ix = x >= x0 && x < x1, iy = y >= y0 && y < y1, iz = z >= z0 && z < z1;
         if ((int)ix + (int)iy + (int)iz != 2) continue;  // face layer of the brick, not an edge
-        const int b = x + kBoxX * (y + kBoxY * z);
+        const int b = x + G.xx * (y + G.xy * z);
         int bin = b;
-        if (!ix) bin = b + (x < 2 ? 1 : -1);
-        if (!iy) bin = b + (y < 2 ? kBoxX : -kBoxX);
-        if (!iz) bin = b + (z < 2 ? kBoxX * kBoxY : -kBoxX * kBoxY);
+        if (!ix) bin = b + (x < x0 ? 1 : -1);
+        if (!iy) bin = b + (y < y0 ? G.xx : -G.xx);
+        if (!iz) bin = b + (z < z0 ? G.xx * G.xy : -G.xx * G.xy);
         if (f_ok(fl[b]) && f_tileleaf(fl[bin]) && !all_nbrs(b)) return fail("unstaged neighbour of a ring cell");
       }
   return true;
+}
+
+// Bricks of a shape holding the level's octs, in order of their first oct.
+std::vector<std::vector<int>> group_bricks(const std::vector<int32_t> &pos, int noct, const BrickShape &sh) {
+  std::unordered_map<uint64_t, int> brick;
+  std::vector<std::vector<int>> members;
+  brick.reserve((size_t)noct / 4 + 16);
+  for (int i = 0; i < noct; i++) {
+    const uint64_t bk = ((uint64_t)(pos[3 * i] / sh.bx) << 42) | ((uint64_t)(pos[3 * i + 1] / sh.by) << 21) |
+                        (uint64_t)(pos[3 * i + 2] / sh.bz);
+    auto it = brick.find(bk);
+    if (it == brick.end()) {
+      it = brick.emplace(bk, (int)members.size()).first;
+      members.emplace_back();
+    }
+    members[it->second].push_back(i);
+  }
+  return members;
+}
+
+// Relative cost of one tile of each shape (a 2x2x2-oct brick stages and
+// reconstructs more ring cells per cell); used when a level is planned without
+// measurement.
+constexpr double kTileCost[kNumShapes] = {1.0, 1.3};
+
+int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) {
+  HostLevel &lv = H.lev[L];
+  lv.tiles.clear();
+  lv.keys.clear();
+  lv.inj_cells.clear();
+  lv.reads_coarse = false;
+  lv.shape = 0;
+  if (lv.noct == 0) return 0;
+  int shape = shape_req;
+  std::vector<std::vector<int>> members;
+  if (shape < 0 || shape >= kNumShapes) {
+    // without a requested shape: the cheaper by tiles x tile cost
+    double best = 0;
+    for (int s = 0; s < kNumShapes; s++) {
+      auto m = group_bricks(lv.pos, lv.noct, kShapes[s]);
+      const double c = kTileCost[s] * (double)((m.size() + kShapes[s].nb - 1) / kShapes[s].nb);
+      if (s == 0 || c < best) {
+        best = c;
+        shape = s;
+        members = std::move(m);
+      }
+    }
+  } else {
+    members = group_bricks(lv.pos, lv.noct, kShapes[shape]);
+  }
+  const BrickShape &sh = kShapes[shape];
+  const Box G(sh);
+  lv.shape = shape;
+  std::vector<uint8_t> corrected;
+  if (L > H.lcoarse) corrected.assign((size_t)8 * H.lev[L - 1].noct, 0);
+  const size_t ntiles = (members.size() + sh.nb - 1) / sh.nb;
+  lv.tiles.resize(ntiles);
+  lv.keys.assign(ntiles * (size_t)sh.tile_slots(), kKeyNone);
+  for (size_t t = 0; t < ntiles; t++) {
+    TileDesc &td = lv.tiles[t];
+    std::memset(&td, 0, sizeof(td));
+    for (int nb = 0; nb < sh.nb; nb++) {
+      const size_t m = t * sh.nb + nb;
+      if (m >= members.size()) break;
+      const int o0 = members[m][0];
+      const int ox = pos_floor(lv.pos[3 * o0], sh.bx), oy = pos_floor(lv.pos[3 * o0 + 1], sh.by),
+                oz = pos_floor(lv.pos[3 * o0 + 2], sh.bz);
+      if (nb == 0) {
+        td.ox = ox;
+        td.oy = oy;
+        td.oz = oz;
+      }
+      uint32_t *keys = &lv.keys[t * sh.tile_slots() + (size_t)nb * sh.slots()];
+      uint32_t bmask = 0;
+      if (!plan_brick(P, L, G, members[m], lv.pos, ox, oy, oz, keys, bmask) ||
+          !check_brick(P, L, G, keys, bmask, corrected.empty() ? nullptr : &corrected)) {
+        err = P.msg;
+        return (int)P.err;
+      }
+      td.mask |= bmask << (nb * sh.octs());
+      td.noct += (int)members[m].size();
+    }
+  }
+  for (size_t i = 0; i < corrected.size(); i++)
+    if (corrected[i]) lv.inj_cells.push_back((int32_t)i);
+  for (uint32_t key : lv.keys)
+    if (key != kKeyNone && (key >> 28) == kKeyInj) lv.reads_coarse = true;
+  return 0;
 }
 
 }  // namespace
@@ -276,7 +375,7 @@ bool check_brick(Planner &P, int L, const uint32_t *keys, uint32_t mask, std::ve
 int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string &err);
 
 int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int trans, int plan_lo, int plan_hi,
-                    HostTree &H, std::string &err) {
+                    HostTree &H, std::string &err, const int *shapes) {
   H = HostTree();
   H.lcoarse = lcoarse;
   H.lmax = lmax;
@@ -318,16 +417,10 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
     P.face[L].assign((size_t)6 * lv.noct, kKeyNone);
     for (int i = 0; i < lv.noct; i++)
       for (int k = 0; k < 6; k++) P.face[L][6 * i + k] = P.real_nbr(L, i, k);
-  }
-  for (int L = std::max(lcoarse, plan_lo); L <= std::min(lmax, plan_hi); L++) {
-    HostLevel &lv = H.lev[L];
-    if (lv.noct == 0) continue;
-    // integer oct positions on the level grid, grouped into bricks in list order
+    // integer oct positions on the level grid
     const double scale = std::ldexp(1.0, L - 1);
     const int n = 1 << (L - 1);
-    std::vector<int32_t> pos((size_t)3 * lv.noct);
-    std::unordered_map<uint64_t, int> brick;
-    std::vector<std::vector<int>> members;
+    lv.pos.assign((size_t)3 * lv.noct, 0);
     for (int i = 0; i < lv.noct; i++) {
       const struct OCT *o = lv.octs[i];
       const double q[3] = {o->x * scale, o->y * scale, o->z * scale};
@@ -337,42 +430,37 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
           err = "oct position off the level grid at level " + std::to_string(L);
           return EMMA_ST_TREE;
         }
-        pos[3 * i + a] = (int32_t)r;
-      }
-      const uint64_t bk = ((uint64_t)(pos[3 * i] / kBrickX) << 42) | ((uint64_t)(pos[3 * i + 1] / kBrickY) << 21) |
-                          (uint64_t)(pos[3 * i + 2] / kBrickZ);
-      auto it = brick.find(bk);
-      if (it == brick.end()) {
-        it = brick.emplace(bk, (int)members.size()).first;
-        members.emplace_back();
-      }
-      members[it->second].push_back(i);
-    }
-    std::vector<uint8_t> corrected;
-    if (L > lcoarse) corrected.assign((size_t)8 * H.lev[L - 1].noct, 0);
-    lv.tiles.resize(members.size());
-    lv.keys.assign(members.size() * (size_t)kSlots, kKeyNone);
-    for (size_t t = 0; t < members.size(); t++) {
-      const int o0 = members[t][0];
-      TileDesc &td = lv.tiles[t];
-      std::memset(&td, 0, sizeof(td));
-      td.ox = pos[3 * o0] / kBrickX * kBrickX;
-      td.oy = pos[3 * o0 + 1] / kBrickY * kBrickY;
-      td.oz = pos[3 * o0 + 2] / kBrickZ * kBrickZ;
-      td.noct = (int)members[t].size();
-      uint32_t *keys = &lv.keys[t * kSlots];
-      if (!plan_brick(P, L, members[t], pos, td.ox, td.oy, td.oz, keys, td.mask) ||
-          !check_brick(P, L, keys, td.mask, corrected.empty() ? nullptr : &corrected)) {
-        err = P.msg;
-        return (int)P.err;
+        lv.pos[3 * i + a] = (int32_t)r;
       }
     }
-    for (size_t i = 0; i < corrected.size(); i++)
-      if (corrected[i]) lv.inj_cells.push_back((int32_t)i);
-    for (uint32_t key : lv.keys)
-      if (key != kKeyNone && (key >> 28) == kKeyInj) lv.reads_coarse = true;
+  }
+  for (int L = std::max(lcoarse, plan_lo); L <= std::min(lmax, plan_hi); L++) {
+    const int rc = plan_level(P, H, L, shapes ? shapes[L] : -1, err);
+    if (rc != 0) return rc;
   }
   return validate_host_tree(H, plan_lo, plan_hi, err);
+}
+
+int replan_level(HostTree &H, int L, int shape, std::string &err) {
+  if (L < H.lcoarse || L > H.lmax) {
+    err = "level outside the mirrored tree";
+    return EMMA_ST_ARG;
+  }
+  Planner P(H);
+  P.idx.resize((size_t)H.lmax + 2);
+  P.face.resize((size_t)H.lmax + 1);
+  for (int l = std::max(H.lcoarse, L - 1); l <= L; l++) {
+    const HostLevel &lv = H.lev[l];
+    P.idx[l].init(lv.octs.size());
+    for (int i = 0; i < lv.noct; i++) P.idx[l].put(lv.octs[i], i);
+  }
+  HostLevel &lv = H.lev[L];
+  P.face[L].assign((size_t)6 * lv.noct, kKeyNone);
+  for (int i = 0; i < lv.noct; i++)
+    for (int k = 0; k < 6; k++) P.face[L][6 * i + k] = P.real_nbr(L, i, k);
+  const int rc = plan_level(P, H, L, shape, err);
+  if (rc != 0) return rc;
+  return validate_host_tree(H, L, L, err);
 }
 
 // Every index a level kernel dereferences comes from these arrays; check them
@@ -382,7 +470,12 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
     const HostLevel &lv = H.lev[L];
     const long long ncoarse8 = (L > H.lcoarse) ? 8LL * H.lev[L - 1].noct : 0;
     const long long nfine = (L < H.lmax) ? H.lev[L + 1].noct : 0;
-    if (lv.keys.size() != lv.tiles.size() * (size_t)kSlots) {
+    if (lv.shape < 0 || lv.shape >= kNumShapes) {
+      err = "invalid brick shape at level " + std::to_string(L);
+      return EMMA_ST_TREE;
+    }
+    const BrickShape &sh = kShapes[lv.shape];
+    if (lv.keys.size() != lv.tiles.size() * (size_t)sh.tile_slots()) {
       err = "slot keys do not match the tiles at level " + std::to_string(L);
       return EMMA_ST_TREE;
     }
@@ -394,8 +487,9 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
         err = "invalid tile descriptor at level " + std::to_string(L);
         return EMMA_ST_TREE;
       }
-      for (int s = 0; s < kSlots; s++) {
-        const uint32_t key = lv.keys[t * kSlots + s];
+      const uint32_t *keys = &lv.keys[t * (size_t)sh.tile_slots()];
+      for (int s = 0; s < sh.tile_slots(); s++) {
+        const uint32_t key = keys[s];
         if (key == kKeyNone) continue;
         const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
         const bool ok = (kind == kKeyReal || (kind >= kKeyGhost0 && kind < kKeyGhost0 + 6)) ? (idx < (uint32_t)lv.noct)
@@ -406,10 +500,11 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
           return EMMA_ST_TREE;
         }
       }
-      for (int m = 0; m < kTileOcts; m++) {
+      for (int m = 0; m < sh.nb * sh.octs(); m++) {
         if (!((td.mask >> m) & 1)) continue;
-        const int sx = 1 + m % kBrickX, sy = 1 + (m / kBrickX) % kBrickY, sz = 1 + m / (kBrickX * kBrickY);
-        const uint32_t key = lv.keys[t * kSlots + sx + kSlotX * (sy + kSlotY * sz)];
+        const int nb = m / sh.octs(), i = m % sh.octs();
+        const int sx = 1 + i % sh.bx, sy = 1 + (i / sh.bx) % sh.by, sz = 1 + i / (sh.bx * sh.by);
+        const uint32_t key = keys[nb * sh.slots() + sx + (sh.bx + 2) * (sy + (sh.by + 2) * sz)];
         if ((key >> 28) != kKeyReal || seen[key & 0x0FFFFFFFu]) {
           err = "tile oct missing or advanced twice at level " + std::to_string(L);
           return EMMA_ST_TREE;

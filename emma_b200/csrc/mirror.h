@@ -19,6 +19,8 @@ struct HostLevel {
   std::vector<uint32_t> keys;         // kSlots slot keys per tile
   std::vector<int32_t> inj_cells;     // level L-1 cells that receive fine->coarse corrections
   bool reads_coarse = false;          // some tile stages an injected level L-1 cell
+  int shape = 0;                      // brick shape of the plan (kShapes)
+  std::vector<int32_t> pos;           // per oct: integer position on the level grid (x,y,z)
 };
 
 struct HostTree {
@@ -29,8 +31,14 @@ struct HostTree {
 // Build the mirror of levels lcoarse..lmax and the tile plans of levels
 // plan_lo..plan_hi (a plan of level L needs the mirror of L-1 when L-1 >=
 // lcoarse).  Returns 0 on success, else an EMMA_ST_* bit with a message in `err`.
+// shapes (optional, indexed by level): brick shape of each plan, -1 = the
+// cheaper by tile count x tile cost.
 int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int trans, int plan_lo, int plan_hi,
-                    HostTree &H, std::string &err);
+                    HostTree &H, std::string &err, const int *shapes = nullptr);
+
+// Re-plan level L of a built tree with brick shape `shape` (the autotuner's
+// candidates); validates the new plan.
+int replan_level(HostTree &H, int L, int shape, std::string &err);
 
 // Bounds check of every index the level kernels read (run by build_host_tree).
 int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string &err);

@@ -16,26 +16,32 @@ constexpr uint32_t kKeyReal = 0, kKeyInj = 1, kKeyGhost0 = 2;
 constexpr uint32_t kKeyNone = 0xFFFFFFFFu;
 constexpr uint32_t key_make(uint32_t kind, uint32_t idx) { return (kind << 28) | idx; }
 
-// Brick tiles.  A tile is one brick of 4 x 4 x 2 oct positions of a level's
-// grid holding at least one oct of the level (mask: which).  The kernel stages
-// a 6 x 6 x 4 box of virtual-oct slots (the brick and a ring of one oct), i.e.
-// 12 x 12 x 8 cells, so that every neighbour a stencil reads sits at a fixed
-// offset (+-1, +-12, +-144 cells).  Slot s = sx + 6 (sy + 6 sz); the brick
-// interior is sx,sy in 1..4, sz in 1..2; slots no stencil reads hold kKeyNone.
-constexpr int kBrickX = 4, kBrickY = 4, kBrickZ = 2, kTileOcts = kBrickX * kBrickY * kBrickZ;
-constexpr int kSlotX = kBrickX + 2, kSlotY = kBrickY + 2, kSlotZ = kBrickZ + 2;
-constexpr int kSlots = kSlotX * kSlotY * kSlotZ;                       // 144
-constexpr int kBoxX = 2 * kSlotX, kBoxY = 2 * kSlotY, kBoxZ = 2 * kSlotZ;
-constexpr int kBox = kBoxX * kBoxY * kBoxZ;                            // 1152 staged cells
-constexpr int kNT = 8 * kTileOcts;                                     // 256 brick cells = threads
-constexpr int kHaloCells = 2 * (8 * 4) * 2 + 2 * (8 * 8);              // 256 cells face-adjacent to the brick
-constexpr int kFacesX = 9 * 8 * 4, kFacesY = 8 * 9 * 4, kFacesZ = 8 * 8 * 5;
-constexpr int kFaces = kFacesX + kFacesY + kFacesZ;                    // 896 faces of the brick cells
+// Brick tiles.  A brick is BX x BY x BZ oct positions of a level's grid; a
+// tile is NB bricks that hold at least one oct of the level, advanced by one
+// CTA of kThreads threads (one per brick cell).  For each brick the kernel
+// stages a (BX+2) x (BY+2) x (BZ+2) box of virtual-oct slots (the brick and a
+// ring of one oct), so every neighbour a stencil reads sits at a fixed offset.
+// Slot s = sx + SX (sy + SY sz); the brick interior is sx in 1..BX etc.; slots
+// no stencil reads hold kKeyNone.  Two shapes: 4x4x2 octs x 1 brick (complete
+// levels) and 2x2x2 octs (the children of one parent oct) x 4 bricks (sparse
+// refined levels); the autotuner picks one per level.
+constexpr int kThreads = 256;
+struct BrickShape {
+  int bx, by, bz, nb;
+  constexpr int octs() const { return bx * by * bz; }
+  constexpr int slots() const { return (bx + 2) * (by + 2) * (bz + 2); }
+  constexpr int tile_slots() const { return nb * slots(); }
+};
+constexpr int kNumShapes = 2;
+constexpr BrickShape kShapes[kNumShapes] = {{4, 4, 2, 1}, {2, 2, 2, 4}};
+static_assert(kShapes[0].nb * 8 * kShapes[0].octs() == kThreads, "one thread per brick cell");
+static_assert(kShapes[1].nb * 8 * kShapes[1].octs() == kThreads, "one thread per brick cell");
+constexpr int kTileOcts = 32;  // octs per tile (mask bits), both shapes
 
 struct TileDesc {
-  uint32_t mask;  // bit (ix + 4 iy + 16 iz): brick position holds an oct of this level
+  uint32_t mask;  // bit (nb * octs + ix + BX (iy + BY iz)): brick nb holds an oct at that position
   int noct;       // octs in the tile (popcount of mask)
-  int ox, oy, oz; // brick origin in oct coordinates of the level
+  int ox, oy, oz; // origin of the first brick in oct coordinates of the level
   int pad[3];
 };
 
@@ -58,7 +64,9 @@ struct LevelArgs {
   const uint8_t *split;  // per oct bitmask of split cells
   const int *child;      // per cell: child oct index at L+1, -1 for a leaf
   const TileDesc *tiles;
-  const uint32_t *keys;  // kSlots keys per tile
+  const uint32_t *keys;  // kShapes[shape].tile_slots() keys per tile
+  int shape;             // brick shape of the plan (index into kShapes)
+  int pad_shape;
   double dt, dx;
   int ntiles;
   int wait_slot;      // level whose tiles must all be updated before this level's

@@ -12,23 +12,26 @@ import numpy as np
 from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
-def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True):
+def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0):
+    """tile_octs: 0 = brick shape autotuned per level at upload, 32 = 4x4x2-oct
+    bricks, 8 = 2x2x2-oct bricks (four per tile)."""
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
     o.use_graph = 1 if use_graph else 0
+    o.tile_octs = tile_octs
     return o
 
 
 class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
-    def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True):
+    def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0):
         self.tree = tree
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
-        self.trans, self.cfl, self.use_graph = trans, cfl, use_graph
+        self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
         L = lib()
-        o = options(precision, trans, cfl, use_graph=use_graph)
+        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
         check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
         L.emma_hydro_clear_status()
@@ -37,7 +40,7 @@ class ResidentHydro:
         self.tsim = 0.0
 
     def set_precision(self, precision):
-        o = options(precision, self.trans, self.cfl, use_graph=self.use_graph)
+        o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs)
         check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):
@@ -84,6 +87,14 @@ class ResidentHydro:
 
     def status(self):
         return lib().emma_hydro_status()
+
+    def tuning(self, level):
+        """Autotuner record of a level: (octs per brick, CTAs per SM, sweep) with
+        sweep[shape][ctas-1] the measured ms per launch (0 = not tried)."""
+        octs, ctas = ctypes.c_int(), ctypes.c_int()
+        sweep = np.zeros(8)
+        rc = lib().emma_hydro_tuning(level, ctypes.byref(octs), ctypes.byref(ctas), ptr(sweep))
+        return (octs.value, ctas.value, sweep.reshape(2, 4)) if rc == 0 else None
 
     def download(self):
         check(lib().emma_hydro_tree_download(self.tree.firstoct), "tree_download")

@@ -59,7 +59,7 @@ struct EmmaHydroOptions {
   int precision;        /* EMMA_PREC_* */
   int trans_flags;      /* EMMA_TRANS_* */
   double cfl;           /* Courant number of the level time step (reference param.h: 0.85) */
-  int tile_octs;        /* octs per CTA tile (0 = autotuned) */
+  int tile_octs;        /* octs per brick: 0 = autotuned per level, 32 = 4x4x2, 8 = 2x2x2 */
   int device;           /* CUDA device ordinal */
   int use_graph;        /* coarse steps as a captured CUDA graph with a device-side schedule */
 };
@@ -146,6 +146,14 @@ void emma_hydro_reset_counters(void);
 /* Average device time (ms) of the level kernel launches since the last reset,
  * measured with CUDA events on the launching stream, and their count. */
 int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cells);
+
+/* Autotuner record of a resident level (emma_hydro_tree_upload tunes every
+ * level when options.tile_octs == 0): the chosen brick (32 = 4x4x2 octs, one
+ * per tile; 8 = 2x2x2 octs, four per tile), the CTAs per SM of its launches,
+ * and the measured ms per launch of every candidate, sweep_ms[4*shape + ctas-1]
+ * (shape 0: 4x4x2, 1: 2x2x2; 0 = not tried).  Returns EMMA_ST_ARG if the level
+ * was not tuned. */
+int emma_hydro_tuning(int level, int *tile_octs, int *ctas_per_sm, double *sweep_ms);
 
 /* Planning diagnostics, host only (no GPU needed): per level lcoarse..lmax,
  * stats5[5*(L-lcoarse)+{0..4}] = octs, tiles (4x4x2-oct bricks), max staged

@@ -20,9 +20,9 @@ GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
 CFL = 0.8
 
 
-def run_gpu(cfg, nsteps, precision=PREC_FP64):
+def run_gpu(cfg, nsteps, precision=PREC_FP64, tile_octs=0):
     t = cfg.build()
-    r = ResidentHydro(t, precision=precision, trans=cfg.trans, cfl=CFL)
+    r = ResidentHydro(t, precision=precision, trans=cfg.trans, cfl=CFL, tile_octs=tile_octs)
     for _ in range(nsteps):
         r.coarse_step(nsub=cfg.nsub)
     st = r.status()
@@ -241,3 +241,66 @@ def test_async_steps_and_device_time(gpu):
     assert tsim == tsim_o
     r.download()
     assert_close(t, to, [4], 1e-12)
+
+
+# ---------------------------------------------------------------- brick shapes
+# tile_octs=32: 4x4x2-oct bricks, one per tile; 8: 2x2x2-oct bricks, four per
+# tile; 0: chosen per level by the autotuner at upload.
+
+@pytest.mark.parametrize("tile_octs", [32, 8])
+@pytest.mark.parametrize("base,radii", [(4, (0.3, 0.15)), (3, (0.35, 0.2))])
+def test_fp64_amr_one_step_each_shape(gpu, base, radii, tile_octs):
+    cfg = configs.small_amr(base=base, radii=radii)
+    tg, r, st = run_gpu(cfg, 1, tile_octs=tile_octs)
+    assert st == 0
+    for l in range(cfg.lcoarse, cfg.lmax + 1):
+        assert r.tuning(l)[0] == tile_octs
+    to, tsim = run_oracle(cfg, 1)
+    assert r.tsim == tsim
+    assert_close(tg, to, range(cfg.lcoarse, cfg.lmax + 1), 1e-12)
+
+
+@pytest.mark.parametrize("cfg", [configs.random_uniform(level=4), configs.sod(level=5)], ids=["uniform", "sod"])
+def test_fp64_small_bricks_uniform_and_transmissive(gpu, cfg):
+    tg, r, st = run_gpu(cfg, 2, tile_octs=8)
+    assert st == 0
+    to, tsim = run_oracle(cfg, 2)
+    assert r.tsim == tsim
+    assert_close(tg, to, [cfg.lcoarse], 1e-12)
+
+
+def test_mixed_small_bricks_l1_and_conservation(gpu):
+    cfg = configs.random_uniform(level=5)
+    tm, r, st = run_gpu(cfg, 5, precision=PREC_MIXED, tile_octs=8)
+    assert st == 0
+    to, _ = run_oracle(cfg, 5)
+    fm, fo = tm.get_fields(5), to.get_fields(5)
+    assert l1_rel(fm[0], fo[0]) <= 1e-5 and l1_rel(fm[4], fo[4]) <= 1e-5
+    f0 = cfg.build().get_fields(5)
+    assert abs(fm[0].sum() - f0[0].sum()) <= 1e-12 * f0[0].sum()
+    assert abs(fm[6].sum() - f0[6].sum()) <= 1e-12 * f0[6].sum()
+
+
+def test_autotuner_record_and_batched_step(gpu):
+    """The autotuner times every candidate on every level, keeps the fastest, and
+    the tuned plans (possibly of both shapes in one batched launch) match the oracle."""
+    cfg = configs.small_amr(base=4, radii=(0.3, 0.15))
+    t = cfg.build()
+    r = ResidentHydro(t, precision=PREC_FP64, cfl=CFL, use_graph=True)
+    for l in range(cfg.lcoarse, cfg.lmax + 1):
+        octs, ctas, sweep = r.tuning(l)
+        assert octs in (32, 8) and ctas >= 1
+        tried = sweep[sweep > 0]
+        assert tried.size >= 1
+        k = 0 if octs == 32 else 1
+        assert sweep[k, ctas - 1] == tried.min()
+    # the complete base level is only tried with 4x4x2 bricks
+    assert r.tuning(cfg.lcoarse)[2][1].max() == 0
+    for _ in range(2):
+        r.coarse_step(nsub=1)
+    assert r.status() == 0
+    r.download()
+    to = cfg.build()
+    tsim, _, err = oracle.Restatement().run(to.firstoct, cfg.lcoarse, cfg.lmax, 2, CFL, nsub=1)
+    assert err == 0 and r.tsim == tsim
+    assert_close(t, to, range(cfg.lcoarse, cfg.lmax + 1), 1e-12)
