@@ -166,6 +166,13 @@ def run_mine(args, rank, world):
     for prec_name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
         # whole coarse steps: CUDA graph with the device-side level schedule
         r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=True)
+        tuning = {}
+        for l in levels:
+            rec = r.tuning(l)
+            if rec is not None:
+                tuning[str(l)] = {"tile_octs": rec[0], "ctas_per_sm": rec[1],
+                                  "sweep_ms": {"4x4x2": [round(x, 4) for x in rec[2][0][:3]],
+                                               "2x2x2": [round(x, 4) for x in rec[2][1][:3]]}}
         init_states = {l: r.state(l) for l in levels}
         r.coarse_step(nsub=cfg.nsub)  # builds and instantiates the graph
         for _ in range(max(args.warmup - 1, 0)):
@@ -192,10 +199,11 @@ def run_mine(args, rank, world):
         status = r.status()
         launches_per_step = graph_kernel_count(cfg, tree)
         res = {"ms": ms, "updates": updates, "launches": launches_per_step * args.steps, "status": status,
-               "clocks": clk.summary()}
+               "clocks": clk.summary(), "autotune": tuning}
         # level-kernel time per launch: the same steps on the host-driven schedule,
         # each level-kernel launch timed with CUDA events on the library stream
-        r2 = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=False)
+        r2 = r
+        r2.set_use_graph(False)
         for _ in range(2):
             r2.coarse_step(nsub=cfg.nsub)
         L.emma_hydro_reset_counters()
@@ -208,7 +216,7 @@ def run_mine(args, rank, world):
         L.emma_hydro_kernel_timing(ctypes.byref(kavg), ctypes.byref(kcnt), ctypes.byref(kcells))
         res.update(kernel_avg_ms=kavg.value, kernel_launches=kcnt.value, kernel_cells=kcells.value)
         # e2e through the C ABI with host buffers: H2D states, coarse step, D2H states
-        r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=True)
+        r.set_use_graph(True)
         pinned = {l: torch.from_numpy(init_states[l]).pin_memory() for l in levels}
         outs = {l: torch.empty_like(pinned[l]).pin_memory() for l in levels}
         r.coarse_step(nsub=cfg.nsub)
@@ -238,6 +246,7 @@ def run_mine(args, rank, world):
         for l in levels:
             r.set_state(l, init_states[l])
         r.tsim = 0.0
+        r.adt[:] = 0.0
         for _ in range(min(args.steps, 10)):
             r.coarse_step(nsub=cfg.nsub)
         res["final"] = {l: r.state(l) for l in levels}
@@ -396,6 +405,8 @@ def main():
                      "cells_per_launch": cells_per_launch, "avg_launch_ms": mixed["kernel_avg_ms"]},
         "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": mixed["h2d"],
                 "d2h_bytes_per_step": mixed["d2h"]},
+        "autotune": {"mixed": mixed["autotune"], "fp64": fp64["autotune"],
+                     "candidates": "brick 4x4x2 octs x1 or 2x2x2 octs x4 per 256-thread tile; 1..occupancy CTAs per SM"},
         "gpu_launches": mixed["launches"],
         "clocks": mixed["clocks"],
         "status": mixed["status"],

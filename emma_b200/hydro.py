@@ -30,6 +30,7 @@ class ResidentHydro:
         self.tree = tree
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
         self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
+        self.precision = precision
         L = lib()
         o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
@@ -39,7 +40,15 @@ class ResidentHydro:
         self.adt = np.zeros(self.lmax)
         self.tsim = 0.0
 
+    def set_use_graph(self, use_graph):
+        """Switch between CUDA-graph coarse steps and the host-driven schedule
+        (the resident tree and its tuned plans stay)."""
+        self.use_graph = use_graph
+        o = options(self.precision, self.trans, self.cfl, use_graph=use_graph, tile_octs=self.tile_octs)
+        check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
+
     def set_precision(self, precision):
+        self.precision = precision
         o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs)
         check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
