@@ -21,6 +21,7 @@
 // cell's reconstruction up to 9 times and each face twice
 // (src/hydro_utils.c:1407-2238, 2973-3303).
 #pragma once
+#include <type_traits>
 #include "hydro_math.cuh"
 #include "plan_types.h"
 
@@ -139,7 +140,7 @@ static_assert(GeomA::kOcts == 32 && GeomB::kOcts == 8, "shapes match kShapes");
 
 // Per-CTA slot tables of both shapes (tile independent), at the start of
 // shared memory: box cell of child 0, brick position bit (255 outside the
-// brick), brick cell of child 0.
+// brick).
 template <class G>
 struct SlotTab {
   static constexpr size_t bytes = ((size_t)G::kSlots * 4 + 15) & ~size_t(15);
@@ -151,13 +152,11 @@ template <class G>
 __device__ __forceinline__ void slot_tables(unsigned char *tab) {
   uint16_t *sBase = reinterpret_cast<uint16_t *>(tab);
   uint8_t *sBit = tab + 2 * G::kSlots;
-  uint8_t *sTb = tab + 3 * G::kSlots;
   for (int s = threadIdx.x; s < G::kSlots; s += blockDim.x) {
     const int sz = s / (G::SX * G::SY), sy = (s / G::SX) % G::SY, sx = s % G::SX;
     sBase[s] = (uint16_t)(2 * sx + G::XX * (2 * sy + G::XY * 2 * sz));
     const bool inner = sx >= 1 && sx <= G::SX - 2 && sy >= 1 && sy <= G::SY - 2 && sz >= 1 && sz <= G::SZ - 2;
     sBit[s] = inner ? (uint8_t)((sx - 1) + (G::SX - 2) * ((sy - 1) + (G::SY - 2) * (sz - 1))) : (uint8_t)255;
-    sTb[s] = inner ? (uint8_t)(2 * (sx - 1) + G::CX * (2 * (sy - 1) + G::CY * 2 * (sz - 1))) : (uint8_t)0;
   }
 }
 
@@ -180,12 +179,11 @@ struct TileSmem {
   static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * NBOX);          // R   [NBOX] p
   static constexpr size_t off_M = a16(off_Wp + sizeof(R) * NBOX);              // R4  [5][kThreads]
   static constexpr size_t off_HS = a16(off_M + sizeof(R) * 4 * 5 * kThreads);  // R4  [2][NRING] ring faces
-  static constexpr size_t off_Q = a16(off_HS + sizeof(R) * 4 * 2 * NRING);     // f64 [5][kThreads] (FP32 path)
-  static constexpr size_t q_bytes = kF64 ? 0 : sizeof(double) * 5 * kThreads;
+  static constexpr size_t off_end = a16(off_HS + sizeof(R) * 4 * 2 * NRING);
   // face fluxes: the FP32 path reuses the staged box, dead after reconstruction
-  static constexpr size_t off_F = kF64 ? a16(off_Q + q_bytes) : off_W;  // R4 [NF]
+  static constexpr size_t off_F = kF64 ? off_end : off_W;               // R4 [NF]
   static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
-  static constexpr size_t bytes = kF64 ? a16(off_F1 + sizeof(R) * NF) : a16(off_Q + q_bytes);
+  static constexpr size_t bytes = kF64 ? a16(off_F1 + sizeof(R) * NF) : off_end;
   static_assert(kF64 || off_F1 + sizeof(R) * NF <= off_M, "FP32 face fluxes must fit in the staged box");
 };
 
@@ -204,13 +202,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   uint8_t *sCmk = smem + SM::off_cmk;
   const uint16_t *sBase = reinterpret_cast<const uint16_t *>(tab);
   const uint8_t *sBit = tab + 2 * G::kSlots;
-  const uint8_t *sTb = tab + 3 * G::kSlots;
   uint8_t *sSt = smem + SM::off_st;
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
   R *sWp = reinterpret_cast<R *>(smem + SM::off_Wp);
   R *sM = reinterpret_cast<R *>(smem + SM::off_M);
   R *sHS = reinterpret_cast<R *>(smem + SM::off_HS);
-  double *sQ = reinterpret_cast<double *>(smem + SM::off_Q);
   R *sF = reinterpret_cast<R *>(smem + SM::off_F);
   R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
 
@@ -277,7 +273,6 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     // from one pair of the boundary oct too (the mirror maps keep x-pairs).
     const int q = tid & 3, s0 = tid >> 2, c0 = 2 * q;
     const int cb = G::XX * ((q & 1) + G::XY * (q >> 1));
-    const int ct = G::CX * ((q & 1) + G::CY * (q >> 1));
     unsigned mir = 0;  // per ghost face k, 4 bits: source pair, element of child c0, of child c0+1
 #pragma unroll
     for (int k = 0; k < 6; k++) {
@@ -327,16 +322,6 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       const uint8_t f0 = sf | (((spm >> c0) & 1) ? kFSplit : 0), f1 = sf | (((spm >> (c0 + 1)) & 1) ? kFSplit : 0);
       sSt[b0] = f0;
       sSt[b0 + 1] = f1;
-      if constexpr (!F64) {
-        if (sf & kFTile) {
-          const int t = nb * G::kCells + sTb[s] + ct;
-#pragma unroll
-          for (int v = 0; v < 5; v++) {
-            sQ[v * kThreads + t] = x0[v];
-            sQ[v * kThreads + t + 1] = x1[v];
-          }
-        }
-      }
     }
   }
   __syncthreads();
@@ -427,56 +412,65 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   };
 
   // ------------------------------------------------------------------ P2
-  // Rounds 0..2: the -d face of every brick cell; then the + faces on the brick
-  // boundaries.  One HLLC call site for all rounds.
-  constexpr int kPlusTasks = G::kNB * G::kPlus;
+  // Per axis d (a compile-time constant, so the solver's axis selects fold): the
+  // -d face of every brick cell, then the +d faces on the brick boundaries,
+  // run by the last warps (z, then y, then x from the top).  One HLLC call site
+  // per axis: a face on a brick boundary, solved by both bricks, rounds the same.
+  auto solve_axis = [&](auto dc) {
+    constexpr int d = decltype(dc)::value;
+    constexpr int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+    constexpr int ts = (d == 0) ? 1 : ((d == 1) ? G::CX : G::CX * G::CY);
+    constexpr int nplus = G::kNB * ((d == 0) ? G::kPX : ((d == 1) ? G::kPY : G::kPZ));
+    constexpr int start = kThreads - G::kNB * G::kPZ - ((d < 2) ? G::kNB * G::kPY : 0) - ((d < 1) ? G::kNB * G::kPX : 0);
+    static_assert(start >= 0 && start + nplus <= kThreads, "plus faces fit the CTA");
 #pragma unroll 1
-  for (int w = tid; w < 3 * kThreads + kPlusTasks; w += kThreads) {
-    int d, e, tL, bL, jL = -1, tR, bR, jR = -1;
-    if (w < 3 * kThreads) {
-      d = w / kThreads;
-      const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
-      const int ts = (d == 0) ? 1 : ((d == 1) ? G::CX : G::CX * G::CY);
-      const int coord = (d == 0) ? tx : ((d == 1) ? ty : tz);
-      e = tn * G::kFaces + G::face_index(d, tx, ty, tz);
-      tR = tid;
-      bR = tb;
-      tL = tid - ts;
-      bL = tb - bs;
-      if (coord == 0) jL = tn * G::kRing + G::ring_index(d, false, tx, ty, tz);
-    } else {
-      const int p = w - 3 * kThreads, nb = p / G::kPlus;
-      int j = p - nb * G::kPlus, x, y, z;
-      if (j < G::kPX) {
-        d = 0; x = G::CX - 1; y = j % G::CY; z = j / G::CY;
-      } else if (j < G::kPX + G::kPY) {
-        j -= G::kPX;
-        d = 1; x = j % G::CX; y = G::CY - 1; z = j / G::CX;
+    for (int pass = 0; pass < 2; pass++) {
+      int e, tL, bL, jL = -1, tR, bR, jR = -1;
+      if (pass == 0) {
+        const int coord = (d == 0) ? tx : ((d == 1) ? ty : tz);
+        e = tn * G::kFaces + G::face_index(d, tx, ty, tz);
+        tR = tid;
+        bR = tb;
+        tL = tid - ts;
+        bL = tb - bs;
+        if (coord == 0) jL = tn * G::kRing + G::ring_index(d, false, tx, ty, tz);
       } else {
-        j -= G::kPX + G::kPY;
-        d = 2; x = j % G::CX; y = j / G::CX; z = G::CZ - 1;
+        const int p = tid - start;
+        if (p < 0 || p >= nplus) break;
+        constexpr int per = nplus / G::kNB;
+        const int nb = p / per, j = p - nb * per;
+        int x, y, z;
+        if (d == 0) {
+          x = G::CX - 1; y = j % G::CY; z = j / G::CY;
+        } else if (d == 1) {
+          x = j % G::CX; y = G::CY - 1; z = j / G::CX;
+        } else {
+          x = j % G::CX; y = j / G::CX; z = G::CZ - 1;
+        }
+        tL = nb * G::kCells + x + G::CX * (y + G::CY * z);
+        bL = nb * G::kBox + G::box_of(x, y, z);
+        tR = tL;
+        bR = bL + bs;
+        jR = nb * G::kRing + G::ring_index(d, true, x, y, z);
+        e = nb * G::kFaces + G::face_index(d, x + (d == 0), y + (d == 1), z + (d == 2));
       }
-      const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
-      tL = nb * G::kCells + x + G::CX * (y + G::CY * z);
-      bL = nb * G::kBox + G::box_of(x, y, z);
-      tR = tL;
-      bR = bL + bs;
-      jR = nb * G::kRing + G::ring_index(d, true, x, y, z);
-      e = nb * G::kFaces + G::face_index(d, x + (d == 0), y + (d == 1), z + (d == 2));
+      const uint8_t fL = sSt[bL], fR = sSt[bR];
+      R F[5] = {0, 0, 0, 0, 0};
+      if ((f_tileleaf(fL) || f_tileleaf(fR)) && f_ok(fL) && f_ok(fR)) {
+        R WL[7], WR[7];
+        if (jL >= 0) ring_face(jL, WL);
+        else brick_face(tL, bL, 2 * d + 1, WL);
+        if (jR >= 0) ring_face(jR, WR);
+        else brick_face(tR, bR, 2 * d, WR);
+        M::hllc(WL, WR, d, F, st);
+      }
+      V::st(sF, e, F[0], F[1], F[2], F[3]);
+      sF1[e] = F[4];
     }
-    const uint8_t fL = sSt[bL], fR = sSt[bR];
-    R F[5] = {0, 0, 0, 0, 0};
-    if ((f_tileleaf(fL) || f_tileleaf(fR)) && f_ok(fL) && f_ok(fR)) {
-      R WL[7], WR[7];
-      if (jL >= 0) ring_face(jL, WL);
-      else brick_face(tL, bL, 2 * d + 1, WL);
-      if (jR >= 0) ring_face(jR, WR);
-      else brick_face(tR, bR, 2 * d, WR);
-      M::hllc(WL, WR, d, F, st);
-    }
-    V::st(sF, e, F[0], F[1], F[2], F[3]);
-    sF1[e] = F[4];
-  }
+  };
+  solve_axis(std::integral_constant<int, 0>{});
+  solve_axis(std::integral_constant<int, 1>{});
+  solve_axis(std::integral_constant<int, 2>{});
   __syncthreads();
 
   // ------------------------------------------------------------------ P3
@@ -502,13 +496,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     const int s = tn * G::kSlots + ((tx + 2) >> 1) + G::SX * (((ty + 2) >> 1) + G::SY * ((tz + 2) >> 1));
     const int c = (tx & 1) | ((ty & 1) << 1) | ((tz & 1) << 2);
     const long long gi = 8LL * (sKey[s] & 0x0FFFFFFFu) + c;
-    double q[5];
+    double q[5];  // the FP64 state: staged (plain path) or read again from L2 (mixed path)
     if constexpr (F64) {
       V::ld(sW, tb, q[0], q[1], q[2], q[3]);
       q[4] = sWp[tb];
     } else {
 #pragma unroll
-      for (int v = 0; v < 5; v++) q[v] = sQ[v * kThreads + tid];
+      for (int v = 0; v < 5; v++) q[v] = __ldg(A.W + v * N8 + gi);
     }
     double Wout[5];
     if (fme & kFSplit) {
@@ -674,8 +668,14 @@ constexpr size_t level_smem_bytes(unsigned shapes) {
 // tile waiting for a finer level (listed first) never blocks the CTAs that
 // still have to finish that level.  SHAPES: the brick shapes the levels of the
 // launch use (bit i: kShapes[i]); each level's plan names its own.
+// Occupancy targets: the FP32 kernel with 4x4x2 bricks only fits 4 CTAs per SM
+// (64 registers, 55 KB of shared memory); with 2x2x2 bricks shared memory
+// allows 2; the FP64 kernel 1.
 template <class M, unsigned SHAPES>
-__global__ void __launch_bounds__(kThreads, (sizeof(typename M::R) == 8) ? 1 : 3) level_batch_kernel(const BatchArgs Bt) {
+constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? 1 : (SHAPES == 1u ? 4 : 2);
+
+template <class M, unsigned SHAPES>
+__global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
   if constexpr ((SHAPES & 1u) != 0) slot_tables<GeomA>(smem);
