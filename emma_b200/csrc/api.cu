@@ -277,8 +277,16 @@ inline void finish_prims(struct Wtype &W) {
   W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
 }
 
+// The level's state changed outside the device schedule: its next CFL step
+// comes from the reduction kernel again.
+cudaError_t mark_stale(int level) {
+  return cudaMemsetAsync(&g.d_S->fresh[level], 0, sizeof(int), g.stream);
+}
+
+// fuse_cfl: the launch also accumulates each level's max signal speed of the
+// state it writes (the device schedule's next CFL step, SchedState::smax_next).
 bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, long long cells, unsigned shapes,
-                  int ctas) {
+                  int ctas, bool fuse_cfl = false) {
   BatchArgs a;
   a.lv = d_lv;
   a.work = work;
@@ -287,6 +295,7 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
   a.gate = gate;
   a.status = g.d_status;
   a.wait_limit = kWaitLimit;
+  a.smax = fuse_cfl ? g.d_S->smax_next : nullptr;
   TimedLaunch tl{};
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(g.stream, &cap);
@@ -383,11 +392,12 @@ bool emit_level(int L, int nsub) {
     if (d.C != nullptr)
       k_clear<<<(unsigned)std::max<long long>(1, std::min<long long>((n5 + 255) / 256, 4LL * g.nsm)), 256, 0,
                 g.stream>>>(d.C, n5, gate);
-    if (!ck(launch_cfl(t.d_lv, L, d.n8, gate, &S->smax[L], g.nsm, g.stream), "cfl launch")) return false;
+    // the separate CFL reduction runs only when the level's state was not written by the level kernel
+    if (!ck(launch_cfl(t.d_lv, L, d.n8, &S->cfl_gate[L], &S->smax[L], g.nsm, g.stream), "cfl launch")) return false;
     k_sub_dt<<<1, 1, 0, g.stream>>>(S, L);
     if (has_fine && !emit_level(L + 1, nsub)) return false;
     k_sub_prelaunch<<<1, 1, 0, g.stream>>>(S, t.d_lv, L, has_fine ? 1 : 0);
-    if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf, 1u << d.shape, d.ctas)) return false;
+    if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf, 1u << d.shape, d.ctas, true)) return false;
     k_sub_end<<<1, 1, 0, g.stream>>>(S, t.d_lv, L);
     if (!ck(cudaGetLastError(), "schedule kernel")) return false;
   }
@@ -400,13 +410,15 @@ bool emit_coarse_step(int nsub) {
   SchedState *S = g.d_S;
   const int lc = t.lcoarse, lf = finest_level();
   if (nsub == 1 || lf == lc) {
-    // one dt for every level: CFL per level, then all levels in one launch
+    // one dt for every level: CFL per level (from the previous launch's fused maxima, or a
+    // reduction kernel where the state was set from the host), then all levels in one launch
+    k_batch_pre<<<1, 1, 0, g.stream>>>(S, t.d_lv);
     for (int L = lc; L <= lf; L++) {
       const DevLevel &d = t.lev[L];
-      if (!ck(cudaMemsetAsync(&S->smax[L], 0, sizeof(unsigned long long), g.stream), "memset smax")) return false;
       if (d.C != nullptr && !ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C"))
         return false;
-      if (!ck(launch_cfl(t.d_lv, L, d.n8, nullptr, &S->smax[L], g.nsm, g.stream), "cfl launch")) return false;
+      if (!ck(launch_cfl(t.d_lv, L, d.n8, &S->cfl_gate[L], &S->smax[L], g.nsm, g.stream), "cfl launch"))
+        return false;
     }
     k_batch_begin<<<1, 1, 0, g.stream>>>(S, t.d_lv, g.d_done);
     long long cells = 0;
@@ -420,7 +432,7 @@ bool emit_coarse_step(int nsub) {
         ctas = t.lev[L].ctas;
       }
     }
-    if (!launch_batch(t.d_lv, g.d_work_all, g.nwork_all, nullptr, cells, shapes, ctas)) return false;
+    if (!launch_batch(t.d_lv, g.d_work_all, g.nwork_all, nullptr, cells, shapes, ctas, true)) return false;
     k_batch_end<<<1, 1, 0, g.stream>>>(S, t.d_lv);
     return ck(cudaGetLastError(), "schedule kernel");
   }
@@ -789,6 +801,7 @@ int emma_hydro_fields_upload(struct OCT **firstoct) {
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
     pack_level(h, 0, g.pin);
     CK(cudaMemcpyAsync(W, g.pin, bytes, cudaMemcpyHostToDevice, g.stream));
+    CK(mark_stale(L));
     CK(cudaStreamSynchronize(g.stream));
   }
   return 0;
@@ -858,6 +871,7 @@ int emma_hydro_set_level_state(int level, const double *host_in) {
   double *W = current_state(level);
   if (W == nullptr) return EMMA_ST_CUDA;
   CK(cudaMemcpyAsync(W, host_in, sizeof(double) * 5 * d.n8, cudaMemcpyHostToDevice, g.stream));
+  CK(mark_stale(level));
   CK(cudaStreamSynchronize(g.stream));
   return 0;
 }
@@ -899,6 +913,7 @@ int emma_hydro_advance_level(int level, double dt) {
   if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return EMMA_ST_CUDA;
   k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
   CK(cudaGetLastError());
+  CK(mark_stale(level));
   g.updates += d.leaf;
   return 0;
 }

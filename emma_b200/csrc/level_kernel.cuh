@@ -146,7 +146,8 @@ struct SlotTab {
   static constexpr size_t bytes = ((size_t)G::kSlots * 4 + 15) & ~size_t(15);
 };
 constexpr size_t kTabOffB = SlotTab<GeomA>::bytes;
-constexpr size_t kTabBytes = kTabOffB + SlotTab<GeomB>::bytes;
+constexpr size_t kSmaxOff = kTabOffB + SlotTab<GeomB>::bytes;  // u64 [kMaxLevels] per-CTA signal-speed maxima
+constexpr size_t kTabBytes = kSmaxOff + 8 * kMaxLevels;
 
 template <class G>
 __device__ __forceinline__ void slot_tables(unsigned char *tab) {
@@ -492,6 +493,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     __syncthreads();
   }
   const uint8_t fme = sSt[tb];
+  double smx = 0.;  // |v| + c_s of the state this thread writes
   if (fme & kFTile) {
     const int s = tn * G::kSlots + ((tx + 2) >> 1) + G::SX * (((ty + 2) >> 1) + G::SY * ((tz + 2) >> 1));
     const int c = (tx & 1) | ((ty & 1) << 1) | ((tz & 1) << 2);
@@ -647,6 +649,20 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) A.Wn[v * N8 + gi] = Wout[v];
+    if (Bt.smax != nullptr) {
+      // the next time step's CFL term of this cell, as L_comptstep_hydro evaluates it
+      // (src/advanceamr.c:122-128): IEEE operations, no contraction
+      const double va = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Wout[1], Wout[1]), __dmul_rn(Wout[2], Wout[2])),
+                                             __dmul_rn(Wout[3], Wout[3])));
+      const double aa = __dsqrt_rn(__ddiv_rn(__dmul_rn(5. / 3., Wout[4]), Wout[0]));
+      smx = fmax(smx, __dadd_rn(va, aa));  // fmax drops NaN like the reference's FMAX
+    }
+  }
+  if (Bt.smax != nullptr) {
+    for (int o = 16; o > 0; o >>= 1) smx = fmax(smx, __shfl_xor_sync(0xffffffffu, smx, o));
+    if ((tid & 31) == 0 && smx > 0.)
+      atomicMax(reinterpret_cast<unsigned long long *>(smem + kSmaxOff) + slot,
+                (unsigned long long)__double_as_longlong(smx));
   }
   __syncthreads();
   if (tid == 0) {
@@ -680,6 +696,8 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
   if constexpr ((SHAPES & 1u) != 0) slot_tables<GeomA>(smem);
   if constexpr ((SHAPES & 2u) != 0) slot_tables<GeomB>(smem + kTabOffB);
+  unsigned long long *sSmax = reinterpret_cast<unsigned long long *>(smem + kSmaxOff);
+  if (threadIdx.x < kMaxLevels) sSmax[threadIdx.x] = 0ULL;
   __syncthreads();
   unsigned st = 0;
   for (int w = blockIdx.x; w < Bt.nwork; w += gridDim.x) {
@@ -696,6 +714,9 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch
     }
     __syncthreads();
   }
+  // non-negative doubles order like their bit patterns
+  if (Bt.smax != nullptr && threadIdx.x < kMaxLevels && sSmax[threadIdx.x] != 0ULL)
+    atomicMax(Bt.smax + threadIdx.x, sSmax[threadIdx.x]);
   if (st) atomicOr(Bt.status, st);
 }
 

@@ -84,6 +84,8 @@ struct BatchArgs {
   const int *gate;      // launch does nothing unless *gate != 0 (null: always run)
   unsigned *status;
   long long wait_limit; // bounded spin on `done` before reporting a timeout
+  unsigned long long *smax;  // per slot: max signal speed |v| + c_s of the states written
+                             // (bits of a non-negative double, atomicMax), or null
 };
 
 constexpr int kWorkSlotShift = 24;

@@ -17,8 +17,12 @@
 
 namespace emma {
 
+// The level's max signal speed: accumulated by the level kernel that wrote the
+// current state, or, when the state was set from the host, from the CFL
+// reduction kernel.  Both evaluate |v| + sqrt(gamma p / rho) with the same
+// IEEE operations, so the dt is the same either way.
 __device__ __forceinline__ double smax_of(const SchedState *S, int L) {
-  return __longlong_as_double((long long)S->smax[L]);
+  return __longlong_as_double((long long)(S->fresh[L] ? S->smax_next[L] : S->smax[L]));
 }
 
 // L_comptstep_hydro's final step (src/advanceamr.c:135): dt = CFL dx / (3 Smax)
@@ -62,6 +66,14 @@ __global__ void k_clear(double *p, long long n, const int *gate) {
 // overwritten by the finer level's, src/advanceamr.c:808-858).  All levels then
 // go through one launch, finest first, each level's update waiting for the finer
 // level's (corrections, new state for split-cell averaging).
+// before the CFL reductions of a batched step: which of them must run
+__global__ void k_batch_pre(SchedState *S, LevelArgs *lv) {
+  for (int L = S->lcoarse; L <= S->lmax; L++) {
+    S->cfl_gate[L] = (lv[L].noct > 0) && !S->fresh[L];
+    S->smax[L] = 0ULL;
+  }
+}
+
 __global__ void k_batch_begin(SchedState *S, LevelArgs *lv, unsigned *done) {
   const int lc = S->lcoarse, lm = S->lmax;
   double *adt = S->adt;
@@ -77,6 +89,7 @@ __global__ void k_batch_begin(SchedState *S, LevelArgs *lv, unsigned *done) {
     if (adt[L - 2] < adt[L - 1]) adt[L - 1] = adt[L - 2];
     else adt[L - 1] = fmin(adt[L - 1], adt[L - 2] - 0.);
   }
+  for (int L = lc; L <= lm; L++) S->smax_next[L] = 0ULL;  // the launch accumulates the new maxima
   int lf = lc;
   while (lf < lm && lv[lf + 1].noct > 0) lf++;
   const double dtf = adt[lf - 1];
@@ -105,6 +118,7 @@ __global__ void k_batch_end(SchedState *S, LevelArgs *lv) {
     lv[L].Wn = t;
     lv[L].wait_slot = -1;
     S->updates += lv[L].leaf;
+    S->fresh[L] = 1;
   }
   S->tsim += S->adt[lc - 1];
 }
@@ -122,6 +136,7 @@ __global__ void k_sub_begin(SchedState *S, int L, int it) {
     S->active[L] = S->active[L] && (S->dtacc[L] < S->adt[L - 2]) && (S->is[L] < S->nsub);
   }
   S->smax[L] = 0ULL;
+  S->cfl_gate[L] = S->active[L] && !S->fresh[L];
 }
 
 // dt of the iteration (src/advanceamr.c:708-830)
@@ -154,6 +169,7 @@ __global__ void k_sub_prelaunch(SchedState *S, LevelArgs *lv, int L, int has_fin
   a.Cc = (L > lc && lv[L - 1].noct > 0) ? lv[L - 1].C : nullptr;
   a.Wf = (L < lm && lv[L + 1].noct > 0) ? lv[L + 1].W : nullptr;
   a.wait_slot = -1;
+  S->smax_next[L] = 0ULL;  // the launch accumulates the new maximum
 }
 
 // bookkeeping of the iteration (src/advanceamr.c:1278-1281)
@@ -166,6 +182,7 @@ __global__ void k_sub_end(SchedState *S, LevelArgs *lv, int L) {
   S->tloc[L] += S->adt[L - 1];
   S->is[L]++;
   S->updates += lv[L].leaf;
+  S->fresh[L] = 1;
 }
 
 __global__ void k_sub_final(SchedState *S) { S->tsim += S->adt[S->lcoarse - 1]; }

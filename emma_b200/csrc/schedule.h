@@ -8,7 +8,12 @@ struct SchedState {
   double tsim, dt_param, time_max, cfl;
   double adt[kMaxLevels];               // the reference's adt array, index level-1
   double dx[kMaxLevels];                // cell size per level
-  unsigned long long smax[kMaxLevels];  // max signal speed per level (bits of a non-negative double)
+  unsigned long long smax[kMaxLevels];  // max signal speed per level from the CFL reduction kernel
+                                        // (bits of a non-negative double)
+  unsigned long long smax_next[kMaxLevels];  // the same, accumulated by the level kernel over the
+                                             // state it writes
+  int fresh[kMaxLevels];                // smax_next holds the max of the level's current state
+  int cfl_gate[kMaxLevels];             // the CFL reduction kernel runs (state changed elsewhere)
   double dtacc[kMaxLevels];             // dt accumulated by the current Advance_level(L) call
   double tloc[kMaxLevels];              // its local time
   int is[kMaxLevels];                   // its iteration count
@@ -22,6 +27,7 @@ __global__ void k_set_args(LevelArgs *lv, int slot, LevelArgs a);
 __global__ void k_bind_level(LevelArgs *lv, int L, int lcoarse, int lmax, double dt);
 __global__ void k_swap_level(LevelArgs *lv, int L, const int *gate);
 __global__ void k_clear(double *p, long long n, const int *gate);
+__global__ void k_batch_pre(SchedState *S, LevelArgs *lv);
 __global__ void k_batch_begin(SchedState *S, LevelArgs *lv, unsigned *done);
 __global__ void k_batch_end(SchedState *S, LevelArgs *lv);
 __global__ void k_sub_begin(SchedState *S, int L, int it);
