@@ -141,6 +141,17 @@ struct MathF64 {
     return p;
   }
 
+  // Two-rarefaction star state of findPressure_Hybrid (src/hydro_utils.c:645-650),
+  // {p*, u*}.  Not inlined: its pow() expansions would otherwise be repeated in
+  // every copy of the Riemann solver and crowd the instruction cache.
+  static __device__ __noinline__ double2 trrs(double aL, double aR, double uL, double uR, double pL, double pR) {
+    const double z = (kGam - 1.) / (2. * kGam);
+    const double iz = (2. * kGam) / (kGam - 1.);
+    const double pstar = pow((aL + aR - (kGam - 1.) / 2. * (uR - uL)) / (aL / pow(pL, z) + aR / pow(pR, z)), iz);
+    const double ustar = uL - 2. * aL / (kGam - 1.) * (pow(pstar / pL, z) - 1.);
+    return make_double2(pstar, ustar);
+  }
+
   // findPressure_Hybrid + speedestimate*_HLLC (src/hydro_utils.c:625,1264)
   static __device__ __forceinline__ void speeds(const double WL[7], const double WR[7], int n, double &SL, double &SR,
                                                 double &ustar, unsigned &st) {
@@ -155,10 +166,9 @@ struct MathF64 {
     if (((pmax / pmin) < 2.) && ((pmin < pstar) && (pstar < pmax))) {
       ustar = 0.5 * ((L.u + R.u) + (L.p - R.p) / (dbar * abar));
     } else if (pstar < pmin) {
-      double z = (kGam - 1.) / (2. * kGam);
-      double iz = (2. * kGam) / (kGam - 1.);
-      pstar = pow((L.a + R.a - (kGam - 1.) / 2. * (R.u - L.u)) / (L.a / pow(L.p, z) + R.a / pow(R.p, z)), iz);
-      ustar = L.u - 2. * L.a / (kGam - 1.) * (pow(pstar / L.p, z) - 1.);
+      const double2 r = trrs(L.a, R.a, L.u, R.u, L.p, R.p);
+      pstar = r.x;
+      ustar = r.y;
     } else {
       double p0 = fmax(0., ppvrs);
       double AL = 2. / ((kGam + 1.) * L.d), AR = 2. / ((kGam + 1.) * R.d);

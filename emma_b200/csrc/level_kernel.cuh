@@ -413,7 +413,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   };
 
   // ------------------------------------------------------------------ P2
-  // Per axis d (a compile-time constant, so the solver's axis selects fold): the
+  // FP32: per axis d (a compile-time constant, so the solver's axis selects fold): the
   // -d face of every brick cell, then the +d faces on the brick boundaries,
   // run by the last warps (z, then y, then x from the top).  One HLLC call site
   // per axis: a face on a brick boundary, solved by both bricks, rounds the same.
@@ -469,9 +469,62 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       sF1[e] = F[4];
     }
   };
-  solve_axis(std::integral_constant<int, 0>{});
-  solve_axis(std::integral_constant<int, 1>{});
-  solve_axis(std::integral_constant<int, 2>{});
+  if constexpr (!F64) {
+    solve_axis(std::integral_constant<int, 0>{});
+    solve_axis(std::integral_constant<int, 1>{});
+    solve_axis(std::integral_constant<int, 2>{});
+  } else {
+    // FP64: one loop over all faces with the axis at run time (one copy of the
+    // FP64 solver; three copies measured slower on trees with strong rarefactions)
+    constexpr int kPlusTasks = G::kNB * G::kPlus;
+#pragma unroll 1
+    for (int w = tid; w < 3 * kThreads + kPlusTasks; w += kThreads) {
+      int d, e, tL, bL, jL = -1, tR, bR, jR = -1;
+      if (w < 3 * kThreads) {
+        d = w / kThreads;
+        const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+        const int ts = (d == 0) ? 1 : ((d == 1) ? G::CX : G::CX * G::CY);
+        const int coord = (d == 0) ? tx : ((d == 1) ? ty : tz);
+        e = tn * G::kFaces + G::face_index(d, tx, ty, tz);
+        tR = tid;
+        bR = tb;
+        tL = tid - ts;
+        bL = tb - bs;
+        if (coord == 0) jL = tn * G::kRing + G::ring_index(d, false, tx, ty, tz);
+      } else {
+        const int p = w - 3 * kThreads, nb = p / G::kPlus;
+        int j = p - nb * G::kPlus, x, y, z;
+        if (j < G::kPX) {
+          d = 0; x = G::CX - 1; y = j % G::CY; z = j / G::CY;
+        } else if (j < G::kPX + G::kPY) {
+          j -= G::kPX;
+          d = 1; x = j % G::CX; y = G::CY - 1; z = j / G::CX;
+        } else {
+          j -= G::kPX + G::kPY;
+          d = 2; x = j % G::CX; y = j / G::CX; z = G::CZ - 1;
+        }
+        const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+        tL = nb * G::kCells + x + G::CX * (y + G::CY * z);
+        bL = nb * G::kBox + G::box_of(x, y, z);
+        tR = tL;
+        bR = bL + bs;
+        jR = nb * G::kRing + G::ring_index(d, true, x, y, z);
+        e = nb * G::kFaces + G::face_index(d, x + (d == 0), y + (d == 1), z + (d == 2));
+      }
+      const uint8_t fL = sSt[bL], fR = sSt[bR];
+      R F[5] = {0, 0, 0, 0, 0};
+      if ((f_tileleaf(fL) || f_tileleaf(fR)) && f_ok(fL) && f_ok(fR)) {
+        R WL[7], WR[7];
+        if (jL >= 0) ring_face(jL, WL);
+        else brick_face(tL, bL, 2 * d + 1, WL);
+        if (jR >= 0) ring_face(jR, WR);
+        else brick_face(tR, bR, 2 * d, WR);
+        M::hllc(WL, WR, d, F, st);
+      }
+      V::st(sF, e, F[0], F[1], F[2], F[3]);
+      sF1[e] = F[4];
+    }
+  }
   __syncthreads();
 
   // ------------------------------------------------------------------ P3
