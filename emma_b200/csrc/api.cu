@@ -776,7 +776,10 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
   CK(cudaMemcpy(g.d_S, &h, sizeof(SchedState), cudaMemcpyHostToDevice));
   rc = emma_hydro_fields_upload(firstoct);
   if (rc != 0) return rc;
-  if (!autotune_tree(g.res, shape_req)) return EMMA_ST_CUDA;
+  // EMMA_HYDRO_AUTOTUNE=0: no timing pass (plans by the cost model, CTAs at the
+  // occupancy limit), e.g. under a profiler, whose overhead distorts the timings
+  const char *tune = std::getenv("EMMA_HYDRO_AUTOTUNE");
+  if (!(tune != nullptr && tune[0] == '0') && !autotune_tree(g.res, shape_req)) return EMMA_ST_CUDA;
   // batched work list: finest level first, each level's tiles in order
   std::vector<int> all;
   for (int L = lmax; L >= lcoarse; L--)

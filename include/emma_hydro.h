@@ -152,7 +152,8 @@ int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cel
  * per tile; 8 = 2x2x2 octs, four per tile), the CTAs per SM of its launches,
  * and the measured ms per launch of every candidate, sweep_ms[4*shape + ctas-1]
  * (shape 0: 4x4x2, 1: 2x2x2; 0 = not tried).  Returns EMMA_ST_ARG if the level
- * was not tuned. */
+ * was not tuned.  EMMA_HYDRO_AUTOTUNE=0 in the environment skips the timing pass
+ * (shape from a tile-count cost model, CTAs at the occupancy limit). */
 int emma_hydro_tuning(int level, int *tile_octs, int *ctas_per_sm, double *sweep_ms);
 
 /* Planning diagnostics, host only (no GPU needed): per level lcoarse..lmax,
