@@ -397,20 +397,24 @@ struct MathF32 {
     const float E = p * (1.f / (G - 1.f)) + 0.5f * d * (un * un + t1 * t1 + t2 * t2);
     const float mn = d * un;
     float G0 = mn, GN = mn * un + p, G1 = mn * t1, G2 = mn * t2, G4 = un * (E + p);
+    // star-region correction, evaluated without branches and selected: inside the
+    // star region (SL < 0 < SR) the side condition holds for every non-NaN u*
     const bool star = !(SL >= 0.f || SR <= 0.f);
+    const bool side = (SL < 0.f && ustar >= 0.f) || (ustar <= 0.f && SR > 0.f);
+    const float S = useL ? SL : SR;
+    const float Smu = S - un;
+    const float fact = fdiv(d * Smu, S - ustar);
+    const float H0 = G0 + (fact - d) * S;
+    const float HN = GN + (fact * ustar - mn) * S;
+    const float H1 = G1 + (fact - d) * t1 * S;
+    const float H2 = G2 + (fact - d) * t2 * S;
+    const float H4 = G4 + (fact * (E * id + (ustar - un) * (ustar + fdiv(p, d * Smu))) - E) * S;
     if (star) {
-      if ((SL < 0.f && ustar >= 0.f) || (ustar <= 0.f && SR > 0.f)) {
-        const float S = useL ? SL : SR;
-        const float Smu = S - un;
-        const float fact = fdiv(d * Smu, S - ustar);
-        G0 += (fact - d) * S;
-        GN += (fact * ustar - mn) * S;
-        G1 += (fact - d) * t1 * S;
-        G2 += (fact - d) * t2 * S;
-        G4 += (fact * (E * id + (ustar - un) * (ustar + fdiv(p, d * Smu))) - E) * S;
-      } else {
-        G0 = GN = G1 = G2 = G4 = 0.f;
-      }
+      G0 = side ? H0 : 0.f;
+      GN = side ? HN : 0.f;
+      G1 = side ? H1 : 0.f;
+      G2 = side ? H2 : 0.f;
+      G4 = side ? H4 : 0.f;
     }
     F[0] = G0;
     F[1] = (n == 0) ? GN : G1;

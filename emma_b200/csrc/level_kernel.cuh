@@ -170,12 +170,13 @@ struct TileSmem {
   static constexpr int NF = G::kNB * G::kFaces;
   static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
   static constexpr size_t off_args = kTabBytes;                                // LevelArgs of the tile's level
-  static constexpr size_t off_key = a16(off_args + sizeof(LevelArgs));         // u32 [NS]
-  static constexpr size_t off_ob = a16(off_key + 4 * NS);                      // i32 [NS] source offset
-  static constexpr size_t off_sf = a16(off_ob + 4 * NS);                       // u8  [NS] slot flags
-  static constexpr size_t off_spm = a16(off_sf + NS);                          // u8  [NS] split mask (cell order)
-  static constexpr size_t off_cmk = a16(off_spm + NS);                         // u8  [NS] cell map
-  static constexpr size_t off_st = a16(off_cmk + NS);                          // u8  [NBOX] cell flags
+  // per-slot descriptors, two buffers: the current tile's and the next tile's
+  static constexpr size_t off_key = a16(off_args + sizeof(LevelArgs));         // u32 [2][NS]
+  static constexpr size_t off_ob = a16(off_key + 4 * 2 * NS);                  // i32 [2][NS] source offset
+  static constexpr size_t off_sf = a16(off_ob + 4 * 2 * NS);                   // u8  [2][NS] slot flags
+  static constexpr size_t off_spm = a16(off_sf + 2 * NS);                      // u8  [2][NS] split mask (cell order)
+  static constexpr size_t off_cmk = a16(off_spm + 2 * NS);                     // u8  [2][NS] cell map
+  static constexpr size_t off_st = a16(off_cmk + 2 * NS);                      // u8  [NBOX] cell flags
   static constexpr size_t off_W = a16(off_st + NBOX);                          // R4  [NBOX] (d,u,v,w)
   static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * NBOX);          // R   [NBOX] p
   static constexpr size_t off_M = a16(off_Wp + sizeof(R) * NBOX);              // R4  [5][kThreads]
@@ -188,19 +189,26 @@ struct TileSmem {
   static_assert(kF64 || off_F1 + sizeof(R) * NF <= off_M, "FP32 face fluxes must fit in the staged box");
 };
 
+// One tile.  Software pipeline over the tiles of a CTA: the level's arguments
+// stay in shared memory while consecutive tiles belong to the same level, and
+// the next tile's slot descriptors (next_tile >= 0: same level) are loaded
+// while this tile is reconstructed and solved, into the other descriptor
+// buffer; `cur`/`have` track which buffer holds the current tile's.
 template <class M, class G>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
-                                           unsigned char *smem, const unsigned char *tab, unsigned &st) {
+                                           const int next_tile, unsigned char *smem, const unsigned char *tab,
+                                           unsigned &st, int &cur, bool &have, int &args_slot) {
   using R = typename M::R;
   using SM = TileSmem<M, G>;
   constexpr bool F64 = SM::kF64;
   constexpr int NS = SM::NS, NRING = SM::NRING;
   using V = Q4<R>;
-  uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key);
-  int *sOb = reinterpret_cast<int *>(smem + SM::off_ob);
-  uint8_t *sSf = smem + SM::off_sf;
-  uint8_t *sSpm = smem + SM::off_spm;
-  uint8_t *sCmk = smem + SM::off_cmk;
+  uint32_t *sKey = reinterpret_cast<uint32_t *>(smem + SM::off_key) + cur * NS;
+  int *sOb = reinterpret_cast<int *>(smem + SM::off_ob) + cur * NS;
+  uint8_t *sSf = smem + SM::off_sf + cur * NS;
+  uint8_t *sSpm = smem + SM::off_spm + cur * NS;
+  uint8_t *sCmk = smem + SM::off_cmk + cur * NS;
+  const int nxt = NS * (1 - 2 * cur);  // offset of the other buffer
   const uint16_t *sBase = reinterpret_cast<const uint16_t *>(tab);
   const uint8_t *sBit = tab + 2 * G::kSlots;
   uint8_t *sSt = smem + SM::off_st;
@@ -212,12 +220,15 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
 
   const int tid = threadIdx.x;
-  // the level's arguments, read once per tile into shared memory
+  // the level's arguments in shared memory, read again only when the level changes
   LevelArgs &A = *reinterpret_cast<LevelArgs *>(smem + SM::off_args);
   static_assert(sizeof(LevelArgs) % 4 == 0, "LevelArgs copied as 32-bit words");
-  if (tid < (int)(sizeof(LevelArgs) / 4))
-    reinterpret_cast<uint32_t *>(&A)[tid] = reinterpret_cast<const uint32_t *>(gA)[tid];
-  __syncthreads();
+  if (slot != args_slot) {
+    if (tid < (int)(sizeof(LevelArgs) / 4))
+      reinterpret_cast<uint32_t *>(&A)[tid] = reinterpret_cast<const uint32_t *>(gA)[tid];
+    __syncthreads();
+    args_slot = slot;
+  }
   const long long N8 = 8LL * A.noct;
   const int tn = tid / G::kCells, tt = tid - tn * G::kCells;  // brick of the tile, cell of the brick
   int tx, ty, tz;
@@ -227,47 +238,53 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 
   // ------------------------------------------------------------------ P0
   // per slot: key, source offset, flags, split mask in cell order, cell map
-  // (0: cell c of an oct, 1: an injected cell, 2+k: mirror across face k)
-  {
+  // (0: cell c of an oct, 1: an injected cell, 2+k: mirror across face k);
+  // `raw` is the split byte of a real or ghost slot's oct
+  auto build = [&](int i, uint32_t key, uint8_t raw, uint32_t mask, int off) {
+    const int nb = i / G::kSlots, s = i - nb * G::kSlots;
+    uint8_t sf = 0, spm = 0, cmk = 0;
+    int ob = 0;
+    if (key != kKeyNone) {
+      const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
+      sf = kFPresent;
+      if (kind == kKeyReal) {
+        ob = 8 * (int)idx;
+        spm = raw;
+        const uint8_t bit = sBit[s];
+        if (bit != 255 && ((mask >> (nb * G::kOcts + bit)) & 1)) sf |= kFTile;
+      } else if (kind == kKeyInj) {
+        cmk = 1;
+        if (A.Wc != nullptr) {
+          ob = (int)idx;
+          sf |= kFInj;
+        } else {
+          st |= kStTree;  // plan/launch mismatch: never read through a null level
+        }
+      } else {
+        const int k0 = (int)(kind - kKeyGhost0);
+        ob = 8 * (int)idx;
+        cmk = (uint8_t)(2 + k0);
+#pragma unroll
+        for (int c = 0; c < 8; c++) spm |= (uint8_t)(((raw >> c_mirror[k0][c]) & 1) << c);
+      }
+    }
+    sKey[off + i] = key;
+    sOb[off + i] = ob;
+    sSf[off + i] = sf;
+    sSpm[off + i] = spm;
+    sCmk[off + i] = cmk;
+  };
+  auto split_of = [&](uint32_t key) -> uint8_t {
+    return (key != kKeyNone && (key >> 28) != kKeyInj) ? A.split[key & 0x0FFFFFFFu] : (uint8_t)0;
+  };
+  if (!have) {
     const uint32_t mask = A.tiles[tile].mask;
     for (int i = tid; i < NS; i += kThreads) {
-      const int nb = i / G::kSlots, s = i - nb * G::kSlots;
       const uint32_t key = A.keys[(size_t)tile * NS + i];
-      uint8_t sf = 0, spm = 0, cmk = 0;
-      int ob = 0;
-      if (key != kKeyNone) {
-        const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
-        sf = kFPresent;
-        if (kind == kKeyReal) {
-          ob = 8 * (int)idx;
-          spm = A.split[idx];
-          const uint8_t bit = sBit[s];
-          if (bit != 255 && ((mask >> (nb * G::kOcts + bit)) & 1)) sf |= kFTile;
-        } else if (kind == kKeyInj) {
-          cmk = 1;
-          if (A.Wc != nullptr) {
-            ob = (int)idx;
-            sf |= kFInj;
-          } else {
-            st |= kStTree;  // plan/launch mismatch: never read through a null level
-          }
-        } else {
-          const int k0 = (int)(kind - kKeyGhost0);
-          ob = 8 * (int)idx;
-          cmk = (uint8_t)(2 + k0);
-          const uint8_t raw = A.split[idx];
-#pragma unroll
-          for (int c = 0; c < 8; c++) spm |= (uint8_t)(((raw >> c_mirror[k0][c]) & 1) << c);
-        }
-      }
-      sKey[i] = key;
-      sOb[i] = ob;
-      sSf[i] = sf;
-      sSpm[i] = spm;
-      sCmk[i] = cmk;
+      build(i, key, split_of(key), mask, 0);
     }
+    __syncthreads();
   }
-  __syncthreads();
   {
     // Thread tid stages the pair q = tid & 3 of x-neighbour children (2q, 2q+1)
     // of slots tid/4 + 64 m, two cells per 16-byte load.  Ghost children come
@@ -326,6 +343,15 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
   }
   __syncthreads();
+  // the next tile's slot keys and mask (consumed after the reconstruction phase)
+  static_assert(NS <= kThreads, "one slot descriptor per thread");
+  const bool pre = next_tile >= 0 && tid < NS;
+  uint32_t nkey = kKeyNone, nmask = 0;
+  uint8_t nraw = 0;
+  if (pre) {
+    nmask = __ldg(&A.tiles[next_tile].mask);
+    nkey = __ldg(A.keys + (size_t)next_tile * NS + tid);
+  }
 
   auto q_at = [&](int b, R q[5]) {
     V::ld(sW, b, q[0], q[1], q[2], q[3]);
@@ -389,6 +415,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
   }
   __syncthreads();
+  if (pre) nraw = split_of(nkey);
 
   // face state k of brick cell t (index into the tile's cells, box cell b)
   auto brick_face = [&](int t, int b, int k, R W[7]) {
@@ -717,11 +744,14 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       atomicMax(reinterpret_cast<unsigned long long *>(smem + kSmaxOff) + slot,
                 (unsigned long long)__double_as_longlong(smx));
   }
+  if (pre) build(tid, nkey, nraw, nmask, nxt);
   __syncthreads();
   if (tid == 0) {
     __threadfence();
     atomicAdd(Bt.done + slot, 1u);
   }
+  have = next_tile >= 0;
+  if (have) cur ^= 1;
 }
 
 // Bytes of dynamic shared memory of a kernel handling the shapes in `shapes`
@@ -742,6 +772,9 @@ constexpr size_t level_smem_bytes(unsigned shapes) {
 // allows 2; the FP64 kernel 1.
 template <class M, unsigned SHAPES>
 constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? 1 : (SHAPES == 1u ? 4 : 2);
+// 228 KB of shared memory per SM, 1 KB reserved per CTA
+static_assert(4 * (TileSmem<MathF32, GeomA>::bytes + 1024) <= 228 * 1024, "4 FP32 4x4x2 CTAs per SM");
+static_assert(2 * (TileSmem<MathF32, GeomB>::bytes + 1024) <= 228 * 1024, "2 FP32 2x2x2 CTAs per SM");
 
 template <class M, unsigned SHAPES>
 __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch_kernel(const BatchArgs Bt) {
@@ -753,17 +786,28 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch
   if (threadIdx.x < kMaxLevels) sSmax[threadIdx.x] = 0ULL;
   __syncthreads();
   unsigned st = 0;
+  int cur = 0, args_slot = -1;
+  bool have = false;
+  constexpr int kTileMask = (1 << kWorkSlotShift) - 1;
   for (int w = blockIdx.x; w < Bt.nwork; w += gridDim.x) {
     const int item = Bt.work[w];
-    const int slot = item >> kWorkSlotShift, tile = item & ((1 << kWorkSlotShift) - 1);
+    const int slot = item >> kWorkSlotShift, tile = item & kTileMask;
+    // this CTA's next item: its descriptors are prefetched if it is on the same level
+    int next_tile = -1;
+    if (w + (int)gridDim.x < Bt.nwork) {
+      const int itn = Bt.work[w + gridDim.x];
+      if ((itn >> kWorkSlotShift) == slot) next_tile = itn & kTileMask;
+    }
     const LevelArgs *gA = Bt.lv + slot;
     if constexpr (SHAPES == 1u) {
-      level_tile<M, GeomA>(Bt, gA, slot, tile, smem, smem, st);
+      level_tile<M, GeomA>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
     } else if constexpr (SHAPES == 2u) {
-      level_tile<M, GeomB>(Bt, gA, slot, tile, smem, smem + kTabOffB, st);
+      level_tile<M, GeomB>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
     } else {
-      if (gA->shape == 0) level_tile<M, GeomA>(Bt, gA, slot, tile, smem, smem, st);
-      else level_tile<M, GeomB>(Bt, gA, slot, tile, smem, smem + kTabOffB, st);
+      if (gA->shape == 0)
+        level_tile<M, GeomA>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+      else
+        level_tile<M, GeomB>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
     }
     __syncthreads();
   }
