@@ -46,7 +46,7 @@ def _gauss_field(n, rng, slope, kmin, kmax, kfilter=None):
     if kfilter is not None:
         amp *= np.exp(-k * k / (4.0 * kfilter * kfilter))  # sqrt of exp(-k^2/(2 kf^2))
     noise = rng.standard_normal((n, n, n))
-    f = np.fft.irfftn(np.fft.rfftn(noise) * amp, s=(n, n, n))
+    f = np.fft.irfftn(np.fft.rfftn(noise) * amp, s=(n, n, n), axes=(0, 1, 2))
     f -= f.mean()
     return f / f.std()
 
@@ -249,7 +249,7 @@ def cosmo(base=7, lmax=10, seed=SEED, sigma=None, steps=20, target_cells=(5e6, 1
         k2[0, 0, 0] = 1.0
         dk = np.fft.rfftn(delta)
         phik = -dk / k2
-        vel = [np.fft.irfftn(1j * kk * phik, s=(n, n, n)) for kk in (kx, ky, kz)]
+        vel = [np.fft.irfftn(1j * kk * phik, s=(n, n, n), axes=(0, 1, 2)) for kk in (kx, ky, kz)]
         cs = np.sqrt(GAMMA * 1e-2 * np.mean(rho ** (GAMMA - 1.0)))
         vr = np.sqrt(np.mean(vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2))
         vel = [v * (0.3 * cs / vr) for v in vel]

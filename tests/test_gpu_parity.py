@@ -304,3 +304,27 @@ def test_autotuner_record_and_batched_step(gpu):
     tsim, _, err = oracle.Restatement().run(to.firstoct, cfg.lcoarse, cfg.lmax, 2, CFL, nsub=1)
     assert err == 0 and r.tsim == tsim
     assert_close(t, to, range(cfg.lcoarse, cfg.lmax + 1), 1e-12)
+
+
+@pytest.mark.parametrize("lmax", [7, 8])
+def test_fp64_cosmology_tree_one_step(gpu, lmax):
+    """Strongly refined tree (density > 8x mean, the reference's 26-neighbour check
+    rule), subcycled; the autotuner picks the bricks per level."""
+    cfg = configs.cosmo(base=5, lmax=lmax)
+    tg, r, st = run_gpu(cfg, 1)
+    assert st == 0
+    to, tsim = run_oracle(cfg, 1)
+    assert r.tsim == tsim
+    assert_close(tg, to, range(cfg.lcoarse, cfg.lmax + 1), 1e-12)
+
+
+def test_mixed_cosmology_tree_l1(gpu):
+    cfg = configs.cosmo(base=5, lmax=7)
+    tm, r, st = run_gpu(cfg, 3, precision=PREC_MIXED)
+    assert st == 0
+    to, _ = run_oracle(cfg, 3)
+    for l in range(cfg.lcoarse, cfg.lmax + 1):
+        leaf = ~to.split_mask(l)
+        fm, fo = tm.get_fields(l), to.get_fields(l)
+        assert l1_rel(fm[0][leaf], fo[0][leaf]) <= 1e-5
+        assert l1_rel(fm[4][leaf], fo[4][leaf]) <= 1e-5
