@@ -280,7 +280,10 @@ inline void finish_prims(struct Wtype &W) {
 // The level's state changed outside the device schedule: its next CFL step
 // comes from the reduction kernel again.
 cudaError_t mark_stale(int level) {
-  return cudaMemsetAsync(&g.d_S->fresh[level], 0, sizeof(int), g.stream);
+  cudaError_t e = cudaMemsetAsync(&g.d_S->fresh[level], 0, sizeof(int), g.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&g.d_S->smax[level], 0, sizeof(unsigned long long), g.stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(&g.d_S->stale[level], 1, sizeof(int), g.stream);  // nonzero
+  return e;
 }
 
 // fuse_cfl: the launch also accumulates each level's max signal speed of the
@@ -412,12 +415,11 @@ bool emit_coarse_step(int nsub) {
   if (nsub == 1 || lf == lc) {
     // one dt for every level: CFL per level (from the previous launch's fused maxima, or a
     // reduction kernel where the state was set from the host), then all levels in one launch
-    k_batch_pre<<<1, 1, 0, g.stream>>>(S, t.d_lv);
     for (int L = lc; L <= lf; L++) {
       const DevLevel &d = t.lev[L];
       if (d.C != nullptr && !ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C"))
         return false;
-      if (!ck(launch_cfl(t.d_lv, L, d.n8, &S->cfl_gate[L], &S->smax[L], g.nsm, g.stream), "cfl launch"))
+      if (!ck(launch_cfl(t.d_lv, L, d.n8, &S->stale[L], &S->smax[L], g.nsm, g.stream), "cfl launch"))
         return false;
     }
     k_batch_begin<<<1, 1, 0, g.stream>>>(S, t.d_lv, g.d_done);

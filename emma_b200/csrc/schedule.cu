@@ -66,14 +66,6 @@ __global__ void k_clear(double *p, long long n, const int *gate) {
 // overwritten by the finer level's, src/advanceamr.c:808-858).  All levels then
 // go through one launch, finest first, each level's update waiting for the finer
 // level's (corrections, new state for split-cell averaging).
-// before the CFL reductions of a batched step: which of them must run
-__global__ void k_batch_pre(SchedState *S, LevelArgs *lv) {
-  for (int L = S->lcoarse; L <= S->lmax; L++) {
-    S->cfl_gate[L] = (lv[L].noct > 0) && !S->fresh[L];
-    S->smax[L] = 0ULL;
-  }
-}
-
 __global__ void k_batch_begin(SchedState *S, LevelArgs *lv, unsigned *done) {
   const int lc = S->lcoarse, lm = S->lmax;
   double *adt = S->adt;
@@ -119,6 +111,7 @@ __global__ void k_batch_end(SchedState *S, LevelArgs *lv) {
     lv[L].wait_slot = -1;
     S->updates += lv[L].leaf;
     S->fresh[L] = 1;
+    S->stale[L] = 0;
   }
   S->tsim += S->adt[lc - 1];
 }
@@ -136,7 +129,7 @@ __global__ void k_sub_begin(SchedState *S, int L, int it) {
     S->active[L] = S->active[L] && (S->dtacc[L] < S->adt[L - 2]) && (S->is[L] < S->nsub);
   }
   S->smax[L] = 0ULL;
-  S->cfl_gate[L] = S->active[L] && !S->fresh[L];
+  S->cfl_gate[L] = S->active[L] && S->stale[L];
 }
 
 // dt of the iteration (src/advanceamr.c:708-830)
@@ -183,6 +176,7 @@ __global__ void k_sub_end(SchedState *S, LevelArgs *lv, int L) {
   S->is[L]++;
   S->updates += lv[L].leaf;
   S->fresh[L] = 1;
+  S->stale[L] = 0;
 }
 
 __global__ void k_sub_final(SchedState *S) { S->tsim += S->adt[S->lcoarse - 1]; }

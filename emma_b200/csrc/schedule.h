@@ -13,7 +13,9 @@ struct SchedState {
   unsigned long long smax_next[kMaxLevels];  // the same, accumulated by the level kernel over the
                                              // state it writes
   int fresh[kMaxLevels];                // smax_next holds the max of the level's current state
-  int cfl_gate[kMaxLevels];             // the CFL reduction kernel runs (state changed elsewhere)
+  int stale[kMaxLevels];                // !fresh: the state was set from the host (smax is then
+                                        // zeroed with it, for the reduction kernel)
+  int cfl_gate[kMaxLevels];             // subcycled iteration: active and stale
   double dtacc[kMaxLevels];             // dt accumulated by the current Advance_level(L) call
   double tloc[kMaxLevels];              // its local time
   int is[kMaxLevels];                   // its iteration count
@@ -27,7 +29,6 @@ __global__ void k_set_args(LevelArgs *lv, int slot, LevelArgs a);
 __global__ void k_bind_level(LevelArgs *lv, int L, int lcoarse, int lmax, double dt);
 __global__ void k_swap_level(LevelArgs *lv, int L, const int *gate);
 __global__ void k_clear(double *p, long long n, const int *gate);
-__global__ void k_batch_pre(SchedState *S, LevelArgs *lv);
 __global__ void k_batch_begin(SchedState *S, LevelArgs *lv, unsigned *done);
 __global__ void k_batch_end(SchedState *S, LevelArgs *lv);
 __global__ void k_sub_begin(SchedState *S, int L, int it);
