@@ -62,6 +62,7 @@ SIGNATURES = [
     ("emma_hydro_reset_counters", None, []),
     ("emma_hydro_kernel_timing", c_int, [P(c_double), P(c_ll), P(c_ll)]),
     ("emma_hydro_tuning", c_int, [c_int, P(c_int), P(c_int), c_void_p]),
+    ("emma_hydro_probe_wait_timeout", c_int, [c_ll]),
     ("emma_hydro_plan_stats", c_int, [c_void_p, c_int, c_int, c_int, c_void_p]),
     ("emma_hydro_level_dt_noalloc", c_int, [c_void_p, c_ll, c_int, c_double, c_void_p, P(c_double)]),
     ("emma_tree_create", c_void_p, [c_int, c_int, c_ll]),

@@ -67,6 +67,7 @@ struct Ctx {
   bool own_stream = true;
   int nsm = 148;
   unsigned *d_status = nullptr;
+  long long wait_limit = kWaitLimit;  // polls of a bounded device-side wait
   unsigned *d_done = nullptr;    // kMaxLevels completion counters
   SchedState *d_S = nullptr;
   SchedState *h_S = nullptr;     // pinned staging of the schedule state
@@ -297,7 +298,7 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
   a.done = g.d_done;
   a.gate = gate;
   a.status = g.d_status;
-  a.wait_limit = kWaitLimit;
+  a.wait_limit = g.wait_limit;
   a.smax = fuse_cfl ? g.d_S->smax_next : nullptr;
   TimedLaunch tl{};
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
@@ -998,6 +999,41 @@ void emma_hydro_reset_counters(void) {
     g.free_events.push_back(t.b);
   }
   g.launches.clear();
+}
+
+int emma_hydro_probe_wait_timeout(long long polls) {
+  if (!g.res.valid) {
+    fail(EMMA_ST_ARG, "no tree uploaded");
+    return EMMA_ST_ARG;
+  }
+  if (polls < 0) return EMMA_ST_ARG;
+  const int L = g.res.lcoarse;
+  const DevLevel &d = g.res.lev[L];
+  if (d.ntiles == 0) return EMMA_ST_ARG;
+  unsigned status0 = 0, bits = 0;
+  CK(cudaStreamSynchronize(g.stream));
+  CK(cudaMemcpy(&status0, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  CK(cudaMemset(g.d_status, 0, sizeof(unsigned)));
+  CK(cudaMemset(g.d_done, 0, sizeof(unsigned) * kMaxLevels));
+  // dt = 0, then the level's update waits for all of the level's own tiles:
+  // a count that no tile can reach before its own wait ends
+  k_bind_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, L, g.res.lcoarse, g.res.lmax, 0.);
+  const int self = L;
+  CK(cudaMemcpyAsync(&g.res.d_lv[L].wait_slot, &self, sizeof(int), cudaMemcpyHostToDevice, g.stream));
+  const long long limit0 = g.wait_limit;
+  const bool timing0 = g.timing;
+  g.wait_limit = polls;
+  g.timing = false;
+  const bool ok = launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, 0, 1u << d.shape, d.ctas);
+  g.wait_limit = limit0;
+  g.timing = timing0;
+  k_bind_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, L, g.res.lcoarse, g.res.lmax, 0.);  // wait_slot back to -1
+  CK(cudaStreamSynchronize(g.stream));
+  if (!ok) return EMMA_ST_CUDA;
+  CK(cudaMemcpy(&bits, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(g.d_status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice));
+  CK(cudaMemset(g.d_done, 0, sizeof(unsigned) * kMaxLevels));
+  return (int)bits;
 }
 
 int emma_hydro_tuning(int level, int *tile_octs, int *ctas_per_sm, double *sweep_ms) {

@@ -367,6 +367,14 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
     if (corrected[i]) lv.inj_cells.push_back((int32_t)i);
   for (uint32_t key : lv.keys)
     if (key != kKeyNone && (key >> 28) == kKeyInj) lv.reads_coarse = true;
+  if (lv.reads_coarse && H.trans != 0) {
+    // the reference's transmissive build (-DHYDROTEST) fills coarser neighbours by
+    // limited interpolation (coarse2fine_hydro2, src/hydro_utils.c:311), not by
+    // the injection this path stages
+    err = "transmissive boundaries with a coarser neighbour at level " + std::to_string(L) +
+          ": the reference interpolates coarse neighbours in that build, which is not staged here";
+    return EMMA_ST_TREE;
+  }
   return 0;
 }
 

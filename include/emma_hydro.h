@@ -156,6 +156,15 @@ int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cel
  * (shape from a tile-count cost model, CTAs at the occupancy limit). */
 int emma_hydro_tuning(int level, int *tile_octs, int *ctas_per_sm, double *sweep_ms);
 
+/* Diagnostics of the bounded device-side waits (a batched launch's update phase
+ * waits for the finer level's tiles; every wait gives up after a bounded number
+ * of polls and reports EMMA_ST_TIMEOUT instead of hanging).  Launches the
+ * coarsest resident level once with its update waiting for a completion count
+ * that no tile can reach, each wait bounded by `polls` (64 ns each), and returns
+ * the status bits of that launch (EMMA_ST_TIMEOUT expected).  The resident state,
+ * the sticky status and the completion counters are left as they were. */
+int emma_hydro_probe_wait_timeout(long long polls);
+
 /* Planning diagnostics, host only (no GPU needed): per level lcoarse..lmax,
  * stats5[5*(L-lcoarse)+{0..4}] = octs, tiles (4x4x2-oct bricks), max staged
  * octs per tile, staged octs summed over the tiles, leaf cells.  Returns
