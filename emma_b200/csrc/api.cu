@@ -22,6 +22,7 @@ cudaError_t launch_level_f32(const BatchArgs &a, unsigned shapes, int nsm, int c
                              int *occupancy);
 cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *gate, unsigned long long *out, int nsm,
                        cudaStream_t s);
+cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s);
 }  // namespace emma
 
 using namespace emma;
@@ -40,6 +41,9 @@ struct DevLevel {
   TileDesc *tiles = nullptr;
   uint32_t *keys = nullptr;
   int *work = nullptr;  // (L << 24) | tile for every tile of the level
+  int *vcell = nullptr;    // transmissive build: interpolated coarser cells and their slope neighbours
+  double *Wv = nullptr;    // their 8 interpolated sub-cells
+  long long nv = 0;
   int shape = 0;        // brick shape of the plan (kShapes)
   int ctas = 0;         // CTAs per SM of its launches (0: the occupancy limit)
   // autotuner record: chosen shape/CTAs and the swept times (ms per launch, 0 = not run)
@@ -171,6 +175,8 @@ void free_level(DevLevel &d) {
   cudaFree(d.tiles);
   cudaFree(d.keys);
   cudaFree(d.work);
+  cudaFree(d.vcell);
+  cudaFree(d.Wv);
   d = DevLevel();
 }
 
@@ -224,6 +230,11 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     if (!upload_vec(&d.child, h.child)) return false;
     if (!upload_vec(&d.tiles, h.tiles)) return false;
     if (!upload_vec(&d.keys, h.keys)) return false;
+    d.nv = (long long)h.interp.size() / 7;
+    if (d.nv > 0) {
+      if (!upload_vec(&d.vcell, h.interp)) return false;
+      if (!ck(cudaMalloc(&d.Wv, sizeof(double) * 5 * 8 * (size_t)d.nv), "cudaMalloc Wv")) return false;
+    }
     std::vector<int> work((size_t)d.ntiles);
     for (int i = 0; i < d.ntiles; i++) work[i] = (L << kWorkSlotShift) | i;
     if (!upload_vec(&d.work, work)) return false;
@@ -242,6 +253,9 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     a.tiles = d.tiles;
     a.keys = d.keys;
     a.shape = h.shape;
+    a.Wv = d.Wv;
+    a.vcell = d.vcell;
+    a.nv = d.nv;
     a.dx = std::pow(0.5, L);
     a.ntiles = d.ntiles;
     a.wait_slot = -1;
@@ -401,6 +415,7 @@ bool emit_level(int L, int nsub) {
     k_sub_dt<<<1, 1, 0, g.stream>>>(S, L);
     if (has_fine && !emit_level(L + 1, nsub)) return false;
     k_sub_prelaunch<<<1, 1, 0, g.stream>>>(S, t.d_lv, L, has_fine ? 1 : 0);
+    if (!ck(launch_interp(t.d_lv, L, d.nv, gate, g.nsm, g.stream), "interpolation launch")) return false;
     if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf, 1u << d.shape, d.ctas, true)) return false;
     k_sub_end<<<1, 1, 0, g.stream>>>(S, t.d_lv, L);
     if (!ck(cudaGetLastError(), "schedule kernel")) return false;
@@ -424,6 +439,8 @@ bool emit_coarse_step(int nsub) {
         return false;
     }
     k_batch_begin<<<1, 1, 0, g.stream>>>(S, t.d_lv, g.d_done);
+    for (int L = lc; L <= lf; L++)
+      if (!ck(launch_interp(t.d_lv, L, t.lev[L].nv, nullptr, g.nsm, g.stream), "interpolation launch")) return false;
     long long cells = 0;
     unsigned shapes = 0;
     int ctas = 0, most = -1;
@@ -613,6 +630,19 @@ int requested_shape(int tile_octs) {
   return -2;
 }
 
+// Point a level slot at a plan (tiles, keys, brick shape, interpolation list).
+bool bind_plan(LevelArgs *slot, TileDesc *tiles, uint32_t *keys, int shape, int ntiles, double *Wv, int *vcell,
+               long long nv) {
+  return ck(cudaMemcpyAsync(&slot->tiles, &tiles, sizeof(tiles), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaMemcpyAsync(&slot->keys, &keys, sizeof(keys), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaMemcpyAsync(&slot->shape, &shape, sizeof(int), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaMemcpyAsync(&slot->ntiles, &ntiles, sizeof(int), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaMemcpyAsync(&slot->Wv, &Wv, sizeof(Wv), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaMemcpyAsync(&slot->vcell, &vcell, sizeof(vcell), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaMemcpyAsync(&slot->nv, &nv, sizeof(nv), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaStreamSynchronize(g.stream), "bind");
+}
+
 // Autotuner.  For every level of the resident tree it times single-level
 // launches of the level kernel on the level's own state (dt = 0: the arithmetic
 // of a real step, no change of state) for each candidate brick shape (4x4x2
@@ -642,36 +672,38 @@ bool autotune_tree(Tree &t, int shape_req) {
     for (int s = 0; s < kNumShapes && ok; s++) {
       if (shape_req >= 0 && s != shape_req) continue;
       if (shape_req < 0 && complete && s != 0) continue;
-      // the candidate plan on the device (the current one, or a re-plan)
+      // the candidate plan on the device (the current one, or a re-plan with its
+      // own interpolation list and buffer)
       TileDesc *tiles = d.tiles;
       uint32_t *keys = d.keys;
-      int *work = d.work;
+      int *work = d.work, *vcell = d.vcell;
+      double *Wv = d.Wv;
+      long long nv = d.nv;
       int ntiles = d.ntiles;
       HostLevel alt;
       if (s != d.shape) {
         std::string err;
-        alt = h;
         HostLevel saved = h;
-        h = alt;
         const int rc = replan_level(t.host, L, s, err);
         alt = h;
         h = saved;
         if (rc != 0) continue;  // shape not plannable here: skip the candidate
         ntiles = (int)alt.tiles.size();
+        nv = (long long)alt.interp.size() / 7;
         std::vector<int> wl((size_t)ntiles);
         for (int i = 0; i < ntiles; i++) wl[i] = (L << kWorkSlotShift) | i;
-        if (!upload_vec(&tiles, alt.tiles) || !upload_vec(&keys, alt.keys) || !upload_vec(&work, wl)) {
+        vcell = nullptr;
+        Wv = nullptr;
+        if (!upload_vec(&tiles, alt.tiles) || !upload_vec(&keys, alt.keys) || !upload_vec(&work, wl) ||
+            (nv > 0 && (!upload_vec(&vcell, alt.interp) ||
+                        !ck(cudaMalloc(&Wv, sizeof(double) * 5 * 8 * (size_t)nv), "cudaMalloc Wv")))) {
           ok = false;
           break;
         }
       }
-      LevelArgs *slot = t.d_lv + L;
-      const int shape_i = s;
-      ok = ck(cudaMemcpyAsync(&slot->tiles, &tiles, sizeof(tiles), cudaMemcpyHostToDevice, g.stream), "tune") &&
-           ck(cudaMemcpyAsync(&slot->keys, &keys, sizeof(keys), cudaMemcpyHostToDevice, g.stream), "tune") &&
-           ck(cudaMemcpyAsync(&slot->shape, &shape_i, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune") &&
-           ck(cudaMemcpyAsync(&slot->ntiles, &ntiles, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune");
+      ok = bind_plan(t.d_lv + L, tiles, keys, s, ntiles, Wv, vcell, nv);
       k_bind_level<<<1, 1, 0, g.stream>>>(t.d_lv, L, t.lcoarse, t.lmax, 0.);
+      if (ok) ok = ck(launch_interp(t.d_lv, L, nv, nullptr, g.nsm, g.stream), "interpolation launch");
       int occ = 0;
       BatchArgs probe{};
       if (ok)
@@ -695,32 +727,34 @@ bool autotune_tree(Tree &t, int shape_req) {
         }
       }
       if (s != d.shape) {
+        cudaStreamSynchronize(g.stream);
         if (ok && best_shape == s) {
           // the re-plan wins so far: it becomes the level's plan
-          cudaStreamSynchronize(g.stream);
           cudaFree(d.tiles);
           cudaFree(d.keys);
           cudaFree(d.work);
+          cudaFree(d.vcell);
+          cudaFree(d.Wv);
           d.tiles = tiles;
           d.keys = keys;
           d.work = work;
+          d.vcell = vcell;
+          d.Wv = Wv;
+          d.nv = nv;
           d.ntiles = ntiles;
           d.shape = s;
           h = alt;
         } else {
-          cudaStreamSynchronize(g.stream);
           cudaFree(tiles);
           cudaFree(keys);
           cudaFree(work);
+          cudaFree(vcell);
+          cudaFree(Wv);
         }
       }
     }
     // bind the kept plan
-    LevelArgs *slot = t.d_lv + L;
-    ok = ok && ck(cudaMemcpyAsync(&slot->tiles, &d.tiles, sizeof(d.tiles), cudaMemcpyHostToDevice, g.stream), "tune") &&
-         ck(cudaMemcpyAsync(&slot->keys, &d.keys, sizeof(d.keys), cudaMemcpyHostToDevice, g.stream), "tune") &&
-         ck(cudaMemcpyAsync(&slot->shape, &d.shape, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune") &&
-         ck(cudaMemcpyAsync(&slot->ntiles, &d.ntiles, sizeof(int), cudaMemcpyHostToDevice, g.stream), "tune") &&
+    ok = ok && bind_plan(t.d_lv + L, d.tiles, d.keys, d.shape, d.ntiles, d.Wv, d.vcell, d.nv) &&
          ck(cudaStreamSynchronize(g.stream), "tune");
     d.ctas = best_ctas;
     d.tuned = ok;
@@ -916,6 +950,7 @@ int emma_hydro_advance_level(int level, double dt) {
   if (d.noct == 0) return 0;
   k_bind_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, g.res.lcoarse, g.res.lmax, dt);
   CK(cudaGetLastError());
+  CK(launch_interp(g.res.d_lv, level, d.nv, nullptr, g.nsm, g.stream));
   if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return EMMA_ST_CUDA;
   k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
   CK(cudaGetLastError());
@@ -1192,6 +1227,9 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   a.tiles = d.tiles;
   a.keys = d.keys;
   a.shape = h.shape;
+  a.Wv = d.Wv;
+  a.vcell = d.vcell;
+  a.nv = d.nv;
   a.dt = dtnew;
   a.dx = std::pow(0.5, level);
   a.ntiles = d.ntiles;
@@ -1199,6 +1237,7 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   a.leaf = d.leaf;
   k_set_args<<<1, 1, 0, g.stream>>>(g.drop.d_lv, level, a);
   if (!ck(cudaGetLastError(), "k_set_args")) return 0;
+  if (!ck(launch_interp(g.drop.d_lv, level, d.nv, nullptr, g.nsm, g.stream), "interpolation launch")) return 0;
   if (!launch_batch(g.drop.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return 0;
   // download the level's new state into fieldnew (leaf cells)
   if (!ck(cudaMemcpyAsync(g.pin, d.W1, sizeof(double) * 5 * n8, cudaMemcpyDeviceToHost, g.stream), "D2H Wn")) return 0;

@@ -42,3 +42,50 @@ cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *g
 }
 
 }  // namespace emma
+
+namespace emma {
+
+// coarse2fine_hydro2 (src/hydro_utils.c:311-420) for the transmissive build's
+// gather: each listed level L-1 cell is interpolated into 8 sub-cells with
+// minmod-limited slopes from its listed neighbours, W = W0 + ox Dx + oy Dy + oz Dz
+// with o = -0.25 or +0.25, evaluated in that order (built with -fmad=false).
+__device__ __forceinline__ double minmod_w(double m, double p) {
+  if (p > 0) return fmax(fmax(0., fmin(m, p)), fmin(m, p));
+  return fmin(fmin(0., fmax(m, p)), fmax(m, p));
+}
+
+__global__ void interp_coarse_kernel(const LevelArgs *lv, int slot, const int *gate) {
+  if (gate != nullptr && *gate == 0) return;
+  const LevelArgs &A = lv[slot];
+  const double *Wc = A.Wc;
+  if (Wc == nullptr || A.Wv == nullptr) return;
+  const long long nc8 = A.nc8, nv = A.nv, nv8 = 8 * A.nv;
+  for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nv; j += (long long)gridDim.x * blockDim.x) {
+    const int *vc = A.vcell + 7 * j;
+    double q0[5], D[3][5];
+#pragma unroll
+    for (int v = 0; v < 5; v++) q0[v] = Wc[v * nc8 + vc[0]];
+#pragma unroll
+    for (int dir = 0; dir < 3; dir++) {
+      const int cm = vc[1 + 2 * dir], cp = vc[2 + 2 * dir];
+#pragma unroll
+      for (int v = 0; v < 5; v++) D[dir][v] = minmod_w(q0[v] - Wc[v * nc8 + cm], Wc[v * nc8 + cp] - q0[v]);
+    }
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      const double ox = (c & 1) ? 0.25 : -0.25, oy = ((c >> 1) & 1) ? 0.25 : -0.25, oz = (c >> 2) ? 0.25 : -0.25;
+#pragma unroll
+      for (int v = 0; v < 5; v++) A.Wv[v * nv8 + 8 * j + c] = q0[v] + ox * D[0][v] + oy * D[1][v] + oz * D[2][v];
+    }
+  }
+}
+
+cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s) {
+  if (nv <= 0) return cudaSuccess;
+  long long blocks = (nv + 127) / 128;
+  if (blocks > 4LL * nsm) blocks = 4LL * nsm;
+  interp_coarse_kernel<<<(unsigned)blocks, 128, 0, s>>>(lv, slot, gate);
+  return cudaGetLastError();
+}
+
+}  // namespace emma

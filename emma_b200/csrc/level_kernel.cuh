@@ -65,8 +65,8 @@ __constant__ uint8_t c_mirror[6][8] = {
     {0, 0, 2, 2, 4, 4, 6, 6}, {1, 1, 3, 3, 5, 5, 7, 7}, {0, 1, 0, 1, 4, 5, 4, 5},
     {2, 3, 2, 3, 7, 6, 6, 7}, {0, 1, 2, 3, 0, 1, 2, 3}, {4, 5, 6, 7, 4, 5, 6, 7}};
 
-// cell flags of the staged box
-constexpr uint8_t kFPresent = 1, kFSplit = 2, kFTile = 4, kFInj = 8;
+// cell flags of the staged box (kFInterp: the slot reads the interpolated coarse cells)
+constexpr uint8_t kFPresent = 1, kFSplit = 2, kFTile = 4, kFInj = 8, kFInterp = 16;
 __device__ __forceinline__ bool f_ok(uint8_t f) { return (f & (kFPresent | kFSplit)) == kFPresent; }
 __device__ __forceinline__ bool f_tileleaf(uint8_t f) {
   return (f & (kFPresent | kFSplit | kFTile)) == (kFPresent | kFTile);
@@ -260,6 +260,14 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         } else {
           st |= kStTree;  // plan/launch mismatch: never read through a null level
         }
+      } else if (kind == kKeyInterp) {
+        if (A.Wv != nullptr) {  // 8 interpolated sub-cells, laid out like an oct
+          ob = 8 * (int)idx;
+          sf |= kFInj | kFInterp;
+        } else {
+          st |= kStTree;
+          cmk = 1;
+        }
       } else {
         const int k0 = (int)(kind - kKeyGhost0);
         ob = 8 * (int)idx;
@@ -275,7 +283,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     sCmk[off + i] = cmk;
   };
   auto split_of = [&](uint32_t key) -> uint8_t {
-    return (key != kKeyNone && (key >> 28) != kKeyInj) ? A.split[key & 0x0FFFFFFFu] : (uint8_t)0;
+    const uint32_t kind = key >> 28;
+    return (key != kKeyNone && kind != kKeyInj && kind != kKeyInterp) ? A.split[key & 0x0FFFFFFFu] : (uint8_t)0;
   };
   if (!have) {
     const uint32_t mask = A.tiles[tile].mask;
@@ -323,11 +332,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       } else {
         unsigned code = (unsigned)q | (1u << 3);  // pair q, elements 0 and 1
         if (cmk >= 2) code = (mir >> (4 * (cmk - 2))) & 15u;
-        const double *p = W + (long long)sOb[sg] + 2 * (code & 3);
+        const bool itp = sf & kFInterp;
+        const double *p = (itp ? A.Wv : W) + (long long)sOb[sg] + 2 * (code & 3);
+        const long long stride = itp ? 8 * A.nv : N8;
         const bool e0 = (code >> 2) & 1, e1 = (code >> 3) & 1;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          const double2 x = __ldg(reinterpret_cast<const double2 *>(p + v * N8));
+          const double2 x = __ldg(reinterpret_cast<const double2 *>(p + v * stride));
           x0[v] = e0 ? x.y : x.x;
           x1[v] = e1 ? x.y : x.x;
         }
@@ -718,8 +729,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         if (!(sSt[b2] & kFInj) || A.Cc == nullptr) continue;
         const int bl = b2 - bo;
         const int x2 = bl % G::XX, y2 = (bl / G::XX) % G::XY, z2 = bl / G::XS;
-        const long long cc =
-            sKey[tn * G::kSlots + (x2 >> 1) + G::SX * ((y2 >> 1) + G::SY * (z2 >> 1))] & 0x0FFFFFFFu;
+        const uint32_t ck = sKey[tn * G::kSlots + (x2 >> 1) + G::SX * ((y2 >> 1) + G::SY * (z2 >> 1))];
+        const long long cc = ((ck >> 28) == kKeyInterp) ? A.vcell[7 * (ck & 0x0FFFFFFFu)] : (ck & 0x0FFFFFFFu);
         const double one = (k & 1) ? 1. : -1.;
         double F[5];
         flux5(k, F);

@@ -310,6 +310,7 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
   lv.tiles.clear();
   lv.keys.clear();
   lv.inj_cells.clear();
+  lv.interp.clear();
   lv.reads_coarse = false;
   lv.shape = 0;
   if (lv.noct == 0) return 0;
@@ -368,12 +369,51 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
   for (uint32_t key : lv.keys)
     if (key != kKeyNone && (key >> 28) == kKeyInj) lv.reads_coarse = true;
   if (lv.reads_coarse && H.trans != 0) {
-    // the reference's transmissive build (-DHYDROTEST) fills coarser neighbours by
-    // limited interpolation (coarse2fine_hydro2, src/hydro_utils.c:311), not by
-    // the injection this path stages
-    err = "transmissive boundaries with a coarser neighbour at level " + std::to_string(L) +
-          ": the reference interpolates coarse neighbours in that build, which is not staged here";
-    return EMMA_ST_TREE;
+    // The reference's transmissive build (-DHYDROTEST) fills a coarser neighbour
+    // by limited-slope interpolation (coarse2fine_hydro2, src/hydro_utils.c:311)
+    // instead of injection: every injected slot becomes an interpolated one, with
+    // the coarse cell and the 6 cells its slopes are taken from.
+    const HostLevel &lc = H.lev[L - 1];
+    std::unordered_map<uint32_t, int> jof;
+    for (uint32_t &key : lv.keys) {
+      if (key == kKeyNone || (key >> 28) != kKeyInj) continue;
+      const uint32_t cell = key & 0x0FFFFFFFu;
+      auto it = jof.find(cell);
+      if (it == jof.end()) {
+        const int j = (int)jof.size();
+        it = jof.emplace(cell, j).first;
+        const int io = (int)(cell >> 3), c = (int)(cell & 7);
+        struct OCT *oc = lc.octs[io];
+        const double dxcur = std::pow(0.5, oc->level);
+        int nb[6];
+        int wm = -1, wp = -1;  // like the reference, a missing neighbour keeps the previous one
+        for (int dir = 0; dir < 3; dir++) {
+          for (int side = 0; side < 2; side++) {
+            const int k = 2 * dir + side;
+            int &w = side ? wp : wm;
+            const int c2 = c ^ (1 << dir);
+            if (inside(c, k)) {
+              w = 8 * io + c2;
+            } else if (oc->nei[k] != nullptr && oc->nei[k]->child != nullptr) {
+              const int jo = P.idx[L - 1].get(oc->nei[k]->child);
+              if (jo >= 0) w = 8 * jo + c2;
+            }
+            const bool bnd = side ? ((k == 1 && oc->x + 2. * dxcur == 1.) || (k == 3 && oc->y + 2. * dxcur == 1.) ||
+                                     (k == 5 && oc->z + 2. * dxcur == 1.))
+                                  : ((k == 0 && oc->x == 0.) || (k == 2 && oc->y == 0.) || (k == 4 && oc->z == 0.));
+            if (((H.trans >> k) & 1) && bnd) w = (int)cell;
+            if (w < 0) {
+              err = "coarse cell without a slope neighbour at level " + std::to_string(L - 1);
+              return EMMA_ST_TREE;
+            }
+            nb[k] = w;
+          }
+        }
+        lv.interp.push_back((int32_t)cell);
+        for (int k = 0; k < 6; k++) lv.interp.push_back(nb[k]);
+      }
+      key = key_make(kKeyInterp, (uint32_t)it->second);
+    }
   }
   return 0;
 }
@@ -502,7 +542,8 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
         const uint32_t kind = key >> 28, idx = key & 0x0FFFFFFFu;
         const bool ok = (kind == kKeyReal || (kind >= kKeyGhost0 && kind < kKeyGhost0 + 6)) ? (idx < (uint32_t)lv.noct)
                         : (kind == kKeyInj) ? ((long long)idx < ncoarse8)
-                                            : false;
+                        : (kind == kKeyInterp) ? ((size_t)idx < lv.interp.size() / 7)
+                                               : false;
         if (!ok) {
           err = "invalid staged key at level " + std::to_string(L);
           return EMMA_ST_TREE;
@@ -535,6 +576,15 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
     for (int32_t c : lv.inj_cells)
       if (c < 0 || c >= ncoarse8) {
         err = "invalid injected cell at level " + std::to_string(L);
+        return EMMA_ST_TREE;
+      }
+    if (lv.interp.size() % 7 != 0) {
+      err = "invalid interpolation list at level " + std::to_string(L);
+      return EMMA_ST_TREE;
+    }
+    for (int32_t c : lv.interp)
+      if (c < 0 || c >= ncoarse8) {
+        err = "invalid interpolated cell at level " + std::to_string(L);
         return EMMA_ST_TREE;
       }
   }

@@ -19,6 +19,8 @@ struct HostLevel {
   std::vector<uint32_t> keys;         // kSlots slot keys per tile
   std::vector<int32_t> inj_cells;     // level L-1 cells that receive fine->coarse corrections
   bool reads_coarse = false;          // some tile stages an injected level L-1 cell
+  std::vector<int32_t> interp;        // transmissive builds: per interpolated level L-1 cell,
+                                      // the cell and its 6 slope neighbours (7 entries)
   int shape = 0;                      // brick shape of the plan (kShapes)
   std::vector<int32_t> pos;           // per oct: integer position on the level grid (x,y,z)
 };

@@ -12,7 +12,11 @@ namespace emma {
 //   kKeyGhost0 + k  : transmissive ghost across face k of an oct of this level,
 //                     filled through the reference's mirror map of face k
 //                     (src/hydro_utils.c:2504-2610)
-constexpr uint32_t kKeyReal = 0, kKeyInj = 1, kKeyGhost0 = 2;
+//   kKeyInterp      : a coarser leaf cell interpolated into 8 cells, as the
+//                     reference's transmissive build (-DHYDROTEST) gathers it
+//                     (coarse2fine_hydro2, src/hydro_utils.c:311); index into
+//                     the level's interpolation list
+constexpr uint32_t kKeyReal = 0, kKeyInj = 1, kKeyGhost0 = 2, kKeyInterp = 8;
 constexpr uint32_t kKeyNone = 0xFFFFFFFFu;
 constexpr uint32_t key_make(uint32_t kind, uint32_t idx) { return (kind << 28) | idx; }
 
@@ -61,6 +65,10 @@ struct LevelArgs {
   long long nc8;      // plane stride of Wc/Cc
   const double *Wf;   // level L+1 state for split-cell averaging, may be null
   long long nf8;      // plane stride of Wf
+  double *Wv;         // interpolated coarser cells: planes d,u,v,w,p of 8 * nv
+  const int *vcell;   // per interpolated cell: the level L-1 cell, then its 6 neighbours
+                      // (-x,+x,-y,+y,-z,+z) the slopes are taken from
+  long long nv;       // interpolated coarser cells
   const uint8_t *split;  // per oct bitmask of split cells
   const int *child;      // per cell: child oct index at L+1, -1 for a leaf
   const TileDesc *tiles;

@@ -45,18 +45,26 @@ def test_fully_refined_tree_plans():
     assert list(st[0:2]) == [64, 2] and list(st[5:7]) == [512, 16]
 
 
-def test_transmissive_boundary_with_refinement_is_refused():
+def test_transmissive_boundary_with_refinement_plans():
     """With transmissive boundaries (the reference's HYDROTEST build) coarser
-    neighbours are interpolated, which the device path does not stage: the
-    planner reports a tree error instead of producing a plan."""
+    neighbours are interpolated (coarse2fine_hydro2); the planner lists the coarse
+    cells and their slope neighbours, including a refined region that touches the
+    transmissive boundary."""
     from emma_b200 import OctTree
-    import numpy as np
     t = OctTree(3, 4)
     t.refine_where(3, lambda c: c[:, 0] < 0.3)  # refined region touching x = 0
     st = (ctypes.c_longlong * 10)()
-    rc = lib().emma_hydro_plan_stats(t.firstoct, 3, 4, 0x3, st)
-    assert rc & 0x08  # EMMA_ST_TREE
-    assert b"coarser neighbour" in lib().emma_hydro_last_error()
-    lib().emma_hydro_clear_status()
-    # the same tree with periodic boundaries plans
+    assert lib().emma_hydro_plan_stats(t.firstoct, 3, 4, 0x3, st) == 0, lib().emma_hydro_last_error()
     assert lib().emma_hydro_plan_stats(t.firstoct, 3, 4, 0, st) == 0
+
+
+def test_transmissive_corners_are_refused():
+    """Transmissive boundaries on two axes meet at box edges, where a stencil needs
+    a ghost of a ghost; the planner reports a tree error instead of staging one."""
+    from emma_b200 import configs
+    t = configs.random_uniform(level=4).build()
+    st = (ctypes.c_longlong * 5)()
+    assert lib().emma_hydro_plan_stats(t.firstoct, 4, 4, 0x3F, st) & 0x08
+    assert lib().emma_hydro_plan_stats(t.firstoct, 4, 4, 0x0F, st) & 0x08
+    lib().emma_hydro_clear_status()
+    assert lib().emma_hydro_plan_stats(t.firstoct, 4, 4, 0x03, st) == 0
