@@ -6,8 +6,11 @@ A step is one coarse step of the hydro-only level schedule over the whole tree
 (all levels, subcycled), i.e. one pass of the hot path over one batch of
 synthetic input.  `value` = cell-updates/s of the mixed-precision path with the
 state resident in HBM (one cell-update = one leaf cell advanced by one level
-substep).  `e2e` = the same metric through the C ABI with host buffers: every
-step uploads the level states from pinned host memory and downloads them.
+substep).  `e2e` = the same metric through the reference-facing entries on the
+host OCT tree: every step calls clean_new_hydro + HydroSolver on each level, which
+pack the level's cells, copy them to the device and back and unpack them.
+`e2e_resident` = the resident C ABI with host buffers: every step uploads the
+level states from pinned host memory and downloads them.
 The FP64 plain path is timed on the same workload and reported beside it.
 
 Multi-GPU: the path is run as independent replicas (one per rank), value =
@@ -250,7 +253,13 @@ def run_mine(args, rank, world):
         for _ in range(min(args.steps, 10)):
             r.coarse_step(nsub=cfg.nsub)
         res["final"] = {l: r.state(l) for l in levels}
+        res["dt"] = {l: float(r.adt[l - 1]) for l in levels}
         results[prec_name] = res
+    # e2e through the reference-facing entries on the host tree: every step calls
+    # clean_new_hydro + HydroSolver once per level (finest first) at the level's
+    # CFL step; each call packs the level from the OCT structs, copies it to the
+    # device, runs the level kernel, copies it back and unpacks it
+    results["dropin"] = run_dropin(args, L, cfg, tree, levels, results["mixed"]["dt"], world)
     # L1 of the mixed path against the FP64 path (the FP64 path equals the oracle to 1e-12)
     fm, ff = results["mixed"]["final"], results["fp64"]["final"]
     num = {k: 0.0 for k in ("rho", "p", "v")}
@@ -265,6 +274,38 @@ def run_mine(args, rank, world):
             den[k] += np.abs(y).sum() * dv
     l1 = {k: float(num[k] / den[k]) for k in num}
     return cfg, tree, results, l1, build_s, flush
+
+
+def run_dropin(args, L, cfg, tree, levels, dts, world):
+    """Times the drop-in HydroSolver (mixed precision) on the host tree, wall
+    clock around synchronous calls; returns ms, cell-updates and bytes copied."""
+    import torch
+    from emma_b200 import PREC_MIXED
+    from emma_b200.hydro import options, clean_new_hydro, HydroSolver
+    o = options(PREC_MIXED, cfg.trans, cfg.cfl)
+    L.emma_hydro_set_options(ctypes.byref(o))
+    order = sorted(levels, reverse=True)
+    leaf = sum(int((~tree.split_mask(l)).sum()) for l in order)
+    for _ in range(max(args.warmup, 1)):  # the first call of a level builds its mirror
+        for l in order:
+            clean_new_hydro(l, tree.firstoct)
+            HydroSolver(l, tree.firstoct, dts[l])
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    L.emma_hydro_reset_counters()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        for l in order:
+            clean_new_hydro(l, tree.firstoct)
+            HydroSolver(l, tree.firstoct, dts[l])
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    h2d, d2h = ctypes.c_longlong(), ctypes.c_longlong()
+    L.emma_hydro_transfer_bytes(ctypes.byref(h2d), ctypes.byref(d2h))
+    return {"ms": ms, "updates": L.emma_hydro_cell_updates(), "leaf_per_step": leaf,
+            "h2d": h2d.value // max(args.steps, 1), "d2h": d2h.value // max(args.steps, 1),
+            "status": L.emma_hydro_status()}
 
 
 def cpu_baseline_sample(config):
@@ -367,15 +408,17 @@ def main():
     cfg, tree, res, l1, build_s, flushed = run_mine(args, rank, world)
     mixed, fp64 = res["mixed"], res["fp64"]
     # max over ranks of the timed device time
-    ms_m, ms_f, ms_e = mixed["ms"], fp64["ms"], mixed["e2e_ms"]
+    dropin = res["dropin"]
+    ms_m, ms_f, ms_e, ms_d = mixed["ms"], fp64["ms"], mixed["e2e_ms"], dropin["ms"]
     if world > 1:
-        t = torch.tensor([ms_m, ms_f, ms_e], device="cuda")
+        t = torch.tensor([ms_m, ms_f, ms_e, ms_d], device="cuda")
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_m, ms_f, ms_e = (float(x) for x in t.cpu())
+        ms_m, ms_f, ms_e, ms_d = (float(x) for x in t.cpu())
     upd_m = mixed["updates"] * world
     value = upd_m / (ms_m * 1e-3)
     value_fp64 = fp64["updates"] * world / (ms_f * 1e-3)
-    e2e = mixed["updates"] * world / (ms_e * 1e-3)
+    e2e_resident = mixed["updates"] * world / (ms_e * 1e-3)
+    e2e = dropin["updates"] * world / (ms_d * 1e-3)
     peak, peak_kind = peaks()
     cells_per_launch = mixed["kernel_cells"] / max(mixed["kernel_launches"], 1)
     achieved = ALG_BYTES_PER_CELL * cells_per_launch / (mixed["kernel_avg_ms"] * 1e-3) / 1e9
@@ -403,8 +446,13 @@ def main():
                      "peak_source": peak_kind, "traffic": (tpc * cells_per_launch) if tpc else None,
                      "kernel": "level_batch_kernel<MathF32>", "alg_bytes_per_cell": ALG_BYTES_PER_CELL,
                      "cells_per_launch": cells_per_launch, "avg_launch_ms": mixed["kernel_avg_ms"]},
-        "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": mixed["h2d"],
-                "d2h_bytes_per_step": mixed["d2h"]},
+        "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": dropin["h2d"],
+                "d2h_bytes_per_step": dropin["d2h"], "ms_per_step": ms_d / args.steps,
+                "api": "clean_new_hydro + HydroSolver per level on the host OCT tree (mixed), wall clock",
+                "leaf_cells_per_step": dropin["leaf_per_step"], "status": dropin["status"]},
+        "e2e_resident": {"value": e2e_resident, "unit": "cell-updates/s", "h2d_bytes_per_step": mixed["h2d"],
+                         "d2h_bytes_per_step": mixed["d2h"],
+                         "api": "emma_hydro_set_level_state + coarse step + emma_hydro_get_level_state, pinned host"},
         "autotune": {"mixed": mixed["autotune"], "fp64": fp64["autotune"],
                      "candidates": "brick 4x4x2 octs x1 or 2x2x2 octs x4 per 256-thread tile; 1..occupancy CTAs per SM"},
         "gpu_launches": mixed["launches"],

@@ -44,6 +44,8 @@ SIGNATURES = [
     ("emma_hydro_shutdown", None, []),
     ("emma_hydro_set_stream", c_int, [c_void_p]),
     ("emma_hydro_kernel_launches", c_ll, []),
+    ("emma_hydro_transfer_bytes", c_int, [P(c_ll), P(c_ll)]),
+    ("emma_hydro_dropin_profile", c_int, [P(ctypes.c_double)]),
     ("emma_hydro_tree_upload", c_int, [c_void_p, c_int, c_int, c_int]),
     ("emma_hydro_tree_download", c_int, [c_void_p]),
     ("emma_hydro_fields_upload", c_int, [c_void_p]),

@@ -3,6 +3,8 @@
 // the reference's names.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -36,6 +38,7 @@ struct DevLevel {
   int L = 0, noct = 0, ntiles = 0;
   long long n8 = 0, leaf = 0;
   double *W0 = nullptr, *W1 = nullptr, *C = nullptr, *B = nullptr;
+  double *WB = nullptr;  // drop-in levels: one allocation of W0 (5 planes) followed by B (6 planes)
   uint8_t *split = nullptr;
   int *child = nullptr;
   TileDesc *tiles = nullptr;
@@ -82,23 +85,32 @@ struct Ctx {
   int nwork_all = 0;
   cudaGraphExec_t graph = nullptr;
   int graph_nsub = -1, graph_prec = -1;
-  // drop-in cache
-  struct OCT **drop_first = nullptr;
-  int drop_level = -1;
-  std::vector<long long> drop_sig;
-  Tree drop;
+  // drop-in cache: one mirror of levels L-1..L+1 per advanced level L, so that a
+  // driver cycling through its levels does not rebuild one on every call
+  struct DropCache {
+    struct OCT **first = nullptr;
+    std::vector<unsigned long long> sig;
+    Tree t;
+  };
+  DropCache drop[kMaxLevels];
+  std::vector<struct OCT *> lists[kMaxLevels];  // last walk of each level's oct list
+  std::vector<struct OCT *> list_tmp;
   // pinned staging
   double *pin = nullptr;
   size_t pin_bytes = 0;
   // counters and timing
   long long updates = 0;
   long long kernel_launches = 0;
+  long long h2d_bytes = 0, d2h_bytes = 0;  // host<->device state copies
+  double dropin_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // phases of the last drop-in call
+  std::vector<cudaEvent_t> range_ev;        // per host thread and sub-range of a drop-in download
   bool timing = true;
   std::vector<TimedLaunch> launches;
   std::vector<cudaEvent_t> free_events;
 };
 
 Ctx g;
+using Clock = std::chrono::steady_clock;
 
 void fail(unsigned bit, const std::string &msg) {
   g.status |= bit;
@@ -142,21 +154,35 @@ bool ensure_pin(size_t bytes) {
   return true;
 }
 
+// Host threads of a parallel pass over n items: up to 16, one for small passes.
+unsigned range_threads(long long n) {
+  const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+  return n < 4096 ? 1u : nt;
+}
+
+// Runs f(t, a, b) over [0, n) split into contiguous ranges, one per host
+// thread t; every range start is a multiple of `align`.
 template <class F>
-void parallel_for(long long n, F f) {
-  unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  if (n < 4096 || nt == 1) {
-    f(0LL, n);
+void parallel_ranges(long long n, F f, long long align = 1) {
+  const unsigned nt = range_threads(n);
+  if (nt == 1) {
+    f(0, 0LL, n);
     return;
   }
   std::vector<std::thread> th;
   long long chunk = (n + nt - 1) / nt;
+  chunk = (chunk + align - 1) / align * align;
   for (unsigned t = 0; t < nt; t++) {
     long long a = t * chunk, b = std::min(n, a + chunk);
     if (a >= b) break;
-    th.emplace_back([=] { f(a, b); });
+    th.emplace_back([=] { f((int)t, a, b); });
   }
   for (auto &t : th) t.join();
+}
+
+template <class F>
+void parallel_for(long long n, F f, long long align = 1) {
+  parallel_ranges(n, [&](int, long long a, long long b) { f(a, b); }, align);
 }
 
 void drop_graph() {
@@ -166,10 +192,14 @@ void drop_graph() {
 }
 
 void free_level(DevLevel &d) {
-  cudaFree(d.W0);
+  if (d.WB != nullptr) {
+    cudaFree(d.WB);
+  } else {
+    cudaFree(d.W0);
+    cudaFree(d.B);
+  }
   cudaFree(d.W1);
   cudaFree(d.C);
-  cudaFree(d.B);
   cudaFree(d.split);
   cudaFree(d.child);
   cudaFree(d.tiles);
@@ -186,6 +216,14 @@ void free_tree(Tree &t) {
   cudaFree(t.d_lv);
   t.d_lv = nullptr;
   t.valid = false;
+}
+
+void drop_all() {
+  for (auto &c : g.drop) {
+    free_tree(c.t);
+    c.first = nullptr;
+    c.sig.clear();
+  }
 }
 
 template <class T>
@@ -214,7 +252,15 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     d.ntiles = (int)h.tiles.size();
     d.shape = h.shape;
     const size_t bytes = sizeof(double) * 5 * (size_t)std::max<long long>(d.n8, 1);
-    if (!ck(cudaMalloc(&d.W0, bytes), "cudaMalloc W")) return false;
+    if (with_base && !h.tiles.empty()) {
+      // W0 and the base B in one block: the drop-in upload copies all 11 planes of
+      // an oct range with one pitched copy
+      if (!ck(cudaMalloc(&d.WB, sizeof(double) * 11 * (size_t)d.n8), "cudaMalloc W+B")) return false;
+      d.W0 = d.WB;
+      d.B = d.WB + 5 * d.n8;
+    } else if (!ck(cudaMalloc(&d.W0, bytes), "cudaMalloc W")) {
+      return false;
+    }
     if (!ck(cudaMalloc(&d.W1, bytes), "cudaMalloc Wn")) return false;
     // corrections arrive only from the finer level: a level without split cells has none
     bool has_split = false;
@@ -223,9 +269,6 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
       if (!ck(cudaMalloc(&d.C, bytes), "cudaMalloc C")) return false;
       if (!ck(cudaMemset(d.C, 0, bytes), "cudaMemset C")) return false;
     }
-    if (with_base && !h.tiles.empty())
-      if (!ck(cudaMalloc(&d.B, sizeof(double) * 6 * (size_t)std::max<long long>(d.n8, 1)), "cudaMalloc B"))
-        return false;
     if (!upload_vec(&d.split, h.split)) return false;
     if (!upload_vec(&d.child, h.child)) return false;
     if (!upload_vec(&d.tiles, h.tiles)) return false;
@@ -290,6 +333,68 @@ void pack_level(const HostLevel &h, int which, double *out) {
 inline void finish_prims(struct Wtype &W) {
   W.a = std::sqrt(kG * W.p / W.d);
   W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
+}
+
+// Packs octs [a, b) of a level in one pass over their cells: `field` into the 5
+// planes of pw, `fieldnew` (with E) into the 6 planes of pb (planes of 8*noct).
+void pack_cells(const HostLevel &h, long long a, long long b, double *pw, double *pb) {
+  const long long n8 = 8LL * h.noct;
+  for (long long i = a; i < b; i++) {
+    const struct OCT *o = h.octs[i];
+    for (int c = 0; c < 8; c++) {
+      const struct Wtype &W = o->cell[c].field, &N = o->cell[c].fieldnew;
+      const long long k = 8 * i + c;
+      pw[k] = W.d;
+      pw[n8 + k] = W.u;
+      pw[2 * n8 + k] = W.v;
+      pw[3 * n8 + k] = W.w;
+      pw[4 * n8 + k] = W.p;
+      pb[k] = N.d;
+      pb[n8 + k] = N.u;
+      pb[2 * n8 + k] = N.v;
+      pb[3 * n8 + k] = N.w;
+      pb[4 * n8 + k] = N.p;
+      pb[5 * n8 + k] = N.E;
+    }
+  }
+}
+
+// Writes the 5 planes of p (planes of 8*noct) into `fieldnew` of the leaf cells
+// of octs [a, b), with a and E; `also_field` copies the result into `field`.
+void unpack_cells(const HostLevel &h, long long a, long long b, const double *p, bool also_field) {
+  const long long n8 = 8LL * h.noct;
+  for (long long i = a; i < b; i++) {
+    struct OCT *o = h.octs[i];
+    for (int c = 0; c < 8; c++) {
+      if (o->cell[c].child != nullptr) continue;
+      const long long k = 8 * i + c;
+      struct Wtype &W = o->cell[c].fieldnew;
+      W.d = p[k];
+      W.u = p[n8 + k];
+      W.v = p[2 * n8 + k];
+      W.w = p[3 * n8 + k];
+      W.p = p[4 * n8 + k];
+      finish_prims(W);
+      if (also_field) o->cell[c].field = W;
+    }
+  }
+}
+
+// Sub-ranges of one host thread's oct range in a drop-in transfer: each is
+// packed (unpacked) while the copy engine moves another.
+constexpr int kSubRanges = 8;
+long long dropin_subrange(long long noct) {
+  const long long per_thread = (noct + range_threads(noct) - 1) / range_threads(noct);
+  return std::max<long long>(1024, (per_thread + kSubRanges - 1) / kSubRanges);
+}
+
+bool ensure_range_events() {
+  while (g.range_ev.size() < 16 * (size_t)kSubRanges) {
+    cudaEvent_t e;
+    if (!ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return false;
+    g.range_ev.push_back(e);
+  }
+  return true;
 }
 
 // The level's state changed outside the device schedule: its next CFL step
@@ -576,9 +681,7 @@ int emma_hydro_set_options(const struct EmmaHydroOptions *opt) {
     cudaStreamSynchronize(g.stream);
     drop_graph();
     free_tree(g.res);
-    free_tree(g.drop);
-    g.drop_level = -1;
-    g.drop_first = nullptr;
+    drop_all();
   }
   return 0;
 }
@@ -588,13 +691,15 @@ void emma_hydro_shutdown(void) {
   cudaStreamSynchronize(g.stream);
   drop_graph();
   free_tree(g.res);
-  free_tree(g.drop);
+  drop_all();
   cudaFree(g.d_work_all);
   for (auto &t : g.launches) {
     cudaEventDestroy(t.a);
     cudaEventDestroy(t.b);
   }
   for (auto e : g.free_events) cudaEventDestroy(e);
+  for (auto e : g.range_ev) cudaEventDestroy(e);
+  g.range_ev.clear();
   cudaFree(g.d_status);
   cudaFree(g.d_done);
   cudaFree(g.d_S);
@@ -841,6 +946,7 @@ int emma_hydro_fields_upload(struct OCT **firstoct) {
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
     pack_level(h, 0, g.pin);
     CK(cudaMemcpyAsync(W, g.pin, bytes, cudaMemcpyHostToDevice, g.stream));
+    g.h2d_bytes += (long long)bytes;
     CK(mark_stale(L));
     CK(cudaStreamSynchronize(g.stream));
   }
@@ -862,6 +968,7 @@ int emma_hydro_tree_download(struct OCT **firstoct) {
     const size_t bytes = sizeof(double) * 5 * (size_t)n8;
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
     CK(cudaMemcpyAsync(g.pin, W, bytes, cudaMemcpyDeviceToHost, g.stream));
+    g.d2h_bytes += (long long)bytes;
     CK(cudaStreamSynchronize(g.stream));
     const double *p = g.pin;
     parallel_for(h.noct, [&](long long a, long long b) {
@@ -901,6 +1008,7 @@ int emma_hydro_get_level_state(int level, double *host_out) {
   double *W = current_state(level);
   if (W == nullptr) return EMMA_ST_CUDA;
   CK(cudaMemcpyAsync(host_out, W, sizeof(double) * 5 * d.n8, cudaMemcpyDeviceToHost, g.stream));
+  g.d2h_bytes += (long long)sizeof(double) * 5 * d.n8;
   CK(cudaStreamSynchronize(g.stream));
   return 0;
 }
@@ -911,6 +1019,7 @@ int emma_hydro_set_level_state(int level, const double *host_in) {
   double *W = current_state(level);
   if (W == nullptr) return EMMA_ST_CUDA;
   CK(cudaMemcpyAsync(W, host_in, sizeof(double) * 5 * d.n8, cudaMemcpyHostToDevice, g.stream));
+  g.h2d_bytes += (long long)sizeof(double) * 5 * d.n8;
   CK(mark_stale(level));
   CK(cudaStreamSynchronize(g.stream));
   return 0;
@@ -1021,9 +1130,23 @@ long long emma_hydro_cell_updates(void) {
 
 long long emma_hydro_kernel_launches(void) { return g.kernel_launches; }
 
+int emma_hydro_dropin_profile(double *ms8) {
+  if (ms8 == nullptr) return EMMA_ST_ARG;
+  for (int i = 0; i < 8; i++) ms8[i] = g.dropin_ms[i];
+  return 0;
+}
+
+int emma_hydro_transfer_bytes(long long *h2d, long long *d2h) {
+  if (h2d == nullptr || d2h == nullptr) return EMMA_ST_ARG;
+  *h2d = g.h2d_bytes;
+  *d2h = g.d2h_bytes;
+  return 0;
+}
+
 void emma_hydro_reset_counters(void) {
   g.updates = 0;
   g.kernel_launches = 0;
+  g.h2d_bytes = g.d2h_bytes = 0;
   if (g.ready) {
     cudaStreamSynchronize(g.stream);
     if (g.d_S) cudaMemsetAsync(&g.d_S->updates, 0, sizeof(long long), g.stream);
@@ -1139,77 +1262,152 @@ int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int tran
 
 static int dropin_rank(struct CPUINFO *cpu) { return cpu ? *reinterpret_cast<const int *>(cpu) : 0; }
 
-static std::vector<long long> tree_signature(struct OCT **firstoct, int lo, int hi) {
-  std::vector<long long> sig;
-  sig.push_back((long long)(uintptr_t)firstoct);
-  for (int L = lo; L <= hi; L++) {
-    long long n = 0, h = 1469598103934665603LL;
-    for (struct OCT *o = firstoct[L - 1]; o != nullptr; o = o->next) {
-      n++;
-      h = (h ^ (long long)(uintptr_t)o) * 1099511628211LL;
-      for (int c = 0; c < 8; c++) h = (h ^ (o->cell[c].child != nullptr)) * 1099511628211LL;
-    }
-    sig.push_back(n);
-    sig.push_back(h);
+// Oct pointers of level `level` in list order (firstoct[level-1] on).  The
+// serial walk follows `next` only (one cache line per oct) and prefetches
+// those lines along the previous walk of the same level, so an unchanged list
+// is read at memory bandwidth instead of one memory latency per oct; a
+// prefetch never faults, so a list that changed is still walked correctly.
+// Everything else reads the octs in parallel.  The result stays valid until the
+// next walk of the level.
+static const std::vector<struct OCT *> &walk_level(struct OCT **firstoct, int level) {
+  std::vector<struct OCT *> &prev = g.lists[level];
+  std::vector<struct OCT *> &out = g.list_tmp;
+  out.clear();
+  constexpr size_t kAhead = 24;
+  const size_t np = prev.size();
+  size_t i = 0;
+  for (struct OCT *o = firstoct[level - 1]; o != nullptr; o = o->next, i++) {
+    if (i + kAhead < np) __builtin_prefetch(&prev[i + kAhead]->next);
+    out.push_back(o);
   }
-  return sig;
+  prev.swap(out);
+  return prev;
 }
 
-int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struct HGRID *stencil, int stride,
-                    REAL dxcur, REAL dtnew) {
-  (void)stencil;
-  (void)stride;
-  (void)dxcur;
+static inline unsigned long long mix64(unsigned long long z) {  // SplitMix64 finaliser
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+  return z ^ (z >> 31);
+}
+
+// Order-sensitive hash of a level's oct addresses and child-presence bits (the
+// parts of the tree a drop-in mirror depends on); `*split` = a cell has a child.
+static unsigned long long level_hash(const std::vector<struct OCT *> &v, bool *split) {
+  const long long n = (long long)v.size();
+  const long long chunk = 8192;
+  const long long nchunk = (n + chunk - 1) / chunk;
+  std::vector<unsigned long long> part((size_t)nchunk, 0);
+  std::vector<char> any((size_t)nchunk, 0);
+  // chunk-wise partial sums: the total does not depend on the thread count
+  parallel_for(n, [&](long long a, long long b) {
+    for (long long j = (a + chunk - 1) / chunk; j * chunk < b; j++) {
+      unsigned long long s = 0;
+      bool f = false;
+      const long long e = std::min(n, (j + 1) * chunk);
+      for (long long i = j * chunk; i < e; i++) {
+        const struct OCT *o = v[i];
+        unsigned long long bits = 0;
+        for (int c = 0; c < 8; c++) bits |= (unsigned long long)(o->cell[c].child != nullptr) << c;
+        f = f || bits != 0;
+        s += mix64((unsigned long long)(uintptr_t)o ^ (bits << 56) ^ ((unsigned long long)i * 0x9e3779b97f4a7c15ULL));
+      }
+      part[j] = s;
+      any[j] = f;
+    }
+  }, chunk);
+  unsigned long long h = (unsigned long long)n;
+  bool f = false;
+  for (long long j = 0; j < nchunk; j++) {
+    h += part[j];
+    f = f || any[j];
+  }
+  *split = f;
+  return h;
+}
+
+// One drop-in advance of `level` on the host tree.  With `final_update` it also
+// performs HydroSolver's closing loop on the level (field := fieldnew on
+// leaves, primitive mean of the children on split cells), the leaf copy fused
+// into the download.  Returns the number of octs advanced (0 on error).
+static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu, double dtnew, bool final_update) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return 0;
   if (firstoct == nullptr || level < 2 || level >= kMaxLevels - 1 || firstoct[level - 1] == nullptr) return 0;
   const int rank = dropin_rank(cpu);
+  const auto t0 = Clock::now();
   // levels present around `level`: L-1 always exists; L+1 only if a cell is split
-  bool has_fine = false;
-  for (struct OCT *o = firstoct[level - 1]; o != nullptr && !has_fine; o = o->next)
-    for (int c = 0; c < 8; c++)
-      if (o->cell[c].child != nullptr) has_fine = true;
-  const int lo = level - 1, hi = has_fine ? level + 1 : level;
-  std::vector<long long> sig = tree_signature(firstoct, lo, hi);
-  if (g.drop_first != firstoct || g.drop_level != level || sig != g.drop_sig || !g.drop.valid) {
+  bool split_l = false, unused = false;
+  const std::vector<struct OCT *> &wl = walk_level(firstoct, level);
+  const std::vector<struct OCT *> &wc = walk_level(firstoct, level - 1);
+  std::vector<unsigned long long> sig;
+  sig.push_back((unsigned long long)(uintptr_t)firstoct);
+  sig.push_back(level_hash(wc, &unused));
+  sig.push_back(level_hash(wl, &split_l));
+  if (split_l) sig.push_back(level_hash(walk_level(firstoct, level + 1), &unused));
+  const int lo = level - 1, hi = split_l ? level + 1 : level;
+  const auto tw = Clock::now();
+  Ctx::DropCache &cache = g.drop[level];
+  if (cache.first != firstoct || sig != cache.sig || !cache.t.valid) {
     cudaStreamSynchronize(g.stream);
-    free_tree(g.drop);
-    g.drop_level = -1;
+    free_tree(cache.t);
+    cache.first = nullptr;
+    cache.sig.clear();
     std::string err;
     std::vector<int> shapes((size_t)hi + 1, std::max(-1, requested_shape(g.opt.tile_octs)));
-    int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, g.drop.host, err,
+    int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, cache.t.host, err,
                              shapes.data());
     if (rc != 0) {
       fail((unsigned)rc, err);
       return 0;
     }
-    if (!alloc_tree(g.drop.host, g.drop, true)) return 0;
-    g.drop_first = firstoct;
-    g.drop_level = level;
-    g.drop_sig = sig;
+    if (!alloc_tree(cache.t.host, cache.t, true)) return 0;
+    cache.first = firstoct;
+    cache.sig = sig;
   }
-  HostTree &H = g.drop.host;
+  Tree &T = cache.t;
+  HostTree &H = T.host;
   const HostLevel &h = H.lev[level];
   const HostLevel &hc = H.lev[level - 1];
-  DevLevel &d = g.drop.lev[level];
-  DevLevel &dc = g.drop.lev[level - 1];
+  DevLevel &d = T.lev[level];
+  DevLevel &dc = T.lev[level - 1];
   if (h.noct == 0) return 0;
   const long long n8 = d.n8, nc8 = dc.n8;
-  const size_t need = sizeof(double) * std::max<long long>(11 * n8, 5 * nc8);
-  if (!ensure_pin(need)) return 0;
-  // upload: level field (5 planes) + fieldnew (6 planes), coarser field
-  pack_level(h, 0, g.pin);
-  pack_level(h, 1, g.pin + 5 * n8);
-  if (!ck(cudaMemcpyAsync(d.W0, g.pin, sizeof(double) * 5 * n8, cudaMemcpyHostToDevice, g.stream), "H2D W")) return 0;
-  if (!ck(cudaMemcpyAsync(d.B, g.pin + 5 * n8, sizeof(double) * 6 * n8, cudaMemcpyHostToDevice, g.stream), "H2D B"))
-    return 0;
   const bool coarse = nc8 > 0 && h.reads_coarse && dc.C != nullptr;
+  // pinned staging: level field (5 planes) | level fieldnew (6 planes) | coarser
+  // level (5 planes) | device status word
+  if (!ensure_pin(sizeof(double) * (11 * n8 + 5 * nc8 + 1)) || !ensure_range_events()) return 0;
+  double *pw = g.pin, *pb = g.pin + 5 * n8, *pc = g.pin + 11 * n8;
+  unsigned *pst = reinterpret_cast<unsigned *>(pc + 5 * nc8);
+  const auto t1 = Clock::now();
+  // upload: each host thread packs its oct range in sub-ranges (field and
+  // fieldnew in one pass over the cells) and queues one pitched copy of the 11
+  // planes of each sub-range as soon as it is packed, so the copy engine runs
+  // while the rest is still being packed
+  if (d.WB == nullptr) {
+    fail(EMMA_ST_TREE, "drop-in level without staging block");
+    return 0;
+  }
+  const size_t pitch = sizeof(double) * (size_t)n8;
+  const long long sub = dropin_subrange(h.noct);
+  std::atomic<bool> copies_ok{true};
+  parallel_ranges(h.noct, [&](int, long long a0, long long b0) {
+    for (long long s0 = a0; s0 < b0; s0 += sub) {
+      const long long s1 = std::min(b0, s0 + sub);
+      pack_cells(h, s0, s1, pw, pb);
+      if (cudaMemcpy2DAsync(d.WB + 8 * s0, pitch, pw + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 11,
+                            cudaMemcpyHostToDevice, g.stream) != cudaSuccess)
+        copies_ok = false;
+    }
+  });
+  if (!copies_ok) return ck(cudaGetLastError(), "H2D level state"), 0;
+  g.h2d_bytes += (long long)sizeof(double) * 11 * n8;
   if (coarse) {
-    if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
-    pack_level(hc, 0, g.pin);
-    if (!ck(cudaMemcpyAsync(dc.W0, g.pin, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))
+    pack_level(hc, 0, pc);
+    if (!ck(cudaMemcpyAsync(dc.W0, pc, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))
       return 0;
+    g.h2d_bytes += (long long)sizeof(double) * 5 * nc8;
     if (!ck(cudaMemsetAsync(dc.C, 0, sizeof(double) * 5 * nc8, g.stream), "memset Cc")) return 0;
   }
+  const auto t2 = Clock::now();
   LevelArgs a;
   std::memset(&a, 0, sizeof(a));
   a.L = level;
@@ -1235,38 +1433,63 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
   a.ntiles = d.ntiles;
   a.wait_slot = -1;
   a.leaf = d.leaf;
-  k_set_args<<<1, 1, 0, g.stream>>>(g.drop.d_lv, level, a);
+  k_set_args<<<1, 1, 0, g.stream>>>(T.d_lv, level, a);
   if (!ck(cudaGetLastError(), "k_set_args")) return 0;
-  if (!ck(launch_interp(g.drop.d_lv, level, d.nv, nullptr, g.nsm, g.stream), "interpolation launch")) return 0;
-  if (!launch_batch(g.drop.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return 0;
-  // download the level's new state into fieldnew (leaf cells)
-  if (!ck(cudaMemcpyAsync(g.pin, d.W1, sizeof(double) * 5 * n8, cudaMemcpyDeviceToHost, g.stream), "D2H Wn")) return 0;
-  if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
-  {
-    const double *p = g.pin;
-    parallel_for(h.noct, [&](long long a0, long long b0) {
-      for (long long i = a0; i < b0; i++) {
-        struct OCT *o = h.octs[i];
-        for (int c = 0; c < 8; c++) {
-          if (o->cell[c].child != nullptr) continue;
-          const long long k = 8 * i + c;
-          struct Wtype &W = o->cell[c].fieldnew;
-          W.d = p[k];
-          W.u = p[n8 + k];
-          W.v = p[2 * n8 + k];
-          W.w = p[3 * n8 + k];
-          W.p = p[4 * n8 + k];
-          finish_prims(W);
-        }
-      }
-    });
+  if (!ck(launch_interp(T.d_lv, level, d.nv, nullptr, g.nsm, g.stream), "interpolation launch")) return 0;
+  if (!launch_batch(T.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return 0;
+  // device status and the corrections first, then the level's new state range by
+  // range: each host thread waits for its own range and unpacks it into fieldnew
+  // (and field, for HydroSolver) while later ranges are still being copied
+  *pst = 0;
+  if (!ck(cudaMemcpyAsync(pst, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, g.stream), "D2H status"))
+    return 0;
+  if (coarse) {
+    if (!ck(cudaMemcpyAsync(pc, dc.C, sizeof(double) * 5 * nc8, cudaMemcpyDeviceToHost, g.stream), "D2H Cc"))
+      return 0;
+    g.d2h_bytes += (long long)sizeof(double) * 5 * nc8;
   }
+  const auto t3 = Clock::now();
+  std::atomic<bool> wait_ok{true};
+  std::atomic<long long> wait_ns{0};
+  const unsigned bad = EMMA_ST_TREE | EMMA_ST_CUDA;
+  parallel_ranges(h.noct, [&](int t, long long a0, long long b0) {
+    // queue the copies of all sub-ranges of this thread, each followed by an event
+    cudaEvent_t *ev = &g.range_ev[(size_t)t * kSubRanges];
+    int nq = 0;
+    for (long long s0 = a0; s0 < b0 && nq < kSubRanges; s0 += sub, nq++) {
+      const long long s1 = std::min(b0, s0 + sub);
+      if (cudaMemcpy2DAsync(pw + 8 * s0, pitch, d.W1 + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 5,
+                            cudaMemcpyDeviceToHost, g.stream) != cudaSuccess ||
+          cudaEventRecord(ev[nq], g.stream) != cudaSuccess) {
+        wait_ok = false;
+        return;
+      }
+    }
+    // then unpack each as it lands
+    int k = 0;
+    for (long long s0 = a0; s0 < b0 && k < nq; s0 += sub, k++) {
+      const auto w0 = Clock::now();
+      const bool ok = cudaEventSynchronize(ev[k]) == cudaSuccess;
+      wait_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - w0).count();
+      if (!ok) {
+        wait_ok = false;
+        return;
+      }
+      // a kernel that found an invalid state leaves the host tree as it was
+      if ((g.status | *reinterpret_cast<volatile unsigned *>(pst)) & bad) return;
+      unpack_cells(h, s0, std::min(b0, s0 + sub), pw, final_update);
+    }
+  });
+  if (!wait_ok) return ck(cudaStreamSynchronize(g.stream), "D2H level state"), ck(cudaGetLastError(), "D2H"), 0;
+  g.d2h_bytes += (long long)sizeof(double) * 5 * n8;
+  g.status |= *pst;
+  if (g.status & bad) return 0;
+  const auto t4 = Clock::now();
+  g.dropin_ms[3] = std::chrono::duration<double, std::milli>(t4 - t2).count();
+  g.dropin_ms[4] = 1e-6 * (double)wait_ns.load() / (double)std::max<size_t>(1, range_threads(h.noct));
   // fine -> coarse corrections: fieldnew = U2W(W2U(fieldnew) + dU) per coarse cell
   if (coarse) {
-    if (!ck(cudaMemcpyAsync(g.pin, dc.C, sizeof(double) * 5 * nc8, cudaMemcpyDeviceToHost, g.stream), "D2H Cc"))
-      return 0;
-    if (!ck(cudaStreamSynchronize(g.stream), "sync")) return 0;
-    const double *p = g.pin;
+    const double *p = pc;
     for (int32_t k : h.inj_cells) {
       struct Wtype &W = hc.octs[k >> 3]->cell[k & 7].fieldnew;
       double Ud = W.d, Udu = W.d * W.u, Udv = W.d * W.v, Udw = W.d * W.w, UE = W.E;
@@ -1286,46 +1509,73 @@ int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struc
     }
   }
   g.updates += d.leaf;
-  if (emma_hydro_status() & (EMMA_ST_TREE | EMMA_ST_CUDA)) return 0;
+  const auto t5 = Clock::now();
+  // the rest of the final update: octs of other ranks (not mirrored) and split
+  // cells (src/hydro_utils.c:3408-3483)
+  if (final_update && (split_l || (long long)wl.size() != h.noct)) {
+    parallel_for((long long)wl.size(), [&](long long a0, long long b0) {
+      for (long long i = a0; i < b0; i++) {
+        struct OCT *o = wl[i];
+        for (int c = 0; c < 8; c++) {
+          struct CELL *cell = &o->cell[c];
+          if (cell->child == nullptr) {
+            if (o->cpu != rank) cell->field = cell->fieldnew;
+            continue;
+          }
+          struct Wtype W;
+          std::memset(&W, 0, sizeof(W));
+          for (int j = 0; j < 8; j++) {
+            const struct Wtype &Wc = cell->child->cell[j].field;
+            W.d += Wc.d * 0.125;
+            W.u += Wc.u * 0.125;
+            W.v += Wc.v * 0.125;
+            W.w += Wc.w * 0.125;
+            W.p += Wc.p * 0.125;
+          }
+          W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
+          cell->field = W;
+        }
+      }
+    });
+  }
+  const auto t6 = Clock::now();
+  auto ms = [](Clock::time_point x, Clock::time_point y) { return std::chrono::duration<double, std::milli>(y - x).count(); };
+  g.dropin_ms[0] = ms(t0, tw);
+  g.dropin_ms[1] = ms(tw, t1);
+  g.dropin_ms[2] = ms(t1, t2);
+  g.dropin_ms[5] = ms(t4, t5);
+  g.dropin_ms[6] = ms(t5, t6);
+  g.dropin_ms[7] = ms(t0, t6);
   return h.noct;
+}
+
+int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struct HGRID *stencil, int stride,
+                    REAL dxcur, REAL dtnew) {
+  (void)stencil;
+  (void)stride;
+  (void)dxcur;
+  return dropin_advance(firstoct, level, cpu, dtnew, false);
 }
 
 void HydroSolver(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu,
                  struct HGRID *stencil, int stride, REAL dtnew) {
   (void)param;
-  const double dxcur = std::pow(0.5, level);
-  const int nread = advancehydroGPU(firstoct, level, cpu, stencil, stride, dxcur, dtnew);
-  if (nread <= 0) return;
-  // field := fieldnew on leaves; split cells := primitive mean of the children
-  // (src/hydro_utils.c:3408-3483)
-  for (struct OCT *o = firstoct[level - 1]; o != nullptr; o = o->next)
-    for (int c = 0; c < 8; c++) {
-      struct CELL *cell = &o->cell[c];
-      if (cell->child == nullptr) {
-        cell->field = cell->fieldnew;
-      } else {
-        struct Wtype W;
-        std::memset(&W, 0, sizeof(W));
-        for (int i = 0; i < 8; i++) {
-          const struct Wtype &Wc = cell->child->cell[i].field;
-          W.d += Wc.d * 0.125;
-          W.u += Wc.u * 0.125;
-          W.v += Wc.v * 0.125;
-          W.w += Wc.w * 0.125;
-          W.p += Wc.p * 0.125;
-        }
-        W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
-        cell->field = W;
-      }
-    }
+  (void)stencil;
+  (void)stride;
+  dropin_advance(firstoct, level, cpu, dtnew, true);
 }
 
+// fieldnew := field on every cell of the level (src/hydro_utils.c clean_new_hydro)
 void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu) {
   (void)param;
   (void)cpu;
   if (firstoct == nullptr || level < 1) return;
-  for (struct OCT *o = firstoct[level - 1]; o != nullptr; o = o->next)
-    for (int c = 0; c < 8; c++) o->cell[c].fieldnew = o->cell[c].field;
+  if (level >= kMaxLevels) return;
+  const std::vector<struct OCT *> &v = walk_level(firstoct, level);
+  parallel_for((long long)v.size(), [&](long long a0, long long b0) {
+    for (long long i = a0; i < b0; i++)
+      for (int c = 0; c < 8; c++) v[i]->cell[c].fieldnew = v[i]->cell[c].field;
+  });
 }
 
 void create_hydstencil_GPU(struct CPUINFO *cpu, int stride) {
@@ -1339,9 +1589,7 @@ void destroy_hydstencil_GPU(struct CPUINFO *cpu, int stride) {
   (void)stride;
   if (!g.ready) return;
   cudaStreamSynchronize(g.stream);
-  free_tree(g.drop);
-  g.drop_level = -1;
-  g.drop_first = nullptr;
+  drop_all();
 }
 
 void create_pinned_stencil(struct HGRID **stencil, int stride) {

@@ -142,6 +142,16 @@ long long emma_hydro_level_leaf_cells(int level);
 long long emma_hydro_cell_updates(void);
 /* Kernels of this library launched since the last reset. */
 long long emma_hydro_kernel_launches(void);
+/* Bytes of field state copied host->device and device->host by this library
+ * since the last reset (drop-in entries, state set/get, tree fields upload and
+ * download; not the one-off topology and plan uploads). */
+int emma_hydro_transfer_bytes(long long *h2d, long long *d2h);
+/* Host-side phases (ms) of the last advancehydroGPU / HydroSolver call:
+ * [0] walk and hash of the level lists, [1] mirror build (0 when cached),
+ * [2] pack + queue of the uploads, [3] kernel launch, download and unpack,
+ * [4] mean wait of a host thread for its downloaded range, [5] fine->coarse
+ * corrections, [6] rest of HydroSolver's final update, [7] the whole call. */
+int emma_hydro_dropin_profile(double *ms8);
 void emma_hydro_reset_counters(void);
 /* Average device time (ms) of the level kernel launches since the last reset,
  * measured with CUDA events on the launching stream, and their count. */

@@ -145,6 +145,32 @@ def test_dropin_hydrosolver_matches_oracle(gpu):
         assert e.max() <= 1e-12, (l, e.max())
 
 
+def test_dropin_advancehydrogpu_writes_fieldnew_only(gpu):
+    """advancehydroGPU alone (src/hydro_utils_gpu.cu:2470): fieldnew of the level's
+    leaves and the coarser level's corrected cells equal the oracle's HydroSolver
+    result; `field` stays as it was."""
+    cfg = configs.small_amr(base=4, radii=(0.3, 0.15))
+    tg, to = cfg.build(), cfg.build()
+    R = oracle.Restatement()
+    H.lib().emma_hydro_clear_status()
+    for l in (4, 5, 6):
+        H.clean_new_hydro(l, tg.firstoct)
+        R.clean_new(to.firstoct, l)
+    before = tg.get_fields(6)
+    for l in (6, 5):
+        assert H.advancehydroGPU(tg.firstoct, l, 1e-3) == tg.noct(l)
+        assert R.hydro_solver(to.firstoct, l, 1e-3) == 0
+    assert H.lib().emma_hydro_status() == 0
+    assert np.array_equal(tg.get_fields(6), before)
+    for l in (5, 6):
+        leaf = ~tg.split_mask(l)
+        e = per_cell_rel(tg.get_fields(l, which=1)[:5][:, leaf], to.get_fields(l, which=1)[:5][:, leaf])
+        assert e.max() <= 1e-12, (l, e.max())
+    # level 4 received level 5's fine->coarse corrections in fieldnew
+    e = per_cell_rel(tg.get_fields(4, which=1)[:5], to.get_fields(4, which=1)[:5])
+    assert e.max() <= 1e-12, e.max()
+
+
 def test_mixed_precision_l1_and_conservation(gpu):
     cfg = configs.random_uniform(level=5)
     tm, r, st = run_gpu(cfg, 10, precision=PREC_MIXED)
