@@ -83,6 +83,10 @@ struct MathF64 {
     for (int i = 0; i < 5; i++) W[i] = q0[i] + fx * D[0][i] + fy * D[1][i] + fz * D[2][i] + Wt[i];
     W[4] = fmax(W[4], kPmin);
     if (W[0] < 0) st |= kStNegDensity;
+    face_finish(W);
+  }
+  // E and a of a face state from its (d,u,v,w,p)
+  static __device__ __forceinline__ void face_finish(double W[7]) {
     W[6] = W[4] / (kGam - 1.) + 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]);
     W[5] = sqrt(kGam * W[4] / W[0]);
   }
@@ -199,8 +203,7 @@ struct MathF64 {
     for (int i = 0; i < 5; i++) W[i] = q0[i] + f * Dax[i] + Wt[i];
     W[4] = fmax(W[4], kPmin);
     if (W[0] < 0) st |= kStNegDensity;
-    W[6] = W[4] / (kGam - 1.) + 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]);
-    W[5] = sqrt(kGam * W[4] / W[0]);
+    face_finish(W);
   }
 
   // State rotated to the face frame: r = {d, u_n, u_t1, u_t2, p, E, |m|^2},

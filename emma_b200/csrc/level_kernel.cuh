@@ -179,14 +179,21 @@ struct TileSmem {
   static constexpr size_t off_st = a16(off_cmk + 2 * NS);                      // u8  [NBOX] cell flags
   static constexpr size_t off_W = a16(off_st + NBOX);                          // R4  [NBOX] (d,u,v,w)
   static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * NBOX);          // R   [NBOX] p
-  static constexpr size_t off_M = a16(off_Wp + sizeof(R) * NBOX);              // R4  [5][kThreads]
-  static constexpr size_t off_HS = a16(off_M + sizeof(R) * 4 * 5 * kThreads);  // R4  [2][NRING] ring faces
-  static constexpr size_t off_end = a16(off_HS + sizeof(R) * 4 * 2 * NRING);
-  // face fluxes: the FP32 path reuses the staged box, dead after reconstruction
-  static constexpr size_t off_F = kF64 ? off_end : off_W;               // R4 [NF]
+  // reconstruction of the brick cells: R4 groups [kMG][kThreads] (slopes, predicted
+  // state; FP64 also the centre state, so that the box is dead after P1), then the
+  // FP64 centre pressure R [kThreads]
+  static constexpr int kMG = kF64 ? 6 : 5;
+  static constexpr size_t off_M = a16(off_Wp + sizeof(R) * NBOX);
+  static constexpr size_t off_Mp = off_M + sizeof(R) * 4 * kMG * kThreads;
+  // ring face states: FP32 R4 [2][NRING] (d,u,v,w | p,1/d,a); FP64 R4 [NRING] + R [NRING]
+  // (d,u,v,w | p: a and E are recomputed by the consumer)
+  static constexpr size_t off_HS = a16(off_Mp + (kF64 ? sizeof(R) * kThreads : 0));
+  static constexpr size_t off_end = a16(off_HS + (kF64 ? sizeof(R) * 5 * NRING : sizeof(R) * 4 * 2 * NRING));
+  // face fluxes reuse the staged box, dead after reconstruction
+  static constexpr size_t off_F = off_W;                               // R4 [NF]
   static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
-  static constexpr size_t bytes = kF64 ? a16(off_F1 + sizeof(R) * NF) : off_end;
-  static_assert(kF64 || off_F1 + sizeof(R) * NF <= off_M, "FP32 face fluxes must fit in the staged box");
+  static constexpr size_t bytes = off_end;
+  static_assert(off_F1 + sizeof(R) * NF <= off_M, "face fluxes must fit in the staged box");
 };
 
 // One tile.  Software pipeline over the tiles of a CTA: the level's arguments
@@ -215,6 +222,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   R *sW = reinterpret_cast<R *>(smem + SM::off_W);
   R *sWp = reinterpret_cast<R *>(smem + SM::off_Wp);
   R *sM = reinterpret_cast<R *>(smem + SM::off_M);
+  R *sMp = reinterpret_cast<R *>(smem + SM::off_Mp);
   R *sHS = reinterpret_cast<R *>(smem + SM::off_HS);
   R *sF = reinterpret_cast<R *>(smem + SM::off_F);
   R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
@@ -385,6 +393,12 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       if (!need && f_ok(f))
         need = f_tileleaf(sSt[tb - 1]) || f_tileleaf(sSt[tb + 1]) || f_tileleaf(sSt[tb - G::XX]) ||
                f_tileleaf(sSt[tb + G::XX]) || f_tileleaf(sSt[tb - G::XS]) || f_tileleaf(sSt[tb + G::XS]);
+      if constexpr (F64) {  // the centre state, for the face states and the update
+        R q[5];
+        q_at(tb, q);
+        V::st(sM, 5 * kThreads + tid, q[0], q[1], q[2], q[3]);
+        sMp[tid] = q[4];
+      }
     } else {
       r = w - kThreads;
       const int nb = r / G::kRing;
@@ -419,10 +433,15 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       R Dax[5], W[7];
 #pragma unroll
       for (int v = 0; v < 5; v++) Dax[v] = (ax == 0) ? D[0][v] : ((ax == 1) ? D[1][v] : D[2][v]);
-      if constexpr (F64) M::face_ax(q0, Dax, Wt, k, W, st);
-      else M::face_px(X, Dax, k, W, st);
-      V::st(sHS, r, W[0], W[1], W[2], W[3]);
-      V::st(sHS, NRING + r, W[4], W[5], W[6], (R)0);
+      if constexpr (F64) {
+        M::face_ax(q0, Dax, Wt, k, W, st);
+        V::st(sHS, r, W[0], W[1], W[2], W[3]);
+        sHS[4 * NRING + r] = W[4];
+      } else {
+        M::face_px(X, Dax, k, W, st);
+        V::st(sHS, r, W[0], W[1], W[2], W[3]);
+        V::st(sHS, NRING + r, W[4], W[5], W[6], (R)0);
+      }
     }
   }
   __syncthreads();
@@ -438,16 +457,22 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     Dax[4] = (ax == 0) ? p0 : ((ax == 1) ? p1 : p2);
     if constexpr (F64) {
       R q0[5];
-      q_at(b, q0);
+      V::ld(sM, 5 * kThreads + t, q0[0], q0[1], q0[2], q0[3]);
+      q0[4] = sMp[t];
       M::face_ax(q0, Dax, X, k, W, st);
     } else {
       M::face_px(X, Dax, k, W, st);
     }
   };
   auto ring_face = [&](int r, R W[7]) {
-    R pad;
     V::ld(sHS, r, W[0], W[1], W[2], W[3]);
-    V::ld(sHS, NRING + r, W[4], W[5], W[6], pad);
+    if constexpr (F64) {
+      W[4] = sHS[4 * NRING + r];
+      M::face_finish(W);
+    } else {
+      R pad;
+      V::ld(sHS, NRING + r, W[4], W[5], W[6], pad);
+    }
   };
 
   // ------------------------------------------------------------------ P2
@@ -591,8 +616,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     const long long gi = 8LL * (sKey[s] & 0x0FFFFFFFu) + c;
     double q[5];  // the FP64 state: staged (plain path) or read again from L2 (mixed path)
     if constexpr (F64) {
-      V::ld(sW, tb, q[0], q[1], q[2], q[3]);
-      q[4] = sWp[tb];
+      V::ld(sM, 5 * kThreads + tid, q[0], q[1], q[2], q[3]);
+      q[4] = sMp[tid];
     } else {
 #pragma unroll
       for (int v = 0; v < 5; v++) q[v] = __ldg(A.W + v * N8 + gi);
@@ -780,12 +805,14 @@ constexpr size_t level_smem_bytes(unsigned shapes) {
 // launch use (bit i: kShapes[i]); each level's plan names its own.
 // Occupancy targets: the FP32 kernel with 4x4x2 bricks only fits 4 CTAs per SM
 // (64 registers, 55 KB of shared memory); with 2x2x2 bricks shared memory
-// allows 2; the FP64 kernel 1.
+// allows 2; the FP64 kernel 2 with 4x4x2 bricks (128 registers, 110 KB), 1 with
+// 2x2x2 bricks.
 template <class M, unsigned SHAPES>
-constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? 1 : (SHAPES == 1u ? 4 : 2);
+constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? (SHAPES == 1u ? 2 : 1) : (SHAPES == 1u ? 4 : 2);
 // 228 KB of shared memory per SM, 1 KB reserved per CTA
 static_assert(4 * (TileSmem<MathF32, GeomA>::bytes + 1024) <= 228 * 1024, "4 FP32 4x4x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF32, GeomB>::bytes + 1024) <= 228 * 1024, "2 FP32 2x2x2 CTAs per SM");
+static_assert(2 * (TileSmem<MathF64, GeomA>::bytes + 1024) <= 228 * 1024, "2 FP64 4x4x2 CTAs per SM");
 
 template <class M, unsigned SHAPES>
 __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch_kernel(const BatchArgs Bt) {
