@@ -43,6 +43,11 @@ typedef struct oCell {
   struct oOct *child;
   double marked;
   int idx;
+#ifdef ORC_WGRAV
+  double gd, gp;   /* struct Gtype gdata (src/prototypes.h:818) */
+  double pnew, res;
+  double f[3];     /* gravitational acceleration of the cell */
+#endif
   oW field;
   oW fieldnew;
 } oCell;
@@ -55,8 +60,13 @@ typedef struct oOct {
   int cpu;
   int level;
 } oOct;
+#ifdef ORC_WGRAV
+_Static_assert(sizeof(oCell) == 192, "CELL layout (-DWGRAV)");
+_Static_assert(sizeof(oOct) == 1648, "OCT layout (-DWGRAV)");
+#else
 _Static_assert(sizeof(oCell) == 136, "CELL layout");
 _Static_assert(sizeof(oOct) == 1200, "OCT layout");
+#endif
 
 static int g_err = 0;
 static long long g_updates = 0;
@@ -146,6 +156,9 @@ static void predictor(const oW *W0, double dt, double dx, double D[3][5], double
 typedef struct {
   oW w[27][8];
   char split[27][8];
+#ifdef ORC_WGRAV
+  double f[27][8][3]; /* force of each stencil cell */
+#endif
   /* memoised MUSCL face states, 6 per stencil cell */
   oW face[27][8][6];
   char done[27][8];
@@ -180,6 +193,12 @@ static void muscl_cell(Stencil *st, int slot, int ic, double dt, double dx) {
     Wi->d = r[0]; Wi->u = r[1]; Wi->v = r[2]; Wi->w = r[3];
     Wi->p = fmax(r[4], P_MIN);
     if (Wi->d < 0) g_err |= ORC_ERR_NEG_DENSITY;
+#ifdef ORC_WGRAV
+    /* half-step gravity kick of the face velocities (src/hydro_utils.c:1219-1226) */
+    Wi->u += -st->f[slot][ic][0] * 0.5 * dt;
+    Wi->v += -st->f[slot][ic][1] * 0.5 * dt;
+    Wi->w += -st->f[slot][ic][2] * 0.5 * dt;
+#endif
     get_E(Wi);
     Wi->a = sqrt(GAM * Wi->p / Wi->d);
   }
@@ -395,6 +414,7 @@ static void interp_coarse(oCell *cell, oW Wi[8], int flags) {
       }
 }
 
+
 /* mirror maps of the transmissive ghost octs (src/hydro_utils.c:2504-2610) */
 static const int MIRROR[6][8] = {
     {0, 0, 2, 2, 4, 4, 6, 6}, /* -x */
@@ -417,6 +437,44 @@ static int at_boundary(const oOct *o, int k) {
     default: return (o->z + 2. * dx) == 1.;
   }
 }
+
+#ifdef ORC_WGRAV
+/* coarse2fine_forcelin (src/poisson_utils.c:315-425): the force of a coarse leaf
+ * cell spread over its 8 sub-cells by unlimited one-sided differences: a
+ * sub-cell on the - side of an axis uses f0 - f(-neighbour), on the + side
+ * f(+neighbour) - f0, times an offset of -/+1/4; transmissive faces use the
+ * cell itself as the neighbour. */
+static void force_lin(oCell *cell, double floc[24], int flags) {
+  oOct *oct = oct_of(cell);
+  const double *U0 = cell->f;
+  double D[6][3];
+  int dir, i, ix, iy, iz;
+  for (dir = 0; dir < 3; dir++) {
+    const double *Um = NULL, *Up = NULL;
+    int same, nc;
+    cell_nei(cell->idx, 2 * dir, &same, &nc);
+    if (same) Um = oct->cell[nc].f;
+    else if (oct->nei[2 * dir] != NULL && oct->nei[2 * dir]->child != NULL) Um = oct->nei[2 * dir]->child->cell[nc].f;
+    if (!same && flag_on(flags, TFLAG[2 * dir]) && at_boundary(oct, 2 * dir)) Um = U0;
+    cell_nei(cell->idx, 2 * dir + 1, &same, &nc);
+    if (same) Up = oct->cell[nc].f;
+    else if (oct->nei[2 * dir + 1] != NULL && oct->nei[2 * dir + 1]->child != NULL)
+      Up = oct->nei[2 * dir + 1]->child->cell[nc].f;
+    if (!same && flag_on(flags, TFLAG[2 * dir + 1]) && at_boundary(oct, 2 * dir + 1)) Up = U0;
+    if (Um == NULL || Up == NULL) { g_err |= ORC_ERR_TREE; Um = Up = U0; }
+    for (i = 0; i < 3; i++) D[2 * dir][i] = U0[i] - Um[i];
+    for (i = 0; i < 3; i++) D[2 * dir + 1][i] = Up[i] - U0[i];
+  }
+  for (iz = 0; iz < 2; iz++)
+    for (iy = 0; iy < 2; iy++)
+      for (ix = 0; ix < 2; ix++) {
+        double *fp = floc + 3 * (ix + 2 * iy + 4 * iz);
+        for (i = 0; i < 3; i++)
+          fp[i] = U0[i] + D[ix][i] * (-0.25 + ix * 0.5) + D[2 + iy][i] * (-0.25 + iy * 0.5) +
+                  D[4 + iz][i] * (-0.25 + iz * 0.5);
+      }
+}
+#endif
 
 /* One step of the recursive neighbour walk: from the level-(L-1) cell `cell`,
  * find the level-(L-1) cell across direction k, fill stencil slot `slot`, and
@@ -449,17 +507,29 @@ static oCell *fill_slot(Stencil *st, int slot, oCell *cell, int k, int flags) {
     }
   }
   if (nc == NULL) { g_err |= ORC_ERR_TREE; return NULL; }
+#ifdef ORC_WGRAV
+  double floc[24];
+#endif
   if (nc->child != NULL) {
     for (c = 0; c < 8; c++) { Wi[c] = nc->child->cell[c].field; ch[c] = (nc->child->cell[c].child != NULL); }
+#ifdef ORC_WGRAV
+    for (c = 0; c < 8; c++) memcpy(floc + 3 * c, nc->child->cell[c].f, sizeof(double) * 3);
+#endif
   } else {
     if (hydrotest) interp_coarse(nc, Wi, flags);
     else for (c = 0; c < 8; c++) Wi[c] = nc->field;
     for (c = 0; c < 8; c++) ch[c] = 0;
+#ifdef ORC_WGRAV
+    force_lin(nc, floc, flags);
+#endif
   }
   for (c = 0; c < 8; c++) {
     int s = map ? map[c] : c;
     st->w[slot][c] = Wi[s];
     st->split[slot][c] = ch[s];
+#ifdef ORC_WGRAV
+    memcpy(st->f[slot][c], floc + 3 * s, sizeof(double) * 3);
+#endif
   }
   return nc;
 }
@@ -492,6 +562,9 @@ static void gather(Stencil *st, oOct *o, int flags) {
   for (c = 0; c < 8; c++) {
     st->w[13][c] = o->cell[c].field;
     st->split[13][c] = (o->cell[c].child != NULL);
+#ifdef ORC_WGRAV
+    memcpy(st->f[13][c], o->cell[c].f, sizeof(double) * 3);
+#endif
   }
   visit[13] = 1;
   for (k = 0; k < 6; k++) {
@@ -619,6 +692,32 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
   return g_err;
 }
 
+#ifdef ORC_WGRAV
+/* grav_correction (src/hydro_utils.c:2388-2444, PRIMITIVE): the full-step
+ * gravity kick of the leaf velocities after HydroSolver, then E. */
+int orc_grav_correction(void **firstoct_v, int level, double dt) {
+  oOct **firstoct = (oOct **)firstoct_v;
+  oOct *o;
+  int c, err = 0;
+  for (o = firstoct[level - 1]; o != NULL; o = o->next) {
+    if (o->cpu != 0) continue;
+    for (c = 0; c < 8; c++) {
+      oCell *cell = &o->cell[c];
+      oW W;
+      if (cell->child != NULL) continue;
+      W = cell->field;
+      W.u += (-cell->f[0] * dt);
+      W.v += (-cell->f[1] * dt);
+      W.w += (-cell->f[2] * dt);
+      get_E(&W);
+      if (W.p < 0) err |= ORC_ERR_NAN;
+      cell->field = W;
+    }
+  }
+  return err;
+}
+#endif
+
 void orc_clean_new_hydro(void **firstoct_v, int level) {
   oOct **firstoct = (oOct **)firstoct_v;
   oOct *o;
@@ -682,6 +781,9 @@ static double advance_level(Sched *S, int level, double tloc) {
       if (level == S->lcoarse) adt[level - 2] = adt[level - 1];
     }
     S->err |= orc_hydro_solver((void **)S->first, level, adt[level - 1], S->flags);
+#ifdef ORC_WGRAV
+    S->err |= orc_grav_correction((void **)S->first, level, adt[level - 1]); /* src/advanceamr.c:999 */
+#endif
     dt += adt[level - 1];
     tloc += adt[level - 1];
     is++;

@@ -38,6 +38,11 @@ extern "C" {
 int orc_hydro_solver(void **firstoct, int level, double dt, int flags);
 void orc_clean_new_hydro(void **firstoct, int level);
 double orc_comptstep_hydro(void **firstoct, int level, double cfl);
+/* Built with -DORC_WGRAV (liboracle_grav.so): the tree carries the -DWGRAV cell
+ * layout (192-byte CELL with the force f[3]), the MUSCL face states get the
+ * half-step gravity kick and the schedule calls grav_correction after each
+ * HydroSolver (src/advanceamr.c:999). */
+int orc_grav_correction(void **firstoct, int level, double dt);
 /* Hydro-only Advance_level schedule; returns tsim after `nsteps` coarse steps.
  * adt has lmax entries (in/out), like the reference's adt array. */
 double orc_run(void **firstoct, int lcoarse, int lmax, int nsteps, double dt_param,

@@ -4,9 +4,10 @@ TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
 bench.py's CPU-baseline / reference arm, always as the checker or the timed CPU
 baseline, never on the product path.
 
-  Restatement  -- oracle/_build/liboracle.so, the C restatement of the hydro level
-                  advance (hydro_oracle.c); runs in place on any struct OCT tree.
-  RefTree      -- oracle/_ref/libemmaref[_tx].so, the reference's own CPU hydro
+  Restatement  -- oracle/_build/liboracle[_grav].so, the C restatement of the hydro
+                  level advance (hydro_oracle.c); runs in place on any struct OCT tree
+                  (_grav: the -DWGRAV cell layout, gravity-coupled hydro).
+  RefTree      -- oracle/_ref/libemmaref[_tx|_grav].so, the reference's own CPU hydro
                   compiled from its sources with ref_driver.c (tree built by the
                   reference's build_initial_grid / L_refine_cells).
 """
@@ -17,8 +18,10 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
+ORACLE_LIB_GRAV = os.path.join(HERE, "_build", "liboracle_grav.so")
 REF_LIB = os.path.join(HERE, "_ref", "libemmaref.so")
 REF_LIB_TX = os.path.join(HERE, "_ref", "libemmaref_tx.so")
+REF_LIB_GRAV = os.path.join(HERE, "_ref", "libemmaref_grav.so")
 
 HYDROTEST = 0x40
 c_int, c_double, c_void_p, c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
@@ -34,13 +37,15 @@ def flags_for(trans):
 
 
 class Restatement:
-    _lib = None
+    """grav=True: the -DWGRAV layout and gravity coupling (liboracle_grav.so)."""
+    _libs = {}
 
-    def __init__(self):
-        if Restatement._lib is None:
-            if not os.path.exists(ORACLE_LIB):
-                raise RuntimeError(f"oracle restatement not built: {ORACLE_LIB}")
-            L = ctypes.CDLL(ORACLE_LIB)
+    def __init__(self, grav=False):
+        path = ORACLE_LIB_GRAV if grav else ORACLE_LIB
+        if path not in Restatement._libs:
+            if not os.path.exists(path):
+                raise RuntimeError(f"oracle restatement not built: {path}")
+            L = ctypes.CDLL(path)
             L.orc_hydro_solver.argtypes = [c_void_p, c_int, c_double, c_int]
             L.orc_hydro_solver.restype = c_int
             L.orc_clean_new_hydro.argtypes = [c_void_p, c_int]
@@ -50,8 +55,12 @@ class Restatement:
                                   c_double, c_void_p, ctypes.POINTER(c_int), ctypes.POINTER(c_int)]
             L.orc_run.restype = c_double
             L.orc_cell_updates.restype = c_ll
-            Restatement._lib = L
-        self.L = Restatement._lib
+            if grav:
+                L.orc_grav_correction.argtypes = [c_void_p, c_int, c_double]
+                L.orc_grav_correction.restype = c_int
+            Restatement._libs[path] = L
+        self.L = Restatement._libs[path]
+        self.grav = grav
 
     def run(self, firstoct, lcoarse, lmax, nsteps, cfl, trans=0, nsub=2, dt_param=1e9, time_max=1e9, tsim0=0.0):
         adt = np.zeros(lmax)
@@ -69,6 +78,12 @@ class Restatement:
     def comptstep(self, firstoct, level, cfl):
         return self.L.orc_comptstep_hydro(firstoct, level, cfl)
 
+    def grav_correction(self, firstoct, level, dt):
+        return self.L.orc_grav_correction(firstoct, level, dt)
+
+    def sizeof_oct(self):
+        return self.L.orc_sizeof_oct()
+
     def cell_updates(self):
         return self.L.orc_cell_updates()
 
@@ -76,8 +91,8 @@ class Restatement:
         self.L.orc_reset_counters()
 
 
-def ref_available(tx=False):
-    return os.path.exists(REF_LIB_TX if tx else REF_LIB)
+def ref_available(tx=False, grav=False):
+    return os.path.exists(REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
 
 
 class RefTree:
@@ -85,8 +100,9 @@ class RefTree:
 
     _libs = {}
 
-    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024):
-        path = REF_LIB_TX if tx else REF_LIB
+    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False):
+        assert not (tx and grav), "no transmissive gravity build"
+        path = REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB)
         if path not in RefTree._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"reference oracle not built: {path}")
@@ -102,6 +118,7 @@ class RefTree:
             L.ref_adt.restype = c_double
             L.ref_init.argtypes = [c_int, c_int, c_int, c_int]
             RefTree._libs[path] = L
+        self.grav = grav
         self.L = RefTree._libs[path]
         self.lcoarse, self.lmax = lcoarse, lmax
         if ngridmax is None:
@@ -146,6 +163,14 @@ class RefTree:
         if n:
             self.L.ref_get_field(level, which, _p(out))
         return out
+
+    def set_force(self, level, fx, fy, fz):
+        """Gravitational acceleration of every cell of a level (gravity build only)."""
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fx, fy, fz)]
+        self.L.ref_set_force(level, *[_p(a) for a in arrs])
+
+    def sizeof_oct(self):
+        return self.L.ref_sizeof_oct()
 
     def topology(self, level):
         n = self.noct(level)

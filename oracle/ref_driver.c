@@ -242,6 +242,20 @@ void ref_set_field(int level, const double *d, const double *u, const double *v,
   }
 }
 
+#ifdef WGRAV
+/* Set the gravitational acceleration f[3] of every cell of a level (list order). */
+void ref_set_force(int level, const double *fx, const double *fy, const double *fz) {
+  int i = 0, c;
+  struct OCT *o;
+  for (o = g_first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) {
+      o->cell[c].f[0] = fx[8 * i + c];
+      o->cell[c].f[1] = fy[8 * i + c];
+      o->cell[c].f[2] = fz[8 * i + c];
+    }
+}
+#endif
+
 /* Export d,u,v,w,p,a,E of field (which=0) or fieldnew (which=1) as 7 planes. */
 void ref_get_field(int level, int which, double *out) {
   int n = g_cpu.noct[level - 1] * 8, i = 0, c;
@@ -304,6 +318,9 @@ static REAL advance_level(int level, REAL tloc) {
       }
     }
     ref_hydro_solver(level, adt[level - 1]);                       /* :989 */
+#ifdef WGRAV
+    grav_correction(level, &g_param, g_first, &g_cpu, adt[level - 1]); /* :999 */
+#endif
     dt += adt[level - 1];                                          /* :1278 */
     tloc += adt[level - 1];
     is++;
@@ -344,3 +361,24 @@ void dumpIO(REAL tsim, struct RUNPARAMS *param, struct CPUINFO *cpu, struct OCT 
   fprintf(stderr, "ref_driver: dumpIO is not part of the oracle\n");
   abort();
 }
+
+#ifdef WGRAV
+/* -DWGRAV builds leave out src/tools.c, whose multicheck reads a member that
+ * exists only with -DPIC; these stand in for the three functions of it that
+ * other compiled files reference.  Only myradixsort is reached (the single-rank
+ * neighbour list of setup_mpi, src/communication.c:232): ascending order. */
+REAL multicheck(struct OCT **firstoct, int *npart, int levelcoarse, int levelmax, int rank, struct CPUINFO *cpu,
+                struct RUNPARAMS *param, int label) {
+  (void)firstoct; (void)npart; (void)levelcoarse; (void)levelmax; (void)rank; (void)cpu; (void)param; (void)label;
+  return 0.;
+}
+void grid_census(struct RUNPARAMS *param, struct CPUINFO *cpu) { (void)param; (void)cpu; }
+void myradixsort(int *a, int n) {
+  int i, j;
+  for (i = 1; i < n; i++) {
+    int x = a[i];
+    for (j = i - 1; j >= 0 && a[j] > x; j--) a[j + 1] = a[j];
+    a[j + 1] = x;
+  }
+}
+#endif

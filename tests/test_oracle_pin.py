@@ -29,8 +29,15 @@ def random_fields(tree, levels, seed=12345):
         tree.set_fields(l, d, u, v, w, p)
 
 
-def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None):
-    ref = oracle.RefTree(base, lmax, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)))
+def random_forces(tree, levels, seed=54321, amp=0.5):
+    rng = np.random.default_rng(seed)
+    for l in levels:
+        n8 = 8 * tree.noct(l)
+        tree.set_force(l, *(rng.uniform(-amp, amp, n8) for _ in range(3)))
+
+
+def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, grav=False):
+    ref = oracle.RefTree(base, lmax, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)), grav=grav)
     for i, r in enumerate(radii):
         ref.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
     if fields is None:
@@ -38,14 +45,17 @@ def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None):
     else:
         for l in range(base, lmax + 1):
             ref.set_fields(l, *fields(ref.cell_centres(l)))
+    if grav:
+        random_forces(ref, range(base, lmax + 1))
+        assert ref.sizeof_oct() == oracle.Restatement(grav=True).sizeof_oct() == 1648
     base_ptr = ref.L.ref_grid_base()
-    nbytes = ref.ngridmax * 1200
+    nbytes = ref.ngridmax * ref.sizeof_oct()
     snap = ctypes.string_at(base_ptr, nbytes)
     t1, adt1 = ref.run(nsteps)
     A = {l: (ref.get_fields(l, 0), ref.get_fields(l, 1)) for l in range(base, lmax + 1)}
     ctypes.memmove(base_ptr, snap, nbytes)
     trans = 3 if tx else 0
-    t2, adt2, err = oracle.Restatement().run(ref.firstoct, base, lmax, nsteps, 0.8, trans=trans)
+    t2, adt2, err = oracle.Restatement(grav=grav).run(ref.firstoct, base, lmax, nsteps, 0.8, trans=trans)
     assert err == 0
     assert t1 == t2 and np.array_equal(adt1, adt2)
     for l in range(base, lmax + 1):
@@ -83,6 +93,22 @@ def test_pin_sod_tube():
                         np.where(c[:, 0] < 0.5, 1.0, 0.1))
     assert sod.trans == 3
     ref_vs_restatement(True, 4, 4, (), 10, fields=fields)
+
+
+needs_ref_grav = pytest.mark.skipif(not oracle.ref_available(grav=True), reason="oracle/_ref gravity build absent")
+
+
+@needs_ref_grav
+def test_pin_gravity_uniform():
+    """-DWGRAV: face-state kick, grav_correction after each HydroSolver."""
+    ref_vs_restatement(False, 4, 4, (), 3, grav=True)
+
+
+@needs_ref_grav
+def test_pin_gravity_amr():
+    """-DWGRAV on two refined levels: forces of injected coarse cells interpolated
+    (coarse2fine_forcelin) in the gather."""
+    ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, grav=True)
 
 
 def _golden_cases():
