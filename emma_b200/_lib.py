@@ -19,7 +19,7 @@ P = ctypes.POINTER
 
 class EmmaHydroOptions(ctypes.Structure):
     _fields_ = [("precision", c_int), ("trans_flags", c_int), ("cfl", c_double),
-                ("tile_octs", c_int), ("device", c_int), ("use_graph", c_int)]
+                ("tile_octs", c_int), ("device", c_int), ("use_graph", c_int), ("gravity", c_int)]
 
 
 PREC_FP64, PREC_MIXED = 0, 1
@@ -59,6 +59,8 @@ SIGNATURES = [
     ("emma_hydro_level_noct", c_int, [c_int]),
     ("emma_hydro_get_level_state", c_int, [c_int, c_void_p]),
     ("emma_hydro_set_level_state", c_int, [c_int, c_void_p]),
+    ("emma_hydro_set_level_force", c_int, [c_int, c_void_p]),
+    ("emma_hydro_set_level_force_device", c_int, [c_int, c_void_p]),
     ("emma_hydro_level_leaf_cells", c_ll, [c_int]),
     ("emma_hydro_cell_updates", c_ll, []),
     ("emma_hydro_reset_counters", None, []),

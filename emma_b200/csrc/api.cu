@@ -44,8 +44,10 @@ struct DevLevel {
   TileDesc *tiles = nullptr;
   uint32_t *keys = nullptr;
   int *work = nullptr;  // (L << 24) | tile for every tile of the level
-  int *vcell = nullptr;    // transmissive build: interpolated coarser cells and their slope neighbours
-  double *Wv = nullptr;    // their 8 interpolated sub-cells
+  int *vcell = nullptr;    // transmissive or gravity build: interpolated coarser cells and their slope neighbours
+  double *Wv = nullptr;    // their 8 interpolated (gravity build: injected) sub-cells
+  double *F = nullptr;     // gravity build: acceleration planes fx,fy,fz of the level's cells
+  double *Fv = nullptr;    // gravity build: interpolated accelerations of the listed coarser cells
   long long nv = 0;
   int shape = 0;        // brick shape of the plan (kShapes)
   int ctas = 0;         // CTAs per SM of its launches (0: the occupancy limit)
@@ -207,6 +209,8 @@ void free_level(DevLevel &d) {
   cudaFree(d.work);
   cudaFree(d.vcell);
   cudaFree(d.Wv);
+  cudaFree(d.F);
+  cudaFree(d.Fv);
   d = DevLevel();
 }
 
@@ -277,6 +281,11 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     if (d.nv > 0) {
       if (!upload_vec(&d.vcell, h.interp)) return false;
       if (!ck(cudaMalloc(&d.Wv, sizeof(double) * 5 * 8 * (size_t)d.nv), "cudaMalloc Wv")) return false;
+      if (H.grav && !ck(cudaMalloc(&d.Fv, sizeof(double) * 3 * 8 * (size_t)d.nv), "cudaMalloc Fv")) return false;
+    }
+    if (H.grav) {  // accelerations start at zero until the caller sets them
+      const size_t fb = sizeof(double) * 3 * (size_t)std::max<long long>(d.n8, 1);
+      if (!ck(cudaMalloc(&d.F, fb), "cudaMalloc F") || !ck(cudaMemset(d.F, 0, fb), "cudaMemset F")) return false;
     }
     std::vector<int> work((size_t)d.ntiles);
     for (int i = 0; i < d.ntiles; i++) work[i] = (L << kWorkSlotShift) | i;
@@ -303,6 +312,11 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     a.ntiles = d.ntiles;
     a.wait_slot = -1;
     a.leaf = d.leaf;
+    a.F = d.F;
+    a.Fc = (L > H.lcoarse) ? t.lev[L - 1].F : nullptr;
+    a.Fv = d.Fv;
+    a.gcorr = H.grav;
+    a.wv_inject = H.grav;
     k_set_args<<<1, 1, 0, g.stream>>>(t.d_lv, L, a);
     if (!ck(cudaGetLastError(), "k_set_args")) return false;
   }
@@ -428,6 +442,8 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
     tl.b = get_event();
     cudaEventRecord(tl.a, g.stream);
   }
+  // the resident tree of a gravity upload runs the gravity-coupled variant
+  if (d_lv == g.res.d_lv && g.res.host.grav) shapes |= kLaunchGrav;
   cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED)
                       ? launch_level_f32(a, shapes, g.nsm, ctas, g.stream, nullptr)
                       : launch_level_fp64(a, shapes, g.nsm, ctas, g.stream, nullptr);
@@ -647,6 +663,7 @@ void emma_hydro_default_options(struct EmmaHydroOptions *opt) {
   opt->tile_octs = 0;
   opt->device = 0;
   opt->use_graph = 1;
+  opt->gravity = 0;
 }
 
 int emma_hydro_init(const struct EmmaHydroOptions *opt) {
@@ -674,10 +691,11 @@ int emma_hydro_init(const struct EmmaHydroOptions *opt) {
 int emma_hydro_set_options(const struct EmmaHydroOptions *opt) {
   if (opt == nullptr) return EMMA_ST_ARG;
   if (!g.ready) return emma_hydro_init(opt);
-  const int old_trans = g.opt.trans_flags;
+  const int old_trans = g.opt.trans_flags, old_grav = g.opt.gravity;
   g.opt = *opt;
-  if (old_trans != opt->trans_flags) {
-    // the tile plans encode the boundary ghosts: a resident tree must be uploaded again
+  if (old_trans != opt->trans_flags || old_grav != opt->gravity) {
+    // the tile plans encode the boundary ghosts and the gravity interpolation lists:
+    // a resident tree must be uploaded again
     cudaStreamSynchronize(g.stream);
     drop_graph();
     free_tree(g.res);
@@ -737,7 +755,7 @@ int requested_shape(int tile_octs) {
 
 // Point a level slot at a plan (tiles, keys, brick shape, interpolation list).
 bool bind_plan(LevelArgs *slot, TileDesc *tiles, uint32_t *keys, int shape, int ntiles, double *Wv, int *vcell,
-               long long nv) {
+               long long nv, double *Fv) {
   return ck(cudaMemcpyAsync(&slot->tiles, &tiles, sizeof(tiles), cudaMemcpyHostToDevice, g.stream), "bind") &&
          ck(cudaMemcpyAsync(&slot->keys, &keys, sizeof(keys), cudaMemcpyHostToDevice, g.stream), "bind") &&
          ck(cudaMemcpyAsync(&slot->shape, &shape, sizeof(int), cudaMemcpyHostToDevice, g.stream), "bind") &&
@@ -745,6 +763,7 @@ bool bind_plan(LevelArgs *slot, TileDesc *tiles, uint32_t *keys, int shape, int 
          ck(cudaMemcpyAsync(&slot->Wv, &Wv, sizeof(Wv), cudaMemcpyHostToDevice, g.stream), "bind") &&
          ck(cudaMemcpyAsync(&slot->vcell, &vcell, sizeof(vcell), cudaMemcpyHostToDevice, g.stream), "bind") &&
          ck(cudaMemcpyAsync(&slot->nv, &nv, sizeof(nv), cudaMemcpyHostToDevice, g.stream), "bind") &&
+         ck(cudaMemcpyAsync(&slot->Fv, &Fv, sizeof(Fv), cudaMemcpyHostToDevice, g.stream), "bind") &&
          ck(cudaStreamSynchronize(g.stream), "bind");
 }
 
@@ -782,7 +801,7 @@ bool autotune_tree(Tree &t, int shape_req) {
       TileDesc *tiles = d.tiles;
       uint32_t *keys = d.keys;
       int *work = d.work, *vcell = d.vcell;
-      double *Wv = d.Wv;
+      double *Wv = d.Wv, *Fv = d.Fv;
       long long nv = d.nv;
       int ntiles = d.ntiles;
       HostLevel alt;
@@ -799,21 +818,24 @@ bool autotune_tree(Tree &t, int shape_req) {
         for (int i = 0; i < ntiles; i++) wl[i] = (L << kWorkSlotShift) | i;
         vcell = nullptr;
         Wv = nullptr;
+        Fv = nullptr;
         if (!upload_vec(&tiles, alt.tiles) || !upload_vec(&keys, alt.keys) || !upload_vec(&work, wl) ||
             (nv > 0 && (!upload_vec(&vcell, alt.interp) ||
-                        !ck(cudaMalloc(&Wv, sizeof(double) * 5 * 8 * (size_t)nv), "cudaMalloc Wv")))) {
+                        !ck(cudaMalloc(&Wv, sizeof(double) * 5 * 8 * (size_t)nv), "cudaMalloc Wv"))) ||
+            (nv > 0 && t.host.grav && !ck(cudaMalloc(&Fv, sizeof(double) * 3 * 8 * (size_t)nv), "cudaMalloc Fv"))) {
           ok = false;
           break;
         }
       }
-      ok = bind_plan(t.d_lv + L, tiles, keys, s, ntiles, Wv, vcell, nv);
+      ok = bind_plan(t.d_lv + L, tiles, keys, s, ntiles, Wv, vcell, nv, Fv);
       k_bind_level<<<1, 1, 0, g.stream>>>(t.d_lv, L, t.lcoarse, t.lmax, 0.);
       if (ok) ok = ck(launch_interp(t.d_lv, L, nv, nullptr, g.nsm, g.stream), "interpolation launch");
       int occ = 0;
       BatchArgs probe{};
       if (ok)
-        ok = ck((g.opt.precision == EMMA_PREC_MIXED) ? launch_level_f32(probe, 1u << s, g.nsm, 0, g.stream, &occ)
-                                                      : launch_level_fp64(probe, 1u << s, g.nsm, 0, g.stream, &occ),
+        ok = ck((g.opt.precision == EMMA_PREC_MIXED)
+                    ? launch_level_f32(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u), g.nsm, 0, g.stream, &occ)
+                    : launch_level_fp64(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u), g.nsm, 0, g.stream, &occ),
                 "occupancy");
       for (int c = 1; ok && c <= std::min(occ, 4); c++) {
         double ms = 0;
@@ -840,11 +862,13 @@ bool autotune_tree(Tree &t, int shape_req) {
           cudaFree(d.work);
           cudaFree(d.vcell);
           cudaFree(d.Wv);
+          cudaFree(d.Fv);
           d.tiles = tiles;
           d.keys = keys;
           d.work = work;
           d.vcell = vcell;
           d.Wv = Wv;
+          d.Fv = Fv;
           d.nv = nv;
           d.ntiles = ntiles;
           d.shape = s;
@@ -855,11 +879,12 @@ bool autotune_tree(Tree &t, int shape_req) {
           cudaFree(work);
           cudaFree(vcell);
           cudaFree(Wv);
+          cudaFree(Fv);
         }
       }
     }
     // bind the kept plan
-    ok = ok && bind_plan(t.d_lv + L, d.tiles, d.keys, d.shape, d.ntiles, d.Wv, d.vcell, d.nv) &&
+    ok = ok && bind_plan(t.d_lv + L, d.tiles, d.keys, d.shape, d.ntiles, d.Wv, d.vcell, d.nv, d.Fv) &&
          ck(cudaStreamSynchronize(g.stream), "tune");
     d.ctas = best_ctas;
     d.tuned = ok;
@@ -899,7 +924,7 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
   }
   std::vector<int> shapes((size_t)lmax + 1, shape_req);
   int rc = build_host_tree(firstoct, lcoarse, lmax, rank, g.opt.trans_flags, lcoarse, lmax, g.res.host, err,
-                           shapes.data());
+                           shapes.data(), g.opt.gravity);
   if (rc != 0) {
     fail((unsigned)rc, err);
     return rc;
@@ -1022,6 +1047,30 @@ int emma_hydro_set_level_state(int level, const double *host_in) {
   g.h2d_bytes += (long long)sizeof(double) * 5 * d.n8;
   CK(mark_stale(level));
   CK(cudaStreamSynchronize(g.stream));
+  return 0;
+}
+
+int emma_hydro_set_level_force(int level, const double *host_f) {
+  if (!level_ok(level) || host_f == nullptr) return EMMA_ST_ARG;
+  const DevLevel &d = g.res.lev[level];
+  if (d.F == nullptr) {
+    fail(EMMA_ST_ARG, "emma_hydro_set_level_force: the tree was uploaded without gravity coupling");
+    return EMMA_ST_ARG;
+  }
+  CK(cudaMemcpyAsync(d.F, host_f, sizeof(double) * 3 * d.n8, cudaMemcpyHostToDevice, g.stream));
+  g.h2d_bytes += (long long)sizeof(double) * 3 * d.n8;
+  CK(cudaStreamSynchronize(g.stream));
+  return 0;
+}
+
+int emma_hydro_set_level_force_device(int level, const double *dev_f) {
+  if (!level_ok(level) || dev_f == nullptr) return EMMA_ST_ARG;
+  const DevLevel &d = g.res.lev[level];
+  if (d.F == nullptr) {
+    fail(EMMA_ST_ARG, "emma_hydro_set_level_force_device: the tree was uploaded without gravity coupling");
+    return EMMA_ST_ARG;
+  }
+  CK(cudaMemcpyAsync(d.F, dev_f, sizeof(double) * 3 * d.n8, cudaMemcpyDeviceToDevice, g.stream));
   return 0;
 }
 

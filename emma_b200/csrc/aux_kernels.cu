@@ -54,6 +54,11 @@ __device__ __forceinline__ double minmod_w(double m, double p) {
   return fmin(fmin(0., fmax(m, p)), fmax(m, p));
 }
 
+// Gravity builds (A.wv_inject): the listed cells keep the injected state (the
+// default gather, src/hydro_utils.c:2912-2944) and their force is spread by
+// coarse2fine_forcelin (src/poisson_utils.c:315-425): unlimited one-sided
+// differences, f = f0 + Dx ox + Dy oy + Dz oz with D = f0 - f(-nei) on the -
+// side of an axis and f(+nei) - f0 on the + side.
 __global__ void interp_coarse_kernel(const LevelArgs *lv, int slot, const int *gate) {
   if (gate != nullptr && *gate == 0) return;
   const LevelArgs &A = lv[slot];
@@ -62,6 +67,36 @@ __global__ void interp_coarse_kernel(const LevelArgs *lv, int slot, const int *g
   const long long nc8 = A.nc8, nv = A.nv, nv8 = 8 * A.nv;
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nv; j += (long long)gridDim.x * blockDim.x) {
     const int *vc = A.vcell + 7 * j;
+    if (A.Fv != nullptr && A.Fc != nullptr) {
+      double f0[3], Dm[3][3], Dp[3][3];
+#pragma unroll
+      for (int v = 0; v < 3; v++) f0[v] = A.Fc[v * nc8 + vc[0]];
+#pragma unroll
+      for (int dir = 0; dir < 3; dir++)
+#pragma unroll
+        for (int v = 0; v < 3; v++) {
+          Dm[dir][v] = f0[v] - A.Fc[v * nc8 + vc[1 + 2 * dir]];
+          Dp[dir][v] = A.Fc[v * nc8 + vc[2 + 2 * dir]] - f0[v];
+        }
+#pragma unroll
+      for (int c = 0; c < 8; c++) {
+        const int ix = c & 1, iy = (c >> 1) & 1, iz = c >> 2;
+#pragma unroll
+        for (int v = 0; v < 3; v++)
+          A.Fv[v * nv8 + 8 * j + c] = f0[v] + (ix ? Dp[0][v] : Dm[0][v]) * (-0.25 + ix * 0.5) +
+                                      (iy ? Dp[1][v] : Dm[1][v]) * (-0.25 + iy * 0.5) +
+                                      (iz ? Dp[2][v] : Dm[2][v]) * (-0.25 + iz * 0.5);
+      }
+    }
+    if (A.wv_inject) {
+#pragma unroll
+      for (int v = 0; v < 5; v++) {
+        const double q = Wc[v * nc8 + vc[0]];
+#pragma unroll
+        for (int c = 0; c < 8; c++) A.Wv[v * nv8 + 8 * j + c] = q;
+      }
+      continue;
+    }
     double q0[5], D[3][5];
 #pragma unroll
     for (int v = 0; v < 5; v++) q0[v] = Wc[v * nc8 + vc[0]];

@@ -196,13 +196,20 @@ struct MathF64 {
 
   // Face state toward face k from the slope along k's axis only (the other
   // axes enter the reference's sum with coefficient 0).
+  // g (optional): the gravity kick -f dt/2 of the face velocities, added after
+  // the pressure floor and before E and a (src/hydro_utils.c:1219-1226)
   static __device__ __forceinline__ void face_ax(const double q0[5], const double Dax[5], const double Wt[5], int k,
-                                                 double W[7], unsigned &st) {
+                                                 double W[7], unsigned &st, const double *g = nullptr) {
     const double f = (k & 1) ? 0.5 : -0.5;
 #pragma unroll
     for (int i = 0; i < 5; i++) W[i] = q0[i] + f * Dax[i] + Wt[i];
     W[4] = fmax(W[4], kPmin);
     if (W[0] < 0) st |= kStNegDensity;
+    if (g != nullptr) {
+      W[1] += g[0];
+      W[2] += g[1];
+      W[3] += g[2];
+    }
     face_finish(W);
   }
 

@@ -201,7 +201,7 @@ struct TileSmem {
 // the next tile's slot descriptors (next_tile >= 0: same level) are loaded
 // while this tile is reconstructed and solved, into the other descriptor
 // buffer; `cur`/`have` track which buffer holds the current tile's.
-template <class M, class G>
+template <class M, class G, bool GRAV>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
                                            const int next_tile, unsigned char *smem, const unsigned char *tab,
                                            unsigned &st, int &cur, bool &have, int &args_slot) {
@@ -376,6 +376,23 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     V::ld(sW, b, q[0], q[1], q[2], q[3]);
     q[4] = sWp[b];
   };
+  // gravity kick -f dt/2 (the reference's expression, in FP64) of box cell b:
+  // the force of the level's cell, or the interpolated force of an injected one
+  const bool grav = GRAV && A.F != nullptr;
+  auto kick_of = [&](int b, R g[3]) {
+    const int nb = b / G::kBox, bl = b - nb * G::kBox;
+    const int x2 = bl % G::XX, y2 = (bl / G::XX) % G::XY, z2 = bl / G::XS;
+    const uint32_t key = sKey[nb * G::kSlots + (x2 >> 1) + G::SX * ((y2 >> 1) + G::SY * (z2 >> 1))];
+    const long long off = 8LL * (key & 0x0FFFFFFFu) + ((x2 & 1) | ((y2 & 1) << 1) | ((z2 & 1) << 2));
+    const uint32_t kind = key >> 28;
+    const double *src = (kind == kKeyReal) ? A.F : ((kind == kKeyInterp) ? A.Fv : nullptr);
+    const long long stride = (kind == kKeyReal) ? N8 : 8 * A.nv;
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+      const double f = (key != kKeyNone && src != nullptr) ? __ldg(src + v * stride + off) : 0.;
+      g[v] = (R)(-f * 0.5 * A.dt);
+    }
+  };
 
   // ------------------------------------------------------------------ P1
   // Items < kThreads: brick cell tid (slopes and predictor, when it is a leaf of
@@ -422,6 +439,16 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     // X = W0 + Wt (FP32 path) or Wt (FP64 path, which adds W0 in the reference's order)
 #pragma unroll
     for (int v = 0; v < 5; v++) X[v] = F64 ? Wt[v] : q0[v] + Wt[v];
+    R gk[3] = {(R)0, (R)0, (R)0};
+    if (grav) {
+      kick_of(b, gk);
+      // FP32: the kick joins the predicted state, for the brick and the ring alike
+      if constexpr (!F64) {
+        X[1] += gk[0];
+        X[2] += gk[1];
+        X[3] += gk[2];
+      }
+    }
     if (w < kThreads) {
       // groups: D_x(d,u,v,w), D_y, D_z, X(d,u,v,w), (D_x.p, D_y.p, D_z.p, X.p)
 #pragma unroll
@@ -434,7 +461,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 #pragma unroll
       for (int v = 0; v < 5; v++) Dax[v] = (ax == 0) ? D[0][v] : ((ax == 1) ? D[1][v] : D[2][v]);
       if constexpr (F64) {
-        M::face_ax(q0, Dax, Wt, k, W, st);
+        M::face_ax(q0, Dax, Wt, k, W, st, grav ? gk : nullptr);
         V::st(sHS, r, W[0], W[1], W[2], W[3]);
         sHS[4 * NRING + r] = W[4];
       } else {
@@ -459,7 +486,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       R q0[5];
       V::ld(sM, 5 * kThreads + t, q0[0], q0[1], q0[2], q0[3]);
       q0[4] = sMp[t];
-      M::face_ax(q0, Dax, X, k, W, st);
+      if (grav) {
+        R gk[3];
+        kick_of(b, gk);
+        M::face_ax(q0, Dax, X, k, W, st, gk);
+      } else {
+        M::face_ax(q0, Dax, X, k, W, st);
+      }
     } else {
       M::face_px(X, Dax, k, W, st);
     }
@@ -745,6 +778,12 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       }
       Wout[4] = fmax(Wout[4], kPmin);
       if (isnan(Wout[1]) || isnan(Wout[4]) || isnan(Wout[0])) st |= kStNan;
+      // grav_correction (src/hydro_utils.c:2388-2444, PRIMITIVE): full-step kick of the
+      // leaf velocities after the update, before the next step's CFL term
+      if (A.gcorr && grav) {
+#pragma unroll
+        for (int v = 0; v < 3; v++) Wout[1 + v] += (-__ldg(A.F + v * N8 + gi) * A.dt);
+      }
 
       // fine -> coarse correction into unsplit coarser neighbours (src/hydro_utils.c:3206-3295)
 #pragma unroll
@@ -814,7 +853,7 @@ static_assert(4 * (TileSmem<MathF32, GeomA>::bytes + 1024) <= 228 * 1024, "4 FP3
 static_assert(2 * (TileSmem<MathF32, GeomB>::bytes + 1024) <= 228 * 1024, "2 FP32 2x2x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF64, GeomA>::bytes + 1024) <= 228 * 1024, "2 FP64 4x4x2 CTAs per SM");
 
-template <class M, unsigned SHAPES>
+template <class M, unsigned SHAPES, bool GRAV>
 __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
@@ -838,14 +877,14 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch
     }
     const LevelArgs *gA = Bt.lv + slot;
     if constexpr (SHAPES == 1u) {
-      level_tile<M, GeomA>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+      level_tile<M, GeomA, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
     } else if constexpr (SHAPES == 2u) {
-      level_tile<M, GeomB>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
+      level_tile<M, GeomB, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
     } else {
       if (gA->shape == 0)
-        level_tile<M, GeomA>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+        level_tile<M, GeomA, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
       else
-        level_tile<M, GeomB>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
+        level_tile<M, GeomB, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
     }
     __syncthreads();
   }
@@ -861,10 +900,10 @@ namespace emma {
 
 // Launch of a work list on a persistent grid of ctas_per_sm CTAs per SM (0 or
 // above the occupancy limit: the limit), so that every CTA is co-resident.
-template <class M, unsigned SHAPES>
+template <class M, unsigned SHAPES, bool GRAV>
 cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cudaStream_t s, int *occupancy) {
   static int occ = 0;
-  auto k = level_batch_kernel<M, SHAPES>;
+  auto k = level_batch_kernel<M, SHAPES, GRAV>;
   constexpr size_t bytes = level_smem_bytes<M>(SHAPES);
   if (occ == 0) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -886,9 +925,12 @@ template <class M>
 cudaError_t launch_level_any(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
                              int *occupancy) {
   switch (shapes) {
-    case 1u: return launch_level_shapes<M, 1u>(a, nsm, ctas_per_sm, s, occupancy);
-    case 2u: return launch_level_shapes<M, 2u>(a, nsm, ctas_per_sm, s, occupancy);
-    case 3u: return launch_level_shapes<M, 3u>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u: return launch_level_shapes<M, 1u, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u: return launch_level_shapes<M, 2u, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u: return launch_level_shapes<M, 3u, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u | kLaunchGrav: return launch_level_shapes<M, 1u, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u | kLaunchGrav: return launch_level_shapes<M, 2u, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u | kLaunchGrav: return launch_level_shapes<M, 3u, true>(a, nsm, ctas_per_sm, s, occupancy);
     default: return cudaErrorInvalidValue;
   }
 }

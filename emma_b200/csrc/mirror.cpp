@@ -368,11 +368,14 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
     if (corrected[i]) lv.inj_cells.push_back((int32_t)i);
   for (uint32_t key : lv.keys)
     if (key != kKeyNone && (key >> 28) == kKeyInj) lv.reads_coarse = true;
-  if (lv.reads_coarse && H.trans != 0) {
+  if (lv.reads_coarse && (H.trans != 0 || H.grav != 0)) {
     // The reference's transmissive build (-DHYDROTEST) fills a coarser neighbour
     // by limited-slope interpolation (coarse2fine_hydro2, src/hydro_utils.c:311)
     // instead of injection: every injected slot becomes an interpolated one, with
-    // the coarse cell and the 6 cells its slopes are taken from.
+    // the coarse cell and the 6 cells its slopes are taken from.  A gravity build
+    // keeps the injected field but spreads the coarse cell's force over the 8
+    // sub-cells from the same 6 neighbours (coarse2fine_forcelin,
+    // src/poisson_utils.c:315), which dereferences every neighbour: none may miss.
     const HostLevel &lc = H.lev[L - 1];
     std::unordered_map<uint32_t, int> jof;
     for (uint32_t &key : lv.keys) {
@@ -388,6 +391,7 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
         int nb[6];
         int wm = -1, wp = -1;  // like the reference, a missing neighbour keeps the previous one
         for (int dir = 0; dir < 3; dir++) {
+          if (H.grav) wm = wp = -1;
           for (int side = 0; side < 2; side++) {
             const int k = 2 * dir + side;
             int &w = side ? wp : wm;
@@ -423,8 +427,13 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
 int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string &err);
 
 int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int trans, int plan_lo, int plan_hi,
-                    HostTree &H, std::string &err, const int *shapes) {
+                    HostTree &H, std::string &err, const int *shapes, int grav) {
   H = HostTree();
+  if (grav && trans) {
+    err = "gravity coupling with transmissive boundaries is not supported";
+    return EMMA_ST_ARG;
+  }
+  H.grav = grav ? 1 : 0;
   H.lcoarse = lcoarse;
   H.lmax = lmax;
   H.rank = rank;

@@ -19,14 +19,15 @@ struct HostLevel {
   std::vector<uint32_t> keys;         // kSlots slot keys per tile
   std::vector<int32_t> inj_cells;     // level L-1 cells that receive fine->coarse corrections
   bool reads_coarse = false;          // some tile stages an injected level L-1 cell
-  std::vector<int32_t> interp;        // transmissive builds: per interpolated level L-1 cell,
-                                      // the cell and its 6 slope neighbours (7 entries)
+  std::vector<int32_t> interp;        // transmissive or gravity builds: per interpolated level L-1
+                                      // cell, the cell and its 6 slope neighbours (7 entries)
   int shape = 0;                      // brick shape of the plan (kShapes)
   std::vector<int32_t> pos;           // per oct: integer position on the level grid (x,y,z)
 };
 
 struct HostTree {
   int lcoarse = 0, lmax = 0, rank = 0, trans = 0;
+  int grav = 0;  // gravity coupling: injected coarser cells carry interpolated forces
   std::vector<HostLevel> lev;  // indexed by level (0..lmax)
 };
 
@@ -34,9 +35,11 @@ struct HostTree {
 // plan_lo..plan_hi (a plan of level L needs the mirror of L-1 when L-1 >=
 // lcoarse).  Returns 0 on success, else an EMMA_ST_* bit with a message in `err`.
 // shapes (optional, indexed by level): brick shape of each plan, -1 = the
-// cheaper by tile count x tile cost.
+// cheaper by tile count x tile cost.  grav: gravity-coupled build (every
+// injected coarser cell gets an interpolation entry for its force; not
+// combined with transmissive boundaries).
 int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int trans, int plan_lo, int plan_hi,
-                    HostTree &H, std::string &err, const int *shapes = nullptr);
+                    HostTree &H, std::string &err, const int *shapes = nullptr, int grav = 0);
 
 // Re-plan level L of a built tree with brick shape `shape` (the autotuner's
 // candidates); validates the new plan.

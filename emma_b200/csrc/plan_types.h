@@ -37,6 +37,9 @@ struct BrickShape {
   constexpr int tile_slots() const { return nb * slots(); }
 };
 constexpr int kNumShapes = 2;
+// Launch flag beside the shape bits of a level-kernel launch: the gravity-coupled
+// variant (levels with accelerations); the plain variant has no gravity code.
+constexpr unsigned kLaunchGrav = 4u;
 constexpr BrickShape kShapes[kNumShapes] = {{4, 4, 2, 1}, {2, 2, 2, 4}};
 static_assert(kShapes[0].nb * 8 * kShapes[0].octs() == kThreads, "one thread per brick cell");
 static_assert(kShapes[1].nb * 8 * kShapes[1].octs() == kThreads, "one thread per brick cell");
@@ -80,6 +83,13 @@ struct LevelArgs {
   int wait_slot;      // level whose tiles must all be updated before this level's
                       // update phase starts (batched launches), -1 for none
   long long leaf;     // leaf cells (cell-updates of one substep)
+  // gravity coupling (-DWGRAV), all null/0 without it
+  const double *F;    // acceleration of the level's cells: planes fx,fy,fz of 8*noct
+  const double *Fc;   // acceleration of level L-1 (read by the interpolation kernel)
+  double *Fv;         // accelerations of the interpolated coarser cells: planes of 8 * nv
+  int gcorr;          // apply grav_correction (src/hydro_utils.c:2388-2444) to the new state
+  int wv_inject;      // the interpolation list fills Wv by injection (gravity build), not by
+                      // limited-slope interpolation (transmissive build)
 };
 
 // A launch of the level kernel: a list of (level slot, tile) work items,

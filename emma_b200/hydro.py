@@ -12,27 +12,31 @@ import numpy as np
 from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
-def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0):
+def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0, gravity=False):
     """tile_octs: 0 = brick shape autotuned per level at upload, 32 = 4x4x2-oct
-    bricks, 8 = 2x2x2-oct bricks (four per tile)."""
+    bricks, 8 = 2x2x2-oct bricks (four per tile).  gravity: the -DWGRAV coupling
+    (forces from ResidentHydro.set_force)."""
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
     o.use_graph = 1 if use_graph else 0
     o.tile_octs = tile_octs
+    o.gravity = 1 if gravity else 0
     return o
 
 
 class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
-    def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0):
+    def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0,
+                 gravity=False):
         self.tree = tree
+        self.gravity = gravity
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
         self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
         self.precision = precision
         L = lib()
-        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs)
+        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
         check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
         L.emma_hydro_clear_status()
@@ -44,12 +48,14 @@ class ResidentHydro:
         """Switch between CUDA-graph coarse steps and the host-driven schedule
         (the resident tree and its tuned plans stay)."""
         self.use_graph = use_graph
-        o = options(self.precision, self.trans, self.cfl, use_graph=use_graph, tile_octs=self.tile_octs)
+        o = options(self.precision, self.trans, self.cfl, use_graph=use_graph, tile_octs=self.tile_octs,
+                    gravity=self.gravity)
         check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def set_precision(self, precision):
         self.precision = precision
-        o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs)
+        o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
+                    gravity=self.gravity)
         check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):
@@ -75,6 +81,11 @@ class ResidentHydro:
     def set_state(self, level, st):
         st = np.ascontiguousarray(st, dtype=np.float64)
         check(lib().emma_hydro_set_level_state(level, ptr(st)), "set_level_state")
+
+    def set_force(self, level, fx, fy, fz):
+        """Gravitational acceleration of the level's cells (gravity=True uploads)."""
+        f = np.ascontiguousarray(np.stack([fx, fy, fz]), dtype=np.float64)
+        check(lib().emma_hydro_set_level_force(level, ptr(f)), "set_level_force")
 
     def comptstep(self, level):
         dt = ctypes.c_double()

@@ -62,6 +62,12 @@ struct EmmaHydroOptions {
   int tile_octs;        /* octs per brick: 0 = autotuned per level, 32 = 4x4x2, 8 = 2x2x2 */
   int device;           /* CUDA device ordinal */
   int use_graph;        /* coarse steps as a captured CUDA graph with a device-side schedule */
+  int gravity;          /* gravity coupling of the reference's -DWGRAV build (resident mode):
+                           half-step kick -f dt/2 of the MUSCL face velocities
+                           (src/hydro_utils.c:1219-1226) and grav_correction after each
+                           level update (src/hydro_utils.c:2388, called at
+                           src/advanceamr.c:999); the accelerations f come from
+                           emma_hydro_set_level_force.  Not with trans_flags. */
 };
 void emma_hydro_default_options(struct EmmaHydroOptions *opt);
 
@@ -136,6 +142,11 @@ int emma_hydro_set_time(double tsim, const double *adt);
 int emma_hydro_level_noct(int level);
 int emma_hydro_get_level_state(int level, double *host_out);
 int emma_hydro_set_level_state(int level, const double *host_in);
+/* Gravity builds: the gravitational acceleration of the level's cells, 3 planes
+ * (fx, fy, fz) of 8*noct doubles in list order, from host or device memory
+ * (the reference's cell f[3], src/prototypes.h:841); zero after an upload. */
+int emma_hydro_set_level_force(int level, const double *host_f);
+int emma_hydro_set_level_force_device(int level, const double *dev_f);
 /* Leaf cell count of a level (cells advanced per level substep). */
 long long emma_hydro_level_leaf_cells(int level);
 /* Cell-updates performed since the last reset (leaf cells x level substeps). */

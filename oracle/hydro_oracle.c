@@ -809,3 +809,155 @@ double orc_run(void **firstoct, int lcoarse, int lmax, int nsteps, double dt_par
   if (err) *err = S.err;
   return tsim;
 }
+
+#ifdef ORC_WGRAV
+/* ---------------------------------------------- plain-layout tree -> -DWGRAV copy
+ * Test helper: the product library's trees use the default (no WGRAV) layout;
+ * this copies one, pointers remapped, into the gravity layout so the gravity
+ * restatement can run on the same octs in the same list order.  Forces start
+ * at zero. */
+typedef struct pCell {
+  struct pOct *child;
+  double marked;
+  int idx;
+  oW field;
+  oW fieldnew;
+} pCell;
+typedef struct pOct {
+  pCell cell[8];
+  pCell *nei[6];
+  pCell *parent;
+  struct pOct *next, *prev, *nexthash;
+  double x, y, z;
+  int cpu;
+  int level;
+} pOct;
+_Static_assert(sizeof(pOct) == 1200, "plain OCT layout");
+
+typedef struct {
+  oOct *octs;
+  const pOct **src;  /* sorted by address, with the copy index in idx */
+  long *idx;
+  long n;
+  oCell root;
+  oOct **first;
+  int lmax;
+} GravClone;
+
+static GravClone *g_sort_ctx;
+static int cmp_src(const void *a, const void *b) {
+  const pOct *x = g_sort_ctx->src[*(const long *)a], *y = g_sort_ctx->src[*(const long *)b];
+  return (x > y) - (x < y);
+}
+
+static oOct *clone_oct(GravClone *C, const pOct *o) {
+  long lo = 0, hi = C->n - 1;
+  if (o == NULL) return NULL;
+  while (lo <= hi) {
+    long m = (lo + hi) / 2;
+    const pOct *x = C->src[C->idx[m]];
+    if (x == o) return &C->octs[C->idx[m]];
+    if (x < o) lo = m + 1;
+    else hi = m - 1;
+  }
+  return NULL;
+}
+
+/* A cell pointer of the source tree: a cell of a copied oct, or the stand-in
+ * root cell (the parent-level cell whose child is the level-1 oct). */
+static oCell *clone_cell(GravClone *C, const pCell *c, const pOct *top, int *err) {
+  oOct *o;
+  if (c == NULL) return NULL;
+  if (c->child == top && top != NULL) return &C->root;
+  o = clone_oct(C, (const pOct *)((const char *)c - (size_t)c->idx * sizeof(pCell)));
+  if (o == NULL) { *err = 1; return NULL; }
+  return &o->cell[c->idx];
+}
+
+void *orc_grav_clone(void **src_first_v, int lmax) {
+  const pOct **src_first = (const pOct **)src_first_v;
+  GravClone *C = (GravClone *)calloc(1, sizeof(GravClone));
+  const pOct *o, *top = src_first[0];
+  long n = 0, i;
+  int l, c, k, err = 0;
+  C->lmax = lmax;
+  for (l = 1; l <= lmax; l++)
+    for (o = src_first[l - 1]; o != NULL; o = o->next) n++;
+  C->n = n;
+  C->octs = (oOct *)calloc((size_t)(n > 0 ? n : 1), sizeof(oOct));
+  C->src = (const pOct **)malloc(sizeof(pOct *) * (size_t)(n > 0 ? n : 1));
+  C->idx = (long *)malloc(sizeof(long) * (size_t)(n > 0 ? n : 1));
+  C->first = (oOct **)calloc((size_t)lmax, sizeof(oOct *));
+  n = 0;
+  for (l = 1; l <= lmax; l++)
+    for (o = src_first[l - 1]; o != NULL; o = o->next) { C->src[n] = o; C->idx[n] = n; n++; }
+  g_sort_ctx = C;
+  qsort(C->idx, (size_t)n, sizeof(long), cmp_src);
+  C->root.child = clone_oct(C, top);
+  for (i = 0; i < n; i++) {
+    const pOct *s = C->src[i];
+    oOct *d = &C->octs[i];
+    for (c = 0; c < 8; c++) {
+      d->cell[c].child = clone_oct(C, s->cell[c].child);
+      d->cell[c].marked = s->cell[c].marked;
+      d->cell[c].idx = s->cell[c].idx;
+      d->cell[c].field = s->cell[c].field;
+      d->cell[c].fieldnew = s->cell[c].fieldnew;
+    }
+    for (k = 0; k < 6; k++) d->nei[k] = clone_cell(C, s->nei[k], top, &err);
+    d->parent = clone_cell(C, s->parent, top, &err);
+    d->next = clone_oct(C, s->next);
+    d->prev = clone_oct(C, s->prev);
+    d->x = s->x; d->y = s->y; d->z = s->z;
+    d->cpu = s->cpu;
+    d->level = s->level;
+  }
+  for (l = 1; l <= lmax; l++) C->first[l - 1] = clone_oct(C, src_first[l - 1]);
+  if (err) {
+    orc_grav_free(C);
+    return NULL;
+  }
+  return C;
+}
+
+void **orc_grav_first(void *h) { return (void **)((GravClone *)h)->first; }
+
+void orc_grav_set_force(void *h, int level, const double *fx, const double *fy, const double *fz) {
+  GravClone *C = (GravClone *)h;
+  oOct *o;
+  long i = 0;
+  int c;
+  for (o = C->first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) {
+      o->cell[c].f[0] = fx[8 * i + c];
+      o->cell[c].f[1] = fy[8 * i + c];
+      o->cell[c].f[2] = fz[8 * i + c];
+    }
+}
+
+/* d,u,v,w,p,a,E of field (which=0) or fieldnew (which=1) as 7 planes, list order */
+void orc_grav_get_field(void *h, int level, int which, double *out) {
+  GravClone *C = (GravClone *)h;
+  oOct *o;
+  long i = 0, n = 0;
+  int c;
+  for (o = C->first[level - 1]; o != NULL; o = o->next) n++;
+  for (o = C->first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) {
+      const oW *W = which ? &o->cell[c].fieldnew : &o->cell[c].field;
+      long k = 8 * i + c;
+      out[k] = W->d; out[8 * n + k] = W->u; out[16 * n + k] = W->v; out[24 * n + k] = W->w;
+      out[32 * n + k] = W->p; out[40 * n + k] = W->a; out[48 * n + k] = W->E;
+    }
+}
+
+void orc_grav_free(void *h) {
+  GravClone *C = (GravClone *)h;
+  if (C == NULL) return;
+  free(C->octs);
+  free(C->src);
+  free(C->idx);
+  free(C->first);
+  free(C);
+}
+#endif

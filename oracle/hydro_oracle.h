@@ -43,6 +43,14 @@ double orc_comptstep_hydro(void **firstoct, int level, double cfl);
  * half-step gravity kick and the schedule calls grav_correction after each
  * HydroSolver (src/advanceamr.c:999). */
 int orc_grav_correction(void **firstoct, int level, double dt);
+/* Gravity build: copy of a default-layout tree (levels 1..lmax, pointers
+ * remapped, forces zero) in the -DWGRAV layout; NULL if a pointer leads out of
+ * the tree.  orc_grav_first gives its firstoct array. */
+void *orc_grav_clone(void **src_firstoct, int lmax);
+void **orc_grav_first(void *clone);
+void orc_grav_set_force(void *clone, int level, const double *fx, const double *fy, const double *fz);
+void orc_grav_get_field(void *clone, int level, int which, double *out);
+void orc_grav_free(void *clone);
 /* Hydro-only Advance_level schedule; returns tsim after `nsteps` coarse steps.
  * adt has lmax entries (in/out), like the reference's adt array. */
 double orc_run(void **firstoct, int lcoarse, int lmax, int nsteps, double dt_param,

@@ -91,6 +91,51 @@ class Restatement:
         self.L.orc_reset_counters()
 
 
+class GravClone:
+    """Copy of a default-layout tree in the -DWGRAV layout (liboracle_grav.so), for
+    running the gravity restatement on the same octs and list order."""
+
+    def __init__(self, tree):
+        R = Restatement(grav=True)
+        L = R.L
+        L.orc_grav_clone.restype = c_void_p
+        L.orc_grav_clone.argtypes = [c_void_p, c_int]
+        L.orc_grav_first.restype = c_void_p
+        L.orc_grav_first.argtypes = [c_void_p]
+        L.orc_grav_set_force.argtypes = [c_void_p, c_int, c_void_p, c_void_p, c_void_p]
+        L.orc_grav_get_field.argtypes = [c_void_p, c_int, c_int, c_void_p]
+        L.orc_grav_free.argtypes = [c_void_p]
+        self.R, self.L, self.src = R, L, tree
+        self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
+        self.h = L.orc_grav_clone(tree.firstoct, tree.lmax)
+        if not self.h:
+            raise RuntimeError("tree copy into the gravity layout failed")
+
+    @property
+    def firstoct(self):
+        return self.L.orc_grav_first(self.h)
+
+    def set_force(self, level, fx, fy, fz):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fx, fy, fz)]
+        self.L.orc_grav_set_force(self.h, level, *[_p(a) for a in arrs])
+
+    def get_fields(self, level, which=0):
+        n = self.src.noct(level)
+        out = np.zeros((7, 8 * n))
+        if n:
+            self.L.orc_grav_get_field(self.h, level, which, _p(out))
+        return out
+
+    def run(self, nsteps, cfl, nsub=2, dt_param=1e9, time_max=1e9, tsim0=0.0):
+        return self.R.run(self.firstoct, self.lcoarse, self.lmax, nsteps, cfl, nsub=nsub, dt_param=dt_param,
+                          time_max=time_max, tsim0=tsim0)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.orc_grav_free(self.h)
+            self.h = None
+
+
 def ref_available(tx=False, grav=False):
     return os.path.exists(REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
 

@@ -111,6 +111,49 @@ def test_pin_gravity_amr():
     ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, grav=True)
 
 
+def _amr_tree(base, lmax, radii, seed=12345):
+    t = OctTree(base, lmax)
+    for i, r in enumerate(radii):
+        t.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
+    random_fields(t, range(base, lmax + 1), seed)
+    return t
+
+
+def test_gravity_clone_without_force_is_plain_hydro():
+    """The gravity restatement on a layout copy with zero force reproduces the
+    plain restatement bit for bit (the copy keeps octs, links and list order)."""
+    t = _amr_tree(4, 6, (0.3, 0.15))
+    gc = oracle.GravClone(t)
+    t1, adt1, e1 = gc.run(2, 0.8)
+    t2, adt2, e2 = oracle.Restatement().run(t.firstoct, 4, 6, 2, 0.8)
+    assert e1 == e2 == 0 and t1 == t2 and np.array_equal(adt1, adt2)
+    for l in range(4, 7):
+        assert np.array_equal(gc.get_fields(l), t.get_fields(l)), l
+
+
+@needs_ref_grav
+def test_gravity_clone_matches_reference_tree():
+    """Gravity restatement on a copy of the library's tree == the reference's
+    -DWGRAV hydro on its own tree, same configuration, forces and fields."""
+    base, lmax, radii = 4, 6, (0.3, 0.15)
+    t = _amr_tree(base, lmax, radii)
+    ref = oracle.RefTree(base, lmax, ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)), grav=True)
+    for i, r in enumerate(radii):
+        ref.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
+    random_fields(ref, range(base, lmax + 1))
+    random_forces(ref, range(base, lmax + 1))
+    gc = oracle.GravClone(t)
+    rng = np.random.default_rng(54321)
+    for l in range(base, lmax + 1):
+        n8 = 8 * t.noct(l)
+        gc.set_force(l, *(rng.uniform(-0.5, 0.5, n8) for _ in range(3)))
+    t1, adt1 = ref.run(2)
+    t2, adt2, err = gc.run(2, 0.8)
+    assert err == 0 and t1 == t2 and np.array_equal(adt1, adt2)
+    for l in range(base, lmax + 1):
+        assert np.array_equal(ref.get_fields(l), gc.get_fields(l)), l
+
+
 def _golden_cases():
     return sorted(f for f in os.listdir(GOLDEN) if f.endswith(".npz")) if os.path.isdir(GOLDEN) else []
 
