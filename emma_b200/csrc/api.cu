@@ -24,7 +24,8 @@ cudaError_t launch_level_f32(const BatchArgs &a, unsigned shapes, int nsm, int c
                              int *occupancy);
 cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *gate, unsigned long long *out, int nsm,
                        cudaStream_t s);
-cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s);
+cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s,
+                          bool grav);
 }  // namespace emma
 
 using namespace emma;
@@ -280,7 +281,8 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     d.nv = (long long)h.interp.size() / 7;
     if (d.nv > 0) {
       if (!upload_vec(&d.vcell, h.interp)) return false;
-      if (!ck(cudaMalloc(&d.Wv, sizeof(double) * 5 * 8 * (size_t)d.nv), "cudaMalloc Wv")) return false;
+      // transmissive builds interpolate the states, gravity builds the forces
+      if (!H.grav && !ck(cudaMalloc(&d.Wv, sizeof(double) * 5 * 8 * (size_t)d.nv), "cudaMalloc Wv")) return false;
       if (H.grav && !ck(cudaMalloc(&d.Fv, sizeof(double) * 3 * 8 * (size_t)d.nv), "cudaMalloc Fv")) return false;
     }
     if (H.grav) {  // accelerations start at zero until the caller sets them
@@ -536,7 +538,7 @@ bool emit_level(int L, int nsub) {
     k_sub_dt<<<1, 1, 0, g.stream>>>(S, L);
     if (has_fine && !emit_level(L + 1, nsub)) return false;
     k_sub_prelaunch<<<1, 1, 0, g.stream>>>(S, t.d_lv, L, has_fine ? 1 : 0);
-    if (!ck(launch_interp(t.d_lv, L, d.nv, gate, g.nsm, g.stream), "interpolation launch")) return false;
+    if (!ck(launch_interp(t.d_lv, L, d.nv, gate, g.nsm, g.stream, t.host.grav), "interpolation launch")) return false;
     if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf, 1u << d.shape, d.ctas, true)) return false;
     k_sub_end<<<1, 1, 0, g.stream>>>(S, t.d_lv, L);
     if (!ck(cudaGetLastError(), "schedule kernel")) return false;
@@ -561,7 +563,8 @@ bool emit_coarse_step(int nsub) {
     }
     k_batch_begin<<<1, 1, 0, g.stream>>>(S, t.d_lv, g.d_done);
     for (int L = lc; L <= lf; L++)
-      if (!ck(launch_interp(t.d_lv, L, t.lev[L].nv, nullptr, g.nsm, g.stream), "interpolation launch")) return false;
+      if (!ck(launch_interp(t.d_lv, L, t.lev[L].nv, nullptr, g.nsm, g.stream, t.host.grav), "interpolation launch"))
+        return false;
     long long cells = 0;
     unsigned shapes = 0;
     int ctas = 0, most = -1;
@@ -821,7 +824,7 @@ bool autotune_tree(Tree &t, int shape_req) {
         Fv = nullptr;
         if (!upload_vec(&tiles, alt.tiles) || !upload_vec(&keys, alt.keys) || !upload_vec(&work, wl) ||
             (nv > 0 && (!upload_vec(&vcell, alt.interp) ||
-                        !ck(cudaMalloc(&Wv, sizeof(double) * 5 * 8 * (size_t)nv), "cudaMalloc Wv"))) ||
+                        (!t.host.grav && !ck(cudaMalloc(&Wv, sizeof(double) * 5 * 8 * (size_t)nv), "cudaMalloc Wv")))) ||
             (nv > 0 && t.host.grav && !ck(cudaMalloc(&Fv, sizeof(double) * 3 * 8 * (size_t)nv), "cudaMalloc Fv"))) {
           ok = false;
           break;
@@ -829,7 +832,7 @@ bool autotune_tree(Tree &t, int shape_req) {
       }
       ok = bind_plan(t.d_lv + L, tiles, keys, s, ntiles, Wv, vcell, nv, Fv);
       k_bind_level<<<1, 1, 0, g.stream>>>(t.d_lv, L, t.lcoarse, t.lmax, 0.);
-      if (ok) ok = ck(launch_interp(t.d_lv, L, nv, nullptr, g.nsm, g.stream), "interpolation launch");
+      if (ok) ok = ck(launch_interp(t.d_lv, L, nv, nullptr, g.nsm, g.stream, t.host.grav), "interpolation launch");
       int occ = 0;
       BatchArgs probe{};
       if (ok)
@@ -1108,7 +1111,7 @@ int emma_hydro_advance_level(int level, double dt) {
   if (d.noct == 0) return 0;
   k_bind_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, g.res.lcoarse, g.res.lmax, dt);
   CK(cudaGetLastError());
-  CK(launch_interp(g.res.d_lv, level, d.nv, nullptr, g.nsm, g.stream));
+  CK(launch_interp(g.res.d_lv, level, d.nv, nullptr, g.nsm, g.stream, g.res.host.grav));
   if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return EMMA_ST_CUDA;
   k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
   CK(cudaGetLastError());
@@ -1484,7 +1487,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   a.leaf = d.leaf;
   k_set_args<<<1, 1, 0, g.stream>>>(T.d_lv, level, a);
   if (!ck(cudaGetLastError(), "k_set_args")) return 0;
-  if (!ck(launch_interp(T.d_lv, level, d.nv, nullptr, g.nsm, g.stream), "interpolation launch")) return 0;
+  if (!ck(launch_interp(T.d_lv, level, d.nv, nullptr, g.nsm, g.stream, false), "interpolation launch")) return 0;
   if (!launch_batch(T.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return 0;
   // device status and the corrections first, then the level's new state range by
   // range: each host thread waits for its own range and unpacks it into fieldnew

@@ -54,11 +54,6 @@ __device__ __forceinline__ double minmod_w(double m, double p) {
   return fmin(fmin(0., fmax(m, p)), fmax(m, p));
 }
 
-// Gravity builds (A.wv_inject): the listed cells keep the injected state (the
-// default gather, src/hydro_utils.c:2912-2944) and their force is spread by
-// coarse2fine_forcelin (src/poisson_utils.c:315-425): unlimited one-sided
-// differences, f = f0 + Dx ox + Dy oy + Dz oz with D = f0 - f(-nei) on the -
-// side of an axis and f(+nei) - f0 on the + side.
 __global__ void interp_coarse_kernel(const LevelArgs *lv, int slot, const int *gate) {
   if (gate != nullptr && *gate == 0) return;
   const LevelArgs &A = lv[slot];
@@ -67,36 +62,6 @@ __global__ void interp_coarse_kernel(const LevelArgs *lv, int slot, const int *g
   const long long nc8 = A.nc8, nv = A.nv, nv8 = 8 * A.nv;
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nv; j += (long long)gridDim.x * blockDim.x) {
     const int *vc = A.vcell + 7 * j;
-    if (A.Fv != nullptr && A.Fc != nullptr) {
-      double f0[3], Dm[3][3], Dp[3][3];
-#pragma unroll
-      for (int v = 0; v < 3; v++) f0[v] = A.Fc[v * nc8 + vc[0]];
-#pragma unroll
-      for (int dir = 0; dir < 3; dir++)
-#pragma unroll
-        for (int v = 0; v < 3; v++) {
-          Dm[dir][v] = f0[v] - A.Fc[v * nc8 + vc[1 + 2 * dir]];
-          Dp[dir][v] = A.Fc[v * nc8 + vc[2 + 2 * dir]] - f0[v];
-        }
-#pragma unroll
-      for (int c = 0; c < 8; c++) {
-        const int ix = c & 1, iy = (c >> 1) & 1, iz = c >> 2;
-#pragma unroll
-        for (int v = 0; v < 3; v++)
-          A.Fv[v * nv8 + 8 * j + c] = f0[v] + (ix ? Dp[0][v] : Dm[0][v]) * (-0.25 + ix * 0.5) +
-                                      (iy ? Dp[1][v] : Dm[1][v]) * (-0.25 + iy * 0.5) +
-                                      (iz ? Dp[2][v] : Dm[2][v]) * (-0.25 + iz * 0.5);
-      }
-    }
-    if (A.wv_inject) {
-#pragma unroll
-      for (int v = 0; v < 5; v++) {
-        const double q = Wc[v * nc8 + vc[0]];
-#pragma unroll
-        for (int c = 0; c < 8; c++) A.Wv[v * nv8 + 8 * j + c] = q;
-      }
-      continue;
-    }
     double q0[5], D[3][5];
 #pragma unroll
     for (int v = 0; v < 5; v++) q0[v] = Wc[v * nc8 + vc[0]];
@@ -115,8 +80,44 @@ __global__ void interp_coarse_kernel(const LevelArgs *lv, int slot, const int *g
   }
 }
 
-cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s) {
+// Gravity builds: the force of each listed coarse cell spread over its 8
+// sub-cells by coarse2fine_forcelin (src/poisson_utils.c:315-425): unlimited
+// one-sided differences, f = f0 + Dx ox + Dy oy + Dz oz with D = f0 - f(-nei)
+// for a sub-cell on the - side of an axis and f(+nei) - f0 on the + side,
+// o = -1/4 or +1/4 (built with -fmad=false).  One thread per sub-cell.
+__global__ void force_interp_kernel(const LevelArgs *lv, int slot, const int *gate) {
+  if (gate != nullptr && *gate == 0) return;
+  const LevelArgs &A = lv[slot];
+  if (A.Fc == nullptr || A.Fv == nullptr) return;
+  const long long nc8 = A.nc8, nv8 = 8 * A.nv;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv8; i += (long long)gridDim.x * blockDim.x) {
+    const long long j = i >> 3;
+    const int c = (int)(i & 7), ix = c & 1, iy = (c >> 1) & 1, iz = c >> 2;
+    const int *vc = A.vcell + 7 * j;
+    const int c0 = vc[0], nx = vc[1 + ix], ny = vc[3 + iy], nz = vc[5 + iz];
+#pragma unroll
+    for (int v = 0; v < 3; v++) {
+      const double *F = A.Fc + v * nc8;
+      const double f0 = F[c0];
+      const double dx = ix ? F[nx] - f0 : f0 - F[nx];
+      const double dy = iy ? F[ny] - f0 : f0 - F[ny];
+      const double dz = iz ? F[nz] - f0 : f0 - F[nz];
+      A.Fv[v * nv8 + i] = f0 + dx * (-0.25 + ix * 0.5) + dy * (-0.25 + iy * 0.5) + dz * (-0.25 + iz * 0.5);
+    }
+  }
+}
+
+// grav: the level belongs to a gravity build (forces interpolated, states injected),
+// else a transmissive build (states interpolated)
+cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s,
+                          bool grav) {
   if (nv <= 0) return cudaSuccess;
+  if (grav) {
+    long long blocks = (8 * nv + 255) / 256;
+    if (blocks > 8LL * nsm) blocks = 8LL * nsm;
+    force_interp_kernel<<<(unsigned)blocks, 256, 0, s>>>(lv, slot, gate);
+    return cudaGetLastError();
+  }
   long long blocks = (nv + 127) / 128;
   if (blocks > 4LL * nsm) blocks = 4LL * nsm;
   interp_coarse_kernel<<<(unsigned)blocks, 128, 0, s>>>(lv, slot, gate);

@@ -194,6 +194,10 @@ struct TileSmem {
   static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
   static constexpr size_t bytes = off_end;
   static_assert(off_F1 + sizeof(R) * NF <= off_M, "face fluxes must fit in the staged box");
+  // FP64 gravity kicks of the brick cells during P2/P3: R [3][kThreads] at the end of
+  // the staged box, after the face fluxes
+  static constexpr size_t off_K = off_M - sizeof(R) * 3 * kThreads;
+  static_assert(!kF64 || off_K >= off_F1 + sizeof(R) * NF, "FP64 kicks must not overlap the face fluxes");
 };
 
 // One tile.  Software pipeline over the tiles of a CTA: the level's arguments
@@ -269,7 +273,15 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
           st |= kStTree;  // plan/launch mismatch: never read through a null level
         }
       } else if (kind == kKeyInterp) {
-        if (A.Wv != nullptr) {  // 8 interpolated sub-cells, laid out like an oct
+        if (A.wv_inject) {  // gravity build: the coarse cell injected (its force is interpolated)
+          cmk = 1;
+          if (A.Wc != nullptr && A.vcell != nullptr) {
+            ob = __ldg(A.vcell + 7 * (size_t)idx);
+            sf |= kFInj;
+          } else {
+            st |= kStTree;
+          }
+        } else if (A.Wv != nullptr) {  // 8 interpolated sub-cells, laid out like an oct
           ob = 8 * (int)idx;
           sf |= kFInj | kFInterp;
         } else {
@@ -473,6 +485,19 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   }
   __syncthreads();
   if (pre) nraw = split_of(nkey);
+  // FP64 gravity: the kick of each brick cell once, for its six face states (the
+  // box is dead after P1; the kicks sit after the face fluxes)
+  R *sK = reinterpret_cast<R *>(smem + SM::off_K);
+  if constexpr (F64 && GRAV) {
+    if (grav) {
+      R gk[3];
+      kick_of(tb, gk);
+      sK[tid] = gk[0];
+      sK[kThreads + tid] = gk[1];
+      sK[2 * kThreads + tid] = gk[2];
+      __syncthreads();
+    }
+  }
 
   // face state k of brick cell t (index into the tile's cells, box cell b)
   auto brick_face = [&](int t, int b, int k, R W[7]) {
@@ -487,8 +512,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       V::ld(sM, 5 * kThreads + t, q0[0], q0[1], q0[2], q0[3]);
       q0[4] = sMp[t];
       if (grav) {
-        R gk[3];
-        kick_of(b, gk);
+        const R gk[3] = {sK[t], sK[kThreads + t], sK[2 * kThreads + t]};
         M::face_ax(q0, Dax, X, k, W, st, gk);
       } else {
         M::face_ax(q0, Dax, X, k, W, st);
