@@ -10,8 +10,10 @@ import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libemmahydro.so")
+LIB_PATH_GRAV = os.path.join(_HERE, "libemmahydro_grav.so")
 
 _lib = None
+_lib_grav = None
 
 c_int, c_double, c_ll, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p
 P = ctypes.POINTER
@@ -81,21 +83,32 @@ SIGNATURES = [
 ]
 
 
-def lib():
-    """Load libemmahydro.so once; raise if it is not built."""
-    global _lib
-    if _lib is not None:
-        return _lib
-    if not os.path.exists(LIB_PATH):
-        raise RuntimeError(f"libemmahydro.so is not built ({LIB_PATH}); run emma_b200.build.build()")
+GRAV_SIGNATURES = [
+    ("grav_correction", None, [c_int, c_void_p, c_void_p, c_void_p, c_double]),
+    ("emma_tree_set_force", None, [c_void_p, c_int, c_void_p, c_void_p, c_void_p]),
+]
+
+
+def lib(grav=False):
+    """Load libemmahydro.so (grav: libemmahydro_grav.so, the -DWGRAV cell layout)
+    once; raise if it is not built."""
+    global _lib, _lib_grav
+    if (_lib_grav if grav else _lib) is not None:
+        return _lib_grav if grav else _lib
+    path = LIB_PATH_GRAV if grav else LIB_PATH
+    if not os.path.exists(path):
+        raise RuntimeError(f"{os.path.basename(path)} is not built ({path}); run emma_b200.build.build()")
     # RTLD_LOCAL: the drop-in entries carry the reference's names (HydroSolver, ...);
     # they must not interpose on another library that defines the same symbols
-    L = ctypes.CDLL(LIB_PATH, mode=ctypes.RTLD_LOCAL)
-    for name, res, args in SIGNATURES:
+    L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
+    for name, res, args in SIGNATURES + (GRAV_SIGNATURES if grav else []):
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
-    _lib = L
+    if grav:
+        _lib_grav = L
+    else:
+        _lib = L
     return L
 
 
@@ -105,8 +118,8 @@ def ptr(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-def check(rc, what=""):
+def check(rc, what="", grav=False):
     """Raise on a non-zero status bitmask returned by the library."""
     if rc != 0:
-        msg = lib().emma_hydro_last_error().decode(errors="replace")
+        msg = lib(grav).emma_hydro_last_error().decode(errors="replace")
         raise RuntimeError(f"libemmahydro {what} failed: status=0x{rc & 0xffffffff:x} {msg}")

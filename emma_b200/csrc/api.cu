@@ -13,6 +13,9 @@
 #include <thread>
 #include <vector>
 #include "emma_hydro.h"
+#ifdef EMMA_WGRAV
+#include "emma_hydro_grav.h"
+#endif
 #include "mirror.h"
 #include "plan_types.h"
 #include "schedule.h"
@@ -114,6 +117,14 @@ struct Ctx {
 
 Ctx g;
 using Clock = std::chrono::steady_clock;
+
+// The drop-in entries of a library built for the reference's -DWGRAV cell layout
+// (libemmahydro_grav.so) run the gravity-coupled advance: the cells carry f[3].
+#ifdef EMMA_WGRAV
+constexpr int kDropinGrav = 1;
+#else
+constexpr int kDropinGrav = 0;
+#endif
 
 void fail(unsigned bit, const std::string &msg) {
   g.status |= bit;
@@ -346,6 +357,22 @@ void pack_level(const HostLevel &h, int which, double *out) {
   });
 }
 
+#ifdef EMMA_WGRAV
+// Pack the accelerations f[3] of octs [a, b) of a level into 3 planes of 8*noct.
+void pack_force(const HostLevel &h, long long a, long long b, double *out) {
+  const long long n8 = 8LL * h.noct;
+  for (long long i = a; i < b; i++) {
+    const struct OCT *o = h.octs[i];
+    for (int c = 0; c < 8; c++) {
+      const long long k = 8 * i + c;
+      out[k] = o->cell[c].f[0];
+      out[n8 + k] = o->cell[c].f[1];
+      out[2 * n8 + k] = o->cell[c].f[2];
+    }
+  }
+}
+#endif
+
 inline void finish_prims(struct Wtype &W) {
   W.a = std::sqrt(kG * W.p / W.d);
   W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
@@ -425,7 +452,7 @@ cudaError_t mark_stale(int level) {
 // fuse_cfl: the launch also accumulates each level's max signal speed of the
 // state it writes (the device schedule's next CFL step, SchedState::smax_next).
 bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, long long cells, unsigned shapes,
-                  int ctas, bool fuse_cfl = false) {
+                  int ctas, bool fuse_cfl = false, bool grav = false) {
   BatchArgs a;
   a.lv = d_lv;
   a.work = work;
@@ -444,8 +471,8 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
     tl.b = get_event();
     cudaEventRecord(tl.a, g.stream);
   }
-  // the resident tree of a gravity upload runs the gravity-coupled variant
-  if (d_lv == g.res.d_lv && g.res.host.grav) shapes |= kLaunchGrav;
+  // the levels of a gravity build run the gravity-coupled variant
+  if (grav || (d_lv == g.res.d_lv && g.res.host.grav)) shapes |= kLaunchGrav;
   cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED)
                       ? launch_level_f32(a, shapes, g.nsm, ctas, g.stream, nullptr)
                       : launch_level_fp64(a, shapes, g.nsm, ctas, g.stream, nullptr);
@@ -977,6 +1004,17 @@ int emma_hydro_fields_upload(struct OCT **firstoct) {
     g.h2d_bytes += (long long)bytes;
     CK(mark_stale(L));
     CK(cudaStreamSynchronize(g.stream));
+#ifdef EMMA_WGRAV
+    // the cells' accelerations, when the tree was uploaded with gravity coupling
+    const DevLevel &d = g.res.lev[L];
+    if (d.F != nullptr) {
+      if (!ensure_pin(3 * bytes / 5)) return EMMA_ST_CUDA;
+      parallel_for(h.noct, [&](long long a0, long long b0) { pack_force(h, a0, b0, g.pin); });
+      CK(cudaMemcpyAsync(d.F, g.pin, 3 * bytes / 5, cudaMemcpyHostToDevice, g.stream));
+      g.h2d_bytes += (long long)(3 * bytes / 5);
+      CK(cudaStreamSynchronize(g.stream));
+    }
+#endif
   }
   return 0;
 }
@@ -1406,7 +1444,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     std::string err;
     std::vector<int> shapes((size_t)hi + 1, std::max(-1, requested_shape(g.opt.tile_octs)));
     int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, cache.t.host, err,
-                             shapes.data());
+                             shapes.data(), kDropinGrav);
     if (rc != 0) {
       fail((unsigned)rc, err);
       return 0;
@@ -1425,10 +1463,13 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   const long long n8 = d.n8, nc8 = dc.n8;
   const bool coarse = nc8 > 0 && h.reads_coarse && dc.C != nullptr;
   // pinned staging: level field (5 planes) | level fieldnew (6 planes) | coarser
-  // level (5 planes) | device status word
-  if (!ensure_pin(sizeof(double) * (11 * n8 + 5 * nc8 + 1)) || !ensure_range_events()) return 0;
+  // level (5 planes) | gravity builds: level and coarser accelerations (3 + 3
+  // planes) | device status word
+  const long long nf = kDropinGrav ? 3 * (n8 + nc8) : 0;
+  if (!ensure_pin(sizeof(double) * (11 * n8 + 5 * nc8 + nf + 1)) || !ensure_range_events()) return 0;
   double *pw = g.pin, *pb = g.pin + 5 * n8, *pc = g.pin + 11 * n8;
-  unsigned *pst = reinterpret_cast<unsigned *>(pc + 5 * nc8);
+  [[maybe_unused]] double *pf = pc + 5 * nc8, *pfc = pf + 3 * n8;
+  unsigned *pst = reinterpret_cast<unsigned *>(pc + 5 * nc8 + nf);
   const auto t1 = Clock::now();
   // upload: each host thread packs its oct range in sub-ranges (field and
   // fieldnew in one pass over the cells) and queues one pitched copy of the 11
@@ -1448,10 +1489,16 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
       if (cudaMemcpy2DAsync(d.WB + 8 * s0, pitch, pw + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 11,
                             cudaMemcpyHostToDevice, g.stream) != cudaSuccess)
         copies_ok = false;
+#ifdef EMMA_WGRAV
+      pack_force(h, s0, s1, pf);
+      if (d.F == nullptr || cudaMemcpy2DAsync(d.F + 8 * s0, pitch, pf + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0),
+                                              3, cudaMemcpyHostToDevice, g.stream) != cudaSuccess)
+        copies_ok = false;
+#endif
     }
   });
   if (!copies_ok) return ck(cudaGetLastError(), "H2D level state"), 0;
-  g.h2d_bytes += (long long)sizeof(double) * 11 * n8;
+  g.h2d_bytes += (long long)sizeof(double) * (11 + 3 * kDropinGrav) * n8;
   if (coarse) {
     pack_level(hc, 0, pc);
     if (!ck(cudaMemcpyAsync(dc.W0, pc, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))
@@ -1459,6 +1506,15 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     g.h2d_bytes += (long long)sizeof(double) * 5 * nc8;
     if (!ck(cudaMemsetAsync(dc.C, 0, sizeof(double) * 5 * nc8, g.stream), "memset Cc")) return 0;
   }
+#ifdef EMMA_WGRAV
+  // the coarser level's accelerations, for the forces of its injected cells
+  if (d.nv > 0 && dc.F != nullptr) {
+    parallel_for(hc.noct, [&](long long a0, long long b0) { pack_force(hc, a0, b0, pfc); });
+    if (!ck(cudaMemcpyAsync(dc.F, pfc, sizeof(double) * 3 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Fc"))
+      return 0;
+    g.h2d_bytes += (long long)sizeof(double) * 3 * nc8;
+  }
+#endif
   const auto t2 = Clock::now();
   LevelArgs a;
   std::memset(&a, 0, sizeof(a));
@@ -1485,10 +1541,17 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   a.ntiles = d.ntiles;
   a.wait_slot = -1;
   a.leaf = d.leaf;
+  // gravity builds: the caller applies grav_correction itself (src/advanceamr.c:999)
+  a.F = d.F;
+  a.Fc = dc.F;
+  a.Fv = d.Fv;
+  a.gcorr = 0;
+  a.wv_inject = H.grav;
   k_set_args<<<1, 1, 0, g.stream>>>(T.d_lv, level, a);
   if (!ck(cudaGetLastError(), "k_set_args")) return 0;
-  if (!ck(launch_interp(T.d_lv, level, d.nv, nullptr, g.nsm, g.stream, false), "interpolation launch")) return 0;
-  if (!launch_batch(T.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return 0;
+  if (!ck(launch_interp(T.d_lv, level, d.nv, nullptr, g.nsm, g.stream, H.grav != 0), "interpolation launch"))
+    return 0;
+  if (!launch_batch(T.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas, false, H.grav != 0)) return 0;
   // device status and the corrections first, then the level's new state range by
   // range: each host thread waits for its own range and unpacks it into fieldnew
   // (and field, for HydroSolver) while later ranges are still being copied
@@ -1629,6 +1692,38 @@ void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, 
       for (int c = 0; c < 8; c++) v[i]->cell[c].fieldnew = v[i]->cell[c].field;
   });
 }
+
+#ifdef EMMA_WGRAV
+// grav_correction (src/hydro_utils.c:2388-2444, PRIMITIVE): after HydroSolver,
+// the leaf cells of rank cpu->rank get the full-step kick u += -f dt, then E;
+// `a` is left as it was, as in the reference.  A negative pressure (an abort in
+// the reference) sets EMMA_ST_NAN.
+void grav_correction(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu, REAL dt) {
+  (void)param;
+  if (firstoct == nullptr || level < 1 || level >= kMaxLevels) return;
+  const int rank = dropin_rank(cpu);
+  const std::vector<struct OCT *> &v = walk_level(firstoct, level);
+  std::atomic<bool> neg{false};
+  parallel_for((long long)v.size(), [&](long long a0, long long b0) {
+    for (long long i = a0; i < b0; i++) {
+      struct OCT *o = v[i];
+      if (o->cpu != rank) continue;
+      for (int c = 0; c < 8; c++) {
+        struct CELL *cell = &o->cell[c];
+        if (cell->child != nullptr) continue;
+        struct Wtype W = cell->field;
+        W.u += (-cell->f[0] * dt);
+        W.v += (-cell->f[1] * dt);
+        W.w += (-cell->f[2] * dt);
+        W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
+        if (W.p < 0) neg = true;
+        cell->field = W;
+      }
+    }
+  });
+  if (neg) fail(EMMA_ST_NAN, "grav_correction: negative pressure");
+}
+#endif
 
 void create_hydstencil_GPU(struct CPUINFO *cpu, int stride) {
   (void)cpu;

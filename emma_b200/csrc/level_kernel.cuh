@@ -921,6 +921,12 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch
 }  // namespace emma
 
 namespace emma {
+// The launchers have internal linkage: their occupancy cache is a static local,
+// and a template's static local would otherwise be one object for every library
+// of the process that holds the same instantiation (libemmahydro.so and
+// libemmahydro_grav.so share these object files), so the second library would
+// skip setting its own kernel's shared-memory limit.
+namespace {
 
 // Launch of a work list on a persistent grid of ctas_per_sm CTAs per SM (0 or
 // above the occupancy limit: the limit), so that every CTA is co-resident.
@@ -959,4 +965,5 @@ cudaError_t launch_level_any(const BatchArgs &a, unsigned shapes, int nsm, int c
   }
 }
 
+}  // namespace
 }  // namespace emma

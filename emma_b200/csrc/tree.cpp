@@ -21,6 +21,9 @@
 #include <unordered_map>
 #include <vector>
 #include "emma_hydro.h"
+#ifdef EMMA_WGRAV
+#include "emma_hydro_grav.h"
+#endif
 
 struct EmmaTree {
   // octs live in fixed-size blocks so that pointers stay valid as the tree grows
@@ -205,6 +208,18 @@ void emma_tree_get_field(struct EmmaTree *t, int level, int which, double *out7)
       out7[6 * n + k] = W->E;
     }
 }
+
+#ifdef EMMA_WGRAV
+void emma_tree_set_force(struct EmmaTree *t, int level, const double *fx, const double *fy, const double *fz) {
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) {
+      o->cell[c].f[0] = fx[8 * i + c];
+      o->cell[c].f[1] = fy[8 * i + c];
+      o->cell[c].f[2] = fz[8 * i + c];
+    }
+}
+#endif
 
 // Same encoding as the oracle driver's export: cell code = (oct index in its
 // level list)*8 + cell index; -2 for the root stand-in cell; -1 for NULL.

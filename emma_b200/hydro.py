@@ -120,15 +120,21 @@ class ResidentHydro:
         check(lib().emma_hydro_tree_download(self.tree.firstoct), "tree_download")
 
 
-def HydroSolver(level, firstoct, dtnew, cpu=None):
-    """Drop-in HydroSolver (src/hydro_utils.c:3378) on a host tree."""
-    lib().HydroSolver(level, None, firstoct, cpu, None, 0, dtnew)
+def HydroSolver(level, firstoct, dtnew, cpu=None, grav=False):
+    """Drop-in HydroSolver (src/hydro_utils.c:3378) on a host tree; grav: a tree of
+    the -DWGRAV layout through libemmahydro_grav.so (gravity-coupled advance)."""
+    lib(grav).HydroSolver(level, None, firstoct, cpu, None, 0, dtnew)
 
 
-def advancehydroGPU(firstoct, level, dtnew, cpu=None):
+def advancehydroGPU(firstoct, level, dtnew, cpu=None, grav=False):
     """Drop-in advancehydroGPU (src/hydro_utils_gpu.cu:2470); returns octs advanced."""
-    return lib().advancehydroGPU(firstoct, level, cpu, None, 0, 0.5 ** level, dtnew)
+    return lib(grav).advancehydroGPU(firstoct, level, cpu, None, 0, 0.5 ** level, dtnew)
 
 
-def clean_new_hydro(level, firstoct):
-    lib().clean_new_hydro(level, None, firstoct, None)
+def clean_new_hydro(level, firstoct, grav=False):
+    lib(grav).clean_new_hydro(level, None, firstoct, None)
+
+
+def grav_correction(level, firstoct, dt, cpu=None):
+    """Drop-in grav_correction (src/hydro_utils.c:2388) of libemmahydro_grav.so."""
+    lib(True).grav_correction(level, None, firstoct, cpu, dt)

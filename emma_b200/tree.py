@@ -16,15 +16,19 @@ CELL_OFF = np.array([[c % 2, (c // 2) % 2, c // 4] for c in range(8)], dtype=np.
 class OctTree:
     """An EMMA oct tree in host memory (levels lcoarse..lmax are hydro levels)."""
 
-    def __init__(self, lcoarse, lmax, ngridmax=0):
+    def __init__(self, lcoarse, lmax, ngridmax=0, grav=False):
+        """grav: the reference's -DWGRAV cell layout (built by libemmahydro_grav.so),
+        for the gravity-coupled drop-in entries."""
         self.lcoarse, self.lmax = lcoarse, lmax
-        self._t = lib().emma_tree_create(lcoarse, lmax, ngridmax)
+        self.grav = grav
+        self._L = lib(grav)
+        self._t = self._L.emma_tree_create(lcoarse, lmax, ngridmax)
         if not self._t:
             raise RuntimeError("emma_tree_create failed")
 
     def close(self):
         if self._t:
-            lib().emma_tree_destroy(self._t)
+            self._L.emma_tree_destroy(self._t)
             self._t = None
 
     def __del__(self):
@@ -35,16 +39,16 @@ class OctTree:
 
     @property
     def firstoct(self):
-        return lib().emma_tree_firstoct(self._t)
+        return self._L.emma_tree_firstoct(self._t)
 
     def noct(self, level):
-        return lib().emma_tree_noct(self._t, level)
+        return self._L.emma_tree_noct(self._t, level)
 
     def oct_xyz(self, level):
         n = self.noct(level)
         out = np.zeros((n, 3))
         if n:
-            lib().emma_tree_oct_xyz(self._t, level, ptr(out))
+            self._L.emma_tree_oct_xyz(self._t, level, ptr(out))
         return out
 
     def cell_centres(self, level):
@@ -55,7 +59,7 @@ class OctTree:
     def refine(self, level, mark):
         mark = np.ascontiguousarray(mark, dtype=np.int8)
         assert mark.size == 8 * self.noct(level)
-        rc = lib().emma_tree_refine(self._t, level, ptr(mark))
+        rc = self._L.emma_tree_refine(self._t, level, ptr(mark))
         if rc < 0:
             raise RuntimeError(f"refinement of level {level} refused for {-rc} cells (2:1 rule)")
         return rc
@@ -65,14 +69,20 @@ class OctTree:
 
     def set_fields(self, level, d, u, v, w, p):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (d, u, v, w, p)]
-        lib().emma_tree_set_field(self._t, level, *[ptr(a) for a in arrs])
+        self._L.emma_tree_set_field(self._t, level, *[ptr(a) for a in arrs])
+
+    def set_force(self, level, fx, fy, fz):
+        """Gravitational acceleration f[3] of every cell of a level (grav trees only)."""
+        assert self.grav, "the default cell layout has no force"
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fx, fy, fz)]
+        self._L.emma_tree_set_force(self._t, level, *[ptr(a) for a in arrs])
 
     def get_fields(self, level, which=0):
         """(7, 8*noct): d,u,v,w,p,a,E of `field` (which=0) or `fieldnew` (which=1)."""
         n = self.noct(level)
         out = np.zeros((7, 8 * n))
         if n:
-            lib().emma_tree_get_field(self._t, level, which, ptr(out))
+            self._L.emma_tree_get_field(self._t, level, which, ptr(out))
         return out
 
     def topology(self, level):
@@ -82,7 +92,7 @@ class OctTree:
         ch = np.zeros(8 * n, np.int32)
         lev = np.zeros(n, np.int32)
         if n:
-            lib().emma_tree_topology(self._t, level, ptr(nei), ptr(par), ptr(ch), ptr(lev))
+            self._L.emma_tree_topology(self._t, level, ptr(nei), ptr(par), ptr(ch), ptr(lev))
         return nei.reshape(n, 6), par, ch.reshape(n, 8), lev
 
     def split_mask(self, level):

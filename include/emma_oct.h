@@ -1,12 +1,14 @@
 /*
  * emma_oct.h -- the oct-tree memory layout that EMMA's hydro entry points pass
- * around, declared for a build with -DWHYDRO2 (and neither -DWGRAV, -DWRAD,
- * -DPIC nor -DWRADHYD), REAL = double, NVAR = 6.
+ * around, declared for a build with -DWHYDRO2 (and neither -DWRAD, -DPIC nor
+ * -DWRADHYD), REAL = double, NVAR = 6; with EMMA_WGRAV defined, for the
+ * reference's -DWGRAV build (libemmahydro_grav.so).
  *
  * This is an interface, not an implementation: libemmahydro reads and writes the
  * caller's tree in place, so the field order, types and padding must be exactly
  * those of the reference (src/prototypes.h:611 Wtype, :653 Utype, :825 CELL,
- * :1028 OCT).  Sizes are checked at compile time: CELL 136 B, OCT 1200 B.
+ * :1028 OCT).  Sizes are checked at compile time: CELL 136 B, OCT 1200 B
+ * (EMMA_WGRAV: CELL 192 B, OCT 1648 B).
  * Only the members the hydro path uses are named; nothing else is assumed.
  */
 #ifndef EMMA_OCT_H
@@ -26,10 +28,22 @@ struct Wtype {           /* primitive state of a cell, src/prototypes.h:611 */
 
 struct OCT;
 
-struct CELL {            /* src/prototypes.h:825 (WHYDRO2 members only) */
+#ifdef EMMA_WGRAV
+struct Gtype {           /* src/prototypes.h:818 */
+  REAL d, p;             /* density contrast, potential */
+};
+#endif
+
+struct CELL {            /* src/prototypes.h:825 (WHYDRO2 [+ WGRAV] members only) */
   struct OCT *child;     /* finer oct, NULL for a leaf */
   REAL marked;           /* refinement mark */
   int idx;               /* index of the cell within its oct: ix + 2 iy + 4 iz */
+#ifdef EMMA_WGRAV
+  struct Gtype gdata;
+  REAL pnew;             /* new potential */
+  REAL res;              /* residual */
+  REAL f[3];             /* gravitational acceleration of the cell */
+#endif
   struct Wtype field;    /* state at the start of the level step */
   struct Wtype fieldnew; /* state being built during the level step */
 };
@@ -58,12 +72,19 @@ struct HGRID;
 }
 #endif
 
-#ifdef __cplusplus
-static_assert(sizeof(struct CELL) == 136, "struct CELL must match the reference layout");
-static_assert(sizeof(struct OCT) == 1200, "struct OCT must match the reference layout");
+#ifdef EMMA_WGRAV
+#define EMMA_SIZEOF_CELL 192
+#define EMMA_SIZEOF_OCT 1648
 #else
-_Static_assert(sizeof(struct CELL) == 136, "struct CELL must match the reference layout");
-_Static_assert(sizeof(struct OCT) == 1200, "struct OCT must match the reference layout");
+#define EMMA_SIZEOF_CELL 136
+#define EMMA_SIZEOF_OCT 1200
+#endif
+#ifdef __cplusplus
+static_assert(sizeof(struct CELL) == EMMA_SIZEOF_CELL, "struct CELL must match the reference layout");
+static_assert(sizeof(struct OCT) == EMMA_SIZEOF_OCT, "struct OCT must match the reference layout");
+#else
+_Static_assert(sizeof(struct CELL) == EMMA_SIZEOF_CELL, "struct CELL must match the reference layout");
+_Static_assert(sizeof(struct OCT) == EMMA_SIZEOF_OCT, "struct OCT must match the reference layout");
 #endif
 
 #endif

@@ -115,6 +115,9 @@ class GravClone:
     def firstoct(self):
         return self.L.orc_grav_first(self.h)
 
+    def noct(self, level):
+        return self.src.noct(level)
+
     def set_force(self, level, fx, fy, fz):
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fx, fy, fz)]
         self.L.orc_grav_set_force(self.h, level, *[_p(a) for a in arrs])

@@ -8,9 +8,13 @@ from conftest import ROOT
 HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.join(ROOT, "include"))) if f.endswith(".h")]
 
 
-def declared_functions():
+GRAV_HEADER = os.path.join(ROOT, "include", "emma_hydro_grav.h")
+
+
+def declared_functions(headers=None):
+    """Functions declared in the headers (default: all but the gravity library's own)."""
     names = set()
-    for h in HEADERS:
+    for h in (headers if headers is not None else [h for h in HEADERS if h != GRAV_HEADER]):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         src = re.sub(r"//[^\n]*", "", src)
@@ -35,6 +39,18 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
     bound = {n for n, _, _ in SIGNATURES}
     assert declared_functions() <= bound, declared_functions() - bound
+
+
+def test_gravity_library_exports_everything():
+    """libemmahydro_grav.so (the -DWGRAV cell layout) exports the default entries
+    and its own (grav_correction, the force setter of test trees)."""
+    from emma_b200._lib import LIB_PATH_GRAV, SIGNATURES, GRAV_SIGNATURES
+    L = ctypes.CDLL(LIB_PATH_GRAV)
+    names = declared_functions(HEADERS)
+    assert {"grav_correction", "emma_tree_set_force"} <= names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert names <= {n for n, _, _ in SIGNATURES + GRAV_SIGNATURES}
 
 
 def test_struct_layout_matches_reference():

@@ -139,3 +139,38 @@ def test_set_force_needs_a_gravity_upload(gpu):
     with pytest.raises(RuntimeError):
         r.set_force(3, np.zeros(n8), np.zeros(n8), np.zeros(n8))
     lib().emma_hydro_clear_status()
+
+
+def test_dropin_gravity_matches_oracle(gpu):
+    """libemmahydro_grav.so (the reference's -DWGRAV cell layout): drop-in
+    HydroSolver + grav_correction level by level, as Advance_level calls them,
+    on the caller's tree, against the gravity oracle on an identical tree."""
+    from emma_b200 import OctTree
+    from emma_b200 import hydro as H
+    from test_oracle_pin import random_fields, random_forces
+
+    def build():
+        t = OctTree(4, 6, grav=True)
+        for i, rad in enumerate((0.3, 0.15)):
+            t.refine_where(4 + i, lambda c, rad=rad: np.linalg.norm(c - 0.5, axis=1) < rad)
+        random_fields(t, range(4, 7))
+        random_forces(t, range(4, 7))
+        return t
+
+    tg, to = build(), build()
+    R = oracle.Restatement(grav=True)
+    L = lib(True)
+    L.emma_hydro_clear_status()
+    dts = {4: 2e-3, 5: 1e-3, 6: 5e-4}
+    for l in (4, 5, 6):
+        H.clean_new_hydro(l, tg.firstoct, grav=True)
+        R.clean_new(to.firstoct, l)
+    for l in (6, 6, 5, 6, 6, 5, 4):
+        H.HydroSolver(l, tg.firstoct, dts[l], grav=True)
+        H.grav_correction(l, tg.firstoct, dts[l])
+        assert R.hydro_solver(to.firstoct, l, dts[l]) == 0
+        assert R.grav_correction(to.firstoct, l, dts[l]) == 0
+    assert L.emma_hydro_status() == 0, L.emma_hydro_last_error()
+    for l in (4, 5, 6):
+        e = per_cell_rel(tg.get_fields(l)[:5], to.get_fields(l)[:5])
+        assert e.max() <= 1e-12, (l, e.max())

@@ -154,6 +154,50 @@ def test_gravity_clone_matches_reference_tree():
         assert np.array_equal(ref.get_fields(l), gc.get_fields(l)), l
 
 
+def test_gravity_layout_tree_equals_layout_copy():
+    """A tree built in the -DWGRAV layout (libemmahydro_grav.so) and a copy of the
+    default-layout tree give the same gravity restatement results bit for bit."""
+    base, lmax, radii = 4, 6, (0.3, 0.15)
+    tp = _amr_tree(base, lmax, radii)
+    tg = OctTree(base, lmax, grav=True)
+    for i, r in enumerate(radii):
+        tg.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
+    random_fields(tg, range(base, lmax + 1))
+    random_forces(tg, range(base, lmax + 1))
+    gc = oracle.GravClone(tp)
+    random_forces(gc, range(base, lmax + 1))
+    t1, adt1, e1 = oracle.Restatement(grav=True).run(tg.firstoct, base, lmax, 2, 0.8)
+    t2, adt2, e2 = gc.run(2, 0.8)
+    assert e1 == e2 == 0 and t1 == t2 and np.array_equal(adt1, adt2)
+    for l in range(base, lmax + 1):
+        assert np.array_equal(tg.get_fields(l), gc.get_fields(l)), l
+
+
+def test_dropin_grav_correction_matches_oracle():
+    """libemmahydro_grav.so's grav_correction (host loop, no GPU) == the oracle's."""
+    from emma_b200 import hydro as H
+    trees = []
+    for _ in range(2):
+        t = OctTree(4, 5, grav=True)
+        t.refine_where(4, lambda c: np.linalg.norm(c - 0.5, axis=1) < 0.3)
+        random_fields(t, (4, 5))
+        random_forces(t, (4, 5))
+        trees.append(t)
+    for l in (5, 4):
+        H.grav_correction(l, trees[0].firstoct, 3e-3)
+        assert oracle.Restatement(grav=True).grav_correction(trees[1].firstoct, l, 3e-3) == 0
+    for l in (4, 5):
+        assert np.array_equal(trees[0].get_fields(l), trees[1].get_fields(l)), l
+    assert not np.array_equal(trees[0].get_fields(5), _amr_fields_only(4, 5))
+
+
+def _amr_fields_only(base, level):
+    t = OctTree(base, level, grav=True)
+    t.refine_where(base, lambda c: np.linalg.norm(c - 0.5, axis=1) < 0.3)
+    random_fields(t, (base, level))
+    return t.get_fields(level)
+
+
 def _golden_cases():
     return sorted(f for f in os.listdir(GOLDEN) if f.endswith(".npz")) if os.path.isdir(GOLDEN) else []
 
