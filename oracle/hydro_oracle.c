@@ -99,13 +99,15 @@ static void to_cons(const oW *W, oU *U) {
   U->eint = W->p / (GAM - 1.);
   U->E = W->E;
 }
-static void to_prim(const oU *U, oW *W) {
+/* dual: -DDUAL_E, the pressure from the tracked internal energy (src/hydro_utils.c:45-49) */
+static void to_prim(const oU *U, oW *W, int dual) {
   double dl = (U->d == 0. ? DEF_DENS : U->d);
   W->d = U->d;
   W->u = U->du / dl;
   W->v = U->dv / dl;
   W->w = U->dw / dl;
-  W->p = (GAM - 1.) * (U->E - ((U->du) * (U->du) + (U->dv) * (U->dv) + (U->dw) * (U->dw)) / (dl)*0.5);
+  if (dual) W->p = U->eint * (GAM - 1.);
+  else W->p = (GAM - 1.) * (U->E - ((U->du) * (U->du) + (U->dv) * (U->dv) + (U->dw) * (U->dw)) / (dl)*0.5);
   W->E = U->E;
   W->a = sqrt(GAM * W->p / dl);
 }
@@ -332,8 +334,11 @@ static void euler_flux(const oU *U, int n, double f[5]) {
 }
 
 /* HLLC flux across a face normal to axis n from left/right MUSCL states
- * (src/hydro_utils.c:2055-2138, same branches for y :1783, z :1508). */
-static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5]) {
+ * (src/hydro_utils.c:2055-2138, same branches for y :1783, z :1508).
+ * us (optional, -DDUAL_E): the state Us of the branch taken (the upwind state or
+ * the star state), from which the sweeps take the internal-energy flux and the
+ * face velocity of divu (src/hydro_utils.c:2126-2129). */
+static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us) {
   double SL, SR, ustar;
   oU UL, UR;
   int k;
@@ -343,8 +348,10 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5]) {
   to_cons(WR, &UR);
   if (SL >= 0.) {
     euler_flux(&UL, n, F);
+    if (us) *us = UL;
   } else if (SR <= 0.) {
     euler_flux(&UR, n, F);
+    if (us) *us = UR;
   } else if ((SL < 0.) && (ustar >= 0.)) {
     const oW *W = WL;
     const oU *U = &UL;
@@ -355,6 +362,13 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5]) {
     F[0] += (fact * 1. - U->d) * SL;
     for (k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : vel[k]) - mom[k]) * SL;
     F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SL - un)))) - U->E) * SL;
+    if (us) {
+      double m[3];
+      for (k = 0; k < 3; k++) m[k] = fact * (k == n ? ustar : vel[k]);
+      us->d = fact * 1.;
+      us->du = m[0]; us->dv = m[1]; us->dw = m[2];
+      us->E = fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SL - un))));
+    }
   } else if ((ustar <= 0.) && (SR > 0.)) {
     const oW *W = WR;
     const oU *U = &UR;
@@ -365,6 +379,13 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5]) {
     F[0] += (fact * 1. - U->d) * SR;
     for (k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : vel[k]) - mom[k]) * SR;
     F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SR - un)))) - U->E) * SR;
+    if (us) {
+      double m[3];
+      for (k = 0; k < 3; k++) m[k] = fact * (k == n ? ustar : vel[k]);
+      us->d = fact * 1.;
+      us->du = m[0]; us->dv = m[1]; us->dw = m[2];
+      us->E = fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SR - un))));
+    }
   }
 }
 
@@ -584,27 +605,43 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
   oOct *o;
   int c, k, n = 0;
   g_err = 0;
+  const int dual = flag_on(flags, ORC_DUAL_E);
   for (o = firstoct[level - 1]; o != NULL; o = o->next) {
-    double flux[8][6][5];
+    double flux[8][6][6];  /* 6th component: internal-energy flux (-DDUAL_E) */
+    double divu[8];
     if (o->cpu != 0) continue;
     n++;
     gather(&g_st, o, flags);
     /* sweeps x, y, z: two faces per cell per direction, split neighbours cancelled */
     for (c = 0; c < 8; c++) {
       int dir;
+      /* -DDUAL_E: eint of the cell's old state (W2U of its field) */
+      const double eold = g_st.w[13][c].p / (GAM - 1.);
+      divu[c] = 0.;
       for (dir = 0; dir < 3; dir++) {
         int s;
         for (s = 0; s < 2; s++) {
           int kf = 2 * dir + s, same, vc, nslot;
           const oW *Wc, *Wn;
-          double F[5];
+          double F[6];
+          oU us;
           cell_nei(c, kf, &same, &vc);
           nslot = same ? 13 : FACE_SLOT[kf];
           Wc = face_state(&g_st, 13, c, kf, dt, dx);
           Wn = face_state(&g_st, nslot, vc, kf ^ 1, dt, dx);
-          if (s == 0) hllc_flux(Wn, Wc, dir, F);
-          else hllc_flux(Wc, Wn, dir, F);
-          for (k = 0; k < 5; k++) flux[c][kf][k] = F[k] * (double)(!g_st.split[nslot][vc]);
+          if (s == 0) hllc_flux(Wn, Wc, dir, F, dual ? &us : NULL);
+          else hllc_flux(Wc, Wn, dir, F, dual ? &us : NULL);
+          F[5] = 0.;
+          if (dual) {
+            /* src/hydro_utils.c:2126-2129: ebar, the internal-energy flux and the
+             * p div(u) term of the face (summed whether or not the neighbour is split) */
+            double mom[3] = {us.du, us.dv, us.dw};
+            double ebar = (us.E - 0.5 * (us.du * us.du + us.dv * us.dv + us.dw * us.dw) / us.d);
+            double divuloc = (GAM - 1.) * (mom[dir] / us.d) * eold;
+            F[5] = (mom[dir] / us.d * ebar);
+            divu[c] += (s == 0) ? -divuloc : divuloc;
+          }
+          for (k = 0; k < 6; k++) flux[c][kf][k] = F[k] * (double)(!g_st.split[nslot][vc]);
         }
       }
     }
@@ -621,6 +658,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
           dU.dv += flux[c][f][2] * dtsurdx * one;
           dU.dw += flux[c][f][3] * dtsurdx * one;
           dU.E += flux[c][f][4] * dtsurdx * one;
+          dU.eint += flux[c][f][5] * dtsurdx * one;
           one *= -1.;
         }
         if (isnan(cell->fieldnew.u)) g_err |= ORC_ERR_NAN;
@@ -631,9 +669,16 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
         U.dw += dU.dw;
         U.E += dU.E;
         ekin = 0.5 * (U.du * U.du + U.dv * U.dv + U.dw * U.dw) / U.d;
-        U.eint = U.E - ekin;
+        if (dual) {
+          /* src/hydro_utils.c:3167-3177: tracked eint, unless E - Ekin is well resolved */
+          U.eint += dU.eint;
+          U.eint += (-divu[c] * dtsurdx);
+          if ((U.E - ekin) > 0.5 * pow(divu[c], 2)) U.eint = U.E - ekin;
+        } else {
+          U.eint = U.E - ekin;
+        }
         U.eint = fmax(U.eint * (GAM - 1.), P_MIN) / (GAM - 1.);
-        to_prim(&U, &cell->fieldnew);
+        to_prim(&U, &cell->fieldnew, dual);
         cell->fieldnew.p = fmax(cell->fieldnew.p, P_MIN);
         cell->fieldnew.a = sqrt(GAM * cell->fieldnew.p / cell->fieldnew.d);
         get_E(&cell->fieldnew);
@@ -657,7 +702,8 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
           U.dv += flux[c][k][2] * dtsurdx * one * 0.125;
           U.dw += flux[c][k][3] * dtsurdx * one * 0.125;
           U.E += flux[c][k][4] * dtsurdx * one * 0.125;
-          to_prim(&U, &W);
+          if (dual) U.eint += flux[c][k][5] * dtsurdx * one * 0.125;
+          to_prim(&U, &W, dual);
           cc->fieldnew = W;
         }
       }

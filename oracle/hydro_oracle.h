@@ -26,6 +26,7 @@ extern "C" {
 #define ORC_TRANSZM 0x10
 #define ORC_TRANSZP 0x20
 #define ORC_HYDROTEST 0x40 /* -DHYDROTEST gather (src/hydro_utils.c:2464-2845) */
+#define ORC_DUAL_E 0x80    /* -DDUAL_E: tracked internal energy (src/hydro_utils.c:45-49, 2126-2129, 3167-3180) */
 
 /* error bits returned by the entry points (the reference aborts instead) */
 #define ORC_ERR_NEG_DENSITY 0x01   /* src/hydro_utils.c:1212 */

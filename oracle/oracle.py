@@ -22,8 +22,10 @@ ORACLE_LIB_GRAV = os.path.join(HERE, "_build", "liboracle_grav.so")
 REF_LIB = os.path.join(HERE, "_ref", "libemmaref.so")
 REF_LIB_TX = os.path.join(HERE, "_ref", "libemmaref_tx.so")
 REF_LIB_GRAV = os.path.join(HERE, "_ref", "libemmaref_grav.so")
+REF_LIB_DUAL = os.path.join(HERE, "_ref", "libemmaref_dual.so")
 
 HYDROTEST = 0x40
+DUAL_E = 0x80
 c_int, c_double, c_void_p, c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
 
 
@@ -31,9 +33,10 @@ def _p(a):
     return ctypes.c_void_p(a.ctypes.data)
 
 
-def flags_for(trans):
-    """Oracle flags for the library's transmissive flags (which follow HYDROTEST semantics)."""
-    return (trans | HYDROTEST) if trans else 0
+def flags_for(trans, dual=False):
+    """Oracle flags for the library's transmissive flags (which follow HYDROTEST
+    semantics) and dual-energy option."""
+    return ((trans | HYDROTEST) if trans else 0) | (DUAL_E if dual else 0)
 
 
 class Restatement:
@@ -62,15 +65,16 @@ class Restatement:
         self.L = Restatement._libs[path]
         self.grav = grav
 
-    def run(self, firstoct, lcoarse, lmax, nsteps, cfl, trans=0, nsub=2, dt_param=1e9, time_max=1e9, tsim0=0.0):
+    def run(self, firstoct, lcoarse, lmax, nsteps, cfl, trans=0, nsub=2, dt_param=1e9, time_max=1e9, tsim0=0.0,
+            dual=False):
         adt = np.zeros(lmax)
         nd, err = c_int(), c_int()
-        t = self.L.orc_run(firstoct, lcoarse, lmax, nsteps, dt_param, time_max, nsub, cfl, flags_for(trans),
+        t = self.L.orc_run(firstoct, lcoarse, lmax, nsteps, dt_param, time_max, nsub, cfl, flags_for(trans, dual),
                            tsim0, _p(adt), ctypes.byref(nd), ctypes.byref(err))
         return t, adt, err.value
 
-    def hydro_solver(self, firstoct, level, dt, trans=0):
-        return self.L.orc_hydro_solver(firstoct, level, dt, flags_for(trans))
+    def hydro_solver(self, firstoct, level, dt, trans=0, dual=False):
+        return self.L.orc_hydro_solver(firstoct, level, dt, flags_for(trans, dual))
 
     def clean_new(self, firstoct, level):
         self.L.orc_clean_new_hydro(firstoct, level)
@@ -139,8 +143,8 @@ class GravClone:
             self.h = None
 
 
-def ref_available(tx=False, grav=False):
-    return os.path.exists(REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
+def ref_available(tx=False, grav=False, dual=False):
+    return os.path.exists(REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB)))
 
 
 class RefTree:
@@ -148,9 +152,9 @@ class RefTree:
 
     _libs = {}
 
-    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False):
-        assert not (tx and grav), "no transmissive gravity build"
-        path = REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB)
+    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False, dual=False):
+        assert (tx + grav + dual) <= 1, "one build variant at a time"
+        path = REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
         if path not in RefTree._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"reference oracle not built: {path}")

@@ -36,8 +36,9 @@ def random_forces(tree, levels, seed=54321, amp=0.5):
         tree.set_force(l, *(rng.uniform(-amp, amp, n8) for _ in range(3)))
 
 
-def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, grav=False):
-    ref = oracle.RefTree(base, lmax, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)), grav=grav)
+def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, grav=False, dual=False):
+    ref = oracle.RefTree(base, lmax, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)), grav=grav,
+                         dual=dual)
     for i, r in enumerate(radii):
         ref.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
     if fields is None:
@@ -55,7 +56,7 @@ def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, g
     A = {l: (ref.get_fields(l, 0), ref.get_fields(l, 1)) for l in range(base, lmax + 1)}
     ctypes.memmove(base_ptr, snap, nbytes)
     trans = 3 if tx else 0
-    t2, adt2, err = oracle.Restatement(grav=grav).run(ref.firstoct, base, lmax, nsteps, 0.8, trans=trans)
+    t2, adt2, err = oracle.Restatement(grav=grav).run(ref.firstoct, base, lmax, nsteps, 0.8, trans=trans, dual=dual)
     assert err == 0
     assert t1 == t2 and np.array_equal(adt1, adt2)
     for l in range(base, lmax + 1):
@@ -109,6 +110,30 @@ def test_pin_gravity_amr():
     """-DWGRAV on two refined levels: forces of injected coarse cells interpolated
     (coarse2fine_forcelin) in the gather."""
     ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, grav=True)
+
+
+needs_ref_dual = pytest.mark.skipif(not oracle.ref_available(dual=True), reason="oracle/_ref dual-energy build absent")
+
+
+@needs_ref_dual
+def test_pin_dual_energy_uniform():
+    """-DDUAL_E: tracked internal energy with its flux, the p div(u) term and the
+    E - Ekin switch (src/hydro_utils.c:3167-3180)."""
+    ref_vs_restatement(False, 4, 4, (), 3, dual=True)
+
+
+@needs_ref_dual
+def test_pin_dual_energy_amr():
+    ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, dual=True)
+
+
+@needs_ref_dual
+def test_pin_dual_energy_strong_shocks():
+    """Pressure jumps of 1e4 make the E - Ekin switch go both ways."""
+    def fields(c):
+        r = np.linalg.norm(c - 0.5, axis=1)
+        return (1.0 + 0 * r, 0.5 * np.sin(6.3 * c[:, 1]), 0 * r, 0 * r, np.where(r < 0.15, 1e2, 1e-2))
+    ref_vs_restatement(False, 4, 5, (0.3,), 4, fields=fields, dual=True)
 
 
 def _amr_tree(base, lmax, radii, seed=12345):
