@@ -21,7 +21,8 @@ P = ctypes.POINTER
 
 class EmmaHydroOptions(ctypes.Structure):
     _fields_ = [("precision", c_int), ("trans_flags", c_int), ("cfl", c_double),
-                ("tile_octs", c_int), ("device", c_int), ("use_graph", c_int), ("gravity", c_int)]
+                ("tile_octs", c_int), ("device", c_int), ("use_graph", c_int), ("gravity", c_int),
+                ("dual_energy", c_int)]
 
 
 PREC_FP64, PREC_MIXED = 0, 1

@@ -52,6 +52,7 @@ struct DevLevel {
   double *Wv = nullptr;    // their 8 interpolated (gravity build: injected) sub-cells
   double *F = nullptr;     // gravity build: acceleration planes fx,fy,fz of the level's cells
   double *Fv = nullptr;    // gravity build: interpolated accelerations of the listed coarser cells
+  uint8_t *az = nullptr;   // dual energy: per cell, a split cell whose stored sound speed is 0
   long long nv = 0;
   int shape = 0;        // brick shape of the plan (kShapes)
   int ctas = 0;         // CTAs per SM of its launches (0: the occupancy limit)
@@ -125,6 +126,9 @@ constexpr int kDropinGrav = 1;
 #else
 constexpr int kDropinGrav = 0;
 #endif
+
+// Planes of a correction buffer: d, du, dv, dw, E, and with dual energy eint.
+inline long long cplanes() { return g.opt.dual_energy ? 6 : 5; }
 
 void fail(unsigned bit, const std::string &msg) {
   g.status |= bit;
@@ -223,6 +227,7 @@ void free_level(DevLevel &d) {
   cudaFree(d.Wv);
   cudaFree(d.F);
   cudaFree(d.Fv);
+  cudaFree(d.az);
   d = DevLevel();
 }
 
@@ -282,8 +287,9 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     bool has_split = false;
     for (uint8_t m : h.split) has_split = has_split || m != 0;
     if (has_split) {
-      if (!ck(cudaMalloc(&d.C, bytes), "cudaMalloc C")) return false;
-      if (!ck(cudaMemset(d.C, 0, bytes), "cudaMemset C")) return false;
+      const size_t cb = sizeof(double) * cplanes() * (size_t)std::max<long long>(d.n8, 1);
+      if (!ck(cudaMalloc(&d.C, cb), "cudaMalloc C")) return false;
+      if (!ck(cudaMemset(d.C, 0, cb), "cudaMemset C")) return false;
     }
     if (!upload_vec(&d.split, h.split)) return false;
     if (!upload_vec(&d.child, h.child)) return false;
@@ -295,6 +301,11 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
       // transmissive builds interpolate the states, gravity builds the forces
       if (!H.grav && !ck(cudaMalloc(&d.Wv, sizeof(double) * 5 * 8 * (size_t)d.nv), "cudaMalloc Wv")) return false;
       if (H.grav && !ck(cudaMalloc(&d.Fv, sizeof(double) * 3 * 8 * (size_t)d.nv), "cudaMalloc Fv")) return false;
+    }
+    if (g.opt.dual_energy) {
+      if (!ck(cudaMalloc(&d.az, (size_t)std::max<long long>(d.n8, 1)), "cudaMalloc az") ||
+          !ck(cudaMemset(d.az, 0, (size_t)std::max<long long>(d.n8, 1)), "cudaMemset az"))
+        return false;
     }
     if (H.grav) {  // accelerations start at zero until the caller sets them
       const size_t fb = sizeof(double) * 3 * (size_t)std::max<long long>(d.n8, 1);
@@ -330,6 +341,8 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     a.Fv = d.Fv;
     a.gcorr = H.grav;
     a.wv_inject = H.grav;
+    a.az = d.az;
+    a.azall = (!with_base && g.opt.dual_energy) ? &g.d_S->azall[L] : nullptr;  // resident levels only
     k_set_args<<<1, 1, 0, g.stream>>>(t.d_lv, L, a);
     if (!ck(cudaGetLastError(), "k_set_args")) return false;
   }
@@ -372,6 +385,15 @@ void pack_force(const HostLevel &h, long long a, long long b, double *out) {
   }
 }
 #endif
+
+// Dual energy: az[8i+c] = 1 for a split cell whose stored sound speed is 0 (the
+// reference's averaging leaves it so), octs [a, b) of a level.
+void pack_az(const HostLevel &h, long long a, long long b, uint8_t *az) {
+  for (long long i = a; i < b; i++) {
+    const struct OCT *o = h.octs[i];
+    for (int c = 0; c < 8; c++) az[8 * i + c] = (o->cell[c].child != nullptr && o->cell[c].field.a == 0.) ? 1 : 0;
+  }
+}
 
 inline void finish_prims(struct Wtype &W) {
   W.a = std::sqrt(kG * W.p / W.d);
@@ -471,8 +493,9 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
     tl.b = get_event();
     cudaEventRecord(tl.a, g.stream);
   }
-  // the levels of a gravity build run the gravity-coupled variant
+  // the levels of a gravity build run the gravity-coupled variant; dual energy its own
   if (grav || (d_lv == g.res.d_lv && g.res.host.grav)) shapes |= kLaunchGrav;
+  if (g.opt.dual_energy) shapes |= kLaunchDual;
   cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED)
                       ? launch_level_f32(a, shapes, g.nsm, ctas, g.stream, nullptr)
                       : launch_level_fp64(a, shapes, g.nsm, ctas, g.stream, nullptr);
@@ -556,7 +579,7 @@ bool emit_level(int L, int nsub) {
   for (int it = 0; it < nsub; it++) {
     k_sub_begin<<<1, 1, 0, g.stream>>>(S, L, it);
     const int *gate = &S->active[L];
-    const long long n5 = 5 * d.n8;
+    const long long n5 = cplanes() * d.n8;
     if (d.C != nullptr)
       k_clear<<<(unsigned)std::max<long long>(1, std::min<long long>((n5 + 255) / 256, 4LL * g.nsm)), 256, 0,
                 g.stream>>>(d.C, n5, gate);
@@ -583,7 +606,7 @@ bool emit_coarse_step(int nsub) {
     // reduction kernel where the state was set from the host), then all levels in one launch
     for (int L = lc; L <= lf; L++) {
       const DevLevel &d = t.lev[L];
-      if (d.C != nullptr && !ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C"))
+      if (d.C != nullptr && !ck(cudaMemsetAsync(d.C, 0, sizeof(double) * cplanes() * d.n8, g.stream), "memset C"))
         return false;
       if (!ck(launch_cfl(t.d_lv, L, d.n8, &S->stale[L], &S->smax[L], g.nsm, g.stream), "cfl launch"))
         return false;
@@ -694,6 +717,7 @@ void emma_hydro_default_options(struct EmmaHydroOptions *opt) {
   opt->device = 0;
   opt->use_graph = 1;
   opt->gravity = 0;
+  opt->dual_energy = 0;
 }
 
 int emma_hydro_init(const struct EmmaHydroOptions *opt) {
@@ -721,9 +745,9 @@ int emma_hydro_init(const struct EmmaHydroOptions *opt) {
 int emma_hydro_set_options(const struct EmmaHydroOptions *opt) {
   if (opt == nullptr) return EMMA_ST_ARG;
   if (!g.ready) return emma_hydro_init(opt);
-  const int old_trans = g.opt.trans_flags, old_grav = g.opt.gravity;
+  const int old_trans = g.opt.trans_flags, old_grav = g.opt.gravity, old_dual = g.opt.dual_energy;
   g.opt = *opt;
-  if (old_trans != opt->trans_flags || old_grav != opt->gravity) {
+  if (old_trans != opt->trans_flags || old_grav != opt->gravity || old_dual != opt->dual_energy) {
     // the tile plans encode the boundary ghosts and the gravity interpolation lists:
     // a resident tree must be uploaded again
     cudaStreamSynchronize(g.stream);
@@ -864,8 +888,10 @@ bool autotune_tree(Tree &t, int shape_req) {
       BatchArgs probe{};
       if (ok)
         ok = ck((g.opt.precision == EMMA_PREC_MIXED)
-                    ? launch_level_f32(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u), g.nsm, 0, g.stream, &occ)
-                    : launch_level_fp64(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u), g.nsm, 0, g.stream, &occ),
+                    ? launch_level_f32(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u) |
+                                                  (g.opt.dual_energy ? kLaunchDual : 0u), g.nsm, 0, g.stream, &occ)
+                    : launch_level_fp64(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u) |
+                                                   (g.opt.dual_energy ? kLaunchDual : 0u), g.nsm, 0, g.stream, &occ),
                 "occupancy");
       for (int c = 1; ok && c <= std::min(occ, 4); c++) {
         double ms = 0;
@@ -922,7 +948,7 @@ bool autotune_tree(Tree &t, int shape_req) {
   // undo the trial launches: corrections, completion counters, status
   for (int L = t.lcoarse; L <= t.lmax && ok; L++) {
     const DevLevel &d = t.lev[L];
-    if (d.C != nullptr) ok = ck(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream), "memset C");
+    if (d.C != nullptr) ok = ck(cudaMemsetAsync(d.C, 0, sizeof(double) * cplanes() * d.n8, g.stream), "memset C");
   }
   ok = ok && ck(cudaMemsetAsync(g.d_done, 0, sizeof(unsigned) * kMaxLevels, g.stream), "memset done") &&
        ck(cudaMemcpyAsync(g.d_status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice, g.stream), "status") &&
@@ -954,7 +980,7 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
   }
   std::vector<int> shapes((size_t)lmax + 1, shape_req);
   int rc = build_host_tree(firstoct, lcoarse, lmax, rank, g.opt.trans_flags, lcoarse, lmax, g.res.host, err,
-                           shapes.data(), g.opt.gravity);
+                           shapes.data(), g.opt.gravity, g.opt.dual_energy);
   if (rc != 0) {
     fail((unsigned)rc, err);
     return rc;
@@ -1004,6 +1030,14 @@ int emma_hydro_fields_upload(struct OCT **firstoct) {
     g.h2d_bytes += (long long)bytes;
     CK(mark_stale(L));
     CK(cudaStreamSynchronize(g.stream));
+    const DevLevel &dl = g.res.lev[L];
+    if (dl.az != nullptr) {  // dual energy: split cells with a stored sound speed of 0
+      uint8_t *pz = reinterpret_cast<uint8_t *>(g.pin);
+      parallel_for(h.noct, [&](long long a0, long long b0) { pack_az(h, a0, b0, pz); });
+      CK(cudaMemcpyAsync(dl.az, pz, (size_t)dl.n8, cudaMemcpyHostToDevice, g.stream));
+      CK(cudaMemsetAsync(&g.d_S->azall[L], 0, sizeof(int), g.stream));
+      CK(cudaStreamSynchronize(g.stream));
+    }
 #ifdef EMMA_WGRAV
     // the cells' accelerations, when the tree was uploaded with gravity coupling
     const DevLevel &d = g.res.lev[L];
@@ -1087,6 +1121,10 @@ int emma_hydro_set_level_state(int level, const double *host_in) {
   CK(cudaMemcpyAsync(W, host_in, sizeof(double) * 5 * d.n8, cudaMemcpyHostToDevice, g.stream));
   g.h2d_bytes += (long long)sizeof(double) * 5 * d.n8;
   CK(mark_stale(level));
+  if (d.az != nullptr) {  // a state set from primitives: every sound speed follows from p and rho
+    CK(cudaMemsetAsync(d.az, 0, (size_t)d.n8, g.stream));
+    CK(cudaMemsetAsync(&g.d_S->azall[level], 0, sizeof(int), g.stream));
+  }
   CK(cudaStreamSynchronize(g.stream));
   return 0;
 }
@@ -1119,7 +1157,7 @@ int emma_hydro_clean_new(int level) {
   if (!level_ok(level)) return EMMA_ST_ARG;
   const DevLevel &d = g.res.lev[level];
   if (d.n8 == 0 || d.C == nullptr) return 0;
-  CK(cudaMemsetAsync(d.C, 0, sizeof(double) * 5 * d.n8, g.stream));
+  CK(cudaMemsetAsync(d.C, 0, sizeof(double) * cplanes() * d.n8, g.stream));
   return 0;
 }
 
@@ -1154,6 +1192,7 @@ int emma_hydro_advance_level(int level, double dt) {
   k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
   CK(cudaGetLastError());
   CK(mark_stale(level));
+  if (d.az != nullptr) CK(cudaMemsetAsync(&g.d_S->azall[level], 1, sizeof(int), g.stream));  // nonzero
   g.updates += d.leaf;
   return 0;
 }
@@ -1444,7 +1483,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     std::string err;
     std::vector<int> shapes((size_t)hi + 1, std::max(-1, requested_shape(g.opt.tile_octs)));
     int rc = build_host_tree(firstoct, lo, hi, rank, g.opt.trans_flags, level, level, cache.t.host, err,
-                             shapes.data(), kDropinGrav);
+                             shapes.data(), kDropinGrav, g.opt.dual_energy);
     if (rc != 0) {
       fail((unsigned)rc, err);
       return 0;
@@ -1465,11 +1504,12 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   // pinned staging: level field (5 planes) | level fieldnew (6 planes) | coarser
   // level (5 planes) | gravity builds: level and coarser accelerations (3 + 3
   // planes) | device status word
-  const long long nf = kDropinGrav ? 3 * (n8 + nc8) : 0;
-  if (!ensure_pin(sizeof(double) * (11 * n8 + 5 * nc8 + nf + 1)) || !ensure_range_events()) return 0;
+  const long long nf = kDropinGrav ? 3 * (n8 + nc8) : 0, ncp = cplanes();
+  // (+ n8 bytes for the dual-energy sound-speed flags after the status word)
+  if (!ensure_pin(sizeof(double) * (11 * n8 + ncp * nc8 + nf + 2) + (size_t)n8) || !ensure_range_events()) return 0;
   double *pw = g.pin, *pb = g.pin + 5 * n8, *pc = g.pin + 11 * n8;
-  [[maybe_unused]] double *pf = pc + 5 * nc8, *pfc = pf + 3 * n8;
-  unsigned *pst = reinterpret_cast<unsigned *>(pc + 5 * nc8 + nf);
+  [[maybe_unused]] double *pf = pc + ncp * nc8, *pfc = pf + 3 * n8;
+  unsigned *pst = reinterpret_cast<unsigned *>(pc + ncp * nc8 + nf);
   const auto t1 = Clock::now();
   // upload: each host thread packs its oct range in sub-ranges (field and
   // fieldnew in one pass over the cells) and queues one pitched copy of the 11
@@ -1498,13 +1538,18 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     }
   });
   if (!copies_ok) return ck(cudaGetLastError(), "H2D level state"), 0;
+  if (d.az != nullptr) {  // dual energy: the split cells' stored sound speeds of 0
+    uint8_t *pz = reinterpret_cast<uint8_t *>(pst + 4);
+    parallel_for(h.noct, [&](long long a0, long long b0) { pack_az(h, a0, b0, pz); });
+    if (!ck(cudaMemcpyAsync(d.az, pz, (size_t)n8, cudaMemcpyHostToDevice, g.stream), "H2D az")) return 0;
+  }
   g.h2d_bytes += (long long)sizeof(double) * (11 + 3 * kDropinGrav) * n8;
   if (coarse) {
     pack_level(hc, 0, pc);
     if (!ck(cudaMemcpyAsync(dc.W0, pc, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))
       return 0;
     g.h2d_bytes += (long long)sizeof(double) * 5 * nc8;
-    if (!ck(cudaMemsetAsync(dc.C, 0, sizeof(double) * 5 * nc8, g.stream), "memset Cc")) return 0;
+    if (!ck(cudaMemsetAsync(dc.C, 0, sizeof(double) * ncp * nc8, g.stream), "memset Cc")) return 0;
   }
 #ifdef EMMA_WGRAV
   // the coarser level's accelerations, for the forces of its injected cells
@@ -1547,6 +1592,8 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   a.Fv = d.Fv;
   a.gcorr = 0;
   a.wv_inject = H.grav;
+  a.az = d.az;  // dual energy: from the caller's cells, every call
+  a.azall = nullptr;
   k_set_args<<<1, 1, 0, g.stream>>>(T.d_lv, level, a);
   if (!ck(cudaGetLastError(), "k_set_args")) return 0;
   if (!ck(launch_interp(T.d_lv, level, d.nv, nullptr, g.nsm, g.stream, H.grav != 0), "interpolation launch"))
@@ -1559,9 +1606,9 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   if (!ck(cudaMemcpyAsync(pst, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, g.stream), "D2H status"))
     return 0;
   if (coarse) {
-    if (!ck(cudaMemcpyAsync(pc, dc.C, sizeof(double) * 5 * nc8, cudaMemcpyDeviceToHost, g.stream), "D2H Cc"))
+    if (!ck(cudaMemcpyAsync(pc, dc.C, sizeof(double) * ncp * nc8, cudaMemcpyDeviceToHost, g.stream), "D2H Cc"))
       return 0;
-    g.d2h_bytes += (long long)sizeof(double) * 5 * nc8;
+    g.d2h_bytes += (long long)sizeof(double) * ncp * nc8;
   }
   const auto t3 = Clock::now();
   std::atomic<bool> wait_ok{true};
@@ -1605,20 +1652,23 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   // fine -> coarse corrections: fieldnew = U2W(W2U(fieldnew) + dU) per coarse cell
   if (coarse) {
     const double *p = pc;
+    const bool dual = g.opt.dual_energy != 0;
     for (int32_t k : h.inj_cells) {
       struct Wtype &W = hc.octs[k >> 3]->cell[k & 7].fieldnew;
-      double Ud = W.d, Udu = W.d * W.u, Udv = W.d * W.v, Udw = W.d * W.w, UE = W.E;
+      double Ud = W.d, Udu = W.d * W.u, Udv = W.d * W.v, Udw = W.d * W.w, UE = W.E, Ue = W.p / (kG - 1.);
       Ud += p[k];
       Udu += p[nc8 + k];
       Udv += p[2 * nc8 + k];
       Udw += p[3 * nc8 + k];
       UE += p[4 * nc8 + k];
+      if (dual) Ue += p[5 * nc8 + k];
       const double dl = (Ud == 0. ? 10. : Ud);
       W.d = Ud;
       W.u = Udu / dl;
       W.v = Udv / dl;
       W.w = Udw / dl;
-      W.p = (kG - 1.) * (UE - ((Udu) * (Udu) + (Udv) * (Udv) + (Udw) * (Udw)) / (dl)*0.5);
+      // U2W: the pressure from E - Ekin, or from the tracked eint (-DDUAL_E)
+      W.p = dual ? Ue * (kG - 1.) : (kG - 1.) * (UE - ((Udu) * (Udu) + (Udv) * (Udv) + (Udw) * (Udw)) / (dl)*0.5);
       W.E = UE;
       W.a = std::sqrt(kG * W.p / dl);
     }

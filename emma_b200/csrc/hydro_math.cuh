@@ -40,14 +40,16 @@ struct MathF64 {
 
   // MUSCL_BOUND2 slopes + matrix_jacobian predictor (src/hydro_utils.c:976-1189).
   // q0: cell, qm/qp: neighbours per axis.  Out: D[3][5] slopes, Wt[5] predictor.
+  // azero: the cell's stored sound speed is 0 (an averaged split cell)
   static __device__ __forceinline__ void muscl(const double q0[5], const double qm[3][5], const double qp[3][5],
-                                               double dt, double dx, double D[3][5], double Wt[5]) {
+                                               double dt, double dx, double D[3][5], double Wt[5],
+                                               bool azero = false) {
 #pragma unroll
     for (int dir = 0; dir < 3; dir++)
 #pragma unroll
       for (int k = 0; k < 5; k++) D[dir][k] = limit(q0[k] - qm[dir][k], qp[dir][k] - q0[k]);
     // stored sound speed of the cell, as U2W/scatter computes it (src/hydro_utils.c:64,3186)
-    const double a0 = sqrt(kGam * q0[4] / q0[0]);
+    const double a0 = azero ? 0. : sqrt(kGam * q0[4] / q0[0]);
     const double daa = q0[0] * a0 * a0;
     const double id = 1. / q0[0];
     double acc[5] = {0., 0., 0., 0., 0.};
@@ -239,17 +241,25 @@ struct MathF64 {
 
   // HLLC flux across a face normal to axis n (src/hydro_utils.c:2055-2138),
   // returned in x,y,z order: F = {mass, mom_x, mom_y, mom_z, energy}.
+  // du (dual-energy builds, optional): from the state Us of the branch taken (the
+  // upwind or the star state), du[0] = Us.m_n / Us.d and du[1] = ebar =
+  // Us.E - |Us.m|^2 / (2 Us.d) (src/hydro_utils.c:2126-2128).
   static __device__ __forceinline__ void hllc(const double WL[7], const double WR[7], int n, double F[5],
-                                              unsigned &st) {
+                                              unsigned &st, double *du = nullptr) {
     double SL, SR, ustar;
     speeds(WL, WR, n, SL, SR, ustar, st);
     double rL[7], rR[7], G[5] = {0., 0., 0., 0., 0.};
     rotate(WL, n, rL);
     rotate(WR, n, rR);
-    if (SL >= 0.) {
-      euler_rot(rL, G);
-    } else if (SR <= 0.) {
-      euler_rot(rR, G);
+    if (du != nullptr) du[0] = du[1] = 0.;
+    if (SL >= 0. || SR <= 0.) {
+      const double *r = (SL >= 0.) ? rL : rR;
+      euler_rot(r, G);
+      if (du != nullptr) {  // Us = W2U of the upwind face state
+        const double mn = r[0] * r[1];
+        du[0] = mn / r[0];
+        du[1] = (r[5] - 0.5 * r[6] / r[0]);
+      }
     } else {
       const bool left = (SL < 0.) && (ustar >= 0.);
       const bool right = (ustar <= 0.) && (SR > 0.);
@@ -259,11 +269,18 @@ struct MathF64 {
         euler_rot(r, G);
         const double d = r[0], un = r[1], E = r[5];
         const double fact = d * (S - un) / (S - ustar);
+        const double Es = (E / d + (ustar - un) * (ustar + r[4] / (d * (S - un))));
         G[0] += (fact * 1. - d) * S;
         G[1] += (fact * ustar - d * un) * S;
         G[2] += (fact * r[2] - d * r[2]) * S;
         G[3] += (fact * r[3] - d * r[3]) * S;
-        G[4] += (fact * (E / d + (ustar - un) * (ustar + r[4] / (d * (S - un)))) - E) * S;
+        G[4] += (fact * Es - E) * S;
+        if (du != nullptr) {  // the star state: momenta in x,y,z order for the sum of squares
+          const double ds = fact * 1., mn = fact * ustar, m1 = fact * r[2], m2 = fact * r[3];
+          const double mm = (n == 2) ? ((m1 * m1 + m2 * m2) + mn * mn) : ((mn * mn + m1 * m1) + m2 * m2);
+          du[0] = mn / ds;
+          du[1] = (fact * Es - 0.5 * mm / ds);
+        }
       }
     }
     F[0] = G[0];
@@ -290,13 +307,13 @@ struct MathF32 {
   }
 
   static __device__ __forceinline__ void muscl(const float q0[5], const float qm[3][5], const float qp[3][5],
-                                               float dtdx_half, float D[3][5], float Wt[5]) {
+                                               float dtdx_half, float D[3][5], float Wt[5], bool azero = false) {
 #pragma unroll
     for (int dir = 0; dir < 3; dir++)
 #pragma unroll
       for (int k = 0; k < 5; k++) D[dir][k] = limit(q0[k] - qm[dir][k], qp[dir][k] - q0[k]);
     const float id = rcp(q0[0]);
-    const float gp = G * q0[4];  // d a^2
+    const float gp = azero ? 0.f : G * q0[4];  // d a^2
     float acc0 = q0[1] * D[0][0] + q0[0] * D[0][1] + q0[2] * D[1][0] + q0[0] * D[1][2] + q0[3] * D[2][0] + q0[0] * D[2][3];
     float acc1 = q0[1] * D[0][1] + id * D[0][4] + q0[2] * D[1][1] + q0[3] * D[2][1];
     float acc2 = q0[1] * D[0][2] + q0[2] * D[1][2] + id * D[1][4] + q0[3] * D[2][2];
@@ -360,7 +377,12 @@ struct MathF32 {
   }
 
   // HLLC flux across a face normal to axis n; states W = {d,u,v,w,p,1/d,a}.
-  static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st) {
+  // du (dual-energy builds, optional): the upwind or star state's normal velocity
+  // and ebar = Us.E - |Us.m|^2 / (2 Us.d), the latter in a form free of the
+  // E - Ekin cancellation: p/(g-1) upwind, fact (p/((g-1) d) + (u*-u)((u*-u)/2 +
+  // p/(d (S-u)))) in the star region (algebraically the reference's expression).
+  static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st,
+                                              float *du = nullptr) {
     const float dL = WL[0], pL = WL[4], iL = WL[5], aL = WL[6];
     const float dR = WR[0], pR = WR[4], iR = WR[5], aR = WR[6];
     const float uL = (n == 0) ? WL[1] : ((n == 1) ? WL[2] : WL[3]);
@@ -425,6 +447,12 @@ struct MathF32 {
       G1 = side ? H1 : 0.f;
       G2 = side ? H2 : 0.f;
       G4 = side ? H4 : 0.f;
+    }
+    if (du != nullptr) {
+      const float ig = 1.f / (G - 1.f), dd = ustar - un;
+      const float es = fact * (p * ig * id + dd * (0.5f * dd + fdiv(p, d * Smu)));
+      du[0] = star ? (side ? ustar : 0.f) : un;
+      du[1] = star ? (side ? es : 0.f) : p * ig;
     }
     F[0] = G0;
     F[1] = (n == 0) ? GN : G1;

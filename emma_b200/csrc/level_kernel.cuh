@@ -67,6 +67,7 @@ __constant__ uint8_t c_mirror[6][8] = {
 
 // cell flags of the staged box (kFInterp: the slot reads the interpolated coarse cells)
 constexpr uint8_t kFPresent = 1, kFSplit = 2, kFTile = 4, kFInj = 8, kFInterp = 16;
+constexpr uint8_t kFAzero = 32;  // dual energy: a split cell whose stored sound speed is 0
 __device__ __forceinline__ bool f_ok(uint8_t f) { return (f & (kFPresent | kFSplit)) == kFPresent; }
 __device__ __forceinline__ bool f_tileleaf(uint8_t f) {
   return (f & (kFPresent | kFSplit | kFTile)) == (kFPresent | kFTile);
@@ -161,8 +162,9 @@ __device__ __forceinline__ void slot_tables(unsigned char *tab) {
   }
 }
 
-// Shared memory of one tile, after the slot tables.
-template <class M, class G>
+// Shared memory of one tile, after the slot tables.  DUAL: dual-energy builds add
+// the internal-energy flux and the normal star velocity of every face.
+template <class M, class G, bool DUAL = false>
 struct TileSmem {
   using R = typename M::R;
   static constexpr bool kF64 = sizeof(R) == 8;
@@ -192,7 +194,9 @@ struct TileSmem {
   // face fluxes reuse the staged box, dead after reconstruction
   static constexpr size_t off_F = off_W;                               // R4 [NF]
   static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
-  static constexpr size_t bytes = off_end;
+  static constexpr size_t off_F5 = off_end;                       // R [NF] (DUAL)
+  static constexpr size_t off_S = a16(off_F5 + sizeof(R) * NF);  // R [NF] (DUAL)
+  static constexpr size_t bytes = DUAL ? a16(off_S + sizeof(R) * NF) : off_end;
   static_assert(off_F1 + sizeof(R) * NF <= off_M, "face fluxes must fit in the staged box");
   // FP64 gravity kicks of the brick cells during P2/P3: R [3][kThreads] at the end of
   // the staged box, after the face fluxes
@@ -205,12 +209,12 @@ struct TileSmem {
 // the next tile's slot descriptors (next_tile >= 0: same level) are loaded
 // while this tile is reconstructed and solved, into the other descriptor
 // buffer; `cur`/`have` track which buffer holds the current tile's.
-template <class M, class G, bool GRAV>
+template <class M, class G, bool GRAV, bool DUAL>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
                                            const int next_tile, unsigned char *smem, const unsigned char *tab,
                                            unsigned &st, int &cur, bool &have, int &args_slot) {
   using R = typename M::R;
-  using SM = TileSmem<M, G>;
+  using SM = TileSmem<M, G, DUAL>;
   constexpr bool F64 = SM::kF64;
   constexpr int NS = SM::NS, NRING = SM::NRING;
   using V = Q4<R>;
@@ -230,6 +234,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   R *sHS = reinterpret_cast<R *>(smem + SM::off_HS);
   R *sF = reinterpret_cast<R *>(smem + SM::off_F);
   R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
+  R *sF5 = reinterpret_cast<R *>(smem + SM::off_F5);
+  R *sS = reinterpret_cast<R *>(smem + SM::off_S);
+  // cells whose face states are built: leaves; dual-energy builds also split cells,
+  // whose faces enter the p div(u) term (src/hydro_utils.c:2126-2129 sum every face)
+  auto recon_ok = [](uint8_t f) { return DUAL ? (f & kFPresent) != 0 : f_ok(f); };
 
   const int tid = threadIdx.x;
   // the level's arguments in shared memory, read again only when the level changes
@@ -368,7 +377,20 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       sWp[b0] = (R)x0[4];
       sWp[b0 + 1] = (R)x1[4];
       const uint8_t spm = sSpm[sg];
-      const uint8_t f0 = sf | (((spm >> c0) & 1) ? kFSplit : 0), f1 = sf | (((spm >> (c0 + 1)) & 1) ? kFSplit : 0);
+      uint8_t f0 = sf | (((spm >> c0) & 1) ? kFSplit : 0), f1 = sf | (((spm >> (c0 + 1)) & 1) ? kFSplit : 0);
+      if constexpr (DUAL) {
+        // split cells of the level whose stored sound speed is 0
+        if (cmk != 1 && !(sf & kFInterp) && ((f0 | f1) & kFSplit)) {
+          const bool all = A.azall != nullptr && *A.azall != 0;
+          unsigned code = (unsigned)q | (1u << 3);
+          if (cmk >= 2) code = (mir >> (4 * (cmk - 2))) & 15u;
+          const long long ib = (long long)sOb[sg] + 2 * (code & 3);
+          const bool a0 = all || (A.az != nullptr && A.az[ib + ((code >> 2) & 1)]);
+          const bool a1 = all || (A.az != nullptr && A.az[ib + ((code >> 3) & 1)]);
+          if ((f0 & kFSplit) && a0) f0 |= kFAzero;
+          if ((f1 & kFSplit) && a1) f1 |= kFAzero;
+        }
+      }
       sSt[b0] = f0;
       sSt[b0 + 1] = f1;
     }
@@ -419,7 +441,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     if (w < kThreads) {
       const uint8_t f = sSt[tb];
       need = f_tileleaf(f);
-      if (!need && f_ok(f))
+      if (!need && recon_ok(f))
         need = f_tileleaf(sSt[tb - 1]) || f_tileleaf(sSt[tb + 1]) || f_tileleaf(sSt[tb - G::XX]) ||
                f_tileleaf(sSt[tb + G::XX]) || f_tileleaf(sSt[tb - G::XS]) || f_tileleaf(sSt[tb + G::XS]);
       if constexpr (F64) {  // the centre state, for the face states and the update
@@ -435,7 +457,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       G::ring_cell(r - nb * G::kRing, b, k, bin);
       b += nb * G::kBox;
       bin += nb * G::kBox;
-      need = f_ok(sSt[b]) && f_tileleaf(sSt[bin]);
+      need = recon_ok(sSt[b]) && f_tileleaf(sSt[bin]);
     }
     if (!need) continue;
     R q0[5], qm[3][5], qp[3][5], D[3][5], Wt[5], X[5];
@@ -446,8 +468,9 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     q_at(b + G::XX, qp[1]);
     q_at(b - G::XS, qm[2]);
     q_at(b + G::XS, qp[2]);
-    if constexpr (F64) M::muscl(q0, qm, qp, A.dt, A.dx, D, Wt);
-    else M::muscl(q0, qm, qp, (R)(A.dt / A.dx * 0.5), D, Wt);
+    const bool azero = DUAL && (sSt[b] & kFAzero);
+    if constexpr (F64) M::muscl(q0, qm, qp, A.dt, A.dx, D, Wt, azero);
+    else M::muscl(q0, qm, qp, (R)(A.dt / A.dx * 0.5), D, Wt, azero);
     // X = W0 + Wt (FP32 path) or Wt (FP64 path, which adds W0 in the reference's order)
 #pragma unroll
     for (int v = 0; v < 5; v++) X[v] = F64 ? Wt[v] : q0[v] + Wt[v];
@@ -532,6 +555,33 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
   };
 
+  // One face e normal to axis d between left (brick cell tL at box cell bL, or
+  // ring face jL) and right; the flux is zero across a split cell, and without a
+  // leaf of the tile on either side the face is not solved.
+  auto solve_face = [&](int d, int e, int tL, int bL, int jL, int tR, int bR, int jR) {
+    const uint8_t fL = sSt[bL], fR = sSt[bR];
+    R F[5] = {0, 0, 0, 0, 0}, du[2] = {0, 0};
+    if ((f_tileleaf(fL) || f_tileleaf(fR)) && recon_ok(fL) && recon_ok(fR)) {
+      R WL[7], WR[7];
+      if (jL >= 0) ring_face(jL, WL);
+      else brick_face(tL, bL, 2 * d + 1, WL);
+      if (jR >= 0) ring_face(jR, WR);
+      else brick_face(tR, bR, 2 * d, WR);
+      M::hllc(WL, WR, d, F, st, DUAL ? du : nullptr);
+      if (DUAL && !(f_ok(fL) && f_ok(fR))) {
+#pragma unroll
+        for (int v = 0; v < 5; v++) F[v] = (R)0;
+        du[1] = (R)0;  // the internal-energy flux is cancelled too; u* stays for div(u)
+      }
+    }
+    V::st(sF, e, F[0], F[1], F[2], F[3]);
+    sF1[e] = F[4];
+    if constexpr (DUAL) {
+      sF5[e] = du[0] * du[1];  // (Us.m_n / Us.d) ebar (src/hydro_utils.c:2128)
+      sS[e] = du[0];
+    }
+  };
+
   // ------------------------------------------------------------------ P2
   // FP32: per axis d (a compile-time constant, so the solver's axis selects fold): the
   // -d face of every brick cell, then the +d faces on the brick boundaries,
@@ -575,18 +625,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         jR = nb * G::kRing + G::ring_index(d, true, x, y, z);
         e = nb * G::kFaces + G::face_index(d, x + (d == 0), y + (d == 1), z + (d == 2));
       }
-      const uint8_t fL = sSt[bL], fR = sSt[bR];
-      R F[5] = {0, 0, 0, 0, 0};
-      if ((f_tileleaf(fL) || f_tileleaf(fR)) && f_ok(fL) && f_ok(fR)) {
-        R WL[7], WR[7];
-        if (jL >= 0) ring_face(jL, WL);
-        else brick_face(tL, bL, 2 * d + 1, WL);
-        if (jR >= 0) ring_face(jR, WR);
-        else brick_face(tR, bR, 2 * d, WR);
-        M::hllc(WL, WR, d, F, st);
-      }
-      V::st(sF, e, F[0], F[1], F[2], F[3]);
-      sF1[e] = F[4];
+      solve_face(d, e, tL, bL, jL, tR, bR, jR);
     }
   };
   if constexpr (!F64) {
@@ -631,18 +670,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         jR = nb * G::kRing + G::ring_index(d, true, x, y, z);
         e = nb * G::kFaces + G::face_index(d, x + (d == 0), y + (d == 1), z + (d == 2));
       }
-      const uint8_t fL = sSt[bL], fR = sSt[bR];
-      R F[5] = {0, 0, 0, 0, 0};
-      if ((f_tileleaf(fL) || f_tileleaf(fR)) && f_ok(fL) && f_ok(fR)) {
-        R WL[7], WR[7];
-        if (jL >= 0) ring_face(jL, WL);
-        else brick_face(tL, bL, 2 * d + 1, WL);
-        if (jR >= 0) ring_face(jR, WR);
-        else brick_face(tR, bR, 2 * d, WR);
-        M::hllc(WL, WR, d, F, st);
-      }
-      V::st(sF, e, F[0], F[1], F[2], F[3]);
-      sF1[e] = F[4];
+      solve_face(d, e, tL, bL, jL, tR, bR, jR);
     }
   }
   __syncthreads();
@@ -715,7 +743,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         F[3] = (double)f3;
         F[4] = (double)sF1[e];
       };
+      auto face_of = [&](int k) {
+        return (k < 2) ? (ex + (k & 1)) : ((k < 4) ? (ey + G::CX * (k & 1)) : (ez + G::CX * G::CY * (k & 1)));
+      };
       double Ud, Udu, Udv, Udw, UE;
+      double Ue = 0.;  // dual energy: the tracked internal energy of the base state
       if (A.B != nullptr) {  // drop-in: W2U of the caller's fieldnew
         const double bd = A.B[gi];
         Ud = bd;
@@ -723,12 +755,33 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         Udv = bd * A.B[2 * N8 + gi];
         Udw = bd * A.B[3 * N8 + gi];
         UE = A.B[5 * N8 + gi];
+        if constexpr (DUAL) Ue = A.B[4 * N8 + gi] / (kGam - 1.);
       } else {  // resident: W2U(field) + corrections received from the finer level
         Ud = q[0];
         Udu = q[0] * q[1];
         Udv = q[0] * q[2];
         Udw = q[0] * q[3];
         UE = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        if constexpr (DUAL) {
+          Ue = q[4] / (kGam - 1.);
+          if (A.C != nullptr) Ue += __ldcg(A.C + 5 * N8 + gi);
+        }
+      }
+      // dual energy (src/hydro_utils.c:2126-2129, 3064, 3167-3177): the internal-energy
+      // flux divergence and the p div(u) term, summed over the faces in the
+      // reference's order (x-, x+, y-, y+, z-, z+), eold the cell's old eint
+      double dUe = 0., divu = 0.;
+      if constexpr (DUAL) {
+        const double eold = q[4] / (kGam - 1.);
+        double one = 1.;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          const int e = face_of(k);
+          dUe += (double)sF5[e] * dtsurdx * one;
+          const double dl = (kGam - 1.) * (double)sS[e] * eold;
+          divu += (k & 1) ? dl : -dl;
+          one *= -1.;
+        }
       }
       if constexpr (F64) {
         // updatefield (src/hydro_utils.c:3050-3082): dU = sum over faces -x,+x,-y,+y,-z,+z
@@ -800,6 +853,16 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         Wout[3] = Udw * inv;
         Wout[4] = (kGam - 1.) * (UE - (Udu * Udu + Udv * Udv + Udw * Udw) * inv * 0.5);
       }
+      if constexpr (DUAL) {
+        // the tracked eint, unless E - Ekin is well resolved against div(u); the
+        // floor; the pressure from eint (src/hydro_utils.c:3164-3182, 45-46)
+        const double ekin = 0.5 * (Udu * Udu + Udv * Udv + Udw * Udw) / Ud;
+        double eint = Ue + dUe;
+        eint = eint + (-divu * dtsurdx);
+        if ((UE - ekin) > 0.5 * (divu * divu)) eint = UE - ekin;
+        eint = fmax(eint * (kGam - 1.), kPmin) / (kGam - 1.);
+        Wout[4] = eint * (kGam - 1.);
+      }
       Wout[4] = fmax(Wout[4], kPmin);
       if (isnan(Wout[1]) || isnan(Wout[4]) || isnan(Wout[0])) st |= kStNan;
       // grav_correction (src/hydro_utils.c:2388-2444, PRIMITIVE): full-step kick of the
@@ -824,6 +887,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         flux5(k, F);
 #pragma unroll
         for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, F[v] * dtsurdx * one * 0.125);
+        if constexpr (DUAL) atomicAdd(A.Cc + 5 * A.nc8 + cc, (double)sF5[face_of(k)] * dtsurdx * one * 0.125);
       }
     }
 #pragma unroll
@@ -855,9 +919,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 
 // Bytes of dynamic shared memory of a kernel handling the shapes in `shapes`
 // (bit i: kShapes[i]).
-template <class M>
+template <class M, bool DUAL = false>
 constexpr size_t level_smem_bytes(unsigned shapes) {
-  const size_t a = (shapes & 1u) ? TileSmem<M, GeomA>::bytes : 0, b = (shapes & 2u) ? TileSmem<M, GeomB>::bytes : 0;
+  const size_t a = (shapes & 1u) ? TileSmem<M, GeomA, DUAL>::bytes : 0,
+               b = (shapes & 2u) ? TileSmem<M, GeomB, DUAL>::bytes : 0;
   return a > b ? a : b;
 }
 
@@ -870,15 +935,19 @@ constexpr size_t level_smem_bytes(unsigned shapes) {
 // (64 registers, 55 KB of shared memory); with 2x2x2 bricks shared memory
 // allows 2; the FP64 kernel 2 with 4x4x2 bricks (128 registers, 110 KB), 1 with
 // 2x2x2 bricks.
-template <class M, unsigned SHAPES>
-constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? (SHAPES == 1u ? 2 : 1) : (SHAPES == 1u ? 4 : 2);
+template <class M, unsigned SHAPES, bool DUAL = false>
+constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? ((SHAPES == 1u && !DUAL) ? 2 : 1)
+                                                         : (SHAPES == 1u ? (DUAL ? 3 : 4) : 2);
 // 228 KB of shared memory per SM, 1 KB reserved per CTA
 static_assert(4 * (TileSmem<MathF32, GeomA>::bytes + 1024) <= 228 * 1024, "4 FP32 4x4x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF32, GeomB>::bytes + 1024) <= 228 * 1024, "2 FP32 2x2x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF64, GeomA>::bytes + 1024) <= 228 * 1024, "2 FP64 4x4x2 CTAs per SM");
+static_assert(3 * (TileSmem<MathF32, GeomA, true>::bytes + 1024) <= 228 * 1024, "3 dual-energy FP32 4x4x2 CTAs");
+static_assert(2 * (TileSmem<MathF32, GeomB, true>::bytes + 1024) <= 228 * 1024, "2 dual-energy FP32 2x2x2 CTAs");
+static_assert(TileSmem<MathF64, GeomB, true>::bytes + 1024 <= 227 * 1024, "a dual-energy FP64 2x2x2 CTA");
 
-template <class M, unsigned SHAPES, bool GRAV>
-__global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch_kernel(const BatchArgs Bt) {
+template <class M, unsigned SHAPES, bool GRAV, bool DUAL>
+__global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL>)) level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
   if constexpr ((SHAPES & 1u) != 0) slot_tables<GeomA>(smem);
@@ -901,14 +970,14 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES>)) level_batch
     }
     const LevelArgs *gA = Bt.lv + slot;
     if constexpr (SHAPES == 1u) {
-      level_tile<M, GeomA, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+      level_tile<M, GeomA, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
     } else if constexpr (SHAPES == 2u) {
-      level_tile<M, GeomB, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
+      level_tile<M, GeomB, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
     } else {
       if (gA->shape == 0)
-        level_tile<M, GeomA, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+        level_tile<M, GeomA, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
       else
-        level_tile<M, GeomB, GRAV>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
+        level_tile<M, GeomB, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
     }
     __syncthreads();
   }
@@ -930,11 +999,11 @@ namespace {
 
 // Launch of a work list on a persistent grid of ctas_per_sm CTAs per SM (0 or
 // above the occupancy limit: the limit), so that every CTA is co-resident.
-template <class M, unsigned SHAPES, bool GRAV>
+template <class M, unsigned SHAPES, bool GRAV, bool DUAL>
 cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cudaStream_t s, int *occupancy) {
   static int occ = 0;
-  auto k = level_batch_kernel<M, SHAPES, GRAV>;
-  constexpr size_t bytes = level_smem_bytes<M>(SHAPES);
+  auto k = level_batch_kernel<M, SHAPES, GRAV, DUAL>;
+  constexpr size_t bytes = level_smem_bytes<M, DUAL>(SHAPES);
   if (occ == 0) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
@@ -954,13 +1023,20 @@ cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cu
 template <class M>
 cudaError_t launch_level_any(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
                              int *occupancy) {
+  constexpr unsigned G = kLaunchGrav, D = kLaunchDual;
   switch (shapes) {
-    case 1u: return launch_level_shapes<M, 1u, false>(a, nsm, ctas_per_sm, s, occupancy);
-    case 2u: return launch_level_shapes<M, 2u, false>(a, nsm, ctas_per_sm, s, occupancy);
-    case 3u: return launch_level_shapes<M, 3u, false>(a, nsm, ctas_per_sm, s, occupancy);
-    case 1u | kLaunchGrav: return launch_level_shapes<M, 1u, true>(a, nsm, ctas_per_sm, s, occupancy);
-    case 2u | kLaunchGrav: return launch_level_shapes<M, 2u, true>(a, nsm, ctas_per_sm, s, occupancy);
-    case 3u | kLaunchGrav: return launch_level_shapes<M, 3u, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u: return launch_level_shapes<M, 1u, false, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u: return launch_level_shapes<M, 2u, false, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u: return launch_level_shapes<M, 3u, false, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u | G: return launch_level_shapes<M, 1u, true, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u | G: return launch_level_shapes<M, 2u, true, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u | G: return launch_level_shapes<M, 3u, true, false>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u | D: return launch_level_shapes<M, 1u, false, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u | D: return launch_level_shapes<M, 2u, false, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u | D: return launch_level_shapes<M, 3u, false, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u | G | D: return launch_level_shapes<M, 1u, true, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u | G | D: return launch_level_shapes<M, 2u, true, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u | G | D: return launch_level_shapes<M, 3u, true, true>(a, nsm, ctas_per_sm, s, occupancy);
     default: return cudaErrorInvalidValue;
   }
 }

@@ -235,6 +235,8 @@ bool check_brick(Planner &P, int L, const Box &G, const uint32_t *keys, uint32_t
       fl[b] = f;
     }
   }
+  // cells whose face states the kernel builds (dual energy: split cells too)
+  auto recon = [&](uint8_t f) { return P.H.dual ? (f & kFPresent) != 0 : f_ok(f); };
   auto all_nbrs = [&](int b) {
     for (int a = 0; a < 3; a++)
       if (!(fl[b - G.stride(a)] & kFPresent) || !(fl[b + G.stride(a)] & kFPresent)) return false;
@@ -254,7 +256,7 @@ bool check_brick(Planner &P, int L, const Box &G, const uint32_t *keys, uint32_t
         bool near = f_tileleaf(fl[b]);
         for (int a = 0; a < 3; a++)
           near = near || f_tileleaf(fl[b - G.stride(a)]) || f_tileleaf(fl[b + G.stride(a)]);
-        if (f_ok(fl[b]) && near && !all_nbrs(b)) return fail("unstaged neighbour of a reconstructed cell");
+        if (recon(fl[b]) && near && !all_nbrs(b)) return fail("unstaged neighbour of a reconstructed cell");
         if (!f_tileleaf(fl[b])) continue;
         for (int a = 0; a < 3; a++)
           for (int sgn = -1; sgn <= 1; sgn += 2) {
@@ -277,7 +279,7 @@ bool check_brick(Planner &P, int L, const Box &G, const uint32_t *keys, uint32_t
         if (!ix) bin = b + (x < x0 ? 1 : -1);
         if (!iy) bin = b + (y < y0 ? G.xx : -G.xx);
         if (!iz) bin = b + (z < z0 ? G.xx * G.xy : -G.xx * G.xy);
-        if (f_ok(fl[b]) && f_tileleaf(fl[bin]) && !all_nbrs(b)) return fail("unstaged neighbour of a ring cell");
+        if (recon(fl[b]) && f_tileleaf(fl[bin]) && !all_nbrs(b)) return fail("unstaged neighbour of a ring cell");
       }
   return true;
 }
@@ -427,8 +429,9 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
 int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string &err);
 
 int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int trans, int plan_lo, int plan_hi,
-                    HostTree &H, std::string &err, const int *shapes, int grav) {
+                    HostTree &H, std::string &err, const int *shapes, int grav, int dual) {
   H = HostTree();
+  H.dual = dual ? 1 : 0;
   if (grav && trans) {
     err = "gravity coupling with transmissive boundaries is not supported";
     return EMMA_ST_ARG;

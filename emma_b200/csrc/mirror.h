@@ -28,6 +28,7 @@ struct HostLevel {
 struct HostTree {
   int lcoarse = 0, lmax = 0, rank = 0, trans = 0;
   int grav = 0;  // gravity coupling: injected coarser cells carry interpolated forces
+  int dual = 0;  // dual energy: split cells next to a leaf are reconstructed too (their faces enter div u)
   std::vector<HostLevel> lev;  // indexed by level (0..lmax)
 };
 
@@ -37,9 +38,10 @@ struct HostTree {
 // shapes (optional, indexed by level): brick shape of each plan, -1 = the
 // cheaper by tile count x tile cost.  grav: gravity-coupled build (every
 // injected coarser cell gets an interpolation entry for its force; not
-// combined with transmissive boundaries).
+// combined with transmissive boundaries).  dual: dual-energy build (the planner
+// checks the kernel's reconstruction rule of that build).
 int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int trans, int plan_lo, int plan_hi,
-                    HostTree &H, std::string &err, const int *shapes = nullptr, int grav = 0);
+                    HostTree &H, std::string &err, const int *shapes = nullptr, int grav = 0, int dual = 0);
 
 // Re-plan level L of a built tree with brick shape `shape` (the autotuner's
 // candidates); validates the new plan.

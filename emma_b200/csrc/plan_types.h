@@ -40,6 +40,8 @@ constexpr int kNumShapes = 2;
 // Launch flag beside the shape bits of a level-kernel launch: the gravity-coupled
 // variant (levels with accelerations); the plain variant has no gravity code.
 constexpr unsigned kLaunchGrav = 4u;
+// ... and the dual-energy variant (-DDUAL_E: tracked internal energy, 6 correction planes).
+constexpr unsigned kLaunchDual = 8u;
 constexpr BrickShape kShapes[kNumShapes] = {{4, 4, 2, 1}, {2, 2, 2, 4}};
 static_assert(kShapes[0].nb * 8 * kShapes[0].octs() == kThreads, "one thread per brick cell");
 static_assert(kShapes[1].nb * 8 * kShapes[1].octs() == kThreads, "one thread per brick cell");
@@ -90,6 +92,11 @@ struct LevelArgs {
   int gcorr;          // apply grav_correction (src/hydro_utils.c:2388-2444) to the new state
   int wv_inject;      // the interpolation list fills Wv by injection (gravity build), not by
                       // limited-slope interpolation (transmissive build)
+  // dual energy: split cells whose stored sound speed is 0 (the reference's
+  // averaging leaves a = 0, src/hydro_utils.c:3417-3481, and its predictor reads the
+  // stored a, :976-1120): per cell, or every split cell once *azall != 0
+  const uint8_t *az;
+  const int *azall;
 };
 
 // A launch of the level kernel: a list of (level slot, tile) work items,

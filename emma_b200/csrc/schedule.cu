@@ -112,6 +112,7 @@ __global__ void k_batch_end(SchedState *S, LevelArgs *lv) {
     S->updates += lv[L].leaf;
     S->fresh[L] = 1;
     S->stale[L] = 0;
+    S->azall[L] = 1;
   }
   S->tsim += S->adt[lc - 1];
 }
@@ -177,6 +178,7 @@ __global__ void k_sub_end(SchedState *S, LevelArgs *lv, int L) {
   S->updates += lv[L].leaf;
   S->fresh[L] = 1;
   S->stale[L] = 0;
+  S->azall[L] = 1;
 }
 
 __global__ void k_sub_final(SchedState *S) { S->tsim += S->adt[S->lcoarse - 1]; }

@@ -16,6 +16,8 @@ struct SchedState {
   int stale[kMaxLevels];                // !fresh: the state was set from the host (smax is then
                                         // zeroed with it, for the reduction kernel)
   int cfl_gate[kMaxLevels];             // subcycled iteration: active and stale
+  int azall[kMaxLevels];                // the level was updated since its state was set: every
+                                        // split cell holds the averaged state (sound speed 0)
   double dtacc[kMaxLevels];             // dt accumulated by the current Advance_level(L) call
   double tloc[kMaxLevels];              // its local time
   int is[kMaxLevels];                   // its iteration count

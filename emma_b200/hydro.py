@@ -12,16 +12,18 @@ import numpy as np
 from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
-def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0, gravity=False):
+def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0, gravity=False,
+            dual=False):
     """tile_octs: 0 = brick shape autotuned per level at upload, 32 = 4x4x2-oct
     bricks, 8 = 2x2x2-oct bricks (four per tile).  gravity: the -DWGRAV coupling
-    (forces from ResidentHydro.set_force)."""
+    (forces from ResidentHydro.set_force).  dual: the -DDUAL_E tracked internal energy."""
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
     o.use_graph = 1 if use_graph else 0
     o.tile_octs = tile_octs
     o.gravity = 1 if gravity else 0
+    o.dual_energy = 1 if dual else 0
     return o
 
 
@@ -29,14 +31,14 @@ class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
     def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0,
-                 gravity=False):
+                 gravity=False, dual=False):
         self.tree = tree
-        self.gravity = gravity
+        self.gravity, self.dual = gravity, dual
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
         self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
         self.precision = precision
         L = lib()
-        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity)
+        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity, dual=dual)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
         check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
         L.emma_hydro_clear_status()
@@ -49,13 +51,13 @@ class ResidentHydro:
         (the resident tree and its tuned plans stay)."""
         self.use_graph = use_graph
         o = options(self.precision, self.trans, self.cfl, use_graph=use_graph, tile_octs=self.tile_octs,
-                    gravity=self.gravity)
+                    gravity=self.gravity, dual=self.dual)
         check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def set_precision(self, precision):
         self.precision = precision
         o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
-                    gravity=self.gravity)
+                    gravity=self.gravity, dual=self.dual)
         check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):

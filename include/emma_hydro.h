@@ -68,6 +68,11 @@ struct EmmaHydroOptions {
                            level update (src/hydro_utils.c:2388, called at
                            src/advanceamr.c:999); the accelerations f come from
                            emma_hydro_set_level_force.  Not with trans_flags. */
+  int dual_energy;      /* the reference's -DDUAL_E build (its production default,
+                           init/param_init.mk): the internal energy is tracked with its
+                           flux and a p div(u) term, and the pressure comes from it unless
+                           E - Ekin is resolved (src/hydro_utils.c:45-49, 2126-2129,
+                           3164-3182).  Drop-in and resident modes. */
 };
 void emma_hydro_default_options(struct EmmaHydroOptions *opt);
 
