@@ -168,7 +168,8 @@ def run_mine(args, rank, world):
     results = {}
     for prec_name, prec in (("fp64", PREC_FP64), ("mixed", PREC_MIXED)):
         # whole coarse steps: CUDA graph with the device-side level schedule
-        r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=True, gravity=args.gravity)
+        r = ResidentHydro(tree, precision=prec, trans=cfg.trans, cfl=cfg.cfl, use_graph=True, gravity=args.gravity,
+                          dual=args.dual)
         if args.gravity:
             for l in levels:
                 r.set_force(l, *synthetic_force(tree, l))
@@ -293,7 +294,7 @@ def run_dropin(args, L, cfg, tree, levels, dts, world):
     import torch
     from emma_b200 import PREC_MIXED
     from emma_b200.hydro import options, clean_new_hydro, HydroSolver
-    o = options(PREC_MIXED, cfg.trans, cfg.cfl)
+    o = options(PREC_MIXED, cfg.trans, cfg.cfl, dual=args.dual)
     L.emma_hydro_set_options(ctypes.byref(o))
     order = sorted(levels, reverse=True)
     leaf = sum(int((~tree.split_mask(l)).sum()) for l in order)
@@ -407,6 +408,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gravity", action="store_true",
                     help="gravity-coupled hydro (-DWGRAV) with a smooth synthetic acceleration field")
+    ap.add_argument("--dual", action="store_true", help="dual-energy hydro (-DDUAL_E)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -452,7 +454,7 @@ def main():
                    "precision": "mixed (FP32 reconstruction/HLLC, FP64 compensated update)",
                    "l2": "flushed between steps (256 MiB write)" if flushed else "state larger than L2",
                    "parallelism": f"replicas x{world}", "cfl": cfg.cfl, "nsub": cfg.nsub,
-                   "gravity": bool(args.gravity)},
+                   "gravity": bool(args.gravity), "dual_energy": bool(args.dual)},
         "fp64": {"value": value_fp64, "unit": "cell-updates/s", "ms_per_step": ms_f / args.steps,
                  "roofline_frac": achieved_f / peak, "status": fp64["status"]},
         "mixed_over_fp64": value / value_fp64,
