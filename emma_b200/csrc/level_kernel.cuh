@@ -28,15 +28,18 @@
 namespace emma {
 
 // 4-wide shared-memory groups: one 128-bit access per group for FP32 (float4),
-// two for FP64 (double2 pairs).
+// two for FP64 (double2 pairs).  Element i of arrays of n groups (n a compile-time
+// constant at every call site; consecutive arrays of n groups each may follow):
+// FP32 stores the 4 values together; FP64 stores (x,y) and (z,w) in two planes of
+// n double2 each, so that consecutive threads touch consecutive 16-byte words.
 template <class R>
 struct Q4;
 template <>
 struct Q4<float> {
-  static __device__ __forceinline__ void st(float *b, int i, float x, float y, float z, float w) {
+  static __device__ __forceinline__ void st(float *b, int i, int, float x, float y, float z, float w) {
     reinterpret_cast<float4 *>(b)[i] = make_float4(x, y, z, w);
   }
-  static __device__ __forceinline__ void ld(const float *b, int i, float &x, float &y, float &z, float &w) {
+  static __device__ __forceinline__ void ld(const float *b, int i, int, float &x, float &y, float &z, float &w) {
     const float4 v = reinterpret_cast<const float4 *>(b)[i];
     x = v.x;
     y = v.y;
@@ -46,13 +49,18 @@ struct Q4<float> {
 };
 template <>
 struct Q4<double> {
-  static __device__ __forceinline__ void st(double *b, int i, double x, double y, double z, double w) {
-    reinterpret_cast<double2 *>(b)[2 * i] = make_double2(x, y);
-    reinterpret_cast<double2 *>(b)[2 * i + 1] = make_double2(z, w);
+  static __device__ __forceinline__ void st(double *b, int i, int n, double x, double y, double z, double w) {
+    const int g = i / n, j = i - g * n;
+    double2 *p = reinterpret_cast<double2 *>(b) + 2 * n * g;
+    p[j] = make_double2(x, y);
+    p[n + j] = make_double2(z, w);
   }
-  static __device__ __forceinline__ void ld(const double *b, int i, double &x, double &y, double &z, double &w) {
-    const double2 a = reinterpret_cast<const double2 *>(b)[2 * i];
-    const double2 c = reinterpret_cast<const double2 *>(b)[2 * i + 1];
+  static __device__ __forceinline__ void ld(const double *b, int i, int n, double &x, double &y, double &z,
+                                            double &w) {
+    const int g = i / n, j = i - g * n;
+    const double2 *p = reinterpret_cast<const double2 *>(b) + 2 * n * g;
+    const double2 a = p[j];
+    const double2 c = p[n + j];
     x = a.x;
     y = a.y;
     z = c.x;
@@ -372,8 +380,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
           x1[v] = e1 ? x.y : x.x;
         }
       }
-      V::st(sW, b0, (R)x0[0], (R)x0[1], (R)x0[2], (R)x0[3]);
-      V::st(sW, b0 + 1, (R)x1[0], (R)x1[1], (R)x1[2], (R)x1[3]);
+      V::st(sW, b0, SM::NBOX, (R)x0[0], (R)x0[1], (R)x0[2], (R)x0[3]);
+      V::st(sW, b0 + 1, SM::NBOX, (R)x1[0], (R)x1[1], (R)x1[2], (R)x1[3]);
       sWp[b0] = (R)x0[4];
       sWp[b0 + 1] = (R)x1[4];
       const uint8_t spm = sSpm[sg];
@@ -407,7 +415,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   }
 
   auto q_at = [&](int b, R q[5]) {
-    V::ld(sW, b, q[0], q[1], q[2], q[3]);
+    V::ld(sW, b, SM::NBOX, q[0], q[1], q[2], q[3]);
     q[4] = sWp[b];
   };
   // gravity kick -f dt/2 (the reference's expression, in FP64) of box cell b:
@@ -447,7 +455,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       if constexpr (F64) {  // the centre state, for the face states and the update
         R q[5];
         q_at(tb, q);
-        V::st(sM, 5 * kThreads + tid, q[0], q[1], q[2], q[3]);
+        V::st(sM, 5 * kThreads + tid, kThreads, q[0], q[1], q[2], q[3]);
         sMp[tid] = q[4];
       }
     } else {
@@ -487,9 +495,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     if (w < kThreads) {
       // groups: D_x(d,u,v,w), D_y, D_z, X(d,u,v,w), (D_x.p, D_y.p, D_z.p, X.p)
 #pragma unroll
-      for (int dir = 0; dir < 3; dir++) V::st(sM, dir * kThreads + tid, D[dir][0], D[dir][1], D[dir][2], D[dir][3]);
-      V::st(sM, 3 * kThreads + tid, X[0], X[1], X[2], X[3]);
-      V::st(sM, 4 * kThreads + tid, D[0][4], D[1][4], D[2][4], X[4]);
+      for (int dir = 0; dir < 3; dir++)
+        V::st(sM, dir * kThreads + tid, kThreads, D[dir][0], D[dir][1], D[dir][2], D[dir][3]);
+      V::st(sM, 3 * kThreads + tid, kThreads, X[0], X[1], X[2], X[3]);
+      V::st(sM, 4 * kThreads + tid, kThreads, D[0][4], D[1][4], D[2][4], X[4]);
     } else {
       const int ax = k >> 1;
       R Dax[5], W[7];
@@ -497,12 +506,12 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       for (int v = 0; v < 5; v++) Dax[v] = (ax == 0) ? D[0][v] : ((ax == 1) ? D[1][v] : D[2][v]);
       if constexpr (F64) {
         M::face_ax(q0, Dax, Wt, k, W, st, grav ? gk : nullptr);
-        V::st(sHS, r, W[0], W[1], W[2], W[3]);
+        V::st(sHS, r, NRING, W[0], W[1], W[2], W[3]);
         sHS[4 * NRING + r] = W[4];
       } else {
         M::face_px(X, Dax, k, W, st);
-        V::st(sHS, r, W[0], W[1], W[2], W[3]);
-        V::st(sHS, NRING + r, W[4], W[5], W[6], (R)0);
+        V::st(sHS, r, NRING, W[0], W[1], W[2], W[3]);
+        V::st(sHS, NRING + r, NRING, W[4], W[5], W[6], (R)0);
       }
     }
   }
@@ -526,13 +535,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   auto brick_face = [&](int t, int b, int k, R W[7]) {
     const int ax = k >> 1;
     R Dax[5], X[5], p0, p1, p2;
-    V::ld(sM, ax * kThreads + t, Dax[0], Dax[1], Dax[2], Dax[3]);
-    V::ld(sM, 3 * kThreads + t, X[0], X[1], X[2], X[3]);
-    V::ld(sM, 4 * kThreads + t, p0, p1, p2, X[4]);
+    V::ld(sM, ax * kThreads + t, kThreads, Dax[0], Dax[1], Dax[2], Dax[3]);
+    V::ld(sM, 3 * kThreads + t, kThreads, X[0], X[1], X[2], X[3]);
+    V::ld(sM, 4 * kThreads + t, kThreads, p0, p1, p2, X[4]);
     Dax[4] = (ax == 0) ? p0 : ((ax == 1) ? p1 : p2);
     if constexpr (F64) {
       R q0[5];
-      V::ld(sM, 5 * kThreads + t, q0[0], q0[1], q0[2], q0[3]);
+      V::ld(sM, 5 * kThreads + t, kThreads, q0[0], q0[1], q0[2], q0[3]);
       q0[4] = sMp[t];
       if (grav) {
         const R gk[3] = {sK[t], sK[kThreads + t], sK[2 * kThreads + t]};
@@ -545,13 +554,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
   };
   auto ring_face = [&](int r, R W[7]) {
-    V::ld(sHS, r, W[0], W[1], W[2], W[3]);
+    V::ld(sHS, r, NRING, W[0], W[1], W[2], W[3]);
     if constexpr (F64) {
       W[4] = sHS[4 * NRING + r];
       M::face_finish(W);
     } else {
       R pad;
-      V::ld(sHS, NRING + r, W[4], W[5], W[6], pad);
+      V::ld(sHS, NRING + r, NRING, W[4], W[5], W[6], pad);
     }
   };
 
@@ -574,7 +583,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         du[1] = (R)0;  // the internal-energy flux is cancelled too; u* stays for div(u)
       }
     }
-    V::st(sF, e, F[0], F[1], F[2], F[3]);
+    V::st(sF, e, SM::NF, F[0], F[1], F[2], F[3]);
     sF1[e] = F[4];
     if constexpr (DUAL) {
       sF5[e] = du[0] * du[1];  // (Us.m_n / Us.d) ebar (src/hydro_utils.c:2128)
@@ -701,7 +710,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     const long long gi = 8LL * (sKey[s] & 0x0FFFFFFFu) + c;
     double q[5];  // the FP64 state: staged (plain path) or read again from L2 (mixed path)
     if constexpr (F64) {
-      V::ld(sM, 5 * kThreads + tid, q[0], q[1], q[2], q[3]);
+      V::ld(sM, 5 * kThreads + tid, kThreads, q[0], q[1], q[2], q[3]);
       q[4] = sMp[tid];
     } else {
 #pragma unroll
@@ -736,7 +745,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       auto flux5 = [&](int k, double F[5]) {
         const int e = (k < 2) ? (ex + (k & 1)) : ((k < 4) ? (ey + G::CX * (k & 1)) : (ez + G::CX * G::CY * (k & 1)));
         R f0, f1, f2, f3;
-        V::ld(sF, e, f0, f1, f2, f3);
+        V::ld(sF, e, SM::NF, f0, f1, f2, f3);
         F[0] = (double)f0;
         F[1] = (double)f1;
         F[2] = (double)f2;
