@@ -88,6 +88,7 @@ struct Ctx {
   unsigned status = 0;
   std::string last_error;
   Tree res;                      // resident tree
+  struct OCT **res_first = nullptr;  // the firstoct array it was uploaded from
   int *d_work_all = nullptr;     // batched work list, finest level first
   int nwork_all = 0;
   cudaGraphExec_t graph = nullptr;
@@ -960,6 +961,10 @@ bool autotune_tree(Tree &t, int shape_req) {
   return ok;
 }
 
+int emma_hydro_is_resident(struct OCT **firstoct) {
+  return (g.ready && g.res.valid && firstoct != nullptr && g.res_first == firstoct) ? 1 : 0;
+}
+
 int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int rank) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
   if (firstoct == nullptr || lcoarse < 2 || lmax < lcoarse || lmax >= kMaxLevels) {
@@ -986,6 +991,7 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
     return rc;
   }
   if (!alloc_tree(g.res.host, g.res, false)) return EMMA_ST_CUDA;
+  g.res_first = firstoct;
   // schedule constants
   SchedState &h = *g.h_S;
   std::memset(&h, 0, sizeof(h));

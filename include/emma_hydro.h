@@ -143,6 +143,28 @@ int emma_hydro_advance_coarse_step_async(double dt_param, double time_max, int n
 int emma_hydro_get_time(double *tsim, double *adt);
 int emma_hydro_set_time(double tsim, const double *adt);
 
+/* 1 if a resident tree was uploaded from this firstoct array (and not freed since). */
+int emma_hydro_is_resident(struct OCT **firstoct);
+
+/* Checkpoints in the reference's raw-OCT restart format.  emma_hydro_save_amr
+ * writes what save_amr (src/restart.c:12-103, -DWHYDRO2 build) writes: tsim,
+ * tinit, nsteps, ndumps, lcoarse, lmax, adt[0..lmax-1], the 7 unit scales
+ * (unit_l, unit_v, unit_t, unit_n, unit_mass, unit_d, unit_N), the addresses of
+ * firstoct[0], of its cell 0 and `proot`, then each oct of levels 1..lmax in list
+ * order as its address and its bytes; for a resident tree of the same firstoct
+ * the device state is downloaded into the tree first.  emma_hydro_restore_amr
+ * reads such a file back as restore_amr (src/restart.c:108-328) does: into the
+ * caller's pool of ngridmax octs starting at firstoct[0] (octs at their snapshot
+ * offset, pointers shifted, level-1 parents set to `root`), rebuilding firstoct
+ * and lastoct (levelmax entries) and the free-oct chain (*freeoct). */
+int emma_hydro_save_amr(const char *filename, struct OCT **firstoct, double tsim, double tinit, int nsteps,
+                        int ndumps, int lcoarse, int lmax, const double *adt, const double *units7,
+                        const void *proot);
+int emma_hydro_restore_amr(const char *filename, struct OCT **firstoct, struct OCT **lastoct, int levelmax,
+                           long long ngridmax, struct CELL *root, double *tsim, double *tinit, int *nsteps,
+                           int *ndumps, int *lcoarse, int *lmax, double *adt, double *units7,
+                           struct OCT **freeoct);
+
 /* SoA access for tests and I/O: 5 planes (d,u,v,w,p) of 8*noct doubles each, list order. */
 int emma_hydro_level_noct(int level);
 int emma_hydro_get_level_state(int level, double *host_out);

@@ -224,6 +224,34 @@ class RefTree:
     def sizeof_oct(self):
         return self.L.ref_sizeof_oct()
 
+    def save_amr(self, filename, tsim, tinit, nsteps, ndumps, units7):
+        """The reference's save_amr (src/restart.c:12) of this tree."""
+        u = np.ascontiguousarray(units7, dtype=np.float64)
+        self.L.ref_save_amr.argtypes = [ctypes.c_char_p, c_double, c_double, c_int, c_int, c_void_p]
+        self.L.ref_save_amr(filename.encode(), tsim, tinit, nsteps, ndumps, _p(u))
+
+    def restore_amr(self, filename):
+        """The reference's restore_amr (src/restart.c:108) into this tree's pool."""
+        t, ti, ns, nd = c_double(), c_double(), c_int(), c_int()
+        self.L.ref_restore_amr.argtypes = [ctypes.c_char_p] + [ctypes.c_void_p] * 4
+        self.L.ref_restore_amr(filename.encode(), ctypes.byref(t), ctypes.byref(ti), ctypes.byref(ns),
+                               ctypes.byref(nd))
+        return t.value, ti.value, ns.value, nd.value
+
+    def pool(self):
+        """(lastoct array, root cell, pool size in octs) of the reference's tree."""
+        for n in ("ref_lastoct_array", "ref_root_cell", "ref_freeoct"):
+            getattr(self.L, n).restype = c_void_p
+        return self.L.ref_lastoct_array(), self.L.ref_root_cell(), self.L.ref_ngridmax()
+
+    def set_freeoct(self, f):
+        self.L.ref_set_freeoct.argtypes = [c_void_p]
+        self.L.ref_set_freeoct(f)
+
+    def freeoct(self):
+        self.L.ref_freeoct.restype = c_void_p
+        return self.L.ref_freeoct()
+
     def topology(self, level):
         n = self.noct(level)
         nei = np.zeros(6 * n, np.int32)

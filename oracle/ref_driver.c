@@ -30,6 +30,7 @@
 #include "oct.h"
 #include "hydro_utils.h"
 #include "segment.h"
+#include "restart.h"
 
 /* defined in src/advanceamr.c:92 (compiled through ref_advanceamr_cfl.c) */
 REAL L_comptstep_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct,
@@ -255,6 +256,25 @@ void ref_set_force(int level, const double *fx, const double *fy, const double *
     }
 }
 #endif
+
+/* Checkpoints through the reference's own src/restart.c (save_amr / restore_amr),
+ * units from `units7` (unit_l, _v, _t, _n, _mass, _d, _N), no particles. */
+void ref_save_amr(const char *filename, double tsim, double tinit, int nsteps, int ndumps, const double *units7) {
+  g_param.unit.unit_l = units7[0]; g_param.unit.unit_v = units7[1]; g_param.unit.unit_t = units7[2];
+  g_param.unit.unit_n = units7[3]; g_param.unit.unit_mass = units7[4]; g_param.unit.unit_d = units7[5];
+  g_param.unit.unit_N = units7[6];
+  save_amr((char *)filename, g_first, tsim, tinit, nsteps, ndumps, &g_param, &g_cpu, NULL, g_adt);
+}
+void ref_restore_amr(const char *filename, double *tsim, double *tinit, int *nsteps, int *ndumps) {
+  g_cpu.freeoct = restore_amr((char *)filename, g_first, g_last, tsim, tinit, nsteps, ndumps, &g_param, &g_cpu,
+                              NULL, g_adt, &g_root);
+  recount();
+}
+void *ref_lastoct_array(void) { return g_last; }
+void *ref_root_cell(void) { return &g_root; }
+void *ref_freeoct(void) { return g_cpu.freeoct; }
+void ref_set_freeoct(void *f) { g_cpu.freeoct = (struct OCT *)f; recount(); }
+int ref_ngridmax(void) { return g_ngridmax; }
 
 /* Export d,u,v,w,p,a,E of field (which=0) or fieldnew (which=1) as 7 planes. */
 void ref_get_field(int level, int which, double *out) {
