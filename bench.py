@@ -281,6 +281,17 @@ def run_mine(args, rank, world):
     return cfg, tree, results, l1, build_s, flush
 
 
+def max_over_ranks(values, world, device):
+    """Each timing as the maximum over the ranks of the job (replicas: every rank
+    advanced its own copy; the job took as long as the slowest rank)."""
+    if world <= 1:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return [float(x) for x in t.cpu()]
+
+
 def synthetic_force(tree, level, amp=0.5):
     """Smooth periodic acceleration field (gravity workloads): a few Fourier modes."""
     c = tree.cell_centres(level)
@@ -426,10 +437,7 @@ def main():
     dropin = res["dropin"]
     ms_m, ms_f, ms_e = mixed["ms"], fp64["ms"], mixed["e2e_ms"]
     ms_d = dropin["ms"] if dropin is not None else ms_e
-    if world > 1:
-        t = torch.tensor([ms_m, ms_f, ms_e, ms_d], device="cuda")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        ms_m, ms_f, ms_e, ms_d = (float(x) for x in t.cpu())
+    ms_m, ms_f, ms_e, ms_d = max_over_ranks([ms_m, ms_f, ms_e, ms_d], world, "cuda")
     upd_m = mixed["updates"] * world
     value = upd_m / (ms_m * 1e-3)
     value_fp64 = fp64["updates"] * world / (ms_f * 1e-3)
