@@ -132,3 +132,36 @@ def test_dual_dropin_matches_oracle(gpu):
     for l in (4, 5, 6):
         e = per_cell_rel(tg.get_fields(l)[:5], to.get_fields(l)[:5])
         assert e.max() <= 1e-12, (l, e.max())
+
+
+def test_dual_sod_tube_transmissive(gpu):
+    """Dual energy with transmissive x boundaries (the HYDROTEST gather)."""
+    cfg = configs.sod(level=5)
+    lib().emma_hydro_clear_status()
+    r = ResidentHydro(cfg.build(), precision=PREC_FP64, trans=cfg.trans, cfl=CFL, dual=True)
+    for _ in range(3):
+        r.coarse_step(nsub=cfg.nsub)
+    assert r.status() == 0
+    to = cfg.build()
+    tsim, adt, err = oracle.Restatement().run(to.firstoct, cfg.lcoarse, cfg.lmax, 3, CFL, trans=cfg.trans,
+                                              nsub=cfg.nsub, dual=True)
+    assert err == 0 and r.tsim == tsim
+    assert per_cell_rel(r.state(5), to.get_fields(5)[:5]).max() <= 1e-12
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_dual_single_substep_batched_and_host_schedules(gpu, use_graph):
+    """nsub = 1: all levels in one batched launch (graph) or level by level from the
+    host; the averaged split cells' zero sound speed is tracked on both."""
+    cfg, fields = shock_cfg()
+    levels = range(cfg.lcoarse, cfg.lmax + 1)
+    r = ResidentHydro(build(cfg, fields), precision=PREC_FP64, cfl=CFL, dual=True, use_graph=use_graph)
+    for _ in range(3):
+        r.coarse_step(nsub=1)
+    assert r.status() == 0
+    to = build(cfg, fields)
+    tsim, adt, err = oracle.Restatement().run(to.firstoct, cfg.lcoarse, cfg.lmax, 3, CFL, nsub=1, dual=True)
+    assert err == 0 and abs(r.tsim - tsim) <= 1e-14 * tsim
+    for l in levels:
+        e = per_cell_rel(r.state(l), to.get_fields(l)[:5])
+        assert e.max() <= 1e-10, (l, e.max())

@@ -174,3 +174,27 @@ def test_dropin_gravity_matches_oracle(gpu):
     for l in (4, 5, 6):
         e = per_cell_rel(tg.get_fields(l)[:5], to.get_fields(l)[:5])
         assert e.max() <= 1e-12, (l, e.max())
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_gravity_single_substep_batched_and_host_schedules(gpu, use_graph):
+    """nsub = 1 (one batched launch over all levels on the graph schedule) and the
+    host-driven schedule, both against the gravity oracle."""
+    cfg = configs.small_amr(base=4, radii=(0.3, 0.15))
+    levels = range(cfg.lcoarse, cfg.lmax + 1)
+    tg = cfg.build()
+    f = forces(tg, levels)
+    r = ResidentHydro(tg, precision=PREC_FP64, cfl=CFL, gravity=True, use_graph=use_graph)
+    for l in levels:
+        r.set_force(l, *f[l])
+    for _ in range(3):
+        r.coarse_step(nsub=1)
+    assert r.status() == 0
+    gc = oracle.GravClone(cfg.build())
+    for l in levels:
+        gc.set_force(l, *f[l])
+    tsim, adt, err = gc.run(3, CFL, nsub=1)
+    assert err == 0 and abs(r.tsim - tsim) <= 1e-14 * tsim
+    for l in levels:
+        e = per_cell_rel(r.state(l), gc.get_fields(l)[:5])
+        assert e.max() <= 1e-10, (l, e.max())
