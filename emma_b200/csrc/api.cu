@@ -29,6 +29,8 @@ cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *g
                        cudaStream_t s);
 cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s,
                           bool grav);
+cudaError_t launch_dropin_base(const double *wb, double *base, long long n8, const double *exc, long long nexc, int nsm,
+                               cudaStream_t s);
 }  // namespace emma
 
 using namespace emma;
@@ -112,6 +114,11 @@ struct Ctx {
   long long h2d_bytes = 0, d2h_bytes = 0;  // host<->device state copies
   double dropin_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // phases of the last drop-in call
   std::vector<cudaEvent_t> range_ev;        // per host thread and sub-range of a drop-in download
+  std::vector<double> exc[16];              // per host thread: drop-in cells whose fieldnew differs
+  double *pin_exc = nullptr;                // their pinned staging
+  size_t pin_exc_bytes = 0;
+  double *d_exc = nullptr;                  // and device copy
+  size_t d_exc_bytes = 0;
   bool timing = true;
   std::vector<TimedLaunch> launches;
   std::vector<cudaEvent_t> free_events;
@@ -275,11 +282,12 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     d.shape = h.shape;
     const size_t bytes = sizeof(double) * 5 * (size_t)std::max<long long>(d.n8, 1);
     if (with_base && !h.tiles.empty()) {
-      // W0 and the base B in one block: the drop-in upload copies all 11 planes of
-      // an oct range with one pitched copy
-      if (!ck(cudaMalloc(&d.WB, sizeof(double) * 11 * (size_t)d.n8), "cudaMalloc W+B")) return false;
+      // drop-in levels: W0 (5 planes) and E of `field` (1 plane) in one block, uploaded
+      // by one pitched copy per oct range, then the base B (6 planes: fieldnew), built
+      // on the device from them and the cells where fieldnew differs from field
+      if (!ck(cudaMalloc(&d.WB, sizeof(double) * 12 * (size_t)d.n8), "cudaMalloc W+B")) return false;
       d.W0 = d.WB;
-      d.B = d.WB + 5 * d.n8;
+      d.B = d.WB + 6 * d.n8;
     } else if (!ck(cudaMalloc(&d.W0, bytes), "cudaMalloc W")) {
       return false;
     }
@@ -401,9 +409,11 @@ inline void finish_prims(struct Wtype &W) {
   W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
 }
 
-// Packs octs [a, b) of a level in one pass over their cells: `field` into the 5
-// planes of pw, `fieldnew` (with E) into the 6 planes of pb (planes of 8*noct).
-void pack_cells(const HostLevel &h, long long a, long long b, double *pw, double *pb) {
+// Packs octs [a, b) of a level in one pass over their cells: `field` with E into
+// the 6 planes of pw (planes of 8*noct); every cell whose `fieldnew` differs from
+// `field` (after clean_new_hydro: the cells a finer level corrected) appends
+// {cell, d, u, v, w, p, E, 0} of its fieldnew to exc.
+void pack_cells(const HostLevel &h, long long a, long long b, double *pw, std::vector<double> &exc) {
   const long long n8 = 8LL * h.noct;
   for (long long i = a; i < b; i++) {
     const struct OCT *o = h.octs[i];
@@ -415,12 +425,11 @@ void pack_cells(const HostLevel &h, long long a, long long b, double *pw, double
       pw[2 * n8 + k] = W.v;
       pw[3 * n8 + k] = W.w;
       pw[4 * n8 + k] = W.p;
-      pb[k] = N.d;
-      pb[n8 + k] = N.u;
-      pb[2 * n8 + k] = N.v;
-      pb[3 * n8 + k] = N.w;
-      pb[4 * n8 + k] = N.p;
-      pb[5 * n8 + k] = N.E;
+      pw[5 * n8 + k] = W.E;
+      if (std::memcmp(&W, &N, 5 * sizeof(double)) != 0 || std::memcmp(&W.E, &N.E, sizeof(double)) != 0) {
+        const double e[8] = {(double)k, N.d, N.u, N.v, N.w, N.p, N.E, 0.};
+        exc.insert(exc.end(), e, e + 8);
+      }
     }
   }
 }
@@ -773,6 +782,8 @@ void emma_hydro_shutdown(void) {
   for (auto e : g.free_events) cudaEventDestroy(e);
   for (auto e : g.range_ev) cudaEventDestroy(e);
   g.range_ev.clear();
+  if (g.pin_exc) cudaFreeHost(g.pin_exc);
+  cudaFree(g.d_exc);
   cudaFree(g.d_status);
   cudaFree(g.d_done);
   cudaFree(g.d_S);
@@ -1507,20 +1518,20 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   if (h.noct == 0) return 0;
   const long long n8 = d.n8, nc8 = dc.n8;
   const bool coarse = nc8 > 0 && h.reads_coarse && dc.C != nullptr;
-  // pinned staging: level field (5 planes) | level fieldnew (6 planes) | coarser
+  // pinned staging: level field with E (6 planes; the new state on the way back) | coarser
   // level (5 planes) | gravity builds: level and coarser accelerations (3 + 3
   // planes) | device status word
   const long long nf = kDropinGrav ? 3 * (n8 + nc8) : 0, ncp = cplanes();
   // (+ n8 bytes for the dual-energy sound-speed flags after the status word)
-  if (!ensure_pin(sizeof(double) * (11 * n8 + ncp * nc8 + nf + 2) + (size_t)n8) || !ensure_range_events()) return 0;
-  double *pw = g.pin, *pb = g.pin + 5 * n8, *pc = g.pin + 11 * n8;
+  if (!ensure_pin(sizeof(double) * (6 * n8 + ncp * nc8 + nf + 2) + (size_t)n8) || !ensure_range_events()) return 0;
+  double *pw = g.pin, *pc = g.pin + 6 * n8;
   [[maybe_unused]] double *pf = pc + ncp * nc8, *pfc = pf + 3 * n8;
   unsigned *pst = reinterpret_cast<unsigned *>(pc + ncp * nc8 + nf);
   const auto t1 = Clock::now();
-  // upload: each host thread packs its oct range in sub-ranges (field and
-  // fieldnew in one pass over the cells) and queues one pitched copy of the 11
-  // planes of each sub-range as soon as it is packed, so the copy engine runs
-  // while the rest is still being packed
+  // upload: each host thread packs its oct range in sub-ranges (field and the
+  // cells whose fieldnew differs, in one pass over the cells) and queues one
+  // pitched copy of the 6 planes of each sub-range as soon as it is packed, so the
+  // copy engine runs while the rest is still being packed
   if (d.WB == nullptr) {
     fail(EMMA_ST_TREE, "drop-in level without staging block");
     return 0;
@@ -1528,11 +1539,12 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   const size_t pitch = sizeof(double) * (size_t)n8;
   const long long sub = dropin_subrange(h.noct);
   std::atomic<bool> copies_ok{true};
-  parallel_ranges(h.noct, [&](int, long long a0, long long b0) {
+  for (auto &e : g.exc) e.clear();
+  parallel_ranges(h.noct, [&](int t, long long a0, long long b0) {
     for (long long s0 = a0; s0 < b0; s0 += sub) {
       const long long s1 = std::min(b0, s0 + sub);
-      pack_cells(h, s0, s1, pw, pb);
-      if (cudaMemcpy2DAsync(d.WB + 8 * s0, pitch, pw + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 11,
+      pack_cells(h, s0, s1, pw, g.exc[t]);
+      if (cudaMemcpy2DAsync(d.WB + 8 * s0, pitch, pw + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 6,
                             cudaMemcpyHostToDevice, g.stream) != cudaSuccess)
         copies_ok = false;
 #ifdef EMMA_WGRAV
@@ -1544,12 +1556,43 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     }
   });
   if (!copies_ok) return ck(cudaGetLastError(), "H2D level state"), 0;
+  {
+    // the base fieldnew: field, then the cells where it differs
+    size_t nexc = 0;
+    for (auto &e : g.exc) nexc += e.size() / 8;
+    const size_t eb = sizeof(double) * 8 * std::max<size_t>(nexc, 1);
+    if (eb > g.pin_exc_bytes) {
+      if (g.pin_exc) cudaFreeHost(g.pin_exc);
+      g.pin_exc = nullptr;
+      g.pin_exc_bytes = 0;
+      if (!ck(cudaMallocHost(&g.pin_exc, eb), "cudaMallocHost exceptions")) return 0;
+      g.pin_exc_bytes = eb;
+    }
+    if (eb > g.d_exc_bytes) {
+      cudaFree(g.d_exc);
+      g.d_exc = nullptr;
+      g.d_exc_bytes = 0;
+      if (!ck(cudaMalloc(&g.d_exc, eb), "cudaMalloc exceptions")) return 0;
+      g.d_exc_bytes = eb;
+    }
+    size_t at = 0;
+    for (auto &e : g.exc) {
+      std::memcpy(g.pin_exc + at, e.data(), sizeof(double) * e.size());
+      at += e.size();
+    }
+    if (nexc > 0 &&
+        !ck(cudaMemcpyAsync(g.d_exc, g.pin_exc, sizeof(double) * 8 * nexc, cudaMemcpyHostToDevice, g.stream),
+            "H2D exceptions"))
+      return 0;
+    if (!ck(launch_dropin_base(d.WB, d.B, n8, g.d_exc, (long long)nexc, g.nsm, g.stream), "base launch")) return 0;
+    g.h2d_bytes += (long long)(sizeof(double) * 8 * nexc);
+  }
   if (d.az != nullptr) {  // dual energy: the split cells' stored sound speeds of 0
     uint8_t *pz = reinterpret_cast<uint8_t *>(pst + 4);
     parallel_for(h.noct, [&](long long a0, long long b0) { pack_az(h, a0, b0, pz); });
     if (!ck(cudaMemcpyAsync(d.az, pz, (size_t)n8, cudaMemcpyHostToDevice, g.stream), "H2D az")) return 0;
   }
-  g.h2d_bytes += (long long)sizeof(double) * (11 + 3 * kDropinGrav) * n8;
+  g.h2d_bytes += (long long)sizeof(double) * (6 + 3 * kDropinGrav) * n8;
   if (coarse) {
     pack_level(hc, 0, pc);
     if (!ck(cudaMemcpyAsync(dc.W0, pc, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))

@@ -26,3 +26,20 @@ def gpu():
     if not gpu_available():
         pytest.skip("no CUDA device")
     return True
+
+
+@pytest.fixture(autouse=True)
+def default_library_options(request):
+    """GPU tests start from the library's default options: the options are global
+    state of libemmahydro (a ResidentHydro sets them), and the drop-in entries run
+    with whatever was set last."""
+    if request.node.get_closest_marker("gpu") is not None and gpu_available():
+        import ctypes
+        from emma_b200 import lib
+        from emma_b200._lib import EmmaHydroOptions
+        L = lib()
+        o = EmmaHydroOptions()
+        L.emma_hydro_default_options(ctypes.byref(o))
+        L.emma_hydro_set_options(ctypes.byref(o))
+        L.emma_hydro_clear_status()
+    yield
