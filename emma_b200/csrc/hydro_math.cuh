@@ -74,19 +74,6 @@ struct MathF64 {
     for (int i = 0; i < 5; i++) Wt[i] = acc[i] * fac;
   }
 
-  // Face state k of a cell from its slopes and predictor (src/hydro_utils.c:1166-1247):
-  // W0 +-D/2 + Wt, pressure floor, then E and a.  Returns the 7 values d,u,v,w,p,a,E.
-  static __device__ __forceinline__ void face(const double q0[5], const double D[3][5], const double Wt[5], int k,
-                                              double W[7], unsigned &st) {
-    const double fx = (k == 0) ? -0.5 : (k == 1 ? 0.5 : 0.0);
-    const double fy = (k == 2) ? -0.5 : (k == 3 ? 0.5 : 0.0);
-    const double fz = (k == 4) ? -0.5 : (k == 5 ? 0.5 : 0.0);
-#pragma unroll
-    for (int i = 0; i < 5; i++) W[i] = q0[i] + fx * D[0][i] + fy * D[1][i] + fz * D[2][i] + Wt[i];
-    W[4] = fmax(W[4], kPmin);
-    if (W[0] < 0) st |= kStNegDensity;
-    face_finish(W);
-  }
   // E and a of a face state from its (d,u,v,w,p)
   static __device__ __forceinline__ void face_finish(double W[7]) {
     W[6] = W[4] / (kGam - 1.) + 0.5 * W[0] * (W[1] * W[1] + W[2] * W[2] + W[3] * W[3]);
@@ -324,19 +311,6 @@ struct MathF32 {
     Wt[2] = -dtdx_half * acc2;
     Wt[3] = -dtdx_half * acc3;
     Wt[4] = -dtdx_half * acc4;
-  }
-
-  // Face state toward face k: W0 +- D_axis/2 + Wt, pressure floor.
-  // W = {d, u, v, w, p, 1/d, a}.
-  static __device__ __forceinline__ void face_ax(const float q0[5], const float Dax[5], const float Wt[5], int k,
-                                                 float W[7], unsigned &st) {
-    const float s = (k & 1) ? 0.5f : -0.5f;
-#pragma unroll
-    for (int i = 0; i < 5; i++) W[i] = q0[i] + s * Dax[i] + Wt[i];
-    W[4] = fmaxf(W[4], (float)kPmin);
-    if (W[0] < 0.f) st |= kStNegDensity;
-    W[5] = rcp(W[0]);
-    W[6] = sqrtf(G * W[4] * W[5]);
   }
 
   // Face state toward face k from the predicted centre state X = W0 + Wt.
