@@ -354,3 +354,42 @@ def test_mixed_cosmology_tree_l1(gpu):
         fm, fo = tm.get_fields(l), to.get_fields(l)
         assert l1_rel(fm[0][leaf], fo[0][leaf]) <= 1e-5
         assert l1_rel(fm[4][leaf], fo[4][leaf]) <= 1e-5
+
+
+def _totals(states, levels, tree):
+    m = e = 0.0
+    for l in levels:
+        f = states[l]
+        leaf = ~tree.split_mask(l)
+        dv = 0.5 ** (3 * l)
+        m += f[0][leaf].sum() * dv
+        e += (f[4] / (5. / 3. - 1.) + 0.5 * f[0] * (f[1] ** 2 + f[2] ** 2 + f[3] ** 2))[leaf].sum() * dv
+    return m, e
+
+
+@pytest.mark.parametrize("config", ["turb", "roofline"])
+def test_full_size_conservation_and_mixed_l1(gpu, config):
+    """The benchmark workloads at full size (turbulent box 128^3, random box 256^3),
+    where the oracle is too slow: size-independent properties.  Mass and total
+    energy are conserved to 1e-12 on the periodic box by both paths; the mixed
+    path stays within L1 1e-5 of the FP64 path."""
+    cfg = configs.turb() if config == "turb" else configs.random_uniform(level=8)
+    t = cfg.build()
+    levels = [cfg.lcoarse]
+    l = cfg.lcoarse
+    init = {l: t.get_fields(l)[:5]}
+    m0, e0 = _totals(init, levels, t)
+    out = {}
+    for prec in (PREC_FP64, PREC_MIXED):
+        r = ResidentHydro(t, precision=prec, cfl=CFL)
+        for _ in range(3):
+            r.coarse_step(nsub=cfg.nsub)
+        assert r.status() == 0
+        out[prec] = {l: r.state(l)}
+        m1, e1 = _totals(out[prec], levels, t)
+        assert abs(m1 - m0) <= 1e-12 * m0, (prec, m1, m0)
+        assert abs(e1 - e0) <= 1e-12 * e0, (prec, e1, e0)
+    fm, ff = out[PREC_MIXED][l], out[PREC_FP64][l]
+    assert l1_rel(fm[0], ff[0]) <= 1e-5
+    assert l1_rel(fm[4], ff[4]) <= 1e-5
+    assert l1_rel(np.sqrt((fm[1:4] ** 2).sum(0)), np.sqrt((ff[1:4] ** 2).sum(0))) <= 1e-5
