@@ -66,7 +66,7 @@ struct CPUINFO;
 struct RUNPARAMS;
 struct HGRID;
 
-#define EMMA_SIZEOF_HGRID 16576 /* sizeof(struct HGRID) for this build */
+#define EMMA_SIZEOF_HGRID 16576 /* sizeof(struct HGRID) with the flags above (-DWHYDRO2, NVAR 6) */
 
 #ifdef __cplusplus
 }
