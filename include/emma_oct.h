@@ -66,7 +66,13 @@ struct CPUINFO;
 struct RUNPARAMS;
 struct HGRID;
 
-#define EMMA_SIZEOF_HGRID 16576 /* sizeof(struct HGRID) with the flags above (-DWHYDRO2, NVAR 6) */
+/* sizeof(struct HGRID) with the flags above (-DWHYDRO2, NVAR 6; the stencil cells
+ * also carry f[3] with -DWGRAV) */
+#ifdef EMMA_WGRAV
+#define EMMA_SIZEOF_HGRID 21760
+#else
+#define EMMA_SIZEOF_HGRID 16576
+#endif
 
 #ifdef __cplusplus
 }

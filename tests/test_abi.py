@@ -57,3 +57,17 @@ def test_struct_layout_matches_reference():
     # struct OCT must be 1200 bytes (src/prototypes.h:1028 with -DWHYDRO2, REAL=double)
     from oracle import Restatement
     assert Restatement().L.orc_sizeof_oct() == 1200
+
+
+def test_hgrid_size_matches_reference_builds():
+    """create_pinned_stencil allocates EMMA_SIZEOF_HGRID bytes per stencil entry:
+    the reference's sizeof(struct HGRID) in the default and the -DWGRAV build."""
+    import re
+    import oracle
+    src = open(os.path.join(ROOT, "include", "emma_oct.h")).read()
+    grav, plain = (int(x) for x in re.findall(r"#define EMMA_SIZEOF_HGRID (\d+)", src))
+    for name, want in (("libemmaref.so", plain), ("libemmaref_grav.so", grav)):
+        path = os.path.join(ROOT, "oracle", "_ref", name)
+        if not os.path.exists(path):
+            continue
+        assert ctypes.CDLL(path, mode=os.RTLD_LOCAL | os.RTLD_NOW).ref_sizeof_hgrid() == want, name
