@@ -7,4 +7,4 @@ and the synthetic benchmark configurations.
 from ._lib import (PREC_FP64, PREC_MIXED, TRANS_XM, TRANS_XP, TRANS_YM, TRANS_YP, TRANS_ZM,  # noqa: F401
                    TRANS_ZP, lib)
 from .tree import OctTree  # noqa: F401
-from .hydro import ResidentHydro, HydroSolver, advancehydroGPU, clean_new_hydro  # noqa: F401
+from .hydro import ResidentHydro, HydroSolver, advancehydroGPU, clean_new_hydro, CpuInfo, RunParams  # noqa: F401

@@ -86,6 +86,8 @@ SIGNATURES = [
     ("emma_tree_oct_xyz", None, [c_void_p, c_int, c_void_p]),
     ("emma_tree_set_field", None, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("emma_tree_get_field", None, [c_void_p, c_int, c_int, c_void_p]),
+    ("emma_tree_put_field", None, [c_void_p, c_int, c_int, c_void_p]),
+    ("emma_tree_set_cpu", None, [c_void_p, c_int, c_void_p]),
     ("emma_tree_topology", None, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
 ]
 

@@ -6,6 +6,7 @@
 #include <atomic>
 #include <chrono>
 #include <cmath>
+#include <cstddef>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -1001,6 +1002,14 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
     fail((unsigned)rc, err);
     return rc;
   }
+  if (g.res.host.ghosts) {
+    // a resident tree is advanced for many levels and steps without the host: the
+    // boundary octs of a multi-rank run would never be refreshed between solves
+    g.res.host = HostTree();
+    fail(EMMA_ST_ARG, "the level lists hold octs of other ranks: a multi-rank run advances through the drop-in "
+                      "entries, between the exchanges of its boundary octs");
+    return EMMA_ST_ARG;
+  }
   if (!alloc_tree(g.res.host, g.res, false)) return EMMA_ST_CUDA;
   g.res_first = firstoct;
   // schedule constants
@@ -1391,7 +1400,7 @@ int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int tran
       mh += s;
     }
     long long *o = stats5 + 5 * (L - lcoarse);
-    o[0] = h.noct;
+    o[0] = h.nown;
     o[1] = (long long)h.tiles.size();
     o[2] = ms;
     o[3] = mh;
@@ -1436,9 +1445,10 @@ static inline unsigned long long mix64(unsigned long long z) {  // SplitMix64 fi
   return z ^ (z >> 31);
 }
 
-// Order-sensitive hash of a level's oct addresses and child-presence bits (the
-// parts of the tree a drop-in mirror depends on); `*split` = a cell has a child.
-static unsigned long long level_hash(const std::vector<struct OCT *> &v, bool *split) {
+// Order-sensitive hash of a level's oct addresses, child-presence bits and
+// ownership (cpu == rank): the parts of the tree a drop-in mirror depends on;
+// `*split` = a cell has a child.
+static unsigned long long level_hash(const std::vector<struct OCT *> &v, int rank, bool *split) {
   const long long n = (long long)v.size();
   const long long chunk = 8192;
   const long long nchunk = (n + chunk - 1) / chunk;
@@ -1455,6 +1465,7 @@ static unsigned long long level_hash(const std::vector<struct OCT *> &v, bool *s
         unsigned long long bits = 0;
         for (int c = 0; c < 8; c++) bits |= (unsigned long long)(o->cell[c].child != nullptr) << c;
         f = f || bits != 0;
+        bits |= (unsigned long long)(o->cpu == rank) << 8;
         s += mix64((unsigned long long)(uintptr_t)o ^ (bits << 56) ^ ((unsigned long long)i * 0x9e3779b97f4a7c15ULL));
       }
       part[j] = s;
@@ -1486,9 +1497,9 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   const std::vector<struct OCT *> &wc = walk_level(firstoct, level - 1);
   std::vector<unsigned long long> sig;
   sig.push_back((unsigned long long)(uintptr_t)firstoct);
-  sig.push_back(level_hash(wc, &unused));
-  sig.push_back(level_hash(wl, &split_l));
-  if (split_l) sig.push_back(level_hash(walk_level(firstoct, level + 1), &unused));
+  sig.push_back(level_hash(wc, rank, &unused));
+  sig.push_back(level_hash(wl, rank, &split_l));
+  if (split_l) sig.push_back(level_hash(walk_level(firstoct, level + 1), rank, &unused));
   const int lo = level - 1, hi = split_l ? level + 1 : level;
   const auto tw = Clock::now();
   Ctx::DropCache &cache = g.drop[level];
@@ -1515,7 +1526,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   const HostLevel &hc = H.lev[level - 1];
   DevLevel &d = T.lev[level];
   DevLevel &dc = T.lev[level - 1];
-  if (h.noct == 0) return 0;
+  if (h.nown == 0) return 0;
   const long long n8 = d.n8, nc8 = dc.n8;
   const bool coarse = nc8 > 0 && h.reads_coarse && dc.C != nullptr;
   // pinned staging: level field with E (6 planes; the new state on the way back) | coarser
@@ -1663,12 +1674,14 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   std::atomic<bool> wait_ok{true};
   std::atomic<long long> wait_ns{0};
   const unsigned bad = EMMA_ST_TREE | EMMA_ST_CUDA;
-  parallel_ranges(h.noct, [&](int t, long long a0, long long b0) {
+  // this rank's octs only (the first nown): octs of other ranks are not advanced
+  const long long sub_own = dropin_subrange(h.nown);
+  parallel_ranges(h.nown, [&](int t, long long a0, long long b0) {
     // queue the copies of all sub-ranges of this thread, each followed by an event
     cudaEvent_t *ev = &g.range_ev[(size_t)t * kSubRanges];
     int nq = 0;
-    for (long long s0 = a0; s0 < b0 && nq < kSubRanges; s0 += sub, nq++) {
-      const long long s1 = std::min(b0, s0 + sub);
+    for (long long s0 = a0; s0 < b0 && nq < kSubRanges; s0 += sub_own, nq++) {
+      const long long s1 = std::min(b0, s0 + sub_own);
       if (cudaMemcpy2DAsync(pw + 8 * s0, pitch, d.W1 + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 5,
                             cudaMemcpyDeviceToHost, g.stream) != cudaSuccess ||
           cudaEventRecord(ev[nq], g.stream) != cudaSuccess) {
@@ -1678,7 +1691,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     }
     // then unpack each as it lands
     int k = 0;
-    for (long long s0 = a0; s0 < b0 && k < nq; s0 += sub, k++) {
+    for (long long s0 = a0; s0 < b0 && k < nq; s0 += sub_own, k++) {
       const auto w0 = Clock::now();
       const bool ok = cudaEventSynchronize(ev[k]) == cudaSuccess;
       wait_ns += std::chrono::duration_cast<std::chrono::nanoseconds>(Clock::now() - w0).count();
@@ -1688,16 +1701,16 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
       }
       // a kernel that found an invalid state leaves the host tree as it was
       if ((g.status | *reinterpret_cast<volatile unsigned *>(pst)) & bad) return;
-      unpack_cells(h, s0, std::min(b0, s0 + sub), pw, final_update);
+      unpack_cells(h, s0, std::min(b0, s0 + sub_own), pw, final_update);
     }
   });
   if (!wait_ok) return ck(cudaStreamSynchronize(g.stream), "D2H level state"), ck(cudaGetLastError(), "D2H"), 0;
-  g.d2h_bytes += (long long)sizeof(double) * 5 * n8;
+  g.d2h_bytes += (long long)sizeof(double) * 5 * 8 * h.nown;
   g.status |= *pst;
   if (g.status & bad) return 0;
   const auto t4 = Clock::now();
   g.dropin_ms[3] = std::chrono::duration<double, std::milli>(t4 - t2).count();
-  g.dropin_ms[4] = 1e-6 * (double)wait_ns.load() / (double)std::max<size_t>(1, range_threads(h.noct));
+  g.dropin_ms[4] = 1e-6 * (double)wait_ns.load() / (double)std::max<size_t>(1, range_threads(h.nown));
   // fine -> coarse corrections: fieldnew = U2W(W2U(fieldnew) + dU) per coarse cell
   if (coarse) {
     const double *p = pc;
@@ -1724,18 +1737,16 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   }
   g.updates += d.leaf;
   const auto t5 = Clock::now();
-  // the rest of the final update: octs of other ranks (not mirrored) and split
-  // cells (src/hydro_utils.c:3408-3483)
-  if (final_update && (split_l || (long long)wl.size() != h.noct)) {
+  // the rest of the final update: split cells of this rank's octs (the octs of
+  // other ranks are left to the caller's exchange, src/hydro_utils.c:3408-3483)
+  if (final_update && split_l) {
     parallel_for((long long)wl.size(), [&](long long a0, long long b0) {
       for (long long i = a0; i < b0; i++) {
         struct OCT *o = wl[i];
+        if (o->cpu != rank) continue;
         for (int c = 0; c < 8; c++) {
           struct CELL *cell = &o->cell[c];
-          if (cell->child == nullptr) {
-            if (o->cpu != rank) cell->field = cell->fieldnew;
-            continue;
-          }
+          if (cell->child == nullptr) continue;
           struct Wtype W;
           std::memset(&W, 0, sizeof(W));
           for (int j = 0; j < 8; j++) {
@@ -1760,7 +1771,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   g.dropin_ms[5] = ms(t4, t5);
   g.dropin_ms[6] = ms(t5, t6);
   g.dropin_ms[7] = ms(t0, t6);
-  return h.noct;
+  return h.nown;
 }
 
 int advancehydroGPU(struct OCT **firstoct, int level, struct CPUINFO *cpu, struct HGRID *stencil, int stride,
@@ -1779,10 +1790,22 @@ void HydroSolver(int level, struct RUNPARAMS *param, struct OCT **firstoct, stru
   dropin_advance(firstoct, level, cpu, dtnew, true);
 }
 
-// fieldnew := field on every cell of the level (src/hydro_utils.c clean_new_hydro)
+// The leading members of the reference's struct RUNPARAMS (src/prototypes.h,
+// npartmax..lmax, REAL = double); clean_new_hydro reads lcoarse.
+struct RunParamsHead {
+  int npartmax, ngridmax, nbuff, ndumps;
+  double dt_dump;
+  int nsteps, lcoarse, lmax;
+};
+static_assert(offsetof(RunParamsHead, lcoarse) == 28, "RUNPARAMS head layout");
+
+// fieldnew := field on every cell of the level (src/hydro_utils.c:3501-3522).
+// A multi-rank run (-DWMPI, :3524-3544) also zeroes fieldnew of the octs of
+// other ranks one level coarser when level > lcoarse, so that they collect only
+// this rank's fine->coarse corrections (src/communication.c:2959 sends them to
+// their owners).  Ranks of a single-rank tree are all cpu->rank: nothing is
+// zeroed.  Without `param` every level above 1 counts as finer than lcoarse.
 void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu) {
-  (void)param;
-  (void)cpu;
   if (firstoct == nullptr || level < 1) return;
   if (level >= kMaxLevels) return;
   const std::vector<struct OCT *> &v = walk_level(firstoct, level);
@@ -1790,6 +1813,12 @@ void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, 
     for (long long i = a0; i < b0; i++)
       for (int c = 0; c < 8; c++) v[i]->cell[c].fieldnew = v[i]->cell[c].field;
   });
+  const int rank = dropin_rank(cpu);
+  const int lcoarse = param ? reinterpret_cast<const RunParamsHead *>(param)->lcoarse : 1;
+  if (level > lcoarse && level >= 2)
+    for (struct OCT *o = firstoct[level - 2]; o != nullptr; o = o->next)
+      if (o->cpu != rank)
+        for (int c = 0; c < 8; c++) std::memset(&o->cell[c].fieldnew, 0, sizeof(struct Wtype));
 }
 
 #ifdef EMMA_WGRAV

@@ -284,7 +284,8 @@ bool check_brick(Planner &P, int L, const Box &G, const uint32_t *keys, uint32_t
   return true;
 }
 
-// Bricks of a shape holding the level's octs, in order of their first oct.
+// Bricks of a shape holding the first `noct` octs of the level (this rank's), in
+// order of their first oct.
 std::vector<std::vector<int>> group_bricks(const std::vector<int32_t> &pos, int noct, const BrickShape &sh) {
   std::unordered_map<uint64_t, int> brick;
   std::vector<std::vector<int>> members;
@@ -315,14 +316,14 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
   lv.interp.clear();
   lv.reads_coarse = false;
   lv.shape = 0;
-  if (lv.noct == 0) return 0;
+  if (lv.nown == 0) return 0;
   int shape = shape_req;
   std::vector<std::vector<int>> members;
   if (shape < 0 || shape >= kNumShapes) {
     // without a requested shape: the cheaper by tiles x tile cost
     double best = 0;
     for (int s = 0; s < kNumShapes; s++) {
-      auto m = group_bricks(lv.pos, lv.noct, kShapes[s]);
+      auto m = group_bricks(lv.pos, lv.nown, kShapes[s]);
       const double c = kTileCost[s] * (double)((m.size() + kShapes[s].nb - 1) / kShapes[s].nb);
       if (s == 0 || c < best) {
         best = c;
@@ -331,7 +332,7 @@ int plan_level(Planner &P, HostTree &H, int L, int shape_req, std::string &err) 
       }
     }
   } else {
-    members = group_bricks(lv.pos, lv.noct, kShapes[shape]);
+    members = group_bricks(lv.pos, lv.nown, kShapes[shape]);
   }
   const BrickShape &sh = kShapes[shape];
   const Box G(sh);
@@ -450,7 +451,16 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
     lv.L = L;
     for (struct OCT *o = firstoct[L - 1]; o != nullptr; o = o->next)
       if (o->cpu == rank) lv.octs.push_back(o);
+    lv.nown = (int)lv.octs.size();
+    // octs of other ranks (the boundary octs of a multi-rank run, refreshed by the
+    // caller's exchange before each solve): staged as neighbours, never advanced;
+    // their coarser cells collect fine->coarse corrections in fieldnew like this
+    // rank's (src/hydro_utils.c:2997,3124,3417 skip them; src/communication.c:510
+    // sends those fieldnew back to the owners)
+    for (struct OCT *o = firstoct[L - 1]; o != nullptr; o = o->next)
+      if (o->cpu != rank) lv.octs.push_back(o);
     lv.noct = (int)lv.octs.size();
+    if (lv.noct > lv.nown) H.ghosts = 1;
     if (lv.noct >= (1 << 25)) {
       err = "level too large for 28-bit keys";
       return EMMA_ST_ARG;
@@ -470,7 +480,7 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
           lv.split[i] |= (uint8_t)(1 << c);
           const int j = (L + 1 <= lmax) ? P.idx[L + 1].get(ch) : -1;
           lv.child[8 * i + c] = j;
-        } else {
+        } else if (i < lv.nown) {
           lv.leaf++;
         }
       }
@@ -566,7 +576,7 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
         const int nb = m / sh.octs(), i = m % sh.octs();
         const int sx = 1 + i % sh.bx, sy = 1 + (i / sh.bx) % sh.by, sz = 1 + i / (sh.bx * sh.by);
         const uint32_t key = keys[nb * sh.slots() + sx + (sh.bx + 2) * (sy + (sh.by + 2) * sz)];
-        if ((key >> 28) != kKeyReal || seen[key & 0x0FFFFFFFu]) {
+        if ((key >> 28) != kKeyReal || (key & 0x0FFFFFFFu) >= (uint32_t)lv.nown || seen[key & 0x0FFFFFFFu]) {
           err = "tile oct missing or advanced twice at level " + std::to_string(L);
           return EMMA_ST_TREE;
         }
@@ -574,11 +584,11 @@ int validate_host_tree(const HostTree &H, int plan_lo, int plan_hi, std::string 
         covered++;
       }
     }
-    if (covered != lv.noct) {
+    if (covered != lv.nown) {
       err = "tiles do not cover level " + std::to_string(L);
       return EMMA_ST_TREE;
     }
-    for (size_t i = 0; i < lv.child.size(); i++) {
+    for (size_t i = 0; i < 8 * (size_t)lv.nown; i++) {  // children of this rank's octs
       const bool split = (lv.split[i >> 3] >> (i & 7)) & 1;
       if (split && (lv.child[i] < 0 || lv.child[i] >= nfine) && L < H.lmax) {
         err = "split cell without a mirrored child at level " + std::to_string(L);

@@ -10,9 +10,11 @@ namespace emma {
 
 struct HostLevel {
   int L = 0;
-  int noct = 0;
-  long long leaf = 0;                 // leaf cells
-  std::vector<struct OCT *> octs;     // list order (cpu == rank)
+  int noct = 0;                       // mirrored octs: nown of this rank, then ghosts
+  int nown = 0;                       // octs with cpu == rank (advanced); octs[nown..noct) are the
+                                      // octs of other ranks (staged as neighbours, never advanced)
+  long long leaf = 0;                 // leaf cells of this rank's octs
+  std::vector<struct OCT *> octs;     // this rank's octs in list order, then the others in list order
   std::vector<uint8_t> split;         // per oct: bit c set if cell c has a child
   std::vector<int32_t> child;         // per cell: index of the child oct at L+1, or -1
   std::vector<TileDesc> tiles;        // brick tiles, in order of their first oct in the list
@@ -29,6 +31,7 @@ struct HostTree {
   int lcoarse = 0, lmax = 0, rank = 0, trans = 0;
   int grav = 0;  // gravity coupling: injected coarser cells carry interpolated forces
   int dual = 0;  // dual energy: split cells next to a leaf are reconstructed too (their faces enter div u)
+  int ghosts = 0;  // some level list holds octs of other ranks (a multi-rank run's boundary octs)
   std::vector<HostLevel> lev;  // indexed by level (0..lmax)
 };
 

@@ -209,6 +209,27 @@ void emma_tree_get_field(struct EmmaTree *t, int level, int which, double *out7)
     }
 }
 
+void emma_tree_put_field(struct EmmaTree *t, int level, int which, const double *in7) {
+  long long n = 8LL * emma_tree_noct(t, level), i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) {
+      struct Wtype *W = which ? &o->cell[c].fieldnew : &o->cell[c].field;
+      long long k = 8 * i + c;
+      W->d = in7[k];
+      W->u = in7[n + k];
+      W->v = in7[2 * n + k];
+      W->w = in7[3 * n + k];
+      W->p = in7[4 * n + k];
+      W->a = in7[5 * n + k];
+      W->E = in7[6 * n + k];
+    }
+}
+
+void emma_tree_set_cpu(struct EmmaTree *t, int level, const int *cpu) {
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++) o->cpu = cpu[i];
+}
+
 #ifdef EMMA_WGRAV
 void emma_tree_set_force(struct EmmaTree *t, int level, const double *fx, const double *fy, const double *fz) {
   long long i = 0;

@@ -122,21 +122,43 @@ class ResidentHydro:
         check(lib().emma_hydro_tree_download(self.tree.firstoct), "tree_download")
 
 
+class CpuInfo(ctypes.Structure):
+    """The part of the reference's struct CPUINFO (src/prototypes.h) the drop-in
+    entries read: `rank`, its first member."""
+    _fields_ = [("rank", ctypes.c_int), ("nproc", ctypes.c_int)]
+
+
+class RunParams(ctypes.Structure):
+    """The leading members of the reference's struct RUNPARAMS (src/prototypes.h,
+    REAL = double) up to lmax; clean_new_hydro reads lcoarse."""
+    _fields_ = [("npartmax", ctypes.c_int), ("ngridmax", ctypes.c_int), ("nbuff", ctypes.c_int),
+                ("ndumps", ctypes.c_int), ("dt_dump", ctypes.c_double), ("nsteps", ctypes.c_int),
+                ("lcoarse", ctypes.c_int), ("lmax", ctypes.c_int)]
+
+
+def _ref(x):
+    return None if x is None else ctypes.byref(x)
+
+
 def HydroSolver(level, firstoct, dtnew, cpu=None, grav=False):
     """Drop-in HydroSolver (src/hydro_utils.c:3378) on a host tree; grav: a tree of
-    the -DWGRAV layout through libemmahydro_grav.so (gravity-coupled advance)."""
-    lib(grav).HydroSolver(level, None, firstoct, cpu, None, 0, dtnew)
+    the -DWGRAV layout through libemmahydro_grav.so (gravity-coupled advance).
+    cpu: a CpuInfo (advance the octs of cpu.rank only), or None for rank 0."""
+    lib(grav).HydroSolver(level, None, firstoct, _ref(cpu), None, 0, dtnew)
 
 
 def advancehydroGPU(firstoct, level, dtnew, cpu=None, grav=False):
     """Drop-in advancehydroGPU (src/hydro_utils_gpu.cu:2470); returns octs advanced."""
-    return lib(grav).advancehydroGPU(firstoct, level, cpu, None, 0, 0.5 ** level, dtnew)
+    return lib(grav).advancehydroGPU(firstoct, level, _ref(cpu), None, 0, 0.5 ** level, dtnew)
 
 
-def clean_new_hydro(level, firstoct, grav=False):
-    lib(grav).clean_new_hydro(level, None, firstoct, None)
+def clean_new_hydro(level, firstoct, grav=False, cpu=None, param=None):
+    """Drop-in clean_new_hydro (src/hydro_utils.c:3501); param: a RunParams
+    (its lcoarse decides whether the coarser level's octs of other ranks start
+    from zero, as in a -DWMPI run)."""
+    lib(grav).clean_new_hydro(level, _ref(param), firstoct, _ref(cpu))
 
 
 def grav_correction(level, firstoct, dt, cpu=None):
     """Drop-in grav_correction (src/hydro_utils.c:2388) of libemmahydro_grav.so."""
-    lib(True).grav_correction(level, None, firstoct, cpu, dt)
+    lib(True).grav_correction(level, None, firstoct, _ref(cpu), dt)

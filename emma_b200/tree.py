@@ -85,6 +85,22 @@ class OctTree:
             self._L.emma_tree_get_field(self._t, level, which, ptr(out))
         return out
 
+    def put_fields(self, level, w7, which=0):
+        """Write (7, 8*noct) d,u,v,w,p,a,E as they are into `field` (which=0) or
+        `fieldnew` (which=1): the inverse of get_fields."""
+        n = self.noct(level)
+        w7 = np.ascontiguousarray(w7, dtype=np.float64)
+        assert w7.shape == (7, 8 * n)
+        if n:
+            self._L.emma_tree_put_field(self._t, level, which, ptr(w7))
+
+    def set_cpu(self, level, ranks):
+        """Owner rank (struct OCT cpu) of every oct of a level, in list order."""
+        r = np.ascontiguousarray(ranks, dtype=np.int32)
+        assert r.size == self.noct(level)
+        if r.size:
+            self._L.emma_tree_set_cpu(self._t, level, ptr(r))
+
     def topology(self, level):
         n = self.noct(level)
         nei = np.zeros(6 * n, np.int32)

@@ -251,6 +251,12 @@ void emma_tree_oct_xyz(struct EmmaTree *t, int level, double *xyz);
 void emma_tree_set_field(struct EmmaTree *t, int level, const double *d, const double *u,
                          const double *v, const double *w, const double *p);
 void emma_tree_get_field(struct EmmaTree *t, int level, int which, double *out7);
+/* Inverse of emma_tree_get_field: writes d,u,v,w,p,a,E (planes of 8*noct) as
+ * they are into `field` (which=0) or `fieldnew` (which=1). */
+void emma_tree_put_field(struct EmmaTree *t, int level, int which, const double *in7);
+/* Owner rank (struct OCT cpu) of every oct of the level, in list order: the
+ * octs of other ranks are a multi-rank run's boundary octs. */
+void emma_tree_set_cpu(struct EmmaTree *t, int level, const int *cpu);
 void emma_tree_topology(struct EmmaTree *t, int level, int *nei, int *parent, int *child, int *lev);
 
 #ifdef __cplusplus

@@ -30,3 +30,28 @@ def l1_rel(a, b, vol=None):
 
 def same_tree_fields(tree_a, tree_b, levels, which=0):
     return all(np.array_equal(tree_a.get_fields(l, which), tree_b.get_fields(l, which)) for l in levels)
+
+
+def rank_of_octs(tree, level, partition):
+    """Owner rank of every oct of a level, from the position of its level-lcoarse
+    ancestor (finer octs inherit their owner, as in the reference's Hilbert-key
+    partition): `partition(ix, iy, iz)` on the integer ancestor coordinates."""
+    n = 1 << (tree.lcoarse - 1)
+    xyz = tree.oct_xyz(level).reshape(-1, 3)
+    ijk = np.floor(xyz * n).astype(np.int64)
+    return np.asarray(partition(ijk[:, 0], ijk[:, 1], ijk[:, 2]), dtype=np.int32)
+
+
+def assign_ranks(tree, partition, levels=None):
+    """Tag every oct of levels 1..lmax (or `levels`) with its owner rank."""
+    for l in (range(1, tree.lmax + 1) if levels is None else levels):
+        if tree.noct(l):
+            tree.set_cpu(l, rank_of_octs(tree, l, partition))
+
+
+# partitions of the level-lcoarse grid (n octs per axis) used by the multi-rank tests
+PARTITIONS = {
+    "halves": (2, lambda i, j, k, n=8: (i >= n // 2).astype(np.int32)),
+    "quadrants": (4, lambda i, j, k, n=8: ((i >= n // 2) + 2 * (j >= n // 2)).astype(np.int32)),
+    "stripes3": (3, lambda i, j, k: ((i + j + k) % 3).astype(np.int32)),
+}

@@ -68,3 +68,24 @@ def test_transmissive_corners_are_refused():
     assert lib().emma_hydro_plan_stats(t.firstoct, 4, 4, 0x0F, st) & 0x08
     lib().emma_hydro_clear_status()
     assert lib().emma_hydro_plan_stats(t.firstoct, 4, 4, 0x03, st) == 0
+
+
+@pytest.mark.parametrize("part", ["halves", "quadrants", "stripes3"])
+def test_multi_rank_tree_plans_this_ranks_octs(part):
+    """Octs of other ranks (a multi-rank run's boundary octs) are staged as
+    neighbours and never tiled: the plan of rank 0 covers exactly its own octs
+    and leaf cells."""
+    from helpers import PARTITIONS, assign_ranks, rank_of_octs
+    cfg = configs.small_amr(base=4, radii=(0.3, 0.15))
+    t = cfg.build()
+    nrank, fn = PARTITIONS[part]
+    assign_ranks(t, fn)
+    rc, stats = plan_stats(cfg, t)
+    assert rc == 0, lib().emma_hydro_last_error()
+    for i, (octs, tiles, max_staged, staged, leaf) in enumerate(stats):
+        l = cfg.lcoarse + i
+        own = rank_of_octs(t, l, fn) == 0
+        assert octs == own.sum()
+        leaves = ~t.split_mask(l).reshape(-1, 8)
+        assert leaf == leaves[own].sum()
+        assert (tiles > 0) == (octs > 0)
