@@ -9,7 +9,10 @@
 #include <cstddef>
 #include <cstdio>
 #include <cstdlib>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -40,6 +43,8 @@ namespace {
 
 constexpr double kG = 5. / 3.;
 constexpr long long kWaitLimit = 1LL << 24;  // ~1 s of __nanosleep(64) polls
+constexpr unsigned kMaxHostThreads = 64;      // host threads of the drop-in's parallel passes
+constexpr unsigned kDefaultHostThreads = 32;  // without EMMA_HYDRO_HOST_THREADS
 
 struct DevLevel {
   int L = 0, noct = 0, ntiles = 0;
@@ -115,7 +120,7 @@ struct Ctx {
   long long h2d_bytes = 0, d2h_bytes = 0;  // host<->device state copies
   double dropin_ms[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // phases of the last drop-in call
   std::vector<cudaEvent_t> range_ev;        // per host thread and sub-range of a drop-in download
-  std::vector<double> exc[16];              // per host thread: drop-in cells whose fieldnew differs
+  std::vector<double> exc[kMaxHostThreads];  // per host thread: drop-in cells whose fieldnew differs
   double *pin_exc = nullptr;                // their pinned staging
   size_t pin_exc_bytes = 0;
   double *d_exc = nullptr;                  // and device copy
@@ -181,11 +186,82 @@ bool ensure_pin(size_t bytes) {
   return true;
 }
 
-// Host threads of a parallel pass over n items: up to 16, one for small passes.
-unsigned range_threads(long long n) {
-  const unsigned nt = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-  return n < 4096 ? 1u : nt;
+// Persistent host workers for the drop-in's parallel passes over the caller's
+// tree (packing, unpacking, hashing, clean_new_hydro): several passes run per
+// call, so threads are started once instead of per pass.  run(nt, job) runs
+// job(t) for t in [0, nt), t = 0 on the calling thread, and returns when all
+// are done; workers make the caller's CUDA device current before their share.
+// Never destroyed: the workers sleep on the condition variable until exit.
+class HostPool {
+ public:
+  explicit HostPool(unsigned n) : n_(n) {
+    for (unsigned i = 1; i < n; i++) std::thread([this, i] { loop(i); }).detach();
+  }
+  unsigned size() const { return n_; }
+  void run(unsigned nt, const std::function<void(unsigned)> &job) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    {
+      std::lock_guard<std::mutex> lk(m_);
+      job_ = &job;
+      nt_ = nt;
+      dev_ = dev;
+      pending_ = nt - 1;
+      gen_++;
+    }
+    cv_.notify_all();
+    job(0);
+    std::unique_lock<std::mutex> lk(m_);
+    done_.wait(lk, [&] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void loop(unsigned i) {
+    unsigned long long seen = 0;
+    int dev_set = -1;
+    for (;;) {
+      const std::function<void(unsigned)> *job = nullptr;
+      int dev = 0;
+      {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [&] { return gen_ != seen; });
+        seen = gen_;
+        if (i >= nt_) continue;
+        job = job_;
+        dev = dev_;
+      }
+      if (dev != dev_set && cudaSetDevice(dev) == cudaSuccess) dev_set = dev;
+      (*job)(i);
+      std::lock_guard<std::mutex> lk(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  const unsigned n_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  const std::function<void(unsigned)> *job_ = nullptr;
+  unsigned nt_ = 0, pending_ = 0;
+  int dev_ = 0;
+  unsigned long long gen_ = 0;
+};
+
+// Host threads of the parallel passes: EMMA_HYDRO_HOST_THREADS if set, else the
+// hardware threads, at most kMaxHostThreads (and kDefaultHostThreads by default).
+HostPool &host_pool() {
+  static HostPool *pool = [] {
+    unsigned n = std::min(kDefaultHostThreads, std::max(1u, std::thread::hardware_concurrency()));
+    if (const char *e = std::getenv("EMMA_HYDRO_HOST_THREADS")) {
+      const long v = std::strtol(e, nullptr, 10);
+      if (v >= 1) n = (unsigned)std::min<long>(v, (long)kMaxHostThreads);
+    }
+    return new HostPool(n);
+  }();
+  return *pool;
 }
+
+// Host threads of a parallel pass over n items: the pool, one for small passes.
+unsigned range_threads(long long n) { return n < 4096 ? 1u : host_pool().size(); }
 
 // Runs f(t, a, b) over [0, n) split into contiguous ranges, one per host
 // thread t; every range start is a multiple of `align`.
@@ -196,15 +272,13 @@ void parallel_ranges(long long n, F f, long long align = 1) {
     f(0, 0LL, n);
     return;
   }
-  std::vector<std::thread> th;
   long long chunk = (n + nt - 1) / nt;
   chunk = (chunk + align - 1) / align * align;
-  for (unsigned t = 0; t < nt; t++) {
-    long long a = t * chunk, b = std::min(n, a + chunk);
-    if (a >= b) break;
-    th.emplace_back([=] { f((int)t, a, b); });
-  }
-  for (auto &t : th) t.join();
+  const std::function<void(unsigned)> job = [&](unsigned t) {
+    const long long a = t * chunk, b = std::min(n, a + chunk);
+    if (a < b) f((int)t, a, b);
+  };
+  host_pool().run(nt, job);
 }
 
 template <class F>
@@ -465,7 +539,7 @@ long long dropin_subrange(long long noct) {
 }
 
 bool ensure_range_events() {
-  while (g.range_ev.size() < 16 * (size_t)kSubRanges) {
+  while (g.range_ev.size() < kMaxHostThreads * (size_t)kSubRanges) {
     cudaEvent_t e;
     if (!ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate")) return false;
     g.range_ev.push_back(e);
@@ -1809,9 +1883,15 @@ void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, 
   if (firstoct == nullptr || level < 1) return;
   if (level >= kMaxLevels) return;
   const std::vector<struct OCT *> &v = walk_level(firstoct, level);
+  // written only where the bytes differ: after HydroSolver's final update most
+  // cells already hold fieldnew == field, and a cache line left clean is not
+  // written back to memory (the pass then costs one read of the cells)
   parallel_for((long long)v.size(), [&](long long a0, long long b0) {
     for (long long i = a0; i < b0; i++)
-      for (int c = 0; c < 8; c++) v[i]->cell[c].fieldnew = v[i]->cell[c].field;
+      for (int c = 0; c < 8; c++) {
+        struct CELL &cl = v[i]->cell[c];
+        if (std::memcmp(&cl.fieldnew, &cl.field, sizeof(struct Wtype)) != 0) cl.fieldnew = cl.field;
+      }
   });
   const int rank = dropin_rank(cpu);
   const int lcoarse = param ? reinterpret_cast<const RunParamsHead *>(param)->lcoarse : 1;

@@ -60,8 +60,9 @@ struct OCT {             /* src/prototypes.h:1028 */
   int level;             /* level of the cells of this oct */
 };
 
-/* Opaque in this library: only `rank` (the first member, offset 0 under every
- * compile-time flag set of the reference) is read by the drop-in entries. */
+/* Opaque in this library: the drop-in entries read only CPUINFO's `rank` (the
+ * first member, offset 0 under every compile-time flag set of the reference) and,
+ * in clean_new_hydro, RUNPARAMS's `lcoarse` (offset 28 with REAL = double). */
 struct CPUINFO;
 struct RUNPARAMS;
 struct HGRID;

@@ -49,9 +49,13 @@ def assign_ranks(tree, partition, levels=None):
             tree.set_cpu(l, rank_of_octs(tree, l, partition))
 
 
-# partitions of the level-lcoarse grid (n octs per axis) used by the multi-rank tests
+# partitions of the 8^3-oct level-lcoarse grid used by the multi-rank tests; the
+# off-centre cuts of "slabs" and "quadrants" cross the coarse-fine boundaries of
+# trees refined in spheres about the box centre, so fine->coarse corrections go
+# from one rank to another (central cuts only meet fine octs across faces)
 PARTITIONS = {
-    "halves": (2, lambda i, j, k, n=8: (i >= n // 2).astype(np.int32)),
-    "quadrants": (4, lambda i, j, k, n=8: ((i >= n // 2) + 2 * (j >= n // 2)).astype(np.int32)),
+    "halves": (2, lambda i, j, k: (i >= 4).astype(np.int32)),
+    "slabs": (2, lambda i, j, k: (i >= 5).astype(np.int32)),
+    "quadrants": (4, lambda i, j, k: ((i >= 5) + 2 * (j >= 3)).astype(np.int32)),
     "stripes3": (3, lambda i, j, k: ((i + j + k) % 3).astype(np.int32)),
 }

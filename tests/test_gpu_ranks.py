@@ -168,7 +168,7 @@ def check_owned(trees, owner, ref, tol=1e-12):
                 assert e.max() <= tol, (l, r, e.max())
 
 
-@pytest.mark.parametrize("part", ["halves", "quadrants", "stripes3"])
+@pytest.mark.parametrize("part", ["slabs", "quadrants", "stripes3"])
 def test_multi_rank_dropin_matches_single_rank_oracle(gpu, part):
     trees, owner = run_ranks(part)
     check_owned(trees, owner, run_single())
@@ -186,7 +186,7 @@ def test_multi_rank_dropin_dual_energy(gpu):
     L.emma_hydro_default_options(ctypes.byref(o))
     o.dual_energy = 1
     assert L.emma_hydro_set_options(ctypes.byref(o)) == 0
-    trees, owner = run_ranks("halves", dual=True)
+    trees, owner = run_ranks("slabs", dual=True)
     check_owned(trees, owner, run_single(dual=True))
 
 
