@@ -64,6 +64,8 @@ SIGNATURES = [
     ("emma_hydro_set_level_state", c_int, [c_int, c_void_p]),
     ("emma_hydro_set_level_force", c_int, [c_int, c_void_p]),
     ("emma_hydro_is_resident", c_int, [c_void_p]),
+    ("emma_hydro_dump_alloct", c_int, [ctypes.c_char_p, c_void_p, c_int, c_int, c_int, c_int, c_double, c_int,
+                                       c_void_p, c_void_p]),
     ("emma_hydro_save_amr", c_int, [ctypes.c_char_p, c_void_p, c_double, c_double, c_int, c_int, c_int, c_int,
                                     c_void_p, c_void_p, c_void_p]),
     ("emma_hydro_restore_amr", c_int, [ctypes.c_char_p, c_void_p, c_void_p, c_int, c_ll, c_void_p, P(c_double),

@@ -35,6 +35,9 @@ cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int
                           bool grav);
 cudaError_t launch_dropin_base(const double *wb, double *base, long long n8, const double *exc, long long nexc, int nsm,
                                cudaStream_t s);
+bool resident_level(struct OCT **firstoct, int level, const HostLevel **h, const double **W, const uint8_t **split,
+                    cudaStream_t *stream, int *nsm);
+void release_dump_staging();
 }  // namespace emma
 
 using namespace emma;
@@ -771,6 +774,20 @@ bool write_sched_params(double dt_param, double time_max, int nsub, const double
 
 }  // namespace
 
+// The resident tree's mirror of a level and the level's current device state (5
+// planes), for the field dumps; false unless `firstoct` is the resident tree's.
+bool emma::resident_level(struct OCT **firstoct, int level, const HostLevel **h, const double **W,
+                          const uint8_t **split, cudaStream_t *stream, int *nsm) {
+  if (!(g.ready && g.res.valid && firstoct != nullptr && g.res_first == firstoct)) return false;
+  if (level < g.res.lcoarse || level > g.res.lmax) return false;
+  *h = &g.res.host.lev[level];
+  *W = current_state(level);
+  *split = g.res.lev[level].split;
+  *stream = g.stream;
+  *nsm = g.nsm;
+  return *W != nullptr;
+}
+
 extern "C" {
 
 int emma_hydro_status(void) {
@@ -865,6 +882,7 @@ void emma_hydro_shutdown(void) {
   cudaFreeHost(g.h_S);
   if (g.pin) cudaFreeHost(g.pin);
   if (g.own_stream) cudaStreamDestroy(g.stream);
+  release_dump_staging();
   g = Ctx();
 }
 

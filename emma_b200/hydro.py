@@ -159,6 +159,16 @@ def clean_new_hydro(level, firstoct, grav=False, cpu=None, param=None):
     lib(grav).clean_new_hydro(level, _ref(param), firstoct, _ref(cpu))
 
 
+def dump_alloct(folder, firstoct, lcoarse, lmax, ids, names, rank=0, ndumps=0, tsim=0.0, grav=False):
+    """Field dump in the reference's ALLOCT format (dumpalloct_serial, src/io.c:1233):
+    one file per (id, name) under folder (ending in '/').  A tree resident on the
+    GPU dumps its hydro fields (ids 13-17) from the device state."""
+    idv = (ctypes.c_int * len(ids))(*ids)
+    nv = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
+    return lib(grav).emma_hydro_dump_alloct(folder.encode(), firstoct, lcoarse, lmax, rank, ndumps, tsim, len(ids),
+                                            ctypes.cast(idv, ctypes.c_void_p), ctypes.cast(nv, ctypes.c_void_p))
+
+
 def grav_correction(level, firstoct, dt, cpu=None):
     """Drop-in grav_correction (src/hydro_utils.c:2388) of libemmahydro_grav.so."""
     lib(True).grav_correction(level, None, firstoct, _ref(cpu), dt)

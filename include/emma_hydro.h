@@ -165,6 +165,21 @@ int emma_hydro_restore_amr(const char *filename, struct OCT **firstoct, struct O
                            int *ndumps, int *lcoarse, int *lmax, double *adt, double *units7,
                            struct OCT **freeoct);
 
+/* Field dump in the reference's ALLOCT format, dumpalloct_serial (src/io.c:1233).
+ * One file per field i: <folder>grid_<names[i]>/<names[i]>.<ndumps %05d>.p<rank %05d>
+ * (folder ends with '/'; the directory is created), holding int n_cell and seven
+ * 4-byte words (the first 4 bytes of the double tsim, then xmin, xmax, ymin, ymax,
+ * zmin, zmax of the dumped octs as floats), then one float per dumped cell: the
+ * cells without a child (every cell at lmax) of the octs with cpu == rank, levels
+ * lcoarse..lmax in list order.  ids are assign_grid_field's (src/io.c:32): 0-2
+ * cell corner x,y,z, 3 level, 4 cpu, 12 marked, 13-17 field d,u,v,w,p; the
+ * -DWGRAV library also 5 gdata.d, 7 gdata.p, 8 res, 9-11 f.  For a tree resident
+ * on the GPU, ids 13-17 come from the device state (compacted to floats on the
+ * GPU), the others from the host tree.  Returns 0, EMMA_ST_ARG (bad argument,
+ * unknown id, file error) or EMMA_ST_CUDA. */
+int emma_hydro_dump_alloct(const char *folder, struct OCT **firstoct, int lcoarse, int lmax, int rank, int ndumps,
+                           double tsim, int nfields, const int *ids, const char *const *names);
+
 /* SoA access for tests and I/O: 5 planes (d,u,v,w,p) of 8*noct doubles each, list order. */
 int emma_hydro_level_noct(int level);
 int emma_hydro_get_level_state(int level, double *host_out);

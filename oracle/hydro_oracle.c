@@ -15,7 +15,10 @@
  *   scatter + fine->coarse correction       src/hydro_utils.c:3096-3303
  *   field := fieldnew, split-cell averaging src/hydro_utils.c:3408-3483
  * plus clean_new_hydro (:3501), L_comptstep_hydro (src/advanceamr.c:92) and the
- * hydro-only subset of Advance_level (src/advanceamr.c:243-1299).
+ * hydro-only subset of Advance_level (src/advanceamr.c:243-1299), and the
+ * ALLOCT field dump dumpalloct_serial (src/io.c:1233) -- the dump alone is
+ * parity unpinned: io.c does not build without MPI and the reference holds no
+ * dump fixtures, so it follows the source as read.
  *
  * Every floating-point expression keeps the reference's operation order so the
  * results are bit-identical when both are built with gcc -O2 -ffp-contract=off
@@ -1007,3 +1010,107 @@ void orc_grav_free(void *h) {
   free(C);
 }
 #endif
+
+/* ---- ALLOCT field dump: dumpalloct_serial (src/io.c:1233-1358) -------------
+ * For each selected field: directory <folder>grid_<name>/ (mkdir 0755) and file
+ * <name>.<ndumps %05d>.p<rank %05d> in it (:1274-1283).  Header (:1291-1298,
+ * rewritten with the final values at :1349-1356): int n_cell, then tsim, xmin,
+ * xmax, ymin, ymax, zmin, zmax as 4-byte words; tsim is the caller's double, of
+ * which fwrite(&tsim, sizeof(float)) writes the first 4 bytes.  Body
+ * (:1304-1340): levels lcoarse..lmax, the octs of `rank` in list order
+ * (cpu->octList, src/oct.c:250-270), and in each oct the cells without a child
+ * (every cell when the oct is at lmax), one float per field and cell, the value of
+ * assign_grid_field (src/io.c:32-104): 0-2 cell corner x,y,z, 3 level, 4 cpu,
+ * 12 marked, 13-17 field d,u,v,w,p; with ORC_WGRAV 5 gdata.d, 7 gdata.p, 8 res,
+ * 9-11 f[0..2].  The bounds are the min of the oct corners and the max of corner
+ * + oct size 0.5^(level-1) over the dumped cells, kept as floats.
+ * Returns 0, or -1 for an id this layout has no member for or an I/O error. */
+#include <stdio.h>
+#include <sys/stat.h>
+
+static int orc_grid_field(int id, const oOct *o, const oCell *c, float *v) {
+  const double dxc = pow(0.5, o->level);
+  switch (id) {
+    case 0: *v = (float)(o->x + (double)(c->idx & 1) * dxc); return 0;
+    case 1: *v = (float)(o->y + (double)((c->idx >> 1) & 1) * dxc); return 0;
+    case 2: *v = (float)(o->z + (double)(c->idx >> 2) * dxc); return 0;
+    case 3: *v = (float)o->level; return 0;
+    case 4: *v = (float)o->cpu; return 0;
+#ifdef ORC_WGRAV
+    case 5: *v = (float)c->gd; return 0;
+    case 7: *v = (float)c->gp; return 0;
+    case 8: *v = (float)c->res; return 0;
+    case 9: case 10: case 11: *v = (float)c->f[id - 9]; return 0;
+#endif
+    case 12: *v = (float)c->marked; return 0;
+    case 13: *v = (float)c->field.d; return 0;
+    case 14: *v = (float)c->field.u; return 0;
+    case 15: *v = (float)c->field.v; return 0;
+    case 16: *v = (float)c->field.w; return 0;
+    case 17: *v = (float)c->field.p; return 0;
+    default: return -1;
+  }
+}
+
+static void orc_alloct_header(FILE *f, int n, double tsim, const float b[6]) {
+  fwrite(&n, sizeof(int), 1, f);
+  fwrite(&tsim, 4, 1, f);
+  fwrite(b, sizeof(float), 6, f);
+}
+
+int orc_dump_alloct(const char *folder, void **firstoct, int lcoarse, int lmax, int rank, int ndumps, double tsim,
+                    int nfields, const int *ids, const char *const *names) {
+  FILE *fp[32];
+  float b[6] = {2.f, -1.f, 2.f, -1.f, 2.f, -1.f};  /* xmin, xmax, ymin, ymax, zmin, zmax */
+  int n = 0, i, level, c, rc = 0;
+  char dir[512], path[1024];
+  if (nfields < 1 || nfields > 32) return -1;
+  for (i = 0; i < nfields; i++) {
+    float probe;
+    oCell dummy_cell;
+    oOct dummy_oct;
+    memset(&dummy_oct, 0, sizeof(dummy_oct));
+    memset(&dummy_cell, 0, sizeof(dummy_cell));
+    if (orc_grid_field(ids[i], &dummy_oct, &dummy_cell, &probe) != 0) return -1;
+  }
+  for (i = 0; i < nfields; i++) {
+    snprintf(dir, sizeof(dir), "%sgrid_%s/", folder, names[i]);
+    mkdir(dir, 0755);
+    snprintf(path, sizeof(path), "%s%s.%05d.p%05d", dir, names[i], ndumps, rank);
+    fp[i] = fopen(path, "wb");
+    if (fp[i] == NULL) {
+      while (i-- > 0) fclose(fp[i]);
+      return -1;
+    }
+    orc_alloct_header(fp[i], 0, tsim, b);
+  }
+  for (level = lcoarse; level <= lmax; level++) {
+    const double dx = pow(0.5, level - 1);
+    const oOct *o;
+    for (o = (const oOct *)firstoct[level - 1]; o != NULL; o = o->next) {
+      if (o->cpu != rank) continue;
+      for (c = 0; c < 8; c++) {
+        if (o->cell[c].child != NULL && o->level != lmax) continue;
+        n++;
+        for (i = 0; i < nfields; i++) {
+          float v;
+          orc_grid_field(ids[i], o, &o->cell[c], &v);
+          fwrite(&v, sizeof(float), 1, fp[i]);
+        }
+        if (o->x < b[0]) b[0] = (float)o->x;
+        if (o->y < b[2]) b[2] = (float)o->y;
+        if (o->z < b[4]) b[4] = (float)o->z;
+        if (o->x + dx > b[1]) b[1] = (float)(o->x + dx);
+        if (o->y + dx > b[3]) b[3] = (float)(o->y + dx);
+        if (o->z + dx > b[5]) b[5] = (float)(o->z + dx);
+      }
+    }
+  }
+  for (i = 0; i < nfields; i++) {
+    rewind(fp[i]);
+    orc_alloct_header(fp[i], n, tsim, b);
+    if (ferror(fp[i])) rc = -1;
+    if (fclose(fp[i]) != 0) rc = -1;
+  }
+  return rc;
+}

@@ -61,6 +61,10 @@ long long orc_cell_updates(void);
 void orc_reset_counters(void);
 int orc_sizeof_oct(void);
 
+/* ALLOCT field dump, dumpalloct_serial (src/io.c:1233): see hydro_oracle.c */
+int orc_dump_alloct(const char *folder, void **firstoct, int lcoarse, int lmax, int rank, int ndumps, double tsim,
+                    int nfields, const int *ids, const char *const *names);
+
 #ifdef __cplusplus
 }
 #endif

@@ -61,6 +61,9 @@ class Restatement:
             if grav:
                 L.orc_grav_correction.argtypes = [c_void_p, c_int, c_double]
                 L.orc_grav_correction.restype = c_int
+            L.orc_dump_alloct.argtypes = [ctypes.c_char_p, c_void_p, c_int, c_int, c_int, c_int, c_double, c_int,
+                                          c_void_p, c_void_p]
+            L.orc_dump_alloct.restype = c_int
             Restatement._libs[path] = L
         self.L = Restatement._libs[path]
         self.grav = grav
@@ -84,6 +87,13 @@ class Restatement:
 
     def grav_correction(self, firstoct, level, dt):
         return self.L.orc_grav_correction(firstoct, level, dt)
+
+    def dump_alloct(self, folder, firstoct, lcoarse, lmax, ids, names, rank=0, ndumps=0, tsim=0.0):
+        """dumpalloct_serial (src/io.c:1233) restated: one file per field under folder."""
+        idv = (c_int * len(ids))(*ids)
+        nv = (ctypes.c_char_p * len(names))(*[n.encode() for n in names])
+        return self.L.orc_dump_alloct(folder.encode(), firstoct, lcoarse, lmax, rank, ndumps, tsim, len(ids),
+                                      ctypes.cast(idv, c_void_p), ctypes.cast(nv, c_void_p))
 
     def sizeof_oct(self):
         return self.L.orc_sizeof_oct()
