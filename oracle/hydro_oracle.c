@@ -39,8 +39,16 @@
 #define ERR_TOL 1e-10     /* ERRTOL, src/hydro_utils.c:18 */
 
 /* ---- memory layout of the reference tree (src/prototypes.h:611,825,1028) */
+#ifdef ORC_WRADHYD
+/* -DWRADHYD: the ionised density dX, advected with the gas (NVAR 7; YHE = 0
+ * without -DHELIUM / -DHESIMPLE, src/param.h:47-54) */
+#define YHE_ (0.)
+typedef struct { double d, u, v, w, p, a, E, dX; } oW;      /* struct Wtype */
+typedef struct { double d, du, dv, dw, E, eint, dX; } oU;  /* struct Utype */
+#else
 typedef struct { double d, u, v, w, p, a, E; } oW;      /* struct Wtype */
 typedef struct { double d, du, dv, dw, E, eint; } oU;  /* struct Utype */
+#endif
 struct oOct;
 typedef struct oCell {
   struct oOct *child;
@@ -63,9 +71,14 @@ typedef struct oOct {
   int cpu;
   int level;
 } oOct;
-#ifdef ORC_WGRAV
+#if defined(ORC_WGRAV) && defined(ORC_WRADHYD)
+#error "the gravity and tracer layouts are built separately"
+#elif defined(ORC_WGRAV)
 _Static_assert(sizeof(oCell) == 192, "CELL layout (-DWGRAV)");
 _Static_assert(sizeof(oOct) == 1648, "OCT layout (-DWGRAV)");
+#elif defined(ORC_WRADHYD)
+_Static_assert(sizeof(oCell) == 152, "CELL layout (-DWRADHYD)");
+_Static_assert(sizeof(oOct) == 1328, "OCT layout (-DWRADHYD)");
 #else
 _Static_assert(sizeof(oCell) == 136, "CELL layout");
 _Static_assert(sizeof(oOct) == 1200, "OCT layout");
@@ -101,6 +114,9 @@ static void to_cons(const oW *W, oU *U) {
   U->dw = W->d * W->w;
   U->eint = W->p / (GAM - 1.);
   U->E = W->E;
+#ifdef ORC_WRADHYD
+  U->dX = W->dX;
+#endif
 }
 /* dual: -DDUAL_E, the pressure from the tracked internal energy (src/hydro_utils.c:45-49) */
 static void to_prim(const oU *U, oW *W, int dual) {
@@ -112,6 +128,9 @@ static void to_prim(const oU *U, oW *W, int dual) {
   if (dual) W->p = U->eint * (GAM - 1.);
   else W->p = (GAM - 1.) * (U->E - ((U->du) * (U->du) + (U->dv) * (U->dv) + (U->dw) * (U->dw)) / (dl)*0.5);
   W->E = U->E;
+#ifdef ORC_WRADHYD
+  W->dX = U->dX;
+#endif
   W->a = sqrt(GAM * W->p / dl);
 }
 
@@ -206,6 +225,14 @@ static void muscl_cell(Stencil *st, int slot, int ic, double dt, double dx) {
 #endif
     get_E(Wi);
     Wi->a = sqrt(GAM * Wi->p / Wi->d);
+#ifdef ORC_WRADHYD
+    /* the face value is the face density times the centre's ionised fraction; the
+     * reconstructed dX is overwritten (src/hydro_utils.c:1244-1246) */
+    {
+      double X0 = W0->dX / (W0->d * (1. - YHE_));
+      Wi->dX = Wi->d * (1. - YHE_) * X0;
+    }
+#endif
   }
   st->done[slot][ic] = 1;
 }
@@ -335,26 +362,40 @@ static void euler_flux(const oU *U, int n, double f[5]) {
   f[1 + t2] = mn * m[t2] / U->d;
   f[4] = GAM * mn / U->d * U->E - 0.5 * (GAM - 1.) * mn / (U->d * U->d) * all;
 }
+#ifdef ORC_WRADHYD
+/* tracer flux f[6] of getflux_{X,Y,Z} (src/hydro_utils.c:925,943,961) */
+static double tracer_flux(const oU *U, int n) {
+  double m[3] = {U->du, U->dv, U->dw};
+  return m[n] * U->dX / U->d;
+}
+#endif
 
 /* HLLC flux across a face normal to axis n from left/right MUSCL states
  * (src/hydro_utils.c:2055-2138, same branches for y :1783, z :1508).
  * us (optional, -DDUAL_E): the state Us of the branch taken (the upwind state or
  * the star state), from which the sweeps take the internal-energy flux and the
  * face velocity of divu (src/hydro_utils.c:2126-2129). */
-static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us) {
+static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us, double *fx) {
   double SL, SR, ustar;
   oU UL, UR;
   int k;
   for (k = 0; k < 5; k++) F[k] = 0.;
+  if (fx) *fx = 0.;
   wave_speeds(WL, WR, n, &SL, &SR, &ustar);
   to_cons(WL, &UL);
   to_cons(WR, &UR);
   if (SL >= 0.) {
     euler_flux(&UL, n, F);
     if (us) *us = UL;
+#ifdef ORC_WRADHYD
+    if (fx) *fx = tracer_flux(&UL, n);
+#endif
   } else if (SR <= 0.) {
     euler_flux(&UR, n, F);
     if (us) *us = UR;
+#ifdef ORC_WRADHYD
+    if (fx) *fx = tracer_flux(&UR, n);
+#endif
   } else if ((SL < 0.) && (ustar >= 0.)) {
     const oW *W = WL;
     const oU *U = &UL;
@@ -365,6 +406,10 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us) {
     F[0] += (fact * 1. - U->d) * SL;
     for (k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : vel[k]) - mom[k]) * SL;
     F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SL - un)))) - U->E) * SL;
+#ifdef ORC_WRADHYD
+    /* src/hydro_utils.c:1534-1535 (and :1809, :2115 for y, x) */
+    if (fx) *fx = tracer_flux(U, n) + (fact * W->dX / W->d - U->dX) * SL;
+#endif
     if (us) {
       double m[3];
       for (k = 0; k < 3; k++) m[k] = fact * (k == n ? ustar : vel[k]);
@@ -382,6 +427,9 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us) {
     F[0] += (fact * 1. - U->d) * SR;
     for (k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : vel[k]) - mom[k]) * SR;
     F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SR - un)))) - U->E) * SR;
+#ifdef ORC_WRADHYD
+    if (fx) *fx = tracer_flux(U, n) + (fact * W->dX / W->d - U->dX) * SR;
+#endif
     if (us) {
       double m[3];
       for (k = 0; k < 3; k++) m[k] = fact * (k == n ? ustar : vel[k]);
@@ -610,7 +658,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
   g_err = 0;
   const int dual = flag_on(flags, ORC_DUAL_E);
   for (o = firstoct[level - 1]; o != NULL; o = o->next) {
-    double flux[8][6][6];  /* 6th component: internal-energy flux (-DDUAL_E) */
+    double flux[8][6][7];  /* [5]: internal-energy flux (-DDUAL_E), [6]: tracer flux (-DWRADHYD) */
     double divu[8];
     if (o->cpu != 0) continue;
     n++;
@@ -626,14 +674,20 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
         for (s = 0; s < 2; s++) {
           int kf = 2 * dir + s, same, vc, nslot;
           const oW *Wc, *Wn;
-          double F[6];
+          double F[7];
           oU us;
           cell_nei(c, kf, &same, &vc);
           nslot = same ? 13 : FACE_SLOT[kf];
           Wc = face_state(&g_st, 13, c, kf, dt, dx);
           Wn = face_state(&g_st, nslot, vc, kf ^ 1, dt, dx);
-          if (s == 0) hllc_flux(Wn, Wc, dir, F, dual ? &us : NULL);
-          else hllc_flux(Wc, Wn, dir, F, dual ? &us : NULL);
+          F[6] = 0.;
+#ifdef ORC_WRADHYD
+          if (s == 0) hllc_flux(Wn, Wc, dir, F, dual ? &us : NULL, &F[6]);
+          else hllc_flux(Wc, Wn, dir, F, dual ? &us : NULL, &F[6]);
+#else
+          if (s == 0) hllc_flux(Wn, Wc, dir, F, dual ? &us : NULL, NULL);
+          else hllc_flux(Wc, Wn, dir, F, dual ? &us : NULL, NULL);
+#endif
           F[5] = 0.;
           if (dual) {
             /* src/hydro_utils.c:2126-2129: ebar, the internal-energy flux and the
@@ -644,7 +698,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
             F[5] = (mom[dir] / us.d * ebar);
             divu[c] += (s == 0) ? -divuloc : divuloc;
           }
-          for (k = 0; k < 6; k++) flux[c][kf][k] = F[k] * (double)(!g_st.split[nslot][vc]);
+          for (k = 0; k < 7; k++) flux[c][kf][k] = F[k] * (double)(!g_st.split[nslot][vc]);
         }
       }
     }
@@ -652,9 +706,10 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
     for (c = 0; c < 8; c++) {
       oCell *cell = &o->cell[c];
       if (!g_st.split[13][c]) {
-        oU dU = {0., 0., 0., 0., 0., 0.}, U;
+        oU dU, U;
         double one = 1., ekin;
         int f;
+        memset(&dU, 0, sizeof(dU));
         for (f = 0; f < 6; f++) {
           dU.d += flux[c][f][0] * dtsurdx * one;
           dU.du += flux[c][f][1] * dtsurdx * one;
@@ -662,6 +717,9 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
           dU.dw += flux[c][f][3] * dtsurdx * one;
           dU.E += flux[c][f][4] * dtsurdx * one;
           dU.eint += flux[c][f][5] * dtsurdx * one;
+#ifdef ORC_WRADHYD
+          dU.dX += flux[c][f][6] * dtsurdx * one;  /* src/hydro_utils.c:3068 */
+#endif
           one *= -1.;
         }
         if (isnan(cell->fieldnew.u)) g_err |= ORC_ERR_NAN;
@@ -671,6 +729,9 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
         U.dv += dU.dv;
         U.dw += dU.dw;
         U.E += dU.E;
+#ifdef ORC_WRADHYD
+        U.dX += dU.dX;  /* src/hydro_utils.c:3158 */
+#endif
         ekin = 0.5 * (U.du * U.du + U.dv * U.dv + U.dw * U.dw) / U.d;
         if (dual) {
           /* src/hydro_utils.c:3167-3177: tracked eint, unless E - Ekin is well resolved */
@@ -686,6 +747,11 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
         cell->fieldnew.a = sqrt(GAM * cell->fieldnew.p / cell->fieldnew.d);
         get_E(&cell->fieldnew);
         if (isnan(cell->fieldnew.u)) g_err |= ORC_ERR_NAN;
+#ifdef ORC_WRADHYD
+        /* ceiling of the ionised fraction (src/hydro_utils.c:3197-3198) */
+        if (cell->fieldnew.dX < 0) cell->fieldnew.dX = 0.;
+        if (cell->fieldnew.dX > (cell->fieldnew.d * (1. - YHE_))) cell->fieldnew.dX = cell->fieldnew.d * (1. - YHE_);
+#endif
       }
       /* fine -> coarse flux correction into unsplit coarse neighbours */
       for (k = 0; k < 6; k++) {
@@ -706,6 +772,9 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
           U.dw += flux[c][k][3] * dtsurdx * one * 0.125;
           U.E += flux[c][k][4] * dtsurdx * one * 0.125;
           if (dual) U.eint += flux[c][k][5] * dtsurdx * one * 0.125;
+#ifdef ORC_WRADHYD
+          U.dX += flux[c][k][6] * dtsurdx * one * 0.125;
+#endif
           to_prim(&U, &W, dual);
           cc->fieldnew = W;
         }
@@ -731,6 +800,9 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
             W.v += Wc->v * 0.125;
             W.w += Wc->w * 0.125;
             W.p += Wc->p * 0.125;
+#ifdef ORC_WRADHYD
+            W.dX += Wc->dX * 0.125;  /* src/hydro_utils.c:3460 */
+#endif
           }
           get_E(&W);
           cell->field = W;

@@ -19,10 +19,12 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 ORACLE_LIB_GRAV = os.path.join(HERE, "_build", "liboracle_grav.so")
+ORACLE_LIB_RH = os.path.join(HERE, "_build", "liboracle_rh.so")
 REF_LIB = os.path.join(HERE, "_ref", "libemmaref.so")
 REF_LIB_TX = os.path.join(HERE, "_ref", "libemmaref_tx.so")
 REF_LIB_GRAV = os.path.join(HERE, "_ref", "libemmaref_grav.so")
 REF_LIB_DUAL = os.path.join(HERE, "_ref", "libemmaref_dual.so")
+REF_LIB_RH = os.path.join(HERE, "_ref", "libemmaref_rh.so")
 
 HYDROTEST = 0x40
 DUAL_E = 0x80
@@ -40,11 +42,13 @@ def flags_for(trans, dual=False):
 
 
 class Restatement:
-    """grav=True: the -DWGRAV layout and gravity coupling (liboracle_grav.so)."""
+    """grav=True: the -DWGRAV layout and gravity coupling (liboracle_grav.so);
+    rh=True: the -DWRADHYD layout with the advected ionised density (liboracle_rh.so)."""
     _libs = {}
 
-    def __init__(self, grav=False):
-        path = ORACLE_LIB_GRAV if grav else ORACLE_LIB
+    def __init__(self, grav=False, rh=False):
+        assert not (grav and rh), "one layout at a time"
+        path = ORACLE_LIB_GRAV if grav else (ORACLE_LIB_RH if rh else ORACLE_LIB)
         if path not in Restatement._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"oracle restatement not built: {path}")
@@ -153,8 +157,14 @@ class GravClone:
             self.h = None
 
 
-def ref_available(tx=False, grav=False, dual=False):
-    return os.path.exists(REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB)))
+def _ref_path(tx=False, grav=False, dual=False, rh=False):
+    if rh:
+        return REF_LIB_RH
+    return REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
+
+
+def ref_available(tx=False, grav=False, dual=False, rh=False):
+    return os.path.exists(_ref_path(tx, grav, dual, rh))
 
 
 class RefTree:
@@ -162,9 +172,9 @@ class RefTree:
 
     _libs = {}
 
-    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False, dual=False):
-        assert (tx + grav + dual) <= 1, "one build variant at a time"
-        path = REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
+    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False, dual=False, rh=False):
+        assert (tx + grav + dual + rh) <= 1, "one build variant at a time"
+        path = _ref_path(tx, grav, dual, rh)
         if path not in RefTree._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"reference oracle not built: {path}")
@@ -195,6 +205,18 @@ class RefTree:
 
     def noct(self, level):
         return self.L.ref_noct(level)
+
+    def set_tracer(self, level, dX):
+        """-DWRADHYD build: the ionised density dX of field and fieldnew (list order)."""
+        a = np.ascontiguousarray(dX, dtype=np.float64)
+        self.L.ref_set_tracer.argtypes = [c_int, c_void_p]
+        self.L.ref_set_tracer(level, _p(a))
+
+    def get_tracer(self, level, which=0):
+        out = np.zeros(8 * self.noct(level))
+        self.L.ref_get_tracer.argtypes = [c_int, c_int, c_void_p]
+        self.L.ref_get_tracer(level, which, _p(out))
+        return out
 
     def oct_xyz(self, level):
         n = self.noct(level)

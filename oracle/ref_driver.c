@@ -257,6 +257,26 @@ void ref_set_force(int level, const double *fx, const double *fy, const double *
 }
 #endif
 
+#ifdef WRADHYD
+/* Set the ionised density dX of field and fieldnew of every cell of a level
+ * (list order), and read it back from field (which=0) or fieldnew (which=1). */
+void ref_set_tracer(int level, const double *dX) {
+  int i = 0, c;
+  struct OCT *o;
+  for (o = g_first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) {
+      o->cell[c].field.dX = dX[8 * i + c];
+      o->cell[c].fieldnew.dX = dX[8 * i + c];
+    }
+}
+void ref_get_tracer(int level, int which, double *out) {
+  int i = 0, c;
+  struct OCT *o;
+  for (o = g_first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) out[8 * i + c] = which ? o->cell[c].fieldnew.dX : o->cell[c].field.dX;
+}
+#endif
+
 /* Checkpoints through the reference's own src/restart.c (save_amr / restore_amr),
  * units from `units7` (unit_l, _v, _t, _n, _mass, _d, _N), no particles. */
 void ref_save_amr(const char *filename, double tsim, double tinit, int nsteps, int ndumps, const double *units7) {

@@ -36,9 +36,17 @@ def random_forces(tree, levels, seed=54321, amp=0.5):
         tree.set_force(l, *(rng.uniform(-amp, amp, n8) for _ in range(3)))
 
 
-def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, grav=False, dual=False):
+def random_tracer(tree, levels, seed=777):
+    """Ionised density dX = d * x with x uniform in [0, 1] (-DWRADHYD trees)."""
+    rng = np.random.default_rng(seed)
+    for l in levels:
+        d = tree.get_fields(l, 0)[0]
+        tree.set_tracer(l, d * rng.uniform(0.0, 1.0, d.size))
+
+
+def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, grav=False, dual=False, rh=False):
     ref = oracle.RefTree(base, lmax, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)), grav=grav,
-                         dual=dual)
+                         dual=dual, rh=rh)
     for i, r in enumerate(radii):
         ref.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
     if fields is None:
@@ -49,14 +57,19 @@ def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, g
     if grav:
         random_forces(ref, range(base, lmax + 1))
         assert ref.sizeof_oct() == oracle.Restatement(grav=True).sizeof_oct() == 1648
+    if rh:
+        random_tracer(ref, range(base, lmax + 1))
+        assert ref.sizeof_oct() == oracle.Restatement(rh=True).sizeof_oct() == 1328
     base_ptr = ref.L.ref_grid_base()
     nbytes = ref.ngridmax * ref.sizeof_oct()
     snap = ctypes.string_at(base_ptr, nbytes)
     t1, adt1 = ref.run(nsteps)
     A = {l: (ref.get_fields(l, 0), ref.get_fields(l, 1)) for l in range(base, lmax + 1)}
+    AX = {l: (ref.get_tracer(l, 0), ref.get_tracer(l, 1)) for l in range(base, lmax + 1)} if rh else None
     ctypes.memmove(base_ptr, snap, nbytes)
     trans = 3 if tx else 0
-    t2, adt2, err = oracle.Restatement(grav=grav).run(ref.firstoct, base, lmax, nsteps, 0.8, trans=trans, dual=dual)
+    t2, adt2, err = oracle.Restatement(grav=grav, rh=rh).run(ref.firstoct, base, lmax, nsteps, 0.8, trans=trans,
+                                                              dual=dual)
     assert err == 0
     assert t1 == t2 and np.array_equal(adt1, adt2)
     for l in range(base, lmax + 1):
@@ -65,6 +78,9 @@ def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, g
         leaf = ~(ref.topology(l)[2].reshape(-1) >= 0)
         # fieldnew of split cells holds stale stencil data in the reference; not part of the state
         assert np.array_equal(fnA[:, leaf], ref.get_fields(l, 1)[:, leaf]), f"fieldnew, level {l}"
+        if rh:
+            assert np.array_equal(AX[l][0], ref.get_tracer(l, 0)), f"dX, level {l}"
+            assert np.array_equal(AX[l][1][leaf], ref.get_tracer(l, 1)[leaf]), f"fieldnew dX, level {l}"
 
 
 @needs_ref
@@ -110,6 +126,21 @@ def test_pin_gravity_amr():
     """-DWGRAV on two refined levels: forces of injected coarse cells interpolated
     (coarse2fine_forcelin) in the gather."""
     ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, grav=True)
+
+
+needs_ref_rh = pytest.mark.skipif(not oracle.ref_available(rh=True), reason="oracle/_ref -DWRADHYD build absent")
+
+
+@needs_ref_rh
+def test_pin_tracer_uniform():
+    """-DWRADHYD: the ionised density dX advected with the mass flux (face values
+    from the centre fraction), its ceiling and fine->coarse corrections."""
+    ref_vs_restatement(False, 4, 4, (), 3, rh=True)
+
+
+@needs_ref_rh
+def test_pin_tracer_amr():
+    ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, rh=True)
 
 
 needs_ref_dual = pytest.mark.skipif(not oracle.ref_available(dual=True), reason="oracle/_ref dual-energy build absent")
