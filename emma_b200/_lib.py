@@ -11,9 +11,9 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libemmahydro.so")
 LIB_PATH_GRAV = os.path.join(_HERE, "libemmahydro_grav.so")
+LIB_PATH_RH = os.path.join(_HERE, "libemmahydro_rh.so")
 
-_lib = None
-_lib_grav = None
+_libs = {}
 
 c_int, c_double, c_ll, c_void_p = ctypes.c_int, ctypes.c_double, ctypes.c_longlong, ctypes.c_void_p
 P = ctypes.POINTER
@@ -100,26 +100,31 @@ GRAV_SIGNATURES = [
 ]
 
 
+RH_SIGNATURES = [
+    ("emma_tree_set_tracer", None, [c_void_p, c_int, c_void_p]),
+    ("emma_tree_get_tracer", None, [c_void_p, c_int, c_int, c_void_p]),
+]
+
+
 def lib(grav=False):
-    """Load libemmahydro.so (grav: libemmahydro_grav.so, the -DWGRAV cell layout)
-    once; raise if it is not built."""
-    global _lib, _lib_grav
-    if (_lib_grav if grav else _lib) is not None:
-        return _lib_grav if grav else _lib
-    path = LIB_PATH_GRAV if grav else LIB_PATH
+    """Load libemmahydro.so once; grav=True: libemmahydro_grav.so (the -DWGRAV cell
+    layout), grav="rh": libemmahydro_rh.so (the -DWRADHYD layout).  Raises if the
+    library is not built."""
+    key = "rh" if grav == "rh" else ("grav" if grav else "plain")
+    if key in _libs:
+        return _libs[key]
+    path = {"plain": LIB_PATH, "grav": LIB_PATH_GRAV, "rh": LIB_PATH_RH}[key]
     if not os.path.exists(path):
         raise RuntimeError(f"{os.path.basename(path)} is not built ({path}); run emma_b200.build.build()")
     # RTLD_LOCAL: the drop-in entries carry the reference's names (HydroSolver, ...);
     # they must not interpose on another library that defines the same symbols
     L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
-    for name, res, args in SIGNATURES + (GRAV_SIGNATURES if grav else []):
+    extra = {"plain": [], "grav": GRAV_SIGNATURES, "rh": RH_SIGNATURES}[key]
+    for name, res, args in SIGNATURES + extra:
         fn = getattr(L, name)
         fn.restype = res
         fn.argtypes = args
-    if grav:
-        _lib_grav = L
-    else:
-        _lib = L
+    _libs[key] = L
     return L
 
 

@@ -34,7 +34,7 @@ cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *g
 cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s,
                           bool grav);
 cudaError_t launch_dropin_base(const double *wb, double *base, long long n8, const double *exc, long long nexc, int nsm,
-                               cudaStream_t s);
+                               cudaStream_t s, int np);
 bool resident_level(struct OCT **firstoct, int level, const HostLevel **h, const double **W, const uint8_t **split,
                     cudaStream_t *stream, int *nsm);
 void release_dump_staging();
@@ -53,7 +53,8 @@ struct DevLevel {
   int L = 0, noct = 0, ntiles = 0;
   long long n8 = 0, leaf = 0;
   double *W0 = nullptr, *W1 = nullptr, *C = nullptr, *B = nullptr;
-  double *WB = nullptr;  // drop-in levels: one allocation of W0 (5 planes) followed by B (6 planes)
+  double *WB = nullptr;  // drop-in levels: one allocation of W0 (5 planes), E (, dX), then B (d,u,v,w,p,E (, dX))
+  double *X = nullptr, *Xn = nullptr;  // tracer builds: dX of the level's field and the new dX
   uint8_t *split = nullptr;
   int *child = nullptr;
   TileDesc *tiles = nullptr;
@@ -143,9 +144,20 @@ constexpr int kDropinGrav = 1;
 #else
 constexpr int kDropinGrav = 0;
 #endif
+// ... and those of a library built for its -DWRADHYD layout (libemmahydro_rh.so)
+// advance the ionised density dX too (drop-in entries only).
+#ifdef EMMA_WRADHYD
+constexpr int kDropinTracer = 1;
+#else
+constexpr int kDropinTracer = 0;
+#endif
 
-// Planes of a correction buffer: d, du, dv, dw, E, and with dual energy eint.
-inline long long cplanes() { return g.opt.dual_energy ? 6 : 5; }
+// Planes of a correction buffer: d, du, dv, dw, E, with dual energy eint, in a
+// tracer build dX (plane kXPlane; the tracer build has no dual energy).
+inline long long cplanes() { return (g.opt.dual_energy ? 6 : 5) + kDropinTracer; }
+// Planes of a drop-in level's `field` upload and of its base fieldnew: d,u,v,w,p,E (+ dX)
+constexpr int kFieldPlanes = 6 + kDropinTracer;
+static_assert(!kDropinTracer || kXPlane == 5, "tracer corrections follow the five conserved planes");
 
 void fail(unsigned bit, const std::string &msg) {
   g.status |= bit;
@@ -358,18 +370,23 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     d.leaf = h.leaf;
     d.ntiles = (int)h.tiles.size();
     d.shape = h.shape;
-    const size_t bytes = sizeof(double) * 5 * (size_t)std::max<long long>(d.n8, 1);
+    // state planes d,u,v,w,p (tracer builds: + dX)
+    const size_t bytes = sizeof(double) * (5 + kDropinTracer) * (size_t)std::max<long long>(d.n8, 1);
     if (with_base && !h.tiles.empty()) {
-      // drop-in levels: W0 (5 planes) and E of `field` (1 plane) in one block, uploaded
-      // by one pitched copy per oct range, then the base B (6 planes: fieldnew), built
-      // on the device from them and the cells where fieldnew differs from field
-      if (!ck(cudaMalloc(&d.WB, sizeof(double) * 12 * (size_t)d.n8), "cudaMalloc W+B")) return false;
+      // drop-in levels: W0 (5 planes), E (and dX) of `field` in one block, uploaded
+      // by one pitched copy per oct range, then the base B (the same planes of
+      // fieldnew), built on the device from them and the cells where fieldnew differs
+      if (!ck(cudaMalloc(&d.WB, sizeof(double) * 2 * kFieldPlanes * (size_t)d.n8), "cudaMalloc W+B")) return false;
       d.W0 = d.WB;
-      d.B = d.WB + 6 * d.n8;
+      d.B = d.WB + kFieldPlanes * d.n8;
+      if (kDropinTracer) d.X = d.WB + 6 * d.n8;
     } else if (!ck(cudaMalloc(&d.W0, bytes), "cudaMalloc W")) {
       return false;
+    } else if (kDropinTracer) {
+      d.X = d.W0 + 5 * d.n8;
     }
     if (!ck(cudaMalloc(&d.W1, bytes), "cudaMalloc Wn")) return false;
+    if (kDropinTracer) d.Xn = d.W1 + 5 * d.n8;
     // corrections arrive only from the finer level: a level without split cells has none
     bool has_split = false;
     for (uint8_t m : h.split) has_split = has_split || m != 0;
@@ -504,8 +521,16 @@ void pack_cells(const HostLevel &h, long long a, long long b, double *pw, std::v
       pw[3 * n8 + k] = W.w;
       pw[4 * n8 + k] = W.p;
       pw[5 * n8 + k] = W.E;
-      if (std::memcmp(&W, &N, 5 * sizeof(double)) != 0 || std::memcmp(&W.E, &N.E, sizeof(double)) != 0) {
-        const double e[8] = {(double)k, N.d, N.u, N.v, N.w, N.p, N.E, 0.};
+#ifdef EMMA_WRADHYD
+      pw[6 * n8 + k] = W.dX;
+      const bool tdiff = std::memcmp(&W.dX, &N.dX, sizeof(double)) != 0;
+      const double nx = N.dX;
+#else
+      const bool tdiff = false;
+      const double nx = 0.;
+#endif
+      if (std::memcmp(&W, &N, 5 * sizeof(double)) != 0 || std::memcmp(&W.E, &N.E, sizeof(double)) != 0 || tdiff) {
+        const double e[8] = {(double)k, N.d, N.u, N.v, N.w, N.p, N.E, nx};
         exc.insert(exc.end(), e, e + 8);
       }
     }
@@ -527,6 +552,9 @@ void unpack_cells(const HostLevel &h, long long a, long long b, const double *p,
       W.v = p[2 * n8 + k];
       W.w = p[3 * n8 + k];
       W.p = p[4 * n8 + k];
+#ifdef EMMA_WRADHYD
+      W.dX = p[5 * n8 + k];
+#endif
       finish_prims(W);
       if (also_field) o->cell[c].field = W;
     }
@@ -581,9 +609,11 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
     tl.b = get_event();
     cudaEventRecord(tl.a, g.stream);
   }
-  // the levels of a gravity build run the gravity-coupled variant; dual energy its own
+  // the levels of a gravity build run the gravity-coupled variant; dual energy and the
+  // tracer build their own
   if (grav || (d_lv == g.res.d_lv && g.res.host.grav)) shapes |= kLaunchGrav;
   if (g.opt.dual_energy) shapes |= kLaunchDual;
+  if (kDropinTracer) shapes |= kLaunchTracer;
   cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED)
                       ? launch_level_f32(a, shapes, g.nsm, ctas, g.stream, nullptr)
                       : launch_level_fp64(a, shapes, g.nsm, ctas, g.stream, nullptr);
@@ -1071,6 +1101,10 @@ int emma_hydro_is_resident(struct OCT **firstoct) {
 
 int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int rank) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
+  if (kDropinTracer) {
+    fail(EMMA_ST_ARG, "the -DWRADHYD library advances the tracer through the drop-in entries only");
+    return EMMA_ST_ARG;
+  }
   if (firstoct == nullptr || lcoarse < 2 || lmax < lcoarse || lmax >= kMaxLevels) {
     fail(EMMA_ST_ARG, "bad tree arguments");
     return EMMA_ST_ARG;
@@ -1581,6 +1615,10 @@ static unsigned long long level_hash(const std::vector<struct OCT *> &v, int ran
 static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu, double dtnew, bool final_update) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return 0;
   if (firstoct == nullptr || level < 2 || level >= kMaxLevels - 1 || firstoct[level - 1] == nullptr) return 0;
+  if (kDropinTracer && (g.opt.dual_energy || g.opt.trans_flags)) {
+    fail(EMMA_ST_ARG, "the -DWRADHYD library has neither dual energy nor transmissive boundaries");
+    return 0;
+  }
   const int rank = dropin_rank(cpu);
   const auto t0 = Clock::now();
   // levels present around `level`: L-1 always exists; L+1 only if a cell is split
@@ -1621,13 +1659,14 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   if (h.nown == 0) return 0;
   const long long n8 = d.n8, nc8 = dc.n8;
   const bool coarse = nc8 > 0 && h.reads_coarse && dc.C != nullptr;
-  // pinned staging: level field with E (6 planes; the new state on the way back) | coarser
-  // level (5 planes) | gravity builds: level and coarser accelerations (3 + 3
-  // planes) | device status word
+  // pinned staging: level field with E (and dX) (kFieldPlanes planes; the new state on
+  // the way back) | coarser level (5 planes, and dX) | gravity builds: level and
+  // coarser accelerations (3 + 3 planes) | device status word
   const long long nf = kDropinGrav ? 3 * (n8 + nc8) : 0, ncp = cplanes();
   // (+ n8 bytes for the dual-energy sound-speed flags after the status word)
-  if (!ensure_pin(sizeof(double) * (6 * n8 + ncp * nc8 + nf + 2) + (size_t)n8) || !ensure_range_events()) return 0;
-  double *pw = g.pin, *pc = g.pin + 6 * n8;
+  if (!ensure_pin(sizeof(double) * (kFieldPlanes * n8 + ncp * nc8 + nf + 2) + (size_t)n8) || !ensure_range_events())
+    return 0;
+  double *pw = g.pin, *pc = g.pin + kFieldPlanes * n8;
   [[maybe_unused]] double *pf = pc + ncp * nc8, *pfc = pf + 3 * n8;
   unsigned *pst = reinterpret_cast<unsigned *>(pc + ncp * nc8 + nf);
   const auto t1 = Clock::now();
@@ -1647,7 +1686,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     for (long long s0 = a0; s0 < b0; s0 += sub) {
       const long long s1 = std::min(b0, s0 + sub);
       pack_cells(h, s0, s1, pw, g.exc[t]);
-      if (cudaMemcpy2DAsync(d.WB + 8 * s0, pitch, pw + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 6,
+      if (cudaMemcpy2DAsync(d.WB + 8 * s0, pitch, pw + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), kFieldPlanes,
                             cudaMemcpyHostToDevice, g.stream) != cudaSuccess)
         copies_ok = false;
 #ifdef EMMA_WGRAV
@@ -1687,7 +1726,9 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
         !ck(cudaMemcpyAsync(g.d_exc, g.pin_exc, sizeof(double) * 8 * nexc, cudaMemcpyHostToDevice, g.stream),
             "H2D exceptions"))
       return 0;
-    if (!ck(launch_dropin_base(d.WB, d.B, n8, g.d_exc, (long long)nexc, g.nsm, g.stream), "base launch")) return 0;
+    if (!ck(launch_dropin_base(d.WB, d.B, n8, g.d_exc, (long long)nexc, g.nsm, g.stream, kFieldPlanes),
+            "base launch"))
+      return 0;
     g.h2d_bytes += (long long)(sizeof(double) * 8 * nexc);
   }
   if (d.az != nullptr) {  // dual energy: the split cells' stored sound speeds of 0
@@ -1695,12 +1736,24 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     parallel_for(h.noct, [&](long long a0, long long b0) { pack_az(h, a0, b0, pz); });
     if (!ck(cudaMemcpyAsync(d.az, pz, (size_t)n8, cudaMemcpyHostToDevice, g.stream), "H2D az")) return 0;
   }
-  g.h2d_bytes += (long long)sizeof(double) * (6 + 3 * kDropinGrav) * n8;
+  g.h2d_bytes += (long long)sizeof(double) * (kFieldPlanes + 3 * kDropinGrav) * n8;
   if (coarse) {
     pack_level(hc, 0, pc);
     if (!ck(cudaMemcpyAsync(dc.W0, pc, sizeof(double) * 5 * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Wc"))
       return 0;
     g.h2d_bytes += (long long)sizeof(double) * 5 * nc8;
+#ifdef EMMA_WRADHYD
+    // the coarser level's dX, for the fractions of its injected cells
+    double *px = pc + 5 * nc8;
+    parallel_for(hc.noct, [&](long long a0, long long b0) {
+      for (long long i = a0; i < b0; i++)
+        for (int c = 0; c < 8; c++) px[8 * i + c] = hc.octs[i]->cell[c].field.dX;
+    });
+    if (dc.X == nullptr ||
+        !ck(cudaMemcpyAsync(dc.X, px, sizeof(double) * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Xc"))
+      return 0;
+    g.h2d_bytes += (long long)sizeof(double) * nc8;
+#endif
     if (!ck(cudaMemsetAsync(dc.C, 0, sizeof(double) * ncp * nc8, g.stream), "memset Cc")) return 0;
   }
 #ifdef EMMA_WGRAV
@@ -1746,6 +1799,12 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   a.wv_inject = H.grav;
   a.az = d.az;  // dual energy: from the caller's cells, every call
   a.azall = nullptr;
+  if (kDropinTracer) {  // the tracer planes (the union slots of gravity and dual energy)
+    a.X = d.X;
+    a.Xc = coarse ? dc.X : nullptr;
+    a.Xn = d.Xn;
+    a.BX = d.B + 6 * n8;
+  }
   k_set_args<<<1, 1, 0, g.stream>>>(T.d_lv, level, a);
   if (!ck(cudaGetLastError(), "k_set_args")) return 0;
   if (!ck(launch_interp(T.d_lv, level, d.nv, nullptr, g.nsm, g.stream, H.grav != 0), "interpolation launch"))
@@ -1774,8 +1833,8 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     int nq = 0;
     for (long long s0 = a0; s0 < b0 && nq < kSubRanges; s0 += sub_own, nq++) {
       const long long s1 = std::min(b0, s0 + sub_own);
-      if (cudaMemcpy2DAsync(pw + 8 * s0, pitch, d.W1 + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0), 5,
-                            cudaMemcpyDeviceToHost, g.stream) != cudaSuccess ||
+      if (cudaMemcpy2DAsync(pw + 8 * s0, pitch, d.W1 + 8 * s0, pitch, sizeof(double) * 8 * (s1 - s0),
+                            5 + kDropinTracer, cudaMemcpyDeviceToHost, g.stream) != cudaSuccess ||
           cudaEventRecord(ev[nq], g.stream) != cudaSuccess) {
         wait_ok = false;
         return;
@@ -1797,7 +1856,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
     }
   });
   if (!wait_ok) return ck(cudaStreamSynchronize(g.stream), "D2H level state"), ck(cudaGetLastError(), "D2H"), 0;
-  g.d2h_bytes += (long long)sizeof(double) * 5 * 8 * h.nown;
+  g.d2h_bytes += (long long)sizeof(double) * (5 + kDropinTracer) * 8 * h.nown;
   g.status |= *pst;
   if (g.status & bad) return 0;
   const auto t4 = Clock::now();
@@ -1825,6 +1884,9 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
       W.p = dual ? Ue * (kG - 1.) : (kG - 1.) * (UE - ((Udu) * (Udu) + (Udv) * (Udv) + (Udw) * (Udw)) / (dl)*0.5);
       W.E = UE;
       W.a = std::sqrt(kG * W.p / dl);
+#ifdef EMMA_WRADHYD
+      W.dX = W.dX + p[kXPlane * nc8 + k];  // U.dX = W.dX, corrected, U2W (src/hydro_utils.c:3277)
+#endif
     }
   }
   g.updates += d.leaf;
@@ -1848,6 +1910,9 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
             W.v += Wc.v * 0.125;
             W.w += Wc.w * 0.125;
             W.p += Wc.p * 0.125;
+#ifdef EMMA_WRADHYD
+            W.dX += Wc.dX * 0.125;  // src/hydro_utils.c:3460
+#endif
           }
           W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);
           cell->field = W;

@@ -22,6 +22,7 @@ namespace emma {
 
 constexpr double kGam = 5. / 3.;   // GAMMA, src/param.h:4
 constexpr double kPmin = 1e-10;    // PMIN, src/param.h:20
+constexpr double kYhe = 0.;        // YHE without -DHELIUM / -DHESIMPLE, src/param.h:53 (tracer builds)
 constexpr double kErrTol = 1e-10;  // ERRTOL, src/hydro_utils.c:18
 constexpr int kNiterMax = 10;      // NITERMAX, src/hydro_utils.c:17
 
@@ -232,13 +233,15 @@ struct MathF64 {
   // upwind or the star state), du[0] = Us.m_n / Us.d and du[1] = ebar =
   // Us.E - |Us.m|^2 / (2 Us.d) (src/hydro_utils.c:2126-2128).
   static __device__ __forceinline__ void hllc(const double WL[7], const double WR[7], int n, double F[5],
-                                              unsigned &st, double *du = nullptr) {
+                                              unsigned &st, double *du = nullptr, const double *xs = nullptr,
+                                              double *fx = nullptr) {
     double SL, SR, ustar;
     speeds(WL, WR, n, SL, SR, ustar, st);
     double rL[7], rR[7], G[5] = {0., 0., 0., 0., 0.};
     rotate(WL, n, rL);
     rotate(WR, n, rR);
     if (du != nullptr) du[0] = du[1] = 0.;
+    if (fx != nullptr) *fx = 0.;
     if (SL >= 0. || SR <= 0.) {
       const double *r = (SL >= 0.) ? rL : rR;
       euler_rot(r, G);
@@ -246,6 +249,10 @@ struct MathF64 {
         const double mn = r[0] * r[1];
         du[0] = mn / r[0];
         du[1] = (r[5] - 0.5 * r[6] / r[0]);
+      }
+      if (fx != nullptr) {  // tracer: face dX from the centre fraction, flux du dX / d
+        const double dX = (r[0] * (1. - kYhe)) * xs[(SL >= 0.) ? 0 : 1];
+        *fx = (r[0] * r[1]) * dX / r[0];
       }
     } else {
       const bool left = (SL < 0.) && (ustar >= 0.);
@@ -262,6 +269,10 @@ struct MathF64 {
         G[2] += (fact * r[2] - d * r[2]) * S;
         G[3] += (fact * r[3] - d * r[3]) * S;
         G[4] += (fact * Es - E) * S;
+        if (fx != nullptr) {  // tracer flux with the star correction (src/hydro_utils.c:1534-1535)
+          const double dX = (d * (1. - kYhe)) * xs[left ? 0 : 1];
+          *fx = (d * un) * dX / d + (fact * dX / d - dX) * S;
+        }
         if (du != nullptr) {  // the star state: momenta in x,y,z order for the sum of squares
           const double ds = fact * 1., mn = fact * ustar, m1 = fact * r[2], m2 = fact * r[3];
           const double mm = (n == 2) ? ((m1 * m1 + m2 * m2) + mn * mn) : ((mn * mn + m1 * m1) + m2 * m2);
@@ -356,7 +367,7 @@ struct MathF32 {
   // E - Ekin cancellation: p/(g-1) upwind, fact (p/((g-1) d) + (u*-u)((u*-u)/2 +
   // p/(d (S-u)))) in the star region (algebraically the reference's expression).
   static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st,
-                                              float *du = nullptr) {
+                                              float *du = nullptr, const float *xs = nullptr, float *fx = nullptr) {
     const float dL = WL[0], pL = WL[4], iL = WL[5], aL = WL[6];
     const float dR = WR[0], pR = WR[4], iR = WR[5], aR = WR[6];
     const float uL = (n == 0) ? WL[1] : ((n == 1) ? WL[2] : WL[3]);
@@ -421,6 +432,12 @@ struct MathF32 {
       G1 = side ? H1 : 0.f;
       G2 = side ? H2 : 0.f;
       G4 = side ? H4 : 0.f;
+    }
+    if (fx != nullptr) {  // tracer: face dX from the centre fraction, flux du dX / d (+ star correction)
+      const float dX = d * (1.f - (float)kYhe) * xs[useL ? 0 : 1];
+      const float f6 = mn * dX * id;
+      const float h6 = f6 + (fact * dX * id - dX) * S;
+      *fx = star ? (side ? h6 : 0.f) : f6;
     }
     if (du != nullptr) {
       const float ig = 1.f / (G - 1.f), dd = ustar - un;

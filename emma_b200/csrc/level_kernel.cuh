@@ -171,8 +171,10 @@ __device__ __forceinline__ void slot_tables(unsigned char *tab) {
 }
 
 // Shared memory of one tile, after the slot tables.  DUAL: dual-energy builds add
-// the internal-energy flux and the normal star velocity of every face.
-template <class M, class G, bool DUAL = false>
+// the internal-energy flux and the normal star velocity of every face.  TRACER
+// (-DWRADHYD, not with DUAL): the ionised fraction of every staged cell and the
+// tracer flux of every face.
+template <class M, class G, bool DUAL = false, bool TRACER = false>
 struct TileSmem {
   using R = typename M::R;
   static constexpr bool kF64 = sizeof(R) == 8;
@@ -204,7 +206,10 @@ struct TileSmem {
   static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
   static constexpr size_t off_F5 = off_end;                       // R [NF] (DUAL)
   static constexpr size_t off_S = a16(off_F5 + sizeof(R) * NF);  // R [NF] (DUAL)
-  static constexpr size_t bytes = DUAL ? a16(off_S + sizeof(R) * NF) : off_end;
+  static constexpr size_t off_X = off_end;                        // R [NBOX] (TRACER)
+  static constexpr size_t off_FX = a16(off_X + sizeof(R) * NBOX);  // R [NF] (TRACER)
+  static constexpr size_t bytes = DUAL ? a16(off_S + sizeof(R) * NF) : (TRACER ? a16(off_FX + sizeof(R) * NF) : off_end);
+  static_assert(!(DUAL && TRACER), "the tracer variant has no dual energy");
   static_assert(off_F1 + sizeof(R) * NF <= off_M, "face fluxes must fit in the staged box");
   // FP64 gravity kicks of the brick cells during P2/P3: R [3][kThreads] at the end of
   // the staged box, after the face fluxes
@@ -217,12 +222,12 @@ struct TileSmem {
 // the next tile's slot descriptors (next_tile >= 0: same level) are loaded
 // while this tile is reconstructed and solved, into the other descriptor
 // buffer; `cur`/`have` track which buffer holds the current tile's.
-template <class M, class G, bool GRAV, bool DUAL>
+template <class M, class G, bool GRAV, bool DUAL, bool TRACER = false>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
                                            const int next_tile, unsigned char *smem, const unsigned char *tab,
                                            unsigned &st, int &cur, bool &have, int &args_slot) {
   using R = typename M::R;
-  using SM = TileSmem<M, G, DUAL>;
+  using SM = TileSmem<M, G, DUAL, TRACER>;
   constexpr bool F64 = SM::kF64;
   constexpr int NS = SM::NS, NRING = SM::NRING;
   using V = Q4<R>;
@@ -244,6 +249,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
   R *sF5 = reinterpret_cast<R *>(smem + SM::off_F5);
   R *sS = reinterpret_cast<R *>(smem + SM::off_S);
+  R *sX = reinterpret_cast<R *>(smem + SM::off_X);    // TRACER: dX / (d (1 - YHE)) of the staged cells
+  R *sFX = reinterpret_cast<R *>(smem + SM::off_FX);  // TRACER: face fluxes of dX
   // cells whose face states are built: leaves; dual-energy builds also split cells,
   // whose faces enter the p div(u) term (src/hydro_utils.c:2126-2129 sum every face)
   auto recon_ok = [](uint8_t f) { return DUAL ? (f & kFPresent) != 0 : f_ok(f); };
@@ -360,12 +367,18 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       }
       const int cmk = sCmk[sg];
       double x0[5], x1[5];
+      double t0 = 0., t1 = 0.;  // TRACER: dX of the two cells
       if (cmk == 1) {  // injected coarser cell: one value for both children
         const bool inj = sf & kFInj;
         const double *p = (inj ? Wc : W) + (long long)sOb[sg];
         const long long stride = inj ? nc8 : N8;
 #pragma unroll
         for (int v = 0; v < 5; v++) x0[v] = x1[v] = __ldg(p + v * stride);
+        if constexpr (TRACER) {
+          const double *px = inj ? A.Xc : A.X;
+          if (px != nullptr) t0 = t1 = __ldg(px + (long long)sOb[sg]);
+          else st |= kStTree;
+        }
       } else {
         unsigned code = (unsigned)q | (1u << 3);  // pair q, elements 0 and 1
         if (cmk >= 2) code = (mir >> (4 * (cmk - 2))) & 15u;
@@ -379,6 +392,19 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
           x0[v] = e0 ? x.y : x.x;
           x1[v] = e1 ? x.y : x.x;
         }
+        if constexpr (TRACER) {
+          if (!itp && A.X != nullptr) {
+            const double2 x = __ldg(reinterpret_cast<const double2 *>(A.X + (long long)sOb[sg] + 2 * (code & 3)));
+            t0 = e0 ? x.y : x.x;
+            t1 = e1 ? x.y : x.x;
+          } else {
+            st |= kStTree;  // no tracer for interpolated coarser cells
+          }
+        }
+      }
+      if constexpr (TRACER) {  // X0 = dX / (d (1 - YHE)) (src/hydro_utils.c:1245)
+        sX[b0] = (R)(t0 / (x0[0] * (1. - kYhe)));
+        sX[b0 + 1] = (R)(t1 / (x1[0] * (1. - kYhe)));
       }
       V::st(sW, b0, SM::NBOX, (R)x0[0], (R)x0[1], (R)x0[2], (R)x0[3]);
       V::st(sW, b0 + 1, SM::NBOX, (R)x1[0], (R)x1[1], (R)x1[2], (R)x1[3]);
@@ -569,14 +595,19 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   // leaf of the tile on either side the face is not solved.
   auto solve_face = [&](int d, int e, int tL, int bL, int jL, int tR, int bR, int jR) {
     const uint8_t fL = sSt[bL], fR = sSt[bR];
-    R F[5] = {0, 0, 0, 0, 0}, du[2] = {0, 0};
+    R F[5] = {0, 0, 0, 0, 0}, du[2] = {0, 0}, fx = 0;
     if ((f_tileleaf(fL) || f_tileleaf(fR)) && recon_ok(fL) && recon_ok(fR)) {
       R WL[7], WR[7];
       if (jL >= 0) ring_face(jL, WL);
       else brick_face(tL, bL, 2 * d + 1, WL);
       if (jR >= 0) ring_face(jR, WR);
       else brick_face(tR, bR, 2 * d, WR);
-      M::hllc(WL, WR, d, F, st, DUAL ? du : nullptr);
+      if constexpr (TRACER) {
+        const R xs[2] = {sX[bL], sX[bR]};
+        M::hllc(WL, WR, d, F, st, nullptr, xs, &fx);
+      } else {
+        M::hllc(WL, WR, d, F, st, DUAL ? du : nullptr);
+      }
       if (DUAL && !(f_ok(fL) && f_ok(fR))) {
 #pragma unroll
         for (int v = 0; v < 5; v++) F[v] = (R)0;
@@ -589,6 +620,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       sF5[e] = du[0] * du[1];  // (Us.m_n / Us.d) ebar (src/hydro_utils.c:2128)
       sS[e] = du[0];
     }
+    if constexpr (TRACER) sFX[e] = fx;
   };
 
   // ------------------------------------------------------------------ P2
@@ -717,7 +749,9 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       for (int v = 0; v < 5; v++) q[v] = __ldg(A.W + v * N8 + gi);
     }
     double Wout[5];
+    double Xout = 0.;  // TRACER: the new dX
     if (fme & kFSplit) {
+      if constexpr (TRACER) Xout = (A.X != nullptr) ? __ldg(A.X + gi) : 0.;
       // split cell: primitive mean of the 8 children (src/hydro_utils.c:3420-3481);
       // without the finer level (drop-in mode) the caller averages on the host
       double acc[5] = {0., 0., 0., 0., 0.};
@@ -880,6 +914,22 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 #pragma unroll
         for (int v = 0; v < 3; v++) Wout[1 + v] += (-__ldg(A.F + v * N8 + gi) * A.dt);
       }
+      if constexpr (TRACER) {
+        // dX: the caller's fieldnew (or field + corrections) plus the flux divergence
+        // in the faces' order (src/hydro_utils.c:3068, 3158), then the ceiling
+        // 0 <= dX <= d (1 - YHE) (:3197-3198)
+        double Ux = (A.BX != nullptr) ? A.BX[gi] : ((A.X != nullptr) ? __ldg(A.X + gi) : 0.);
+        if (A.BX == nullptr && A.C != nullptr) Ux += __ldcg(A.C + kXPlane * N8 + gi);
+        double dUx = 0., one = 1.;
+#pragma unroll
+        for (int k = 0; k < 6; k++) {
+          dUx += (double)sFX[face_of(k)] * dtsurdx * one;
+          one *= -1.;
+        }
+        Xout = Ux + dUx;
+        if (Xout < 0) Xout = 0.;
+        if (Xout > (Wout[0] * (1. - kYhe))) Xout = Wout[0] * (1. - kYhe);
+      }
 
       // fine -> coarse correction into unsplit coarser neighbours (src/hydro_utils.c:3206-3295)
 #pragma unroll
@@ -897,10 +947,15 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 #pragma unroll
         for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, F[v] * dtsurdx * one * 0.125);
         if constexpr (DUAL) atomicAdd(A.Cc + 5 * A.nc8 + cc, (double)sF5[face_of(k)] * dtsurdx * one * 0.125);
+        if constexpr (TRACER)
+          atomicAdd(A.Cc + kXPlane * A.nc8 + cc, (double)sFX[face_of(k)] * dtsurdx * one * 0.125);
       }
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) A.Wn[v * N8 + gi] = Wout[v];
+    if constexpr (TRACER) {
+      if (A.Xn != nullptr) A.Xn[gi] = Xout;
+    }
     if (Bt.smax != nullptr) {
       // the next time step's CFL term of this cell, as L_comptstep_hydro evaluates it
       // (src/advanceamr.c:122-128): IEEE operations, no contraction
@@ -928,10 +983,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 
 // Bytes of dynamic shared memory of a kernel handling the shapes in `shapes`
 // (bit i: kShapes[i]).
-template <class M, bool DUAL = false>
+template <class M, bool DUAL = false, bool TRACER = false>
 constexpr size_t level_smem_bytes(unsigned shapes) {
-  const size_t a = (shapes & 1u) ? TileSmem<M, GeomA, DUAL>::bytes : 0,
-               b = (shapes & 2u) ? TileSmem<M, GeomB, DUAL>::bytes : 0;
+  const size_t a = (shapes & 1u) ? TileSmem<M, GeomA, DUAL, TRACER>::bytes : 0,
+               b = (shapes & 2u) ? TileSmem<M, GeomB, DUAL, TRACER>::bytes : 0;
   return a > b ? a : b;
 }
 
@@ -944,9 +999,9 @@ constexpr size_t level_smem_bytes(unsigned shapes) {
 // (64 registers, 55 KB of shared memory); with 2x2x2 bricks shared memory
 // allows 2; the FP64 kernel 2 with 4x4x2 bricks (128 registers, 110 KB), 1 with
 // 2x2x2 bricks.
-template <class M, unsigned SHAPES, bool DUAL = false>
-constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? ((SHAPES == 1u && !DUAL) ? 2 : 1)
-                                                         : (SHAPES == 1u ? (DUAL ? 3 : 4) : 2);
+template <class M, unsigned SHAPES, bool DUAL = false, bool TRACER = false>
+constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? ((SHAPES == 1u && !DUAL && !TRACER) ? 2 : 1)
+                                                         : (SHAPES == 1u ? ((DUAL || TRACER) ? 3 : 4) : 2);
 // 228 KB of shared memory per SM, 1 KB reserved per CTA
 static_assert(4 * (TileSmem<MathF32, GeomA>::bytes + 1024) <= 228 * 1024, "4 FP32 4x4x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF32, GeomB>::bytes + 1024) <= 228 * 1024, "2 FP32 2x2x2 CTAs per SM");
@@ -954,9 +1009,13 @@ static_assert(2 * (TileSmem<MathF64, GeomA>::bytes + 1024) <= 228 * 1024, "2 FP6
 static_assert(3 * (TileSmem<MathF32, GeomA, true>::bytes + 1024) <= 228 * 1024, "3 dual-energy FP32 4x4x2 CTAs");
 static_assert(2 * (TileSmem<MathF32, GeomB, true>::bytes + 1024) <= 228 * 1024, "2 dual-energy FP32 2x2x2 CTAs");
 static_assert(TileSmem<MathF64, GeomB, true>::bytes + 1024 <= 227 * 1024, "a dual-energy FP64 2x2x2 CTA");
+static_assert(3 * (TileSmem<MathF32, GeomA, false, true>::bytes + 1024) <= 228 * 1024, "3 tracer FP32 4x4x2 CTAs");
+static_assert(2 * (TileSmem<MathF32, GeomB, false, true>::bytes + 1024) <= 228 * 1024, "2 tracer FP32 2x2x2 CTAs");
+static_assert(TileSmem<MathF64, GeomB, false, true>::bytes + 1024 <= 227 * 1024, "a tracer FP64 2x2x2 CTA");
 
-template <class M, unsigned SHAPES, bool GRAV, bool DUAL>
-__global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL>)) level_batch_kernel(const BatchArgs Bt) {
+template <class M, unsigned SHAPES, bool GRAV, bool DUAL, bool TRACER = false>
+__global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL, TRACER>))
+    level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
   if constexpr ((SHAPES & 1u) != 0) slot_tables<GeomA>(smem);
@@ -979,14 +1038,16 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL>)) level
     }
     const LevelArgs *gA = Bt.lv + slot;
     if constexpr (SHAPES == 1u) {
-      level_tile<M, GeomA, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+      level_tile<M, GeomA, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
     } else if constexpr (SHAPES == 2u) {
-      level_tile<M, GeomB, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
+      level_tile<M, GeomB, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
+                                               args_slot);
     } else {
       if (gA->shape == 0)
-        level_tile<M, GeomA, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+        level_tile<M, GeomA, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
       else
-        level_tile<M, GeomB, GRAV, DUAL>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have, args_slot);
+        level_tile<M, GeomB, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
+                                                 args_slot);
     }
     __syncthreads();
   }
@@ -1008,11 +1069,11 @@ namespace {
 
 // Launch of a work list on a persistent grid of ctas_per_sm CTAs per SM (0 or
 // above the occupancy limit: the limit), so that every CTA is co-resident.
-template <class M, unsigned SHAPES, bool GRAV, bool DUAL>
+template <class M, unsigned SHAPES, bool GRAV, bool DUAL, bool TRACER = false>
 cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cudaStream_t s, int *occupancy) {
   static int occ = 0;
-  auto k = level_batch_kernel<M, SHAPES, GRAV, DUAL>;
-  constexpr size_t bytes = level_smem_bytes<M, DUAL>(SHAPES);
+  auto k = level_batch_kernel<M, SHAPES, GRAV, DUAL, TRACER>;
+  constexpr size_t bytes = level_smem_bytes<M, DUAL, TRACER>(SHAPES);
   if (occ == 0) {
     cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
@@ -1032,8 +1093,11 @@ cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cu
 template <class M>
 cudaError_t launch_level_any(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
                              int *occupancy) {
-  constexpr unsigned G = kLaunchGrav, D = kLaunchDual;
+  constexpr unsigned G = kLaunchGrav, D = kLaunchDual, T = kLaunchTracer;
   switch (shapes) {
+    case 1u | T: return launch_level_shapes<M, 1u, false, false, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u | T: return launch_level_shapes<M, 2u, false, false, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u | T: return launch_level_shapes<M, 3u, false, false, true>(a, nsm, ctas_per_sm, s, occupancy);
     case 1u: return launch_level_shapes<M, 1u, false, false>(a, nsm, ctas_per_sm, s, occupancy);
     case 2u: return launch_level_shapes<M, 2u, false, false>(a, nsm, ctas_per_sm, s, occupancy);
     case 3u: return launch_level_shapes<M, 3u, false, false>(a, nsm, ctas_per_sm, s, occupancy);

@@ -42,6 +42,10 @@ constexpr int kNumShapes = 2;
 constexpr unsigned kLaunchGrav = 4u;
 // ... and the dual-energy variant (-DDUAL_E: tracked internal energy, 6 correction planes).
 constexpr unsigned kLaunchDual = 8u;
+// ... and the tracer variant (-DWRADHYD: the advected ionised density dX; its
+// corrections are plane kXPlane of Cc).  Not combined with gravity or dual energy.
+constexpr unsigned kLaunchTracer = 16u;
+constexpr int kXPlane = 5;
 constexpr BrickShape kShapes[kNumShapes] = {{4, 4, 2, 1}, {2, 2, 2, 4}};
 static_assert(kShapes[0].nb * 8 * kShapes[0].octs() == kThreads, "one thread per brick cell");
 static_assert(kShapes[1].nb * 8 * kShapes[1].octs() == kThreads, "one thread per brick cell");
@@ -85,9 +89,18 @@ struct LevelArgs {
   int wait_slot;      // level whose tiles must all be updated before this level's
                       // update phase starts (batched launches), -1 for none
   long long leaf;     // leaf cells (cell-updates of one substep)
-  // gravity coupling (-DWGRAV), all null/0 without it
-  const double *F;    // acceleration of the level's cells: planes fx,fy,fz of 8*noct
-  const double *Fc;   // acceleration of level L-1 (read by the interpolation kernel)
+  // gravity coupling (-DWGRAV), all null/0 without it.  The tracer variant
+  // (-DWRADHYD) has neither gravity nor dual energy and reuses their pointer
+  // slots (unions): the struct is copied into every CTA's shared memory, whose
+  // 4-CTA budget of the FP32 kernel leaves no room for more members.
+  union {
+    const double *F;  // acceleration of the level's cells: planes fx,fy,fz of 8*noct
+    const double *X;  // tracer: dX of the level's field (plane of 8*noct)
+  };
+  union {
+    const double *Fc;  // acceleration of level L-1 (read by the interpolation kernel)
+    const double *Xc;  // tracer: dX of level L-1 (injected neighbours)
+  };
   double *Fv;         // accelerations of the interpolated coarser cells: planes of 8 * nv
   int gcorr;          // apply grav_correction (src/hydro_utils.c:2388-2444) to the new state
   int wv_inject;      // the interpolation list fills Wv by injection (gravity build), not by
@@ -95,8 +108,14 @@ struct LevelArgs {
   // dual energy: split cells whose stored sound speed is 0 (the reference's
   // averaging leaves a = 0, src/hydro_utils.c:3417-3481, and its predictor reads the
   // stored a, :976-1120): per cell, or every split cell once *azall != 0
-  const uint8_t *az;
-  const int *azall;
+  union {
+    const uint8_t *az;
+    double *Xn;  // tracer: the new dX written by the level kernel
+  };
+  union {
+    const int *azall;
+    const double *BX;  // tracer: the update base, the caller's fieldnew.dX (drop-in mode)
+  };
 };
 
 // A launch of the level kernel: a list of (level slot, tile) work items,

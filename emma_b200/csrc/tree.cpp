@@ -24,6 +24,9 @@
 #ifdef EMMA_WGRAV
 #include "emma_hydro_grav.h"
 #endif
+#ifdef EMMA_WRADHYD
+#include "emma_hydro_rh.h"
+#endif
 
 struct EmmaTree {
   // octs live in fixed-size blocks so that pointers stay valid as the tree grows
@@ -229,6 +232,20 @@ void emma_tree_set_cpu(struct EmmaTree *t, int level, const int *cpu) {
   long long i = 0;
   for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++) o->cpu = cpu[i];
 }
+
+#ifdef EMMA_WRADHYD
+void emma_tree_set_tracer(struct EmmaTree *t, int level, const double *dX) {
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) o->cell[c].field.dX = o->cell[c].fieldnew.dX = dX[8 * i + c];
+}
+
+void emma_tree_get_tracer(struct EmmaTree *t, int level, int which, double *out) {
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) out[8 * i + c] = which ? o->cell[c].fieldnew.dX : o->cell[c].field.dX;
+}
+#endif
 
 #ifdef EMMA_WGRAV
 void emma_tree_set_force(struct EmmaTree *t, int level, const double *fx, const double *fy, const double *fz) {

@@ -142,8 +142,10 @@ def _ref(x):
 
 def HydroSolver(level, firstoct, dtnew, cpu=None, grav=False):
     """Drop-in HydroSolver (src/hydro_utils.c:3378) on a host tree; grav: a tree of
-    the -DWGRAV layout through libemmahydro_grav.so (gravity-coupled advance).
-    cpu: a CpuInfo (advance the octs of cpu.rank only), or None for rank 0."""
+    the -DWGRAV layout through libemmahydro_grav.so (gravity-coupled advance), or
+    "rh": a tree of the -DWRADHYD layout through libemmahydro_rh.so (the ionised
+    density advected too).  cpu: a CpuInfo (advance the octs of cpu.rank only), or
+    None for rank 0."""
     lib(grav).HydroSolver(level, None, firstoct, _ref(cpu), None, 0, dtnew)
 
 

@@ -16,12 +16,14 @@ CELL_OFF = np.array([[c % 2, (c // 2) % 2, c // 4] for c in range(8)], dtype=np.
 class OctTree:
     """An EMMA oct tree in host memory (levels lcoarse..lmax are hydro levels)."""
 
-    def __init__(self, lcoarse, lmax, ngridmax=0, grav=False):
+    def __init__(self, lcoarse, lmax, ngridmax=0, grav=False, rh=False):
         """grav: the reference's -DWGRAV cell layout (built by libemmahydro_grav.so),
-        for the gravity-coupled drop-in entries."""
+        for the gravity-coupled drop-in entries; rh: its -DWRADHYD layout (the cells
+        carry the ionised density dX; libemmahydro_rh.so)."""
+        assert not (grav and rh), "one cell layout at a time"
         self.lcoarse, self.lmax = lcoarse, lmax
-        self.grav = grav
-        self._L = lib(grav)
+        self.grav, self.rh = grav, rh
+        self._L = lib("rh" if rh else grav)
         self._t = self._L.emma_tree_create(lcoarse, lmax, ngridmax)
         if not self._t:
             raise RuntimeError("emma_tree_create failed")
@@ -76,6 +78,20 @@ class OctTree:
         assert self.grav, "the default cell layout has no force"
         arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (fx, fy, fz)]
         self._L.emma_tree_set_force(self._t, level, *[ptr(a) for a in arrs])
+
+    def set_tracer(self, level, dX):
+        """Ionised density dX of field and fieldnew of every cell of a level (rh trees)."""
+        assert self.rh, "only the -DWRADHYD layout has dX"
+        a = np.ascontiguousarray(dX, dtype=np.float64)
+        assert a.size == 8 * self.noct(level)
+        self._L.emma_tree_set_tracer(self._t, level, ptr(a))
+
+    def get_tracer(self, level, which=0):
+        assert self.rh, "only the -DWRADHYD layout has dX"
+        out = np.zeros(8 * self.noct(level))
+        if out.size:
+            self._L.emma_tree_get_tracer(self._t, level, which, ptr(out))
+        return out
 
     def get_fields(self, level, which=0):
         """(7, 8*noct): d,u,v,w,p,a,E of `field` (which=0) or `fieldnew` (which=1)."""

@@ -2,13 +2,15 @@
  * emma_oct.h -- the oct-tree memory layout that EMMA's hydro entry points pass
  * around, declared for a build with -DWHYDRO2 (and neither -DWRAD, -DPIC nor
  * -DWRADHYD), REAL = double, NVAR = 6; with EMMA_WGRAV defined, for the
- * reference's -DWGRAV build (libemmahydro_grav.so).
+ * reference's -DWGRAV build (libemmahydro_grav.so); with EMMA_WRADHYD defined,
+ * for its -DWRADHYD build without -DHELIUM (NVAR = 7: the ionised density dX
+ * follows E in Wtype; libemmahydro_rh.so).
  *
  * This is an interface, not an implementation: libemmahydro reads and writes the
  * caller's tree in place, so the field order, types and padding must be exactly
  * those of the reference (src/prototypes.h:611 Wtype, :653 Utype, :825 CELL,
  * :1028 OCT).  Sizes are checked at compile time: CELL 136 B, OCT 1200 B
- * (EMMA_WGRAV: CELL 192 B, OCT 1648 B).
+ * (EMMA_WGRAV: CELL 192 B, OCT 1648 B; EMMA_WRADHYD: CELL 152 B, OCT 1328 B).
  * Only the members the hydro path uses are named; nothing else is assumed.
  */
 #ifndef EMMA_OCT_H
@@ -24,7 +26,14 @@ struct Wtype {           /* primitive state of a cell, src/prototypes.h:611 */
   REAL d, u, v, w, p;    /* density, velocity, pressure */
   REAL a;                /* sound speed */
   REAL E;                /* total energy density */
+#ifdef EMMA_WRADHYD
+  REAL dX;               /* ionised density, advected with the gas */
+#endif
 };
+
+#if defined(EMMA_WGRAV) && defined(EMMA_WRADHYD)
+#error "libemmahydro is built for one of the -DWGRAV and -DWRADHYD layouts at a time"
+#endif
 
 struct OCT;
 
@@ -68,9 +77,11 @@ struct RUNPARAMS;
 struct HGRID;
 
 /* sizeof(struct HGRID) with the flags above (-DWHYDRO2, NVAR 6; the stencil cells
- * also carry f[3] with -DWGRAV) */
-#ifdef EMMA_WGRAV
+ * also carry f[3] with -DWGRAV; NVAR 7 with -DWRADHYD) */
+#if defined(EMMA_WGRAV)
 #define EMMA_SIZEOF_HGRID 21760
+#elif defined(EMMA_WRADHYD)
+#define EMMA_SIZEOF_HGRID 18752
 #else
 #define EMMA_SIZEOF_HGRID 16576
 #endif
@@ -79,9 +90,12 @@ struct HGRID;
 }
 #endif
 
-#ifdef EMMA_WGRAV
+#if defined(EMMA_WGRAV)
 #define EMMA_SIZEOF_CELL 192
 #define EMMA_SIZEOF_OCT 1648
+#elif defined(EMMA_WRADHYD)
+#define EMMA_SIZEOF_CELL 152
+#define EMMA_SIZEOF_OCT 1328
 #else
 #define EMMA_SIZEOF_CELL 136
 #define EMMA_SIZEOF_OCT 1200

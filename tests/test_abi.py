@@ -9,12 +9,13 @@ HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.j
 
 
 GRAV_HEADER = os.path.join(ROOT, "include", "emma_hydro_grav.h")
+RH_HEADER = os.path.join(ROOT, "include", "emma_hydro_rh.h")
 
 
 def declared_functions(headers=None):
-    """Functions declared in the headers (default: all but the gravity library's own)."""
+    """Functions declared in the headers (default: all but the layout libraries' own)."""
     names = set()
-    for h in (headers if headers is not None else [h for h in HEADERS if h != GRAV_HEADER]):
+    for h in (headers if headers is not None else [h for h in HEADERS if h not in (GRAV_HEADER, RH_HEADER)]):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         src = re.sub(r"//[^\n]*", "", src)
@@ -46,11 +47,23 @@ def test_gravity_library_exports_everything():
     and its own (grav_correction, the force setter of test trees)."""
     from emma_b200._lib import LIB_PATH_GRAV, SIGNATURES, GRAV_SIGNATURES
     L = ctypes.CDLL(LIB_PATH_GRAV)
-    names = declared_functions(HEADERS)
+    names = declared_functions([h for h in HEADERS if h != RH_HEADER])
     assert {"grav_correction", "emma_tree_set_force"} <= names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
     assert names <= {n for n, _, _ in SIGNATURES + GRAV_SIGNATURES}
+
+
+def test_tracer_library_exports_everything():
+    """libemmahydro_rh.so (the -DWRADHYD cell layout) exports the default entries and
+    the tracer accessors of test trees."""
+    from emma_b200._lib import LIB_PATH_RH, SIGNATURES, RH_SIGNATURES
+    L = ctypes.CDLL(LIB_PATH_RH)
+    names = declared_functions([h for h in HEADERS if h != GRAV_HEADER])
+    assert {"emma_tree_set_tracer", "emma_tree_get_tracer"} <= names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert names <= {n for n, _, _ in SIGNATURES + RH_SIGNATURES}
 
 
 def test_struct_layout_matches_reference():
@@ -65,8 +78,8 @@ def test_hgrid_size_matches_reference_builds():
     import re
     import oracle
     src = open(os.path.join(ROOT, "include", "emma_oct.h")).read()
-    grav, plain = (int(x) for x in re.findall(r"#define EMMA_SIZEOF_HGRID (\d+)", src))
-    for name, want in (("libemmaref.so", plain), ("libemmaref_grav.so", grav)):
+    grav, rh, plain = (int(x) for x in re.findall(r"#define EMMA_SIZEOF_HGRID (\d+)", src))
+    for name, want in (("libemmaref.so", plain), ("libemmaref_grav.so", grav), ("libemmaref_rh.so", rh)):
         path = os.path.join(ROOT, "oracle", "_ref", name)
         if not os.path.exists(path):
             continue
