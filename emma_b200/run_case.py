@@ -1,8 +1,12 @@
 """Run a configuration for a few coarse steps and print the level-kernel timing.
 
     python -m emma_b200.run_case --config random --level 6 --precision mixed --steps 3
+    python -m emma_b200.run_case --config turb --level 7 --precision fp64 --steps 2 --dropin rh
 
-Used to profile one configuration in isolation (for example under ncu).
+Used to profile one configuration in isolation (for example under ncu).  --dropin
+runs the drop-in clean_new_hydro + HydroSolver on the finest level of the host tree
+instead of the resident schedule, through libemmahydro.so (plain) or the -DWRADHYD
+library (rh, with an ionised fraction of 1/2).
 """
 import argparse
 import ctypes
@@ -17,10 +21,13 @@ def main():
     ap.add_argument("--level", type=int, default=6)
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--dropin", default=None, choices=["plain", "rh"])
     a = ap.parse_args()
     cfg = {"random": lambda: configs.random_uniform(level=a.level), "turb": lambda: configs.turb(level=a.level),
            "sod": lambda: configs.sod(level=a.level), "sedov": configs.sedov, "cosmo": configs.cosmo,
            "amr": configs.small_amr}[a.config]()
+    if a.dropin is not None:
+        return dropin(a, cfg)
     tree = cfg.build()
     # host-driven schedule: every level-kernel launch is timed with CUDA events
     r = ResidentHydro(tree, precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64, trans=cfg.trans,
@@ -41,6 +48,31 @@ def main():
                       "avg_launch_ms": tot_ms / max(tot_n, 1), "cells_per_launch": tot_cells / max(tot_n, 1),
                       "kernel_ms_per_step": per_step,
                       "cell_updates_per_s_kernel": tot_cells / (tot_ms * 1e-3) if tot_ms else None}))
+
+
+def dropin(a, cfg):
+    from .tree import OctTree
+    from . import hydro as H
+    from ._lib import EmmaHydroOptions
+    key = "rh" if a.dropin == "rh" else False
+    tree = cfg.build(lambda lc, lm: OctTree(lc, lm, rh=(key == "rh")))
+    level = cfg.lmax
+    if key == "rh":
+        tree.set_tracer(level, 0.5 * tree.get_fields(level, 0)[0])
+    L = lib(key)
+    o = EmmaHydroOptions()
+    L.emma_hydro_default_options(ctypes.byref(o))
+    o.precision = PREC_MIXED if a.precision == "mixed" else PREC_FP64
+    L.emma_hydro_set_options(ctypes.byref(o))
+    L.emma_hydro_reset_counters()
+    for _ in range(a.steps):
+        H.clean_new_hydro(level, tree.firstoct, grav=key)
+        H.HydroSolver(level, tree.firstoct, 1e-4, grav=key)
+    avg, n, cells = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
+    L.emma_hydro_kernel_timing(ctypes.byref(avg), ctypes.byref(n), ctypes.byref(cells))
+    print(json.dumps({"config": cfg.name, "dropin": a.dropin, "precision": a.precision, "status": L.emma_hydro_status(),
+                      "launches": n.value, "avg_launch_ms": avg.value,
+                      "cells_per_launch": cells.value / max(n.value, 1)}))
 
 
 if __name__ == "__main__":
