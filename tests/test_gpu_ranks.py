@@ -190,6 +190,27 @@ def test_multi_rank_dropin_dual_energy(gpu):
     check_owned(trees, owner, run_single(dual=True))
 
 
+def test_multi_rank_dropin_mixed_precision(gpu):
+    """The mixed path on the ranks' trees: L1 <= 1e-5 against the single-rank FP64 oracle."""
+    from emma_b200 import PREC_MIXED
+    from helpers import l1_rel
+    L = lib()
+    o = EmmaHydroOptions()
+    L.emma_hydro_default_options(ctypes.byref(o))
+    o.precision = PREC_MIXED
+    assert L.emma_hydro_set_options(ctypes.byref(o)) == 0
+    trees, owner = run_ranks("stripes3")
+    ref = run_single()
+    for l in range(LC, LMAX + 1):
+        cell_owner = np.repeat(owner[l], 8)
+        g = np.zeros_like(ref.get_fields(l)[:5])
+        for r, t in enumerate(trees):
+            m = cell_owner == r
+            g[:, m] = t.get_fields(l)[:5][:, m]
+        o_ = ref.get_fields(l)[:5]
+        assert l1_rel(g[0], o_[0]) <= 1e-5 and l1_rel(g[4], o_[4]) <= 1e-5, l
+
+
 def test_other_ranks_octs_are_left_alone(gpu):
     """advancehydroGPU returns this rank's oct count and writes no fieldnew of
     another rank's oct at the level; HydroSolver leaves their field as it was."""
