@@ -145,7 +145,8 @@ constexpr int kDropinGrav = 1;
 constexpr int kDropinGrav = 0;
 #endif
 // ... and those of a library built for its -DWRADHYD layout (libemmahydro_rh.so)
-// advance the ionised density dX too (drop-in entries only).
+// advance the ionised density dX too (in the resident mode the sixth plane of every
+// level state).
 #ifdef EMMA_WRADHYD
 constexpr int kDropinTracer = 1;
 #else
@@ -1101,8 +1102,8 @@ int emma_hydro_is_resident(struct OCT **firstoct) {
 
 int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int rank) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
-  if (kDropinTracer) {
-    fail(EMMA_ST_ARG, "the -DWRADHYD library advances the tracer through the drop-in entries only");
+  if (kDropinTracer && (g.opt.dual_energy || g.opt.trans_flags || g.opt.gravity)) {
+    fail(EMMA_ST_ARG, "the -DWRADHYD library has neither dual energy, transmissive boundaries nor gravity");
     return EMMA_ST_ARG;
   }
   if (firstoct == nullptr || lcoarse < 2 || lmax < lcoarse || lmax >= kMaxLevels) {
@@ -1175,9 +1176,19 @@ int emma_hydro_fields_upload(struct OCT **firstoct) {
     if (h.noct == 0) continue;
     double *W = current_state(L);
     if (W == nullptr) return EMMA_ST_CUDA;
-    const size_t bytes = sizeof(double) * 5 * 8 * (size_t)h.noct;
+    // d,u,v,w,p (tracer builds: and dX, the sixth plane of a resident state)
+    const size_t bytes = sizeof(double) * (5 + kDropinTracer) * 8 * (size_t)h.noct;
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
     pack_level(h, 0, g.pin);
+#ifdef EMMA_WRADHYD
+    {
+      double *px = g.pin + 5 * 8LL * h.noct;
+      parallel_for(h.noct, [&](long long a0, long long b0) {
+        for (long long i = a0; i < b0; i++)
+          for (int c = 0; c < 8; c++) px[8 * i + c] = h.octs[i]->cell[c].field.dX;
+      });
+    }
+#endif
     CK(cudaMemcpyAsync(W, g.pin, bytes, cudaMemcpyHostToDevice, g.stream));
     g.h2d_bytes += (long long)bytes;
     CK(mark_stale(L));
@@ -1217,7 +1228,7 @@ int emma_hydro_tree_download(struct OCT **firstoct) {
     double *W = current_state(L);
     if (W == nullptr) return EMMA_ST_CUDA;
     const long long n8 = 8LL * h.noct;
-    const size_t bytes = sizeof(double) * 5 * (size_t)n8;
+    const size_t bytes = sizeof(double) * (5 + kDropinTracer) * (size_t)n8;
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
     CK(cudaMemcpyAsync(g.pin, W, bytes, cudaMemcpyDeviceToHost, g.stream));
     g.d2h_bytes += (long long)bytes;
@@ -1234,6 +1245,9 @@ int emma_hydro_tree_download(struct OCT **firstoct) {
           W.v = p[2 * n8 + k];
           W.w = p[3 * n8 + k];
           W.p = p[4 * n8 + k];
+#ifdef EMMA_WRADHYD
+          W.dX = p[5 * n8 + k];
+#endif
           finish_prims(W);
           if (o->cell[c].child != nullptr) W.a = 0.;  // split cells: as the reference's averaging leaves them
           o->cell[c].fieldnew = W;

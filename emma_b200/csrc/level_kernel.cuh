@@ -266,6 +266,12 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     args_slot = slot;
   }
   const long long N8 = 8LL * A.noct;
+  // TRACER: dX planes.  Drop-in levels (B set) name them; resident levels keep dX as
+  // the sixth plane of every state buffer, so that the schedule's buffer swaps carry it
+  const bool res_tr = TRACER && A.B == nullptr;
+  const double *Xs = res_tr ? A.W + 5 * N8 : A.X;
+  const double *Xcs = res_tr ? (A.Wc != nullptr ? A.Wc + 5 * A.nc8 : nullptr) : A.Xc;
+  double *Xns = res_tr ? A.Wn + 5 * N8 : A.Xn;
   const int tn = tid / G::kCells, tt = tid - tn * G::kCells;  // brick of the tile, cell of the brick
   int tx, ty, tz;
   G::cell_of(tt, tx, ty, tz);
@@ -375,7 +381,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 #pragma unroll
         for (int v = 0; v < 5; v++) x0[v] = x1[v] = __ldg(p + v * stride);
         if constexpr (TRACER) {
-          const double *px = inj ? A.Xc : A.X;
+          const double *px = inj ? Xcs : Xs;
           if (px != nullptr) t0 = t1 = __ldg(px + (long long)sOb[sg]);
           else st |= kStTree;
         }
@@ -393,8 +399,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
           x1[v] = e1 ? x.y : x.x;
         }
         if constexpr (TRACER) {
-          if (!itp && A.X != nullptr) {
-            const double2 x = __ldg(reinterpret_cast<const double2 *>(A.X + (long long)sOb[sg] + 2 * (code & 3)));
+          if (!itp && Xs != nullptr) {
+            const double2 x = __ldg(reinterpret_cast<const double2 *>(Xs + (long long)sOb[sg] + 2 * (code & 3)));
             t0 = e0 ? x.y : x.x;
             t1 = e1 ? x.y : x.x;
           } else {
@@ -751,7 +757,18 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     double Wout[5];
     double Xout = 0.;  // TRACER: the new dX
     if (fme & kFSplit) {
-      if constexpr (TRACER) Xout = (A.X != nullptr) ? __ldg(A.X + gi) : 0.;
+      if constexpr (TRACER) {
+        // the children's mean (src/hydro_utils.c:3460) when the finer level is at hand
+        Xout = (Xs != nullptr) ? __ldg(Xs + gi) : 0.;
+        if (A.Wf != nullptr && res_tr) {
+          const long long ch = A.child[gi];
+          if (ch >= 0) {
+            double ax = 0.;
+            for (int i = 0; i < 8; i++) ax += __ldcg(A.Wf + 5 * A.nf8 + 8 * ch + i) * 0.125;
+            Xout = ax;
+          }
+        }
+      }
       // split cell: primitive mean of the 8 children (src/hydro_utils.c:3420-3481);
       // without the finer level (drop-in mode) the caller averages on the host
       double acc[5] = {0., 0., 0., 0., 0.};
@@ -918,7 +935,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         // dX: the caller's fieldnew (or field + corrections) plus the flux divergence
         // in the faces' order (src/hydro_utils.c:3068, 3158), then the ceiling
         // 0 <= dX <= d (1 - YHE) (:3197-3198)
-        double Ux = (A.BX != nullptr) ? A.BX[gi] : ((A.X != nullptr) ? __ldg(A.X + gi) : 0.);
+        double Ux = (A.BX != nullptr) ? A.BX[gi] : ((Xs != nullptr) ? __ldg(Xs + gi) : 0.);
         if (A.BX == nullptr && A.C != nullptr) Ux += __ldcg(A.C + kXPlane * N8 + gi);
         double dUx = 0., one = 1.;
 #pragma unroll
@@ -954,7 +971,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 #pragma unroll
     for (int v = 0; v < 5; v++) A.Wn[v * N8 + gi] = Wout[v];
     if constexpr (TRACER) {
-      if (A.Xn != nullptr) A.Xn[gi] = Xout;
+      if (Xns != nullptr) Xns[gi] = Xout;
     }
     if (Bt.smax != nullptr) {
       // the next time step's CFL term of this cell, as L_comptstep_hydro evaluates it

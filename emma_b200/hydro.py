@@ -37,7 +37,8 @@ class ResidentHydro:
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
         self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
         self.precision = precision
-        L = lib()
+        # a tree of the -DWRADHYD layout runs on libemmahydro_rh.so (its tracer advanced too)
+        self._L = L = lib("rh" if getattr(tree, "rh", False) else False)
         o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity, dual=dual)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
         check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
@@ -52,74 +53,74 @@ class ResidentHydro:
         self.use_graph = use_graph
         o = options(self.precision, self.trans, self.cfl, use_graph=use_graph, tile_octs=self.tile_octs,
                     gravity=self.gravity, dual=self.dual)
-        check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
+        check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def set_precision(self, precision):
         self.precision = precision
         o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
                     gravity=self.gravity, dual=self.dual)
-        check(lib().emma_hydro_set_options(ctypes.byref(o)), "set_options")
+        check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):
         """Queue one coarse step on the device schedule without waiting."""
-        check(lib().emma_hydro_advance_coarse_step_async(dt_param, time_max, nsub), "advance_coarse_step_async")
+        check(self._L.emma_hydro_advance_coarse_step_async(dt_param, time_max, nsub), "advance_coarse_step_async")
 
     def time(self):
         t = ctypes.c_double()
-        check(lib().emma_hydro_get_time(ctypes.byref(t), ptr(self.adt)), "get_time")
+        check(self._L.emma_hydro_get_time(ctypes.byref(t), ptr(self.adt)), "get_time")
         self.tsim = t.value
         return self.tsim
 
     def noct(self, level):
-        return lib().emma_hydro_level_noct(level)
+        return self._L.emma_hydro_level_noct(level)
 
     def state(self, level):
         n8 = 8 * self.noct(level)
         out = np.zeros((5, n8))
         if n8:
-            check(lib().emma_hydro_get_level_state(level, ptr(out)), "get_level_state")
+            check(self._L.emma_hydro_get_level_state(level, ptr(out)), "get_level_state")
         return out
 
     def set_state(self, level, st):
         st = np.ascontiguousarray(st, dtype=np.float64)
-        check(lib().emma_hydro_set_level_state(level, ptr(st)), "set_level_state")
+        check(self._L.emma_hydro_set_level_state(level, ptr(st)), "set_level_state")
 
     def set_force(self, level, fx, fy, fz):
         """Gravitational acceleration of the level's cells (gravity=True uploads)."""
         f = np.ascontiguousarray(np.stack([fx, fy, fz]), dtype=np.float64)
-        check(lib().emma_hydro_set_level_force(level, ptr(f)), "set_level_force")
+        check(self._L.emma_hydro_set_level_force(level, ptr(f)), "set_level_force")
 
     def comptstep(self, level):
         dt = ctypes.c_double()
-        check(lib().emma_hydro_comptstep(level, ctypes.byref(dt)), "comptstep")
+        check(self._L.emma_hydro_comptstep(level, ctypes.byref(dt)), "comptstep")
         return dt.value
 
     def clean_new(self, level):
-        check(lib().emma_hydro_clean_new(level), "clean_new")
+        check(self._L.emma_hydro_clean_new(level), "clean_new")
 
     def advance_level(self, level, dt):
-        check(lib().emma_hydro_advance_level(level, dt), "advance_level")
+        check(self._L.emma_hydro_advance_level(level, dt), "advance_level")
 
     def coarse_step(self, dt_param=1e9, time_max=1e9, nsub=2):
         t = ctypes.c_double(self.tsim)
-        check(lib().emma_hydro_advance_coarse_step(dt_param, time_max, nsub, ctypes.byref(t), ptr(self.adt)),
+        check(self._L.emma_hydro_advance_coarse_step(dt_param, time_max, nsub, ctypes.byref(t), ptr(self.adt)),
               "advance_coarse_step")
         self.tsim = t.value
         return self.tsim
 
     def status(self):
-        return lib().emma_hydro_status()
+        return self._L.emma_hydro_status()
 
     def tuning(self, level):
         """Autotuner record of a level: (octs per brick, CTAs per SM, sweep) with
         sweep[shape][ctas-1] the measured ms per launch (0 = not tried)."""
         octs, ctas = ctypes.c_int(), ctypes.c_int()
         sweep = np.zeros(8)
-        rc = lib().emma_hydro_tuning(level, ctypes.byref(octs), ctypes.byref(ctas), ptr(sweep))
+        rc = self._L.emma_hydro_tuning(level, ctypes.byref(octs), ctypes.byref(ctas), ptr(sweep))
         return (octs.value, ctas.value, sweep.reshape(2, 4)) if rc == 0 else None
 
     def download(self):
-        check(lib().emma_hydro_tree_download(self.tree.firstoct), "tree_download")
+        check(self._L.emma_hydro_tree_download(self.tree.firstoct), "tree_download")
 
 
 class CpuInfo(ctypes.Structure):

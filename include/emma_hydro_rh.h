@@ -7,9 +7,11 @@
  * gas as the reference's -DWRADHYD hydro does (face values from the centre's
  * ionised fraction, src/hydro_utils.c:1244-1246; HLLC fluxes du dX/d with the star
  * correction; the ceiling 0 <= dX <= d; fine->coarse corrections; split-cell
- * means).  The tracer build has neither dual energy nor transmissive boundaries
- * (EMMA_ST_ARG), and advances through the drop-in entries only (the resident
- * upload returns EMMA_ST_ARG).
+ * means), and so does its resident mode, where dX is the sixth plane of every
+ * level state on the device (emma_hydro_tree_upload / _download move it with the
+ * tree; emma_hydro_get/set_level_state still exchange the first five planes).
+ * The tracer build has neither dual energy, transmissive boundaries nor gravity
+ * (EMMA_ST_ARG).
  */
 #ifndef EMMA_HYDRO_RH_H
 #define EMMA_HYDRO_RH_H

@@ -114,11 +114,9 @@ def test_tracer_total_is_conserved(gpu):
     assert abs(t.get_tracer(4).sum() - m0) <= 1e-12 * m0
 
 
-def test_tracer_library_refuses_resident_mode_and_dual_energy(gpu):
+def test_tracer_library_refuses_dual_energy(gpu):
     L = lib("rh")
     t = build()
-    L.emma_hydro_clear_status()
-    assert L.emma_hydro_tree_upload(t.firstoct, LC, LMAX, 0) == ST_ARG
     o = EmmaHydroOptions()
     L.emma_hydro_default_options(ctypes.byref(o))
     o.dual_energy = 1
@@ -126,4 +124,33 @@ def test_tracer_library_refuses_resident_mode_and_dual_energy(gpu):
     L.emma_hydro_clear_status()
     H.HydroSolver(LMAX, t.firstoct, 1e-4, grav="rh")
     assert L.emma_hydro_status() & ST_ARG
+    set_precision(PREC_FP64)
+
+
+@pytest.mark.parametrize("precision,nsub,use_graph", [(PREC_FP64, 2, True), (PREC_FP64, 1, False),
+                                                      (PREC_MIXED, 2, True)])
+def test_tracer_resident_coarse_steps(gpu, precision, nsub, use_graph):
+    """Resident tree of the -DWRADHYD layout: whole coarse steps on the GPU (device
+    schedule and graph, or host schedule), dX the sixth plane of every state buffer;
+    against the oracle's Advance_level on an identical tree."""
+    from emma_b200 import ResidentHydro
+    tg, to = build(), build()
+    r = ResidentHydro(tg, precision=precision, cfl=0.8, use_graph=use_graph)
+    for _ in range(2):
+        r.coarse_step(nsub=nsub)
+    assert r.status() == 0
+    r.download()
+    tsim, adt, err = oracle.Restatement(rh=True).run(to.firstoct, LC, LMAX, 2, 0.8, nsub=nsub)
+    assert err == 0
+    for l in range(LC, LMAX + 1):
+        d = to.get_fields(l)[0]
+        leaf = ~to.split_mask(l)
+        if precision == PREC_FP64:
+            assert abs(r.tsim - tsim) <= 1e-14 * tsim
+            e = per_cell_rel(tg.get_fields(l)[:5], to.get_fields(l)[:5])
+            assert e.max() <= 1e-11, (l, e.max())
+            ex = np.abs(tg.get_tracer(l) - to.get_tracer(l))[leaf] / d[leaf]
+            assert ex.max() <= 1e-11, (l, ex.max())
+        else:
+            assert l1_rel(tg.get_tracer(l)[leaf], to.get_tracer(l)[leaf]) <= 1e-5, l
     set_precision(PREC_FP64)
