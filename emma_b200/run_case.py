@@ -2,6 +2,7 @@
 
     python -m emma_b200.run_case --config random --level 6 --precision mixed --steps 3
     python -m emma_b200.run_case --config turb --level 7 --precision fp64 --steps 2 --dropin rh
+    python -m emma_b200.run_case --config turb --level 7 --precision mixed --steps 4 --tracer
 
 Used to profile one configuration in isolation (for example under ncu).  --dropin
 runs the drop-in clean_new_hydro + HydroSolver on the finest level of the host tree
@@ -22,17 +23,25 @@ def main():
     ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"])
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--dropin", default=None, choices=["plain", "rh"])
+    ap.add_argument("--tracer", action="store_true", help="resident run of the -DWRADHYD library (dX = d/2)")
     a = ap.parse_args()
     cfg = {"random": lambda: configs.random_uniform(level=a.level), "turb": lambda: configs.turb(level=a.level),
            "sod": lambda: configs.sod(level=a.level), "sedov": configs.sedov, "cosmo": configs.cosmo,
            "amr": configs.small_amr}[a.config]()
     if a.dropin is not None:
         return dropin(a, cfg)
-    tree = cfg.build()
+    if a.tracer:
+        from .tree import OctTree
+        tree = cfg.build(lambda lc, lm: OctTree(lc, lm, rh=True))
+        for lev in range(cfg.lcoarse, cfg.lmax + 1):
+            if tree.noct(lev):
+                tree.set_tracer(lev, 0.5 * tree.get_fields(lev, 0)[0])
+    else:
+        tree = cfg.build()
     # host-driven schedule: every level-kernel launch is timed with CUDA events
     r = ResidentHydro(tree, precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64, trans=cfg.trans,
                       cfl=cfg.cfl, use_graph=False)
-    L = lib()
+    L = lib("rh" if a.tracer else False)
     per_step = []
     tot_ms, tot_n, tot_cells = 0.0, 0, 0
     for _ in range(a.steps):
