@@ -25,6 +25,7 @@ REF_LIB_TX = os.path.join(HERE, "_ref", "libemmaref_tx.so")
 REF_LIB_GRAV = os.path.join(HERE, "_ref", "libemmaref_grav.so")
 REF_LIB_DUAL = os.path.join(HERE, "_ref", "libemmaref_dual.so")
 REF_LIB_RH = os.path.join(HERE, "_ref", "libemmaref_rh.so")
+REF_LIB_SP = os.path.join(HERE, "_ref", "libemmaref_sp.so")
 
 HYDROTEST = 0x40
 DUAL_E = 0x80
@@ -157,14 +158,16 @@ class GravClone:
             self.h = None
 
 
-def _ref_path(tx=False, grav=False, dual=False, rh=False):
+def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False):
+    if sp:
+        return REF_LIB_SP
     if rh:
         return REF_LIB_RH
     return REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
 
 
-def ref_available(tx=False, grav=False, dual=False, rh=False):
-    return os.path.exists(_ref_path(tx, grav, dual, rh))
+def ref_available(tx=False, grav=False, dual=False, rh=False, sp=False):
+    return os.path.exists(_ref_path(tx, grav, dual, rh, sp))
 
 
 class RefTree:
@@ -172,9 +175,11 @@ class RefTree:
 
     _libs = {}
 
-    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False, dual=False, rh=False):
-        assert (tx + grav + dual + rh) <= 1, "one build variant at a time"
-        path = _ref_path(tx, grav, dual, rh)
+    def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False, dual=False, rh=False,
+                 sp=False):
+        """sp: the reference built with -DSINGLEPRECISION (REAL = float)."""
+        assert (tx + grav + dual + rh + sp) <= 1, "one build variant at a time"
+        path = _ref_path(tx, grav, dual, rh, sp)
         if path not in RefTree._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"reference oracle not built: {path}")
