@@ -260,19 +260,29 @@ def _golden_cases():
 
 @pytest.mark.parametrize("name", _golden_cases())
 def test_restatement_reproduces_golden(name):
+    """The reference's outputs committed as fixtures, reproduced bit for bit by the
+    restatement of the same build variant (default, -DDUAL_E, -DWGRAV, -DWRADHYD)."""
     g = np.load(os.path.join(GOLDEN, name))
     base, lmax, nsteps, trans = (int(x) for x in g["meta"][:4])
+    variant = int(g["meta"][4]) if len(g["meta"]) > 4 else 0
     radii = tuple(g["radii"])
-    t = OctTree(base, lmax)
+    t = OctTree(base, lmax, grav=variant == 2, rh=variant == 3)
     for i, r in enumerate(radii):
         t.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
     for l in range(base, lmax + 1):
         t.set_fields(l, *g[f"in_{l}"][:5])
-    tsim, adt, err = oracle.Restatement().run(t.firstoct, base, lmax, nsteps, 0.8, trans=trans)
+        if variant == 2:
+            t.set_force(l, *g[f"in_f_{l}"])
+        if variant == 3:
+            t.set_tracer(l, g[f"in_x_{l}"])
+    R = oracle.Restatement(grav=variant == 2, rh=variant == 3)
+    tsim, adt, err = R.run(t.firstoct, base, lmax, nsteps, 0.8, trans=trans, dual=variant == 1)
     assert err == 0
     assert tsim == float(g["tsim"])
     for l in range(base, lmax + 1):
         assert np.array_equal(t.get_fields(l, 0), g[f"out_{l}"]), f"level {l}"
+        if variant == 3:
+            assert np.array_equal(t.get_tracer(l, 0), g[f"out_x_{l}"]), f"dX, level {l}"
 
 
 @needs_ref
