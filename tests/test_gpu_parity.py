@@ -195,14 +195,23 @@ def _golden_cases():
 
 @pytest.mark.parametrize("name", _golden_cases())
 def test_gpu_reproduces_golden(gpu, name):
+    """The reference's own outputs (tests/golden) from the resident GPU path of the
+    same build variant: default, -DDUAL_E (option), -DWGRAV (the fixture's forces
+    uploaded per level) and -DWRADHYD (a tree of that layout, dX compared too)."""
     g = np.load(os.path.join(GOLDEN, name))
     base, lmax, nsteps, trans = (int(x) for x in g["meta"][:4])
-    t = OctTree(base, lmax)
+    variant = int(g["meta"][4]) if len(g["meta"]) > 4 else 0
+    t = OctTree(base, lmax, rh=variant == 3)
     for i, rr in enumerate(tuple(g["radii"])):
         t.refine_where(base + i, lambda c, rr=rr: np.linalg.norm(c - 0.5, axis=1) < rr)
     for l in range(base, lmax + 1):
         t.set_fields(l, *g[f"in_{l}"][:5])
-    r = ResidentHydro(t, precision=PREC_FP64, trans=trans, cfl=CFL)
+        if variant == 3:
+            t.set_tracer(l, g[f"in_x_{l}"])
+    r = ResidentHydro(t, precision=PREC_FP64, trans=trans, cfl=CFL, gravity=variant == 2, dual=variant == 1)
+    if variant == 2:
+        for l in range(base, lmax + 1):
+            r.set_force(l, *g[f"in_f_{l}"])
     for _ in range(nsteps):
         r.coarse_step()
     assert r.status() == 0
@@ -210,6 +219,10 @@ def test_gpu_reproduces_golden(gpu, name):
     for l in range(base, lmax + 1):
         e = per_cell_rel(t.get_fields(l)[:5], g[f"out_{l}"][:5])
         assert e.max() <= 1e-11, (l, e.max())
+        if variant == 3:
+            d = g[f"out_{l}"][0]
+            leaf = ~t.split_mask(l)
+            assert (np.abs(t.get_tracer(l) - g[f"out_x_{l}"])[leaf] / d[leaf]).max() <= 1e-11, l
 
 
 def _final_states(cfg, nsteps, nsub, use_graph, precision=PREC_FP64):
