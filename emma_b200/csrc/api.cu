@@ -15,6 +15,7 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <pthread.h>
 #include <vector>
 #include "emma_hydro.h"
 #ifdef EMMA_WGRAV
@@ -264,15 +265,24 @@ class HostPool {
 
 // Host threads of the parallel passes: EMMA_HYDRO_HOST_THREADS if set, else the
 // hardware threads, at most kMaxHostThreads (and kDefaultHostThreads by default).
+// A child process forked after the pool started has none of its workers: it
+// starts a pool of its own (the parent's pool object is abandoned in the child).
+std::atomic<bool> g_pool_forked{false};
 HostPool &host_pool() {
-  static HostPool *pool = [] {
+  static HostPool *pool = nullptr;
+  static bool atfork = false;
+  if (pool == nullptr || g_pool_forked.exchange(false)) {
+    if (!atfork) {
+      pthread_atfork(nullptr, nullptr, [] { g_pool_forked = true; });
+      atfork = true;
+    }
     unsigned n = std::min(kDefaultHostThreads, std::max(1u, std::thread::hardware_concurrency()));
     if (const char *e = std::getenv("EMMA_HYDRO_HOST_THREADS")) {
       const long v = std::strtol(e, nullptr, 10);
       if (v >= 1) n = (unsigned)std::min<long>(v, (long)kMaxHostThreads);
     }
-    return new HostPool(n);
-  }();
+    pool = new HostPool(n);
+  }
   return *pool;
 }
 
