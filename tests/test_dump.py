@@ -85,6 +85,22 @@ def test_dump_gravity_layout(tmp_path):
     assert np.any(f0 != 0.0)
 
 
+def test_dump_tracer_layout(tmp_path):
+    """libemmahydro_rh.so reads the 152-byte cells of the -DWRADHYD layout."""
+    t = OctTree(4, 5, rh=True)
+    t.refine_where(4, lambda c: np.linalg.norm(c - 0.5, axis=1) < 0.3)
+    random_fields(t, (4, 5))
+    ids, names = [f[0] for f in FIELDS], [f[1] for f in FIELDS]
+    a, b = str(tmp_path / "lib") + "/", str(tmp_path / "orc") + "/"
+    os.makedirs(a)
+    os.makedirs(b)
+    assert H.dump_alloct(a, t.firstoct, 4, 5, ids, names, grav="rh") == 0
+    assert oracle.Restatement(rh=True).dump_alloct(b, t.firstoct, 4, 5, ids, names) == 0
+    for name in names:
+        rel = f"grid_{name}/{name}.00000.p00000"
+        assert open(a + rel, "rb").read() == open(b + rel, "rb").read(), name
+
+
 def test_dump_refuses_unknown_ids(tmp_path):
     t = configs.small_amr(base=3, radii=(0.3,)).build()
     d = str(tmp_path) + "/"

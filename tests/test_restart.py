@@ -18,8 +18,8 @@ needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref n
 UNITS = np.array([3.1e24, 2.9e7, 1.1e17, 6.0e-1, 2.0e42, 1.7e-29, 1.0e0])
 
 
-def _ref_tree():
-    ref = oracle.RefTree(4, 6, ngridmax=sum(8 ** (l - 1) for l in range(1, 7)))
+def _ref_tree(rh=False):
+    ref = oracle.RefTree(4, 6, ngridmax=sum(8 ** (l - 1) for l in range(1, 7)), rh=rh)
     for i, r in enumerate((0.3, 0.15)):
         ref.refine_where(4 + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
     rng = np.random.default_rng(7)
@@ -27,6 +27,8 @@ def _ref_tree():
         n8 = 8 * ref.noct(l)
         ref.set_fields(l, rng.uniform(0.5, 1.5, n8), *(rng.uniform(-0.5, 0.5, n8) for _ in range(3)),
                        rng.uniform(0.5, 1.5, n8))
+        if rh:
+            ref.set_tracer(l, ref.get_fields(l, 0)[0] * rng.uniform(0.0, 1.0, n8))
     ref.run(2)
     return ref
 
@@ -51,6 +53,20 @@ def test_save_amr_is_byte_identical(tmp_path):
     ref.save_amr(fa, 0.0123, 0.001, 17, 3, UNITS)
     rc = lib().emma_hydro_save_amr(fb.encode(), ref.firstoct, 0.0123, 0.001, 17, 3, 4, 6,
                                    ctypes.c_void_p(adt.ctypes.data), ctypes.c_void_p(UNITS.ctypes.data), None)
+    assert rc == 0
+    a, b = open(fa, "rb").read(), open(fb, "rb").read()
+    assert len(a) == len(b) and a == b
+
+
+@pytest.mark.skipif(not oracle.ref_available(rh=True), reason="oracle/_ref -DWRADHYD build absent")
+def test_save_amr_tracer_layout_is_byte_identical(tmp_path):
+    """libemmahydro_rh.so writes the reference's -DWRADHYD checkpoint (1328-byte octs) byte for byte."""
+    ref = _ref_tree(rh=True)
+    adt = np.array([ref.L.ref_adt(l) for l in range(1, 7)])
+    fa, fb = str(tmp_path / "ref.bin"), str(tmp_path / "lib.bin")
+    ref.save_amr(fa, 0.0123, 0.001, 17, 3, UNITS)
+    rc = lib("rh").emma_hydro_save_amr(fb.encode(), ref.firstoct, 0.0123, 0.001, 17, 3, 4, 6,
+                                       ctypes.c_void_p(adt.ctypes.data), ctypes.c_void_p(UNITS.ctypes.data), None)
     assert rc == 0
     a, b = open(fa, "rb").read(), open(fb, "rb").read()
     assert len(a) == len(b) and a == b
