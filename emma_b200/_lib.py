@@ -103,6 +103,7 @@ GRAV_SIGNATURES = [
 RH_SIGNATURES = [
     ("emma_tree_set_tracer", None, [c_void_p, c_int, c_void_p]),
     ("emma_tree_get_tracer", None, [c_void_p, c_int, c_int, c_void_p]),
+    ("emma_tree_put_tracer", None, [c_void_p, c_int, c_int, c_void_p]),
 ]
 
 

@@ -240,6 +240,12 @@ void emma_tree_set_tracer(struct EmmaTree *t, int level, const double *dX) {
     for (int c = 0; c < 8; c++) o->cell[c].field.dX = o->cell[c].fieldnew.dX = dX[8 * i + c];
 }
 
+void emma_tree_put_tracer(struct EmmaTree *t, int level, int which, const double *dX) {
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) (which ? o->cell[c].fieldnew : o->cell[c].field).dX = dX[8 * i + c];
+}
+
 void emma_tree_get_tracer(struct EmmaTree *t, int level, int which, double *out) {
   long long i = 0;
   for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)

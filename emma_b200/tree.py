@@ -86,6 +86,13 @@ class OctTree:
         assert a.size == 8 * self.noct(level)
         self._L.emma_tree_set_tracer(self._t, level, ptr(a))
 
+    def put_tracer(self, level, dX, which=0):
+        """dX of `field` (which=0) or `fieldnew` (which=1) only (rh trees)."""
+        assert self.rh, "only the -DWRADHYD layout has dX"
+        a = np.ascontiguousarray(dX, dtype=np.float64)
+        assert a.size == 8 * self.noct(level)
+        self._L.emma_tree_put_tracer(self._t, level, which, ptr(a))
+
     def get_tracer(self, level, which=0):
         assert self.rh, "only the -DWRADHYD layout has dX"
         out = np.zeros(8 * self.noct(level))

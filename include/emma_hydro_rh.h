@@ -30,6 +30,8 @@ extern "C" {
  * 8*noct), and dX of field (which=0) or fieldnew (which=1) read back. */
 void emma_tree_set_tracer(struct EmmaTree *t, int level, const double *dX);
 void emma_tree_get_tracer(struct EmmaTree *t, int level, int which, double *out);
+/* dX of field (which=0) or fieldnew (which=1) only. */
+void emma_tree_put_tracer(struct EmmaTree *t, int level, int which, const double *dX);
 
 #ifdef __cplusplus
 }

@@ -36,12 +36,19 @@ DEFDENS = 10.0  # U2W's stand-in density for an empty cell (src/hydro_utils.c:38
 
 
 def build(grav=False):
-    t = OctTree(LC, LMAX, grav=grav)
+    """grav: True (-DWGRAV layout with forces) or "rh" (-DWRADHYD layout with an ionised fraction)."""
+    rh = grav == "rh"
+    t = OctTree(LC, LMAX, grav=(grav is True), rh=rh)
     for i, rad in enumerate((0.3, 0.15)):
         t.refine_where(LC + i, lambda c, rad=rad: np.linalg.norm(c - 0.5, axis=1) < rad)
     random_fields(t, range(LC, LMAX + 1))
-    if grav:
+    if grav is True:
         random_forces(t, range(LC, LMAX + 1))
+    if rh:
+        rng = np.random.default_rng(99)
+        for l in range(LC, LMAX + 1):
+            d = t.get_fields(l, 0)[0]
+            t.set_tracer(l, d * rng.uniform(0.0, 1.0, d.size))
     return t
 
 
@@ -92,6 +99,14 @@ def exchange_fields(trees, owner):
                     m = cell_owner == q
                     w[:, m] = src[q][:, m]
             t.put_fields(l, w)
+        if trees[0].rh:
+            xs = [t.get_tracer(l, 0) for t in trees]
+            for r, t in enumerate(trees):
+                x = xs[r].copy()
+                for q in range(len(trees)):
+                    if q != r:
+                        x[cell_owner == q] = xs[q][cell_owner == q]
+                t.put_tracer(l, x, which=0)
 
 
 def hydro_correct(trees, owner, level, dual):
@@ -100,19 +115,25 @@ def hydro_correct(trees, owner, level, dual):
     lc = level - 1
     cell_owner = np.repeat(owner[lc], 8)
     fnew = [t.get_fields(lc, 1) for t in trees]
+    rh = trees[0].rh
+    xnew = [t.get_tracer(lc, 1) if rh else np.zeros(fnew[0].shape[1]) for t in trees]  # U.dX = W.dX
     out = [f.copy() for f in fnew]
+    xout = [x.copy() for x in xnew]
     sent = 0
     for r in range(len(trees)):
         for q in range(len(trees)):
             if q == r:
                 continue
-            m = (cell_owner == q) & np.any(fnew[r] != 0.0, axis=0)
+            m = (cell_owner == q) & (np.any(fnew[r] != 0.0, axis=0) | (xnew[r] != 0.0))
             if m.any():
                 U = w2u(out[q][:, m], dual) + w2u(fnew[r][:, m], dual)
                 out[q][:, m] = u2w(U, dual)
+                xout[q][m] = xout[q][m] + xnew[r][m]
                 sent += int(m.sum())
     for q, t in enumerate(trees):
         t.put_fields(lc, out[q], which=1)
+        if rh:
+            t.put_tracer(lc, xout[q], which=1)
     return sent
 
 
@@ -135,7 +156,7 @@ def run_ranks(part, grav=False, dual=False, fn=None):
         exchange_fields(trees, owner)
         for r, t in enumerate(trees):
             H.HydroSolver(l, t.firstoct, DTS[l], cpu=cpus[r], grav=grav)
-            if grav:
+            if grav is True:
                 H.grav_correction(l, t.firstoct, DTS[l], cpu=cpus[r])
         assert L.emma_hydro_status() == 0, L.emma_hydro_last_error()
         if l > LC:
@@ -146,13 +167,13 @@ def run_ranks(part, grav=False, dual=False, fn=None):
 
 def run_single(grav=False, dual=False):
     t = build(grav)
-    R = oracle.Restatement(grav=grav)
+    R = oracle.Restatement(grav=(grav is True), rh=(grav == "rh"))
     for op, l in advance_order():
         if op == "clean":
             R.clean_new(t.firstoct, l)
         else:
             assert R.hydro_solver(t.firstoct, l, DTS[l], dual=dual) == 0
-            if grav:
+            if grav is True:
                 assert R.grav_correction(t.firstoct, l, DTS[l]) == 0
     return t
 
@@ -166,6 +187,9 @@ def check_owned(trees, owner, ref, tol=1e-12):
             if m.any():
                 e = per_cell_rel(t.get_fields(l)[:5][:, m], o[:, m])
                 assert e.max() <= tol, (l, r, e.max())
+                if getattr(ref, "rh", False):
+                    ex = np.abs(t.get_tracer(l)[m] - ref.get_tracer(l)[m]) / o[0][m]
+                    assert ex.max() <= tol, (l, r, "dX", ex.max())
 
 
 @pytest.mark.parametrize("part", ["slabs", "quadrants", "stripes3"])
@@ -178,6 +202,12 @@ def test_multi_rank_dropin_gravity(gpu):
     """-DWGRAV layout: grav_correction of each rank's own leaves after its solve."""
     trees, owner = run_ranks("quadrants", grav=True)
     check_owned(trees, owner, run_single(grav=True))
+
+
+def test_multi_rank_dropin_tracer(gpu):
+    """-DWRADHYD layout: dX exchanged with the fields, its corrections sent like theirs."""
+    trees, owner = run_ranks("quadrants", grav="rh")
+    check_owned(trees, owner, run_single(grav="rh"))
 
 
 def test_multi_rank_dropin_dual_energy(gpu):
