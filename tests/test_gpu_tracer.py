@@ -6,7 +6,8 @@ random ionised fraction; the oracle (oracle/hydro_oracle.c built with
 -DORC_WRADHYD, pinned bit for bit to the reference's -DWRADHYD hydro in
 tests/test_oracle_pin.py) runs the same calls on an identical tree.  FP64:
 per-cell relative error <= 1e-12 on d,u,v,w,p and |dX - dX_ref| <= 1e-12 d;
-mixed: L1 <= 1e-5.
+mixed: L1 <= 1e-5.  The resident mode of the same library (dX the sixth plane of
+every state buffer) runs whole coarse steps against the oracle's Advance_level.
 """
 import ctypes
 
