@@ -331,81 +331,95 @@ def run_dropin(args, L, cfg, tree, levels, dts, world):
             "status": L.emma_hydro_status()}
 
 
-def cpu_baseline_sample(config):
-    """The reference's own CPU hydro on a bounded sample of the configuration."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    from emma_b200 import configs
-    if not oracle.ref_available(tx=(config == "sod")):
-        return None
-    if config in ("turb",):
-        cfg, sample = configs.turb(level=6), "one level-6 step of the turbulent box generator (64^3, 262,144 cell-updates)"
-    elif config == "roofline":
-        cfg, sample = configs.random_uniform(level=6), "one level-6 step of the uniform random box (64^3, 262,144 cell-updates)"
-    elif config == "sod":
-        cfg, sample = configs.sod(level=6), "one step of the 64^3 Sod tube (262,144 cell-updates)"
-    else:
-        cfg, sample = configs.sedov(), "one coarse step of the Sedov tree (all levels, subcycled)"
+# Reference samples: the reference's own CPU hydro on the configuration's own tree at
+# its full size.  A uniform level is sampled as a prefix of its oct list (stock
+# clean_new_hydro + HydroSolver on the first REF_SAMPLE_OCTS octs, the rest of the
+# tree in place as their neighbours); an AMR tree runs whole coarse steps.
+REF_SAMPLE_OCTS = 65536
+
+
+def _quiet(fn):
+    """Run fn with the reference's stdout prints silenced."""
     saved = os.dup(1)
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
     try:
-        # room for every oct plus the reference's free-oct chain head (src/emma.c:765)
-        ngrid = sum(8 ** (l - 1) for l in range(1, cfg.lmax + 1)) + 1024
-        ref = oracle.RefTree(cfg.lcoarse, cfg.lmax, tx=(config == "sod"), ngridmax=ngrid)
-        cfg.build(lambda lc, lm: ref)  # the configuration's own generator, on the reference's tree
-        ref.reset_counters()
-        ref.run(1, nsub=cfg.nsub)
-        secs, cells = ref.hydro_seconds(), ref.cell_updates()
+        return fn()
     finally:
         os.dup2(saved, 1)
         os.close(saved)
         os.close(devnull)
-    return {"value": cells / secs, "unit": "cell-updates/s", "cores": 1, "kind": "reference", "sample": sample,
-            "seconds": secs}
+
+
+def reference_tree(config):
+    """The configuration's tree built and filled by the reference (oracle/_ref), or None."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    cfg = build_config(config)
+    tx = bool(cfg.trans)
+    if not oracle.ref_available(tx=tx):
+        return cfg, None
+    # room for every oct plus the reference's free-oct chain head (src/emma.c:765)
+    ngrid = sum(8 ** (l - 1) for l in range(1, cfg.lmax + 1)) + 1024
+    if cfg.lmax > cfg.lcoarse:
+        ngrid = sum(8 ** (l - 1) for l in range(1, cfg.lcoarse + 1)) + 2 * 10 ** 6
+    ref = _quiet(lambda: oracle.RefTree(cfg.lcoarse, cfg.lmax, tx=tx, ngridmax=ngrid))
+    _quiet(lambda: cfg.build(lambda lc, lm: ref))  # the configuration's own generator, on the reference's tree
+    return cfg, ref
+
+
+def reference_steps(cfg, ref, nsteps):
+    """nsteps samples; returns (seconds inside HydroSolver, cell-updates, sample text)."""
+    ref.reset_counters()
+    if cfg.lmax == cfg.lcoarse:
+        n = min(REF_SAMPLE_OCTS, ref.noct(cfg.lcoarse))
+        for _ in range(nsteps):
+            _quiet(lambda: ref.hydro_solver_prefix(cfg.lcoarse, n))
+        sample = (f"clean_new_hydro + HydroSolver on the first {n:,} octs ({8 * n:,} cells) of the "
+                  f"{8 * ref.noct(cfg.lcoarse):,}-cell level-{cfg.lcoarse} list of the full-size tree, per step")
+    else:
+        _quiet(lambda: ref.run(nsteps, nsub=cfg.nsub))
+        sample = "whole coarse steps (all levels, subcycled) of the full-size tree"
+    return ref.hydro_seconds(), ref.cell_updates(), sample
+
+
+def cpu_baseline_sample(config, nsteps=3):
+    """The reference's own CPU hydro on a bounded sample of the same workload."""
+    cfg, ref = reference_tree(config)
+    if ref is None:
+        return None
+    secs, cells, sample = reference_steps(cfg, ref, 1 if cfg.lmax > cfg.lcoarse else nsteps)
+    return {"value": cells / secs, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
+            "sample": f"{cfg.name}: {sample}, {1 if cfg.lmax > cfg.lcoarse else nsteps} step(s)", "seconds": secs}
 
 
 def run_reference(args):
-    """--impl reference: the reference's CPU hydro, each step a bounded sample."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-    from emma_b200 import configs
-    cfgname = args.config
-    tx = cfgname == "sod"
+    """--impl reference: the reference's CPU hydro on the same configuration at its
+    full size, each step a bounded sample (see reference_steps)."""
     line = {"impl": "reference", "metric": METRIC, "unit": "cell-updates/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True}
-    if not oracle.ref_available(tx=tx):
+    t0 = time.time()
+    cfg, ref = reference_tree(args.config)
+    if ref is None:
         line["unavailable"] = "oracle/_ref (the reference CPU hydro compiled from its sources) is not built"
         print(json.dumps(line))
         return
-    level = 6
-    cfg = configs.turb(level=level) if cfgname == "turb" else configs.random_uniform(level=level)
-    saved = os.dup(1)
-    devnull = os.open(os.devnull, os.O_WRONLY)
-    os.dup2(devnull, 1)
-    try:
-        ref = oracle.RefTree(level, level, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, level + 1)) + 16)
-        cfg.build(lambda lc, lm: ref)  # same generator as the configuration, at the sample's size
-        for _ in range(args.warmup):
-            ref.run(1)
-        ref.reset_counters()
-        t0 = time.time()
-        ref.run(args.steps)
-        wall = time.time() - t0
-        secs, cells = ref.hydro_seconds(), ref.cell_updates()
-    finally:
-        os.dup2(saved, 1)
-        os.close(saved)
-        os.close(devnull)
+    build_s = time.time() - t0
+    if args.warmup:
+        reference_steps(cfg, ref, args.warmup)
+    t0 = time.time()
+    secs, cells, sample = reference_steps(cfg, ref, args.steps)
+    wall = time.time() - t0
     v = cells / secs
-    sample = f"each step: one level-{level} step of the {cfgname} generator ({2 ** level}^3 = {8 ** level} cell-updates), 1 core"
+    leaf = sum(int(8 * ref.noct(l)) for l in range(cfg.lcoarse, cfg.lmax + 1))
     line.update({"value": v, "ms_per_step": 1000 * secs / max(args.steps, 1), "scaling": "weak",
                  "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-                 "config": {"workload": f"{cfgname} (reference CPU sample at level {level})", "cells": 8 ** level},
+                 "config": {"workload": cfg.name, "levels": [cfg.lcoarse, cfg.lmax], "tree_cells": leaf,
+                            "sample": sample, "cells_per_step": cells // max(args.steps, 1)},
                  "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "reference",
-                                  "sample": sample},
+                                  "sample": f"{sample}; single-threaded like the reference's hydro"},
                  "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-                 "wall_s": wall})
+                 "wall_s": wall, "tree_build_s": build_s})
     print(json.dumps(line))
 
 
@@ -414,7 +428,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--config", default="turb", choices=["turb", "roofline", "sod", "sedov", "cosmo"])
+    ap.add_argument("--config", default="roofline", choices=["turb", "roofline", "sod", "sedov", "cosmo"])
     ap.add_argument("--impl", default="mine", choices=["mine", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--gravity", action="store_true",

@@ -64,6 +64,7 @@ SIGNATURES = [
     ("emma_hydro_set_level_state", c_int, [c_int, c_void_p]),
     ("emma_hydro_set_level_force", c_int, [c_int, c_void_p]),
     ("emma_hydro_is_resident", c_int, [c_void_p]),
+    ("emma_hydro_tree_release", c_int, [c_void_p]),
     ("emma_hydro_dump_alloct", c_int, [ctypes.c_char_p, c_void_p, c_int, c_int, c_int, c_int, c_double, c_int,
                                        c_void_p, c_void_p]),
     ("emma_hydro_save_amr", c_int, [ctypes.c_char_p, c_void_p, c_double, c_double, c_int, c_int, c_int, c_int,
@@ -80,6 +81,7 @@ SIGNATURES = [
     ("emma_hydro_probe_wait_timeout", c_int, [c_ll]),
     ("emma_hydro_plan_stats", c_int, [c_void_p, c_int, c_int, c_int, c_void_p]),
     ("emma_hydro_level_dt_noalloc", c_int, [c_void_p, c_ll, c_int, c_double, c_void_p, P(c_double)]),
+    ("emma_hydro_noalloc_forget", None, []),
     ("emma_tree_create", c_void_p, [c_int, c_int, c_ll]),
     ("emma_tree_destroy", None, [c_void_p]),
     ("emma_tree_refine", c_int, [c_void_p, c_int, c_void_p]),

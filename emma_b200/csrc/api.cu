@@ -1110,6 +1110,18 @@ int emma_hydro_is_resident(struct OCT **firstoct) {
   return (g.ready && g.res.valid && firstoct != nullptr && g.res_first == firstoct) ? 1 : 0;
 }
 
+int emma_hydro_tree_release(struct OCT **firstoct) {
+  if (!emma_hydro_is_resident(firstoct)) return 0;
+  const cudaError_t e = cudaStreamSynchronize(g.stream);
+  drop_graph();
+  free_tree(g.res);
+  cudaFree(g.d_work_all);
+  g.d_work_all = nullptr;
+  g.nwork_all = 0;
+  g.res_first = nullptr;
+  return e == cudaSuccess ? 0 : EMMA_ST_CUDA;
+}
+
 int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int rank) {
   if (!g.ready && emma_hydro_init(nullptr) != 0) return EMMA_ST_CUDA;
   if (kDropinTracer && (g.opt.dual_energy || g.opt.trans_flags || g.opt.gravity)) {

@@ -51,11 +51,14 @@ struct Planes {
 // [off[oct], off[oct+1]) (split bits that disagree with the offsets) is skipped.
 __global__ void alloct_gather_kernel(const double *__restrict__ W, long long n8, const uint8_t *__restrict__ split,
                                      const int *__restrict__ off, int all, Planes pl, float *__restrict__ out,
-                                     long long nd) {
+                                     long long nd, int *__restrict__ bad) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n8; i += (long long)gridDim.x * blockDim.x) {
     const long long o = i >> 3;
     const unsigned c = (unsigned)(i & 7);
     const unsigned sp = all ? 0u : (unsigned)split[o];
+    // the host's per-oct counts come from the tree's child pointers, the cells picked
+    // here from the device's split bits: a tree refined after its upload disagrees
+    if (c == 0 && __popc(~sp & 0xffu) != off[o + 1] - off[o]) atomicAdd(bad, 1);
     if ((sp >> c) & 1u) continue;
     const long long j = off[o] + __popc(~sp & ((1u << c) - 1u));
     if (j >= off[o + 1]) continue;
@@ -233,22 +236,33 @@ extern "C" int emma_hydro_dump_alloct(const char *folder, struct OCT **firstoct,
         S.release();
         S.device = dev;
       }
-      const size_t ob = sizeof(int) * (octs.size() + 1), vb = sizeof(float) * (size_t)pl.n * nd;
+      // offsets, then one counter of octs whose device split bits disagree with the host tree
+      const size_t ob = sizeof(int) * (octs.size() + 2), vb = sizeof(float) * (size_t)pl.n * nd;
       bool ok = grow(reinterpret_cast<void **>(&S.d_off), &S.off_bytes, ob, false) &&
                 grow(reinterpret_cast<void **>(&S.d_out), &S.out_bytes, vb, false) &&
                 grow(reinterpret_cast<void **>(&S.pin), &S.pin_bytes, vb, true);
       const long long n8 = 8LL * (long long)octs.size();
       const int grid = std::max(1, std::min((int)((n8 + 255) / 256), 8 * std::max(nsm, 1)));
-      ok = ok && cudaMemcpyAsync(S.d_off, off.data(), ob, cudaMemcpyHostToDevice, stream) == cudaSuccess;
+      int *d_bad = S.d_off + octs.size() + 1;
+      int nbad = 0;
+      ok = ok &&
+           cudaMemcpyAsync(S.d_off, off.data(), sizeof(int) * (octs.size() + 1), cudaMemcpyHostToDevice, stream) ==
+               cudaSuccess &&
+           cudaMemsetAsync(d_bad, 0, sizeof(int), stream) == cudaSuccess;
       if (ok) {
         alloct_gather_kernel<<<grid, 256, 0, stream>>>(W, n8, split, S.d_off, level == lmax ? 1 : 0, pl, S.d_out,
-                                                       nd);
+                                                       nd, d_bad);
         ok = cudaGetLastError() == cudaSuccess;
       }
       ok = ok && cudaMemcpyAsync(S.pin, S.d_out, vb, cudaMemcpyDeviceToHost, stream) == cudaSuccess &&
+           cudaMemcpyAsync(&nbad, d_bad, sizeof(int), cudaMemcpyDeviceToHost, stream) == cudaSuccess &&
            cudaStreamSynchronize(stream) == cudaSuccess;
       if (!ok) {
         rc = EMMA_ST_CUDA;
+        break;
+      }
+      if (nbad != 0) {  // refined or coarsened since the upload: upload the tree again
+        rc = EMMA_ST_TREE;
         break;
       }
       for (int i = 0; i < nfields; i++)

@@ -1088,15 +1088,25 @@ namespace {
 // above the occupancy limit: the limit), so that every CTA is co-resident.
 template <class M, unsigned SHAPES, bool GRAV, bool DUAL, bool TRACER = false>
 cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cudaStream_t s, int *occupancy) {
-  static int occ = 0;
+  // per device: the shared-memory limit is a per-device function attribute, and the
+  // co-residency of the persistent grid rests on that device's own occupancy
+  constexpr int kMaxDev = 64;
+  static int occ_dev[kMaxDev] = {0};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  int &occ = occ_dev[dev];
   auto k = level_batch_kernel<M, SHAPES, GRAV, DUAL, TRACER>;
   constexpr size_t bytes = level_smem_bytes<M, DUAL, TRACER>(SHAPES);
   if (occ == 0) {
-    cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k, kThreads, bytes);
+    int o = 0;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, k, kThreads, bytes);
     if (e != cudaSuccess) return e;
-    if (occ < 1) return cudaErrorInvalidConfiguration;
+    if (o < 1) return cudaErrorInvalidConfiguration;
+    occ = o;
   }
   if (occupancy != nullptr) *occupancy = occ;
   if (a.nwork == 0) return cudaSuccess;

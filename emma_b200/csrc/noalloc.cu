@@ -20,10 +20,16 @@
 // Host code only ever uses the array's device address, obtained once per device
 // with cudaGetSymbolAddress on the first call made while that device is
 // current; that first call must therefore not be made during a stream capture.
+// The address is cached for the life of the device's primary context: after a
+// cudaDeviceReset (which unloads this library's module) call
+// emma_hydro_noalloc_forget() before the next call, so that the address is
+// looked up again in the new context.  The per-device cache slots are atomic, so
+// host threads may make first calls concurrently.
 //
 // Built with -fmad=false: the signal speed rounds exactly as the reference's
 // L_comptstep_hydro (src/advanceamr.c:122-135) and emma_hydro_comptstep do.
 #include <cuda_runtime.h>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -40,7 +46,7 @@ constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned long long g_dt_scratch[kMaxBlocks + 1];
 
-unsigned long long *g_scratch_addr[kMaxDevices] = {nullptr};
+std::atomic<unsigned long long *> g_scratch_addr[kMaxDevices];  // zero-initialised (static storage)
 
 __device__ __forceinline__ double block_max(double m) {
   __shared__ double part[kThreads / 32];
@@ -95,12 +101,13 @@ extern "C" int emma_hydro_level_dt_noalloc(const double *d_state, long long ncel
   }
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return EMMA_ST_CUDA;
-  if (g_scratch_addr[dev] == nullptr) {
+  unsigned long long *scratch = g_scratch_addr[dev].load(std::memory_order_acquire);
+  if (scratch == nullptr) {
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_dt_scratch) != cudaSuccess || p == nullptr) return EMMA_ST_CUDA;
-    g_scratch_addr[dev] = static_cast<unsigned long long *>(p);
+    scratch = static_cast<unsigned long long *>(p);
+    g_scratch_addr[dev].store(scratch, std::memory_order_release);
   }
-  unsigned long long *scratch = g_scratch_addr[dev];
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   double smax = 0.;
   if (ncells > 0) {
@@ -120,4 +127,8 @@ extern "C" int emma_hydro_level_dt_noalloc(const double *d_state, long long ncel
   if (smax > 0.) dt = std::fmin(dxcur * cfl / (smax * 3.), dt);
   *dt_out = dt;
   return 0;
+}
+
+extern "C" void emma_hydro_noalloc_forget(void) {
+  for (int d = 0; d < kMaxDevices; d++) g_scratch_addr[d].store(nullptr, std::memory_order_release);
 }

@@ -8,7 +8,8 @@
 // at the same offset from the first oct of the caller's pool, shifts every
 // pointer by the pool offset, rebuilds firstoct/lastoct and chains the unused
 // octs (level 0) of the pool into the free list.  With a resident tree uploaded
-// from the same firstoct, a save first downloads the device state into it.
+// from the same firstoct, a save first downloads the device state into it, and a
+// restore releases it (the pool it mirrored is overwritten).
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -78,6 +79,11 @@ int emma_hydro_restore_amr(const char *filename, struct OCT **firstoct, struct O
       tinit == nullptr || nsteps == nullptr || ndumps == nullptr || lcoarse == nullptr || lmax == nullptr ||
       adt == nullptr || units7 == nullptr || levelmax < 1 || ngridmax < 1)
     return EMMA_ST_ARG;
+  // the pool is overwritten: a resident tree uploaded from it no longer describes
+  // it (its cached oct pointers would write stale device state into the restored
+  // octs at the next download), so it is released; upload the restored tree again
+  const int rel = emma_hydro_tree_release(firstoct);
+  if (rel != 0) return rel;
   struct OCT *root_mem = firstoct[0];  // the pool's first oct
   struct CELL *rootcell_mem = &root_mem->cell[0];
   for (int l = 1; l <= levelmax; l++) firstoct[l - 1] = lastoct[l - 1] = nullptr;

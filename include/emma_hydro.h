@@ -123,6 +123,11 @@ int emma_hydro_tree_upload(struct OCT **firstoct, int lcoarse, int lmax, int ran
 /* Copy the device state back into `field` and `fieldnew` of the host tree
  * (a and E recomputed as the reference stores them). */
 int emma_hydro_tree_download(struct OCT **firstoct);
+/* Release the resident tree uploaded from `firstoct` (no-op for another tree):
+ * device buffers and the captured coarse step are freed, emma_hydro_is_resident
+ * returns 0 afterwards.  emma_hydro_restore_amr calls it, since it overwrites
+ * the pool the resident tree mirrors.  No reference counterpart. */
+int emma_hydro_tree_release(struct OCT **firstoct);
 /* Re-read only the fields (same structure) / write only the fields. */
 int emma_hydro_fields_upload(struct OCT **firstoct);
 
@@ -176,7 +181,8 @@ int emma_hydro_restore_amr(const char *filename, struct OCT **firstoct, struct O
  * -DWGRAV library also 5 gdata.d, 7 gdata.p, 8 res, 9-11 f.  For a tree resident
  * on the GPU, ids 13-17 come from the device state (compacted to floats on the
  * GPU), the others from the host tree.  Returns 0, EMMA_ST_ARG (bad argument,
- * unknown id, file error) or EMMA_ST_CUDA. */
+ * unknown id, file error), EMMA_ST_TREE (a resident tree whose host tree was
+ * refined or coarsened since its upload: upload it again) or EMMA_ST_CUDA. */
 int emma_hydro_dump_alloct(const char *folder, struct OCT **firstoct, int lcoarse, int lmax, int rank, int ndumps,
                            double tsim, int nfields, const int *ids, const char *const *names);
 
@@ -251,6 +257,12 @@ int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int tran
  * touch emma_hydro_status). */
 int emma_hydro_level_dt_noalloc(const double *d_state, long long ncells, int level, double cfl,
                                 void *stream, double *dt_out);
+/* Drops the device addresses of the fixed scratch that emma_hydro_level_dt_noalloc
+ * cached per device.  Call it after a cudaDeviceReset (or any other teardown of a
+ * device's primary context) and before the next emma_hydro_level_dt_noalloc call:
+ * the reset unloads the library's module, so the cached address is stale.  No
+ * counterpart in the reference. */
+void emma_hydro_noalloc_forget(void);
 
 /* --------------------------------------------------- host tree utilities */
 /* Build an oct tree with the reference's construction order

@@ -304,6 +304,13 @@ class RefTree:
         t = self.L.ref_run(nsteps, dt_param, time_max, nsub, tsim0, ctypes.byref(nd))
         return t, np.array([self.L.ref_adt(l) for l in range(1, self.lmax + 1)])
 
+    def hydro_solver_prefix(self, level, nsample):
+        """clean_new_hydro + HydroSolver of the reference on the first `nsample`
+        octs of the level list (a bounded sample of one level step); returns dt."""
+        self.L.ref_hydro_solver_prefix.argtypes = [c_int, c_int]
+        self.L.ref_hydro_solver_prefix.restype = c_double
+        return self.L.ref_hydro_solver_prefix(level, nsample)
+
     def hydro_seconds(self):
         return self.L.ref_hydro_seconds()
 

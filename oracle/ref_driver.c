@@ -331,6 +331,34 @@ void ref_hydro_solver(int level, double dt) {
   g_cell_updates += leaf_cells(level);
 }
 
+/* A bounded sample of one level step on a large level: clean_new_hydro and
+ * HydroSolver run unmodified on the first `nsample` octs of the level list.
+ * The list is cut after that oct for the duration of the calls (both walk
+ * firstoct[level-1] through `next`, src/hydro_utils.c:3322-3366, 3410-3483,
+ * 3501-3546) and relinked afterwards; the gather still reads every neighbour
+ * through the tree's pointers, so each sampled oct does exactly the work of a
+ * whole-level step.  Timed like ref_hydro_solver (HydroSolver only).  The CFL
+ * step of the whole level is taken first (L_comptstep_hydro, untimed). */
+double ref_hydro_solver_prefix(int level, int nsample) {
+  struct OCT *o = g_first[level - 1], *cut;
+  int i;
+  double t0, dt;
+  long long n = 0;
+  if (o == NULL || nsample <= 0) return 0.;
+  for (i = 1; i < nsample && o->next != NULL; i++) o = o->next;
+  cut = o->next;
+  dt = L_comptstep_hydro(level, &g_param, g_first, 1.0, 1.0, &g_cpu, 1e9);
+  o->next = NULL;
+  clean_new_hydro(level, &g_param, g_first, &g_cpu);
+  t0 = now_s();
+  HydroSolver(level, &g_param, g_first, &g_cpu, g_stencil, g_param.hstride, dt);
+  g_hydro_seconds += now_s() - t0;
+  n = leaf_cells(level);
+  o->next = cut;
+  g_cell_updates += n;
+  return dt;
+}
+
 /* -------------------------------------- hydro-only Advance_level schedule */
 static REAL advance_level(int level, REAL tloc) {
   REAL dt = 0., dtnew, dthydro, dtfine;

@@ -406,3 +406,38 @@ def test_full_size_conservation_and_mixed_l1(gpu, config):
     assert l1_rel(fm[0], ff[0]) <= 1e-5
     assert l1_rel(fm[4], ff[4]) <= 1e-5
     assert l1_rel(np.sqrt((fm[1:4] ** 2).sum(0)), np.sqrt((ff[1:4] ** 2).sum(0))) <= 1e-5
+
+
+# The benchmark configurations at their stated sizes: FP64 per-cell <= 1e-12 after one
+# coarse step against the oracle (the oracle takes ~0.4 s for the Sod tube, ~5 s for
+# the 128^3 box, ~40 s for the 256^3 box and ~60 s for the cosmology tree).
+BENCH_CONFIGS = {
+    "sod_l6": lambda: configs.sod(level=6),          # 64^3, transmissive x
+    "turb_128": lambda: configs.turb(),               # 128^3 turbulent box
+    "cosmo_l7_l10": lambda: configs.cosmo(),          # base 128^3, levels 7-10, subcycled
+    "roofline_256": lambda: configs.random_uniform(level=8),  # 256^3 random box
+}
+
+
+@pytest.mark.parametrize("name", list(BENCH_CONFIGS))
+def test_fp64_benchmark_config_one_step(gpu, name):
+    cfg = BENCH_CONFIGS[name]()
+    tg, r, st = run_gpu(cfg, 1)
+    assert st == 0
+    levels = [l for l in range(cfg.lcoarse, cfg.lmax + 1) if tg.noct(l) > 0]
+    to, tsim = run_oracle(cfg, 1)
+    assert r.tsim == tsim
+    for l in levels:  # identical trees: same octs per level, same split cells
+        assert tg.noct(l) == to.noct(l)
+        assert np.array_equal(tg.split_mask(l), to.split_mask(l))
+    assert_close(tg, to, levels, 1e-12)
+
+
+def test_fp64_sod_l6_hundred_steps(gpu):
+    """The Sod configuration as stated (64^3, 100 steps): per cell <= 1e-10."""
+    cfg = configs.sod(level=6)
+    tg, r, st = run_gpu(cfg, 100)
+    assert st == 0
+    to, tsim = run_oracle(cfg, 100)
+    assert abs(r.tsim - tsim) <= 1e-13 * tsim
+    assert_close(tg, to, [6], 1e-10)

@@ -138,3 +138,41 @@ def test_resident_run_checkpoints_its_device_state(gpu, tmp_path):
     assert head[0] == r.tsim
     nocts = sum(t.noct(l) for l in range(1, 7))
     assert len(raw) == 16 + 16 + 6 * 8 + 7 * 8 + 3 * 8 + nocts * (8 + 1200)
+
+
+@pytest.mark.gpu
+@needs_ref
+def test_restore_into_a_resident_pool_releases_it(gpu, tmp_path):
+    """Restoring a checkpoint into the pool a resident tree was uploaded from
+    releases that resident tree: a following save writes the restored tree, byte
+    for byte the checkpoint that was restored (same pool, same addresses), and no
+    stale device state is downloaded into it."""
+    from emma_b200 import ResidentHydro, PREC_FP64
+    ref = _ref_tree()
+    f = str(tmp_path / "ckpt.bin")
+    adt = np.array([ref.L.ref_adt(l) for l in range(1, 7)])
+    ref.save_amr(f, 0.5, 0.0, 9, 2, UNITS)
+    # a resident run on the tree (its device state moves on), then the library's
+    # restore of the checkpoint into the same pool
+    r = ResidentHydro(ref, precision=PREC_FP64, cfl=0.8)
+    r.coarse_step()
+    assert lib().emma_hydro_is_resident(ref.firstoct) == 1
+    last, root, ngrid = ref.pool()
+    ts, ti2, lc, lm = ctypes.c_double(), ctypes.c_double(), ctypes.c_int(), ctypes.c_int()
+    ns2, nd2 = ctypes.c_int(), ctypes.c_int()
+    adt2, units = np.zeros(6), np.zeros(7)
+    free = ctypes.c_void_p()
+    rc = lib().emma_hydro_restore_amr(f.encode(), ref.firstoct, last, 6, ngrid, root, ctypes.byref(ts),
+                                      ctypes.byref(ti2), ctypes.byref(ns2), ctypes.byref(nd2), ctypes.byref(lc),
+                                      ctypes.byref(lm), ctypes.c_void_p(adt2.ctypes.data),
+                                      ctypes.c_void_p(units.ctypes.data), ctypes.byref(free))
+    assert rc == 0
+    ref.set_freeoct(free.value)
+    assert lib().emma_hydro_is_resident(ref.firstoct) == 0
+    assert np.array_equal(adt2, adt)
+    fout = str(tmp_path / "after.bin")
+    rc = lib().emma_hydro_save_amr(fout.encode(), ref.firstoct, 0.5, 0.0, 9, 2, 4, 6,
+                                   ctypes.c_void_p(adt2.ctypes.data), ctypes.c_void_p(UNITS.ctypes.data), None)
+    assert rc == 0
+    a, b = open(f, "rb").read(), open(fout, "rb").read()
+    assert len(a) == len(b) and a == b
