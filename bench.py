@@ -174,12 +174,18 @@ def run_mine(args, rank, world):
             for l in levels:
                 r.set_force(l, *synthetic_force(tree, l))
         tuning = {}
+        kernels = set()
         for l in levels:
             rec = r.tuning(l)
             if rec is not None:
+                planes, csweep = r.column_tuning(l)
                 tuning[str(l)] = {"tile_octs": rec[0], "ctas_per_sm": rec[1],
                                   "sweep_ms": {"4x4x2": [round(x, 4) for x in rec[2][0][:3]],
-                                               "2x2x2": [round(x, 4) for x in rec[2][1][:3]]}}
+                                               "2x2x2": [round(x, 4) for x in rec[2][1][:3]],
+                                               "column_planes_2_4_8_16_32_64": [round(x, 4) for x in csweep]},
+                                  "kernel": f"column ({planes} planes per item)" if planes else "brick"}
+                kernels.add("column_kernel<2>" if planes else
+                            ("level_batch_kernel<MathF32>" if prec == PREC_MIXED else "level_batch_kernel<MathF64>"))
         init_states = {l: r.state(l) for l in levels}
         r.coarse_step(nsub=cfg.nsub)  # builds and instantiates the graph
         for _ in range(max(args.warmup - 1, 0)):
@@ -206,7 +212,7 @@ def run_mine(args, rank, world):
         status = r.status()
         launches_per_step = graph_kernel_count(cfg, tree)
         res = {"ms": ms, "updates": updates, "launches": launches_per_step * args.steps, "status": status,
-               "clocks": clk.summary(), "autotune": tuning}
+               "clocks": clk.summary(), "autotune": tuning, "kernels": sorted(kernels)}
         # level-kernel time per launch: the same steps on the host-driven schedule,
         # each level-kernel launch timed with CUDA events on the library stream
         r2 = r
@@ -483,7 +489,7 @@ def main():
         "l1_vs_fp64": l1,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "peak_source": peak_kind, "traffic": (tpc * cells_per_launch) if tpc else None,
-                     "kernel": "level_batch_kernel<MathF32>", "alg_bytes_per_cell": ALG_BYTES_PER_CELL,
+                     "kernel": " + ".join(mixed["kernels"]), "alg_bytes_per_cell": ALG_BYTES_PER_CELL,
                      "cells_per_launch": cells_per_launch, "avg_launch_ms": mixed["kernel_avg_ms"]},
         "e2e": ({"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": dropin["h2d"],
                  "d2h_bytes_per_step": dropin["d2h"], "ms_per_step": ms_d / args.steps,
@@ -497,7 +503,9 @@ def main():
                          "d2h_bytes_per_step": mixed["d2h"],
                          "api": "emma_hydro_set_level_state + coarse step + emma_hydro_get_level_state, pinned host"},
         "autotune": {"mixed": mixed["autotune"], "fp64": fp64["autotune"],
-                     "candidates": "brick 4x4x2 octs x1 or 2x2x2 octs x4 per 256-thread tile; 1..occupancy CTAs per SM"},
+                     "candidates": "brick 4x4x2 octs x1 or 2x2x2 octs x4 per 256-thread tile, 1..occupancy CTAs "
+                                   "per SM; mixed path on complete periodic levels without split cells: the column "
+                                   "kernel (16x16-cell columns) with 2..64 cell planes per work item"},
         "gpu_launches": mixed["launches"],
         "clocks": mixed["clocks"],
         "status": mixed["status"],

@@ -30,6 +30,7 @@ cudaError_t launch_level_fp64(const BatchArgs &a, unsigned shapes, int nsm, int 
                               int *occupancy);
 cudaError_t launch_level_f32(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
                              int *occupancy);
+cudaError_t launch_column_f32(const ColumnArgs &a, cudaStream_t s);
 cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *gate, unsigned long long *out, int nsm,
                        cudaStream_t s);
 cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s,
@@ -66,6 +67,13 @@ struct DevLevel {
   double *F = nullptr;     // gravity build: acceleration planes fx,fy,fz of the level's cells
   double *Fv = nullptr;    // gravity build: interpolated accelerations of the listed coarser cells
   uint8_t *az = nullptr;   // dual energy: per cell, a split cell whose stored sound speed is 0
+  // column kernel (column_kernel.cuh): a complete periodic level without split cells of a
+  // resident plain-variant tree has the oct index of every oct position; col_nz is the
+  // planes per work item the autotuner chose (0: the brick kernel was faster)
+  int *octidx = nullptr;
+  int col_n = 0;  // octs per side, 0 when the level is not eligible
+  int col_nz = 0;
+  double col_sweep_ms[6] = {};  // planes per item 2, 4, 8, 16, 32, 64 (0 = not tried)
   long long nv = 0;
   int shape = 0;        // brick shape of the plan (kShapes)
   int ctas = 0;         // CTAs per SM of its launches (0: the occupancy limit)
@@ -105,7 +113,7 @@ struct Ctx {
   int *d_work_all = nullptr;     // batched work list, finest level first
   int nwork_all = 0;
   cudaGraphExec_t graph = nullptr;
-  int graph_nsub = -1, graph_prec = -1;
+  int graph_nsub = -1, graph_prec = -1, graph_col = -2;
   // drop-in cache: one mirror of levels L-1..L+1 per advanced level L, so that a
   // driver cycling through its levels does not rebuild one on every call
   struct DropCache {
@@ -316,6 +324,7 @@ void drop_graph() {
   if (g.graph) cudaGraphExecDestroy(g.graph);
   g.graph = nullptr;
   g.graph_nsub = g.graph_prec = -1;
+  g.graph_col = -2;
 }
 
 void free_level(DevLevel &d) {
@@ -337,6 +346,7 @@ void free_level(DevLevel &d) {
   cudaFree(d.F);
   cudaFree(d.Fv);
   cudaFree(d.az);
+  cudaFree(d.octidx);
   d = DevLevel();
 }
 
@@ -366,6 +376,8 @@ bool upload_vec(T **dst, const std::vector<T> &v) {
 
 // Allocate device arrays of the mirrored levels, copy topology + plans, and
 // initialise the device level slots.
+int column_default_nz(const DevLevel &d);
+
 bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
   t.lev.assign(H.lev.size(), DevLevel());
   t.lcoarse = H.lcoarse;
@@ -458,6 +470,24 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     a.wv_inject = H.grav;
     a.az = d.az;
     a.azall = (!with_base && g.opt.dual_energy) ? &g.d_S->azall[L] : nullptr;  // resident levels only
+    // the column kernel: a complete periodic level without split cells of a resident
+    // plain-variant tree (its oct at every position, so no tile plan is read)
+    const long long nside = 1LL << (L - 1);
+    if (!with_base && !has_split && !H.trans && !H.grav && !g.opt.dual_energy && !kDropinTracer && L >= 4 &&
+        h.noct == h.nown && (long long)h.noct == nside * nside * nside && (2 * nside) % kColumnWidth == 0) {
+      std::vector<int> idx((size_t)h.noct, -1);
+      bool full = true;
+      for (int i = 0; i < h.noct && full; i++) {
+        const long long k = ((long long)h.pos[3 * i + 2] * nside + h.pos[3 * i + 1]) * nside + h.pos[3 * i];
+        full = idx[(size_t)k] < 0;
+        idx[(size_t)k] = i;
+      }
+      if (full) {
+        if (!upload_vec(&d.octidx, idx)) return false;
+        d.col_n = (int)nside;
+        d.col_nz = column_default_nz(d);
+      }
+    }
     k_set_args<<<1, 1, 0, g.stream>>>(t.d_lv, L, a);
     if (!ck(cudaGetLastError(), "k_set_args")) return false;
   }
@@ -598,10 +628,63 @@ cudaError_t mark_stale(int level) {
   return e;
 }
 
+// Column kernel: planes per work item (the autotuner's candidates).
+constexpr int kColNz[6] = {2, 4, 8, 16, 32, 64};
+
+bool column_nz_ok(const DevLevel &d, int nz) {
+  const int nc = 2 * d.col_n;
+  return d.col_n > 0 && nz >= 2 && nz % 2 == 0 && nz <= nc && nc % nz == 0;
+}
+
+long long column_items(const DevLevel &d, int nz) {
+  const long long ncol = 2LL * d.col_n / kColumnWidth;
+  return ncol * ncol * (2LL * d.col_n / nz);
+}
+
+// the largest candidate that still gives every SM four work items (two CTAs per SM,
+// two waves), else the smallest valid one
+int column_default_nz(const DevLevel &d) {
+  int best = 0;
+  for (int nz : kColNz) {
+    if (!column_nz_ok(d, nz)) continue;
+    if (best == 0 || column_items(d, nz) >= 4LL * g.nsm) best = nz;
+  }
+  return best;
+}
+
+// planes per item of a launch of resident level L on the column kernel; 0: the
+// brick kernel (FP64 path, ineligible level, option column < 0, or the
+// autotuner found the brick kernel faster)
+int column_nz(int L) {
+  if (L < 0 || !g.res.valid || L < g.res.lcoarse || L > g.res.lmax) return 0;
+  const DevLevel &d = g.res.lev[L];
+  if (d.col_n == 0 || g.opt.precision != EMMA_PREC_MIXED || g.opt.column < 0) return 0;
+  if (g.opt.column > 0) return column_nz_ok(d, g.opt.column) ? g.opt.column : 0;
+  return d.col_nz;
+}
+
+cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl) {
+  const DevLevel &d = g.res.lev[L];
+  ColumnArgs c;
+  c.lv = g.res.d_lv + L;
+  c.L = L;
+  c.octidx = d.octidx;
+  c.n = d.col_n;
+  c.nz = nz;
+  c.ncol = 2 * d.col_n / kColumnWidth;
+  c.nitems = (int)column_items(d, nz);
+  c.gate = gate;
+  c.status = g.d_status;
+  c.smax = fuse_cfl ? g.d_S->smax_next : nullptr;
+  return launch_column_f32(c, g.stream);
+}
+
 // fuse_cfl: the launch also accumulates each level's max signal speed of the
 // state it writes (the device schedule's next CFL step, SchedState::smax_next).
+// col_level: the launch advances resident level col_level alone, which may then
+// run on the column kernel (column_nz).
 bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, long long cells, unsigned shapes,
-                  int ctas, bool fuse_cfl = false, bool grav = false) {
+                  int ctas, bool fuse_cfl = false, bool grav = false, int col_level = -1) {
   BatchArgs a;
   a.lv = d_lv;
   a.work = work;
@@ -625,7 +708,10 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
   if (grav || (d_lv == g.res.d_lv && g.res.host.grav)) shapes |= kLaunchGrav;
   if (g.opt.dual_energy) shapes |= kLaunchDual;
   if (kDropinTracer) shapes |= kLaunchTracer;
-  cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED)
+  const int cnz = (d_lv == g.res.d_lv && !(shapes & (kLaunchGrav | kLaunchDual | kLaunchTracer)))
+                      ? column_nz(col_level) : 0;
+  cudaError_t e = (cnz > 0) ? launch_column(col_level, cnz, gate, fuse_cfl)
+                  : (g.opt.precision == EMMA_PREC_MIXED)
                       ? launch_level_f32(a, shapes, g.nsm, ctas, g.stream, nullptr)
                       : launch_level_fp64(a, shapes, g.nsm, ctas, g.stream, nullptr);
   if (nwork > 0) g.kernel_launches++;
@@ -718,7 +804,7 @@ bool emit_level(int L, int nsub) {
     if (has_fine && !emit_level(L + 1, nsub)) return false;
     k_sub_prelaunch<<<1, 1, 0, g.stream>>>(S, t.d_lv, L, has_fine ? 1 : 0);
     if (!ck(launch_interp(t.d_lv, L, d.nv, gate, g.nsm, g.stream, t.host.grav), "interpolation launch")) return false;
-    if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf, 1u << d.shape, d.ctas, true)) return false;
+    if (!launch_batch(t.d_lv, d.work, d.ntiles, gate, d.leaf, 1u << d.shape, d.ctas, true, false, L)) return false;
     k_sub_end<<<1, 1, 0, g.stream>>>(S, t.d_lv, L);
     if (!ck(cudaGetLastError(), "schedule kernel")) return false;
   }
@@ -755,7 +841,9 @@ bool emit_coarse_step(int nsub) {
         ctas = t.lev[L].ctas;
       }
     }
-    if (!launch_batch(t.d_lv, g.d_work_all, g.nwork_all, nullptr, cells, shapes, ctas, true)) return false;
+    if (!launch_batch(t.d_lv, g.d_work_all, g.nwork_all, nullptr, cells, shapes, ctas, true, false,
+                      lf == lc ? lc : -1))
+      return false;
     k_batch_end<<<1, 1, 0, g.stream>>>(S, t.d_lv);
     return ck(cudaGetLastError(), "schedule kernel");
   }
@@ -765,7 +853,7 @@ bool emit_coarse_step(int nsub) {
 }
 
 bool ensure_graph(int nsub) {
-  if (g.graph && g.graph_nsub == nsub && g.graph_prec == g.opt.precision) return true;
+  if (g.graph && g.graph_nsub == nsub && g.graph_prec == g.opt.precision && g.graph_col == g.opt.column) return true;
   drop_graph();
   cudaGraph_t graph = nullptr;
   if (!ck(cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return false;
@@ -783,6 +871,7 @@ bool ensure_graph(int nsub) {
   }
   g.graph_nsub = nsub;
   g.graph_prec = g.opt.precision;
+  g.graph_col = g.opt.column;
   return true;
 }
 
@@ -861,6 +950,7 @@ void emma_hydro_default_options(struct EmmaHydroOptions *opt) {
   opt->use_graph = 1;
   opt->gravity = 0;
   opt->dual_energy = 0;
+  opt->column = 0;
 }
 
 int emma_hydro_init(const struct EmmaHydroOptions *opt) {
@@ -1090,6 +1180,29 @@ bool autotune_tree(Tree &t, int shape_req) {
          ck(cudaStreamSynchronize(g.stream), "tune");
     d.ctas = best_ctas;
     d.tuned = ok;
+    // the column kernel against the best brick launch, over its planes per work item
+    if (ok && d.col_n > 0 && g.opt.precision == EMMA_PREC_MIXED && g.opt.column == 0 && shape_req < 0) {
+      int best_nz = 0;
+      double best_col = 0;
+      for (int i = 0; i < 6 && ok; i++) {
+        const int nz = kColNz[i];
+        d.col_sweep_ms[i] = 0;
+        if (!column_nz_ok(d, nz)) continue;
+        double ms = 0;
+        for (int rep = 0; rep < 4 && ok; rep++) {  // one warm-up, three timed
+          ok = ck(cudaEventRecord(e0, g.stream), "event") && ck(launch_column(L, nz, nullptr, false), "column") &&
+               ck(cudaEventRecord(e1, g.stream), "event") && ck(cudaEventSynchronize(e1), "event");
+          float f = 0;
+          if (ok && rep > 0 && cudaEventElapsedTime(&f, e0, e1) == cudaSuccess) ms += f / 3.;
+        }
+        d.col_sweep_ms[i] = ms;
+        if (ok && (best_col == 0 || ms < best_col)) {
+          best_col = ms;
+          best_nz = nz;
+        }
+      }
+      d.col_nz = (ok && best_col > 0 && (best == 0 || best_col < best)) ? best_nz : 0;
+    }
   }
   // undo the trial launches: corrections, completion counters, status
   for (int L = t.lcoarse; L <= t.lmax && ok; L++) {
@@ -1376,7 +1489,8 @@ int emma_hydro_advance_level(int level, double dt) {
   k_bind_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, g.res.lcoarse, g.res.lmax, dt);
   CK(cudaGetLastError());
   CK(launch_interp(g.res.d_lv, level, d.nv, nullptr, g.nsm, g.stream, g.res.host.grav));
-  if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas)) return EMMA_ST_CUDA;
+  if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas, false, false, level))
+    return EMMA_ST_CUDA;
   k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
   CK(cudaGetLastError());
   CK(mark_stale(level));
@@ -1509,6 +1623,15 @@ int emma_hydro_probe_wait_timeout(long long polls) {
   CK(cudaMemcpy(g.d_status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice));
   CK(cudaMemset(g.d_done, 0, sizeof(unsigned) * kMaxLevels));
   return (int)bits;
+}
+
+int emma_hydro_column_tuning(int level, int *planes, double *sweep_ms) {
+  if (!level_ok(level)) return EMMA_ST_ARG;
+  const DevLevel &d = g.res.lev[level];
+  if (planes) *planes = column_nz(level);
+  if (sweep_ms)
+    for (int i = 0; i < 6; i++) sweep_ms[i] = d.col_sweep_ms[i];
+  return 0;
 }
 
 int emma_hydro_tuning(int level, int *tile_octs, int *ctas_per_sm, double *sweep_ms) {

@@ -1,6 +1,7 @@
 // level_f32.cu -- mixed-path instantiation of the level kernel: FP32
 // reconstruction, wave speeds and fluxes; FP64 compensated update.
 #include "level_kernel.cuh"
+#include "column_kernel.cuh"
 
 namespace emma {
 
@@ -10,6 +11,24 @@ namespace emma {
 cudaError_t launch_level_f32(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
                              int *occupancy) {
   return launch_level_any<MathF32>(a, shapes, nsm, ctas_per_sm, s, occupancy);
+}
+
+// Column kernel of a complete periodic level (mixed path), two CTAs per SM.
+cudaError_t launch_column_f32(const ColumnArgs &a, cudaStream_t s) {
+  constexpr int kMaxDev = 64;
+  static bool attr_set[kMaxDev] = {false};  // the shared-memory limit is a per-device attribute
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
+  if (!attr_set[dev]) {
+    e = cudaFuncSetAttribute(column_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col::kSmem);
+    if (e != cudaSuccess) return e;
+    attr_set[dev] = true;
+  }
+  if (a.nitems <= 0) return cudaSuccess;
+  column_kernel<2><<<a.nitems, col::kColThreads, col::kSmem, s>>>(a);
+  return cudaGetLastError();
 }
 
 }  // namespace emma

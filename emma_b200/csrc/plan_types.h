@@ -132,6 +132,22 @@ struct BatchArgs {
                              // (bits of a non-negative double, atomicMax), or null
 };
 
+// A launch of the column kernel (column_kernel.cuh): one complete periodic level
+// without split cells, as columns of 16 x 16 cells marching through `nz` planes.
+struct ColumnArgs {
+  const LevelArgs *lv;  // the level's device slot: W, Wn, dt, dx are read at launch
+  int L;
+  const int *octidx;    // oct (list index) at every oct position, ((oz * n + oy) * n + ox)
+  int n;                // octs per side
+  int nz;               // cell planes per work item (even, divides 2n)
+  int ncol;             // columns per side (2n / 16)
+  int nitems;           // ncol * ncol * (2n / nz)
+  const int *gate;      // launch does nothing unless *gate != 0 (null: always)
+  unsigned *status;
+  unsigned long long *smax;  // [L]: max signal speed of the new state (bits of a double), or null
+};
+constexpr int kColumnWidth = 16;  // cells per column side
+
 constexpr int kWorkSlotShift = 24;
 constexpr int kMaxLevels = 32;
 

@@ -13,10 +13,13 @@ from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
 def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0, gravity=False,
-            dual=False):
+            dual=False, column=0):
     """tile_octs: 0 = brick shape autotuned per level at upload, 32 = 4x4x2-oct
     bricks, 8 = 2x2x2-oct bricks (four per tile).  gravity: the -DWGRAV coupling
-    (forces from ResidentHydro.set_force).  dual: the -DDUAL_E tracked internal energy."""
+    (forces from ResidentHydro.set_force).  dual: the -DDUAL_E tracked internal energy.
+    column (mixed path, complete periodic levels without split cells): 0 = the
+    autotuner picks the column kernel or the brick kernel, -1 = brick kernel only,
+    n > 0 = column kernel with n cell planes per work item."""
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
@@ -24,6 +27,7 @@ def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, ti
     o.tile_octs = tile_octs
     o.gravity = 1 if gravity else 0
     o.dual_energy = 1 if dual else 0
+    o.column = column
     return o
 
 
@@ -31,15 +35,17 @@ class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
     def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0,
-                 gravity=False, dual=False):
+                 gravity=False, dual=False, column=0):
         self.tree = tree
+        self.column = column
         self.gravity, self.dual = gravity, dual
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
         self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
         self.precision = precision
         # a tree of the -DWRADHYD layout runs on libemmahydro_rh.so (its tracer advanced too)
         self._L = L = lib("rh" if getattr(tree, "rh", False) else False)
-        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity, dual=dual)
+        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity, dual=dual,
+                    column=column)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
         check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
         L.emma_hydro_clear_status()
@@ -52,13 +58,13 @@ class ResidentHydro:
         (the resident tree and its tuned plans stay)."""
         self.use_graph = use_graph
         o = options(self.precision, self.trans, self.cfl, use_graph=use_graph, tile_octs=self.tile_octs,
-                    gravity=self.gravity, dual=self.dual)
+                    gravity=self.gravity, dual=self.dual, column=self.column)
         check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def set_precision(self, precision):
         self.precision = precision
         o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
-                    gravity=self.gravity, dual=self.dual)
+                    gravity=self.gravity, dual=self.dual, column=self.column)
         check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):
@@ -118,6 +124,21 @@ class ResidentHydro:
         sweep = np.zeros(8)
         rc = self._L.emma_hydro_tuning(level, ctypes.byref(octs), ctypes.byref(ctas), ptr(sweep))
         return (octs.value, ctas.value, sweep.reshape(2, 4)) if rc == 0 else None
+
+    def column_tuning(self, level):
+        """(cell planes per work item of the level's column-kernel launches, 0 = brick
+        kernel; ms per launch the autotuner measured with 2, 4, 8, 16, 32, 64 planes)."""
+        planes = ctypes.c_int()
+        sweep = np.zeros(6)
+        check(self._L.emma_hydro_column_tuning(level, ctypes.byref(planes), ptr(sweep)), "column_tuning")
+        return planes.value, sweep
+
+    def set_column(self, column):
+        """Column-kernel option (see options); the resident tree and its plans stay."""
+        self.column = column
+        o = options(self.precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
+                    gravity=self.gravity, dual=self.dual, column=column)
+        check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
 
     def download(self):
         check(self._L.emma_hydro_tree_download(self.tree.firstoct), "tree_download")

@@ -3,6 +3,7 @@
     python -m emma_b200.run_case --config random --level 6 --precision mixed --steps 3
     python -m emma_b200.run_case --config turb --level 7 --precision fp64 --steps 2 --dropin rh
     python -m emma_b200.run_case --config turb --level 7 --precision mixed --steps 4 --tracer
+    python -m emma_b200.run_case --config random --level 8 --precision mixed --steps 3 --column 32
 
 Used to profile one configuration in isolation (for example under ncu).  --dropin
 runs the drop-in clean_new_hydro + HydroSolver on the finest level of the host tree
@@ -24,6 +25,8 @@ def main():
     ap.add_argument("--steps", type=int, default=3)
     ap.add_argument("--dropin", default=None, choices=["plain", "rh"])
     ap.add_argument("--tracer", action="store_true", help="resident run of the -DWRADHYD library (dX = d/2)")
+    ap.add_argument("--column", type=int, default=0,
+                    help="column kernel of complete periodic levels (mixed): 0 autotuned, -1 off, n planes per item")
     a = ap.parse_args()
     cfg = {"random": lambda: configs.random_uniform(level=a.level), "turb": lambda: configs.turb(level=a.level),
            "sod": lambda: configs.sod(level=a.level), "sedov": configs.sedov, "cosmo": configs.cosmo,
@@ -40,7 +43,7 @@ def main():
         tree = cfg.build()
     # host-driven schedule: every level-kernel launch is timed with CUDA events
     r = ResidentHydro(tree, precision=PREC_MIXED if a.precision == "mixed" else PREC_FP64, trans=cfg.trans,
-                      cfl=cfg.cfl, use_graph=False)
+                      cfl=cfg.cfl, use_graph=False, column=a.column)
     L = lib("rh" if a.tracer else False)
     per_step = []
     tot_ms, tot_n, tot_cells = 0.0, 0, 0
@@ -53,7 +56,8 @@ def main():
         tot_ms += avg.value * n.value
         tot_n += n.value
         tot_cells += cells.value
-    print(json.dumps({"config": cfg.name, "precision": a.precision, "status": r.status(), "launches": tot_n,
+    print(json.dumps({"config": cfg.name, "level": cfg.lcoarse, "precision": a.precision, "status": r.status(),
+                      "column_planes": r.column_tuning(cfg.lcoarse)[0], "launches": tot_n,
                       "avg_launch_ms": tot_ms / max(tot_n, 1), "cells_per_launch": tot_cells / max(tot_n, 1),
                       "kernel_ms_per_step": per_step,
                       "cell_updates_per_s_kernel": tot_cells / (tot_ms * 1e-3) if tot_ms else None}))

@@ -73,6 +73,11 @@ struct EmmaHydroOptions {
                            flux and a p div(u) term, and the pressure comes from it unless
                            E - Ekin is resolved (src/hydro_utils.c:45-49, 2126-2129,
                            3164-3182).  Drop-in and resident modes. */
+  int column;           /* mixed precision, resident complete periodic levels without split
+                           cells (plain variant): 0 = the autotuner picks the column kernel
+                           (16 x 16-cell columns marching through z) or the brick kernel,
+                           -1 = brick kernel only, n > 0 = column kernel with n cell planes
+                           per work item (even, dividing the level's cells per side) */
 };
 void emma_hydro_default_options(struct EmmaHydroOptions *opt);
 
@@ -216,6 +221,11 @@ void emma_hydro_reset_counters(void);
  * measured with CUDA events on the launching stream, and their count. */
 int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cells);
 
+/* Column kernel of a resident level (no reference counterpart): *planes = the cell
+ * planes per work item its launches use with the current options (0: the brick
+ * kernel), sweep_ms[6] = the autotuner's ms per launch with 2, 4, 8, 16, 32, 64
+ * planes per item (0 = not tried). */
+int emma_hydro_column_tuning(int level, int *planes, double *sweep_ms);
 /* Autotuner record of a resident level (emma_hydro_tree_upload tunes every
  * level when options.tile_octs == 0): the chosen brick (32 = 4x4x2 octs, one
  * per tile; 8 = 2x2x2 octs, four per tile), the CTAs per SM of its launches,
