@@ -65,6 +65,11 @@ SIGNATURES = [
     ("emma_hydro_set_level_force", c_int, [c_int, c_void_p]),
     ("emma_hydro_is_resident", c_int, [c_void_p]),
     ("emma_hydro_tree_release", c_int, [c_void_p]),
+    ("emma_hydro_mark_cells", c_int, [c_int, c_void_p, c_void_p, c_int, c_double, c_void_p]),
+    ("emma_hydro_check_rule", c_int, [c_int, c_void_p, c_void_p, c_void_p]),
+    ("emma_hydro_marks_to_host", c_int, [c_void_p, c_int]),
+    ("emma_hydro_refine_cells", c_void_p, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                           c_double]),
     ("emma_hydro_dump_alloct", c_int, [ctypes.c_char_p, c_void_p, c_int, c_int, c_int, c_int, c_double, c_int,
                                        c_void_p, c_void_p]),
     ("emma_hydro_save_amr", c_int, [ctypes.c_char_p, c_void_p, c_double, c_double, c_int, c_int, c_int, c_int,

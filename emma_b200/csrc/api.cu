@@ -16,6 +16,8 @@
 #include <string>
 #include <thread>
 #include <pthread.h>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 #include "emma_hydro.h"
 #ifdef EMMA_WGRAV
@@ -72,6 +74,10 @@ struct DevLevel {
   // planes per work item the autotuner chose (0: the brick kernel was faster)
   int *octidx = nullptr;
   int col_n = 0;  // octs per side, 0 when the level is not eligible
+  // device-side refinement (refine_impl.cuh, resident levels): the oct of this level
+  // across each face of every oct (-1: none), and the refinement mark of every cell
+  int *nb6 = nullptr;
+  int *marks = nullptr;
   int col_nz = 0;
   double col_sweep_ms[6] = {};  // planes per item 2, 4, 8, 16, 32, 64 (0 = not tried)
   long long nv = 0;
@@ -347,6 +353,8 @@ void free_level(DevLevel &d) {
   cudaFree(d.Fv);
   cudaFree(d.az);
   cudaFree(d.octidx);
+  cudaFree(d.nb6);
+  cudaFree(d.marks);
   d = DevLevel();
 }
 
@@ -470,6 +478,13 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
     a.wv_inject = H.grav;
     a.az = d.az;
     a.azall = (!with_base && g.opt.dual_energy) ? &g.d_S->azall[L] : nullptr;  // resident levels only
+    if (!with_base) {  // refinement topology and the cells' marks
+      if (!upload_vec(&d.nb6, h.nb6)) return false;
+      std::vector<int> m((size_t)d.n8);
+      for (int i = 0; i < h.noct; i++)
+        for (int c = 0; c < 8; c++) m[8 * (size_t)i + c] = (int)h.octs[i]->cell[c].marked;
+      if (!upload_vec(&d.marks, m)) return false;
+    }
     // the column kernel: a complete periodic level without split cells of a resident
     // plain-variant tree (its oct at every position, so no tile plan is read)
     const long long nside = 1LL << (L - 1);
@@ -901,6 +916,8 @@ bool write_sched_params(double dt_param, double time_max, int nsub, const double
   }
   return ck(cudaStreamSynchronize(g.stream), "sync");
 }
+
+#include "refine_impl.cuh"
 
 }  // namespace
 
@@ -2141,6 +2158,64 @@ void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, 
     for (struct OCT *o = firstoct[level - 2]; o != nullptr; o = o->next)
       if (o->cpu != rank)
         for (int c = 0; c < 8; c++) std::memset(&o->cell[c].fieldnew, 0, sizeof(struct Wtype));
+}
+
+// ------------------------------------------------ device-side refinement
+int emma_hydro_mark_cells(int level, struct RUNPARAMS *param, struct OCT **firstoct, int nsmooth, REAL threshold,
+                          struct CPUINFO *cpu) {
+  (void)param;
+  (void)cpu;
+  int rc = refine_ok(firstoct, level, false);
+  if (rc != 0) return rc;
+  if (nsmooth < 1) return EMMA_ST_ARG;
+  rc = device_mark_cells(level, nsmooth, threshold);
+  if (rc != 0) return rc;
+  CK(cudaStreamSynchronize(g.stream));
+  return 0;
+}
+
+int emma_hydro_check_rule(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu) {
+  (void)param;
+  (void)cpu;
+  int rc = refine_ok(firstoct, level, false);
+  if (rc != 0) return rc;
+  rc = device_check_rule(level);
+  if (rc != 0) return rc;
+  CK(cudaStreamSynchronize(g.stream));
+  return 0;
+}
+
+int emma_hydro_marks_to_host(struct OCT **firstoct, int level) {
+  const int rc = refine_ok(firstoct, level, false);
+  return rc != 0 ? rc : marks_to_host(level);
+}
+
+struct OCT *emma_hydro_refine_cells(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct OCT **lastoct,
+                                    struct OCT *freeoct, struct CPUINFO *cpu, struct OCT *limit, REAL aexp) {
+  (void)aexp;
+  (void)cpu;
+  if (refine_ok(firstoct, level, true) != 0) return nullptr;
+  if (lastoct == nullptr || freeoct == nullptr || limit == nullptr) {
+    fail(EMMA_ST_ARG, "refine_cells: null lastoct, freeoct or limit");
+    return nullptr;
+  }
+  const int lcoarse = param ? reinterpret_cast<const RunParamsHead *>(param)->lcoarse : g.res.lcoarse;
+  if (marks_to_host(level) != 0) return nullptr;
+  if (cudaStreamSynchronize(g.stream) != cudaSuccess) return nullptr;
+  std::vector<struct OCT *> created;
+  std::string err;
+  struct OCT *f = refine_sweep(level, lcoarse, firstoct, lastoct, freeoct, limit, created, err);
+  if (f == nullptr) {
+    // the host tree may be partly refined: the resident mirror no longer matches it
+    fail(EMMA_ST_TREE, "refine_cells: " + err);
+    emma_hydro_tree_release(firstoct);
+    return nullptr;
+  }
+  if (rebuild_after_refine(firstoct, level, created) != 0) {
+    emma_hydro_tree_release(firstoct);
+    return nullptr;
+  }
+  return f;
 }
 
 #ifdef EMMA_WGRAV

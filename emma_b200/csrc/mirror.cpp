@@ -487,6 +487,13 @@ int build_host_tree(struct OCT **firstoct, int lcoarse, int lmax, int rank, int 
     P.face[L].assign((size_t)6 * lv.noct, kKeyNone);
     for (int i = 0; i < lv.noct; i++)
       for (int k = 0; k < 6; k++) P.face[L][6 * i + k] = P.real_nbr(L, i, k);
+    lv.nb6.assign((size_t)6 * lv.noct, -1);
+    for (size_t j = 0; j < lv.nb6.size(); j++) {
+      const uint32_t key = P.face[L][j], kind = key >> 28;
+      if (key == kKeyNone) continue;
+      if (kind == kKeyReal) lv.nb6[j] = (int32_t)(key & 0x0FFFFFFFu);
+      else if (kind >= kKeyGhost0 && kind < kKeyGhost0 + 6) lv.nb6[j] = -2;
+    }
     // integer oct positions on the level grid
     const double scale = std::ldexp(1.0, L - 1);
     const int n = 1 << (L - 1);

@@ -25,6 +25,9 @@ struct HostLevel {
                                       // cell, the cell and its 6 slope neighbours (7 entries)
   int shape = 0;                      // brick shape of the plan (kShapes)
   std::vector<int32_t> pos;           // per oct: integer position on the level grid (x,y,z)
+  std::vector<int32_t> nb6;           // per oct and face -x,+x,-y,+y,-z,+z: the neighbouring oct of
+                                      // this level, -1 where there is none (coarser leaf or domain
+                                      // edge), -2 across a transmissive boundary
 };
 
 struct HostTree {

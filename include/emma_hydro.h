@@ -133,6 +133,36 @@ int emma_hydro_tree_download(struct OCT **firstoct);
  * returns 0 afterwards.  emma_hydro_restore_amr calls it, since it overwrites
  * the pool the resident tree mirrors.  No reference counterpart. */
 int emma_hydro_tree_release(struct OCT **firstoct);
+/* ------------------------------------------ refinement of a resident tree
+ * The reference's marking and refinement of one level (called by Advance_level,
+ * src/advanceamr.c:348-373 and 1230-1241) on the tree uploaded from `firstoct`,
+ * without moving its fields off the GPU.  Periodic trees of the plain variant
+ * (EMMA_ST_ARG with transmissive boundaries, gravity, dual energy or the
+ * -DWRADHYD library).  The marks of every resident cell live on the device
+ * (uploaded from the cells' `marked`).
+ *
+ * emma_hydro_mark_cells: L_clean_marks + L_mark_cells (src/amr.c:1480, 883):
+ * nsmooth rounds of (keep split cells whose children are marked or split; mark
+ * the 3x3x3 neighbourhood of marked cells; in the first round only, mark cells
+ * whose density exceeds `threshold` -- the criterion of the reference's
+ * -DSNTEST build, src/amr.c:1330-1354, which fixes it at 1.1).
+ * emma_hydro_check_rule: L_check_rule (src/amr.c:746): marks of octs whose 26
+ * neighbours do not all exist become 10.
+ * emma_hydro_marks_to_host: the device marks of a level into the cells' `marked`.
+ * emma_hydro_refine_cells: L_refine_cells (src/amr.c:286), same signature and
+ * return value (the new head of the free-oct chain; NULL and status bits on
+ * failure, where the reference aborts): octs of level+1 are destroyed and created
+ * in the host tree in the reference's order, from and onto the caller's free
+ * chain; their device state is gathered on the device (new cells take the parent
+ * cell's state, src/amr.c:512-520) and the resident mirror is re-planned.  The
+ * caller still calls setOctList for level+1 as L_refine_cells does internally.
+ * `param` supplies lcoarse (NULL: the resident tree's); aexp is unused. */
+int emma_hydro_mark_cells(int level, struct RUNPARAMS *param, struct OCT **firstoct, int nsmooth, REAL threshold,
+                          struct CPUINFO *cpu);
+int emma_hydro_check_rule(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct CPUINFO *cpu);
+int emma_hydro_marks_to_host(struct OCT **firstoct, int level);
+struct OCT *emma_hydro_refine_cells(int level, struct RUNPARAMS *param, struct OCT **firstoct, struct OCT **lastoct,
+                                    struct OCT *freeoct, struct CPUINFO *cpu, struct OCT *limit, REAL aexp);
 /* Re-read only the fields (same structure) / write only the fields. */
 int emma_hydro_fields_upload(struct OCT **firstoct);
 

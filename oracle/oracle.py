@@ -26,6 +26,7 @@ REF_LIB_GRAV = os.path.join(HERE, "_ref", "libemmaref_grav.so")
 REF_LIB_DUAL = os.path.join(HERE, "_ref", "libemmaref_dual.so")
 REF_LIB_RH = os.path.join(HERE, "_ref", "libemmaref_rh.so")
 REF_LIB_SP = os.path.join(HERE, "_ref", "libemmaref_sp.so")
+REF_LIB_MARK = os.path.join(HERE, "_ref", "libemmaref_mark.so")
 
 HYDROTEST = 0x40
 DUAL_E = 0x80
@@ -158,7 +159,9 @@ class GravClone:
             self.h = None
 
 
-def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False):
+def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False):
+    if mark:
+        return REF_LIB_MARK
     if sp:
         return REF_LIB_SP
     if rh:
@@ -166,8 +169,8 @@ def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False):
     return REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
 
 
-def ref_available(tx=False, grav=False, dual=False, rh=False, sp=False):
-    return os.path.exists(_ref_path(tx, grav, dual, rh, sp))
+def ref_available(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False):
+    return os.path.exists(_ref_path(tx, grav, dual, rh, sp, mark))
 
 
 class RefTree:
@@ -176,10 +179,11 @@ class RefTree:
     _libs = {}
 
     def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False, dual=False, rh=False,
-                 sp=False):
-        """sp: the reference built with -DSINGLEPRECISION (REAL = float)."""
-        assert (tx + grav + dual + rh + sp) <= 1, "one build variant at a time"
-        path = _ref_path(tx, grav, dual, rh, sp)
+                 sp=False, mark=False):
+        """sp: the reference built with -DSINGLEPRECISION (REAL = float); mark: its
+        src/amr.c built with the density refinement criterion (ref_amr_sntest.c)."""
+        assert (tx + grav + dual + rh + sp + mark) <= 1, "one build variant at a time"
+        path = _ref_path(tx, grav, dual, rh, sp, mark)
         if path not in RefTree._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"reference oracle not built: {path}")
@@ -310,6 +314,28 @@ class RefTree:
         self.L.ref_hydro_solver_prefix.argtypes = [c_int, c_int]
         self.L.ref_hydro_solver_prefix.restype = c_double
         return self.L.ref_hydro_solver_prefix(level, nsample)
+
+    # refinement of one level (mark-criterion build): L_clean_marks, L_mark_cells,
+    # L_check_rule, L_refine_cells (src/amr.c:1480, 883, 746, 286)
+    def clean_marks(self, level):
+        self.L.ref_clean_marks(level)
+
+    def mark_cells(self, level, nsmooth, threshold):
+        self.L.ref_mark_cells.argtypes = [c_int, c_int, c_double]
+        self.L.ref_mark_cells(level, nsmooth, threshold)
+
+    def check_rule(self, level):
+        self.L.ref_check_rule(level)
+
+    def refine_cells(self, level):
+        self.L.ref_refine_cells(level)
+
+    def marks(self, level):
+        out = np.zeros(8 * self.noct(level))
+        if out.size:
+            self.L.ref_get_marks.argtypes = [c_int, c_void_p]
+            self.L.ref_get_marks(level, _p(out))
+        return out
 
     def hydro_seconds(self):
         return self.L.ref_hydro_seconds()

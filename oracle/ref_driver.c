@@ -359,6 +359,29 @@ double ref_hydro_solver_prefix(int level, int nsample) {
   return dt;
 }
 
+/* ------------------------------------------------ refinement (one level) */
+/* The reference's refinement calls of Advance_level (src/advanceamr.c:348-373,
+ * 1230-1241): L_clean_marks, L_mark_cells (the criterion of this build: see
+ * ref_amr_sntest.c), L_check_rule and L_refine_cells, which takes new octs from
+ * the free-oct chain and returns its new head. */
+void ref_clean_marks(int level) { L_clean_marks(level, g_first); }
+void ref_mark_cells(int level, int nsmooth, double threshold) {
+  L_mark_cells(level, &g_param, g_first, nsmooth, threshold, &g_cpu, NULL, NULL);
+}
+void ref_check_rule(int level) { L_check_rule(level, &g_param, g_first, &g_cpu); }
+void ref_refine_cells(int level) {
+  g_cpu.freeoct = L_refine_cells(level, &g_param, g_first, g_last, g_cpu.freeoct, &g_cpu,
+                                 g_grid + g_ngridmax, 1.0);
+  recount();
+}
+/* marks of a level's cells in list order */
+void ref_get_marks(int level, double *out) {
+  int i = 0, c;
+  struct OCT *o;
+  for (o = g_first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) out[8 * i + c] = o->cell[c].marked;
+}
+
 /* -------------------------------------- hydro-only Advance_level schedule */
 static REAL advance_level(int level, REAL tloc) {
   REAL dt = 0., dtnew, dthydro, dtfine;
