@@ -12,6 +12,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "libemmahydro.so")
 LIB_PATH_GRAV = os.path.join(_HERE, "libemmahydro_grav.so")
 LIB_PATH_RH = os.path.join(_HERE, "libemmahydro_rh.so")
+LIB_PATH_HE = os.path.join(_HERE, "libemmahydro_he.so")
 
 _libs = {}
 
@@ -115,20 +116,28 @@ RH_SIGNATURES = [
 ]
 
 
+HE_SIGNATURES = [
+    ("emma_tree_set_tracer_n", None, [c_void_p, c_int, c_int, c_void_p]),
+    ("emma_tree_get_tracer_n", None, [c_void_p, c_int, c_int, c_int, c_void_p]),
+    ("emma_tree_put_tracer_n", None, [c_void_p, c_int, c_int, c_int, c_void_p]),
+]
+
+
 def lib(grav=False):
     """Load libemmahydro.so once; grav=True: libemmahydro_grav.so (the -DWGRAV cell
-    layout), grav="rh": libemmahydro_rh.so (the -DWRADHYD layout).  Raises if the
-    library is not built."""
-    key = "rh" if grav == "rh" else ("grav" if grav else "plain")
+    layout), grav="rh": libemmahydro_rh.so (the -DWRADHYD layout), grav="he":
+    libemmahydro_he.so (the -DWRADHYD -DHELIUM layout).  Raises if the library is
+    not built."""
+    key = grav if grav in ("rh", "he") else ("grav" if grav else "plain")
     if key in _libs:
         return _libs[key]
-    path = {"plain": LIB_PATH, "grav": LIB_PATH_GRAV, "rh": LIB_PATH_RH}[key]
+    path = {"plain": LIB_PATH, "grav": LIB_PATH_GRAV, "rh": LIB_PATH_RH, "he": LIB_PATH_HE}[key]
     if not os.path.exists(path):
         raise RuntimeError(f"{os.path.basename(path)} is not built ({path}); run emma_b200.build.build()")
     # RTLD_LOCAL: the drop-in entries carry the reference's names (HydroSolver, ...);
     # they must not interpose on another library that defines the same symbols
     L = ctypes.CDLL(path, mode=ctypes.RTLD_LOCAL)
-    extra = {"plain": [], "grav": GRAV_SIGNATURES, "rh": RH_SIGNATURES}[key]
+    extra = {"plain": [], "grav": GRAV_SIGNATURES, "rh": RH_SIGNATURES, "he": RH_SIGNATURES + HE_SIGNATURES}[key]
     for name, res, args in SIGNATURES + extra:
         fn = getattr(L, name)
         fn.restype = res

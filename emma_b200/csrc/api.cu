@@ -38,7 +38,7 @@ cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *g
 cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s,
                           bool grav);
 cudaError_t launch_dropin_base(const double *wb, double *base, long long n8, const double *exc, long long nexc, int nsm,
-                               cudaStream_t s, int np);
+                               cudaStream_t s, int np, int rec);
 bool resident_level(struct OCT **firstoct, int level, const HostLevel **h, const double **W, const uint8_t **split,
                     cudaStream_t *stream, int *nsm);
 void release_dump_staging();
@@ -160,19 +160,32 @@ constexpr int kDropinGrav = 1;
 constexpr int kDropinGrav = 0;
 #endif
 // ... and those of a library built for its -DWRADHYD layout (libemmahydro_rh.so)
-// advance the ionised density dX too (in the resident mode the sixth plane of every
-// level state).
-#ifdef EMMA_WRADHYD
+// advance the ionised density dX too, and with -DHELIUM (libemmahydro_he.so) the
+// helium densities dXHE, dXXHE as well (in the resident mode planes 6.. of every
+// level state).  kDropinTracer: the number of tracers.
+#if defined(EMMA_HELIUM)
+constexpr int kDropinTracer = 3;
+#elif defined(EMMA_WRADHYD)
 constexpr int kDropinTracer = 1;
 #else
 constexpr int kDropinTracer = 0;
 #endif
+// the kernel variant of the tracer builds
+constexpr unsigned kLaunchTracers = kDropinTracer == 3 ? kLaunchHelium : (kDropinTracer == 1 ? kLaunchTracer : 0u);
+#ifdef EMMA_WRADHYD
+// tracer t of a state: dX, then (-DHELIUM) dXHE, dXXHE, which follow it in struct Wtype
+inline double &tracer(struct Wtype &W, int t) { return (&W.dX)[t]; }
+inline double tracer(const struct Wtype &W, int t) { return (&W.dX)[t]; }
+#endif
 
 // Planes of a correction buffer: d, du, dv, dw, E, with dual energy eint, in a
-// tracer build dX (plane kXPlane; the tracer build has no dual energy).
+// tracer build the tracers (planes kXPlane..; the tracer builds have no dual energy).
 inline long long cplanes() { return (g.opt.dual_energy ? 6 : 5) + kDropinTracer; }
-// Planes of a drop-in level's `field` upload and of its base fieldnew: d,u,v,w,p,E (+ dX)
+// Planes of a drop-in level's `field` upload and of its base fieldnew: d,u,v,w,p,E (+ tracers)
 constexpr int kFieldPlanes = 6 + kDropinTracer;
+// doubles per record of a drop-in cell whose fieldnew differs: the cell, then the
+// kFieldPlanes values (at least 8, the record of the builds without tracers)
+constexpr int kExcRec = kFieldPlanes + 1 > 8 ? kFieldPlanes + 1 : 8;
 static_assert(!kDropinTracer || kXPlane == 5, "tracer corrections follow the five conserved planes");
 
 void fail(unsigned bit, const std::string &msg) {
@@ -563,7 +576,7 @@ inline void finish_prims(struct Wtype &W) {
 // Packs octs [a, b) of a level in one pass over their cells: `field` with E into
 // the 6 planes of pw (planes of 8*noct); every cell whose `fieldnew` differs from
 // `field` (after clean_new_hydro: the cells a finer level corrected) appends
-// {cell, d, u, v, w, p, E, 0} of its fieldnew to exc.
+// {cell, d, u, v, w, p, E, tracers} of its fieldnew to exc (kExcRec values).
 void pack_cells(const HostLevel &h, long long a, long long b, double *pw, std::vector<double> &exc) {
   const long long n8 = 8LL * h.noct;
   for (long long i = a; i < b; i++) {
@@ -577,18 +590,17 @@ void pack_cells(const HostLevel &h, long long a, long long b, double *pw, std::v
       pw[3 * n8 + k] = W.w;
       pw[4 * n8 + k] = W.p;
       pw[5 * n8 + k] = W.E;
+      double e[kExcRec] = {(double)k, N.d, N.u, N.v, N.w, N.p, N.E};
+      bool tdiff = false;
 #ifdef EMMA_WRADHYD
-      pw[6 * n8 + k] = W.dX;
-      const bool tdiff = std::memcmp(&W.dX, &N.dX, sizeof(double)) != 0;
-      const double nx = N.dX;
-#else
-      const bool tdiff = false;
-      const double nx = 0.;
-#endif
-      if (std::memcmp(&W, &N, 5 * sizeof(double)) != 0 || std::memcmp(&W.E, &N.E, sizeof(double)) != 0 || tdiff) {
-        const double e[8] = {(double)k, N.d, N.u, N.v, N.w, N.p, N.E, nx};
-        exc.insert(exc.end(), e, e + 8);
+      for (int t = 0; t < kDropinTracer; t++) {
+        pw[(6 + t) * n8 + k] = tracer(W, t);
+        tdiff = tdiff || std::memcmp(&W.dX + t, &N.dX + t, sizeof(double)) != 0;
+        e[7 + t] = tracer(N, t);
       }
+#endif
+      if (std::memcmp(&W, &N, 5 * sizeof(double)) != 0 || std::memcmp(&W.E, &N.E, sizeof(double)) != 0 || tdiff)
+        exc.insert(exc.end(), e, e + kExcRec);
     }
   }
 }
@@ -609,7 +621,7 @@ void unpack_cells(const HostLevel &h, long long a, long long b, const double *p,
       W.w = p[3 * n8 + k];
       W.p = p[4 * n8 + k];
 #ifdef EMMA_WRADHYD
-      W.dX = p[5 * n8 + k];
+      for (int t = 0; t < kDropinTracer; t++) tracer(W, t) = p[(5 + t) * n8 + k];
 #endif
       finish_prims(W);
       if (also_field) o->cell[c].field = W;
@@ -722,8 +734,8 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
   // tracer build their own
   if (grav || (d_lv == g.res.d_lv && g.res.host.grav)) shapes |= kLaunchGrav;
   if (g.opt.dual_energy) shapes |= kLaunchDual;
-  if (kDropinTracer) shapes |= kLaunchTracer;
-  const int cnz = (d_lv == g.res.d_lv && !(shapes & (kLaunchGrav | kLaunchDual | kLaunchTracer)))
+  shapes |= kLaunchTracers;
+  const int cnz = (d_lv == g.res.d_lv && !(shapes & (kLaunchGrav | kLaunchDual | kLaunchTracer | kLaunchHelium)))
                       ? column_nz(col_level) : 0;
   cudaError_t e = (cnz > 0) ? launch_column(col_level, cnz, gate, fuse_cfl)
                   : (g.opt.precision == EMMA_PREC_MIXED)
@@ -1141,9 +1153,9 @@ bool autotune_tree(Tree &t, int shape_req) {
       BatchArgs probe{};
       if (ok)
         ok = ck((g.opt.precision == EMMA_PREC_MIXED)
-                    ? launch_level_f32(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u) |
+                    ? launch_level_f32(probe, (1u << s) | kLaunchTracers | (t.host.grav ? kLaunchGrav : 0u) |
                                                   (g.opt.dual_energy ? kLaunchDual : 0u), g.nsm, 0, g.stream, &occ)
-                    : launch_level_fp64(probe, (1u << s) | (t.host.grav ? kLaunchGrav : 0u) |
+                    : launch_level_fp64(probe, (1u << s) | kLaunchTracers | (t.host.grav ? kLaunchGrav : 0u) |
                                                    (g.opt.dual_energy ? kLaunchDual : 0u), g.nsm, 0, g.stream, &occ),
                 "occupancy");
       for (int c = 1; ok && c <= std::min(occ, 4); c++) {
@@ -1328,16 +1340,16 @@ int emma_hydro_fields_upload(struct OCT **firstoct) {
     if (h.noct == 0) continue;
     double *W = current_state(L);
     if (W == nullptr) return EMMA_ST_CUDA;
-    // d,u,v,w,p (tracer builds: and dX, the sixth plane of a resident state)
+    // d,u,v,w,p (tracer builds: and the tracers, planes 6.. of a resident state)
     const size_t bytes = sizeof(double) * (5 + kDropinTracer) * 8 * (size_t)h.noct;
     if (!ensure_pin(bytes)) return EMMA_ST_CUDA;
     pack_level(h, 0, g.pin);
 #ifdef EMMA_WRADHYD
-    {
-      double *px = g.pin + 5 * 8LL * h.noct;
+    for (int t = 0; t < kDropinTracer; t++) {
+      double *px = g.pin + (5 + t) * 8LL * h.noct;
       parallel_for(h.noct, [&](long long a0, long long b0) {
         for (long long i = a0; i < b0; i++)
-          for (int c = 0; c < 8; c++) px[8 * i + c] = h.octs[i]->cell[c].field.dX;
+          for (int c = 0; c < 8; c++) px[8 * i + c] = tracer(h.octs[i]->cell[c].field, t);
       });
     }
 #endif
@@ -1398,7 +1410,7 @@ int emma_hydro_tree_download(struct OCT **firstoct) {
           W.w = p[3 * n8 + k];
           W.p = p[4 * n8 + k];
 #ifdef EMMA_WRADHYD
-          W.dX = p[5 * n8 + k];
+          for (int t = 0; t < kDropinTracer; t++) tracer(W, t) = p[(5 + t) * n8 + k];
 #endif
           finish_prims(W);
           if (o->cell[c].child != nullptr) W.a = 0.;  // split cells: as the reference's averaging leaves them
@@ -1877,8 +1889,8 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
   {
     // the base fieldnew: field, then the cells where it differs
     size_t nexc = 0;
-    for (auto &e : g.exc) nexc += e.size() / 8;
-    const size_t eb = sizeof(double) * 8 * std::max<size_t>(nexc, 1);
+    for (auto &e : g.exc) nexc += e.size() / kExcRec;
+    const size_t eb = sizeof(double) * kExcRec * std::max<size_t>(nexc, 1);
     if (eb > g.pin_exc_bytes) {
       if (g.pin_exc) cudaFreeHost(g.pin_exc);
       g.pin_exc = nullptr;
@@ -1899,13 +1911,13 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
       at += e.size();
     }
     if (nexc > 0 &&
-        !ck(cudaMemcpyAsync(g.d_exc, g.pin_exc, sizeof(double) * 8 * nexc, cudaMemcpyHostToDevice, g.stream),
+        !ck(cudaMemcpyAsync(g.d_exc, g.pin_exc, sizeof(double) * kExcRec * nexc, cudaMemcpyHostToDevice, g.stream),
             "H2D exceptions"))
       return 0;
-    if (!ck(launch_dropin_base(d.WB, d.B, n8, g.d_exc, (long long)nexc, g.nsm, g.stream, kFieldPlanes),
+    if (!ck(launch_dropin_base(d.WB, d.B, n8, g.d_exc, (long long)nexc, g.nsm, g.stream, kFieldPlanes, kExcRec),
             "base launch"))
       return 0;
-    g.h2d_bytes += (long long)(sizeof(double) * 8 * nexc);
+    g.h2d_bytes += (long long)(sizeof(double) * kExcRec * nexc);
   }
   if (d.az != nullptr) {  // dual energy: the split cells' stored sound speeds of 0
     uint8_t *pz = reinterpret_cast<uint8_t *>(pst + 4);
@@ -1919,16 +1931,18 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
       return 0;
     g.h2d_bytes += (long long)sizeof(double) * 5 * nc8;
 #ifdef EMMA_WRADHYD
-    // the coarser level's dX, for the fractions of its injected cells
+    // the coarser level's tracers, for the fractions of its injected cells
     double *px = pc + 5 * nc8;
     parallel_for(hc.noct, [&](long long a0, long long b0) {
       for (long long i = a0; i < b0; i++)
-        for (int c = 0; c < 8; c++) px[8 * i + c] = hc.octs[i]->cell[c].field.dX;
+        for (int c = 0; c < 8; c++)
+          for (int t = 0; t < kDropinTracer; t++) px[t * nc8 + 8 * i + c] = tracer(hc.octs[i]->cell[c].field, t);
     });
-    if (dc.X == nullptr ||
-        !ck(cudaMemcpyAsync(dc.X, px, sizeof(double) * nc8, cudaMemcpyHostToDevice, g.stream), "H2D Xc"))
+    if (dc.X == nullptr || !ck(cudaMemcpyAsync(dc.X, px, sizeof(double) * kDropinTracer * nc8, cudaMemcpyHostToDevice,
+                                               g.stream),
+                               "H2D Xc"))
       return 0;
-    g.h2d_bytes += (long long)sizeof(double) * nc8;
+    g.h2d_bytes += (long long)sizeof(double) * kDropinTracer * nc8;
 #endif
     if (!ck(cudaMemsetAsync(dc.C, 0, sizeof(double) * ncp * nc8, g.stream), "memset Cc")) return 0;
   }
@@ -2061,7 +2075,8 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
       W.E = UE;
       W.a = std::sqrt(kG * W.p / dl);
 #ifdef EMMA_WRADHYD
-      W.dX = W.dX + p[kXPlane * nc8 + k];  // U.dX = W.dX, corrected, U2W (src/hydro_utils.c:3277)
+      for (int t = 0; t < kDropinTracer; t++)  // U.dT = W.dT, corrected, U2W (src/hydro_utils.c:3277-3281)
+        tracer(W, t) = tracer(W, t) + p[(kXPlane + t) * nc8 + k];
 #endif
     }
   }
@@ -2087,7 +2102,7 @@ static int dropin_advance(struct OCT **firstoct, int level, struct CPUINFO *cpu,
             W.w += Wc.w * 0.125;
             W.p += Wc.p * 0.125;
 #ifdef EMMA_WRADHYD
-            W.dX += Wc.dX * 0.125;  // src/hydro_utils.c:3460
+            for (int t = 0; t < kDropinTracer; t++) tracer(W, t) += tracer(Wc, t) * 0.125;  // src/hydro_utils.c:3446-3460
 #endif
           }
           W.E = W.p / (kG - 1.) + 0.5 * W.d * (W.u * W.u + W.v * W.v + W.w * W.w);

@@ -134,9 +134,9 @@ __global__ void dropin_base_copy(const double *wb, double *base, long long n) {
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     base[i] = wb[i];
 }
-__global__ void dropin_base_scatter(double *base, long long n8, const double *exc, long long nexc, int np) {
+__global__ void dropin_base_scatter(double *base, long long n8, const double *exc, long long nexc, int np, int rec) {
   for (long long j = blockIdx.x * (long long)blockDim.x + threadIdx.x; j < nexc; j += (long long)gridDim.x * blockDim.x) {
-    const double *e = exc + 8 * j;
+    const double *e = exc + (long long)rec * j;
     const long long k = (long long)e[0];
     if (k < 0 || k >= n8) continue;
     for (int v = 0; v < np; v++) base[v * n8 + k] = e[1 + v];
@@ -144,8 +144,8 @@ __global__ void dropin_base_scatter(double *base, long long n8, const double *ex
 }
 
 cudaError_t launch_dropin_base(const double *wb, double *base, long long n8, const double *exc, long long nexc, int nsm,
-                               cudaStream_t s, int np) {
-  if (np < 6 || np > 7) return cudaErrorInvalidValue;  // exception records hold 7 values
+                               cudaStream_t s, int np, int rec) {
+  if (np < 6 || np > 9 || rec < np + 1) return cudaErrorInvalidValue;  // a record: the cell, then np values
   const long long n = np * n8;
   long long blocks = (n + 255) / 256;
   if (blocks > 8LL * nsm) blocks = 8LL * nsm;
@@ -153,7 +153,7 @@ cudaError_t launch_dropin_base(const double *wb, double *base, long long n8, con
   if (nexc > 0) {
     long long b2 = (nexc + 255) / 256;
     if (b2 > 8LL * nsm) b2 = 8LL * nsm;
-    dropin_base_scatter<<<(unsigned)b2, 256, 0, s>>>(base, n8, exc, nexc, np);
+    dropin_base_scatter<<<(unsigned)b2, 256, 0, s>>>(base, n8, exc, nexc, np, rec);
   }
   return cudaGetLastError();
 }

@@ -22,9 +22,19 @@ namespace emma {
 
 constexpr double kGam = 5. / 3.;   // GAMMA, src/param.h:4
 constexpr double kPmin = 1e-10;    // PMIN, src/param.h:20
-constexpr double kYhe = 0.;        // YHE without -DHELIUM / -DHESIMPLE, src/param.h:53 (tracer builds)
 constexpr double kErrTol = 1e-10;  // ERRTOL, src/hydro_utils.c:18
 constexpr int kNiterMax = 10;      // NITERMAX, src/hydro_utils.c:17
+
+// Tracers advected with the gas by the -DWRADHYD builds: NT = 1, the ionised
+// density dX, with the helium mass fraction YHE = 0 (no -DHELIUM, src/param.h:53);
+// NT = 3, dX and the singly and doubly ionised helium densities dXHE, dXXHE, with
+// YHE = 0.24 (-DHELIUM, src/param.h:48).  Tracer t is a part of the mass fraction
+// frac(t): hydrogen 1 - YHE, helium YHE (src/hydro_utils.c:1244-1252).
+template <int NT>
+struct Tracers {
+  static constexpr double kYhe = (NT == 3) ? 0.24 : 0.;
+  __host__ __device__ static constexpr double frac(int t) { return t == 0 ? 1. - kYhe : kYhe; }
+};
 
 // status bits (mirrors EMMA_ST_* of emma_hydro.h)
 constexpr unsigned kStNegDensity = 0x01, kStNegPstar = 0x02, kStNan = 0x04, kStTree = 0x08, kStTimeout = 0x40;
@@ -232,6 +242,9 @@ struct MathF64 {
   // du (dual-energy builds, optional): from the state Us of the branch taken (the
   // upwind or the star state), du[0] = Us.m_n / Us.d and du[1] = ebar =
   // Us.E - |Us.m|^2 / (2 Us.d) (src/hydro_utils.c:2126-2128).
+  // xs, fx (tracer builds, optional): the centre fractions of the NT tracers,
+  // xs[2 t] left and xs[2 t + 1] right, and their fluxes fx[t].
+  template <int NT = 1>
   static __device__ __forceinline__ void hllc(const double WL[7], const double WR[7], int n, double F[5],
                                               unsigned &st, double *du = nullptr, const double *xs = nullptr,
                                               double *fx = nullptr) {
@@ -241,7 +254,8 @@ struct MathF64 {
     rotate(WL, n, rL);
     rotate(WR, n, rR);
     if (du != nullptr) du[0] = du[1] = 0.;
-    if (fx != nullptr) *fx = 0.;
+    if (fx != nullptr)
+      for (int t = 0; t < NT; t++) fx[t] = 0.;
     if (SL >= 0. || SR <= 0.) {
       const double *r = (SL >= 0.) ? rL : rR;
       euler_rot(r, G);
@@ -250,10 +264,11 @@ struct MathF64 {
         du[0] = mn / r[0];
         du[1] = (r[5] - 0.5 * r[6] / r[0]);
       }
-      if (fx != nullptr) {  // tracer: face dX from the centre fraction, flux du dX / d
-        const double dX = (r[0] * (1. - kYhe)) * xs[(SL >= 0.) ? 0 : 1];
-        *fx = (r[0] * r[1]) * dX / r[0];
-      }
+      if (fx != nullptr)  // tracers: face values from the centre fractions, flux du dT / d
+        for (int t = 0; t < NT; t++) {
+          const double dT = (r[0] * Tracers<NT>::frac(t)) * xs[2 * t + ((SL >= 0.) ? 0 : 1)];
+          fx[t] = (r[0] * r[1]) * dT / r[0];
+        }
     } else {
       const bool left = (SL < 0.) && (ustar >= 0.);
       const bool right = (ustar <= 0.) && (SR > 0.);
@@ -269,10 +284,11 @@ struct MathF64 {
         G[2] += (fact * r[2] - d * r[2]) * S;
         G[3] += (fact * r[3] - d * r[3]) * S;
         G[4] += (fact * Es - E) * S;
-        if (fx != nullptr) {  // tracer flux with the star correction (src/hydro_utils.c:1534-1535)
-          const double dX = (d * (1. - kYhe)) * xs[left ? 0 : 1];
-          *fx = (d * un) * dX / d + (fact * dX / d - dX) * S;
-        }
+        if (fx != nullptr)  // tracer fluxes with the star correction (src/hydro_utils.c:1534-1539)
+          for (int t = 0; t < NT; t++) {
+            const double dT = (d * Tracers<NT>::frac(t)) * xs[2 * t + (left ? 0 : 1)];
+            fx[t] = (d * un) * dT / d + (fact * dT / d - dT) * S;
+          }
         if (du != nullptr) {  // the star state: momenta in x,y,z order for the sum of squares
           const double ds = fact * 1., mn = fact * ustar, m1 = fact * r[2], m2 = fact * r[3];
           const double mm = (n == 2) ? ((m1 * m1 + m2 * m2) + mn * mn) : ((mn * mn + m1 * m1) + m2 * m2);
@@ -366,6 +382,7 @@ struct MathF32 {
   // and ebar = Us.E - |Us.m|^2 / (2 Us.d), the latter in a form free of the
   // E - Ekin cancellation: p/(g-1) upwind, fact (p/((g-1) d) + (u*-u)((u*-u)/2 +
   // p/(d (S-u)))) in the star region (algebraically the reference's expression).
+  template <int NT = 1>
   static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st,
                                               float *du = nullptr, const float *xs = nullptr, float *fx = nullptr) {
     const float dL = WL[0], pL = WL[4], iL = WL[5], aL = WL[6];
@@ -433,12 +450,13 @@ struct MathF32 {
       G2 = side ? H2 : 0.f;
       G4 = side ? H4 : 0.f;
     }
-    if (fx != nullptr) {  // tracer: face dX from the centre fraction, flux du dX / d (+ star correction)
-      const float dX = d * (1.f - (float)kYhe) * xs[useL ? 0 : 1];
-      const float f6 = mn * dX * id;
-      const float h6 = f6 + (fact * dX * id - dX) * S;
-      *fx = star ? (side ? h6 : 0.f) : f6;
-    }
+    if (fx != nullptr)  // tracers: face values from the centre fractions, flux du dT / d (+ star correction)
+      for (int t = 0; t < NT; t++) {
+        const float dT = d * (float)Tracers<NT>::frac(t) * xs[2 * t + (useL ? 0 : 1)];
+        const float f6 = mn * dT * id;
+        const float h6 = f6 + (fact * dT * id - dT) * S;
+        fx[t] = star ? (side ? h6 : 0.f) : f6;
+      }
     if (du != nullptr) {
       const float ig = 1.f / (G - 1.f), dd = ustar - un;
       const float es = fact * (p * ig * id + dd * (0.5f * dd + fdiv(p, d * Smu)));

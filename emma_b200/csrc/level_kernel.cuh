@@ -171,10 +171,10 @@ __device__ __forceinline__ void slot_tables(unsigned char *tab) {
 }
 
 // Shared memory of one tile, after the slot tables.  DUAL: dual-energy builds add
-// the internal-energy flux and the normal star velocity of every face.  TRACER
-// (-DWRADHYD, not with DUAL): the ionised fraction of every staged cell and the
-// tracer flux of every face.
-template <class M, class G, bool DUAL = false, bool TRACER = false>
+// the internal-energy flux and the normal star velocity of every face.  NTR
+// tracers (-DWRADHYD: 1, with -DHELIUM: 3; not with DUAL): the fraction of every
+// tracer in every staged cell and the tracer fluxes of every face.
+template <class M, class G, bool DUAL = false, int NTR = 0>
 struct TileSmem {
   using R = typename M::R;
   static constexpr bool kF64 = sizeof(R) == 8;
@@ -206,10 +206,12 @@ struct TileSmem {
   static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
   static constexpr size_t off_F5 = off_end;                       // R [NF] (DUAL)
   static constexpr size_t off_S = a16(off_F5 + sizeof(R) * NF);  // R [NF] (DUAL)
-  static constexpr size_t off_X = off_end;                        // R [NBOX] (TRACER)
-  static constexpr size_t off_FX = a16(off_X + sizeof(R) * NBOX);  // R [NF] (TRACER)
-  static constexpr size_t bytes = DUAL ? a16(off_S + sizeof(R) * NF) : (TRACER ? a16(off_FX + sizeof(R) * NF) : off_end);
-  static_assert(!(DUAL && TRACER), "the tracer variant has no dual energy");
+  static constexpr size_t off_X = off_end;                              // R [NTR][NBOX]
+  static constexpr size_t off_FX = a16(off_X + sizeof(R) * NTR * NBOX);  // R [NTR][NF]
+  static constexpr size_t bytes =
+      DUAL ? a16(off_S + sizeof(R) * NF) : (NTR > 0 ? a16(off_FX + sizeof(R) * NTR * NF) : off_end);
+  static_assert(!(DUAL && NTR > 0), "the tracer variants have no dual energy");
+  static_assert(NTR == 0 || NTR == 1 || NTR == 3, "dX alone, or dX and the two helium tracers");
   static_assert(off_F1 + sizeof(R) * NF <= off_M, "face fluxes must fit in the staged box");
   // FP64 gravity kicks of the brick cells during P2/P3: R [3][kThreads] at the end of
   // the staged box, after the face fluxes
@@ -222,12 +224,14 @@ struct TileSmem {
 // the next tile's slot descriptors (next_tile >= 0: same level) are loaded
 // while this tile is reconstructed and solved, into the other descriptor
 // buffer; `cur`/`have` track which buffer holds the current tile's.
-template <class M, class G, bool GRAV, bool DUAL, bool TRACER = false>
+template <class M, class G, bool GRAV, bool DUAL, int NTR = 0>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
                                            const int next_tile, unsigned char *smem, const unsigned char *tab,
                                            unsigned &st, int &cur, bool &have, int &args_slot) {
   using R = typename M::R;
-  using SM = TileSmem<M, G, DUAL, TRACER>;
+  using SM = TileSmem<M, G, DUAL, NTR>;
+  constexpr bool TRACER = NTR > 0;
+  using TR = Tracers<(NTR > 0 ? NTR : 1)>;
   constexpr bool F64 = SM::kF64;
   constexpr int NS = SM::NS, NRING = SM::NRING;
   using V = Q4<R>;
@@ -249,8 +253,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   R *sF1 = reinterpret_cast<R *>(smem + SM::off_F1);
   R *sF5 = reinterpret_cast<R *>(smem + SM::off_F5);
   R *sS = reinterpret_cast<R *>(smem + SM::off_S);
-  R *sX = reinterpret_cast<R *>(smem + SM::off_X);    // TRACER: dX / (d (1 - YHE)) of the staged cells
-  R *sFX = reinterpret_cast<R *>(smem + SM::off_FX);  // TRACER: face fluxes of dX
+  R *sX = reinterpret_cast<R *>(smem + SM::off_X);    // tracers: dT / (d frac) of the staged cells
+  R *sFX = reinterpret_cast<R *>(smem + SM::off_FX);  // tracers: face fluxes
   // cells whose face states are built: leaves; dual-energy builds also split cells,
   // whose faces enter the p div(u) term (src/hydro_utils.c:2126-2129 sum every face)
   auto recon_ok = [](uint8_t f) { return DUAL ? (f & kFPresent) != 0 : f_ok(f); };
@@ -266,8 +270,9 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     args_slot = slot;
   }
   const long long N8 = 8LL * A.noct;
-  // TRACER: dX planes.  Drop-in levels (B set) name them; resident levels keep dX as
-  // the sixth plane of every state buffer, so that the schedule's buffer swaps carry it
+  // tracer planes (tracer t at plane offset t times the level's plane stride).
+  // Drop-in levels (B set) name them; resident levels keep them as planes 6.. of
+  // every state buffer, so that the schedule's buffer swaps carry them
   const bool res_tr = TRACER && A.B == nullptr;
   const double *Xs = res_tr ? A.W + 5 * N8 : A.X;
   const double *Xcs = res_tr ? (A.Wc != nullptr ? A.Wc + 5 * A.nc8 : nullptr) : A.Xc;
@@ -373,7 +378,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       }
       const int cmk = sCmk[sg];
       double x0[5], x1[5];
-      double t0 = 0., t1 = 0.;  // TRACER: dX of the two cells
+      double t0[NTR > 0 ? NTR : 1] = {}, t1[NTR > 0 ? NTR : 1] = {};  // tracers of the two cells
       if (cmk == 1) {  // injected coarser cell: one value for both children
         const bool inj = sf & kFInj;
         const double *p = (inj ? Wc : W) + (long long)sOb[sg];
@@ -382,8 +387,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         for (int v = 0; v < 5; v++) x0[v] = x1[v] = __ldg(p + v * stride);
         if constexpr (TRACER) {
           const double *px = inj ? Xcs : Xs;
-          if (px != nullptr) t0 = t1 = __ldg(px + (long long)sOb[sg]);
-          else st |= kStTree;
+          const long long ts = inj ? nc8 : N8;
+          if (px != nullptr) {
+#pragma unroll
+            for (int t = 0; t < NTR; t++) t0[t] = t1[t] = __ldg(px + t * ts + (long long)sOb[sg]);
+          } else {
+            st |= kStTree;
+          }
         }
       } else {
         unsigned code = (unsigned)q | (1u << 3);  // pair q, elements 0 and 1
@@ -400,17 +410,24 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         }
         if constexpr (TRACER) {
           if (!itp && Xs != nullptr) {
-            const double2 x = __ldg(reinterpret_cast<const double2 *>(Xs + (long long)sOb[sg] + 2 * (code & 3)));
-            t0 = e0 ? x.y : x.x;
-            t1 = e1 ? x.y : x.x;
+#pragma unroll
+            for (int t = 0; t < NTR; t++) {
+              const double2 x =
+                  __ldg(reinterpret_cast<const double2 *>(Xs + t * N8 + (long long)sOb[sg] + 2 * (code & 3)));
+              t0[t] = e0 ? x.y : x.x;
+              t1[t] = e1 ? x.y : x.x;
+            }
           } else {
             st |= kStTree;  // no tracer for interpolated coarser cells
           }
         }
       }
-      if constexpr (TRACER) {  // X0 = dX / (d (1 - YHE)) (src/hydro_utils.c:1245)
-        sX[b0] = (R)(t0 / (x0[0] * (1. - kYhe)));
-        sX[b0 + 1] = (R)(t1 / (x1[0] * (1. - kYhe)));
+      if constexpr (TRACER) {  // X0 = dT / (d frac) (src/hydro_utils.c:1245, 1248-1251)
+#pragma unroll
+        for (int t = 0; t < NTR; t++) {
+          sX[t * SM::NBOX + b0] = (R)(t0[t] / (x0[0] * (TR::frac(t))));
+          sX[t * SM::NBOX + b0 + 1] = (R)(t1[t] / (x1[0] * (TR::frac(t))));
+        }
       }
       V::st(sW, b0, SM::NBOX, (R)x0[0], (R)x0[1], (R)x0[2], (R)x0[3]);
       V::st(sW, b0 + 1, SM::NBOX, (R)x1[0], (R)x1[1], (R)x1[2], (R)x1[3]);
@@ -601,7 +618,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   // leaf of the tile on either side the face is not solved.
   auto solve_face = [&](int d, int e, int tL, int bL, int jL, int tR, int bR, int jR) {
     const uint8_t fL = sSt[bL], fR = sSt[bR];
-    R F[5] = {0, 0, 0, 0, 0}, du[2] = {0, 0}, fx = 0;
+    R F[5] = {0, 0, 0, 0, 0}, du[2] = {0, 0}, fx[NTR > 0 ? NTR : 1] = {};
     if ((f_tileleaf(fL) || f_tileleaf(fR)) && recon_ok(fL) && recon_ok(fR)) {
       R WL[7], WR[7];
       if (jL >= 0) ring_face(jL, WL);
@@ -609,8 +626,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       if (jR >= 0) ring_face(jR, WR);
       else brick_face(tR, bR, 2 * d, WR);
       if constexpr (TRACER) {
-        const R xs[2] = {sX[bL], sX[bR]};
-        M::hllc(WL, WR, d, F, st, nullptr, xs, &fx);
+        R xs[2 * NTR];
+#pragma unroll
+        for (int t = 0; t < NTR; t++) {
+          xs[2 * t] = sX[t * SM::NBOX + bL];
+          xs[2 * t + 1] = sX[t * SM::NBOX + bR];
+        }
+        M::template hllc<NTR>(WL, WR, d, F, st, nullptr, xs, fx);
       } else {
         M::hllc(WL, WR, d, F, st, DUAL ? du : nullptr);
       }
@@ -626,7 +648,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       sF5[e] = du[0] * du[1];  // (Us.m_n / Us.d) ebar (src/hydro_utils.c:2128)
       sS[e] = du[0];
     }
-    if constexpr (TRACER) sFX[e] = fx;
+    if constexpr (TRACER) {
+#pragma unroll
+      for (int t = 0; t < NTR; t++) sFX[t * SM::NF + e] = fx[t];
+    }
   };
 
   // ------------------------------------------------------------------ P2
@@ -755,17 +780,18 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       for (int v = 0; v < 5; v++) q[v] = __ldg(A.W + v * N8 + gi);
     }
     double Wout[5];
-    double Xout = 0.;  // TRACER: the new dX
+    double Xout[NTR > 0 ? NTR : 1] = {};  // the new tracers
     if (fme & kFSplit) {
       if constexpr (TRACER) {
-        // the children's mean (src/hydro_utils.c:3460) when the finer level is at hand
-        Xout = (Xs != nullptr) ? __ldg(Xs + gi) : 0.;
-        if (A.Wf != nullptr && res_tr) {
-          const long long ch = A.child[gi];
+        // the children's mean (src/hydro_utils.c:3446-3460) when the finer level is at hand
+        const long long ch = (A.Wf != nullptr && res_tr) ? A.child[gi] : -1;
+#pragma unroll
+        for (int t = 0; t < NTR; t++) {
+          Xout[t] = (Xs != nullptr) ? __ldg(Xs + t * N8 + gi) : 0.;
           if (ch >= 0) {
             double ax = 0.;
-            for (int i = 0; i < 8; i++) ax += __ldcg(A.Wf + 5 * A.nf8 + 8 * ch + i) * 0.125;
-            Xout = ax;
+            for (int i = 0; i < 8; i++) ax += __ldcg(A.Wf + (5 + t) * A.nf8 + 8 * ch + i) * 0.125;
+            Xout[t] = ax;
           }
         }
       }
@@ -932,20 +958,25 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         for (int v = 0; v < 3; v++) Wout[1 + v] += (-__ldg(A.F + v * N8 + gi) * A.dt);
       }
       if constexpr (TRACER) {
-        // dX: the caller's fieldnew (or field + corrections) plus the flux divergence
-        // in the faces' order (src/hydro_utils.c:3068, 3158), then the ceiling
-        // 0 <= dX <= d (1 - YHE) (:3197-3198)
-        double Ux = (A.BX != nullptr) ? A.BX[gi] : ((Xs != nullptr) ? __ldg(Xs + gi) : 0.);
-        if (A.BX == nullptr && A.C != nullptr) Ux += __ldcg(A.C + kXPlane * N8 + gi);
-        double dUx = 0., one = 1.;
+        // tracers: the caller's fieldnew (or field + corrections) plus the flux
+        // divergence in the faces' order (src/hydro_utils.c:3068-3072, 3158-3162),
+        // then dX in [0, d (1 - YHE)] and the helium densities below d YHE
+        // (:3197-3203)
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-          dUx += (double)sFX[face_of(k)] * dtsurdx * one;
-          one *= -1.;
+        for (int t = 0; t < NTR; t++) {
+          double Ux = (A.BX != nullptr) ? A.BX[t * N8 + gi] : ((Xs != nullptr) ? __ldg(Xs + t * N8 + gi) : 0.);
+          if (A.BX == nullptr && A.C != nullptr) Ux += __ldcg(A.C + (kXPlane + t) * N8 + gi);
+          double dUx = 0., one = 1.;
+#pragma unroll
+          for (int k = 0; k < 6; k++) {
+            dUx += (double)sFX[t * SM::NF + face_of(k)] * dtsurdx * one;
+            one *= -1.;
+          }
+          double x = Ux + dUx;
+          if (t == 0 && x < 0) x = 0.;
+          if (x > (Wout[0] * (TR::frac(t)))) x = Wout[0] * (TR::frac(t));
+          Xout[t] = x;
         }
-        Xout = Ux + dUx;
-        if (Xout < 0) Xout = 0.;
-        if (Xout > (Wout[0] * (1. - kYhe))) Xout = Wout[0] * (1. - kYhe);
       }
 
       // fine -> coarse correction into unsplit coarser neighbours (src/hydro_utils.c:3206-3295)
@@ -964,14 +995,20 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 #pragma unroll
         for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, F[v] * dtsurdx * one * 0.125);
         if constexpr (DUAL) atomicAdd(A.Cc + 5 * A.nc8 + cc, (double)sF5[face_of(k)] * dtsurdx * one * 0.125);
-        if constexpr (TRACER)
-          atomicAdd(A.Cc + kXPlane * A.nc8 + cc, (double)sFX[face_of(k)] * dtsurdx * one * 0.125);
+        if constexpr (TRACER) {
+#pragma unroll
+          for (int t = 0; t < NTR; t++)
+            atomicAdd(A.Cc + (kXPlane + t) * A.nc8 + cc, (double)sFX[t * SM::NF + face_of(k)] * dtsurdx * one * 0.125);
+        }
       }
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) A.Wn[v * N8 + gi] = Wout[v];
     if constexpr (TRACER) {
-      if (Xns != nullptr) Xns[gi] = Xout;
+      if (Xns != nullptr) {
+#pragma unroll
+        for (int t = 0; t < NTR; t++) Xns[t * N8 + gi] = Xout[t];
+      }
     }
     if (Bt.smax != nullptr) {
       // the next time step's CFL term of this cell, as L_comptstep_hydro evaluates it
@@ -1000,10 +1037,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 
 // Bytes of dynamic shared memory of a kernel handling the shapes in `shapes`
 // (bit i: kShapes[i]).
-template <class M, bool DUAL = false, bool TRACER = false>
+template <class M, bool DUAL = false, int NTR = 0>
 constexpr size_t level_smem_bytes(unsigned shapes) {
-  const size_t a = (shapes & 1u) ? TileSmem<M, GeomA, DUAL, TRACER>::bytes : 0,
-               b = (shapes & 2u) ? TileSmem<M, GeomB, DUAL, TRACER>::bytes : 0;
+  const size_t a = (shapes & 1u) ? TileSmem<M, GeomA, DUAL, NTR>::bytes : 0,
+               b = (shapes & 2u) ? TileSmem<M, GeomB, DUAL, NTR>::bytes : 0;
   return a > b ? a : b;
 }
 
@@ -1016,9 +1053,10 @@ constexpr size_t level_smem_bytes(unsigned shapes) {
 // (64 registers, 55 KB of shared memory); with 2x2x2 bricks shared memory
 // allows 2; the FP64 kernel 2 with 4x4x2 bricks (128 registers, 110 KB), 1 with
 // 2x2x2 bricks.
-template <class M, unsigned SHAPES, bool DUAL = false, bool TRACER = false>
-constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? ((SHAPES == 1u && !DUAL && !TRACER) ? 2 : 1)
-                                                         : (SHAPES == 1u ? ((DUAL || TRACER) ? 3 : 4) : 2);
+template <class M, unsigned SHAPES, bool DUAL = false, int NTR = 0>
+constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? ((SHAPES == 1u && !DUAL && NTR == 0) ? 2 : 1)
+                                                         : (SHAPES == 1u ? (NTR == 3 ? 2 : ((DUAL || NTR > 0) ? 3 : 4))
+                                                                         : (NTR == 3 ? 1 : 2));
 // 228 KB of shared memory per SM, 1 KB reserved per CTA
 static_assert(4 * (TileSmem<MathF32, GeomA>::bytes + 1024) <= 228 * 1024, "4 FP32 4x4x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF32, GeomB>::bytes + 1024) <= 228 * 1024, "2 FP32 2x2x2 CTAs per SM");
@@ -1026,12 +1064,16 @@ static_assert(2 * (TileSmem<MathF64, GeomA>::bytes + 1024) <= 228 * 1024, "2 FP6
 static_assert(3 * (TileSmem<MathF32, GeomA, true>::bytes + 1024) <= 228 * 1024, "3 dual-energy FP32 4x4x2 CTAs");
 static_assert(2 * (TileSmem<MathF32, GeomB, true>::bytes + 1024) <= 228 * 1024, "2 dual-energy FP32 2x2x2 CTAs");
 static_assert(TileSmem<MathF64, GeomB, true>::bytes + 1024 <= 227 * 1024, "a dual-energy FP64 2x2x2 CTA");
-static_assert(3 * (TileSmem<MathF32, GeomA, false, true>::bytes + 1024) <= 228 * 1024, "3 tracer FP32 4x4x2 CTAs");
-static_assert(2 * (TileSmem<MathF32, GeomB, false, true>::bytes + 1024) <= 228 * 1024, "2 tracer FP32 2x2x2 CTAs");
-static_assert(TileSmem<MathF64, GeomB, false, true>::bytes + 1024 <= 227 * 1024, "a tracer FP64 2x2x2 CTA");
+static_assert(3 * (TileSmem<MathF32, GeomA, false, 1>::bytes + 1024) <= 228 * 1024, "3 tracer FP32 4x4x2 CTAs");
+static_assert(2 * (TileSmem<MathF32, GeomB, false, 1>::bytes + 1024) <= 228 * 1024, "2 tracer FP32 2x2x2 CTAs");
+static_assert(TileSmem<MathF64, GeomB, false, 1>::bytes + 1024 <= 227 * 1024, "a tracer FP64 2x2x2 CTA");
+static_assert(2 * (TileSmem<MathF32, GeomA, false, 3>::bytes + 1024) <= 228 * 1024, "2 helium FP32 4x4x2 CTAs");
+static_assert(TileSmem<MathF32, GeomB, false, 3>::bytes + 1024 <= 227 * 1024, "a helium FP32 2x2x2 CTA");
+static_assert(TileSmem<MathF64, GeomA, false, 3>::bytes + 1024 <= 227 * 1024, "a helium FP64 4x4x2 CTA");
+static_assert(TileSmem<MathF64, GeomB, false, 3>::bytes + 1024 <= 227 * 1024, "a helium FP64 2x2x2 CTA");
 
-template <class M, unsigned SHAPES, bool GRAV, bool DUAL, bool TRACER = false>
-__global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL, TRACER>))
+template <class M, unsigned SHAPES, bool GRAV, bool DUAL, int NTR = 0>
+__global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL, NTR>))
     level_batch_kernel(const BatchArgs Bt) {
   extern __shared__ __align__(16) unsigned char smem[];
   if (Bt.gate != nullptr && *Bt.gate == 0) return;
@@ -1055,15 +1097,15 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL, TRACER>
     }
     const LevelArgs *gA = Bt.lv + slot;
     if constexpr (SHAPES == 1u) {
-      level_tile<M, GeomA, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+      level_tile<M, GeomA, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
     } else if constexpr (SHAPES == 2u) {
-      level_tile<M, GeomB, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
+      level_tile<M, GeomB, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
                                                args_slot);
     } else {
       if (gA->shape == 0)
-        level_tile<M, GeomA, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
+        level_tile<M, GeomA, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
       else
-        level_tile<M, GeomB, GRAV, DUAL, TRACER>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
+        level_tile<M, GeomB, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
                                                  args_slot);
     }
     __syncthreads();
@@ -1086,7 +1128,7 @@ namespace {
 
 // Launch of a work list on a persistent grid of ctas_per_sm CTAs per SM (0 or
 // above the occupancy limit: the limit), so that every CTA is co-resident.
-template <class M, unsigned SHAPES, bool GRAV, bool DUAL, bool TRACER = false>
+template <class M, unsigned SHAPES, bool GRAV, bool DUAL, int NTR = 0>
 cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cudaStream_t s, int *occupancy) {
   // per device: the shared-memory limit is a per-device function attribute, and the
   // co-residency of the persistent grid rests on that device's own occupancy
@@ -1097,8 +1139,8 @@ cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cu
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
   int &occ = occ_dev[dev];
-  auto k = level_batch_kernel<M, SHAPES, GRAV, DUAL, TRACER>;
-  constexpr size_t bytes = level_smem_bytes<M, DUAL, TRACER>(SHAPES);
+  auto k = level_batch_kernel<M, SHAPES, GRAV, DUAL, NTR>;
+  constexpr size_t bytes = level_smem_bytes<M, DUAL, NTR>(SHAPES);
   if (occ == 0) {
     e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
     if (e != cudaSuccess) return e;
@@ -1120,11 +1162,14 @@ cudaError_t launch_level_shapes(const BatchArgs &a, int nsm, int ctas_per_sm, cu
 template <class M>
 cudaError_t launch_level_any(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
                              int *occupancy) {
-  constexpr unsigned G = kLaunchGrav, D = kLaunchDual, T = kLaunchTracer;
+  constexpr unsigned G = kLaunchGrav, D = kLaunchDual, T = kLaunchTracer, H = kLaunchHelium;
   switch (shapes) {
-    case 1u | T: return launch_level_shapes<M, 1u, false, false, true>(a, nsm, ctas_per_sm, s, occupancy);
-    case 2u | T: return launch_level_shapes<M, 2u, false, false, true>(a, nsm, ctas_per_sm, s, occupancy);
-    case 3u | T: return launch_level_shapes<M, 3u, false, false, true>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u | T: return launch_level_shapes<M, 1u, false, false, 1>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u | T: return launch_level_shapes<M, 2u, false, false, 1>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u | T: return launch_level_shapes<M, 3u, false, false, 1>(a, nsm, ctas_per_sm, s, occupancy);
+    case 1u | H: return launch_level_shapes<M, 1u, false, false, 3>(a, nsm, ctas_per_sm, s, occupancy);
+    case 2u | H: return launch_level_shapes<M, 2u, false, false, 3>(a, nsm, ctas_per_sm, s, occupancy);
+    case 3u | H: return launch_level_shapes<M, 3u, false, false, 3>(a, nsm, ctas_per_sm, s, occupancy);
     case 1u: return launch_level_shapes<M, 1u, false, false>(a, nsm, ctas_per_sm, s, occupancy);
     case 2u: return launch_level_shapes<M, 2u, false, false>(a, nsm, ctas_per_sm, s, occupancy);
     case 3u: return launch_level_shapes<M, 3u, false, false>(a, nsm, ctas_per_sm, s, occupancy);

@@ -45,6 +45,9 @@ constexpr unsigned kLaunchDual = 8u;
 // ... and the tracer variant (-DWRADHYD: the advected ionised density dX; its
 // corrections are plane kXPlane of Cc).  Not combined with gravity or dual energy.
 constexpr unsigned kLaunchTracer = 16u;
+// ... and its -DHELIUM variant: dX and the helium densities dXHE, dXXHE (corrections
+// in planes kXPlane .. kXPlane + 2 of Cc).
+constexpr unsigned kLaunchHelium = 32u;
 constexpr int kXPlane = 5;
 constexpr BrickShape kShapes[kNumShapes] = {{4, 4, 2, 1}, {2, 2, 2, 4}};
 static_assert(kShapes[0].nb * 8 * kShapes[0].octs() == kThreads, "one thread per brick cell");

@@ -27,6 +27,9 @@
 #ifdef EMMA_WRADHYD
 #include "emma_hydro_rh.h"
 #endif
+#ifdef EMMA_HELIUM
+#include "emma_hydro_he.h"
+#endif
 
 struct EmmaTree {
   // octs live in fixed-size blocks so that pointers stay valid as the tree grows
@@ -250,6 +253,30 @@ void emma_tree_get_tracer(struct EmmaTree *t, int level, int which, double *out)
   long long i = 0;
   for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
     for (int c = 0; c < 8; c++) out[8 * i + c] = which ? o->cell[c].fieldnew.dX : o->cell[c].field.dX;
+}
+#endif
+
+#ifdef EMMA_HELIUM
+// tracer `tr` (0: dX, 1: dXHE, 2: dXXHE, consecutive in struct Wtype)
+void emma_tree_set_tracer_n(struct EmmaTree *t, int level, int tr, const double *x) {
+  if (tr < 0 || tr > 2) return;
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) (&o->cell[c].field.dX)[tr] = (&o->cell[c].fieldnew.dX)[tr] = x[8 * i + c];
+}
+
+void emma_tree_put_tracer_n(struct EmmaTree *t, int level, int tr, int which, const double *x) {
+  if (tr < 0 || tr > 2) return;
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) (&(which ? o->cell[c].fieldnew : o->cell[c].field).dX)[tr] = x[8 * i + c];
+}
+
+void emma_tree_get_tracer_n(struct EmmaTree *t, int level, int tr, int which, double *out) {
+  if (tr < 0 || tr > 2) return;
+  long long i = 0;
+  for (struct OCT *o = t->first[level - 1]; o != nullptr; o = o->next, i++)
+    for (int c = 0; c < 8; c++) out[8 * i + c] = (&(which ? o->cell[c].fieldnew : o->cell[c].field).dX)[tr];
 }
 #endif
 

@@ -43,7 +43,7 @@ class ResidentHydro:
         self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
         self.precision = precision
         # a tree of the -DWRADHYD layout runs on libemmahydro_rh.so (its tracer advanced too)
-        self._L = L = lib("rh" if getattr(tree, "rh", False) else False)
+        self._L = L = lib("he" if getattr(tree, "he", False) else ("rh" if getattr(tree, "rh", False) else False))
         o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity, dual=dual,
                     column=column)
         check(L.emma_hydro_init(ctypes.byref(o)), "init")

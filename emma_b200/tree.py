@@ -16,14 +16,16 @@ CELL_OFF = np.array([[c % 2, (c // 2) % 2, c // 4] for c in range(8)], dtype=np.
 class OctTree:
     """An EMMA oct tree in host memory (levels lcoarse..lmax are hydro levels)."""
 
-    def __init__(self, lcoarse, lmax, ngridmax=0, grav=False, rh=False):
+    def __init__(self, lcoarse, lmax, ngridmax=0, grav=False, rh=False, he=False):
         """grav: the reference's -DWGRAV cell layout (built by libemmahydro_grav.so),
         for the gravity-coupled drop-in entries; rh: its -DWRADHYD layout (the cells
-        carry the ionised density dX; libemmahydro_rh.so)."""
-        assert not (grav and rh), "one cell layout at a time"
+        carry the ionised density dX; libemmahydro_rh.so); he: its -DWRADHYD -DHELIUM
+        layout (dX and the helium densities dXHE, dXXHE; libemmahydro_he.so)."""
+        assert (bool(grav) + bool(rh) + bool(he)) <= 1, "one cell layout at a time"
         self.lcoarse, self.lmax = lcoarse, lmax
-        self.grav, self.rh = grav, rh
-        self._L = lib("rh" if rh else grav)
+        self.grav, self.rh, self.he = grav, rh or he, he
+        self.ntracers = 3 if he else (1 if rh else 0)
+        self._L = lib("he" if he else ("rh" if rh else grav))
         self._t = self._L.emma_tree_create(lcoarse, lmax, ngridmax)
         if not self._t:
             raise RuntimeError("emma_tree_create failed")
@@ -92,6 +94,24 @@ class OctTree:
         a = np.ascontiguousarray(dX, dtype=np.float64)
         assert a.size == 8 * self.noct(level)
         self._L.emma_tree_put_tracer(self._t, level, which, ptr(a))
+
+    def set_tracer_n(self, level, t, x):
+        """Tracer t (0: dX; he trees 1: dXHE, 2: dXXHE) of field and fieldnew."""
+        assert t < self.ntracers, "the cell layout has no such tracer"
+        if not self.he:
+            return self.set_tracer(level, x)
+        a = np.ascontiguousarray(x, dtype=np.float64)
+        assert a.size == 8 * self.noct(level)
+        self._L.emma_tree_set_tracer_n(self._t, level, t, ptr(a))
+
+    def get_tracer_n(self, level, t, which=0):
+        assert t < self.ntracers, "the cell layout has no such tracer"
+        if not self.he:
+            return self.get_tracer(level, which)
+        out = np.zeros(8 * self.noct(level))
+        if out.size:
+            self._L.emma_tree_get_tracer_n(self._t, level, t, which, ptr(out))
+        return out
 
     def get_tracer(self, level, which=0):
         assert self.rh, "only the -DWRADHYD layout has dX"

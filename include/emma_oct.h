@@ -4,13 +4,16 @@
  * -DWRADHYD), REAL = double, NVAR = 6; with EMMA_WGRAV defined, for the
  * reference's -DWGRAV build (libemmahydro_grav.so); with EMMA_WRADHYD defined,
  * for its -DWRADHYD build without -DHELIUM (NVAR = 7: the ionised density dX
- * follows E in Wtype; libemmahydro_rh.so).
+ * follows E in Wtype; libemmahydro_rh.so); with EMMA_HELIUM defined too, for its
+ * -DWRADHYD -DHELIUM build (NVAR = 9: dX, then the singly and doubly ionised
+ * helium densities dXHE, dXXHE; libemmahydro_he.so).
  *
  * This is an interface, not an implementation: libemmahydro reads and writes the
  * caller's tree in place, so the field order, types and padding must be exactly
  * those of the reference (src/prototypes.h:611 Wtype, :653 Utype, :825 CELL,
  * :1028 OCT).  Sizes are checked at compile time: CELL 136 B, OCT 1200 B
- * (EMMA_WGRAV: CELL 192 B, OCT 1648 B; EMMA_WRADHYD: CELL 152 B, OCT 1328 B).
+ * (EMMA_WGRAV: CELL 192 B, OCT 1648 B; EMMA_WRADHYD: CELL 152 B, OCT 1328 B;
+ * EMMA_WRADHYD + EMMA_HELIUM: CELL 184 B, OCT 1584 B).
  * Only the members the hydro path uses are named; nothing else is assumed.
  */
 #ifndef EMMA_OCT_H
@@ -28,8 +31,15 @@ struct Wtype {           /* primitive state of a cell, src/prototypes.h:611 */
   REAL E;                /* total energy density */
 #ifdef EMMA_WRADHYD
   REAL dX;               /* ionised density, advected with the gas */
+#ifdef EMMA_HELIUM
+  REAL dXHE, dXXHE;      /* singly and doubly ionised helium densities */
+#endif
 #endif
 };
+
+#if defined(EMMA_HELIUM) && !defined(EMMA_WRADHYD)
+#error "EMMA_HELIUM extends the -DWRADHYD layout: define EMMA_WRADHYD too"
+#endif
 
 #if defined(EMMA_WGRAV) && defined(EMMA_WRADHYD)
 #error "libemmahydro is built for one of the -DWGRAV and -DWRADHYD layouts at a time"
@@ -80,6 +90,8 @@ struct HGRID;
  * also carry f[3] with -DWGRAV; NVAR 7 with -DWRADHYD) */
 #if defined(EMMA_WGRAV)
 #define EMMA_SIZEOF_HGRID 21760
+#elif defined(EMMA_HELIUM)
+#define EMMA_SIZEOF_HGRID 23104
 #elif defined(EMMA_WRADHYD)
 #define EMMA_SIZEOF_HGRID 18752
 #else
@@ -93,6 +105,9 @@ struct HGRID;
 #if defined(EMMA_WGRAV)
 #define EMMA_SIZEOF_CELL 192
 #define EMMA_SIZEOF_OCT 1648
+#elif defined(EMMA_HELIUM)
+#define EMMA_SIZEOF_CELL 184
+#define EMMA_SIZEOF_OCT 1584
 #elif defined(EMMA_WRADHYD)
 #define EMMA_SIZEOF_CELL 152
 #define EMMA_SIZEOF_OCT 1328

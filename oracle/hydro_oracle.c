@@ -39,10 +39,22 @@
 #define ERR_TOL 1e-10     /* ERRTOL, src/hydro_utils.c:18 */
 
 /* ---- memory layout of the reference tree (src/prototypes.h:611,825,1028) */
-#ifdef ORC_WRADHYD
+#if defined(ORC_HELIUM) && !defined(ORC_WRADHYD)
+#error "ORC_HELIUM extends the -DWRADHYD layout (build with ORC_WRADHYD too)"
+#endif
+#ifdef ORC_HELIUM
+/* -DWRADHYD -DHELIUM: the ionised hydrogen density dX and the singly and doubly
+ * ionised helium densities dXHE, dXXHE, advected with the gas (NVAR 9,
+ * src/prototypes.h:62-66); YHE = 0.24 (src/param.h:47-48) */
+#define YHE_ (0.24)
+#define NTR 3
+typedef struct { double d, u, v, w, p, a, E, dX, dXHE, dXXHE; } oW;      /* struct Wtype */
+typedef struct { double d, du, dv, dw, E, eint, dX, dXHE, dXXHE; } oU;  /* struct Utype */
+#elif defined(ORC_WRADHYD)
 /* -DWRADHYD: the ionised density dX, advected with the gas (NVAR 7; YHE = 0
  * without -DHELIUM / -DHESIMPLE, src/param.h:47-54) */
 #define YHE_ (0.)
+#define NTR 1
 typedef struct { double d, u, v, w, p, a, E, dX; } oW;      /* struct Wtype */
 typedef struct { double d, du, dv, dw, E, eint, dX; } oU;  /* struct Utype */
 #else
@@ -76,12 +88,23 @@ typedef struct oOct {
 #elif defined(ORC_WGRAV)
 _Static_assert(sizeof(oCell) == 192, "CELL layout (-DWGRAV)");
 _Static_assert(sizeof(oOct) == 1648, "OCT layout (-DWGRAV)");
+#elif defined(ORC_HELIUM)
+_Static_assert(sizeof(oCell) == 184, "CELL layout (-DWRADHYD -DHELIUM)");
+_Static_assert(sizeof(oOct) == 1584, "OCT layout (-DWRADHYD -DHELIUM)");
 #elif defined(ORC_WRADHYD)
 _Static_assert(sizeof(oCell) == 152, "CELL layout (-DWRADHYD)");
 _Static_assert(sizeof(oOct) == 1328, "OCT layout (-DWRADHYD)");
 #else
 _Static_assert(sizeof(oCell) == 136, "CELL layout");
 _Static_assert(sizeof(oOct) == 1200, "OCT layout");
+#endif
+
+#ifdef ORC_WRADHYD
+/* tracer t of a state: dX, then (HELIUM) dXHE, dXXHE, consecutive in both types */
+#define TRW(W, t) ((&(W)->dX)[t])
+/* the mass fraction each tracer is a part of (src/hydro_utils.c:1244-1252):
+ * hydrogen 1 - YHE, helium YHE */
+static const double TRFRAC[3] = {1. - YHE_, YHE_, YHE_};
 #endif
 
 static int g_err = 0;
@@ -115,7 +138,7 @@ static void to_cons(const oW *W, oU *U) {
   U->eint = W->p / (GAM - 1.);
   U->E = W->E;
 #ifdef ORC_WRADHYD
-  U->dX = W->dX;
+  for (int t = 0; t < NTR; t++) TRW(U, t) = TRW(W, t);
 #endif
 }
 /* dual: -DDUAL_E, the pressure from the tracked internal energy (src/hydro_utils.c:45-49) */
@@ -129,7 +152,7 @@ static void to_prim(const oU *U, oW *W, int dual) {
   else W->p = (GAM - 1.) * (U->E - ((U->du) * (U->du) + (U->dv) * (U->dv) + (U->dw) * (U->dw)) / (dl)*0.5);
   W->E = U->E;
 #ifdef ORC_WRADHYD
-  W->dX = U->dX;
+  for (int t = 0; t < NTR; t++) TRW(W, t) = TRW(U, t);
 #endif
   W->a = sqrt(GAM * W->p / dl);
 }
@@ -228,9 +251,9 @@ static void muscl_cell(Stencil *st, int slot, int ic, double dt, double dx) {
 #ifdef ORC_WRADHYD
     /* the face value is the face density times the centre's ionised fraction; the
      * reconstructed dX is overwritten (src/hydro_utils.c:1244-1246) */
-    {
-      double X0 = W0->dX / (W0->d * (1. - YHE_));
-      Wi->dX = Wi->d * (1. - YHE_) * X0;
+    for (int t = 0; t < NTR; t++) {
+      double X0 = TRW(W0, t) / (W0->d * (TRFRAC[t]));
+      TRW(Wi, t) = Wi->d * (TRFRAC[t]) * X0;
     }
 #endif
   }
@@ -363,10 +386,10 @@ static void euler_flux(const oU *U, int n, double f[5]) {
   f[4] = GAM * mn / U->d * U->E - 0.5 * (GAM - 1.) * mn / (U->d * U->d) * all;
 }
 #ifdef ORC_WRADHYD
-/* tracer flux f[6] of getflux_{X,Y,Z} (src/hydro_utils.c:925,943,961) */
-static double tracer_flux(const oU *U, int n) {
+/* tracer fluxes f[6..8] of getflux_{X,Y,Z} (src/hydro_utils.c:925-929,943-947,961-965) */
+static double tracer_flux(const oU *U, int n, int t) {
   double m[3] = {U->du, U->dv, U->dw};
-  return m[n] * U->dX / U->d;
+  return m[n] * TRW(U, t) / U->d;
 }
 #endif
 
@@ -380,7 +403,9 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us, do
   oU UL, UR;
   int k;
   for (k = 0; k < 5; k++) F[k] = 0.;
-  if (fx) *fx = 0.;
+#ifdef ORC_WRADHYD
+  if (fx) for (int t = 0; t < NTR; t++) fx[t] = 0.;
+#endif
   wave_speeds(WL, WR, n, &SL, &SR, &ustar);
   to_cons(WL, &UL);
   to_cons(WR, &UR);
@@ -388,13 +413,13 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us, do
     euler_flux(&UL, n, F);
     if (us) *us = UL;
 #ifdef ORC_WRADHYD
-    if (fx) *fx = tracer_flux(&UL, n);
+    if (fx) for (int t = 0; t < NTR; t++) fx[t] = tracer_flux(&UL, n, t);
 #endif
   } else if (SR <= 0.) {
     euler_flux(&UR, n, F);
     if (us) *us = UR;
 #ifdef ORC_WRADHYD
-    if (fx) *fx = tracer_flux(&UR, n);
+    if (fx) for (int t = 0; t < NTR; t++) fx[t] = tracer_flux(&UR, n, t);
 #endif
   } else if ((SL < 0.) && (ustar >= 0.)) {
     const oW *W = WL;
@@ -408,7 +433,8 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us, do
     F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SL - un)))) - U->E) * SL;
 #ifdef ORC_WRADHYD
     /* src/hydro_utils.c:1534-1535 (and :1809, :2115 for y, x) */
-    if (fx) *fx = tracer_flux(U, n) + (fact * W->dX / W->d - U->dX) * SL;
+    if (fx)
+      for (int t = 0; t < NTR; t++) fx[t] = tracer_flux(U, n, t) + (fact * TRW(W, t) / W->d - TRW(U, t)) * SL;
 #endif
     if (us) {
       double m[3];
@@ -428,7 +454,8 @@ static void hllc_flux(const oW *WL, const oW *WR, int n, double F[5], oU *us, do
     for (k = 0; k < 3; k++) F[1 + k] += (fact * (k == n ? ustar : vel[k]) - mom[k]) * SR;
     F[4] += (fact * (U->E / U->d + (ustar - un) * (ustar + W->p / (W->d * (SR - un)))) - U->E) * SR;
 #ifdef ORC_WRADHYD
-    if (fx) *fx = tracer_flux(U, n) + (fact * W->dX / W->d - U->dX) * SR;
+    if (fx)
+      for (int t = 0; t < NTR; t++) fx[t] = tracer_flux(U, n, t) + (fact * TRW(W, t) / W->d - TRW(U, t)) * SR;
 #endif
     if (us) {
       double m[3];
@@ -658,7 +685,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
   g_err = 0;
   const int dual = flag_on(flags, ORC_DUAL_E);
   for (o = firstoct[level - 1]; o != NULL; o = o->next) {
-    double flux[8][6][7];  /* [5]: internal-energy flux (-DDUAL_E), [6]: tracer flux (-DWRADHYD) */
+    double flux[8][6][9];  /* [5]: internal-energy flux (-DDUAL_E), [6..8]: tracer fluxes (-DWRADHYD) */
     double divu[8];
     if (o->cpu != 0) continue;
     n++;
@@ -674,13 +701,13 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
         for (s = 0; s < 2; s++) {
           int kf = 2 * dir + s, same, vc, nslot;
           const oW *Wc, *Wn;
-          double F[7];
+          double F[9];
           oU us;
           cell_nei(c, kf, &same, &vc);
           nslot = same ? 13 : FACE_SLOT[kf];
           Wc = face_state(&g_st, 13, c, kf, dt, dx);
           Wn = face_state(&g_st, nslot, vc, kf ^ 1, dt, dx);
-          F[6] = 0.;
+          F[6] = F[7] = F[8] = 0.;
 #ifdef ORC_WRADHYD
           if (s == 0) hllc_flux(Wn, Wc, dir, F, dual ? &us : NULL, &F[6]);
           else hllc_flux(Wc, Wn, dir, F, dual ? &us : NULL, &F[6]);
@@ -698,7 +725,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
             F[5] = (mom[dir] / us.d * ebar);
             divu[c] += (s == 0) ? -divuloc : divuloc;
           }
-          for (k = 0; k < 7; k++) flux[c][kf][k] = F[k] * (double)(!g_st.split[nslot][vc]);
+          for (k = 0; k < 9; k++) flux[c][kf][k] = F[k] * (double)(!g_st.split[nslot][vc]);
         }
       }
     }
@@ -718,7 +745,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
           dU.E += flux[c][f][4] * dtsurdx * one;
           dU.eint += flux[c][f][5] * dtsurdx * one;
 #ifdef ORC_WRADHYD
-          dU.dX += flux[c][f][6] * dtsurdx * one;  /* src/hydro_utils.c:3068 */
+          for (int t = 0; t < NTR; t++) TRW(&dU, t) += flux[c][f][6 + t] * dtsurdx * one;  /* src/hydro_utils.c:3068-3072 */
 #endif
           one *= -1.;
         }
@@ -730,7 +757,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
         U.dw += dU.dw;
         U.E += dU.E;
 #ifdef ORC_WRADHYD
-        U.dX += dU.dX;  /* src/hydro_utils.c:3158 */
+        for (int t = 0; t < NTR; t++) TRW(&U, t) += TRW(&dU, t);  /* src/hydro_utils.c:3158-3162 */
 #endif
         ekin = 0.5 * (U.du * U.du + U.dv * U.dv + U.dw * U.dw) / U.d;
         if (dual) {
@@ -751,6 +778,11 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
         /* ceiling of the ionised fraction (src/hydro_utils.c:3197-3198) */
         if (cell->fieldnew.dX < 0) cell->fieldnew.dX = 0.;
         if (cell->fieldnew.dX > (cell->fieldnew.d * (1. - YHE_))) cell->fieldnew.dX = cell->fieldnew.d * (1. - YHE_);
+#ifdef ORC_HELIUM
+        /* the helium densities have a ceiling only (src/hydro_utils.c:3199-3202) */
+        if (cell->fieldnew.dXHE > (cell->fieldnew.d * (YHE_))) cell->fieldnew.dXHE = cell->fieldnew.d * (YHE_);
+        if (cell->fieldnew.dXXHE > (cell->fieldnew.d * (YHE_))) cell->fieldnew.dXXHE = cell->fieldnew.d * (YHE_);
+#endif
 #endif
       }
       /* fine -> coarse flux correction into unsplit coarse neighbours */
@@ -773,7 +805,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
           U.E += flux[c][k][4] * dtsurdx * one * 0.125;
           if (dual) U.eint += flux[c][k][5] * dtsurdx * one * 0.125;
 #ifdef ORC_WRADHYD
-          U.dX += flux[c][k][6] * dtsurdx * one * 0.125;
+          for (int t = 0; t < NTR; t++) TRW(&U, t) += flux[c][k][6 + t] * dtsurdx * one * 0.125;
 #endif
           to_prim(&U, &W, dual);
           cc->fieldnew = W;
@@ -801,7 +833,7 @@ int orc_hydro_solver(void **firstoct_v, int level, double dt, int flags) {
             W.w += Wc->w * 0.125;
             W.p += Wc->p * 0.125;
 #ifdef ORC_WRADHYD
-            W.dX += Wc->dX * 0.125;  /* src/hydro_utils.c:3460 */
+            for (int t = 0; t < NTR; t++) TRW(&W, t) += TRW(Wc, t) * 0.125;  /* src/hydro_utils.c:3446-3460 */
 #endif
           }
           get_E(&W);

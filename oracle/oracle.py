@@ -20,6 +20,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "liboracle.so")
 ORACLE_LIB_GRAV = os.path.join(HERE, "_build", "liboracle_grav.so")
 ORACLE_LIB_RH = os.path.join(HERE, "_build", "liboracle_rh.so")
+ORACLE_LIB_HE = os.path.join(HERE, "_build", "liboracle_he.so")
 REF_LIB = os.path.join(HERE, "_ref", "libemmaref.so")
 REF_LIB_TX = os.path.join(HERE, "_ref", "libemmaref_tx.so")
 REF_LIB_GRAV = os.path.join(HERE, "_ref", "libemmaref_grav.so")
@@ -27,6 +28,7 @@ REF_LIB_DUAL = os.path.join(HERE, "_ref", "libemmaref_dual.so")
 REF_LIB_RH = os.path.join(HERE, "_ref", "libemmaref_rh.so")
 REF_LIB_SP = os.path.join(HERE, "_ref", "libemmaref_sp.so")
 REF_LIB_MARK = os.path.join(HERE, "_ref", "libemmaref_mark.so")
+REF_LIB_HE = os.path.join(HERE, "_ref", "libemmaref_he.so")
 
 HYDROTEST = 0x40
 DUAL_E = 0x80
@@ -45,12 +47,13 @@ def flags_for(trans, dual=False):
 
 class Restatement:
     """grav=True: the -DWGRAV layout and gravity coupling (liboracle_grav.so);
-    rh=True: the -DWRADHYD layout with the advected ionised density (liboracle_rh.so)."""
+    rh=True: the -DWRADHYD layout with the advected ionised density (liboracle_rh.so);
+    he=True: its -DHELIUM variant, three tracers (liboracle_he.so)."""
     _libs = {}
 
-    def __init__(self, grav=False, rh=False):
-        assert not (grav and rh), "one layout at a time"
-        path = ORACLE_LIB_GRAV if grav else (ORACLE_LIB_RH if rh else ORACLE_LIB)
+    def __init__(self, grav=False, rh=False, he=False):
+        assert (grav + rh + he) <= 1, "one layout at a time"
+        path = ORACLE_LIB_GRAV if grav else (ORACLE_LIB_RH if rh else (ORACLE_LIB_HE if he else ORACLE_LIB))
         if path not in Restatement._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"oracle restatement not built: {path}")
@@ -159,7 +162,9 @@ class GravClone:
             self.h = None
 
 
-def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False):
+def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False, he=False):
+    if he:
+        return REF_LIB_HE
     if mark:
         return REF_LIB_MARK
     if sp:
@@ -169,8 +174,8 @@ def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False):
     return REF_LIB_DUAL if dual else (REF_LIB_GRAV if grav else (REF_LIB_TX if tx else REF_LIB))
 
 
-def ref_available(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False):
-    return os.path.exists(_ref_path(tx, grav, dual, rh, sp, mark))
+def ref_available(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False, he=False):
+    return os.path.exists(_ref_path(tx, grav, dual, rh, sp, mark, he))
 
 
 class RefTree:
@@ -179,11 +184,12 @@ class RefTree:
     _libs = {}
 
     def __init__(self, lcoarse, lmax, tx=False, ngridmax=None, hstride=1024, grav=False, dual=False, rh=False,
-                 sp=False, mark=False):
+                 sp=False, mark=False, he=False):
         """sp: the reference built with -DSINGLEPRECISION (REAL = float); mark: its
-        src/amr.c built with the density refinement criterion (ref_amr_sntest.c)."""
-        assert (tx + grav + dual + rh + sp + mark) <= 1, "one build variant at a time"
-        path = _ref_path(tx, grav, dual, rh, sp, mark)
+        src/amr.c built with the density refinement criterion (ref_amr_sntest.c);
+        he: built with -DWRADHYD -DHELIUM (three tracers)."""
+        assert (tx + grav + dual + rh + sp + mark + he) <= 1, "one build variant at a time"
+        path = _ref_path(tx, grav, dual, rh, sp, mark, he)
         if path not in RefTree._libs:
             if not os.path.exists(path):
                 raise RuntimeError(f"reference oracle not built: {path}")
@@ -220,6 +226,18 @@ class RefTree:
         a = np.ascontiguousarray(dX, dtype=np.float64)
         self.L.ref_set_tracer.argtypes = [c_int, c_void_p]
         self.L.ref_set_tracer(level, _p(a))
+
+    def set_tracer_n(self, level, t, x):
+        """Tracer t (0: dX; -DHELIUM 1: dXHE, 2: dXXHE) of field and fieldnew."""
+        a = np.ascontiguousarray(x, dtype=np.float64)
+        self.L.ref_set_tracer_n.argtypes = [c_int, c_int, c_void_p]
+        self.L.ref_set_tracer_n(level, t, _p(a))
+
+    def get_tracer_n(self, level, t, which=0):
+        out = np.zeros(8 * self.noct(level))
+        self.L.ref_get_tracer_n.argtypes = [c_int, c_int, c_int, c_void_p]
+        self.L.ref_get_tracer_n(level, t, which, _p(out))
+        return out
 
     def get_tracer(self, level, which=0):
         out = np.zeros(8 * self.noct(level))

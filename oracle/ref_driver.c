@@ -275,6 +275,31 @@ void ref_get_tracer(int level, int which, double *out) {
   for (o = g_first[level - 1]; o != NULL; o = o->next, i++)
     for (c = 0; c < 8; c++) out[8 * i + c] = which ? o->cell[c].fieldnew.dX : o->cell[c].field.dX;
 }
+/* Tracer t (0: dX; with -DHELIUM 1: dXHE, 2: dXXHE, the members that follow dX in
+ * struct Wtype, src/prototypes.h:620-625) of field and fieldnew. */
+#ifdef HELIUM
+#define REF_NTR 3
+#else
+#define REF_NTR 1
+#endif
+int ref_ntracers(void) { return REF_NTR; }
+void ref_set_tracer_n(int level, int t, const double *x) {
+  int i = 0, c;
+  struct OCT *o;
+  if (t < 0 || t >= REF_NTR) return;
+  for (o = g_first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) {
+      (&o->cell[c].field.dX)[t] = x[8 * i + c];
+      (&o->cell[c].fieldnew.dX)[t] = x[8 * i + c];
+    }
+}
+void ref_get_tracer_n(int level, int t, int which, double *out) {
+  int i = 0, c;
+  struct OCT *o;
+  if (t < 0 || t >= REF_NTR) return;
+  for (o = g_first[level - 1]; o != NULL; o = o->next, i++)
+    for (c = 0; c < 8; c++) out[8 * i + c] = which ? (&o->cell[c].fieldnew.dX)[t] : (&o->cell[c].field.dX)[t];
+}
 #endif
 
 /* Checkpoints through the reference's own src/restart.c (save_amr / restore_amr),

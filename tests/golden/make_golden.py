@@ -6,7 +6,8 @@ Each fixture: a seeded small tree (uniform or refined spheres about the box
 centre), the input primitive fields per level, and the reference's `field`
 (d,u,v,w,p,a,E) per level after `nsteps` coarse steps at CFL 0.8.  Build
 variants (meta[4]): 0 the default, 1 -DDUAL_E, 2 -DWGRAV (input forces per
-level), 3 -DWRADHYD (input and output ionised density dX per level).
+level), 3 -DWRADHYD (input and output ionised density dX per level), 4 -DWRADHYD
+-DHELIUM (input and output dX, dXHE, dXXHE per level).
 Existing fixture files are kept; only missing ones are written.
 """
 import os
@@ -27,7 +28,9 @@ CASES = [
     ("amr_l3_4_dual", 3, 4, (0.35,), 2, 0, "random", 1),
     ("amr_l3_4_gravity", 3, 4, (0.35,), 2, 0, "random", 2),
     ("amr_l3_4_tracer", 3, 4, (0.35,), 2, 0, "random", 3),
+    ("amr_l3_4_helium", 3, 4, (0.35,), 2, 0, "random", 4),
 ]
+HELIUM = ((0.76, 1.0), (0.24, 0.6), (0.24, 0.4))  # (mass fraction, top of the ionised share) per tracer
 
 
 def fields(kind, c, rng):
@@ -48,7 +51,7 @@ def main():
         if os.path.exists(path):
             continue
         ref = oracle.RefTree(base, lmax, tx=bool(trans), ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)),
-                             dual=variant == 1, grav=variant == 2, rh=variant == 3)
+                             dual=variant == 1, grav=variant == 2, rh=variant == 3, he=variant == 4)
         for i, r in enumerate(radii):
             ref.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
         rng = np.random.default_rng(12345)
@@ -65,6 +68,11 @@ def main():
                 x = f[0] * rng.uniform(0.0, 1.0, len(f[0]))
                 ref.set_tracer(l, x)
                 out[f"in_x_{l}"] = x
+            if variant == 4:
+                xs = np.array([f[0] * frac * rng.uniform(0.0, top, len(f[0])) for frac, top in HELIUM])
+                for t in range(3):
+                    ref.set_tracer_n(l, t, xs[t])
+                out[f"in_x_{l}"] = xs
         tsim, adt = ref.run(nsteps)
         out["tsim"] = np.array(tsim)
         out["adt"] = adt
@@ -72,6 +80,8 @@ def main():
             out[f"out_{l}"] = ref.get_fields(l, 0)
             if variant == 3:
                 out[f"out_x_{l}"] = ref.get_tracer(l, 0)
+            if variant == 4:
+                out[f"out_x_{l}"] = np.array([ref.get_tracer_n(l, t, 0) for t in range(3)])
         np.savez_compressed(path, **out)
         print(path, os.path.getsize(path), "bytes")
 

@@ -10,12 +10,13 @@ HEADERS = [os.path.join(ROOT, "include", f) for f in sorted(os.listdir(os.path.j
 
 GRAV_HEADER = os.path.join(ROOT, "include", "emma_hydro_grav.h")
 RH_HEADER = os.path.join(ROOT, "include", "emma_hydro_rh.h")
+HE_HEADER = os.path.join(ROOT, "include", "emma_hydro_he.h")
 
 
 def declared_functions(headers=None):
     """Functions declared in the headers (default: all but the layout libraries' own)."""
     names = set()
-    for h in (headers if headers is not None else [h for h in HEADERS if h not in (GRAV_HEADER, RH_HEADER)]):
+    for h in (headers if headers is not None else [h for h in HEADERS if h not in (GRAV_HEADER, RH_HEADER, HE_HEADER)]):
         src = open(h).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         src = re.sub(r"//[^\n]*", "", src)
@@ -47,7 +48,7 @@ def test_gravity_library_exports_everything():
     and its own (grav_correction, the force setter of test trees)."""
     from emma_b200._lib import LIB_PATH_GRAV, SIGNATURES, GRAV_SIGNATURES
     L = ctypes.CDLL(LIB_PATH_GRAV)
-    names = declared_functions([h for h in HEADERS if h != RH_HEADER])
+    names = declared_functions([h for h in HEADERS if h not in (RH_HEADER, HE_HEADER)])
     assert {"grav_correction", "emma_tree_set_force"} <= names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
@@ -59,11 +60,23 @@ def test_tracer_library_exports_everything():
     the tracer accessors of test trees."""
     from emma_b200._lib import LIB_PATH_RH, SIGNATURES, RH_SIGNATURES
     L = ctypes.CDLL(LIB_PATH_RH)
-    names = declared_functions([h for h in HEADERS if h != GRAV_HEADER])
+    names = declared_functions([h for h in HEADERS if h not in (GRAV_HEADER, HE_HEADER)])
     assert {"emma_tree_set_tracer", "emma_tree_get_tracer"} <= names
     missing = [n for n in names if not hasattr(L, n)]
     assert not missing, missing
     assert names <= {n for n, _, _ in SIGNATURES + RH_SIGNATURES}
+
+
+def test_helium_library_exports_everything():
+    """libemmahydro_he.so (the -DWRADHYD -DHELIUM cell layout) exports the default
+    entries, the single-tracer accessors and the three-tracer ones of test trees."""
+    from emma_b200._lib import LIB_PATH_HE, SIGNATURES, RH_SIGNATURES, HE_SIGNATURES
+    L = ctypes.CDLL(LIB_PATH_HE)
+    names = declared_functions([h for h in HEADERS if h != GRAV_HEADER])
+    assert {"emma_tree_set_tracer_n", "emma_tree_get_tracer_n", "emma_tree_put_tracer_n"} <= names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert names <= {n for n, _, _ in SIGNATURES + RH_SIGNATURES + HE_SIGNATURES}
 
 
 def test_struct_layout_matches_reference():
@@ -78,8 +91,9 @@ def test_hgrid_size_matches_reference_builds():
     import re
     import oracle
     src = open(os.path.join(ROOT, "include", "emma_oct.h")).read()
-    grav, rh, plain = (int(x) for x in re.findall(r"#define EMMA_SIZEOF_HGRID (\d+)", src))
-    for name, want in (("libemmaref.so", plain), ("libemmaref_grav.so", grav), ("libemmaref_rh.so", rh)):
+    grav, he, rh, plain = (int(x) for x in re.findall(r"#define EMMA_SIZEOF_HGRID (\d+)", src))
+    for name, want in (("libemmaref.so", plain), ("libemmaref_grav.so", grav), ("libemmaref_rh.so", rh),
+                       ("libemmaref_he.so", he)):
         path = os.path.join(ROOT, "oracle", "_ref", name)
         if not os.path.exists(path):
             continue

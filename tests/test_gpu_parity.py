@@ -197,17 +197,21 @@ def _golden_cases():
 def test_gpu_reproduces_golden(gpu, name):
     """The reference's own outputs (tests/golden) from the resident GPU path of the
     same build variant: default, -DDUAL_E (option), -DWGRAV (the fixture's forces
-    uploaded per level) and -DWRADHYD (a tree of that layout, dX compared too)."""
+    uploaded per level), -DWRADHYD (a tree of that layout, dX compared too) and
+    -DWRADHYD -DHELIUM (its three tracers compared)."""
     g = np.load(os.path.join(GOLDEN, name))
     base, lmax, nsteps, trans = (int(x) for x in g["meta"][:4])
     variant = int(g["meta"][4]) if len(g["meta"]) > 4 else 0
-    t = OctTree(base, lmax, rh=variant == 3)
+    t = OctTree(base, lmax, rh=variant == 3, he=variant == 4)
     for i, rr in enumerate(tuple(g["radii"])):
         t.refine_where(base + i, lambda c, rr=rr: np.linalg.norm(c - 0.5, axis=1) < rr)
     for l in range(base, lmax + 1):
         t.set_fields(l, *g[f"in_{l}"][:5])
         if variant == 3:
             t.set_tracer(l, g[f"in_x_{l}"])
+        if variant == 4:
+            for tr in range(3):
+                t.set_tracer_n(l, tr, g[f"in_x_{l}"][tr])
     r = ResidentHydro(t, precision=PREC_FP64, trans=trans, cfl=CFL, gravity=variant == 2, dual=variant == 1)
     if variant == 2:
         for l in range(base, lmax + 1):
@@ -219,10 +223,13 @@ def test_gpu_reproduces_golden(gpu, name):
     for l in range(base, lmax + 1):
         e = per_cell_rel(t.get_fields(l)[:5], g[f"out_{l}"][:5])
         assert e.max() <= 1e-11, (l, e.max())
-        if variant == 3:
+        if variant in (3, 4):
             d = g[f"out_{l}"][0]
             leaf = ~t.split_mask(l)
-            assert (np.abs(t.get_tracer(l) - g[f"out_x_{l}"])[leaf] / d[leaf]).max() <= 1e-11, l
+            outs = [g[f"out_x_{l}"]] if variant == 3 else list(g[f"out_x_{l}"])
+            for tr, xo in enumerate(outs):
+                x = t.get_tracer_n(l, tr)
+                assert (np.abs(x - xo)[leaf] / d[leaf]).max() <= 1e-11, (l, tr)
 
 
 def _final_states(cfg, nsteps, nsub, use_graph, precision=PREC_FP64):

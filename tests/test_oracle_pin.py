@@ -44,9 +44,20 @@ def random_tracer(tree, levels, seed=777):
         tree.set_tracer(l, d * rng.uniform(0.0, 1.0, d.size))
 
 
-def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, grav=False, dual=False, rh=False):
+def random_helium(tree, levels, seed=77):
+    """-DHELIUM trees: dX = d (1 - YHE) x, dXHE = d YHE y, dXXHE = d YHE z with x, y, z
+    uniform in [0, 1], [0, 0.6], [0, 0.4] (YHE = 0.24)."""
+    rng = np.random.default_rng(seed)
+    for l in levels:
+        d = tree.get_fields(l, 0)[0]
+        for t, (frac, top) in enumerate(((0.76, 1.0), (0.24, 0.6), (0.24, 0.4))):
+            tree.set_tracer_n(l, t, d * frac * rng.uniform(0.0, top, d.size))
+
+
+def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, grav=False, dual=False, rh=False,
+                       he=False):
     ref = oracle.RefTree(base, lmax, tx=tx, ngridmax=sum(8 ** (l - 1) for l in range(1, lmax + 1)), grav=grav,
-                         dual=dual, rh=rh)
+                         dual=dual, rh=rh, he=he)
     for i, r in enumerate(radii):
         ref.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
     if fields is None:
@@ -60,16 +71,20 @@ def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, g
     if rh:
         random_tracer(ref, range(base, lmax + 1))
         assert ref.sizeof_oct() == oracle.Restatement(rh=True).sizeof_oct() == 1328
+    if he:
+        random_helium(ref, range(base, lmax + 1))
+        assert ref.sizeof_oct() == oracle.Restatement(he=True).sizeof_oct() == 1584
+    ntr = 3 if he else (1 if rh else 0)
     base_ptr = ref.L.ref_grid_base()
     nbytes = ref.ngridmax * ref.sizeof_oct()
     snap = ctypes.string_at(base_ptr, nbytes)
     t1, adt1 = ref.run(nsteps)
     A = {l: (ref.get_fields(l, 0), ref.get_fields(l, 1)) for l in range(base, lmax + 1)}
-    AX = {l: (ref.get_tracer(l, 0), ref.get_tracer(l, 1)) for l in range(base, lmax + 1)} if rh else None
+    AX = {l: [(ref.get_tracer_n(l, t, 0), ref.get_tracer_n(l, t, 1)) for t in range(ntr)] for l in range(base, lmax + 1)}
     ctypes.memmove(base_ptr, snap, nbytes)
     trans = 3 if tx else 0
-    t2, adt2, err = oracle.Restatement(grav=grav, rh=rh).run(ref.firstoct, base, lmax, nsteps, 0.8, trans=trans,
-                                                              dual=dual)
+    t2, adt2, err = oracle.Restatement(grav=grav, rh=rh, he=he).run(ref.firstoct, base, lmax, nsteps, 0.8,
+                                                                     trans=trans, dual=dual)
     assert err == 0
     assert t1 == t2 and np.array_equal(adt1, adt2)
     for l in range(base, lmax + 1):
@@ -78,9 +93,9 @@ def ref_vs_restatement(tx, base, lmax, radii, nsteps, seed=12345, fields=None, g
         leaf = ~(ref.topology(l)[2].reshape(-1) >= 0)
         # fieldnew of split cells holds stale stencil data in the reference; not part of the state
         assert np.array_equal(fnA[:, leaf], ref.get_fields(l, 1)[:, leaf]), f"fieldnew, level {l}"
-        if rh:
-            assert np.array_equal(AX[l][0], ref.get_tracer(l, 0)), f"dX, level {l}"
-            assert np.array_equal(AX[l][1][leaf], ref.get_tracer(l, 1)[leaf]), f"fieldnew dX, level {l}"
+        for t in range(ntr):
+            assert np.array_equal(AX[l][t][0], ref.get_tracer_n(l, t, 0)), f"tracer {t}, level {l}"
+            assert np.array_equal(AX[l][t][1][leaf], ref.get_tracer_n(l, t, 1)[leaf]), f"fieldnew tracer {t}, level {l}"
 
 
 @needs_ref
@@ -141,6 +156,20 @@ def test_pin_tracer_uniform():
 @needs_ref_rh
 def test_pin_tracer_amr():
     ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, rh=True)
+
+
+needs_ref_he = pytest.mark.skipif(not oracle.ref_available(he=True), reason="oracle/_ref -DHELIUM build absent")
+
+
+@needs_ref_he
+def test_pin_helium_uniform():
+    """-DWRADHYD -DHELIUM (NVAR 9): the hydrogen and the two helium tracers."""
+    ref_vs_restatement(False, 4, 4, (), 3, he=True)
+
+
+@needs_ref_he
+def test_pin_helium_amr():
+    ref_vs_restatement(False, 4, 6, (0.3, 0.15), 2, he=True)
 
 
 needs_ref_dual = pytest.mark.skipif(not oracle.ref_available(dual=True), reason="oracle/_ref dual-energy build absent")
@@ -261,12 +290,13 @@ def _golden_cases():
 @pytest.mark.parametrize("name", _golden_cases())
 def test_restatement_reproduces_golden(name):
     """The reference's outputs committed as fixtures, reproduced bit for bit by the
-    restatement of the same build variant (default, -DDUAL_E, -DWGRAV, -DWRADHYD)."""
+    restatement of the same build variant (default, -DDUAL_E, -DWGRAV, -DWRADHYD,
+    -DWRADHYD -DHELIUM)."""
     g = np.load(os.path.join(GOLDEN, name))
     base, lmax, nsteps, trans = (int(x) for x in g["meta"][:4])
     variant = int(g["meta"][4]) if len(g["meta"]) > 4 else 0
     radii = tuple(g["radii"])
-    t = OctTree(base, lmax, grav=variant == 2, rh=variant == 3)
+    t = OctTree(base, lmax, grav=variant == 2, rh=variant == 3, he=variant == 4)
     for i, r in enumerate(radii):
         t.refine_where(base + i, lambda c, r=r: np.linalg.norm(c - 0.5, axis=1) < r)
     for l in range(base, lmax + 1):
@@ -275,7 +305,10 @@ def test_restatement_reproduces_golden(name):
             t.set_force(l, *g[f"in_f_{l}"])
         if variant == 3:
             t.set_tracer(l, g[f"in_x_{l}"])
-    R = oracle.Restatement(grav=variant == 2, rh=variant == 3)
+        if variant == 4:
+            for tr in range(3):
+                t.set_tracer_n(l, tr, g[f"in_x_{l}"][tr])
+    R = oracle.Restatement(grav=variant == 2, rh=variant == 3, he=variant == 4)
     tsim, adt, err = R.run(t.firstoct, base, lmax, nsteps, 0.8, trans=trans, dual=variant == 1)
     assert err == 0
     assert tsim == float(g["tsim"])
@@ -283,6 +316,9 @@ def test_restatement_reproduces_golden(name):
         assert np.array_equal(t.get_fields(l, 0), g[f"out_{l}"]), f"level {l}"
         if variant == 3:
             assert np.array_equal(t.get_tracer(l, 0), g[f"out_x_{l}"]), f"dX, level {l}"
+        if variant == 4:
+            for tr in range(3):
+                assert np.array_equal(t.get_tracer_n(l, tr, 0), g[f"out_x_{l}"][tr]), f"tracer {tr}, level {l}"
 
 
 @needs_ref
