@@ -83,6 +83,7 @@ SIGNATURES = [
     ("emma_hydro_cell_updates", c_ll, []),
     ("emma_hydro_reset_counters", None, []),
     ("emma_hydro_kernel_timing", c_int, [P(c_double), P(c_ll), P(c_ll)]),
+    ("emma_hydro_kernel_timing_level", c_int, [c_int, P(c_double), P(c_ll), P(c_ll)]),
     ("emma_hydro_tuning", c_int, [c_int, P(c_int), P(c_int), c_void_p]),
     ("emma_hydro_column_tuning", c_int, [c_int, P(c_int), c_void_p]),
     ("emma_hydro_probe_wait_timeout", c_int, [c_ll]),

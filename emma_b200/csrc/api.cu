@@ -91,6 +91,7 @@ struct DevLevel {
 struct TimedLaunch {
   cudaEvent_t a, b;
   long long cells;
+  int level;  // the resident level a single-level launch advances, -1 for a batched launch
 };
 
 struct Tree {
@@ -745,6 +746,7 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
   if (timed) {
     cudaEventRecord(tl.b, g.stream);
     tl.cells = cells;
+    tl.level = col_level;
     g.launches.push_back(tl);
   }
   return ck(e, "level kernel launch");
@@ -1687,6 +1689,25 @@ int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cel
   }
   if (avg_ms) *avg_ms = g.launches.empty() ? 0. : tot / (double)g.launches.size();
   if (launches) *launches = (long long)g.launches.size();
+  if (cells) *cells = nc;
+  return 0;
+}
+
+int emma_hydro_kernel_timing_level(int level, double *total_ms, long long *launches, long long *cells) {
+  if (!g.ready) return EMMA_ST_ARG;
+  CK(cudaStreamSynchronize(g.stream));
+  double tot = 0.;
+  long long n = 0, nc = 0;
+  for (auto &t : g.launches) {
+    if (t.level != level) continue;
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, t.a, t.b);
+    tot += ms;
+    nc += t.cells;
+    n++;
+  }
+  if (total_ms) *total_ms = tot;
+  if (launches) *launches = n;
   if (cells) *cells = nc;
   return 0;
 }

@@ -47,6 +47,7 @@ def main():
     L = lib("rh" if a.tracer else False)
     per_step = []
     tot_ms, tot_n, tot_cells = 0.0, 0, 0
+    levels = {}
     for _ in range(a.steps):
         L.emma_hydro_reset_counters()
         r.coarse_step(nsub=cfg.nsub)
@@ -56,10 +57,21 @@ def main():
         tot_ms += avg.value * n.value
         tot_n += n.value
         tot_cells += cells.value
+        for lev in range(cfg.lcoarse, cfg.lmax + 1):
+            ms, n, cells = ctypes.c_double(), ctypes.c_longlong(), ctypes.c_longlong()
+            L.emma_hydro_kernel_timing_level(lev, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(cells))
+            if n.value:
+                acc = levels.setdefault(lev, [0.0, 0, 0])
+                acc[0] += ms.value
+                acc[1] += n.value
+                acc[2] += cells.value
+    per_level = {lev: {"ms_per_launch": round(v[0] / v[1], 4), "launches": v[1],
+                       "cell_updates_per_s": v[2] / (v[0] * 1e-3) if v[0] else None}
+                 for lev, v in sorted(levels.items())}
     print(json.dumps({"config": cfg.name, "level": cfg.lcoarse, "precision": a.precision, "status": r.status(),
                       "column_planes": r.column_tuning(cfg.lcoarse)[0], "launches": tot_n,
                       "avg_launch_ms": tot_ms / max(tot_n, 1), "cells_per_launch": tot_cells / max(tot_n, 1),
-                      "kernel_ms_per_step": per_step,
+                      "kernel_ms_per_step": per_step, "per_level": per_level,
                       "cell_updates_per_s_kernel": tot_cells / (tot_ms * 1e-3) if tot_ms else None}))
 
 

@@ -250,6 +250,9 @@ void emma_hydro_reset_counters(void);
 /* Average device time (ms) of the level kernel launches since the last reset,
  * measured with CUDA events on the launching stream, and their count. */
 int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cells);
+/* The same for the single-level launches of one resident level (level -1: the
+ * batched launches): total device time (ms), count and cell-updates. */
+int emma_hydro_kernel_timing_level(int level, double *total_ms, long long *launches, long long *cells);
 
 /* Column kernel of a resident level (no reference counterpart): *planes = the cell
  * planes per work item its launches use with the current options (0: the brick
