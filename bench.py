@@ -129,21 +129,6 @@ def traffic_per_cell(config, precision):
     return None
 
 
-def graph_kernel_count(cfg, tree):
-    """Kernels of this library in one captured coarse step (CFL reductions,
-    schedule kernels, level-kernel launches)."""
-    levels = [l for l in range(cfg.lcoarse, cfg.lmax + 1) if tree.noct(l) > 0]
-    if cfg.nsub == 1 or len(levels) == 1:
-        return len(levels) + 3  # CFL per level, batch begin, level kernel, batch end
-    n, per = 0, 1
-    for l in levels:
-        per *= cfg.nsub
-        # begin, CFL, dt, prelaunch, level kernel, end per gated iteration, plus the
-        # clear of the correction buffer on levels that have a finer level
-        n += per * (6 + (1 if l != levels[-1] else 0))
-    return n + 1
-
-
 def run_mine(args, rank, world):
     import torch
     from emma_b200 import ResidentHydro, PREC_FP64, PREC_MIXED, lib
@@ -210,9 +195,18 @@ def run_mine(args, rank, world):
         ms = sum(a.elapsed_time(b) for a, b in evs)
         updates = L.emma_hydro_cell_updates()
         status = r.status()
-        launches_per_step = graph_kernel_count(cfg, tree)
+        fused, fused_ctas, fused_groups, launches_per_step = r.graph_info()
+        step_mode, step_sweep = r.step_tuning()
+        if step_mode >= 0 and any(step_sweep):
+            tuning["coarse_step"] = {"mode": "fused, %d tile groups per CTA" % step_mode if step_mode else
+                                     "separate launches",
+                                     "ms_per_step": {("separate launches" if k == 0 else f"fused, {k} groups"): round(x, 4)
+                                                     for k, x in enumerate(step_sweep) if x > 0}}
+        if fused:
+            kernels.add("step_kernel<MathF32>" if prec == PREC_MIXED else "step_kernel<MathF64>")
         res = {"ms": ms, "updates": updates, "launches": launches_per_step * args.steps, "status": status,
-               "clocks": clk.summary(), "autotune": tuning, "kernels": sorted(kernels)}
+               "clocks": clk.summary(), "autotune": tuning, "kernels": sorted(kernels),
+               "fused_step": {"ctas": fused_ctas, "tile_groups_per_cta": fused_groups} if fused else None}
         # level-kernel time per launch: the same steps on the host-driven schedule,
         # each level-kernel launch timed with CUDA events on the library stream
         r2 = r
@@ -507,6 +501,8 @@ def main():
                                    "per SM; mixed path on complete periodic levels without split cells: the column "
                                    "kernel (16x16-cell columns) with 2..64 cell planes per work item"},
         "gpu_launches": mixed["launches"],
+        "gpu_launches_per_step": mixed["launches"] // max(args.steps, 1),
+        "fused_step": mixed["fused_step"],
         "clocks": mixed["clocks"],
         "status": mixed["status"],
         "host_tree_build_s": build_s,

@@ -23,7 +23,7 @@ P = ctypes.POINTER
 class EmmaHydroOptions(ctypes.Structure):
     _fields_ = [("precision", c_int), ("trans_flags", c_int), ("cfl", c_double),
                 ("tile_octs", c_int), ("device", c_int), ("use_graph", c_int), ("gravity", c_int),
-                ("dual_energy", c_int), ("column", c_int)]
+                ("dual_energy", c_int), ("column", c_int), ("fused_step", c_int)]
 
 
 PREC_FP64, PREC_MIXED = 0, 1
@@ -84,6 +84,10 @@ SIGNATURES = [
     ("emma_hydro_reset_counters", None, []),
     ("emma_hydro_kernel_timing", c_int, [P(c_double), P(c_ll), P(c_ll)]),
     ("emma_hydro_kernel_timing_level", c_int, [c_int, P(c_double), P(c_ll), P(c_ll)]),
+    ("emma_hydro_graph_info", c_int, [P(c_int), P(c_int), P(c_int), P(c_int)]),
+    ("emma_hydro_fused_job_log", c_int, [c_int, c_void_p, c_void_p, c_void_p]),
+    ("emma_hydro_timed_coarse_steps", c_int, [c_double, c_double, c_int, c_int, P(c_double)]),
+    ("emma_hydro_step_tuning", c_int, [P(c_int), c_void_p]),
     ("emma_hydro_tuning", c_int, [c_int, P(c_int), P(c_int), c_void_p]),
     ("emma_hydro_column_tuning", c_int, [c_int, P(c_int), c_void_p]),
     ("emma_hydro_probe_wait_timeout", c_int, [c_ll]),

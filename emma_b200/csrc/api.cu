@@ -33,6 +33,12 @@ cudaError_t launch_level_fp64(const BatchArgs &a, unsigned shapes, int nsm, int 
 cudaError_t launch_level_f32(const BatchArgs &a, unsigned shapes, int nsm, int ctas_per_sm, cudaStream_t s,
                              int *occupancy);
 cudaError_t launch_column_f32(const ColumnArgs &a, cudaStream_t s);
+cudaError_t launch_step_f32(const StepArgs &a, unsigned variant, int groups, int nsm, cudaStream_t s, int *grid,
+                            int *threads);
+cudaError_t launch_step_fp64(const StepArgs &a, unsigned variant, int groups, int nsm, cudaStream_t s, int *grid,
+                             int *threads);
+int step_groups_f32(unsigned variant, int groups);
+int step_groups_fp64(unsigned variant, int groups);
 cudaError_t launch_cfl(const LevelArgs *lv, int slot, long long n8, const int *gate, unsigned long long *out, int nsm,
                        cudaStream_t s);
 cudaError_t launch_interp(const LevelArgs *lv, int slot, long long nv, const int *gate, int nsm, cudaStream_t s,
@@ -113,6 +119,19 @@ struct Ctx {
   unsigned *d_done = nullptr;    // kMaxLevels completion counters
   SchedState *d_S = nullptr;
   SchedState *h_S = nullptr;     // pinned staging of the schedule state
+  StepCtl *d_ctl = nullptr;      // control block of the fused coarse step
+  StepJobRecord *d_jobt = nullptr;  // release times of its jobs (kStepJobLog)
+  bool c_dirty = false;          // a level's corrections may hold values (read or not) that the
+                                 // fused step, which clears what it reads, would not expect:
+                                 // after separate launches; cleared before a fused step
+  int step_grid = 0, step_threads = 0;  // CTAs and threads per CTA of the last fused step launch
+  // coarse-step mode of the resident tree's subcycled graph: -2 not decided yet,
+  // 0 the level schedule's separate launches, k > 0 the fused kernel with k tile
+  // groups per CTA; the autotuner's times (ms per step; [0] separate launches,
+  // [k] k groups, 0 = not tried) and the nsub and precision it timed
+  int step_groups = -2;
+  double step_sweep[5] = {};
+  int step_tuned_nsub = -1, step_tuned_prec = -1;
   unsigned status = 0;
   std::string last_error;
   Tree res;                      // resident tree
@@ -120,7 +139,9 @@ struct Ctx {
   int *d_work_all = nullptr;     // batched work list, finest level first
   int nwork_all = 0;
   cudaGraphExec_t graph = nullptr;
-  int graph_nsub = -1, graph_prec = -1, graph_col = -2;
+  int graph_nsub = -1, graph_prec = -1, graph_col = -2, graph_groups = -3;
+  bool graph_is_fused = false;   // the captured coarse step is one fused kernel
+  int graph_kernels = 0;         // kernel nodes of the captured coarse step
   // drop-in cache: one mirror of levels L-1..L+1 per advanced level L, so that a
   // driver cycling through its levels does not rebuild one on every call
   struct DropCache {
@@ -345,6 +366,9 @@ void drop_graph() {
   g.graph = nullptr;
   g.graph_nsub = g.graph_prec = -1;
   g.graph_col = -2;
+  g.graph_groups = -3;
+  g.graph_is_fused = false;
+  g.graph_kernels = 0;
 }
 
 void free_level(DevLevel &d) {
@@ -404,6 +428,7 @@ bool alloc_tree(const HostTree &H, Tree &t, bool with_base) {
   t.lev.assign(H.lev.size(), DevLevel());
   t.lcoarse = H.lcoarse;
   t.lmax = H.lmax;
+  if (!with_base) g.step_groups = -2;  // a new resident tree: its coarse-step mode is chosen again
   if (!ck(cudaMalloc(&t.d_lv, sizeof(LevelArgs) * kMaxLevels), "cudaMalloc level slots")) return false;
   if (!ck(cudaMemset(t.d_lv, 0, sizeof(LevelArgs) * kMaxLevels), "cudaMemset level slots")) return false;
   for (int L = H.lcoarse; L <= H.lmax; L++) {
@@ -713,7 +738,7 @@ cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl) {
 // run on the column kernel (column_nz).
 bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, long long cells, unsigned shapes,
                   int ctas, bool fuse_cfl = false, bool grav = false, int col_level = -1) {
-  BatchArgs a;
+  BatchArgs a{};
   a.lv = d_lv;
   a.work = work;
   a.nwork = nwork;
@@ -722,6 +747,8 @@ bool launch_batch(LevelArgs *d_lv, const int *work, int nwork, const int *gate, 
   a.status = g.d_status;
   a.wait_limit = g.wait_limit;
   a.smax = fuse_cfl ? g.d_S->smax_next : nullptr;
+  a.ticket = g.d_S->ticket;
+  a.zero_c = 0;  // the level schedule clears a level's corrections when its iteration starts
   TimedLaunch tl{};
   cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
   cudaStreamIsCapturing(g.stream, &cap);
@@ -840,6 +867,18 @@ bool emit_level(int L, int nsub) {
   return true;
 }
 
+// The subcycled coarse step runs as one fused kernel (step_kernel.cuh) unless the
+// option turns it off or the tree needs work that kernel does not do: the
+// interpolation of coarser neighbours (gravity and transmissive trees) or a level
+// on the column kernel.
+bool fused_step_ok() {
+  if (g.opt.fused_step < 0 || g.res.host.grav || g.opt.trans_flags != 0) return false;
+  if (g.opt.dual_energy && kLaunchTracers != 0u) return false;
+  for (int L = g.res.lcoarse; L <= finest_level(); L++)
+    if (g.res.lev[L].nv > 0 || column_nz(L) > 0) return false;
+  return true;
+}
+
 // one coarse step, all on the device
 bool emit_coarse_step(int nsub) {
   const Tree &t = g.res;
@@ -876,13 +915,37 @@ bool emit_coarse_step(int nsub) {
     k_batch_end<<<1, 1, 0, g.stream>>>(S, t.d_lv);
     return ck(cudaGetLastError(), "schedule kernel");
   }
+  if (g.step_groups > 0 && fused_step_ok()) {
+    // the whole recursion in one persistent kernel (step_kernel.cuh)
+    if (!ck(cudaMemsetAsync(g.d_ctl, 0, sizeof(StepCtl), g.stream), "memset step control")) return false;
+    StepArgs a{};
+    a.lv = t.d_lv;
+    a.S = S;
+    a.ctl = g.d_ctl;
+    a.done = g.d_done;
+    a.status = g.d_status;
+    a.wait_limit = g.wait_limit;
+    a.lfine = lf;
+    a.jobt = g.d_jobt;
+    const unsigned variant = (g.opt.dual_energy ? kLaunchDual : 0u) | kLaunchTracers;
+    const cudaError_t e = (g.opt.precision == EMMA_PREC_MIXED)
+                              ? launch_step_f32(a, variant, g.step_groups, g.nsm, g.stream, &g.step_grid,
+                                                &g.step_threads)
+                              : launch_step_fp64(a, variant, g.step_groups, g.nsm, g.stream, &g.step_grid,
+                                                 &g.step_threads);
+    g.kernel_launches++;
+    g.graph_is_fused = true;
+    return ck(e, "fused coarse step");
+  }
   if (!emit_level(lc, nsub)) return false;
   k_sub_final<<<1, 1, 0, g.stream>>>(S);
   return ck(cudaGetLastError(), "schedule kernel");
 }
 
 bool ensure_graph(int nsub) {
-  if (g.graph && g.graph_nsub == nsub && g.graph_prec == g.opt.precision && g.graph_col == g.opt.column) return true;
+  if (g.graph && g.graph_nsub == nsub && g.graph_prec == g.opt.precision && g.graph_col == g.opt.column &&
+      g.graph_groups == g.step_groups)
+    return true;
   drop_graph();
   cudaGraph_t graph = nullptr;
   if (!ck(cudaStreamBeginCapture(g.stream, cudaStreamCaptureModeThreadLocal), "begin capture")) return false;
@@ -891,6 +954,16 @@ bool ensure_graph(int nsub) {
   if (!ok || !ck(e, "end capture")) {
     if (graph) cudaGraphDestroy(graph);
     return false;
+  }
+  size_t nn = 0;
+  int kn = 0;
+  if (cudaGraphGetNodes(graph, nullptr, &nn) == cudaSuccess && nn > 0) {
+    std::vector<cudaGraphNode_t> nodes(nn);
+    if (cudaGraphGetNodes(graph, nodes.data(), &nn) == cudaSuccess)
+      for (size_t i = 0; i < nn; i++) {
+        cudaGraphNodeType ty;
+        if (cudaGraphNodeGetType(nodes[i], &ty) == cudaSuccess && ty == cudaGraphNodeTypeKernel) kn++;
+      }
   }
   e = cudaGraphInstantiate(&g.graph, graph, 0);
   cudaGraphDestroy(graph);
@@ -901,6 +974,8 @@ bool ensure_graph(int nsub) {
   g.graph_nsub = nsub;
   g.graph_prec = g.opt.precision;
   g.graph_col = g.opt.column;
+  g.graph_groups = g.step_groups;
+  g.graph_kernels = kn;
   return true;
 }
 
@@ -982,6 +1057,7 @@ void emma_hydro_default_options(struct EmmaHydroOptions *opt) {
   opt->gravity = 0;
   opt->dual_energy = 0;
   opt->column = 0;
+  opt->fused_step = 0;
 }
 
 int emma_hydro_init(const struct EmmaHydroOptions *opt) {
@@ -1000,6 +1076,10 @@ int emma_hydro_init(const struct EmmaHydroOptions *opt) {
   CK(cudaMemset(g.d_done, 0, sizeof(unsigned) * kMaxLevels));
   CK(cudaMalloc(&g.d_S, sizeof(SchedState)));
   CK(cudaMemset(g.d_S, 0, sizeof(SchedState)));
+  CK(cudaMalloc(&g.d_ctl, sizeof(StepCtl)));
+  CK(cudaMemset(g.d_ctl, 0, sizeof(StepCtl)));
+  CK(cudaMalloc(&g.d_jobt, sizeof(StepJobRecord) * kStepJobLog));
+  CK(cudaMemset(g.d_jobt, 0, sizeof(StepJobRecord) * kStepJobLog));
   CK(cudaMallocHost(&g.h_S, sizeof(SchedState)));
   std::memset(g.h_S, 0, sizeof(SchedState));
   g.ready = true;
@@ -1011,6 +1091,7 @@ int emma_hydro_set_options(const struct EmmaHydroOptions *opt) {
   if (!g.ready) return emma_hydro_init(opt);
   const int old_trans = g.opt.trans_flags, old_grav = g.opt.gravity, old_dual = g.opt.dual_energy;
   g.opt = *opt;
+  g.step_groups = -2;  // the coarse-step mode is chosen again for the new options
   if (old_trans != opt->trans_flags || old_grav != opt->gravity || old_dual != opt->dual_energy) {
     // the tile plans encode the boundary ghosts and the gravity interpolation lists:
     // a resident tree must be uploaded again
@@ -1041,6 +1122,8 @@ void emma_hydro_shutdown(void) {
   cudaFree(g.d_status);
   cudaFree(g.d_done);
   cudaFree(g.d_S);
+  cudaFree(g.d_ctl);
+  cudaFree(g.d_jobt);
   cudaFreeHost(g.h_S);
   if (g.pin) cudaFreeHost(g.pin);
   if (g.own_stream) cudaStreamDestroy(g.stream);
@@ -1522,11 +1605,126 @@ int emma_hydro_advance_level(int level, double dt) {
   CK(launch_interp(g.res.d_lv, level, d.nv, nullptr, g.nsm, g.stream, g.res.host.grav));
   if (!launch_batch(g.res.d_lv, d.work, d.ntiles, nullptr, d.leaf, 1u << d.shape, d.ctas, false, false, level))
     return EMMA_ST_CUDA;
+  g.c_dirty = true;  // the coarser level's corrections wait for an update of that level
   k_swap_level<<<1, 1, 0, g.stream>>>(g.res.d_lv, level, nullptr);
   CK(cudaGetLastError());
   CK(mark_stale(level));
   if (d.az != nullptr) CK(cudaMemsetAsync(&g.d_S->azall[level], 1, sizeof(int), g.stream));  // nonzero
   g.updates += d.leaf;
+  return 0;
+}
+
+}  // extern "C"
+
+namespace {
+
+// tile groups the fused kernel of this build runs with `groups` requested (0 = as
+// many as fit), 0 if that count is not built
+int step_groups_for(int groups) {
+  const unsigned variant = (g.opt.dual_energy ? kLaunchDual : 0u) | kLaunchTracers;
+  return (g.opt.precision == EMMA_PREC_MIXED) ? step_groups_f32(variant, groups) : step_groups_fp64(variant, groups);
+}
+
+// Coarse-step mode of a subcycled resident tree on the graph.  EmmaHydroOptions.
+// fused_step -1: separate launches; k > 0: the fused kernel with k tile groups (or
+// as many as fit); 0: the autotuner runs three coarse steps in each mode (separate
+// launches; the fused kernel with every built group count) from a snapshot of the
+// tree's state (level states, level slots, schedule state), restores it after
+// each, and keeps the fastest.
+bool choose_step_mode(int nsub) {
+  Tree &t = g.res;
+  const int lc = t.lcoarse, lf = finest_level();
+  if (nsub == 1 || lf == lc || !fused_step_ok()) {
+    g.step_groups = 0;
+    return true;
+  }
+  if (g.opt.fused_step > 0) {
+    const int k = step_groups_for(g.opt.fused_step);
+    g.step_groups = k > 0 ? k : step_groups_for(0);
+    return true;
+  }
+  if (g.step_groups != -2 && g.step_tuned_nsub == nsub && g.step_tuned_prec == g.opt.precision) return true;
+  // snapshot
+  if (!ck(cudaStreamSynchronize(g.stream), "sync")) return false;
+  std::vector<LevelArgs> lv(kMaxLevels);
+  SchedState hs;
+  unsigned status0 = 0;
+  if (!ck(cudaMemcpy(lv.data(), t.d_lv, sizeof(LevelArgs) * kMaxLevels, cudaMemcpyDeviceToHost), "read slots") ||
+      !ck(cudaMemcpy(&hs, g.d_S, sizeof(SchedState), cudaMemcpyDeviceToHost), "read schedule") ||
+      !ck(cudaMemcpy(&status0, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost), "read status"))
+    return false;
+  std::vector<double *> snap(kMaxLevels, nullptr);
+  std::vector<size_t> bytes(kMaxLevels, 0);
+  bool ok = true;
+  for (int L = lc; L <= lf && ok; L++) {
+    bytes[L] = sizeof(double) * (5 + kDropinTracer) * (size_t)t.lev[L].n8;
+    ok = ck(cudaMalloc(&snap[L], bytes[L]), "cudaMalloc snapshot") &&
+         ck(cudaMemcpyAsync(snap[L], lv[L].W, bytes[L], cudaMemcpyDeviceToDevice, g.stream), "snapshot");
+  }
+  auto restore = [&]() {
+    bool r = ck(cudaMemcpyAsync(t.d_lv, lv.data(), sizeof(LevelArgs) * kMaxLevels, cudaMemcpyHostToDevice, g.stream),
+                "restore slots") &&
+             ck(cudaMemcpyAsync(g.d_S, &hs, sizeof(SchedState), cudaMemcpyHostToDevice, g.stream), "restore schedule") &&
+             ck(cudaMemcpyAsync(g.d_status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice, g.stream), "status") &&
+             ck(cudaMemsetAsync(g.d_done, 0, sizeof(unsigned) * kMaxLevels, g.stream), "memset done");
+    for (int L = lc; L <= lf && r; L++) {
+      r = ck(cudaMemcpyAsync(lv[L].W, snap[L], bytes[L], cudaMemcpyDeviceToDevice, g.stream), "restore state");
+      const DevLevel &d = t.lev[L];
+      if (r && d.C != nullptr) r = ck(cudaMemsetAsync(d.C, 0, sizeof(double) * cplanes() * d.n8, g.stream), "memset C");
+    }
+    return r && ck(cudaStreamSynchronize(g.stream), "sync");
+  };
+  ok = ok && restore();  // also clears corrections left by host-driven calls
+  g.c_dirty = false;
+  const long long launches0 = g.kernel_launches;
+  cudaEvent_t e0 = get_event(), e1 = get_event();
+  for (int k = 0; k < 5; k++) g.step_sweep[k] = 0.;
+  int best = 0;
+  double best_ms = 0.;
+  for (int cand = 0; cand <= 4 && ok; cand++) {
+    if (cand > 0 && step_groups_for(cand) != cand) continue;  // this group count is not built
+    g.step_groups = cand;
+    drop_graph();
+    if (!ensure_graph(nsub)) {
+      ok = false;
+      break;
+    }
+    // one step to warm up, two timed, from the snapshot each time
+    ok = ck(cudaGraphLaunch(g.graph, g.stream), "graph launch") && ck(cudaEventRecord(e0, g.stream), "event");
+    for (int i = 0; i < 2 && ok; i++) ok = ck(cudaGraphLaunch(g.graph, g.stream), "graph launch");
+    ok = ok && ck(cudaEventRecord(e1, g.stream), "event") && ck(cudaEventSynchronize(e1), "event");
+    float ms = 0.f;
+    unsigned bits = 0;
+    if (ok) ok = ck(cudaEventElapsedTime(&ms, e0, e1), "event time") &&
+                 ck(cudaMemcpy(&bits, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+    ok = ok && restore();
+    if (!ok) break;
+    if ((bits & ~status0) != 0) continue;  // a mode that raised a status is not kept
+    g.step_sweep[cand] = ms / 2.;
+    if (best_ms == 0. || ms / 2. < best_ms) {
+      best_ms = ms / 2.;
+      best = cand;
+    }
+  }
+  g.free_events.push_back(e0);
+  g.free_events.push_back(e1);
+  for (int L = lc; L <= lf; L++) cudaFree(snap[L]);
+  g.kernel_launches = launches0;
+  drop_graph();
+  g.step_groups = ok ? best : 0;
+  g.step_tuned_nsub = nsub;
+  g.step_tuned_prec = g.opt.precision;
+  return ok;
+}
+
+}  // namespace
+
+extern "C" {
+
+int emma_hydro_step_tuning(int *groups, double *sweep_ms) {
+  if (groups) *groups = g.step_groups;
+  if (sweep_ms)
+    for (int k = 0; k < 5; k++) sweep_ms[k] = g.step_sweep[k];
   return 0;
 }
 
@@ -1555,8 +1753,17 @@ int emma_hydro_advance_coarse_step_async(double dt_param, double time_max, int n
   SchedState &h = *g.h_S;
   if (h.dt_param != dt_param || h.time_max != time_max || h.nsub != nsub || h.cfl != g.opt.cfl)
     if (!write_sched_params(dt_param, time_max, nsub, nullptr, nullptr)) return EMMA_ST_CUDA;
+  if (!choose_step_mode(nsub)) return EMMA_ST_CUDA;
   if (!ensure_graph(nsub)) return EMMA_ST_CUDA;
+  if (g.graph_is_fused && g.c_dirty) {  // the fused step expects every correction at zero
+    for (int L = g.res.lcoarse; L <= g.res.lmax; L++) {
+      const DevLevel &d = g.res.lev[L];
+      if (d.C != nullptr) CK(cudaMemsetAsync(d.C, 0, sizeof(double) * cplanes() * d.n8, g.stream));
+    }
+    g.c_dirty = false;
+  }
   CK(cudaGraphLaunch(g.graph, g.stream));
+  if (!g.graph_is_fused) g.c_dirty = true;
   return 0;
 }
 
@@ -1654,6 +1861,48 @@ int emma_hydro_probe_wait_timeout(long long polls) {
   CK(cudaMemcpy(g.d_status, &status0, sizeof(unsigned), cudaMemcpyHostToDevice));
   CK(cudaMemset(g.d_done, 0, sizeof(unsigned) * kMaxLevels));
   return (int)bits;
+}
+
+int emma_hydro_graph_info(int *fused, int *ctas, int *groups, int *kernel_nodes) {
+  if (fused) *fused = g.graph_is_fused ? 1 : 0;
+  if (ctas) *ctas = g.graph_is_fused ? g.step_grid : 0;
+  if (groups) *groups = g.graph_is_fused ? g.step_threads / kThreads : 0;
+  if (kernel_nodes) *kernel_nodes = g.graph ? g.graph_kernels : 0;
+  return 0;
+}
+
+int emma_hydro_timed_coarse_steps(double dt_param, double time_max, int nsub, int nsteps, double *ms) {
+  if (ms == nullptr || nsteps < 1) return EMMA_ST_ARG;
+  cudaEvent_t a = get_event(), b = get_event();
+  int rc = 0;
+  CK(cudaEventRecord(a, g.stream));
+  for (int i = 0; i < nsteps && rc == 0; i++) rc = emma_hydro_advance_coarse_step_async(dt_param, time_max, nsub);
+  CK(cudaEventRecord(b, g.stream));
+  CK(cudaEventSynchronize(b));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, a, b));
+  *ms = f;
+  g.free_events.push_back(a);
+  g.free_events.push_back(b);
+  return rc;
+}
+
+int emma_hydro_fused_job_log(int max, int *kinds, int *levels, double *release_us) {
+  if (!g.ready || max < 0) return -EMMA_ST_ARG;
+  std::vector<StepJobRecord> rec(kStepJobLog);
+  if (cudaStreamSynchronize(g.stream) != cudaSuccess ||
+      cudaMemcpy(rec.data(), g.d_jobt, sizeof(StepJobRecord) * kStepJobLog, cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -EMMA_ST_CUDA;
+  int n = 0;
+  while (n < (int)kStepJobLog && rec[n].kind >= kJobLevel && rec[n].kind <= kJobDone) {
+    if (n < max) {
+      if (kinds) kinds[n] = rec[n].kind;
+      if (levels) levels[n] = rec[n].L;
+      if (release_us) release_us[n] = (double)(long long)(rec[n].t - rec[0].t) * 1e-3;
+    }
+    if (rec[n++].kind == kJobDone) break;
+  }
+  return n;
 }
 
 int emma_hydro_column_tuning(int level, int *planes, double *sweep_ms) {

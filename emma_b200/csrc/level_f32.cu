@@ -2,6 +2,7 @@
 // reconstruction, wave speeds and fluxes; FP64 compensated update.
 #include "level_kernel.cuh"
 #include "column_kernel.cuh"
+#include "step_kernel.cuh"
 
 namespace emma {
 
@@ -12,6 +13,14 @@ cudaError_t launch_level_f32(const BatchArgs &a, unsigned shapes, int nsm, int c
                              int *occupancy) {
   return launch_level_any<MathF32>(a, shapes, nsm, ctas_per_sm, s, occupancy);
 }
+
+// One fused coarse step of a subcycled tree (step_kernel.cuh).
+cudaError_t launch_step_f32(const StepArgs &a, unsigned variant, int groups, int nsm, cudaStream_t s, int *grid,
+                            int *threads) {
+  return launch_step_any<MathF32>(a, variant, groups, nsm, s, grid, threads);
+}
+
+int step_groups_f32(unsigned variant, int groups) { return step_groups_any<MathF32>(variant, groups); }
 
 // Column kernel of a complete periodic level (mixed path), two CTAs per SM.
 cudaError_t launch_column_f32(const ColumnArgs &a, cudaStream_t s) {

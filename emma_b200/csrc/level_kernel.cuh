@@ -170,6 +170,27 @@ __device__ __forceinline__ void slot_tables(unsigned char *tab) {
   }
 }
 
+// Tile groups.  A tile is advanced by kThreads threads; a CTA of the fused coarse
+// step (step_kernel.cuh) runs several tiles at once, one per group of kThreads
+// threads, each group with its own shared-memory region and its own named
+// barrier (1 + group; barrier 0 stays the CTA-wide __syncthreads).  In the level
+// kernel the CTA is one group and the barrier is __syncthreads.
+__device__ __forceinline__ int tile_group() { return (int)(threadIdx.x / kThreads); }
+template <bool GRP>
+__device__ __forceinline__ void tile_sync() {
+  if constexpr (GRP) asm volatile("bar.sync %0, %1;" ::"r"(1 + tile_group()), "n"(kThreads) : "memory");
+  else __syncthreads();
+}
+// Loads of level states.  COH (the fused coarse step, where a state read here was
+// written by another CTA earlier in the same launch): a plain load, which the
+// acquire at the job barrier orders after those writes, never the non-coherent
+// read-only path.
+template <bool COH, class T>
+__device__ __forceinline__ T ld_state(const T *p) {
+  if constexpr (COH) return *p;
+  else return __ldg(p);
+}
+
 // Shared memory of one tile, after the slot tables.  DUAL: dual-energy builds add
 // the internal-energy flux and the normal star velocity of every face.  NTR
 // tracers (-DWRADHYD: 1, with -DHELIUM: 3; not with DUAL): the fraction of every
@@ -224,10 +245,14 @@ struct TileSmem {
 // the next tile's slot descriptors (next_tile >= 0: same level) are loaded
 // while this tile is reconstructed and solved, into the other descriptor
 // buffer; `cur`/`have` track which buffer holds the current tile's.
-template <class M, class G, bool GRAV, bool DUAL, int NTR = 0>
+// smem: the tile's shared memory, offsets TileSmem (the slot tables at `tab`, the
+// per-CTA signal-speed maxima at sSmax, both shared by the CTA's tile groups).
+// COH: the fused coarse step (ld_state, group barriers).
+template <class M, class G, bool GRAV, bool DUAL, int NTR = 0, bool COH = false>
 __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs *gA, const int slot, const int tile,
                                            const int next_tile, unsigned char *smem, const unsigned char *tab,
-                                           unsigned &st, int &cur, bool &have, int &args_slot) {
+                                           unsigned long long *sSmax, unsigned &st, int &cur, bool &have,
+                                           int &args_slot) {
   using R = typename M::R;
   using SM = TileSmem<M, G, DUAL, NTR>;
   constexpr bool TRACER = NTR > 0;
@@ -259,14 +284,16 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   // whose faces enter the p div(u) term (src/hydro_utils.c:2126-2129 sum every face)
   auto recon_ok = [](uint8_t f) { return DUAL ? (f & kFPresent) != 0 : f_ok(f); };
 
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x % kThreads;
   // the level's arguments in shared memory, read again only when the level changes
   LevelArgs &A = *reinterpret_cast<LevelArgs *>(smem + SM::off_args);
   static_assert(sizeof(LevelArgs) % 4 == 0, "LevelArgs copied as 32-bit words");
   if (slot != args_slot) {
-    if (tid < (int)(sizeof(LevelArgs) / 4))
-      reinterpret_cast<uint32_t *>(&A)[tid] = reinterpret_cast<const uint32_t *>(gA)[tid];
-    __syncthreads();
+    if (tid < (int)(sizeof(LevelArgs) / 4)) {
+      const uint32_t *src = reinterpret_cast<const uint32_t *>(gA) + tid;
+      reinterpret_cast<uint32_t *>(&A)[tid] = *src;
+    }
+    tile_sync<COH>();
     args_slot = slot;
   }
   const long long N8 = 8LL * A.noct;
@@ -347,7 +374,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       const uint32_t key = A.keys[(size_t)tile * NS + i];
       build(i, key, split_of(key), mask, 0);
     }
-    __syncthreads();
+    tile_sync<COH>();
   }
   {
     // Thread tid stages the pair q = tid & 3 of x-neighbour children (2q, 2q+1)
@@ -384,13 +411,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         const double *p = (inj ? Wc : W) + (long long)sOb[sg];
         const long long stride = inj ? nc8 : N8;
 #pragma unroll
-        for (int v = 0; v < 5; v++) x0[v] = x1[v] = __ldg(p + v * stride);
+        for (int v = 0; v < 5; v++) x0[v] = x1[v] = ld_state<COH>(p + v * stride);
         if constexpr (TRACER) {
           const double *px = inj ? Xcs : Xs;
           const long long ts = inj ? nc8 : N8;
           if (px != nullptr) {
 #pragma unroll
-            for (int t = 0; t < NTR; t++) t0[t] = t1[t] = __ldg(px + t * ts + (long long)sOb[sg]);
+            for (int t = 0; t < NTR; t++) t0[t] = t1[t] = ld_state<COH>(px + t * ts + (long long)sOb[sg]);
           } else {
             st |= kStTree;
           }
@@ -404,7 +431,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         const bool e0 = (code >> 2) & 1, e1 = (code >> 3) & 1;
 #pragma unroll
         for (int v = 0; v < 5; v++) {
-          const double2 x = __ldg(reinterpret_cast<const double2 *>(p + v * stride));
+          const double2 x = ld_state<COH>(reinterpret_cast<const double2 *>(p + v * stride));
           x0[v] = e0 ? x.y : x.x;
           x1[v] = e1 ? x.y : x.x;
         }
@@ -413,7 +440,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
 #pragma unroll
             for (int t = 0; t < NTR; t++) {
               const double2 x =
-                  __ldg(reinterpret_cast<const double2 *>(Xs + t * N8 + (long long)sOb[sg] + 2 * (code & 3)));
+                  ld_state<COH>(reinterpret_cast<const double2 *>(Xs + t * N8 + (long long)sOb[sg] + 2 * (code & 3)));
               t0[t] = e0 ? x.y : x.x;
               t1[t] = e1 ? x.y : x.x;
             }
@@ -438,7 +465,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       if constexpr (DUAL) {
         // split cells of the level whose stored sound speed is 0
         if (cmk != 1 && !(sf & kFInterp) && ((f0 | f1) & kFSplit)) {
-          const bool all = A.azall != nullptr && *A.azall != 0;
+          const bool all = A.azall != nullptr && ld_state<COH>(A.azall) != 0;
           unsigned code = (unsigned)q | (1u << 3);
           if (cmk >= 2) code = (mir >> (4 * (cmk - 2))) & 15u;
           const long long ib = (long long)sOb[sg] + 2 * (code & 3);
@@ -452,7 +479,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       sSt[b0 + 1] = f1;
     }
   }
-  __syncthreads();
+  tile_sync<COH>();
   // the next tile's slot keys and mask (consumed after the reconstruction phase)
   static_assert(NS <= kThreads, "one slot descriptor per thread");
   const bool pre = next_tile >= 0 && tid < NS;
@@ -480,7 +507,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     const long long stride = (kind == kKeyReal) ? N8 : 8 * A.nv;
 #pragma unroll
     for (int v = 0; v < 3; v++) {
-      const double f = (key != kKeyNone && src != nullptr) ? __ldg(src + v * stride + off) : 0.;
+      const double f = (key != kKeyNone && src != nullptr) ? ld_state<COH>(src + v * stride + off) : 0.;
       g[v] = (R)(-f * 0.5 * A.dt);
     }
   };
@@ -564,7 +591,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       }
     }
   }
-  __syncthreads();
+  tile_sync<COH>();
   if (pre) nraw = split_of(nkey);
   // FP64 gravity: the kick of each brick cell once, for its six face states (the
   // box is dead after P1; the kicks sit after the face fluxes)
@@ -576,7 +603,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       sK[tid] = gk[0];
       sK[kThreads + tid] = gk[1];
       sK[2 * kThreads + tid] = gk[2];
-      __syncthreads();
+      tile_sync<COH>();
     }
   }
 
@@ -745,7 +772,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       solve_face(d, e, tL, bL, jL, tR, bR, jR);
     }
   }
-  __syncthreads();
+  tile_sync<COH>();
 
   // ------------------------------------------------------------------ P3
   // In a batched launch the finer level's update (its corrections into C and
@@ -763,7 +790,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       }
       __threadfence();
     }
-    __syncthreads();
+    tile_sync<COH>();
   }
   const uint8_t fme = sSt[tb];
   double smx = 0.;  // |v| + c_s of the state this thread writes
@@ -777,7 +804,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       q[4] = sMp[tid];
     } else {
 #pragma unroll
-      for (int v = 0; v < 5; v++) q[v] = __ldg(A.W + v * N8 + gi);
+      for (int v = 0; v < 5; v++) q[v] = ld_state<COH>(A.W + v * N8 + gi);
     }
     double Wout[5];
     double Xout[NTR > 0 ? NTR : 1] = {};  // the new tracers
@@ -787,7 +814,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         const long long ch = (A.Wf != nullptr && res_tr) ? A.child[gi] : -1;
 #pragma unroll
         for (int t = 0; t < NTR; t++) {
-          Xout[t] = (Xs != nullptr) ? __ldg(Xs + t * N8 + gi) : 0.;
+          Xout[t] = (Xs != nullptr) ? ld_state<COH>(Xs + t * N8 + gi) : 0.;
           if (ch >= 0) {
             double ax = 0.;
             for (int i = 0; i < 8; i++) ax += __ldcg(A.Wf + (5 + t) * A.nf8 + 8 * ch + i) * 0.125;
@@ -832,6 +859,17 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       auto face_of = [&](int k) {
         return (k < 2) ? (ex + (k & 1)) : ((k < 4) ? (ey + G::CX * (k & 1)) : (ez + G::CX * G::CY * (k & 1)));
       };
+      // correction plane v of this cell, received from the finer level; with
+      // Bt.zero_c the planes read nonzero are cleared after the update (below), so
+      // that the level's corrections are zero again when the finer level next runs
+      // (the fused coarse step clears no buffer).  The stores wait until every plane
+      // is read: a store between the loads would hold the later loads back.
+      unsigned cnz = 0u;
+      auto take_c = [&](int v) -> double {
+        const double c = __ldcg(A.C + v * N8 + gi);
+        if (c != 0.) cnz |= 1u << v;
+        return c;
+      };
       double Ud, Udu, Udv, Udw, UE;
       double Ue = 0.;  // dual energy: the tracked internal energy of the base state
       if (A.B != nullptr) {  // drop-in: W2U of the caller's fieldnew
@@ -850,7 +888,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         UE = q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
         if constexpr (DUAL) {
           Ue = q[4] / (kGam - 1.);
-          if (A.C != nullptr) Ue += __ldcg(A.C + 5 * N8 + gi);
+          if (A.C != nullptr) Ue += take_c(5);
         }
       }
       // dual energy (src/hydro_utils.c:2126-2129, 3064, 3167-3177): the internal-energy
@@ -884,11 +922,11 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         }
         // scatterstencil central update (src/hydro_utils.c:3129-3188), reference order
         if (A.B == nullptr && A.C != nullptr) {
-          Ud += __ldcg(A.C + gi);
-          Udu += __ldcg(A.C + N8 + gi);
-          Udv += __ldcg(A.C + 2 * N8 + gi);
-          Udw += __ldcg(A.C + 3 * N8 + gi);
-          UE += __ldcg(A.C + 4 * N8 + gi);
+          Ud += take_c(0);
+          Udu += take_c(1);
+          Udv += take_c(2);
+          Udw += take_c(3);
+          UE += take_c(4);
         }
         Ud += dU[0];
         Udu += dU[1];
@@ -914,7 +952,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         };
         if (A.B == nullptr && A.C != nullptr) {
 #pragma unroll
-          for (int v = 0; v < 5; v++) add(v, __ldcg(A.C + v * N8 + gi));
+          for (int v = 0; v < 5; v++) add(v, take_c(v));
         }
 #pragma unroll
         for (int v = 0; v < 5; v++) add(v, dU[v] * dtsurdx);
@@ -955,7 +993,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       // leaf velocities after the update, before the next step's CFL term
       if (A.gcorr && grav) {
 #pragma unroll
-        for (int v = 0; v < 3; v++) Wout[1 + v] += (-__ldg(A.F + v * N8 + gi) * A.dt);
+        for (int v = 0; v < 3; v++) Wout[1 + v] += (-ld_state<COH>(A.F + v * N8 + gi) * A.dt);
       }
       if constexpr (TRACER) {
         // tracers: the caller's fieldnew (or field + corrections) plus the flux
@@ -964,8 +1002,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         // (:3197-3203)
 #pragma unroll
         for (int t = 0; t < NTR; t++) {
-          double Ux = (A.BX != nullptr) ? A.BX[t * N8 + gi] : ((Xs != nullptr) ? __ldg(Xs + t * N8 + gi) : 0.);
-          if (A.BX == nullptr && A.C != nullptr) Ux += __ldcg(A.C + (kXPlane + t) * N8 + gi);
+          double Ux = (A.BX != nullptr) ? A.BX[t * N8 + gi] : ((Xs != nullptr) ? ld_state<COH>(Xs + t * N8 + gi) : 0.);
+          if (A.BX == nullptr && A.C != nullptr) Ux += take_c(kXPlane + t);
           double dUx = 0., one = 1.;
 #pragma unroll
           for (int k = 0; k < 6; k++) {
@@ -1001,6 +1039,8 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
             atomicAdd(A.Cc + (kXPlane + t) * A.nc8 + cc, (double)sFX[t * SM::NF + face_of(k)] * dtsurdx * one * 0.125);
         }
       }
+      if (Bt.zero_c)
+        for (unsigned m = cnz; m != 0u; m &= m - 1u) A.C[(__ffs(m) - 1) * N8 + gi] = 0.;
     }
 #pragma unroll
     for (int v = 0; v < 5; v++) A.Wn[v * N8 + gi] = Wout[v];
@@ -1022,11 +1062,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   if (Bt.smax != nullptr) {
     for (int o = 16; o > 0; o >>= 1) smx = fmax(smx, __shfl_xor_sync(0xffffffffu, smx, o));
     if ((tid & 31) == 0 && smx > 0.)
-      atomicMax(reinterpret_cast<unsigned long long *>(smem + kSmaxOff) + slot,
-                (unsigned long long)__double_as_longlong(smx));
+      atomicMax(sSmax + slot, (unsigned long long)__double_as_longlong(smx));
   }
   if (pre) build(tid, nkey, nraw, nmask, nxt);
-  __syncthreads();
+  tile_sync<COH>();
   if (tid == 0) {
     __threadfence();
     atomicAdd(Bt.done + slot, 1u);
@@ -1086,34 +1125,62 @@ __global__ void __launch_bounds__(kThreads, (kMinBlocks<M, SHAPES, DUAL, NTR>))
   int cur = 0, args_slot = -1;
   bool have = false;
   constexpr int kTileMask = (1 << kWorkSlotShift) - 1;
-  for (int w = blockIdx.x; w < Bt.nwork; w += gridDim.x) {
+  // Work queue: items are taken in list order, one ticket per item.  A CTA holds
+  // the ticket of its tile and of the next one (whose descriptors it prefetches
+  // if it is on the same level) and asks for the one after while it works, so
+  // the atomic's latency hides behind the tile.  Slot 0 of the per-CTA maxima (no
+  // level 0) passes tickets on.  Tickets rise along the list, finest level
+  // first: a tile waiting for a finer level holds no finer item.
+  volatile int *sTicket = reinterpret_cast<volatile int *>(sSmax);
+  if (threadIdx.x == 0) {
+    sTicket[0] = (int)atomicAdd(Bt.ticket, 1u);
+    sTicket[1] = (int)atomicAdd(Bt.ticket, 1u);
+  }
+  __syncthreads();
+  int w = sTicket[0], wn = sTicket[1];
+  while (w < Bt.nwork) {
+    unsigned wnn = 0u;
+    if (threadIdx.x == 0) wnn = atomicAdd(Bt.ticket, 1u);  // read after the tile
     const int item = Bt.work[w];
     const int slot = item >> kWorkSlotShift, tile = item & kTileMask;
-    // this CTA's next item: its descriptors are prefetched if it is on the same level
     int next_tile = -1;
-    if (w + (int)gridDim.x < Bt.nwork) {
-      const int itn = Bt.work[w + gridDim.x];
+    if (wn < Bt.nwork) {
+      const int itn = Bt.work[wn];
       if ((itn >> kWorkSlotShift) == slot) next_tile = itn & kTileMask;
     }
     const LevelArgs *gA = Bt.lv + slot;
     if constexpr (SHAPES == 1u) {
-      level_tile<M, GeomA, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
-    } else if constexpr (SHAPES == 2u) {
-      level_tile<M, GeomB, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
+      level_tile<M, GeomA, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem, sSmax, st, cur, have,
                                                args_slot);
+    } else if constexpr (SHAPES == 2u) {
+      level_tile<M, GeomB, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, sSmax, st, cur,
+                                               have, args_slot);
     } else {
       if (gA->shape == 0)
-        level_tile<M, GeomA, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem, st, cur, have, args_slot);
-      else
-        level_tile<M, GeomB, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, st, cur, have,
+        level_tile<M, GeomA, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem, sSmax, st, cur, have,
                                                  args_slot);
+      else
+        level_tile<M, GeomB, GRAV, DUAL, NTR>(Bt, gA, slot, tile, next_tile, smem, smem + kTabOffB, sSmax, st,
+                                                 cur, have, args_slot);
     }
+    if (threadIdx.x == 0) sTicket[0] = (int)wnn;  // every thread read sTicket before the tile's barriers
     __syncthreads();
+    w = wn;
+    wn = sTicket[0];
   }
   // non-negative doubles order like their bit patterns
-  if (Bt.smax != nullptr && threadIdx.x < kMaxLevels && sSmax[threadIdx.x] != 0ULL)
+  if (Bt.smax != nullptr && threadIdx.x > 0 && threadIdx.x < kMaxLevels && sSmax[threadIdx.x] != 0ULL)
     atomicMax(Bt.smax + threadIdx.x, sSmax[threadIdx.x]);
   if (st) atomicOr(Bt.status, st);
+  // the last CTA to finish puts the queue back for the next launch
+  if (threadIdx.x == 0) {
+    __threadfence();
+    if (atomicAdd(Bt.ticket + 1, 1u) == gridDim.x - 1) {
+      Bt.ticket[0] = 0u;
+      Bt.ticket[1] = 0u;
+      __threadfence();
+    }
+  }
 }
 
 }  // namespace emma

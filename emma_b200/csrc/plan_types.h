@@ -133,6 +133,8 @@ struct BatchArgs {
   long long wait_limit; // bounded spin on `done` before reporting a timeout
   unsigned long long *smax;  // per slot: max signal speed |v| + c_s of the states written
                              // (bits of a non-negative double, atomicMax), or null
+  int zero_c;           // clear each correction once the update has read it
+  unsigned *ticket;     // work queue: [0] next item, [1] CTAs finished (reset by the last)
 };
 
 // A launch of the column kernel (column_kernel.cuh): one complete periodic level

@@ -25,7 +25,41 @@ struct SchedState {
   long long updates;                    // cell-updates performed (leaf cells x substeps)
   int lcoarse, lmax, nsub;
   int gate_all;
+  unsigned ticket[2];                   // work queue of the level kernel: next item, CTAs done
+                                        // (the last CTA of a launch puts both back to 0)
 };
+
+// Control block of the fused coarse step (step_kernel.cuh), zeroed before each
+// launch: the grid-wide job barrier, the job in progress and the schedule's
+// position in Advance_level's recursion.
+struct StepCtl {
+  unsigned epoch;    // jobs published so far
+  unsigned arrived;  // CTAs done with the current job
+  unsigned ticket;   // next work item of the current job
+  int kind, L, n, shape;  // the current job: kind, level, work items, brick shape
+  int pc, pcL;       // schedule position (pc 0: start of the coarse step) and its level
+  int pad[7];
+};
+enum : int { kJobNone = 0, kJobLevel = 1, kJobCfl = 2, kJobDone = 3 };
+
+// Arguments of a fused coarse step.
+struct StepArgs {
+  LevelArgs *lv;
+  SchedState *S;
+  StepCtl *ctl;
+  unsigned *done;       // scratch for the tiles' completion counts
+  unsigned *status;
+  long long wait_limit;  // bounded spin of a CTA waiting for the next job
+  int lfine;             // finest level with octs
+  struct StepJobRecord *jobt;  // optional: kStepJobLog records of the jobs' releases
+};
+// One released job of a fused coarse step: the device time (ns, %globaltimer) at its
+// release, its kind and level.
+struct StepJobRecord {
+  unsigned long long t;
+  int kind, L;
+};
+constexpr unsigned kStepJobLog = 256;
 
 __global__ void k_set_args(LevelArgs *lv, int slot, LevelArgs a);
 __global__ void k_bind_level(LevelArgs *lv, int L, int lcoarse, int lmax, double dt);

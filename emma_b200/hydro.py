@@ -13,13 +13,17 @@ from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
 def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0, gravity=False,
-            dual=False, column=0):
+            dual=False, column=0, fused="auto"):
     """tile_octs: 0 = brick shape autotuned per level at upload, 32 = 4x4x2-oct
     bricks, 8 = 2x2x2-oct bricks (four per tile).  gravity: the -DWGRAV coupling
     (forces from ResidentHydro.set_force).  dual: the -DDUAL_E tracked internal energy.
     column (mixed path, complete periodic levels without split cells): 0 = the
     autotuner picks the column kernel or the brick kernel, -1 = brick kernel only,
-    n > 0 = column kernel with n cell planes per work item."""
+    n > 0 = column kernel with n cell planes per work item.  fused (subcycled
+    coarse steps on the graph): "auto" = the autotuner picks the fused kernel (one
+    persistent kernel per coarse step) or the level schedule's separate launches,
+    True = fused with as many tile groups per CTA as fit, an int k = fused with k
+    groups, False = separate launches."""
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
@@ -28,6 +32,14 @@ def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, ti
     o.gravity = 1 if gravity else 0
     o.dual_energy = 1 if dual else 0
     o.column = column
+    if fused == "auto":
+        o.fused_step = 0
+    elif fused is True:
+        o.fused_step = 99
+    elif fused is False:
+        o.fused_step = -1
+    else:
+        o.fused_step = int(fused)
     return o
 
 
@@ -35,17 +47,17 @@ class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
     def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0,
-                 gravity=False, dual=False, column=0):
+                 gravity=False, dual=False, column=0, fused="auto"):
         self.tree = tree
         self.column = column
+        self.fused = fused
         self.gravity, self.dual = gravity, dual
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
         self.trans, self.cfl, self.use_graph, self.tile_octs = trans, cfl, use_graph, tile_octs
         self.precision = precision
         # a tree of the -DWRADHYD layout runs on libemmahydro_rh.so (its tracer advanced too)
         self._L = L = lib("he" if getattr(tree, "he", False) else ("rh" if getattr(tree, "rh", False) else False))
-        o = options(precision, trans, cfl, use_graph=use_graph, tile_octs=tile_octs, gravity=gravity, dual=dual,
-                    column=column)
+        o = self._options()
         check(L.emma_hydro_init(ctypes.byref(o)), "init")
         check(L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
         L.emma_hydro_clear_status()
@@ -53,19 +65,54 @@ class ResidentHydro:
         self.adt = np.zeros(self.lmax)
         self.tsim = 0.0
 
+    def _options(self):
+        return options(self.precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
+                       gravity=self.gravity, dual=self.dual, column=self.column, fused=self.fused)
+
+    def _apply(self):
+        o = self._options()
+        check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
+
     def set_use_graph(self, use_graph):
         """Switch between CUDA-graph coarse steps and the host-driven schedule
         (the resident tree and its tuned plans stay)."""
         self.use_graph = use_graph
-        o = options(self.precision, self.trans, self.cfl, use_graph=use_graph, tile_octs=self.tile_octs,
-                    gravity=self.gravity, dual=self.dual, column=self.column)
-        check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
+        self._apply()
 
     def set_precision(self, precision):
         self.precision = precision
-        o = options(precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
-                    gravity=self.gravity, dual=self.dual, column=self.column)
-        check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
+        self._apply()
+
+    def set_fused(self, fused):
+        """Mode of subcycled graph steps (see options: "auto", True, k, False)."""
+        self.fused = fused
+        self._apply()
+
+    def graph_info(self):
+        """The captured coarse step: (1 if it is one fused kernel, its CTAs, tile groups
+        per CTA, kernel launches of one coarse step)."""
+        f, ctas, groups, kn = ctypes.c_int(), ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._L.emma_hydro_graph_info(ctypes.byref(f), ctypes.byref(ctas), ctypes.byref(groups),
+                                            ctypes.byref(kn)), "graph_info")
+        return f.value, ctas.value, groups.value, kn.value
+
+    def step_tuning(self):
+        """(coarse-step mode: 0 separate launches, k fused with k tile groups; ms per
+        coarse step the autotuner measured, [0] separate launches, [k] k groups)."""
+        groups = ctypes.c_int()
+        sweep = np.zeros(5)
+        check(self._L.emma_hydro_step_tuning(ctypes.byref(groups), ptr(sweep)), "step_tuning")
+        return groups.value, sweep
+
+    def fused_jobs(self):
+        """The jobs of the last fused coarse step: list of (kind, level, duration in us),
+        kind 1 a level iteration, 2 a CFL reduction (the duration runs from its release
+        to the next job's release, the schedule between them included)."""
+        kinds, levels, t = np.zeros(256, np.int32), np.zeros(256, np.int32), np.zeros(256)
+        n = self._L.emma_hydro_fused_job_log(256, ptr(kinds), ptr(levels), ptr(t))
+        if n < 0:
+            check(-n, "fused_job_log")
+        return [(int(kinds[i]), int(levels[i]), float(t[i + 1] - t[i])) for i in range(n - 1)]
 
     def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):
         """Queue one coarse step on the device schedule without waiting."""
@@ -136,9 +183,7 @@ class ResidentHydro:
     def set_column(self, column):
         """Column-kernel option (see options); the resident tree and its plans stay."""
         self.column = column
-        o = options(self.precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
-                    gravity=self.gravity, dual=self.dual, column=column)
-        check(self._L.emma_hydro_set_options(ctypes.byref(o)), "set_options")
+        self._apply()
 
     def download(self):
         check(self._L.emma_hydro_tree_download(self.tree.firstoct), "tree_download")

@@ -4,11 +4,14 @@
     python -m emma_b200.run_case --config turb --level 7 --precision fp64 --steps 2 --dropin rh
     python -m emma_b200.run_case --config turb --level 7 --precision mixed --steps 4 --tracer
     python -m emma_b200.run_case --config random --level 8 --precision mixed --steps 3 --column 32
+    python -m emma_b200.run_case --config cosmo --precision mixed --steps 3 --graph
 
 Used to profile one configuration in isolation (for example under ncu).  --dropin
 runs the drop-in clean_new_hydro + HydroSolver on the finest level of the host tree
 instead of the resident schedule, through libemmahydro.so (plain) or the -DWRADHYD
-library (rh, with an ionised fraction of 1/2).
+library (rh, with an ionised fraction of 1/2).  --graph adds coarse steps on the CUDA
+graph (device time per step; for a subcycled tree on the fused coarse-step kernel,
+the device time of its jobs summed per level).
 """
 import argparse
 import ctypes
@@ -27,6 +30,10 @@ def main():
     ap.add_argument("--tracer", action="store_true", help="resident run of the -DWRADHYD library (dX = d/2)")
     ap.add_argument("--column", type=int, default=0,
                     help="column kernel of complete periodic levels (mixed): 0 autotuned, -1 off, n planes per item")
+    ap.add_argument("--graph", action="store_true", help="also time coarse steps on the CUDA graph")
+    ap.add_argument("--fused", default="auto", choices=["auto", "on", "off", "2", "3", "4"],
+                    help="subcycled graph steps: autotuned, fused kernel (as many tile groups as fit, or k), "
+                         "or the level schedule's separate launches")
     a = ap.parse_args()
     cfg = {"random": lambda: configs.random_uniform(level=a.level), "turb": lambda: configs.turb(level=a.level),
            "sod": lambda: configs.sod(level=a.level), "sedov": configs.sedov, "cosmo": configs.cosmo,
@@ -73,6 +80,37 @@ def main():
                       "avg_launch_ms": tot_ms / max(tot_n, 1), "cells_per_launch": tot_cells / max(tot_n, 1),
                       "kernel_ms_per_step": per_step, "per_level": per_level,
                       "cell_updates_per_s_kernel": tot_cells / (tot_ms * 1e-3) if tot_ms else None}))
+    if a.graph:
+        graph_steps(a, cfg, r, L)
+
+
+def graph_steps(a, cfg, r, L):
+    """Coarse steps on the CUDA graph, timed with CUDA events on the library's stream."""
+    modes = {"auto": "auto", "on": True, "off": False}
+    r.set_fused(modes[a.fused] if a.fused in modes else int(a.fused))
+    r.set_use_graph(True)
+    r.coarse_step(nsub=cfg.nsub)  # captures the graph
+    ms = []
+    jobs = {}
+    for _ in range(a.steps):
+        t = ctypes.c_double()
+        if L.emma_hydro_timed_coarse_steps(1e9, 1e9, cfg.nsub, 1, ctypes.byref(t)) != 0:
+            raise RuntimeError(L.emma_hydro_last_error().decode())
+        ms.append(round(t.value, 4))
+        info = r.graph_info()
+        if info[0]:
+            for kind, lev, us in r.fused_jobs():
+                k = f"{'level' if kind == 1 else 'cfl'}_{lev}"
+                acc = jobs.setdefault(k, [0.0, 0])
+                acc[0] += us
+                acc[1] += 1
+    f, ctas, groups, kernels = r.graph_info()
+    mode, sweep = r.step_tuning()
+    print(json.dumps({"graph": True, "fused": f, "ctas": ctas, "tile_groups_per_cta": groups,
+                      "step_mode": mode, "step_sweep_ms": [round(x, 4) for x in sweep],
+                      "kernels_per_step": kernels, "ms_per_step": ms, "status": r.status(),
+                      "jobs_us_per_step": {k: round(v[0] / a.steps, 1) for k, v in sorted(jobs.items())},
+                      "jobs_per_step": {k: v[1] // a.steps for k, v in sorted(jobs.items())}}))
 
 
 def dropin(a, cfg):

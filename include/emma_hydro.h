@@ -78,6 +78,14 @@ struct EmmaHydroOptions {
                            (16 x 16-cell columns marching through z) or the brick kernel,
                            -1 = brick kernel only, n > 0 = column kernel with n cell planes
                            per work item (even, dividing the level's cells per side) */
+  int fused_step;       /* subcycled coarse steps of a resident tree on the CUDA graph: one
+                           persistent kernel per coarse step that runs the whole level recursion
+                           (plain, dual-energy and tracer trees without gravity or transmissive
+                           boundaries, no level on the column kernel), or the level schedule as
+                           separate launches.  0 = autotuned at the first graph step (each mode
+                           timed over three coarse steps from a snapshot of the state, which is
+                           then restored), -1 = separate launches, k > 0 = fused with k tile
+                           groups per CTA (as many as fit if k is not built) */
 };
 void emma_hydro_default_options(struct EmmaHydroOptions *opt);
 
@@ -253,6 +261,29 @@ int emma_hydro_kernel_timing(double *avg_ms, long long *launches, long long *cel
 /* The same for the single-level launches of one resident level (level -1: the
  * batched launches): total device time (ms), count and cell-updates. */
 int emma_hydro_kernel_timing_level(int level, double *total_ms, long long *launches, long long *cells);
+
+/* The coarse step captured on the CUDA graph (no reference counterpart): *fused = 1
+ * when it is one persistent kernel running the whole level recursion
+ * (EmmaHydroOptions.fused_step), with *ctas CTAs of *groups tile groups each (0
+ * otherwise); *kernel_nodes = the kernel launches of one captured coarse step (0
+ * before the first graph step). */
+int emma_hydro_graph_info(int *fused, int *ctas, int *groups, int *kernel_nodes);
+/* The coarse-step mode of the resident tree (no reference counterpart): *groups = 0
+ * for the level schedule's separate launches, k > 0 for the fused kernel with k
+ * tile groups per CTA, -2 before the first graph step; sweep_ms[5] = the
+ * autotuner's device time per coarse step of the separate launches ([0]) and of
+ * the fused kernel with k groups ([k]), 0 where not timed. */
+int emma_hydro_step_tuning(int *groups, double *sweep_ms);
+/* The jobs of the last fused coarse step (no reference counterpart), after the
+ * step has run: kinds (1 a level iteration's tiles, 2 a CFL reduction, 3 the end
+ * of the step), levels and the device time in microseconds from the step's first
+ * release to each job's release; up to max records.  Returns the number of jobs,
+ * or a negative status. */
+int emma_hydro_fused_job_log(int max, int *kinds, int *levels, double *release_us);
+/* nsteps coarse steps queued as emma_hydro_advance_coarse_step_async does, with
+ * their device time (ms, CUDA events on the library's stream) in *ms (no
+ * reference counterpart). */
+int emma_hydro_timed_coarse_steps(double dt_param, double time_max, int nsub, int nsteps, double *ms);
 
 /* Column kernel of a resident level (no reference counterpart): *planes = the cell
  * planes per work item its launches use with the current options (0: the brick
