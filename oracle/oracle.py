@@ -29,6 +29,7 @@ REF_LIB_RH = os.path.join(HERE, "_ref", "libemmaref_rh.so")
 REF_LIB_SP = os.path.join(HERE, "_ref", "libemmaref_sp.so")
 REF_LIB_MARK = os.path.join(HERE, "_ref", "libemmaref_mark.so")
 REF_LIB_HE = os.path.join(HERE, "_ref", "libemmaref_he.so")
+REF_LIB_IO = os.path.join(HERE, "_ref", "libemmaref_io.so")
 
 HYDROTEST = 0x40
 DUAL_E = 0x80
@@ -176,6 +177,30 @@ def _ref_path(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False, 
 
 def ref_available(tx=False, grav=False, dual=False, rh=False, sp=False, mark=False, he=False):
     return os.path.exists(_ref_path(tx, grav, dual, rh, sp, mark, he))
+
+
+def ref_dump_available():
+    return os.path.exists(REF_LIB_IO)
+
+
+_io_lib = []
+
+
+def ref_dump_alloct(folder, firstoct, lcoarse, lmax, ids, names, rank=0, ndumps=0, tsim=0.0):
+    """The reference's own dumpalloct_serial (src/io.c:1233, oracle/ref_io_driver.c) on a
+    tree of the plain cell layout (any builder: struct OCT and CELL are the reference's):
+    one file per field under folder (which ends with '/')."""
+    if not _io_lib:
+        L = ctypes.CDLL(REF_LIB_IO, mode=os.RTLD_NOW | os.RTLD_LOCAL)
+        L.ref_dump_alloct.argtypes = [ctypes.c_char_p, c_void_p, c_int, c_int, c_int, c_int, c_double, c_int,
+                                      ctypes.POINTER(c_int), ctypes.POINTER(ctypes.c_char_p)]
+        L.ref_dump_alloct.restype = c_int
+        _io_lib.append(L)
+    n = len(ids)
+    id_arr = (c_int * n)(*ids)
+    name_arr = (ctypes.c_char_p * n)(*[x.encode() for x in names])
+    return _io_lib[0].ref_dump_alloct(folder.encode(), firstoct, lcoarse, lmax, rank, ndumps, tsim, n, id_arr,
+                                      name_arr)
 
 
 class RefTree:

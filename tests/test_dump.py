@@ -4,7 +4,9 @@ The library's files are compared byte for byte with the oracle's restatement of
 dumpalloct_serial (oracle/hydro_oracle.c, orc_dump_alloct) on the same tree:
 host trees on the CPU (single rank, one rank of a multi-rank tree, the -DWGRAV
 layout), and on the GPU a resident tree whose hydro fields are gathered from the
-device state, against the oracle on the downloaded tree.
+device state, against the oracle on the downloaded tree.  For trees of the plain
+cell layout both are also compared with the reference's own dumpalloct_serial
+(src/io.c compiled into oracle/_ref/libemmaref_io.so), which pins the restatement.
 """
 import os
 import struct
@@ -33,14 +35,35 @@ def dump_pair(tmp_path, tree, fields, rank=0, ndumps=3, tsim=0.123456789, grav=F
     assert H.dump_alloct(a, tree.firstoct, lc, lm, ids, names, rank=rank, ndumps=ndumps, tsim=tsim, grav=grav) == 0
     assert oracle.Restatement(grav=grav).dump_alloct(b, tree.firstoct, lc, lm, ids, names, rank=rank,
                                                      ndumps=ndumps, tsim=tsim) == 0
+    ref = None
+    if not grav and oracle.ref_dump_available():
+        ref = str(tmp_path / "ref") + "/"
+        os.makedirs(ref)
+        assert oracle.ref_dump_alloct(ref, tree.firstoct, lc, lm, ids, names, rank=rank, ndumps=ndumps,
+                                      tsim=tsim) == 0
     out = {}
     for name in names:
         rel = f"grid_{name}/{name}.{ndumps:05d}.p{rank:05d}"
         with open(a + rel, "rb") as fa, open(b + rel, "rb") as fb:
             da, db = fa.read(), fb.read()
         assert da == db, name
+        if ref is not None:
+            with open(ref + rel, "rb") as fr:
+                assert fr.read() == da, f"{name}: the reference's dumpalloct_serial"
         out[name] = da
     return out
+
+
+@pytest.mark.skipif(not oracle.ref_dump_available(), reason="oracle/_ref io build absent")
+def test_dump_matches_reference_dumpalloct_serial(tmp_path):
+    """The library's dump and the restatement equal the reference's own function's
+    bytes on trees of several depths and on the cosmology-like tree."""
+    for cfg in (configs.small_amr(base=4, radii=(0.3, 0.15)), configs.small_amr(base=3, radii=(0.3,)),
+                configs.cosmo(base=5, lmax=7)):
+        t = cfg.build()
+        d = tmp_path / cfg.name
+        d.mkdir()
+        dump_pair(d, t, FIELDS, ndumps=7, tsim=0.5 ** 7)
 
 
 def parse(data):
@@ -129,7 +152,15 @@ def test_dump_from_resident_device_state(gpu, tmp_path):
     os.makedirs(b)
     assert oracle.Restatement().dump_alloct(b, t.firstoct, cfg.lcoarse, cfg.lmax, ids, names, ndumps=1,
                                             tsim=r.tsim) == 0
+    c = None
+    if oracle.ref_dump_available():
+        c = str(tmp_path / "ref") + "/"
+        os.makedirs(c)
+        assert oracle.ref_dump_alloct(c, t.firstoct, cfg.lcoarse, cfg.lmax, ids, names, ndumps=1, tsim=r.tsim) == 0
     for name in names:
         rel = f"grid_{name}/{name}.00001.p00000"
         with open(a + rel, "rb") as fa, open(b + rel, "rb") as fb:
-            assert fa.read() == fb.read(), name
+            da = fa.read()
+            assert da == fb.read(), name
+        if c is not None:
+            assert open(c + rel, "rb").read() == da, name
