@@ -201,15 +201,26 @@ struct TileSmem {
   static constexpr bool kF64 = sizeof(R) == 8;
   static constexpr int NS = G::kNB * G::kSlots, NBOX = G::kNB * G::kBox, NRING = G::kNB * G::kRing;
   static constexpr int NF = G::kNB * G::kFaces;
+  // FP64 with dual energy or tracers: the faces are solved in two rounds (x and y,
+  // then z) and each round's fluxes summed into the cells before the next, so that
+  // the per-face arrays fit in the staged box; the tracer fractions are kept only
+  // for the cells a face reads (the brick cells, then the ring)
+  static constexpr bool kR2 = kF64 && (DUAL || NTR > 0);
+  static constexpr int NFA = G::kNB * (G::kFX + G::kFY), NFB = G::kNB * G::kFZ;
+  static constexpr int NFS = kR2 ? NFA : NF;  // face entries of the flux arrays
+  static constexpr int NXC = kThreads + NRING;  // compact tracer cells (kR2)
+  // descriptor buffers: the current tile's and the next tile's (prefetched), or one
+  // (FP64 single tracer: no prefetch, so that two CTAs fit an SM)
+  static constexpr int kDB = (kF64 && NTR == 1) ? 1 : 2;
   static constexpr size_t a16(size_t x) { return (x + 15) & ~size_t(15); }
   static constexpr size_t off_args = kTabBytes;                                // LevelArgs of the tile's level
-  // per-slot descriptors, two buffers: the current tile's and the next tile's
-  static constexpr size_t off_key = a16(off_args + sizeof(LevelArgs));         // u32 [2][NS]
-  static constexpr size_t off_ob = a16(off_key + 4 * 2 * NS);                  // i32 [2][NS] source offset
-  static constexpr size_t off_sf = a16(off_ob + 4 * 2 * NS);                   // u8  [2][NS] slot flags
-  static constexpr size_t off_spm = a16(off_sf + 2 * NS);                      // u8  [2][NS] split mask (cell order)
-  static constexpr size_t off_cmk = a16(off_spm + 2 * NS);                     // u8  [2][NS] cell map
-  static constexpr size_t off_st = a16(off_cmk + 2 * NS);                      // u8  [NBOX] cell flags
+  // per-slot descriptors
+  static constexpr size_t off_key = a16(off_args + sizeof(LevelArgs));         // u32 [kDB][NS]
+  static constexpr size_t off_ob = a16(off_key + 4 * kDB * NS);                // i32 [kDB][NS] source offset
+  static constexpr size_t off_sf = a16(off_ob + 4 * kDB * NS);                 // u8  [kDB][NS] slot flags
+  static constexpr size_t off_spm = a16(off_sf + kDB * NS);                    // u8  [kDB][NS] split mask (cell order)
+  static constexpr size_t off_cmk = a16(off_spm + kDB * NS);                   // u8  [kDB][NS] cell map
+  static constexpr size_t off_st = a16(off_cmk + kDB * NS);                    // u8  [NBOX] cell flags
   static constexpr size_t off_W = a16(off_st + NBOX);                          // R4  [NBOX] (d,u,v,w)
   static constexpr size_t off_Wp = a16(off_W + sizeof(R) * 4 * NBOX);          // R   [NBOX] p
   // reconstruction of the brick cells: R4 groups [kMG][kThreads] (slopes, predicted
@@ -223,21 +234,26 @@ struct TileSmem {
   static constexpr size_t off_HS = a16(off_Mp + (kF64 ? sizeof(R) * kThreads : 0));
   static constexpr size_t off_end = a16(off_HS + (kF64 ? sizeof(R) * 5 * NRING : sizeof(R) * 4 * 2 * NRING));
   // face fluxes reuse the staged box, dead after reconstruction
-  static constexpr size_t off_F = off_W;                               // R4 [NF]
-  static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NF);    // R  [NF]
-  static constexpr size_t off_F5 = off_end;                       // R [NF] (DUAL)
-  static constexpr size_t off_S = a16(off_F5 + sizeof(R) * NF);  // R [NF] (DUAL)
-  static constexpr size_t off_X = off_end;                              // R [NTR][NBOX]
-  static constexpr size_t off_FX = a16(off_X + sizeof(R) * NTR * NBOX);  // R [NTR][NF]
-  static constexpr size_t bytes =
-      DUAL ? a16(off_S + sizeof(R) * NF) : (NTR > 0 ? a16(off_FX + sizeof(R) * NTR * NF) : off_end);
+  static constexpr size_t off_F = off_W;                                // R4 [NFS]
+  static constexpr size_t off_F1 = a16(off_F + sizeof(R) * 4 * NFS);    // R  [NFS]
+  static constexpr size_t off_F5 = kR2 ? a16(off_F1 + sizeof(R) * NFS) : off_end;  // R [NFS] (DUAL)
+  static constexpr size_t off_S = a16(off_F5 + sizeof(R) * NFS);                   // R [NFS] (DUAL)
+  // tracers: fractions R [NTR][NBOX] (kR2: [NTR][NXC], after the ring face states),
+  // face fluxes R [NTR][NFS] (kR2: in the box)
+  static constexpr size_t off_X = off_end;
+  static constexpr size_t off_FX = kR2 ? a16(off_F1 + sizeof(R) * NFS) : a16(off_X + sizeof(R) * NTR * NBOX);
+  static constexpr size_t face_end =
+      DUAL ? a16(off_S + sizeof(R) * NFS) : (NTR > 0 ? a16(off_FX + sizeof(R) * NTR * NFS) : off_F1 + sizeof(R) * NFS);
+  static constexpr size_t bytes = kR2 ? (NTR > 0 ? a16(off_X + sizeof(R) * NTR * NXC) : off_end)
+                                      : (DUAL ? face_end : (NTR > 0 ? face_end : off_end));
   static_assert(!(DUAL && NTR > 0), "the tracer variants have no dual energy");
   static_assert(NTR == 0 || NTR == 1 || NTR == 3, "dX alone, or dX and the two helium tracers");
-  static_assert(off_F1 + sizeof(R) * NF <= off_M, "face fluxes must fit in the staged box");
+  static_assert(off_F1 + sizeof(R) * NFS <= off_M, "face fluxes must fit in the staged box");
   // FP64 gravity kicks of the brick cells during P2/P3: R [3][kThreads] at the end of
   // the staged box, after the face fluxes
   static constexpr size_t off_K = off_M - sizeof(R) * 3 * kThreads;
-  static_assert(!kF64 || off_K >= off_F1 + sizeof(R) * NF, "FP64 kicks must not overlap the face fluxes");
+  static_assert(!kF64 || off_K >= off_F1 + sizeof(R) * NFS, "FP64 kicks must not overlap the face fluxes");
+  static_assert(!kR2 || face_end <= off_K, "two-round face arrays must fit in the staged box before the kicks");
 };
 
 // One tile.  Software pipeline over the tiles of a CTA: the level's arguments
@@ -309,6 +325,18 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   G::cell_of(tt, tx, ty, tz);
   const int bo = tn * G::kBox;                 // this brick's box in the tile's boxes
   const int tb = bo + G::box_of(tx, ty, tz);   // this thread's brick cell
+  // compact tracer cell of box cell b (two-round FP64 layout): the brick cell's
+  // thread, kThreads + its ring cell, or -1 where no face reads it
+  auto xc_of = [&](int b) -> int {
+    const int nb = b / G::kBox, bl = b - nb * G::kBox;
+    const int x = bl % G::XX - 2, y = (bl / G::XX) % G::XY - 2, z = bl / G::XS - 2;
+    const bool ix = x >= 0 && x < G::CX, iy = y >= 0 && y < G::CY, iz = z >= 0 && z < G::CZ;
+    if (ix && iy && iz) return nb * G::kCells + x + G::CX * (y + G::CY * z);
+    if (iy && iz && (x == -1 || x == G::CX)) return kThreads + nb * G::kRing + G::ring_index(0, x == G::CX, x, y, z);
+    if (ix && iz && (y == -1 || y == G::CY)) return kThreads + nb * G::kRing + G::ring_index(1, y == G::CY, x, y, z);
+    if (ix && iy && (z == -1 || z == G::CZ)) return kThreads + nb * G::kRing + G::ring_index(2, z == G::CZ, x, y, z);
+    return -1;
+  };
 
   // ------------------------------------------------------------------ P0
   // per slot: key, source offset, flags, split mask in cell order, cell map
@@ -450,10 +478,19 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         }
       }
       if constexpr (TRACER) {  // X0 = dT / (d frac) (src/hydro_utils.c:1245, 1248-1251)
+        if constexpr (SM::kR2) {  // only the cells a face reads
+          const int xc0 = xc_of(b0), xc1 = xc_of(b0 + 1);
 #pragma unroll
-        for (int t = 0; t < NTR; t++) {
-          sX[t * SM::NBOX + b0] = (R)(t0[t] / (x0[0] * (TR::frac(t))));
-          sX[t * SM::NBOX + b0 + 1] = (R)(t1[t] / (x1[0] * (TR::frac(t))));
+          for (int t = 0; t < NTR; t++) {
+            if (xc0 >= 0) sX[t * SM::NXC + xc0] = (R)(t0[t] / (x0[0] * (TR::frac(t))));
+            if (xc1 >= 0) sX[t * SM::NXC + xc1] = (R)(t1[t] / (x1[0] * (TR::frac(t))));
+          }
+        } else {
+#pragma unroll
+          for (int t = 0; t < NTR; t++) {
+            sX[t * SM::NBOX + b0] = (R)(t0[t] / (x0[0] * (TR::frac(t))));
+            sX[t * SM::NBOX + b0 + 1] = (R)(t1[t] / (x1[0] * (TR::frac(t))));
+          }
         }
       }
       V::st(sW, b0, SM::NBOX, (R)x0[0], (R)x0[1], (R)x0[2], (R)x0[3]);
@@ -482,7 +519,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
   tile_sync<COH>();
   // the next tile's slot keys and mask (consumed after the reconstruction phase)
   static_assert(NS <= kThreads, "one slot descriptor per thread");
-  const bool pre = next_tile >= 0 && tid < NS;
+  const bool pre = SM::kDB > 1 && next_tile >= 0 && tid < NS;
   uint32_t nkey = kKeyNone, nmask = 0;
   uint8_t nraw = 0;
   if (pre) {
@@ -656,8 +693,13 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         R xs[2 * NTR];
 #pragma unroll
         for (int t = 0; t < NTR; t++) {
-          xs[2 * t] = sX[t * SM::NBOX + bL];
-          xs[2 * t + 1] = sX[t * SM::NBOX + bR];
+          if constexpr (SM::kR2) {
+            xs[2 * t] = sX[t * SM::NXC + (jL >= 0 ? kThreads + jL : tL)];
+            xs[2 * t + 1] = sX[t * SM::NXC + (jR >= 0 ? kThreads + jR : tR)];
+          } else {
+            xs[2 * t] = sX[t * SM::NBOX + bL];
+            xs[2 * t + 1] = sX[t * SM::NBOX + bR];
+          }
         }
         M::template hllc<NTR>(WL, WR, d, F, st, nullptr, xs, fx);
       } else {
@@ -669,7 +711,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         du[1] = (R)0;  // the internal-energy flux is cancelled too; u* stays for div(u)
       }
     }
-    V::st(sF, e, SM::NF, F[0], F[1], F[2], F[3]);
+    V::st(sF, e, SM::NFS, F[0], F[1], F[2], F[3]);
     sF1[e] = F[4];
     if constexpr (DUAL) {
       sF5[e] = du[0] * du[1];  // (Us.m_n / Us.d) ebar (src/hydro_utils.c:2128)
@@ -677,7 +719,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     }
     if constexpr (TRACER) {
 #pragma unroll
-      for (int t = 0; t < NTR; t++) sFX[t * SM::NF + e] = fx[t];
+      for (int t = 0; t < NTR; t++) sFX[t * SM::NFS + e] = fx[t];
     }
   };
 
@@ -727,10 +769,116 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       solve_face(d, e, tL, bL, jL, tR, bR, jR);
     }
   };
+  // Two-round FP64 layout: this cell's sums over the faces of the rounds already
+  // solved, in the faces' order -x,+x,-y,+y,-z,+z (the sums of P3 below, split after
+  // the y faces), and the fine->coarse corrections of those faces
+  double aU[5] = {0., 0., 0., 0., 0.}, aUe = 0., aDivu = 0., aX[NTR > 0 ? NTR : 1] = {};
+  auto round_face = [&](int d, int nb, int x, int y, int z) {
+    return (d < 2) ? nb * (G::kFX + G::kFY) + G::face_index(d, x, y, z)
+                   : nb * G::kFZ + G::face_index(2, x, y, z) - (G::kFX + G::kFY);
+  };
+  auto face_sums = [&](int k0, int k1) {
+    const uint8_t f = sSt[tb];
+    if (!(f & kFTile) || (f & kFSplit)) return;
+    const double dtsurdx = A.dt / A.dx;
+    R q4;
+    q4 = sMp[tid];
+    const double eold = (double)q4 / (kGam - 1.);
+#pragma unroll
+    for (int k = k0; k < k1; k++) {
+      const int d = k >> 1, up = k & 1;
+      const int e = round_face(d, tn, tx + (d == 0 ? up : 0), ty + (d == 1 ? up : 0), tz + (d == 2 ? up : 0));
+      const double one = up ? -1. : 1.;
+      double F[5];
+      {
+        R f0, f1, f2, f3;
+        V::ld(sF, e, SM::NFS, f0, f1, f2, f3);
+        F[0] = (double)f0;
+        F[1] = (double)f1;
+        F[2] = (double)f2;
+        F[3] = (double)f3;
+        F[4] = (double)sF1[e];
+      }
+#pragma unroll
+      for (int v = 0; v < 5; v++) aU[v] += F[v] * dtsurdx * one;
+      if constexpr (DUAL) {
+        aUe += (double)sF5[e] * dtsurdx * one;
+        const double dl = (kGam - 1.) * (double)sS[e] * eold;
+        aDivu += up ? dl : -dl;
+      }
+      if constexpr (TRACER) {
+#pragma unroll
+        for (int t = 0; t < NTR; t++) aX[t] += (double)sFX[t * SM::NFS + e] * dtsurdx * one;
+      }
+      // fine -> coarse correction into an unsplit coarser neighbour (src/hydro_utils.c:3206-3295)
+      const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+      const int b2 = up ? tb + bs : tb - bs;
+      if (!(sSt[b2] & kFInj) || A.Cc == nullptr) continue;
+      const int bl = b2 - bo;
+      const int x2 = bl % G::XX, y2 = (bl / G::XX) % G::XY, z2 = bl / G::XS;
+      const uint32_t ck = sKey[tn * G::kSlots + (x2 >> 1) + G::SX * ((y2 >> 1) + G::SY * (z2 >> 1))];
+      const long long cc = ((ck >> 28) == kKeyInterp) ? A.vcell[7 * (ck & 0x0FFFFFFFu)] : (ck & 0x0FFFFFFFu);
+      const double cs = up ? 1. : -1.;
+#pragma unroll
+      for (int v = 0; v < 5; v++) atomicAdd(A.Cc + v * A.nc8 + cc, F[v] * dtsurdx * cs * 0.125);
+      if constexpr (DUAL) atomicAdd(A.Cc + 5 * A.nc8 + cc, (double)sF5[e] * dtsurdx * cs * 0.125);
+      if constexpr (TRACER) {
+#pragma unroll
+        for (int t = 0; t < NTR; t++)
+          atomicAdd(A.Cc + (kXPlane + t) * A.nc8 + cc, (double)sFX[t * SM::NFS + e] * dtsurdx * cs * 0.125);
+      }
+    }
+  };
   if constexpr (!F64) {
     solve_axis(std::integral_constant<int, 0>{});
     solve_axis(std::integral_constant<int, 1>{});
     solve_axis(std::integral_constant<int, 2>{});
+  } else if constexpr (SM::kR2) {
+    // FP64 with dual energy or tracers: the x and y faces, their sums, the z faces
+    // (the axis at run time, one copy of the solver, as below)
+#pragma unroll 1
+    for (int round = 0; round < 2; round++) {
+      const int nmain = (round == 0 ? 2 : 1) * kThreads;
+      const int per = (round == 0) ? (G::kPX + G::kPY) : G::kPZ;
+#pragma unroll 1
+      for (int w = tid; w < nmain + G::kNB * per; w += kThreads) {
+        int d, e, tL, bL, jL = -1, tR, bR, jR = -1;
+        if (w < nmain) {
+          d = (round == 0) ? w / kThreads : 2;
+          const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+          const int ts = (d == 0) ? 1 : ((d == 1) ? G::CX : G::CX * G::CY);
+          const int coord = (d == 0) ? tx : ((d == 1) ? ty : tz);
+          e = round_face(d, tn, tx, ty, tz);
+          tR = tid;
+          bR = tb;
+          tL = tid - ts;
+          bL = tb - bs;
+          if (coord == 0) jL = tn * G::kRing + G::ring_index(d, false, tx, ty, tz);
+        } else {
+          const int p = w - nmain, nb = p / per;
+          int j = p - nb * per, x, y, z;
+          if (round == 1) {
+            d = 2; x = j % G::CX; y = j / G::CX; z = G::CZ - 1;
+          } else if (j < G::kPX) {
+            d = 0; x = G::CX - 1; y = j % G::CY; z = j / G::CY;
+          } else {
+            j -= G::kPX;
+            d = 1; x = j % G::CX; y = G::CY - 1; z = j / G::CX;
+          }
+          const int bs = (d == 0) ? 1 : ((d == 1) ? G::XX : G::XS);
+          tL = nb * G::kCells + x + G::CX * (y + G::CY * z);
+          bL = nb * G::kBox + G::box_of(x, y, z);
+          tR = tL;
+          bR = bL + bs;
+          jR = nb * G::kRing + G::ring_index(d, true, x, y, z);
+          e = round_face(d, nb, x + (d == 0), y + (d == 1), z + (d == 2));
+        }
+        solve_face(d, e, tL, bL, jL, tR, bR, jR);
+      }
+      tile_sync<COH>();
+      face_sums(round == 0 ? 0 : 4, round == 0 ? 4 : 6);
+      if (round == 0) tile_sync<COH>();  // the z faces overwrite the arrays
+    }
   } else {
     // FP64: one loop over all faces with the axis at run time (one copy of the
     // FP64 solver; three copies measured slower on trees with strong rarefactions)
@@ -849,7 +997,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       auto flux5 = [&](int k, double F[5]) {
         const int e = (k < 2) ? (ex + (k & 1)) : ((k < 4) ? (ey + G::CX * (k & 1)) : (ez + G::CX * G::CY * (k & 1)));
         R f0, f1, f2, f3;
-        V::ld(sF, e, SM::NF, f0, f1, f2, f3);
+        V::ld(sF, e, SM::NFS, f0, f1, f2, f3);
         F[0] = (double)f0;
         F[1] = (double)f1;
         F[2] = (double)f2;
@@ -895,7 +1043,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
       // flux divergence and the p div(u) term, summed over the faces in the
       // reference's order (x-, x+, y-, y+, z-, z+), eold the cell's old eint
       double dUe = 0., divu = 0.;
-      if constexpr (DUAL) {
+      if constexpr (DUAL && SM::kR2) {  // summed round by round (face_sums)
+        dUe = aUe;
+        divu = aDivu;
+      } else if constexpr (DUAL) {
         const double eold = q[4] / (kGam - 1.);
         double one = 1.;
 #pragma unroll
@@ -911,14 +1062,19 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         // updatefield (src/hydro_utils.c:3050-3082): dU = sum over faces -x,+x,-y,+y,-z,+z
         // of (+-F dt/dx), signs alternating from +
         double dU[5] = {0., 0., 0., 0., 0.};
-        double one = 1.;
+        if constexpr (SM::kR2) {  // summed round by round (face_sums)
 #pragma unroll
-        for (int k = 0; k < 6; k++) {
-          double F[5];
-          flux5(k, F);
+          for (int v = 0; v < 5; v++) dU[v] = aU[v];
+        } else {
+          double one = 1.;
 #pragma unroll
-          for (int v = 0; v < 5; v++) dU[v] += F[v] * dtsurdx * one;
-          one *= -1.;
+          for (int k = 0; k < 6; k++) {
+            double F[5];
+            flux5(k, F);
+#pragma unroll
+            for (int v = 0; v < 5; v++) dU[v] += F[v] * dtsurdx * one;
+            one *= -1.;
+          }
         }
         // scatterstencil central update (src/hydro_utils.c:3129-3188), reference order
         if (A.B == nullptr && A.C != nullptr) {
@@ -1005,10 +1161,14 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
           double Ux = (A.BX != nullptr) ? A.BX[t * N8 + gi] : ((Xs != nullptr) ? ld_state<COH>(Xs + t * N8 + gi) : 0.);
           if (A.BX == nullptr && A.C != nullptr) Ux += take_c(kXPlane + t);
           double dUx = 0., one = 1.;
+          if constexpr (SM::kR2) {  // summed round by round (face_sums)
+            dUx = aX[t];
+          } else {
 #pragma unroll
-          for (int k = 0; k < 6; k++) {
-            dUx += (double)sFX[t * SM::NF + face_of(k)] * dtsurdx * one;
-            one *= -1.;
+            for (int k = 0; k < 6; k++) {
+              dUx += (double)sFX[t * SM::NFS + face_of(k)] * dtsurdx * one;
+              one *= -1.;
+            }
           }
           double x = Ux + dUx;
           if (t == 0 && x < 0) x = 0.;
@@ -1017,9 +1177,10 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         }
       }
 
-      // fine -> coarse correction into unsplit coarser neighbours (src/hydro_utils.c:3206-3295)
+      // fine -> coarse correction into unsplit coarser neighbours (src/hydro_utils.c:3206-3295);
+      // the two-round layout sent them with its sums
 #pragma unroll
-      for (int k = 0; k < 6; k++) {
+      for (int k = 0; k < (SM::kR2 ? 0 : 6); k++) {
         const int bs = (k < 2) ? 1 : ((k < 4) ? G::XX : G::XS);
         const int b2 = (k & 1) ? tb + bs : tb - bs;
         if (!(sSt[b2] & kFInj) || A.Cc == nullptr) continue;
@@ -1036,7 +1197,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
         if constexpr (TRACER) {
 #pragma unroll
           for (int t = 0; t < NTR; t++)
-            atomicAdd(A.Cc + (kXPlane + t) * A.nc8 + cc, (double)sFX[t * SM::NF + face_of(k)] * dtsurdx * one * 0.125);
+            atomicAdd(A.Cc + (kXPlane + t) * A.nc8 + cc, (double)sFX[t * SM::NFS + face_of(k)] * dtsurdx * one * 0.125);
         }
       }
       if (Bt.zero_c)
@@ -1070,7 +1231,7 @@ __device__ __forceinline__ void level_tile(const BatchArgs &Bt, const LevelArgs 
     __threadfence();
     atomicAdd(Bt.done + slot, 1u);
   }
-  have = next_tile >= 0;
+  have = SM::kDB > 1 && next_tile >= 0;
   if (have) cur ^= 1;
 }
 
@@ -1090,16 +1251,19 @@ constexpr size_t level_smem_bytes(unsigned shapes) {
 // launch use (bit i: kShapes[i]); each level's plan names its own.
 // Occupancy targets: the FP32 kernel with 4x4x2 bricks only fits 4 CTAs per SM
 // (64 registers, 55 KB of shared memory); with 2x2x2 bricks shared memory
-// allows 2; the FP64 kernel 2 with 4x4x2 bricks (128 registers, 110 KB), 1 with
-// 2x2x2 bricks.
+// allows 2; the FP64 kernel 2 with 4x4x2 bricks (128 registers, 110 KB; its
+// dual-energy and single-tracer variants too, through their two-round layout), 1
+// with 2x2x2 bricks.
 template <class M, unsigned SHAPES, bool DUAL = false, int NTR = 0>
-constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? ((SHAPES == 1u && !DUAL && NTR == 0) ? 2 : 1)
+constexpr int kMinBlocks = (sizeof(typename M::R) == 8) ? ((SHAPES == 1u && NTR <= 1) ? 2 : 1)
                                                          : (SHAPES == 1u ? (NTR == 3 ? 2 : ((DUAL || NTR > 0) ? 3 : 4))
                                                                          : (NTR == 3 ? 1 : 2));
 // 228 KB of shared memory per SM, 1 KB reserved per CTA
 static_assert(4 * (TileSmem<MathF32, GeomA>::bytes + 1024) <= 228 * 1024, "4 FP32 4x4x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF32, GeomB>::bytes + 1024) <= 228 * 1024, "2 FP32 2x2x2 CTAs per SM");
 static_assert(2 * (TileSmem<MathF64, GeomA>::bytes + 1024) <= 228 * 1024, "2 FP64 4x4x2 CTAs per SM");
+static_assert(2 * (TileSmem<MathF64, GeomA, true>::bytes + 1024) <= 228 * 1024, "2 dual-energy FP64 4x4x2 CTAs");
+static_assert(2 * (TileSmem<MathF64, GeomA, false, 1>::bytes + 1024) <= 228 * 1024, "2 tracer FP64 4x4x2 CTAs");
 static_assert(3 * (TileSmem<MathF32, GeomA, true>::bytes + 1024) <= 228 * 1024, "3 dual-energy FP32 4x4x2 CTAs");
 static_assert(2 * (TileSmem<MathF32, GeomB, true>::bytes + 1024) <= 228 * 1024, "2 dual-energy FP32 2x2x2 CTAs");
 static_assert(TileSmem<MathF64, GeomB, true>::bytes + 1024 <= 227 * 1024, "a dual-energy FP64 2x2x2 CTA");
