@@ -385,31 +385,37 @@ struct MathF32 {
   template <int NT = 1>
   static __device__ __forceinline__ void hllc(const float WL[7], const float WR[7], int n, float F[5], unsigned &st,
                                               float *du = nullptr, const float *xs = nullptr, float *fx = nullptr) {
-    const float dL = WL[0], pL = WL[4], iL = WL[5], aL = WL[6];
-    const float dR = WR[0], pR = WR[4], iR = WR[5], aR = WR[6];
+    const float dL = WL[0], pL = WL[4], aL = WL[6];
+    const float dR = WR[0], pR = WR[4], aR = WR[6];
     const float uL = (n == 0) ? WL[1] : ((n == 1) ? WL[2] : WL[3]);
     const float uR = (n == 0) ? WR[1] : ((n == 1) ? WR[2] : WR[3]);
-    // hybrid PVRS / TRRS / TSRS star pressure (Toro sec. 9.5.2), as the reference
+    // hybrid PVRS / TRRS / TSRS star pressure (Toro sec. 9.5.2), as the reference.
+    // The three estimates are evaluated without branches and one is selected: a
+    // warp whose faces need different ones pays for each of them either way (and
+    // for the divergence), here without the branch bookkeeping.
     const float dbar = 0.5f * (dL + dR), abar = 0.5f * (aL + aR);
     const float ppvrs = 0.5f * ((pL + pR) + (uL - uR) * dbar * abar);
     const float pmax = fmaxf(pL, pR), pmin = fminf(pL, pR);
-    float pstar = ppvrs, ustar;
-    if ((pmax < 2.f * pmin) && (pmin < pstar) && (pstar < pmax)) {
-      ustar = 0.5f * ((uL + uR) + fdiv(pL - pR, dbar * abar));
-    } else if (pstar < pmin) {
-      const float z = (G - 1.f) / (2.f * G), iz = (2.f * G) / (G - 1.f);
-      const float num = aL + aR - (G - 1.f) * 0.5f * (uR - uL);
-      const float den = aL * __powf(pL, -z) + aR * __powf(pR, -z);
-      pstar = __powf(fdiv(num, den), iz);
-      ustar = uL - 2.f * aL / (G - 1.f) * (__powf(fdiv(pstar, pL), z) - 1.f);
-    } else {
-      const float p0 = fmaxf(0.f, ppvrs);
-      const float AL = 2.f / (G + 1.f) * iL, AR = 2.f / (G + 1.f) * iR;
-      const float BL = (G - 1.f) / (G + 1.f) * pL, BR = (G - 1.f) / (G + 1.f) * pR;
-      const float GL = sqrtf(fdiv(AL, p0 + BL)), GR = sqrtf(fdiv(AR, p0 + BR));
-      pstar = fdiv(GL * pL + GR * pR - (uR - uL), GL + GR);
-      ustar = 0.5f * ((uL + uR) + (pstar - pR) * GR - (pstar - pL) * GL);
-    }
+    const bool use_pvrs = (pmax < 2.f * pmin) && (pmin < ppvrs) && (ppvrs < pmax);
+    const bool use_trrs = !use_pvrs && (ppvrs < pmin);
+    const float u_pv = 0.5f * ((uL + uR) + fdiv(pL - pR, dbar * abar));
+    // two rarefactions: p* = (num/den)^(1/z), and (p*/pL)^z = (num/den) pL^-z
+    constexpr float z = (G - 1.f) / (2.f * G), iz = (2.f * G) / (G - 1.f);
+    const float num = aL + aR - (G - 1.f) * 0.5f * (uR - uL);
+    const float pLz = __powf(pL, -z), pRz = __powf(pR, -z);
+    const float ratio = fdiv(num, aL * pLz + aR * pRz);
+    const float p_tr = __powf(ratio, iz);
+    const float u_tr = uL - 2.f * aL / (G - 1.f) * (ratio * pLz - 1.f);
+    // two shocks: g = sqrt(A / (p0 + B)) with A = 2 / ((G + 1) d), one rsqrt a side
+    const float p0 = fmaxf(0.f, ppvrs);
+    const float BL = (G - 1.f) / (G + 1.f) * pL, BR = (G - 1.f) / (G + 1.f) * pR;
+    const float c2 = 0.8660254037844386f;  // sqrt(2 / (G + 1)) for G = 5/3
+    static_assert(G == 5.f / 3.f, "c2 is sqrt(2 / (G + 1))");
+    const float GL = c2 * rsqrtf(dL * (p0 + BL)), GR = c2 * rsqrtf(dR * (p0 + BR));
+    const float p_ts = fdiv(GL * pL + GR * pR - (uR - uL), GL + GR);
+    const float u_ts = 0.5f * ((uL + uR) + (p_ts - pR) * GR - (p_ts - pL) * GL);
+    float pstar = use_pvrs ? ppvrs : (use_trrs ? p_tr : p_ts);
+    float ustar = use_pvrs ? u_pv : (use_trrs ? u_tr : u_ts);
     if (pstar < 0.f) pstar = pstar_exact(dL, uL, pL, aL, dR, uR, pR, aR, &ustar);
     if (pstar < 0.f) st |= kStNegPstar;
     const float g2 = (G + 1.f) / (2.f * G);
