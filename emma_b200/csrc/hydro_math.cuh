@@ -419,8 +419,10 @@ struct MathF32 {
     if (pstar < 0.f) pstar = pstar_exact(dL, uL, pL, aL, dR, uR, pR, aR, &ustar);
     if (pstar < 0.f) st |= kStNegPstar;
     const float g2 = (G + 1.f) / (2.f * G);
-    const float qL = (pstar <= pL) ? 1.f : sqrtf(1.f + g2 * (fdiv(pstar, pL) - 1.f));
-    const float qR = (pstar <= pR) ? 1.f : sqrtf(1.f + g2 * (fdiv(pstar, pR) - 1.f));
+    // shock factors sqrt(1 + g2 (p*/p - 1)) = sqrt(x / p) = x rsqrt(x p), x = p + g2 (p* - p)
+    const float xL = pL + g2 * (pstar - pL), xR = pR + g2 * (pstar - pR);
+    const float qL = (pstar <= pL) ? 1.f : xL * rsqrtf(xL * pL);
+    const float qR = (pstar <= pR) ? 1.f : xR * rsqrtf(xR * pR);
     float SL = uL - aL * qL, SR = uR + aR * qR;
     if (SL > SR) {
       SL = fminf(uL - aL, uR - aR);
