@@ -7,8 +7,10 @@ same tsim and per-cell states to 1e-13 (the fine->coarse corrections are FP64
 atomics, so the last bits of coarse cells next to finer octs depend on their
 order), with one library kernel per captured coarse step.  Also against the
 oracle directly (FP64 per cell <= 1e-12), after a state set from the host (the
-CFL job), after host-driven level calls (the corrections cleared first), and for
-the dual-energy and tracer variants.
+CFL job), after host-driven level calls (the corrections cleared first), for
+the dual-energy and tracer variants and for fewer tile groups per CTA.  The
+coarse-step mode autotuner times each mode from a snapshot of the state and
+restores it: a run that tuned equals one that did not.
 """
 import numpy as np
 import pytest
