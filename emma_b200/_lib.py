@@ -85,7 +85,7 @@ SIGNATURES = [
     ("emma_hydro_kernel_timing", c_int, [P(c_double), P(c_ll), P(c_ll)]),
     ("emma_hydro_kernel_timing_level", c_int, [c_int, P(c_double), P(c_ll), P(c_ll)]),
     ("emma_hydro_graph_info", c_int, [P(c_int), P(c_int), P(c_int), P(c_int)]),
-    ("emma_hydro_fused_job_log", c_int, [c_int, c_void_p, c_void_p, c_void_p]),
+    ("emma_hydro_fused_job_log", c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("emma_hydro_timed_coarse_steps", c_int, [c_double, c_double, c_int, c_int, P(c_double)]),
     ("emma_hydro_step_tuning", c_int, [P(c_int), c_void_p]),
     ("emma_hydro_tuning", c_int, [c_int, P(c_int), P(c_int), c_void_p]),

@@ -1627,10 +1627,10 @@ int step_groups_for(int groups) {
 
 // Coarse-step mode of a subcycled resident tree on the graph.  EmmaHydroOptions.
 // fused_step -1: separate launches; k > 0: the fused kernel with k tile groups (or
-// as many as fit); 0: the autotuner runs three coarse steps in each mode (separate
+// as many as fit); 0: the autotuner runs five coarse steps in each mode (separate
 // launches; the fused kernel with every built group count) from a snapshot of the
 // tree's state (level states, level slots, schedule state), restores it after
-// each, and keeps the fastest.
+// each, and keeps the mode whose fastest step (of the last four) is the fastest.
 bool choose_step_mode(int nsub) {
   Tree &t = g.res;
   const int lc = t.lcoarse, lf = finest_level();
@@ -1677,7 +1677,9 @@ bool choose_step_mode(int nsub) {
   ok = ok && restore();  // also clears corrections left by host-driven calls
   g.c_dirty = false;
   const long long launches0 = g.kernel_launches;
-  cudaEvent_t e0 = get_event(), e1 = get_event();
+  constexpr int kTimed = 4;
+  cudaEvent_t ev[kTimed + 1];
+  for (int i = 0; i <= kTimed; i++) ev[i] = get_event();
   for (int k = 0; k < 5; k++) g.step_sweep[k] = 0.;
   int best = 0;
   double best_ms = 0.;
@@ -1689,25 +1691,29 @@ bool choose_step_mode(int nsub) {
       ok = false;
       break;
     }
-    // one step to warm up, two timed, from the snapshot each time
-    ok = ck(cudaGraphLaunch(g.graph, g.stream), "graph launch") && ck(cudaEventRecord(e0, g.stream), "event");
-    for (int i = 0; i < 2 && ok; i++) ok = ck(cudaGraphLaunch(g.graph, g.stream), "graph launch");
-    ok = ok && ck(cudaEventRecord(e1, g.stream), "event") && ck(cudaEventSynchronize(e1), "event");
-    float ms = 0.f;
+    // one step to warm up, four timed one by one, from the snapshot each time
+    ok = ck(cudaGraphLaunch(g.graph, g.stream), "graph launch") && ck(cudaEventRecord(ev[0], g.stream), "event");
+    for (int i = 0; i < kTimed && ok; i++)
+      ok = ck(cudaGraphLaunch(g.graph, g.stream), "graph launch") && ck(cudaEventRecord(ev[i + 1], g.stream), "event");
+    ok = ok && ck(cudaEventSynchronize(ev[kTimed]), "event");
+    double ms = 0.;
     unsigned bits = 0;
-    if (ok) ok = ck(cudaEventElapsedTime(&ms, e0, e1), "event time") &&
-                 ck(cudaMemcpy(&bits, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
+    for (int i = 0; i < kTimed && ok; i++) {
+      float m = 0.f;
+      ok = ck(cudaEventElapsedTime(&m, ev[i], ev[i + 1]), "event time");
+      if (i == 0 || m < ms) ms = m;
+    }
+    if (ok) ok = ck(cudaMemcpy(&bits, g.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost), "status");
     ok = ok && restore();
     if (!ok) break;
     if ((bits & ~status0) != 0) continue;  // a mode that raised a status is not kept
-    g.step_sweep[cand] = ms / 2.;
-    if (best_ms == 0. || ms / 2. < best_ms) {
-      best_ms = ms / 2.;
+    g.step_sweep[cand] = ms;
+    if (best_ms == 0. || ms < best_ms) {
+      best_ms = ms;
       best = cand;
     }
   }
-  g.free_events.push_back(e0);
-  g.free_events.push_back(e1);
+  for (int i = 0; i <= kTimed; i++) g.free_events.push_back(ev[i]);
   for (int L = lc; L <= lf; L++) cudaFree(snap[L]);
   g.kernel_launches = launches0;
   drop_graph();
@@ -1887,7 +1893,7 @@ int emma_hydro_timed_coarse_steps(double dt_param, double time_max, int nsub, in
   return rc;
 }
 
-int emma_hydro_fused_job_log(int max, int *kinds, int *levels, double *release_us) {
+int emma_hydro_fused_job_log(int max, int *kinds, int *levels, double *release_us, double *schedule_us) {
   if (!g.ready || max < 0) return -EMMA_ST_ARG;
   std::vector<StepJobRecord> rec(kStepJobLog);
   if (cudaStreamSynchronize(g.stream) != cudaSuccess ||
@@ -1899,6 +1905,7 @@ int emma_hydro_fused_job_log(int max, int *kinds, int *levels, double *release_u
       if (kinds) kinds[n] = rec[n].kind;
       if (levels) levels[n] = rec[n].L;
       if (release_us) release_us[n] = (double)(long long)(rec[n].t - rec[0].t) * 1e-3;
+      if (schedule_us) schedule_us[n] = (double)(long long)(rec[n].t - rec[n].t_all) * 1e-3;
     }
     if (rec[n++].kind == kJobDone) break;
   }

@@ -182,12 +182,13 @@ __device__ __forceinline__ void tile_sync() {
   else __syncthreads();
 }
 // Loads of level states.  COH (the fused coarse step, where a state read here was
-// written by another CTA earlier in the same launch): a plain load, which the
-// acquire at the job barrier orders after those writes, never the non-coherent
-// read-only path.
+// written by another CTA earlier in the same launch): through L2 only (ld.global.cg),
+// never the non-coherent read-only path, whose cache may still hold the lines of an
+// earlier job; measured 2.7% faster than plain L1-allocating loads on the cosmology
+// tree and as fast on the Sedov tree, the staged lines being used once per tile.
 template <bool COH, class T>
 __device__ __forceinline__ T ld_state(const T *p) {
-  if constexpr (COH) return *p;
+  if constexpr (COH) return __ldcg(p);
   else return __ldg(p);
 }
 

@@ -53,10 +53,11 @@ struct StepArgs {
   int lfine;             // finest level with octs
   struct StepJobRecord *jobt;  // optional: kStepJobLog records of the jobs' releases
 };
-// One released job of a fused coarse step: the device time (ns, %globaltimer) at its
-// release, its kind and level.
+// One released job of a fused coarse step: the device times (ns, %globaltimer) at
+// which every CTA had reached the barrier before it and at its release (the
+// schedule ran in between), its kind and level.
 struct StepJobRecord {
-  unsigned long long t;
+  unsigned long long t_all, t;
   int kind, L;
 };
 constexpr unsigned kStepJobLog = 256;

@@ -250,6 +250,8 @@ __global__ void __launch_bounds__(NG * kThreads, 1) step_kernel(const StepArgs P
           __nanosleep(32);
         }
         if (!abort) {
+          unsigned long long t_all = 0;
+          if (P.jobt != nullptr) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_all));
           __threadfence();
           ctl->arrived = 0u;
           step_schedule(P);
@@ -258,6 +260,7 @@ __global__ void __launch_bounds__(NG * kThreads, 1) step_kernel(const StepArgs P
           if (P.jobt != nullptr && seen < kStepJobLog) {  // device time of the release
             unsigned long long t;
             asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            P.jobt[seen].t_all = t_all;
             P.jobt[seen].t = t;
             P.jobt[seen].kind = ctl->kind;
             P.jobt[seen].L = ctl->L;

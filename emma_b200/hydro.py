@@ -105,14 +105,15 @@ class ResidentHydro:
         return groups.value, sweep
 
     def fused_jobs(self):
-        """The jobs of the last fused coarse step: list of (kind, level, duration in us),
-        kind 1 a level iteration, 2 a CFL reduction (the duration runs from its release
-        to the next job's release, the schedule between them included)."""
-        kinds, levels, t = np.zeros(256, np.int32), np.zeros(256, np.int32), np.zeros(256)
-        n = self._L.emma_hydro_fused_job_log(256, ptr(kinds), ptr(levels), ptr(t))
+        """The jobs of the last fused coarse step: list of (kind, level, duration in us,
+        schedule in us), kind 1 a level iteration, 2 a CFL reduction; the duration runs
+        from its release to the next job's release and includes the schedule that ran
+        before that release (the last item)."""
+        kinds, levels, t, sch = np.zeros(256, np.int32), np.zeros(256, np.int32), np.zeros(256), np.zeros(256)
+        n = self._L.emma_hydro_fused_job_log(256, ptr(kinds), ptr(levels), ptr(t), ptr(sch))
         if n < 0:
             check(-n, "fused_job_log")
-        return [(int(kinds[i]), int(levels[i]), float(t[i + 1] - t[i])) for i in range(n - 1)]
+        return [(int(kinds[i]), int(levels[i]), float(t[i + 1] - t[i]), float(sch[i + 1])) for i in range(n - 1)]
 
     def step_async(self, dt_param=1e9, time_max=1e9, nsub=2):
         """Queue one coarse step on the device schedule without waiting."""

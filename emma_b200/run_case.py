@@ -99,18 +99,20 @@ def graph_steps(a, cfg, r, L):
         ms.append(round(t.value, 4))
         info = r.graph_info()
         if info[0]:
-            for kind, lev, us in r.fused_jobs():
+            for kind, lev, us, sched in r.fused_jobs():
                 k = f"{'level' if kind == 1 else 'cfl'}_{lev}"
-                acc = jobs.setdefault(k, [0.0, 0])
+                acc = jobs.setdefault(k, [0.0, 0, 0.0])
                 acc[0] += us
                 acc[1] += 1
+                acc[2] += sched
     f, ctas, groups, kernels = r.graph_info()
     mode, sweep = r.step_tuning()
     print(json.dumps({"graph": True, "fused": f, "ctas": ctas, "tile_groups_per_cta": groups,
                       "step_mode": mode, "step_sweep_ms": [round(x, 4) for x in sweep],
                       "kernels_per_step": kernels, "ms_per_step": ms, "status": r.status(),
                       "jobs_us_per_step": {k: round(v[0] / a.steps, 1) for k, v in sorted(jobs.items())},
-                      "jobs_per_step": {k: v[1] // a.steps for k, v in sorted(jobs.items())}}))
+                      "jobs_per_step": {k: v[1] // a.steps for k, v in sorted(jobs.items())},
+                      "schedule_us_per_step": {k: round(v[2] / a.steps, 1) for k, v in sorted(jobs.items())}}))
 
 
 def dropin(a, cfg):

@@ -271,15 +271,16 @@ int emma_hydro_graph_info(int *fused, int *ctas, int *groups, int *kernel_nodes)
 /* The coarse-step mode of the resident tree (no reference counterpart): *groups = 0
  * for the level schedule's separate launches, k > 0 for the fused kernel with k
  * tile groups per CTA, -2 before the first graph step; sweep_ms[5] = the
- * autotuner's device time per coarse step of the separate launches ([0]) and of
- * the fused kernel with k groups ([k]), 0 where not timed. */
+ * autotuner's device time of the fastest of four coarse steps of the separate
+ * launches ([0]) and of the fused kernel with k groups ([k]), 0 where not timed. */
 int emma_hydro_step_tuning(int *groups, double *sweep_ms);
 /* The jobs of the last fused coarse step (no reference counterpart), after the
  * step has run: kinds (1 a level iteration's tiles, 2 a CFL reduction, 3 the end
- * of the step), levels and the device time in microseconds from the step's first
- * release to each job's release; up to max records.  Returns the number of jobs,
- * or a negative status. */
-int emma_hydro_fused_job_log(int max, int *kinds, int *levels, double *release_us);
+ * of the step), levels, the device time in microseconds from the step's first
+ * release to each job's release, and the time the schedule took before it (from
+ * the last CTA's arrival to the release); up to max records, any pointer may be
+ * NULL.  Returns the number of jobs, or a negative status. */
+int emma_hydro_fused_job_log(int max, int *kinds, int *levels, double *release_us, double *schedule_us);
 /* nsteps coarse steps queued as emma_hydro_advance_coarse_step_async does, with
  * their device time (ms, CUDA events on the library's stream) in *ms (no
  * reference counterpart). */
