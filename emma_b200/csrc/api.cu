@@ -603,6 +603,19 @@ inline void finish_prims(struct Wtype &W) {
 // the 6 planes of pw (planes of 8*noct); every cell whose `fieldnew` differs from
 // `field` (after clean_new_hydro: the cells a finer level corrected) appends
 // {cell, d, u, v, w, p, E, tracers} of its fieldnew to exc (kExcRec values).
+// The OR of the bitwise differences of n doubles: 0 exactly when every bit
+// matches (a memcmp equality test without the call and its branches).
+inline uint64_t bits_xor(const double *a, const double *b, int n) {
+  uint64_t d = 0;
+  for (int k = 0; k < n; k++) {
+    uint64_t x, y;
+    std::memcpy(&x, a + k, sizeof(x));
+    std::memcpy(&y, b + k, sizeof(y));
+    d |= x ^ y;
+  }
+  return d;
+}
+
 void pack_cells(const HostLevel &h, long long a, long long b, double *pw, std::vector<double> &exc) {
   const long long n8 = 8LL * h.noct;
   for (long long i = a; i < b; i++) {
@@ -616,17 +629,19 @@ void pack_cells(const HostLevel &h, long long a, long long b, double *pw, std::v
       pw[3 * n8 + k] = W.w;
       pw[4 * n8 + k] = W.p;
       pw[5 * n8 + k] = W.E;
-      double e[kExcRec] = {(double)k, N.d, N.u, N.v, N.w, N.p, N.E};
-      bool tdiff = false;
+      // fieldnew differs from field in d, u, v, w, p, E or a tracer (a is recomputed)
+      uint64_t diff = bits_xor(&W.d, &N.d, 5) | bits_xor(&W.E, &N.E, 1);
 #ifdef EMMA_WRADHYD
-      for (int t = 0; t < kDropinTracer; t++) {
-        pw[(6 + t) * n8 + k] = tracer(W, t);
-        tdiff = tdiff || std::memcmp(&W.dX + t, &N.dX + t, sizeof(double)) != 0;
-        e[7 + t] = tracer(N, t);
-      }
+      for (int t = 0; t < kDropinTracer; t++) pw[(6 + t) * n8 + k] = tracer(W, t);
+      diff |= bits_xor(&W.dX, &N.dX, kDropinTracer);
 #endif
-      if (std::memcmp(&W, &N, 5 * sizeof(double)) != 0 || std::memcmp(&W.E, &N.E, sizeof(double)) != 0 || tdiff)
+      if (diff != 0) {
+        double e[kExcRec] = {(double)k, N.d, N.u, N.v, N.w, N.p, N.E};
+#ifdef EMMA_WRADHYD
+        for (int t = 0; t < kDropinTracer; t++) e[7 + t] = tracer(N, t);
+#endif
         exc.insert(exc.end(), e, e + kExcRec);
+      }
     }
   }
 }
@@ -2441,7 +2456,8 @@ void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, 
     for (long long i = a0; i < b0; i++)
       for (int c = 0; c < 8; c++) {
         struct CELL &cl = v[i]->cell[c];
-        if (std::memcmp(&cl.fieldnew, &cl.field, sizeof(struct Wtype)) != 0) cl.fieldnew = cl.field;
+        if (bits_xor(&cl.fieldnew.d, &cl.field.d, (int)(sizeof(struct Wtype) / sizeof(double))) != 0)
+          cl.fieldnew = cl.field;
       }
   });
   const int rank = dropin_rank(cpu);
