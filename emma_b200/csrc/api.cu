@@ -15,7 +15,9 @@
 #include <mutex>
 #include <string>
 #include <thread>
+#include <fcntl.h>
 #include <pthread.h>
+#include <unistd.h>
 #include <unordered_map>
 #include <unordered_set>
 #include <vector>
@@ -151,6 +153,7 @@ struct Ctx {
   };
   DropCache drop[kMaxLevels];
   std::vector<struct OCT *> lists[kMaxLevels];  // last walk of each level's oct list
+  uintptr_t list_lo[kMaxLevels] = {}, list_hi[kMaxLevels] = {};  // lowest, highest oct address in it
   std::vector<struct OCT *> list_tmp;
   // pinned staging
   double *pin = nullptr;
@@ -2023,25 +2026,87 @@ int emma_hydro_plan_stats(struct OCT **firstoct, int lcoarse, int lmax, int tran
 
 static int dropin_rank(struct CPUINFO *cpu) { return cpu ? *reinterpret_cast<const int *>(cpu) : 0; }
 
+// [lo, hi) lies in mappings of this process that are readable (/proc/self/maps,
+// whose entries come sorted by address); false when it cannot tell.
+static bool range_readable(uintptr_t lo, uintptr_t hi) {
+  const int fd = open("/proc/self/maps", O_RDONLY | O_CLOEXEC);
+  if (fd < 0) return false;
+  std::string text;
+  char buf[1 << 16];
+  for (;;) {
+    const ssize_t r = read(fd, buf, sizeof(buf));
+    if (r < 0) {
+      close(fd);
+      return false;
+    }
+    if (r == 0) break;
+    text.append(buf, (size_t)r);
+  }
+  close(fd);
+  uintptr_t cur = lo;  // [lo, cur) is covered
+  const char *s = text.c_str();
+  while (*s != '\0' && cur < hi) {
+    char *e = nullptr;
+    const uintptr_t a = (uintptr_t)std::strtoull(s, &e, 16);
+    if (e == nullptr || *e != '-') return false;
+    const uintptr_t b = (uintptr_t)std::strtoull(e + 1, &e, 16);
+    if (e == nullptr || *e != ' ') return false;
+    const bool readable = e[1] == 'r';
+    if (a > cur) return false;  // a gap before the next mapping
+    if (b > cur) {
+      if (!readable) return false;
+      cur = b;
+    }
+    const char *nl = std::strchr(e, '\n');
+    if (nl == nullptr) break;
+    s = nl + 1;
+  }
+  return cur >= hi;
+}
+
 // Oct pointers of level `level` in list order (firstoct[level-1] on).  The
-// serial walk follows `next` only (one cache line per oct) and prefetches
-// those lines along the previous walk of the same level, so an unchanged list
-// is read at memory bandwidth instead of one memory latency per oct; a
-// prefetch never faults, so a list that changed is still walked correctly.
-// Everything else reads the octs in parallel.  The result stays valid until the
-// next walk of the level.
+// result stays valid until the next walk of the level.
+//
+// A list unchanged since the previous walk is confirmed in parallel: every
+// oct's `next` is the following oct of that walk and the last one's is NULL.
+// The confirmation reads the cached octs only when all of them lie in readable
+// mappings of this process (the caller's oct pool), so it cannot fault whatever
+// the caller did to its tree since; a list that changed fails it.  Otherwise
+// (or when it fails) the serial walk follows `next` (one cache line per oct),
+// prefetching those lines along the previous walk (a prefetch never faults).
 static const std::vector<struct OCT *> &walk_level(struct OCT **firstoct, int level) {
   std::vector<struct OCT *> &prev = g.lists[level];
+  const size_t np = prev.size();
+  constexpr size_t kParallelConfirm = 1 << 15;
+  if (np >= kParallelConfirm && prev[0] == firstoct[level - 1] &&
+      range_readable(g.list_lo[level], g.list_hi[level] + sizeof(struct OCT))) {
+    std::atomic<bool> same{true};
+    parallel_for((long long)np, [&](long long a, long long b) {
+      for (long long i = a; i < b; i++) {
+        const struct OCT *nx = (size_t)i + 1 < np ? prev[(size_t)i + 1] : nullptr;
+        if (prev[(size_t)i]->next != nx) {
+          same.store(false, std::memory_order_relaxed);
+          return;
+        }
+        if ((i & 4095) == 0 && !same.load(std::memory_order_relaxed)) return;
+      }
+    });
+    if (same.load()) return prev;
+  }
   std::vector<struct OCT *> &out = g.list_tmp;
   out.clear();
   constexpr size_t kAhead = 24;
-  const size_t np = prev.size();
   size_t i = 0;
+  uintptr_t lo = UINTPTR_MAX, hi = 0;
   for (struct OCT *o = firstoct[level - 1]; o != nullptr; o = o->next, i++) {
     if (i + kAhead < np) __builtin_prefetch(&prev[i + kAhead]->next);
     out.push_back(o);
+    lo = std::min(lo, (uintptr_t)o);
+    hi = std::max(hi, (uintptr_t)o);
   }
   prev.swap(out);
+  g.list_lo[level] = lo;
+  g.list_hi[level] = hi;
   return prev;
 }
 

@@ -399,12 +399,17 @@ struct MathF32 {
     const bool use_pvrs = (pmax < 2.f * pmin) && (pmin < ppvrs) && (ppvrs < pmax);
     const bool use_trrs = !use_pvrs && (ppvrs < pmin);
     const float u_pv = 0.5f * ((uL + uR) + fdiv(pL - pR, dbar * abar));
-    // two rarefactions: p* = (num/den)^(1/z), and (p*/pL)^z = (num/den) pL^-z
-    constexpr float z = (G - 1.f) / (2.f * G), iz = (2.f * G) / (G - 1.f);
+    // two rarefactions: p* = (num/den)^(1/z), and (p*/pL)^z = (num/den) pL^-z;
+    // 1/z = 2G/(G-1) = 5 for G = 5/3: the fifth power by three multiplications
+    // (a negative ratio, a vacuum-generating pair, then gives a negative p* and the
+    // exact solver, as the reference's pow() with its integer exponent does)
+    constexpr float z = (G - 1.f) / (2.f * G);
+    static_assert(2.f * G / (G - 1.f) == 5.f, "p* = ratio^5 needs G = 5/3");
     const float num = aL + aR - (G - 1.f) * 0.5f * (uR - uL);
     const float pLz = __powf(pL, -z), pRz = __powf(pR, -z);
     const float ratio = fdiv(num, aL * pLz + aR * pRz);
-    const float p_tr = __powf(ratio, iz);
+    const float r2 = ratio * ratio;
+    const float p_tr = r2 * r2 * ratio;
     const float u_tr = uL - 2.f * aL / (G - 1.f) * (ratio * pLz - 1.f);
     // two shocks: g = sqrt(A / (p0 + B)) with A = 2 / ((G + 1) d), one rsqrt a side
     const float p0 = fmaxf(0.f, ppvrs);
