@@ -2527,10 +2527,14 @@ void clean_new_hydro(int level, struct RUNPARAMS *param, struct OCT **firstoct, 
   });
   const int rank = dropin_rank(cpu);
   const int lcoarse = param ? reinterpret_cast<const RunParamsHead *>(param)->lcoarse : 1;
-  if (level > lcoarse && level >= 2)
-    for (struct OCT *o = firstoct[level - 2]; o != nullptr; o = o->next)
-      if (o->cpu != rank)
-        for (int c = 0; c < 8; c++) std::memset(&o->cell[c].fieldnew, 0, sizeof(struct Wtype));
+  if (level > lcoarse && level >= 2) {
+    const std::vector<struct OCT *> &vc = walk_level(firstoct, level - 1);
+    parallel_for((long long)vc.size(), [&](long long a0, long long b0) {
+      for (long long i = a0; i < b0; i++)
+        if (vc[i]->cpu != rank)
+          for (int c = 0; c < 8; c++) std::memset(&vc[i]->cell[c].fieldnew, 0, sizeof(struct Wtype));
+    });
+  }
 }
 
 // ------------------------------------------------ device-side refinement
