@@ -88,6 +88,8 @@ struct DevLevel {
   int *marks = nullptr;
   int col_nz = 0;
   double col_sweep_ms[6] = {};  // planes per item 2, 4, 8, 16, 32, 64 (0 = not tried)
+  int col_xs = 0;               // the autotuner's x sweep: 1 warp shuffles, 0 shared memory
+  double col_xs_ms[2] = {};     // its times of the two at col_nz (0 = not timed)
   long long nv = 0;
   int shape = 0;        // brick shape of the plan (kShapes)
   int ctas = 0;         // CTAs per SM of its launches (0: the occupancy limit)
@@ -141,7 +143,7 @@ struct Ctx {
   int *d_work_all = nullptr;     // batched work list, finest level first
   int nwork_all = 0;
   cudaGraphExec_t graph = nullptr;
-  int graph_nsub = -1, graph_prec = -1, graph_col = -2, graph_groups = -3;
+  int graph_nsub = -1, graph_prec = -1, graph_col = -2, graph_colx = -2, graph_groups = -3;
   bool graph_is_fused = false;   // the captured coarse step is one fused kernel
   int graph_kernels = 0;         // kernel nodes of the captured coarse step
   // drop-in cache: one mirror of levels L-1..L+1 per advanced level L, so that a
@@ -369,6 +371,7 @@ void drop_graph() {
   g.graph = nullptr;
   g.graph_nsub = g.graph_prec = -1;
   g.graph_col = -2;
+  g.graph_colx = -2;
   g.graph_groups = -3;
   g.graph_is_fused = false;
   g.graph_kernels = 0;
@@ -734,7 +737,13 @@ int column_nz(int L) {
   return d.col_nz;
 }
 
-cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl) {
+// x sweep of the column-kernel launches of resident level L (ColumnArgs::xshfl)
+int column_xs(int L) {
+  if (g.opt.column_xshfl != 0) return g.opt.column_xshfl > 0 ? 1 : 0;
+  return g.opt.column > 0 ? 0 : g.res.lev[L].col_xs;
+}
+
+cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl, int xs = -1) {
   const DevLevel &d = g.res.lev[L];
   ColumnArgs c;
   c.lv = g.res.d_lv + L;
@@ -747,6 +756,7 @@ cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl) {
   c.gate = gate;
   c.status = g.d_status;
   c.smax = fuse_cfl ? g.d_S->smax_next : nullptr;
+  c.xshfl = xs >= 0 ? xs : column_xs(L);
   return launch_column_f32(c, g.stream);
 }
 
@@ -962,6 +972,7 @@ bool emit_coarse_step(int nsub) {
 
 bool ensure_graph(int nsub) {
   if (g.graph && g.graph_nsub == nsub && g.graph_prec == g.opt.precision && g.graph_col == g.opt.column &&
+      g.graph_colx == g.opt.column_xshfl &&
       g.graph_groups == g.step_groups)
     return true;
   drop_graph();
@@ -992,6 +1003,7 @@ bool ensure_graph(int nsub) {
   g.graph_nsub = nsub;
   g.graph_prec = g.opt.precision;
   g.graph_col = g.opt.column;
+  g.graph_colx = g.opt.column_xshfl;
   g.graph_groups = g.step_groups;
   g.graph_kernels = kn;
   return true;
@@ -1076,6 +1088,7 @@ void emma_hydro_default_options(struct EmmaHydroOptions *opt) {
   opt->dual_energy = 0;
   opt->column = 0;
   opt->fused_step = 0;
+  opt->column_xshfl = 0;
 }
 
 int emma_hydro_init(const struct EmmaHydroOptions *opt) {
@@ -1322,7 +1335,7 @@ bool autotune_tree(Tree &t, int shape_req) {
         if (!column_nz_ok(d, nz)) continue;
         double ms = 0;
         for (int rep = 0; rep < 4 && ok; rep++) {  // one warm-up, three timed
-          ok = ck(cudaEventRecord(e0, g.stream), "event") && ck(launch_column(L, nz, nullptr, false), "column") &&
+          ok = ck(cudaEventRecord(e0, g.stream), "event") && ck(launch_column(L, nz, nullptr, false, 0), "column") &&
                ck(cudaEventRecord(e1, g.stream), "event") && ck(cudaEventSynchronize(e1), "event");
           float f = 0;
           if (ok && rep > 0 && cudaEventElapsedTime(&f, e0, e1) == cudaSuccess) ms += f / 3.;
@@ -1331,6 +1344,25 @@ bool autotune_tree(Tree &t, int shape_req) {
         if (ok && (best_col == 0 || ms < best_col)) {
           best_col = ms;
           best_nz = nz;
+        }
+      }
+      // the warp-shuffle x sweep at the best depth against the shared-memory one
+      d.col_xs = 0;
+      d.col_xs_ms[0] = best_col;
+      d.col_xs_ms[1] = 0;
+      if (ok && best_nz > 0) {
+        double ms = 0;
+        for (int rep = 0; rep < 4 && ok; rep++) {
+          ok = ck(cudaEventRecord(e0, g.stream), "event") &&
+               ck(launch_column(L, best_nz, nullptr, false, 1), "column") && ck(cudaEventRecord(e1, g.stream), "event") &&
+               ck(cudaEventSynchronize(e1), "event");
+          float f = 0;
+          if (ok && rep > 0 && cudaEventElapsedTime(&f, e0, e1) == cudaSuccess) ms += f / 3.;
+        }
+        d.col_xs_ms[1] = ms;
+        if (ok && ms > 0 && ms < best_col) {
+          d.col_xs = 1;
+          best_col = ms;
         }
       }
       d.col_nz = (ok && best_col > 0 && (best == 0 || best_col < best)) ? best_nz : 0;
@@ -1936,6 +1968,17 @@ int emma_hydro_column_tuning(int level, int *planes, double *sweep_ms) {
   if (planes) *planes = column_nz(level);
   if (sweep_ms)
     for (int i = 0; i < 6; i++) sweep_ms[i] = d.col_sweep_ms[i];
+  return 0;
+}
+
+int emma_hydro_column_xshfl(int level, int *xshfl, double *ms) {
+  if (!level_ok(level)) return EMMA_ST_ARG;
+  const DevLevel &d = g.res.lev[level];
+  if (xshfl) *xshfl = column_nz(level) > 0 ? column_xs(level) : 0;
+  if (ms) {
+    ms[0] = d.col_xs_ms[0];
+    ms[1] = d.col_xs_ms[1];
+  }
   return 0;
 }
 

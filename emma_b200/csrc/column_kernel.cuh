@@ -26,6 +26,15 @@
 // is solved at one call site per axis, so a face on the boundary of two columns
 // (or of two z chunks) gets the same bits in both.
 //
+// XS (warp-shuffle x sweep): a warp holds two 16-cell x rows of the column, so
+// the left neighbour of a column cell is the next lane down.  Each column thread
+// computes both x face states of its own cell and passes the +x one up a lane
+// (__shfl_up_sync) instead of reading the left cell's reconstruction from shared
+// memory; the faces inside the column are solved there.  The column's two x
+// boundary faces are solved by the x = -1 and x = 16 ring threads at the one
+// call site of the shared-memory sweep, so a face shared by two columns still
+// gets the same bits in both.  The autotuner times both sweeps.
+//
 // The reference does the same per oct on a 27-oct copy
 // (src/hydro_utils.c:1407-2238, 2973-3303), recomputing each cell's
 // reconstruction up to 9 times and each face twice.
@@ -80,8 +89,9 @@ __device__ __forceinline__ int pidx(int x, int y) { return (y + 2) * PW + (x + 2
 constexpr int kCornerT0 = kInt - 4;  // column threads that also convert a ring corner column
 }  // namespace col
 
-// The mixed path's column kernel: FP32 reconstruction and fluxes, FP64 update.
-template <int MINB>
+// The mixed path's column kernel: FP32 reconstruction and fluxes, FP64 update;
+// XS: x faces inside the column through warp shuffles.
+template <int MINB, bool XS>
 __global__ void __launch_bounds__(col::kColThreads, MINB) column_kernel(const ColumnArgs a) {
   using namespace col;
   using M = MathF32;
@@ -228,13 +238,46 @@ __global__ void __launch_bounds__(col::kColThreads, MINB) column_kernel(const Co
     F1[f] = F[4];
   };
   // the x and y faces each thread solves: column cells their -x and -y faces, the
-  // +x ring the column's +x boundary faces, the +y ring its +y boundary faces
+  // +x ring the column's +x boundary faces, the +y ring its +y boundary faces.
+  // XS: column cells solve their -x face with the shuffle sweep, except those at
+  // x = 0, whose -x face the -x ring solves at the shared-memory call site.
   const int ring = tid - kInt;
-  const bool solve_x = interior || (ring >= 16 && ring < 32);
+  const bool solve_x = XS ? (ring >= 0 && ring < 32) : (interior || (ring >= 16 && ring < 32));
   const bool solve_y = interior || ring >= 48;
-  const int lx = interior ? ((rx == 0) ? kInt + ry : tid - 1) : (ry * TX + TX - 1);
+  // the x face of a solve_x thread: left and right cell, flux entry
+  int lx, rxc, ex;
+  if (interior) {
+    lx = (rx == 0) ? kInt + ry : tid - 1;
+    rxc = tid;
+    ex = tid;
+  } else if (XS && ring < 16) {  // the column's -x boundary face: the ring cell | column cell (0, y)
+    lx = tid;
+    rxc = ry * TX;
+    ex = ry * TX;
+  } else {  // the column's +x boundary face: column cell (15, y) | the ring cell
+    lx = ry * TX + TX - 1;
+    rxc = tid;
+    ex = kInt + ry;
+  }
   const int ly = interior ? ((ry == 0) ? kInt + 32 + rx : tid - TX) : ((TY - 1) * TX + rx);
-  const int ex = interior ? tid : kInt + ry, ey = interior ? tid : kInt + rx;
+  const int ey = interior ? tid : kInt + rx;
+  // XS: the -x faces inside the column; every column thread takes part in the
+  // shuffle (column warps are whole), those at x = 0 drop their result
+  auto solve_x_shfl = [&](const float4 *R, int fb) {
+    float X[5], Dd[5], Wp[7], WL[7], WR[7], F[5];
+    rload(R, tid, std::integral_constant<int, 0>{}, X, Dd);
+    M::face_px(X, Dd, 1, Wp, st);  // toward +x: the right neighbour's left state
+    M::face_px(X, Dd, 0, WR, st);
+#pragma unroll
+    for (int k = 0; k < 7; k++) WL[k] = __shfl_up_sync(0xffffffffu, Wp[k], 1);
+    unsigned sx = 0;
+    M::hllc(WL, WR, 0, F, sx);
+    if (rx != 0) {
+      st |= sx;
+      F4[fb + tid] = make_float4(F[0], F[1], F[2], F[3]);
+      F1[fb + tid] = F[4];
+    }
+  };
   // the +x and +y fluxes of a column cell
   const int px = (rx == TX - 1) ? kInt + ry : tid + 1, py = (ry == TY - 1) ? kInt + rx : tid + TX;
 
@@ -269,7 +312,9 @@ __global__ void __launch_bounds__(col::kColThreads, MINB) column_kernel(const Co
       const float4 *Rc = Rg + (zs & 1) * 5 * kRec, *Rb = Rg + ((zs - 1) & 1) * 5 * kRec;
       const int fb = (zs & 1) * 3 * kFl;
       if (zs < z1) {  // the plane above the column only closes its top face
-        if (solve_x) solve(std::integral_constant<int, 0>{}, Rc, lx, Rc, tid, fb + ex);
+        if constexpr (XS)
+          if (interior) solve_x_shfl(Rc, fb);
+        if (solve_x) solve(std::integral_constant<int, 0>{}, Rc, lx, Rc, rxc, fb + ex);
         if (solve_y) solve(std::integral_constant<int, 1>{}, Rc, ly, Rc, tid, fb + kFl + ey);
       }
       if (interior) solve(std::integral_constant<int, 2>{}, Rb, tid, Rc, tid, fb + 2 * kFl + tid);

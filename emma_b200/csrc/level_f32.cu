@@ -22,7 +22,8 @@ cudaError_t launch_step_f32(const StepArgs &a, unsigned variant, int groups, int
 
 int step_groups_f32(unsigned variant, int groups) { return step_groups_any<MathF32>(variant, groups); }
 
-// Column kernel of a complete periodic level (mixed path), two CTAs per SM.
+// Column kernel of a complete periodic level (mixed path), two CTAs per SM; the
+// shared-memory or the warp-shuffle x sweep (ColumnArgs::xshfl).
 cudaError_t launch_column_f32(const ColumnArgs &a, cudaStream_t s) {
   constexpr int kMaxDev = 64;
   static bool attr_set[kMaxDev] = {false};  // the shared-memory limit is a per-device attribute
@@ -31,12 +32,17 @@ cudaError_t launch_column_f32(const ColumnArgs &a, cudaStream_t s) {
   if (e != cudaSuccess) return e;
   if (dev < 0 || dev >= kMaxDev) return cudaErrorInvalidDevice;
   if (!attr_set[dev]) {
-    e = cudaFuncSetAttribute(column_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col::kSmem);
+    e = cudaFuncSetAttribute(column_kernel<2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col::kSmem);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(column_kernel<2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)col::kSmem);
     if (e != cudaSuccess) return e;
     attr_set[dev] = true;
   }
   if (a.nitems <= 0) return cudaSuccess;
-  column_kernel<2><<<a.nitems, col::kColThreads, col::kSmem, s>>>(a);
+  if (a.xshfl)
+    column_kernel<2, true><<<a.nitems, col::kColThreads, col::kSmem, s>>>(a);
+  else
+    column_kernel<2, false><<<a.nitems, col::kColThreads, col::kSmem, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -150,6 +150,7 @@ struct ColumnArgs {
   const int *gate;      // launch does nothing unless *gate != 0 (null: always)
   unsigned *status;
   unsigned long long *smax;  // [L]: max signal speed of the new state (bits of a double), or null
+  int xshfl;            // x faces inside the column through warp shuffles (column_kernel.cuh XS)
 };
 constexpr int kColumnWidth = 16;  // cells per column side
 

@@ -13,7 +13,7 @@ from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
 def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0, gravity=False,
-            dual=False, column=0, fused="auto"):
+            dual=False, column=0, fused="auto", xshfl=0):
     """tile_octs: 0 = brick shape autotuned per level at upload, 32 = 4x4x2-oct
     bricks, 8 = 2x2x2-oct bricks (four per tile).  gravity: the -DWGRAV coupling
     (forces from ResidentHydro.set_force).  dual: the -DDUAL_E tracked internal energy.
@@ -23,7 +23,8 @@ def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, ti
     coarse steps on the graph): "auto" = the autotuner picks the fused kernel (one
     persistent kernel per coarse step) or the level schedule's separate launches,
     True = fused with as many tile groups per CTA as fit, an int k = fused with k
-    groups, False = separate launches."""
+    groups, False = separate launches.  xshfl (column kernel's x sweep): 0 = the
+    autotuner's pick, 1 = warp shuffles, -1 = shared memory."""
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
@@ -32,6 +33,7 @@ def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, ti
     o.gravity = 1 if gravity else 0
     o.dual_energy = 1 if dual else 0
     o.column = column
+    o.column_xshfl = xshfl
     if fused == "auto":
         o.fused_step = 0
     elif fused is True:
@@ -47,9 +49,10 @@ class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
     def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0,
-                 gravity=False, dual=False, column=0, fused="auto"):
+                 gravity=False, dual=False, column=0, fused="auto", xshfl=0):
         self.tree = tree
         self.column = column
+        self.xshfl = xshfl
         self.fused = fused
         self.gravity, self.dual = gravity, dual
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
@@ -67,7 +70,8 @@ class ResidentHydro:
 
     def _options(self):
         return options(self.precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
-                       gravity=self.gravity, dual=self.dual, column=self.column, fused=self.fused)
+                       gravity=self.gravity, dual=self.dual, column=self.column, fused=self.fused,
+                       xshfl=self.xshfl)
 
     def _apply(self):
         o = self._options()
@@ -181,9 +185,20 @@ class ResidentHydro:
         check(self._L.emma_hydro_column_tuning(level, ctypes.byref(planes), ptr(sweep)), "column_tuning")
         return planes.value, sweep
 
-    def set_column(self, column):
-        """Column-kernel option (see options); the resident tree and its plans stay."""
+    def column_xshfl(self, level):
+        """(1 if the level's column-kernel launches pass x face states by warp shuffle,
+        0 if through shared memory; the autotuner's ms per launch of the shared-memory
+        and the shuffle sweep at the chosen depth, 0 = not timed)."""
+        on = ctypes.c_int()
+        ms = np.zeros(2)
+        check(self._L.emma_hydro_column_xshfl(level, ctypes.byref(on), ptr(ms)), "column_xshfl")
+        return on.value, ms
+
+    def set_column(self, column, xshfl=None):
+        """Column-kernel options (see options); the resident tree and its plans stay."""
         self.column = column
+        if xshfl is not None:
+            self.xshfl = xshfl
         self._apply()
 
     def download(self):

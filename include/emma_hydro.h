@@ -83,9 +83,13 @@ struct EmmaHydroOptions {
                            (plain, dual-energy and tracer trees without gravity or transmissive
                            boundaries, no level on the column kernel), or the level schedule as
                            separate launches.  0 = autotuned at the first graph step (each mode
-                           timed over three coarse steps from a snapshot of the state, which is
+                           timed over five coarse steps from a snapshot of the state, which is
                            then restored), -1 = separate launches, k > 0 = fused with k tile
                            groups per CTA (as many as fit if k is not built) */
+  int column_xshfl;     /* x sweep of the column kernel: the faces inside a 16-cell row solved
+                           from the left cell's face state passed up a lane by a warp shuffle
+                           (1) or read from shared memory (-1); 0 = the faster of the two at
+                           the autotuned depth (shared memory when `column` forces a depth) */
 };
 void emma_hydro_default_options(struct EmmaHydroOptions *opt);
 
@@ -291,6 +295,11 @@ int emma_hydro_timed_coarse_steps(double dt_param, double time_max, int nsub, in
  * kernel), sweep_ms[6] = the autotuner's ms per launch with 2, 4, 8, 16, 32, 64
  * planes per item (0 = not tried). */
 int emma_hydro_column_tuning(int level, int *planes, double *sweep_ms);
+/* The column kernel's x sweep on a resident level (no reference counterpart):
+ * *xshfl = 1 when its launches pass the x face states by warp shuffle, 0 when
+ * they read them from shared memory; ms[2] = the autotuner's ms per launch of the
+ * shared-memory and the shuffle sweep at the chosen depth (0 = not timed). */
+int emma_hydro_column_xshfl(int level, int *xshfl, double *ms);
 /* Autotuner record of a resident level (emma_hydro_tree_upload tunes every
  * level when options.tile_octs == 0): the chosen brick (32 = 4x4x2 octs, one
  * per tile; 8 = 2x2x2 octs, four per tile), the CTAs per SM of its launches,

@@ -6,7 +6,9 @@ steps, mass and total energy conserved to 1e-12 (every face is solved once
 per column and the boundary faces of two columns or z chunks get the same
 bits from both).  Against the brick kernel of the same path: L1 <= 1e-6.  The
 next step's dt from the maximum fused into the kernel equals the FP64
-reduction's over the state it wrote, bit for bit.
+reduction's over the state it wrote, bit for bit.  The warp-shuffle x sweep
+(x face states passed up a lane, the column's x boundary faces solved by the
+ring threads) meets the same bars and matches the shared-memory sweep.
 """
 import numpy as np
 import pytest
@@ -105,7 +107,43 @@ def test_autotuner_sweeps_the_column_kernel(gpu):
     assert (sweep > 0).sum() >= 4  # 2, 4, 8, 16, 32, 64 planes: every divisor of 64 cells tried
     octs, ctas, brick = r.tuning(cfg.lcoarse)
     best_brick = brick[brick > 0].min()
+    best_col = sweep[sweep > 0].min()
+    xs, xms = r.column_xshfl(cfg.lcoarse)
+    # the shuffle x sweep timed at the best depth against the shared-memory one
+    assert xms[0] == best_col and xms[1] > 0
+    best = min(xms)
     if planes:
-        assert sweep[[2, 4, 8, 16, 32, 64].index(planes)] == sweep[sweep > 0].min() <= best_brick
+        assert sweep[[2, 4, 8, 16, 32, 64].index(planes)] == best_col
+        assert xs == (1 if xms[1] < xms[0] else 0)
+        assert best <= best_brick
     else:
-        assert sweep[sweep > 0].min() >= best_brick
+        assert xs == 0 and best >= best_brick
+
+
+@pytest.mark.parametrize("level,nz,with_oracle", [(5, 8, True), (6, 16, True), (7, 32, False)])
+def test_column_warp_shuffle_x_sweep(gpu, level, nz, with_oracle):
+    cfg = configs.random_uniform(level=level)
+    out = {}
+    for xs in (-1, 1):
+        t = cfg.build()
+        m0, e0 = totals(t.get_fields(level)[:5], level)
+        r = ResidentHydro(t, precision=PREC_MIXED, cfl=CFL, column=nz, xshfl=xs)
+        assert r.column_tuning(level)[0] == nz
+        assert r.column_xshfl(level)[0] == (1 if xs > 0 else 0)
+        for _ in range(3):
+            r.coarse_step()
+        assert r.status() == 0
+        fm = r.state(level)
+        m1, e1 = totals(fm, level)
+        assert abs(m1 - m0) <= 1e-12 * m0
+        assert abs(e1 - e0) <= 1e-12 * e0
+        out[xs] = (fm, r.tsim)
+    for x in l1_fields(out[1][0], out[-1][0]):
+        assert x <= 1e-6
+    assert abs(out[1][1] - out[-1][1]) <= 1e-6 * out[-1][1]
+    if with_oracle:
+        to = cfg.build()
+        _, _, err = oracle.Restatement().run(to.firstoct, cfg.lcoarse, cfg.lmax, 3, CFL)
+        assert err == 0
+        for x in l1_fields(out[1][0], to.get_fields(level)[:5]):
+            assert x <= 1e-5
