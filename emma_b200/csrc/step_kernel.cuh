@@ -12,9 +12,12 @@
 // barrier it runs the schedule up to the next job (the same steps, in the same
 // order and with the same IEEE operations, as k_sub_begin / k_sub_dt /
 // k_sub_prelaunch / k_sub_end / k_sub_final) and releases the others.  Only
-// the leader writes the schedule state and the level slots during the launch,
-// so it reads them from its own cache; the signal-speed maxima the other CTAs
-// accumulate with atomics it reads from L2.
+// the leader writes the schedule state and the level slots during the launch.
+// Its threads copy both from L2 (the signal-speed maxima the other CTAs
+// accumulated with atomics included) into CTA 0's tile region, idle between
+// jobs; one thread runs the schedule on that copy and all write it back before
+// the release, so the schedule's many dependent reads cost shared-memory
+// latency instead of an L2 round trip each.
 //
 // Tiles of a level job are taken from a ticket queue by tile groups: a CTA holds
 // as many groups of kThreads threads as the shared memory of the job's brick
@@ -62,12 +65,11 @@ __host__ __device__ constexpr size_t step_smem_bytes() {
 
 // ------------------------------------------------------------------ schedule
 // The dt arithmetic of schedule.cu with explicit IEEE operations (this unit may be
-// built with FMA contraction).
+// built with FMA contraction).  S and lv: the leader's shared-memory copy.
 using VS = SchedState;
 using VLA = LevelArgs;
 __device__ __forceinline__ double step_smax(VS *S, int L) {
-  // accumulated with atomics by every CTA: read from L2
-  return __longlong_as_double((long long)(S->fresh[L] ? __ldcg(S->smax_next + L) : __ldcg(S->smax + L)));
+  return __longlong_as_double((long long)(S->fresh[L] ? S->smax_next[L] : S->smax[L]));
 }
 // L_comptstep_hydro's final step (src/advanceamr.c:135): dt = CFL dx / (3 Smax)
 __device__ __forceinline__ double step_cfl_dt(VS *S, int L) {
@@ -122,12 +124,10 @@ __device__ __forceinline__ void step_sub_end(VS *S, VLA *lv, int L) {
 enum : int { kPcStart = 0, kPcEnter, kPcIter, kPcDt, kPcEnd, kPcReturn };
 
 // Runs Advance_level's recursion from the saved position to the next job and
-// writes it into the control block (one thread).
-static __device__ __noinline__ void step_schedule(const StepArgs &P) {
-  VS *S = P.S;
-  VLA *lv = P.lv;
-  StepCtl *c = P.ctl;
-  const int lc = S->lcoarse, lf = P.lfine;
+// writes it into the control block (one thread; S and lv: the copy in shared
+// memory).
+static __device__ __noinline__ void step_schedule(VS *S, VLA *lv, StepCtl *c, int lf) {
+  const int lc = S->lcoarse;
   int pc = c->pc, L = c->pcL;
   if (pc == kPcStart) {
     pc = kPcEnter;
@@ -203,6 +203,12 @@ __global__ void __launch_bounds__(NG * kThreads, 1) step_kernel(const StepArgs P
   extern __shared__ __align__(16) unsigned char smem[];
   constexpr int NGB = kStepGroupsB<M, DUAL, NTR, NG>;
   static_assert(NG >= 1 && NG <= kStepGroups<M, DUAL, NTR> && NGB >= 1, "a tile of each shape fits");
+  // the leader's copy of the schedule state and the level slots (8-byte words)
+  constexpr int kMirS = (int)(sizeof(SchedState) / 8), kMirL = (int)(kMaxLevels * sizeof(LevelArgs) / 8);
+  static_assert(sizeof(SchedState) % 8 == 0 && sizeof(LevelArgs) % 8 == 0 && kStepRegion0 % 16 == 0, "8-byte words");
+  static_assert(8 * (kMirS + kMirL) <= step_region_bytes<M, GeomA, DUAL, NTR>() &&
+                    8 * (kMirS + kMirL) <= step_region_bytes<M, GeomB, DUAL, NTR>(),
+                "the copy fits in one tile region");
   slot_tables<GeomA>(smem);
   slot_tables<GeomB>(smem + kTabOffB);
   unsigned long long *sSmax = reinterpret_cast<unsigned long long *>(smem + kSmaxOff);
@@ -224,6 +230,7 @@ __global__ void __launch_bounds__(NG * kThreads, 1) step_kernel(const StepArgs P
   unsigned st = 0;
   unsigned seen = 0;  // jobs this CTA has taken
   int kind = kJobNone, L = 0;
+  unsigned long long t_all = 0;  // the leader's job log: when every CTA had arrived
   for (;;) {
     // ---- the end of a job (or the start): flush, arrive, wait for the next job
     __syncthreads();
@@ -238,10 +245,13 @@ __global__ void __launch_bounds__(NG * kThreads, 1) step_kernel(const StepArgs P
       }
       __threadfence();
       atomicAdd(&ctl->arrived, 1u);
-      int abort = 0;
-      long long it = 0;
-      if (blockIdx.x == 0) {
-        // the leader: once every CTA is done with the job, the schedule to the next
+    }
+    if (blockIdx.x == 0) {
+      // the leader: once every CTA is done with the job (thread 0 waits), the
+      // schedule to the next on a shared-memory copy of its state (block-uniform)
+      if (threadIdx.x == 0) {
+        int abort = 0;
+        long long it = 0;
         while (*reinterpret_cast<volatile unsigned *>(&ctl->arrived) < gridDim.x) {
           if (++it > P.wait_limit) {
             abort = 1;
@@ -250,11 +260,31 @@ __global__ void __launch_bounds__(NG * kThreads, 1) step_kernel(const StepArgs P
           __nanosleep(32);
         }
         if (!abort) {
-          unsigned long long t_all = 0;
           if (P.jobt != nullptr) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t_all));
           __threadfence();
           ctl->arrived = 0u;
-          step_schedule(P);
+        }
+        sJob[4] = abort;
+      }
+      __syncthreads();
+      if (!sJob[4]) {
+        unsigned long long *mir = reinterpret_cast<unsigned long long *>(smem + kStepRegion0);
+        const unsigned long long *gS = reinterpret_cast<const unsigned long long *>(P.S);
+        const unsigned long long *gL = reinterpret_cast<const unsigned long long *>(P.lv);
+        for (int i = threadIdx.x; i < kMirS + kMirL; i += blockDim.x)
+          mir[i] = i < kMirS ? __ldcg(gS + i) : __ldcg(gL + (i - kMirS));
+        __syncthreads();
+        if (threadIdx.x == 0) step_schedule(reinterpret_cast<VS *>(mir), reinterpret_cast<VLA *>(mir + kMirS), ctl,
+                                            P.lfine);
+        __syncthreads();
+        unsigned long long *wS = reinterpret_cast<unsigned long long *>(P.S);
+        unsigned long long *wL = reinterpret_cast<unsigned long long *>(P.lv);
+        for (int i = threadIdx.x; i < kMirS + kMirL; i += blockDim.x) {
+          if (i < kMirS) wS[i] = mir[i];
+          else wL[i - kMirS] = mir[i];
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
           // every group starts on two items of its own (below); the queue hands out the rest
           ctl->ticket = 2u * gridDim.x * (ctl->shape == 0 ? NG : NGB);
           if (P.jobt != nullptr && seen < kStepJobLog) {  // device time of the release
@@ -265,11 +295,14 @@ __global__ void __launch_bounds__(NG * kThreads, 1) step_kernel(const StepArgs P
             P.jobt[seen].kind = ctl->kind;
             P.jobt[seen].L = ctl->L;
           }
-          __threadfence();
+          __threadfence();  // the copy written back by every thread (ordered by the barrier) first
           atomicExch(&ctl->epoch, seen + 1);
         }
       }
-      it = 0;
+    }
+    if (threadIdx.x == 0) {
+      int abort = (blockIdx.x == 0) ? sJob[4] : 0;
+      long long it = 0;
       while (!abort && *reinterpret_cast<volatile unsigned *>(&ctl->epoch) == seen) {
         if (++it > P.wait_limit) {
           abort = 1;
