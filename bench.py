@@ -165,13 +165,16 @@ def run_mine(args, rank, world):
             if rec is not None:
                 planes, csweep = r.column_tuning(l)
                 xs, xms = r.column_xshfl(l)
-                sweep = "warp-shuffle" if xs else "shared-memory"
+                bal, bms = r.column_balanced(l)
+                sweep = ("warp-shuffle" if xs else "shared-memory") + " x sweep, " + \
+                    ("balanced runs per CTA" if bal else "items")
                 tuning[str(l)] = {"tile_octs": rec[0], "ctas_per_sm": rec[1],
                                   "sweep_ms": {"4x4x2": [round(x, 4) for x in rec[2][0][:3]],
                                                "2x2x2": [round(x, 4) for x in rec[2][1][:3]],
                                                "column_planes_2_4_8_16_32_64": [round(x, 4) for x in csweep],
-                                               "column_x_sweep_shared_memory_warp_shuffle": [round(x, 4) for x in xms]},
-                                  "kernel": f"column ({planes} planes per item, {sweep} x sweep)" if planes else "brick"}
+                                               "column_x_sweep_shared_memory_warp_shuffle": [round(x, 4) for x in xms],
+                                               "column_items_balanced": [round(x, 4) for x in bms]},
+                                  "kernel": f"column ({planes} planes per item, {sweep})" if planes else "brick"}
                 kernels.add(f"column_kernel<2, {'true' if xs else 'false'}>" if planes else
                             ("level_batch_kernel<MathF32>" if prec == PREC_MIXED else "level_batch_kernel<MathF64>"))
         init_states = {l: r.state(l) for l in levels}

@@ -24,7 +24,7 @@ class EmmaHydroOptions(ctypes.Structure):
     _fields_ = [("precision", c_int), ("trans_flags", c_int), ("cfl", c_double),
                 ("tile_octs", c_int), ("device", c_int), ("use_graph", c_int), ("gravity", c_int),
                 ("dual_energy", c_int), ("column", c_int), ("fused_step", c_int),
-                ("column_xshfl", c_int)]
+                ("column_xshfl", c_int), ("column_balanced", c_int)]
 
 
 PREC_FP64, PREC_MIXED = 0, 1
@@ -92,6 +92,7 @@ SIGNATURES = [
     ("emma_hydro_tuning", c_int, [c_int, P(c_int), P(c_int), c_void_p]),
     ("emma_hydro_column_tuning", c_int, [c_int, P(c_int), c_void_p]),
     ("emma_hydro_column_xshfl", c_int, [c_int, P(c_int), c_void_p]),
+    ("emma_hydro_column_balanced", c_int, [c_int, P(c_int), c_void_p]),
     ("emma_hydro_probe_wait_timeout", c_int, [c_ll]),
     ("emma_hydro_plan_stats", c_int, [c_void_p, c_int, c_int, c_int, c_void_p]),
     ("emma_hydro_level_dt_noalloc", c_int, [c_void_p, c_ll, c_int, c_double, c_void_p, P(c_double)]),

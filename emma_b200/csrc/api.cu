@@ -90,6 +90,8 @@ struct DevLevel {
   double col_sweep_ms[6] = {};  // planes per item 2, 4, 8, 16, 32, 64 (0 = not tried)
   int col_xs = 0;               // the autotuner's x sweep: 1 warp shuffles, 0 shared memory
   double col_xs_ms[2] = {};     // its times of the two at col_nz (0 = not timed)
+  int col_bal = 0;              // the autotuner's work split: 1 balanced runs, 0 items
+  double col_bal_ms[2] = {};    // its times of the two (0 = not timed)
   long long nv = 0;
   int shape = 0;        // brick shape of the plan (kShapes)
   int ctas = 0;         // CTAs per SM of its launches (0: the occupancy limit)
@@ -143,7 +145,7 @@ struct Ctx {
   int *d_work_all = nullptr;     // batched work list, finest level first
   int nwork_all = 0;
   cudaGraphExec_t graph = nullptr;
-  int graph_nsub = -1, graph_prec = -1, graph_col = -2, graph_colx = -2, graph_groups = -3;
+  int graph_nsub = -1, graph_prec = -1, graph_col = -2, graph_colx = -2, graph_colb = -2, graph_groups = -3;
   bool graph_is_fused = false;   // the captured coarse step is one fused kernel
   int graph_kernels = 0;         // kernel nodes of the captured coarse step
   // drop-in cache: one mirror of levels L-1..L+1 per advanced level L, so that a
@@ -372,6 +374,7 @@ void drop_graph() {
   g.graph_nsub = g.graph_prec = -1;
   g.graph_col = -2;
   g.graph_colx = -2;
+  g.graph_colb = -2;
   g.graph_groups = -3;
   g.graph_is_fused = false;
   g.graph_kernels = 0;
@@ -743,7 +746,13 @@ int column_xs(int L) {
   return g.opt.column > 0 ? 0 : g.res.lev[L].col_xs;
 }
 
-cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl, int xs = -1) {
+// work split of the column-kernel launches of resident level L (ColumnArgs::balanced)
+int column_bal(int L) {
+  if (g.opt.column_balanced != 0) return g.opt.column_balanced > 0 ? 1 : 0;
+  return g.opt.column > 0 ? 0 : g.res.lev[L].col_bal;
+}
+
+cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl, int xs = -1, int bal = -1) {
   const DevLevel &d = g.res.lev[L];
   ColumnArgs c;
   c.lv = g.res.d_lv + L;
@@ -752,7 +761,13 @@ cudaError_t launch_column(int L, int nz, const int *gate, bool fuse_cfl, int xs 
   c.n = d.col_n;
   c.nz = nz;
   c.ncol = 2 * d.col_n / kColumnWidth;
-  c.nitems = (int)column_items(d, nz);
+  c.balanced = bal >= 0 ? bal : column_bal(L);
+  if (c.balanced) {  // the kernel's two CTAs per SM, runs of at least 16 column-planes
+    const long long ncol = 2LL * d.col_n / kColumnWidth, planes = ncol * ncol * 2LL * d.col_n;
+    c.nitems = (int)std::max(1LL, std::min(2LL * g.nsm, planes / 16));
+  } else {
+    c.nitems = (int)column_items(d, nz);
+  }
   c.gate = gate;
   c.status = g.d_status;
   c.smax = fuse_cfl ? g.d_S->smax_next : nullptr;
@@ -972,7 +987,7 @@ bool emit_coarse_step(int nsub) {
 
 bool ensure_graph(int nsub) {
   if (g.graph && g.graph_nsub == nsub && g.graph_prec == g.opt.precision && g.graph_col == g.opt.column &&
-      g.graph_colx == g.opt.column_xshfl &&
+      g.graph_colx == g.opt.column_xshfl && g.graph_colb == g.opt.column_balanced &&
       g.graph_groups == g.step_groups)
     return true;
   drop_graph();
@@ -1004,6 +1019,7 @@ bool ensure_graph(int nsub) {
   g.graph_prec = g.opt.precision;
   g.graph_col = g.opt.column;
   g.graph_colx = g.opt.column_xshfl;
+  g.graph_colb = g.opt.column_balanced;
   g.graph_groups = g.step_groups;
   g.graph_kernels = kn;
   return true;
@@ -1089,6 +1105,7 @@ void emma_hydro_default_options(struct EmmaHydroOptions *opt) {
   opt->column = 0;
   opt->fused_step = 0;
   opt->column_xshfl = 0;
+  opt->column_balanced = 0;
 }
 
 int emma_hydro_init(const struct EmmaHydroOptions *opt) {
@@ -1362,6 +1379,25 @@ bool autotune_tree(Tree &t, int shape_req) {
         d.col_xs_ms[1] = ms;
         if (ok && ms > 0 && ms < best_col) {
           d.col_xs = 1;
+          best_col = ms;
+        }
+      }
+      // balanced runs of column-planes (the chosen x sweep) against the items
+      d.col_bal = 0;
+      d.col_bal_ms[0] = best_col;
+      d.col_bal_ms[1] = 0;
+      if (ok && best_nz > 0) {
+        double ms = 0;
+        for (int rep = 0; rep < 4 && ok; rep++) {
+          ok = ck(cudaEventRecord(e0, g.stream), "event") &&
+               ck(launch_column(L, best_nz, nullptr, false, d.col_xs, 1), "column") &&
+               ck(cudaEventRecord(e1, g.stream), "event") && ck(cudaEventSynchronize(e1), "event");
+          float f = 0;
+          if (ok && rep > 0 && cudaEventElapsedTime(&f, e0, e1) == cudaSuccess) ms += f / 3.;
+        }
+        d.col_bal_ms[1] = ms;
+        if (ok && ms > 0 && ms < best_col) {
+          d.col_bal = 1;
           best_col = ms;
         }
       }
@@ -1978,6 +2014,17 @@ int emma_hydro_column_xshfl(int level, int *xshfl, double *ms) {
   if (ms) {
     ms[0] = d.col_xs_ms[0];
     ms[1] = d.col_xs_ms[1];
+  }
+  return 0;
+}
+
+int emma_hydro_column_balanced(int level, int *balanced, double *ms) {
+  if (!level_ok(level)) return EMMA_ST_ARG;
+  const DevLevel &d = g.res.lev[level];
+  if (balanced) *balanced = column_nz(level) > 0 ? column_bal(level) : 0;
+  if (ms) {
+    ms[0] = d.col_bal_ms[0];
+    ms[1] = d.col_bal_ms[1];
   }
   return 0;
 }

@@ -120,8 +120,7 @@ __global__ void __launch_bounds__(col::kColThreads, MINB) column_kernel(const Co
   unsigned st = 0;
   double wmax = 0.;  // exact max signal speed of the cells this warp wrote (warp-uniform)
 
-  const int cx = item % a.ncol, cy = (item / a.ncol) % a.ncol, cz = item / (a.ncol * a.ncol);
-  const int x0 = cx * TX, y0 = cy * TY, z0 = cz * a.nz, z1 = z0 + a.nz;
+  int x0 = 0, y0 = 0;  // the column of the current segment (first cell in x, y)
 
   // this thread's cell (column or ring) and the second column it converts (ring
   // threads: an outer halo column; four column threads: a ring corner column)
@@ -147,9 +146,7 @@ __global__ void __launch_bounds__(col::kColThreads, MINB) column_kernel(const Co
     oxy = (yg >> 1) * n + (xg >> 1);
     cxy = (xg & 1) | ((yg & 1) << 1);
   };
-  int oxy1, cxy1, oxy2, cxy2;
-  xy_part(rx, ry, oxy1, cxy1);
-  xy_part(hx, hy, oxy2, cxy2);
+  int oxy1 = 0, cxy1 = 0, oxy2 = 0, cxy2 = 0;  // set per segment
   auto gidx = [&](int oxy, int cxy, int z) -> long long {
     const int zg = z & cmask;
     const int o = __ldg(octidx + (zg >> 1) * nn + oxy);
@@ -283,120 +280,149 @@ __global__ void __launch_bounds__(col::kColThreads, MINB) column_kernel(const Co
 
   // P slots of planes z-1, z, z+1 rotate through 0..2 (plane z in slot z mod 3)
   auto mod3 = [](int z) { return ((z % 3) + 3) % 3; };
-  // prologue: the two planes below the first reconstructed one
-  {
-    double q[5];
-    for (int z = z0 - 2; z < z0; z++) {
-      load5(gidx(oxy1, cxy1, z), q);
-      pstore(mod3(z), rp, q);
-      if (conv2) {
-        load5(gidx(oxy2, cxy2, z), q);
-        pstore(mod3(z), hp, q);
-      }
-    }
-  }
-  __syncthreads();
-
-  int sc = mod3(z0);  // P slot of the plane converted in this step (s + 3)
-  for (int s = z0 - 3; s < z1; s++) {
-    // ---------------------------------------------------------------- A
-    // loads of plane s+3 first; they land while the faces of plane s+1 are solved
-    const bool conv = s + 3 <= z1 + 1;
-    double q1[5], q2[5];
-    if (conv) {
-      load5(gidx(oxy1, cxy1, s + 3), q1);
-      if (conv2) load5(gidx(oxy2, cxy2, s + 3), q2);
-    }
-    const int zs = s + 1;  // plane whose faces are solved
-    if (zs >= z0 && zs <= z1) {
-      const float4 *Rc = Rg + (zs & 1) * 5 * kRec, *Rb = Rg + ((zs - 1) & 1) * 5 * kRec;
-      const int fb = (zs & 1) * 3 * kFl;
-      if (zs < z1) {  // the plane above the column only closes its top face
-        if constexpr (XS)
-          if (interior) solve_x_shfl(Rc, fb);
-        if (solve_x) solve(std::integral_constant<int, 0>{}, Rc, lx, Rc, rxc, fb + ex);
-        if (solve_y) solve(std::integral_constant<int, 1>{}, Rc, ly, Rc, tid, fb + kFl + ey);
-      }
-      if (interior) solve(std::integral_constant<int, 2>{}, Rb, tid, Rc, tid, fb + 2 * kFl + tid);
-    }
-    if (conv) {
-      pstore(sc, rp, q1);
-      if (conv2) pstore(sc, hp, q2);
-    }
-    __syncthreads();
-    // ---------------------------------------------------------------- B
-    // the FP64 state of plane s is loaded first (from L2: the plane was staged three
-    // steps ago) and lands while plane s+2 is reconstructed
-    const bool upd = s >= z0 && interior;
-    long long gi = 0;
-    double q[5];
-    if (upd) {
-      gi = gidx(oxy1, cxy1, s);
-      load5(gi, q);
-    }
-    const int zr = s + 2;  // plane reconstructed
-    if (zr >= z0 - 1 && zr <= z1) {
-      const int s0 = mod3(zr);
-      reconstruct(s0, s0 == 0 ? 2 : s0 - 1, s0 == 2 ? 0 : s0 + 1, Rg + (zr & 1) * 5 * kRec);
-    }
-    if (upd) {
-      // fluxes of the six faces, -x,+x,-y,+y,-z,+z, summed in FP64 with the signs of
-      // updatefield (src/hydro_utils.c:3050-3082)
-      const int fs = (s & 1) * 3 * kFl, fn = ((s + 1) & 1) * 3 * kFl;
-      const int ef[6] = {fs + tid, fs + px, fs + kFl + tid, fs + kFl + py, fs + 2 * kFl + tid, fn + 2 * kFl + tid};
-      double dU[5] = {0., 0., 0., 0., 0.};
-#pragma unroll
-      for (int k = 0; k < 6; k++) {
-        const float4 f = F4[ef[k]];
-        const float f4 = F1[ef[k]];
-        const double F[5] = {(double)f.x, (double)f.y, (double)f.z, (double)f.w, (double)f4};
-#pragma unroll
-        for (int v = 0; v < 5; v++) dU[v] = (k & 1) ? dU[v] - F[v] : dU[v] + F[v];
-      }
-      // conserved state W2U(W) + dU dt/dx (src/hydro_utils.c:3129-3188).  The mixed
-      // path's compensated sum of the base state and the flux divergence (the brick
-      // kernel's, which also adds the corrections of a finer level) returns the
-      // rounded sum when there are only these two terms, as on a level without split
-      // cells: the compensation term is below half an ulp of the rounded sum.
-      const double Ud = q[0] + dU[0] * dtsurdx;
-      const double Udu = q[0] * q[1] + dU[1] * dtsurdx;
-      const double Udv = q[0] * q[2] + dU[2] * dtsurdx;
-      const double Udw = q[0] * q[3] + dU[3] * dtsurdx;
-      const double UE = (q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3])) + dU[4] * dtsurdx;
-      // U2W (src/hydro_utils.c:35-64), pressure floor
-      const double dl = (Ud == 0. ? 10. : Ud);
-      const double inv = 1. / dl;
-      double Wout[5];
-      Wout[0] = Ud;
-      Wout[1] = Udu * inv;
-      Wout[2] = Udv * inv;
-      Wout[3] = Udw * inv;
-      Wout[4] = fmax((kGam - 1.) * (UE - (Udu * Udu + Udv * Udv + Udw * Udw) * inv * 0.5), kPmin);
-      if (isnan(Wout[1]) || isnan(Wout[4]) || isnan(Wout[0])) st |= kStNan;
-#pragma unroll
-      for (int v = 0; v < 5; v++) Wn[v * N8 + gi] = Wout[v];
-      if (a.smax != nullptr) {
-        // the next CFL step's |v| + c_s (src/advanceamr.c:122-128), exact in FP64 for
-        // every cell that may raise this warp's maximum: an FP32 estimate (relative
-        // error below 2e-6) screens the others out, whole warps at a time
-        const float u = (float)Wout[1], v = (float)Wout[2], w = (float)Wout[3];
-        const float s32 = sqrtf(u * u + v * v + w * w) + sqrtf(5.f / 3.f * (float)Wout[4] / (float)Wout[0]);
-        const bool cand = !(s32 < (float)wmax * (1.f - 1e-5f));
-        if (__any_sync(0xffffffffu, cand)) {
-          double ex = 0.;
-          if (cand) {
-            const double va = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Wout[1], Wout[1]), __dmul_rn(Wout[2], Wout[2])),
-                                                   __dmul_rn(Wout[3], Wout[3])));
-            const double aa = __dsqrt_rn(__ddiv_rn(__dmul_rn(5. / 3., Wout[4]), Wout[0]));
-            ex = fmax(0., __dadd_rn(va, aa));  // fmax drops NaN like the reference's FMAX
-          }
-          for (int o = 16; o > 0; o >>= 1) ex = fmax(ex, __shfl_xor_sync(0xffffffffu, ex, o));
-          wmax = fmax(wmax, ex);
+  // One segment: planes [z0, z1) of the column (cx, cy), the two planes below and
+  // one above it staged and reconstructed as its halo.  The result of a face or
+  // cell does not depend on where a segment starts or ends.
+  auto segment = [&](int cx, int cy, int z0, int z1) {
+    x0 = cx * TX;
+    y0 = cy * TY;
+    xy_part(rx, ry, oxy1, cxy1);
+    xy_part(hx, hy, oxy2, cxy2);
+    // prologue: the two planes below the first reconstructed one
+    {
+      double q[5];
+      for (int z = z0 - 2; z < z0; z++) {
+        load5(gidx(oxy1, cxy1, z), q);
+        pstore(mod3(z), rp, q);
+        if (conv2) {
+          load5(gidx(oxy2, cxy2, z), q);
+          pstore(mod3(z), hp, q);
         }
       }
     }
     __syncthreads();
-    sc = (sc == 2) ? 0 : sc + 1;
+
+    int sc = mod3(z0);  // P slot of the plane converted in this step (s + 3)
+    for (int s = z0 - 3; s < z1; s++) {
+      // ---------------------------------------------------------------- A
+      // loads of plane s+3 first; they land while the faces of plane s+1 are solved
+      const bool conv = s + 3 <= z1 + 1;
+      double q1[5], q2[5];
+      if (conv) {
+        load5(gidx(oxy1, cxy1, s + 3), q1);
+        if (conv2) load5(gidx(oxy2, cxy2, s + 3), q2);
+      }
+      const int zs = s + 1;  // plane whose faces are solved
+      if (zs >= z0 && zs <= z1) {
+        const float4 *Rc = Rg + (zs & 1) * 5 * kRec, *Rb = Rg + ((zs - 1) & 1) * 5 * kRec;
+        const int fb = (zs & 1) * 3 * kFl;
+        if (zs < z1) {  // the plane above the column only closes its top face
+          if constexpr (XS)
+            if (interior) solve_x_shfl(Rc, fb);
+          if (solve_x) solve(std::integral_constant<int, 0>{}, Rc, lx, Rc, rxc, fb + ex);
+          if (solve_y) solve(std::integral_constant<int, 1>{}, Rc, ly, Rc, tid, fb + kFl + ey);
+        }
+        if (interior) solve(std::integral_constant<int, 2>{}, Rb, tid, Rc, tid, fb + 2 * kFl + tid);
+      }
+      if (conv) {
+        pstore(sc, rp, q1);
+        if (conv2) pstore(sc, hp, q2);
+      }
+      __syncthreads();
+      // ---------------------------------------------------------------- B
+      // the FP64 state of plane s is loaded first (from L2: the plane was staged three
+      // steps ago) and lands while plane s+2 is reconstructed
+      const bool upd = s >= z0 && interior;
+      long long gi = 0;
+      double q[5];
+      if (upd) {
+        gi = gidx(oxy1, cxy1, s);
+        load5(gi, q);
+      }
+      const int zr = s + 2;  // plane reconstructed
+      if (zr >= z0 - 1 && zr <= z1) {
+        const int s0 = mod3(zr);
+        reconstruct(s0, s0 == 0 ? 2 : s0 - 1, s0 == 2 ? 0 : s0 + 1, Rg + (zr & 1) * 5 * kRec);
+      }
+      if (upd) {
+        // fluxes of the six faces, -x,+x,-y,+y,-z,+z, summed in FP64 with the signs of
+        // updatefield (src/hydro_utils.c:3050-3082)
+        const int fs = (s & 1) * 3 * kFl, fn = ((s + 1) & 1) * 3 * kFl;
+        const int ef[6] = {fs + tid, fs + px, fs + kFl + tid, fs + kFl + py, fs + 2 * kFl + tid, fn + 2 * kFl + tid};
+        double dU[5] = {0., 0., 0., 0., 0.};
+  #pragma unroll
+        for (int k = 0; k < 6; k++) {
+          const float4 f = F4[ef[k]];
+          const float f4 = F1[ef[k]];
+          const double F[5] = {(double)f.x, (double)f.y, (double)f.z, (double)f.w, (double)f4};
+  #pragma unroll
+          for (int v = 0; v < 5; v++) dU[v] = (k & 1) ? dU[v] - F[v] : dU[v] + F[v];
+        }
+        // conserved state W2U(W) + dU dt/dx (src/hydro_utils.c:3129-3188).  The mixed
+        // path's compensated sum of the base state and the flux divergence (the brick
+        // kernel's, which also adds the corrections of a finer level) returns the
+        // rounded sum when there are only these two terms, as on a level without split
+        // cells: the compensation term is below half an ulp of the rounded sum.
+        const double Ud = q[0] + dU[0] * dtsurdx;
+        const double Udu = q[0] * q[1] + dU[1] * dtsurdx;
+        const double Udv = q[0] * q[2] + dU[2] * dtsurdx;
+        const double Udw = q[0] * q[3] + dU[3] * dtsurdx;
+        const double UE = (q[4] / (kGam - 1.) + 0.5 * q[0] * (q[1] * q[1] + q[2] * q[2] + q[3] * q[3])) + dU[4] * dtsurdx;
+        // U2W (src/hydro_utils.c:35-64), pressure floor
+        const double dl = (Ud == 0. ? 10. : Ud);
+        const double inv = 1. / dl;
+        double Wout[5];
+        Wout[0] = Ud;
+        Wout[1] = Udu * inv;
+        Wout[2] = Udv * inv;
+        Wout[3] = Udw * inv;
+        Wout[4] = fmax((kGam - 1.) * (UE - (Udu * Udu + Udv * Udv + Udw * Udw) * inv * 0.5), kPmin);
+        if (isnan(Wout[1]) || isnan(Wout[4]) || isnan(Wout[0])) st |= kStNan;
+  #pragma unroll
+        for (int v = 0; v < 5; v++) Wn[v * N8 + gi] = Wout[v];
+        if (a.smax != nullptr) {
+          // the next CFL step's |v| + c_s (src/advanceamr.c:122-128), exact in FP64 for
+          // every cell that may raise this warp's maximum: an FP32 estimate (relative
+          // error below 2e-6) screens the others out, whole warps at a time
+          const float u = (float)Wout[1], v = (float)Wout[2], w = (float)Wout[3];
+          const float s32 = sqrtf(u * u + v * v + w * w) + sqrtf(5.f / 3.f * (float)Wout[4] / (float)Wout[0]);
+          const bool cand = !(s32 < (float)wmax * (1.f - 1e-5f));
+          if (__any_sync(0xffffffffu, cand)) {
+            double ex = 0.;
+            if (cand) {
+              const double va = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(Wout[1], Wout[1]), __dmul_rn(Wout[2], Wout[2])),
+                                                     __dmul_rn(Wout[3], Wout[3])));
+              const double aa = __dsqrt_rn(__ddiv_rn(__dmul_rn(5. / 3., Wout[4]), Wout[0]));
+              ex = fmax(0., __dadd_rn(va, aa));  // fmax drops NaN like the reference's FMAX
+            }
+            for (int o = 16; o > 0; o >>= 1) ex = fmax(ex, __shfl_xor_sync(0xffffffffu, ex, o));
+            wmax = fmax(wmax, ex);
+          }
+        }
+      }
+      __syncthreads();
+      sc = (sc == 2) ? 0 : sc + 1;
+    }
+  };
+  // this CTA's range of the level's column-planes (columns in order, each bottom
+  // to top): an item (one column, nz planes), or an equal share of all of them cut
+  // into segments where it crosses into the next column
+  const int per_col = 2 * n;
+  int p0, p1;
+  if (a.balanced) {
+    const long long total = (long long)a.ncol * a.ncol * per_col;
+    p0 = (int)(total * blockIdx.x / gridDim.x);
+    p1 = (int)(total * (blockIdx.x + 1) / gridDim.x);
+  } else {
+    const int cz = item / (a.ncol * a.ncol), col = item % (a.ncol * a.ncol);
+    p0 = col * per_col + cz * a.nz;
+    p1 = p0 + a.nz;
+  }
+  for (int pos = p0; pos < p1;) {
+    const int col = pos / per_col, z = pos - col * per_col;
+    const int zend = (p1 - pos < per_col - z) ? z + (p1 - pos) : per_col;
+    segment(col % a.ncol, col / a.ncol, z, zend);
+    pos += zend - z;
   }
   if (a.smax != nullptr && interior && (tid & 31) == 0 && wmax > 0.)
     atomicMax(a.smax + a.L, (unsigned long long)__double_as_longlong(wmax));

@@ -151,6 +151,7 @@ struct ColumnArgs {
   unsigned *status;
   unsigned long long *smax;  // [L]: max signal speed of the new state (bits of a double), or null
   int xshfl;            // x faces inside the column through warp shuffles (column_kernel.cuh XS)
+  int balanced;         // nitems CTAs, each an equal run of the level's column-planes (nz unused)
 };
 constexpr int kColumnWidth = 16;  // cells per column side
 

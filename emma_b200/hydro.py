@@ -13,7 +13,7 @@ from ._lib import EmmaHydroOptions, PREC_FP64, PREC_MIXED, check, lib, ptr
 
 
 def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, tile_octs=0, gravity=False,
-            dual=False, column=0, fused="auto", xshfl=0):
+            dual=False, column=0, fused="auto", xshfl=0, balanced=0):
     """tile_octs: 0 = brick shape autotuned per level at upload, 32 = 4x4x2-oct
     bricks, 8 = 2x2x2-oct bricks (four per tile).  gravity: the -DWGRAV coupling
     (forces from ResidentHydro.set_force).  dual: the -DDUAL_E tracked internal energy.
@@ -24,7 +24,9 @@ def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, ti
     persistent kernel per coarse step) or the level schedule's separate launches,
     True = fused with as many tile groups per CTA as fit, an int k = fused with k
     groups, False = separate launches.  xshfl (column kernel's x sweep): 0 = the
-    autotuner's pick, 1 = warp shuffles, -1 = shared memory."""
+    autotuner's pick, 1 = warp shuffles, -1 = shared memory.  balanced (column
+    kernel's work split): 0 = the autotuner's pick, 1 = an equal run of the level's
+    column-planes per CTA, -1 = items of the chosen depth."""
     o = EmmaHydroOptions()
     lib().emma_hydro_default_options(ctypes.byref(o))
     o.precision, o.trans_flags, o.cfl, o.device = precision, trans, cfl, device
@@ -34,6 +36,7 @@ def options(precision=PREC_FP64, trans=0, cfl=0.85, device=0, use_graph=True, ti
     o.dual_energy = 1 if dual else 0
     o.column = column
     o.column_xshfl = xshfl
+    o.column_balanced = balanced
     if fused == "auto":
         o.fused_step = 0
     elif fused is True:
@@ -49,10 +52,11 @@ class ResidentHydro:
     """Levels lcoarse..lmax of an oct tree resident on the GPU."""
 
     def __init__(self, tree, precision=PREC_FP64, trans=0, cfl=0.85, rank=0, use_graph=True, tile_octs=0,
-                 gravity=False, dual=False, column=0, fused="auto", xshfl=0):
+                 gravity=False, dual=False, column=0, fused="auto", xshfl=0, balanced=0):
         self.tree = tree
         self.column = column
         self.xshfl = xshfl
+        self.balanced = balanced
         self.fused = fused
         self.gravity, self.dual = gravity, dual
         self.lcoarse, self.lmax = tree.lcoarse, tree.lmax
@@ -71,7 +75,7 @@ class ResidentHydro:
     def _options(self):
         return options(self.precision, self.trans, self.cfl, use_graph=self.use_graph, tile_octs=self.tile_octs,
                        gravity=self.gravity, dual=self.dual, column=self.column, fused=self.fused,
-                       xshfl=self.xshfl)
+                       xshfl=self.xshfl, balanced=self.balanced)
 
     def _apply(self):
         o = self._options()
@@ -192,6 +196,15 @@ class ResidentHydro:
         on = ctypes.c_int()
         ms = np.zeros(2)
         check(self._L.emma_hydro_column_xshfl(level, ctypes.byref(on), ptr(ms)), "column_xshfl")
+        return on.value, ms
+
+    def column_balanced(self, level):
+        """(1 if the level's column-kernel launches give each CTA an equal run of the
+        level's column-planes, 0 for items of the chosen depth; the autotuner's ms per
+        launch of the items and the balanced runs, 0 = not timed)."""
+        on = ctypes.c_int()
+        ms = np.zeros(2)
+        check(self._L.emma_hydro_column_balanced(level, ctypes.byref(on), ptr(ms)), "column_balanced")
         return on.value, ms
 
     def set_column(self, column, xshfl=None):

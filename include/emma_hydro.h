@@ -90,6 +90,10 @@ struct EmmaHydroOptions {
                            from the left cell's face state passed up a lane by a warp shuffle
                            (1) or read from shared memory (-1); 0 = the faster of the two at
                            the autotuned depth (shared memory when `column` forces a depth) */
+  int column_balanced;  /* work of the column kernel: two CTAs per SM, each an equal run of the
+                           level's column-planes (1), or items of `nz` planes handed out by the
+                           block scheduler (-1); 0 = the faster of the two (items when `column`
+                           forces a depth) */
 };
 void emma_hydro_default_options(struct EmmaHydroOptions *opt);
 
@@ -300,6 +304,11 @@ int emma_hydro_column_tuning(int level, int *planes, double *sweep_ms);
  * they read them from shared memory; ms[2] = the autotuner's ms per launch of the
  * shared-memory and the shuffle sweep at the chosen depth (0 = not timed). */
 int emma_hydro_column_xshfl(int level, int *xshfl, double *ms);
+/* The column kernel's work split on a resident level (no reference counterpart):
+ * *balanced = 1 when its launches give every CTA (two per SM) an equal run of the
+ * level's column-planes, 0 for items of the chosen depth; ms[2] = the autotuner's
+ * ms per launch of the two (0 = not timed). */
+int emma_hydro_column_balanced(int level, int *balanced, double *ms);
 /* Autotuner record of a resident level (emma_hydro_tree_upload tunes every
  * level when options.tile_octs == 0): the chosen brick (32 = 4x4x2 octs, one
  * per tile; 8 = 2x2x2 octs, four per tile), the CTAs per SM of its launches,

@@ -8,7 +8,9 @@ bits from both).  Against the brick kernel of the same path: L1 <= 1e-6.  The
 next step's dt from the maximum fused into the kernel equals the FP64
 reduction's over the state it wrote, bit for bit.  The warp-shuffle x sweep
 (x face states passed up a lane, the column's x boundary faces solved by the
-ring threads) meets the same bars and matches the shared-memory sweep.
+ring threads) meets the same bars and matches the shared-memory sweep.  Balanced
+runs of column-planes per CTA (segments that start and end anywhere in a column)
+give the same bits as items of a fixed depth.
 """
 import numpy as np
 import pytest
@@ -109,15 +111,40 @@ def test_autotuner_sweeps_the_column_kernel(gpu):
     best_brick = brick[brick > 0].min()
     best_col = sweep[sweep > 0].min()
     xs, xms = r.column_xshfl(cfg.lcoarse)
-    # the shuffle x sweep timed at the best depth against the shared-memory one
+    bal, bms = r.column_balanced(cfg.lcoarse)
+    # the shuffle x sweep timed at the best depth against the shared-memory one,
+    # then balanced runs (with the faster sweep) against the items
     assert xms[0] == best_col and xms[1] > 0
-    best = min(xms)
+    assert bms[0] == min(xms) and bms[1] > 0
+    best = min(bms)
     if planes:
         assert sweep[[2, 4, 8, 16, 32, 64].index(planes)] == best_col
         assert xs == (1 if xms[1] < xms[0] else 0)
+        assert bal == (1 if bms[1] < bms[0] else 0)
         assert best <= best_brick
     else:
-        assert xs == 0 and best >= best_brick
+        assert xs == 0 and bal == 0 and best >= best_brick
+
+
+@pytest.mark.parametrize("level,xs", [(5, -1), (6, 1), (7, -1), (7, 1)])
+def test_column_balanced_runs_equal_items(gpu, level, xs):
+    cfg = configs.random_uniform(level=level)
+    out = {}
+    for bal in (-1, 1):
+        t = cfg.build()
+        m0, e0 = totals(t.get_fields(level)[:5], level)
+        r = ResidentHydro(t, precision=PREC_MIXED, cfl=CFL, column=8, xshfl=xs, balanced=bal)
+        assert r.column_balanced(level)[0] == (1 if bal > 0 else 0)
+        for _ in range(3):
+            r.coarse_step()
+        assert r.status() == 0
+        fm = r.state(level)
+        m1, e1 = totals(fm, level)
+        assert abs(m1 - m0) <= 1e-12 * m0
+        assert abs(e1 - e0) <= 1e-12 * e0
+        out[bal] = (fm, r.tsim)
+    assert np.array_equal(out[1][0], out[-1][0])
+    assert out[1][1] == out[-1][1]
 
 
 @pytest.mark.parametrize("level,nz,with_oracle", [(5, 8, True), (6, 16, True), (7, 32, False)])
