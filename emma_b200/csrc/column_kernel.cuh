@@ -35,6 +35,12 @@
 // call site of the shared-memory sweep, so a face shared by two columns still
 // gets the same bits in both.  The autotuner times both sweeps.
 //
+// Work: a CTA runs either one item (column, nz planes) or, with
+// ColumnArgs::balanced, an equal share of all the level's column-planes (two
+// CTAs per SM, no partial last wave), cut into segments where it crosses into
+// the next column.  Each segment stages and reconstructs its own z halo; as no
+// face or cell depends on where a segment starts, both give the same bits.
+//
 // The reference does the same per oct on a 27-oct copy
 // (src/hydro_utils.c:1407-2238, 2973-3303), recomputing each cell's
 // reconstruction up to 9 times and each face twice.
